@@ -1,0 +1,150 @@
+/*
+ * seren_gpu.h - C ABI of the B200 force hot path of the SEREN grad-h SPH code.
+ *
+ * One call replaces one OpenMP particle loop of the Fortran reference.  All
+ * arrays are HOST arrays laid out like the Fortran module arrays they replace:
+ * column-major Fortran parray(1:6,1:ptot) is C row-major parray[ptot][6] with
+ * columns x, y, z, m, h, zeta (headers/macros.h:44-55, NDIM=3 block);
+ * v(1:3,p) and a(1:3,p) are [ptot][3]; pplist(1:pp_limit,p) is
+ * [ptot][pp_limit].  Particle ids that cross the boundary (perm_out, pplist,
+ * acclist) use the base given in seren_gpu_params.index_base (1 for Fortran).
+ *
+ * Every function returns SEREN_GPU_OK (0) or one of the SEREN_GPU_ERR_* codes
+ * below; seren_gpu_last_error() gives a one-line reason.  No device code ever
+ * traps: walk caps and capacity limits set an error flag that the host reads.
+ * A context is not thread-safe; call it from one host thread (the Fortran
+ * master thread, outside !$OMP regions).  Each call synchronises its stream
+ * before returning.
+ */
+#ifndef SEREN_GPU_H
+#define SEREN_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SEREN_GPU_OK 0
+#define SEREN_GPU_ERR_ARG 1        /* bad argument or unsupported option         */
+#define SEREN_GPU_ERR_CAPACITY 2   /* ptot > pmax, or cell count > 2*pmax          */
+#define SEREN_GPU_ERR_LMAX 3       /* tree deeper than the supported level count   */
+#define SEREN_GPU_ERR_NONFINITE 4  /* NaN/Inf in positions, masses or h            */
+#define SEREN_GPU_ERR_WALK 5       /* a tree walk hit its iteration cap            */
+#define SEREN_GPU_ERR_NEGATIVE_H 6 /* grad-h produced h < 0 (all_sph_gradh.F90:486) */
+#define SEREN_GPU_ERR_CUDA 7       /* CUDA runtime error                           */
+#define SEREN_GPU_ERR_STATE 8      /* call made before the state it needs exists   */
+
+typedef struct seren_gpu_ctx seren_gpu_ctx;
+
+/* Runtime options of the hot path.  Values come from params.dat and the
+ * compile-time macros of the reference (setup/default_parameters.F90:104-117,
+ * setup/initialize_seren_variables_1.F90:30-39, headers/macros.h:138-139). */
+typedef struct {
+  int32_t ndim;        /* must be 3                                              */
+  int32_t kernel;      /* 0 = M4 (KERNEL=M4), 1 = M4 Thomas-Couchman (M4TC)      */
+  int32_t visc;        /* 0 = MON97 artificial viscosity                         */
+  int32_t precision;   /* 0 = FP64 throughout, 1 = mixed FP32 pair arithmetic    */
+  int32_t pp_gather;   /* target neighbour number (57 for h_fac = 1.2)           */
+  int32_t pp_limit;    /* neighbour-list width, 2*pp_gather                      */
+  int32_t leafmax;     /* must be 8 (LEAFMAX)                                    */
+  int32_t lmax;        /* maximum tree level, <= 30 (LMAX)                       */
+  int32_t index_base;  /* 1: Fortran ids (1..ptot); 0: C ids (0..ptot-1)         */
+  int32_t reserved;
+  double h_fac;        /* h = h_fac*(m/rho)^(1/3)                                */
+  double thetamaxsqd;  /* geometric MAC opening angle squared                    */
+  double alpha;        /* artificial viscosity alpha (beta is always 2*alpha)    */
+  double alpha_min;    /* unused by MON97 without time-dependent viscosity       */
+} seren_gpu_params;
+
+/* Context: device mirrors of the particle arrays, the gravity/hydro tree and
+ * scratch, sized for pmax particles.  Replaces allocate_memory.F90:43-221 for
+ * the arrays of the hot path. */
+int seren_gpu_create(seren_gpu_ctx** ctx, int64_t pmax, const seren_gpu_params* prm);
+void seren_gpu_destroy(seren_gpu_ctx* ctx);
+int seren_gpu_last_error(seren_gpu_ctx* ctx, char* buf, int32_t len);
+
+/* tree_update (main/tree_update.F90:27-60): when do_build != 0,
+ * BHgrav_build (BHtree/BHgrav_build.F90:12-309) and, when do_reorder != 0,
+ * BH_reorder_particles (BHtree/BH_reorder_particles.F90:57-123) with the
+ * device mirrors permuted; then BHgrav_stock (BHtree/BHgrav_stock.F90:11-358),
+ * copy_BHgrav_to_BHhydro and BHhydro_stock.  parray is uploaded first and,
+ * after a reorder, written back in tree order; perm_out[new] = old id
+ * (the reference's dummylist) when not NULL.  The stock uses the h in parray,
+ * i.e. the h from before this step's grad-h solve, as the reference does. */
+int seren_gpu_tree_update(seren_gpu_ctx* ctx, int32_t ptot, double* parray,
+                          int32_t do_build, int32_t do_reorder, int32_t* perm_out);
+
+/* sph_update, GRAD_H_SPH branch (sph_sim/sph_update.F90:57-100):
+ * [BHhydro_hguess when first_call] -> all_sph_gradh for the active particles
+ * -> BHhydro_update_hmax -> get_neib.  v is uploaded; parray columns h and
+ * zeta, rho, omega, div_v and drhodt are written back for the active
+ * particles.  pptot/pplist may be NULL (then the lists stay on the device for
+ * seren_gpu_hydro_forces).  acclist == NULL means every particle is active. */
+int seren_gpu_sph_update(seren_gpu_ctx* ctx, int32_t ptot, const int32_t* acclist,
+                         int32_t nacc, double* parray, const double* v, double* rho,
+                         double* omega, double* div_v, double* drhodt, int32_t* pptot,
+                         int32_t* pplist, int32_t first_call);
+
+/* get_neib alone (sph/get_neib.F90:10-140) after BHhydro_update_hmax, at the
+ * smoothing lengths h[ptot] given (NULL: the ones on the device). */
+int seren_gpu_get_neib(seren_gpu_ctx* ctx, int32_t ptot, const int32_t* acclist,
+                       int32_t nacc, const double* h, int32_t* pptot, int32_t* pplist);
+
+/* sph_hydro_forces (sph_sim/sph_hydro_forces.F90:41-85) with hydro_gradh
+ * (sph/hydro_gradh.F90:9-339, MON97): a[p] is OVERWRITTEN with the hydro
+ * acceleration of each active particle (inactive rows are left as they are). */
+int seren_gpu_hydro_forces(seren_gpu_ctx* ctx, const int32_t* acclist, int32_t nacc,
+                           const double* press, const double* sound, double* a);
+
+/* sph_grav_forces (sph_sim/sph_grav_forces.F90:94-157): BHgrav_accel with
+ * gravity_gradh (BHtree/BHgrav_accel.F90:21-348, gravity/gravity_gradh.F90)
+ * ADDED to a, gpot OVERWRITTEN with the (positive) potential; then, when
+ * nsink > 0, direct_sink_gravity (sinks/direct_sink_gravity.F90:10-64) with
+ * sink_rmh[s] = {x, y, z, m, h} added to a and gpot. */
+int seren_gpu_grav_forces(seren_gpu_ctx* ctx, const int32_t* acclist, int32_t nacc,
+                          double* a, double* gpot, int32_t nsink, const double* sink_rmh);
+
+/* sph_sink_forces (sph_sim/sph_sink_forces.F90:49-110): for each sink, the
+ * tree walk BHgrav_accel(-s) with gravity_meanh plus the sink-sink direct sum.
+ * sink_a[s][3] and sink_gpot[s] are overwritten. */
+int seren_gpu_sink_forces(seren_gpu_ctx* ctx, int32_t nsink, const double* sink_rmh,
+                          double* sink_a, double* sink_gpot);
+
+/* Device-resident force step, the path the Fortran caller reaches with
+ * positions kept on the device between steps: seren_gpu_upload() copies
+ * parray, v and csq = Pconst*T (isothermal c_s^2) once; seren_gpu_force_step()
+ * runs tree build + reorder + stock, [h guess], grad-h, hmax update,
+ * neighbour lists, isothermal thermal (sph/thermal.F90:52-59), hydro and
+ * gravity without touching the host; seren_gpu_drift() moves r += v*dt;
+ * seren_gpu_download() copies results back in tree order (any pointer may be
+ * NULL). */
+int seren_gpu_upload(seren_gpu_ctx* ctx, int32_t ptot, const double* parray,
+                     const double* v, const double* csq);
+int seren_gpu_force_step(seren_gpu_ctx* ctx, int32_t first_call);
+int seren_gpu_drift(seren_gpu_ctx* ctx, double dt);
+int seren_gpu_download(seren_gpu_ctx* ctx, double* parray, double* v, double* rho,
+                       double* omega, double* a, double* gpot, int32_t* perm_total);
+
+/* Tree inspection (BHgrav_node / BHhydro_node of headers/modules.F90:907-959
+ * in the reference's breadth-first cell numbering).  Counts first: pass NULL
+ * arrays to get ctot and ltot.  plist rows hold particle ids (index_base) and
+ * -1 past the leaf count; ifopen is -1 for leaves. */
+int seren_gpu_tree_export(seren_gpu_ctx* ctx, int32_t* ctot, int32_t* ltot,
+                          int32_t* leaf, int32_t* nextcell, int32_t* ifopen,
+                          int32_t* plist /*[ctot+1][8]*/, int32_t* first_cell,
+                          int32_t* last_cell, double* grav_r /*[ctot+1][3]*/,
+                          double* grav_m, double* grav_q /*[ctot+1][5]*/,
+                          double* dminsqd, double* hydro_r /*[ctot+1][3]*/,
+                          double* rmax, double* hrangemax);
+
+/* Per-stage device time of the last seren_gpu_force_step (ms) and the
+ * number of kernels it launched. */
+int seren_gpu_last_step_stats(seren_gpu_ctx* ctx, double* stage_ms /*[8]*/,
+                              int32_t* nlaunch);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SEREN_GPU_H */

@@ -1,0 +1,96 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes binding of the CPU oracle library.
+
+The oracle (oracle/seren_oracle.cpp) is a FP64 restatement of the reference's
+Fortran force path and is the checker for the CUDA library; only tests/,
+__graft_entry__.smoke() and bench.py's CPU-baseline leg use it.  Parity is
+unpinned: the reference ships no golden vectors and cannot be compiled here.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from seren_b200.cabi import HotPath, Params, bind
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "libseren_oracle.so")
+KERNTOT = 10000
+
+_lib = None
+
+
+class Counts(C.Structure):
+    _fields_ = [(n, C.c_int64) for n in (
+        "grav_cells", "grav_pairs", "grav_nodes", "gradh_tests", "gradh_pairs", "gradh_passes",
+        "gradh_walks", "gradh_final_tests", "gradh_final_pairs", "neib_tests", "neib_pairs",
+        "hydro_pairs", "hydro_visc")]
+
+    def as_dict(self):
+        return {n: int(getattr(self, n)) for n, _ in self._fields_}
+
+
+def build(force: bool = False) -> str:
+    """Compile the oracle with its Makefile (g++, -ffp-contract=off, OpenMP)."""
+    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(
+            os.path.getmtime(os.path.join(HERE, f)) for f in ("seren_oracle.cpp", "seren_oracle.h")):
+        subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB
+
+
+def library() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        build()
+        lib = bind(C.CDLL(LIB), "seren_oracle")
+        vp = C.c_void_p
+        lib.seren_oracle_set_threads.argtypes = [C.c_int32]
+        lib.seren_oracle_set_threads.restype = C.c_int
+        lib.seren_oracle_direct_gravity.argtypes = [vp, C.POINTER(C.c_int32), C.c_int32,
+                                                    C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        lib.seren_oracle_direct_gravity.restype = C.c_int
+        lib.seren_oracle_get_counts.argtypes = [vp, C.POINTER(Counts)]
+        lib.seren_oracle_get_counts.restype = C.c_int
+        lib.seren_oracle_kernel_tables.argtypes = [C.c_int32, C.POINTER(C.c_double)]
+        lib.seren_oracle_kernel_tables.restype = C.c_int
+        lib.seren_oracle_stage_seconds.argtypes = [vp, C.POINTER(C.c_double)]
+        lib.seren_oracle_stage_seconds.restype = C.c_int
+        _lib = lib
+    return _lib
+
+
+def set_threads(n: int) -> int:
+    return int(library().seren_oracle_set_threads(int(n)))
+
+
+def kernel_tables(kernel: int = 0) -> np.ndarray:
+    """[9, KERNTOT+1] = w0, w1, w2, w3, w4, w5, w6, wh, wg (setup/kernel.F90)."""
+    t = np.zeros((9, KERNTOT + 1))
+    library().seren_oracle_kernel_tables(kernel, t.ctypes.data_as(C.POINTER(C.c_double)))
+    return t
+
+
+class Oracle(HotPath):
+    def __init__(self, pmax: int, params: Params):
+        super().__init__(library(), "seren_oracle", pmax, params)
+
+    def counts(self) -> dict:
+        c = Counts()
+        self._call("get_counts", self._ctx, C.byref(c))
+        return c.as_dict()
+
+    def stage_seconds(self) -> list:
+        s = (C.c_double * 6)()
+        self._call("stage_seconds", self._ctx, s)
+        return list(s)
+
+    def direct_gravity(self, ids) -> tuple:
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
+        a = np.zeros((ids.size, 3))
+        g = np.zeros(ids.size)
+        self._call("direct_gravity", self._ctx, ids.ctypes.data_as(C.POINTER(C.c_int32)),
+                   ids.size, a.ctypes.data_as(C.POINTER(C.c_double)),
+                   g.ctypes.data_as(C.POINTER(C.c_double)))
+        return a, g

@@ -1,0 +1,670 @@
+// api.cu - the C ABI of include/seren_gpu.h: context management, host <->
+// device transfers and the order of the stages inside each call, which
+// follows the Fortran drivers the calls replace (sph_sim/sph_setup.F90:42-66,
+// main/tree_update.F90:27-60, sph_sim/sph_update.F90:57-100,
+// sph_sim/sph_hydro_forces.F90:41-85, sph_sim/sph_grav_forces.F90:94-157).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "ctx.cuh"
+
+struct seren_gpu_ctx {
+  seren::Ctx c;
+};
+
+namespace seren {
+namespace {
+
+inline int nb(long n, int t) { return (int)((n + t - 1) / t); }
+
+int fail(Ctx& c, int code, const char* msg) {
+  c.err = msg;
+  return code;
+}
+
+int cuda_fail(Ctx& c, cudaError_t e, const char* where) {
+  char buf[256];
+  std::snprintf(buf, sizeof(buf), "%s: %s", where, cudaGetErrorString(e));
+  c.err = buf;
+  return SEREN_GPU_ERR_CUDA;
+}
+
+// Wait for the stream, then turn a device error record into a status.
+int finish(Ctx& c, const char* where) {
+  cudaError_t e = cudaStreamSynchronize(c.st);
+  if (e != cudaSuccess) return cuda_fail(c, e, where);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(c, e, where);
+  DevError de;
+  e = cudaMemcpy(&de, c.d_err, sizeof(DevError), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(c, e, where);
+  if (de.code != 0) {
+    char buf[256];
+    static const char* kn[] = {"?", "bbox", "keys", "sort", "split", "emit", "reorder", "stock",
+                               "hguess", "gradh", "hmax", "neib", "hydro", "grav", "grav_mixed",
+                               "sink", "thermal"};
+    const char* k = (de.where >= 0 && de.where <= 16) ? kn[de.where] : "?";
+    const char* what = de.code == SEREN_GPU_ERR_NONFINITE ? "non-finite input"
+                       : de.code == SEREN_GPU_ERR_WALK     ? "walk or search cap reached"
+                       : de.code == SEREN_GPU_ERR_NEGATIVE_H ? "negative smoothing length"
+                                                             : "device error";
+    std::snprintf(buf, sizeof(buf), "%s: %s in kernel %s (index %d, aux %d)", where, what, k,
+                  de.index, de.aux);
+    c.err = buf;
+    cudaMemset(c.d_err, 0, sizeof(DevError));
+    return de.code;
+  }
+  return SEREN_GPU_OK;
+}
+
+template <class T>
+int alloc(T*& p, size_t n) {
+  return cudaMalloc(&p, sizeof(T) * std::max<size_t>(n, 1)) == cudaSuccess ? 0 : -1;
+}
+
+__global__ void k_unpack_v(const double* __restrict__ st, int n, double4* __restrict__ vel) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  vel[i] = make_double4(st[i * 3 + 0], st[i * 3 + 1], st[i * 3 + 2], 0.0);
+}
+
+__global__ void k_pack_v(double* __restrict__ st, int n, const double4* __restrict__ vel) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double4 v = vel[i];
+  st[i * 3 + 0] = v.x; st[i * 3 + 1] = v.y; st[i * 3 + 2] = v.z;
+}
+
+__global__ void k_iota(int* __restrict__ a, int n) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) a[i] = (int)i;
+}
+
+__global__ void k_set_h(const double* __restrict__ h, int n, double2* __restrict__ hz) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) hz[i].x = h[i];
+}
+
+__global__ void k_pack_hz(const double2* __restrict__ hz, int n, double* __restrict__ st) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  st[i * 2 + 0] = hz[i].x;
+  st[i * 2 + 1] = hz[i].y;
+}
+
+__global__ void k_add_base(const int* __restrict__ src, int* __restrict__ dst, long n, int base) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = src[i] + base;
+}
+
+__global__ void k_drift(int n, double4* __restrict__ pm, const double4* __restrict__ vel, double dt) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double4 p = pm[i];
+  const double4 v = vel[i];
+  p.x = p.x + v.x * dt;
+  p.y = p.y + v.y * dt;
+  p.z = p.z + v.z * dt;
+  pm[i] = p;
+}
+
+// Active list: NULL means all particles (returns nact = ptot and c.act unset).
+int set_active(Ctx& c, const int32_t* acclist, int32_t nacc, int& nact) {
+  c.act = nullptr;
+  if (acclist == nullptr) {
+    nact = c.ptot;
+    return SEREN_GPU_OK;
+  }
+  if (nacc < 0 || nacc > c.ptot) return fail(c, SEREN_GPU_ERR_ARG, "nacc out of range");
+  std::vector<int> a(nacc);
+  for (int i = 0; i < nacc; ++i) {
+    a[i] = acclist[i] - c.prm.index_base;
+    if (a[i] < 0 || a[i] >= c.ptot) return fail(c, SEREN_GPU_ERR_ARG, "acclist id out of range");
+  }
+  // the active buffer lives after the staging area
+  int* d = c.istage;
+  if (nacc > 0) cudaMemcpyAsync(d, a.data(), sizeof(int) * nacc, cudaMemcpyHostToDevice, c.st);
+  c.act = d;
+  nact = nacc;
+  return SEREN_GPU_OK;
+}
+
+// host staging buffer (pinned), grown on demand
+double* pinned(Ctx& c, size_t ndouble) {
+  static_assert(sizeof(double) == 8, "");
+  if (c.h_pin == nullptr) {
+    if (cudaMallocHost(&c.h_pin, sizeof(double) * (size_t)c.pmax * 6) != cudaSuccess) {
+      c.h_pin = nullptr;
+      return nullptr;
+    }
+  }
+  return ndouble <= (size_t)c.pmax * 6 ? c.h_pin : nullptr;
+}
+
+// copy rows of a device [ptot][w] double array to the host array, all rows
+// when every particle is active, else only the active rows
+int d2h_rows(Ctx& c, double* host, const double* dev, int w, const int32_t* acclist, int nact) {
+  const size_t n = (size_t)c.ptot * w;
+  if (acclist == nullptr) {
+    cudaMemcpyAsync(host, dev, sizeof(double) * n, cudaMemcpyDeviceToHost, c.st);
+    return SEREN_GPU_OK;
+  }
+  double* pin = pinned(c, n);
+  if (!pin) return fail(c, SEREN_GPU_ERR_CUDA, "pinned staging allocation failed");
+  cudaMemcpyAsync(pin, dev, sizeof(double) * n, cudaMemcpyDeviceToHost, c.st);
+  cudaError_t e = cudaStreamSynchronize(c.st);
+  if (e != cudaSuccess) return cuda_fail(c, e, "d2h_rows");
+  for (int i = 0; i < nact; ++i) {
+    const size_t p = (size_t)(acclist[i] - c.prm.index_base);
+    for (int k = 0; k < w; ++k) host[p * w + k] = pin[p * w + k];
+  }
+  return SEREN_GPU_OK;
+}
+
+int check_tree(Ctx& c, int32_t ptot) {
+  if (!c.have_tree) return fail(c, SEREN_GPU_ERR_STATE, "no tree: call seren_gpu_tree_update first");
+  if (ptot != c.ptot) return fail(c, SEREN_GPU_ERR_STATE, "ptot differs from the last tree_update");
+  return SEREN_GPU_OK;
+}
+
+void free_all(Ctx& c) {
+  void* ps[] = {c.pm, c.hz, c.vel, c.csq, c.orig, c.pm_alt, c.hz_alt, c.vel_alt, c.csq_alt,
+                c.orig_alt, c.rho, c.omega, c.div_v, c.drhodt, c.press, c.sound, c.acc, c.gpot,
+                c.pptot, c.pplist, c.stage, c.istage, c.keys, c.keys_alt, c.idx, c.idx_alt,
+                c.rs_hist, c.bbox_part, c.branch, c.branch_next, c.nchild, c.choff, c.cstart,
+                c.bflag, c.bscan, c.leaf, c.nextcell, c.ifopen, c.pstart, c.pcount, c.parent,
+                c.level, c.link, c.gA, c.gB, c.gC, c.hA, c.hrm, c.hmax, c.bbmin, c.bbmax, c.d_info,
+                c.d_err, c.d_counts, c.tabA, c.tabG, c.scan.total, c.scan.level_buf[0],
+                c.scan.level_buf[1], c.scan.level_buf[2], c.scan.level_buf[3]};
+  for (void* p : ps)
+    if (p) cudaFree(p);
+  if (c.h_pin) cudaFreeHost(c.h_pin);
+  for (auto& e : c.ev)
+    if (e) cudaEventDestroy(e);
+  if (c.st) cudaStreamDestroy(c.st);
+}
+
+int alloc_all(Ctx& c) {
+  const size_t P = (size_t)c.pmax;
+  const size_t C = (size_t)c.cmax + 1;
+  const size_t L = (size_t)c.prm.pp_limit;
+  const size_t nbr = P / 9 + 2;
+  const size_t rsblk = (P + 4095) / 4096;
+  int bad = 0;
+  bad |= alloc(c.pm, P) | alloc(c.hz, P) | alloc(c.vel, P) | alloc(c.csq, P) | alloc(c.orig, P);
+  bad |= alloc(c.pm_alt, P) | alloc(c.hz_alt, P) | alloc(c.vel_alt, P) | alloc(c.csq_alt, P) |
+         alloc(c.orig_alt, P);
+  bad |= alloc(c.rho, P) | alloc(c.omega, P) | alloc(c.div_v, P) | alloc(c.drhodt, P) |
+         alloc(c.press, P) | alloc(c.sound, P) | alloc(c.acc, 3 * P) | alloc(c.gpot, P);
+  // stage: host-layout arrays and up to 1024 sinks; istage: active list + id arrays
+  bad |= alloc(c.pptot, P) | alloc(c.pplist, P * L) | alloc(c.stage, std::max<size_t>(6 * P, 16384)) |
+         alloc(c.istage, P * L + P);
+  bad |= alloc(c.keys, P) | alloc(c.keys_alt, P) | alloc(c.idx, P) | alloc(c.idx_alt, P) |
+         alloc(c.rs_hist, 256 * rsblk) | alloc(c.bbox_part, 6 * 1184);
+  bad |= alloc(c.branch, nbr) | alloc(c.branch_next, nbr) | alloc(c.nchild, nbr) |
+         alloc(c.choff, nbr) | alloc(c.cstart, 9 * nbr) | alloc(c.bflag, C) | alloc(c.bscan, C);
+  bad |= alloc(c.leaf, C) | alloc(c.nextcell, C) | alloc(c.ifopen, C) | alloc(c.pstart, C) |
+         alloc(c.pcount, C) | alloc(c.parent, C) | alloc(c.level, C) | alloc(c.link, C);
+  bad |= alloc(c.gA, C) | alloc(c.gB, C) | alloc(c.gC, C) | alloc(c.hA, C) | alloc(c.hrm, C) |
+         alloc(c.hmax, C) | alloc(c.bbmin, C) | alloc(c.bbmax, C);
+  bad |= alloc(c.d_info, 1) | alloc(c.d_err, 1) | alloc(c.d_counts, 32);
+  bad |= alloc(c.tabA, KERNTOT + 1) | alloc(c.tabG, KERNTOT + 1);
+  if (bad) return -1;
+  const size_t scan_n = std::max(std::max(256 * rsblk, C), P) + 16;
+  if (scan_scratch_alloc(c.scan, (int)scan_n)) return -1;
+  cudaMemset(c.d_err, 0, sizeof(DevError));
+  cudaMemset(c.d_counts, 0, sizeof(int) * 32);
+  cudaMemset(c.hrm, 0, sizeof(double) * C);
+  for (auto& e : c.ev)
+    if (cudaEventCreate(&e) != cudaSuccess) return -1;
+  // kernel tables
+  std::vector<double> w0, w1, w4, w5, w6, wh, wg;
+  make_kernel_tables(c.prm.kernel, w0, w1, w4, w5, w6, wh, wg);
+  std::vector<double4> ta(KERNTOT + 1), tg(KERNTOT + 1);
+  for (int i = 0; i <= KERNTOT; ++i) {
+    ta[i] = make_double4(w0[i], wh[i], w4[i], wg[i]);
+    tg[i] = make_double4(w5[i], w4[i], w6[i], w1[i]);
+  }
+  if (cudaMemcpy(c.tabA, ta.data(), sizeof(double4) * ta.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+    return -1;
+  if (cudaMemcpy(c.tabG, tg.data(), sizeof(double4) * tg.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+    return -1;
+  return 0;
+}
+
+// new particle set: identity order, clear per-particle state
+void reset_particles(Ctx& c, int ptot) {
+  c.ptot = ptot;
+  c.have_tree = c.have_sph = c.have_v = c.have_csq = false;
+  k_iota<<<nb(ptot, 256), 256, 0, c.st>>>(c.orig, ptot);
+  cudaMemsetAsync(c.vel, 0, sizeof(double4) * ptot, c.st);
+  cudaMemsetAsync(c.csq, 0, sizeof(double) * ptot, c.st);
+  cudaMemsetAsync(c.pptot, 0, sizeof(int) * ptot, c.st);
+}
+
+}  // namespace
+}  // namespace seren
+
+using seren::Ctx;
+using seren::fail;
+using seren::finish;
+using seren::nb;
+
+extern "C" {
+
+int seren_gpu_create(seren_gpu_ctx** out, int64_t pmax, const seren_gpu_params* prm) {
+  if (!out || !prm) return SEREN_GPU_ERR_ARG;
+  *out = nullptr;
+  if (pmax < 1 || pmax > (int64_t)1 << 28) return SEREN_GPU_ERR_ARG;
+  if (prm->ndim != 3 || prm->leafmax != seren::LEAFMAX || prm->lmax < 1 || prm->lmax > 30 ||
+      (prm->kernel != 0 && prm->kernel != 1) || prm->visc != 0 ||
+      (prm->precision != 0 && prm->precision != 1) || prm->pp_gather < 1 || prm->pp_limit < 1 ||
+      (prm->index_base != 0 && prm->index_base != 1) || !(prm->h_fac > 0.0) ||
+      !(prm->thetamaxsqd >= 0.0))
+    return SEREN_GPU_ERR_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return SEREN_GPU_ERR_CUDA;
+  seren_gpu_ctx* h = new seren_gpu_ctx();
+  Ctx& c = h->c;
+  c.prm = *prm;
+  c.pmax = pmax;
+  c.cmax = (int)(2 * pmax);
+  cudaGetDevice(&c.dev);
+  if (cudaStreamCreateWithFlags(&c.st, cudaStreamNonBlocking) != cudaSuccess || seren::alloc_all(c)) {
+    seren::free_all(c);
+    delete h;
+    cudaGetLastError();
+    return SEREN_GPU_ERR_CUDA;
+  }
+  *out = h;
+  return SEREN_GPU_OK;
+}
+
+void seren_gpu_destroy(seren_gpu_ctx* h) {
+  if (!h) return;
+  cudaStreamSynchronize(h->c.st);
+  seren::free_all(h->c);
+  delete h;
+}
+
+int seren_gpu_last_error(seren_gpu_ctx* h, char* buf, int32_t len) {
+  if (!h || !buf || len <= 0) return SEREN_GPU_ERR_ARG;
+  std::snprintf(buf, (size_t)len, "%s", h->c.err.c_str());
+  return SEREN_GPU_OK;
+}
+
+int seren_gpu_tree_update(seren_gpu_ctx* h, int32_t ptot, double* parray, int32_t do_build,
+                          int32_t do_reorder, int32_t* perm_out) {
+  if (!h) return SEREN_GPU_ERR_ARG;
+  Ctx& c = h->c;
+  if (!parray || ptot < 1) return fail(c, SEREN_GPU_ERR_ARG, "parray NULL or ptot < 1");
+  if (ptot > c.pmax) return fail(c, SEREN_GPU_ERR_CAPACITY, "ptot > pmax");
+  if (!do_build && (!c.have_tree || ptot != c.ptot))
+    return fail(c, SEREN_GPU_ERR_STATE, "restock without a tree of this size");
+  if (do_build && !do_reorder)
+    return fail(c, SEREN_GPU_ERR_ARG, "a build requires the particle reorder (REORDER=PARTICLES)");
+  if (ptot != c.ptot) seren::reset_particles(c, ptot);
+  else if (do_build) seren::k_iota<<<nb(ptot, 256), 256, 0, c.st>>>(c.orig, ptot);
+  cudaMemcpyAsync(c.stage, parray, sizeof(double) * 6 * (size_t)ptot, cudaMemcpyHostToDevice, c.st);
+  seren::launch_unpack_parray(c, c.stage, ptot);
+  int rc = finish(c, "tree_update(upload)");
+  if (rc) return rc;
+  if (do_build) {
+    rc = seren::build_tree(c);
+    if (rc) return rc;
+  }
+  seren::launch_stock(c);
+  if (do_build) {
+    seren::launch_pack_parray(c, c.stage, ptot);
+    cudaMemcpyAsync(parray, c.stage, sizeof(double) * 6 * (size_t)ptot, cudaMemcpyDeviceToHost, c.st);
+  }
+  if (perm_out) {
+    if (do_build)
+      cudaMemcpyAsync(perm_out, c.idx, sizeof(int) * ptot, cudaMemcpyDeviceToHost, c.st);
+  }
+  rc = finish(c, "tree_update");
+  if (rc) return rc;
+  if (perm_out) {
+    if (do_build) {
+      if (c.prm.index_base)
+        for (int i = 0; i < ptot; ++i) perm_out[i] += c.prm.index_base;
+    } else {
+      for (int i = 0; i < ptot; ++i) perm_out[i] = i + c.prm.index_base;
+    }
+  }
+  return SEREN_GPU_OK;
+}
+
+int seren_gpu_sph_update(seren_gpu_ctx* h, int32_t ptot, const int32_t* acclist, int32_t nacc,
+                         double* parray, const double* v, double* rho, double* omega,
+                         double* div_v, double* drhodt, int32_t* pptot, int32_t* pplist,
+                         int32_t first_call) {
+  if (!h) return SEREN_GPU_ERR_ARG;
+  Ctx& c = h->c;
+  int rc = seren::check_tree(c, ptot);
+  if (rc) return rc;
+  if (!v) return fail(c, SEREN_GPU_ERR_ARG, "v is NULL");
+  cudaMemcpyAsync(c.stage, v, sizeof(double) * 3 * (size_t)ptot, cudaMemcpyHostToDevice, c.st);
+  seren::k_unpack_v<<<nb(ptot, 256), 256, 0, c.st>>>(c.stage, ptot, c.vel);
+  c.have_v = true;
+  int nact = 0;
+  rc = seren::set_active(c, acclist, nacc, nact);
+  if (rc) return rc;
+  if (first_call) seren::launch_hguess(c);
+  seren::launch_gradh(c, nact);
+  seren::launch_update_hmax(c);
+  seren::launch_neib(c, nact);
+  rc = finish(c, "sph_update");
+  if (rc) return rc;
+  c.have_sph = true;
+  // results back to the host arrays
+  if (parray) {
+    double* pin = seren::pinned(c, (size_t)2 * ptot);
+    if (!pin) return fail(c, SEREN_GPU_ERR_CUDA, "pinned staging allocation failed");
+    seren::k_pack_hz<<<nb(ptot, 256), 256, 0, c.st>>>(c.hz, ptot, c.stage);
+    cudaMemcpyAsync(pin, c.stage, sizeof(double) * 2 * (size_t)ptot, cudaMemcpyDeviceToHost, c.st);
+    cudaError_t e = cudaStreamSynchronize(c.st);
+    if (e != cudaSuccess) return seren::cuda_fail(c, e, "sph_update(h)");
+    if (acclist == nullptr || first_call) {
+      for (int p = 0; p < ptot; ++p) parray[(size_t)p * 6 + 4] = pin[(size_t)p * 2];
+    }
+    const int na = acclist ? nact : ptot;
+    for (int i = 0; i < na; ++i) {
+      const size_t p = acclist ? (size_t)(acclist[i] - c.prm.index_base) : (size_t)i;
+      parray[p * 6 + 4] = pin[p * 2];
+      parray[p * 6 + 5] = pin[p * 2 + 1];
+    }
+  }
+  if (rho && (rc = seren::d2h_rows(c, rho, c.rho, 1, acclist, nact))) return rc;
+  if (omega && (rc = seren::d2h_rows(c, omega, c.omega, 1, acclist, nact))) return rc;
+  if (div_v && (rc = seren::d2h_rows(c, div_v, c.div_v, 1, acclist, nact))) return rc;
+  if (drhodt && (rc = seren::d2h_rows(c, drhodt, c.drhodt, 1, acclist, nact))) return rc;
+  if (pptot || pplist) {
+    const int L = c.prm.pp_limit;
+    std::vector<int> tot(ptot);
+    cudaMemcpyAsync(tot.data(), c.pptot, sizeof(int) * ptot, cudaMemcpyDeviceToHost, c.st);
+    cudaStreamSynchronize(c.st);
+    if (pptot) {
+      if (!acclist) std::memcpy(pptot, tot.data(), sizeof(int) * ptot);
+      else
+        for (int i = 0; i < nact; ++i) {
+          const int p = acclist[i] - c.prm.index_base;
+          pptot[p] = tot[p];
+        }
+    }
+    if (pplist) {
+      int* src = c.pplist;
+      if (c.prm.index_base) {
+        const long n = (long)ptot * L;
+        seren::k_add_base<<<nb(n, 256), 256, 0, c.st>>>(c.pplist, c.istage + ptot, n, c.prm.index_base);
+        src = c.istage + ptot;
+      }
+      if (!acclist) {
+        cudaMemcpyAsync(pplist, src, sizeof(int) * (size_t)ptot * L, cudaMemcpyDeviceToHost, c.st);
+      } else {
+        for (int i = 0; i < nact; ++i) {
+          const int p = acclist[i] - c.prm.index_base;
+          if (tot[p] <= L)
+            cudaMemcpyAsync(pplist + (size_t)p * L, src + (size_t)p * L, sizeof(int) * tot[p],
+                            cudaMemcpyDeviceToHost, c.st);
+        }
+      }
+    }
+  }
+  return finish(c, "sph_update(copy back)");
+}
+
+int seren_gpu_get_neib(seren_gpu_ctx* h, int32_t ptot, const int32_t* acclist, int32_t nacc,
+                       const double* hh, int32_t* pptot, int32_t* pplist) {
+  if (!h) return SEREN_GPU_ERR_ARG;
+  Ctx& c = h->c;
+  int rc = seren::check_tree(c, ptot);
+  if (rc) return rc;
+  if (hh) {
+    cudaMemcpyAsync(c.stage, hh, sizeof(double) * (size_t)ptot, cudaMemcpyHostToDevice, c.st);
+    seren::k_set_h<<<nb(ptot, 256), 256, 0, c.st>>>(c.stage, ptot, c.hz);
+  }
+  int nact = 0;
+  rc = seren::set_active(c, acclist, nacc, nact);
+  if (rc) return rc;
+  seren::launch_update_hmax(c);
+  seren::launch_neib(c, nact);
+  rc = finish(c, "get_neib");
+  if (rc) return rc;
+  const int L = c.prm.pp_limit;
+  std::vector<int> tot(ptot);
+  cudaMemcpy(tot.data(), c.pptot, sizeof(int) * ptot, cudaMemcpyDeviceToHost);
+  std::vector<int> lst;
+  if (pplist) {
+    lst.resize((size_t)ptot * L);
+    cudaMemcpy(lst.data(), c.pplist, sizeof(int) * lst.size(), cudaMemcpyDeviceToHost);
+  }
+  const int na = acclist ? nact : ptot;
+  for (int i = 0; i < na; ++i) {
+    const int p = acclist ? acclist[i] - c.prm.index_base : i;
+    if (pptot) pptot[p] = tot[p];
+    if (pplist && tot[p] <= L)
+      for (int k = 0; k < tot[p]; ++k) pplist[(size_t)p * L + k] = lst[(size_t)p * L + k] + c.prm.index_base;
+  }
+  return SEREN_GPU_OK;
+}
+
+int seren_gpu_hydro_forces(seren_gpu_ctx* h, const int32_t* acclist, int32_t nacc,
+                           const double* press, const double* sound, double* a) {
+  if (!h) return SEREN_GPU_ERR_ARG;
+  Ctx& c = h->c;
+  if (!c.have_sph) return fail(c, SEREN_GPU_ERR_STATE, "call seren_gpu_sph_update first");
+  if (!press || !sound || !a) return fail(c, SEREN_GPU_ERR_ARG, "NULL array");
+  const int ptot = c.ptot;
+  cudaMemcpyAsync(c.press, press, sizeof(double) * ptot, cudaMemcpyHostToDevice, c.st);
+  cudaMemcpyAsync(c.sound, sound, sizeof(double) * ptot, cudaMemcpyHostToDevice, c.st);
+  int nact = 0;
+  int rc = seren::set_active(c, acclist, nacc, nact);
+  if (rc) return rc;
+  seren::launch_hydro(c, nact);
+  rc = finish(c, "hydro_forces");
+  if (rc) return rc;
+  if ((rc = seren::d2h_rows(c, a, c.acc, 3, acclist, nact))) return rc;
+  return finish(c, "hydro_forces(copy back)");
+}
+
+int seren_gpu_grav_forces(seren_gpu_ctx* h, const int32_t* acclist, int32_t nacc, double* a,
+                          double* gpot, int32_t nsink, const double* sink_rmh) {
+  if (!h) return SEREN_GPU_ERR_ARG;
+  Ctx& c = h->c;
+  if (!c.have_tree || c.ptot < 1) return fail(c, SEREN_GPU_ERR_STATE, "no tree");
+  if (!a || !gpot || nsink < 0 || (nsink > 0 && !sink_rmh))
+    return fail(c, SEREN_GPU_ERR_ARG, "bad arguments");
+  if (nsink > 1024) return fail(c, SEREN_GPU_ERR_ARG, "nsink > 1024");
+  const int ptot = c.ptot;
+  cudaMemcpyAsync(c.acc, a, sizeof(double) * 3 * (size_t)ptot, cudaMemcpyHostToDevice, c.st);
+  double* d_sinks = c.stage;
+  if (nsink > 0)
+    cudaMemcpyAsync(d_sinks, sink_rmh, sizeof(double) * 5 * nsink, cudaMemcpyHostToDevice, c.st);
+  int nact = 0;
+  int rc = seren::set_active(c, acclist, nacc, nact);
+  if (rc) return rc;
+  cudaMemsetAsync(c.d_counts, 0, sizeof(int) * 32, c.st);
+  seren::launch_grav(c, nact, nsink, d_sinks);
+  rc = finish(c, "grav_forces");
+  if (rc) return rc;
+  if ((rc = seren::d2h_rows(c, a, c.acc, 3, acclist, nact))) return rc;
+  if ((rc = seren::d2h_rows(c, gpot, c.gpot, 1, acclist, nact))) return rc;
+  return finish(c, "grav_forces(copy back)");
+}
+
+int seren_gpu_sink_forces(seren_gpu_ctx* h, int32_t nsink, const double* sink_rmh, double* sink_a,
+                          double* sink_gpot) {
+  if (!h) return SEREN_GPU_ERR_ARG;
+  Ctx& c = h->c;
+  if (!c.have_tree) return fail(c, SEREN_GPU_ERR_STATE, "no tree");
+  if (nsink < 1 || nsink > 1024 || !sink_rmh || !sink_a || !sink_gpot)
+    return fail(c, SEREN_GPU_ERR_ARG, "bad arguments");
+  double* d_sinks = c.stage;
+  double* d_out = c.stage + 5 * 1024;
+  cudaMemcpyAsync(d_sinks, sink_rmh, sizeof(double) * 5 * nsink, cudaMemcpyHostToDevice, c.st);
+  seren::launch_sink_walk(c, nsink, d_sinks, d_out);
+  std::vector<double> out((size_t)nsink * 4);
+  cudaMemcpyAsync(out.data(), d_out, sizeof(double) * 4 * nsink, cudaMemcpyDeviceToHost, c.st);
+  int rc = finish(c, "sink_forces");
+  if (rc) return rc;
+  for (int s = 0; s < nsink; ++s) {
+    for (int k = 0; k < 3; ++k) sink_a[s * 3 + k] = out[s * 4 + k];
+    sink_gpot[s] = out[s * 4 + 3];
+  }
+  return SEREN_GPU_OK;
+}
+
+int seren_gpu_upload(seren_gpu_ctx* h, int32_t ptot, const double* parray, const double* v,
+                     const double* csq) {
+  if (!h) return SEREN_GPU_ERR_ARG;
+  Ctx& c = h->c;
+  if (!parray || !v || !csq || ptot < 1) return fail(c, SEREN_GPU_ERR_ARG, "NULL array or ptot < 1");
+  if (ptot > c.pmax) return fail(c, SEREN_GPU_ERR_CAPACITY, "ptot > pmax");
+  seren::reset_particles(c, ptot);
+  cudaMemcpyAsync(c.stage, parray, sizeof(double) * 6 * (size_t)ptot, cudaMemcpyHostToDevice, c.st);
+  seren::launch_unpack_parray(c, c.stage, ptot);
+  int rc = finish(c, "upload(parray)");
+  if (rc) return rc;
+  cudaMemcpyAsync(c.stage, v, sizeof(double) * 3 * (size_t)ptot, cudaMemcpyHostToDevice, c.st);
+  seren::k_unpack_v<<<nb(ptot, 256), 256, 0, c.st>>>(c.stage, ptot, c.vel);
+  cudaMemcpyAsync(c.csq, csq, sizeof(double) * (size_t)ptot, cudaMemcpyHostToDevice, c.st);
+  c.have_v = c.have_csq = true;
+  return finish(c, "upload");
+}
+
+int seren_gpu_force_step(seren_gpu_ctx* h, int32_t first_call) {
+  if (!h) return SEREN_GPU_ERR_ARG;
+  Ctx& c = h->c;
+  if (!c.have_v || !c.have_csq || c.ptot < 1)
+    return fail(c, SEREN_GPU_ERR_STATE, "call seren_gpu_upload first");
+  const int n = c.ptot;
+  c.act = nullptr;
+  cudaEventRecord(c.ev[0], c.st);
+  int rc = seren::build_tree(c);
+  if (rc) return rc;
+  seren::launch_stock(c);
+  cudaEventRecord(c.ev[1], c.st);
+  if (first_call) seren::launch_hguess(c);
+  seren::launch_gradh(c, n);
+  cudaEventRecord(c.ev[2], c.st);
+  seren::launch_update_hmax(c);
+  seren::launch_neib(c, n);
+  cudaEventRecord(c.ev[3], c.st);
+  seren::launch_thermal(c);
+  seren::launch_hydro(c, n);
+  cudaEventRecord(c.ev[4], c.st);
+  cudaMemsetAsync(c.d_counts, 0, sizeof(int) * 32, c.st);
+  seren::launch_grav(c, n, 0, nullptr);
+  cudaEventRecord(c.ev[5], c.st);
+  rc = finish(c, "force_step");
+  if (rc) return rc;
+  c.have_sph = true;
+  for (int k = 0; k < 5; ++k) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c.ev[k], c.ev[k + 1]);
+    c.stage_ms[k] = ms;
+  }
+  float tot = 0.f;
+  cudaEventElapsedTime(&tot, c.ev[0], c.ev[5]);
+  c.stage_ms[5] = tot;
+  return SEREN_GPU_OK;
+}
+
+int seren_gpu_drift(seren_gpu_ctx* h, double dt) {
+  if (!h) return SEREN_GPU_ERR_ARG;
+  Ctx& c = h->c;
+  if (!c.have_v) return fail(c, SEREN_GPU_ERR_STATE, "no velocities");
+  seren::k_drift<<<nb(c.ptot, 256), 256, 0, c.st>>>(c.ptot, c.pm, c.vel, dt);
+  return finish(c, "drift");
+}
+
+int seren_gpu_download(seren_gpu_ctx* h, double* parray, double* v, double* rho, double* omega,
+                       double* a, double* gpot, int32_t* perm_total) {
+  if (!h) return SEREN_GPU_ERR_ARG;
+  Ctx& c = h->c;
+  const int n = c.ptot;
+  if (n < 1) return fail(c, SEREN_GPU_ERR_STATE, "nothing uploaded");
+  if (parray) {
+    seren::launch_pack_parray(c, c.stage, n);
+    cudaMemcpyAsync(parray, c.stage, sizeof(double) * 6 * (size_t)n, cudaMemcpyDeviceToHost, c.st);
+    int rc = finish(c, "download(parray)");
+    if (rc) return rc;
+  }
+  if (v) {
+    seren::k_pack_v<<<nb(n, 256), 256, 0, c.st>>>(c.stage, n, c.vel);
+    cudaMemcpyAsync(v, c.stage, sizeof(double) * 3 * (size_t)n, cudaMemcpyDeviceToHost, c.st);
+    int rc = finish(c, "download(v)");
+    if (rc) return rc;
+  }
+  if (rho) cudaMemcpyAsync(rho, c.rho, sizeof(double) * n, cudaMemcpyDeviceToHost, c.st);
+  if (omega) cudaMemcpyAsync(omega, c.omega, sizeof(double) * n, cudaMemcpyDeviceToHost, c.st);
+  if (a) cudaMemcpyAsync(a, c.acc, sizeof(double) * 3 * (size_t)n, cudaMemcpyDeviceToHost, c.st);
+  if (gpot) cudaMemcpyAsync(gpot, c.gpot, sizeof(double) * n, cudaMemcpyDeviceToHost, c.st);
+  if (perm_total) cudaMemcpyAsync(perm_total, c.orig, sizeof(int) * n, cudaMemcpyDeviceToHost, c.st);
+  int rc = finish(c, "download");
+  if (rc) return rc;
+  if (perm_total && c.prm.index_base)
+    for (int i = 0; i < n; ++i) perm_total[i] += c.prm.index_base;
+  return SEREN_GPU_OK;
+}
+
+int seren_gpu_tree_export(seren_gpu_ctx* h, int32_t* ctot, int32_t* ltot, int32_t* leaf,
+                          int32_t* nextcell, int32_t* ifopen, int32_t* plist, int32_t* first_cell,
+                          int32_t* last_cell, double* grav_r, double* grav_m, double* grav_q,
+                          double* dminsqd, double* hydro_r, double* rmax, double* hrangemax) {
+  if (!h) return SEREN_GPU_ERR_ARG;
+  Ctx& c = h->c;
+  if (!c.have_tree) return fail(c, SEREN_GPU_ERR_STATE, "no tree");
+  const int nc = c.info.ctot + 1;
+  if (ctot) *ctot = c.info.ctot;
+  if (ltot) *ltot = c.info.ltot;
+  std::vector<int4> lk(nc);
+  std::vector<double4> a(nc), b(nc), ha(nc);
+  std::vector<double2> cc(nc);
+  std::vector<double> hr(nc);
+  cudaMemcpy(lk.data(), c.link, sizeof(int4) * nc, cudaMemcpyDeviceToHost);
+  cudaMemcpy(a.data(), c.gA, sizeof(double4) * nc, cudaMemcpyDeviceToHost);
+  cudaMemcpy(b.data(), c.gB, sizeof(double4) * nc, cudaMemcpyDeviceToHost);
+  cudaMemcpy(cc.data(), c.gC, sizeof(double2) * nc, cudaMemcpyDeviceToHost);
+  cudaMemcpy(ha.data(), c.hA, sizeof(double4) * nc, cudaMemcpyDeviceToHost);
+  cudaMemcpy(hr.data(), c.hrm, sizeof(double) * nc, cudaMemcpyDeviceToHost);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return seren::cuda_fail(c, e, "tree_export");
+  const int base = c.prm.index_base;
+  for (int i = 0; i < nc; ++i) {
+    if (leaf) leaf[i] = lk[i].x;
+    if (nextcell) nextcell[i] = lk[i].y;
+    if (ifopen) ifopen[i] = lk[i].x > 0 ? -1 : lk[i].z;
+    if (plist)
+      for (int k = 0; k < 8; ++k) plist[i * 8 + k] = (lk[i].x > 0 && k < lk[i].x) ? lk[i].w + k + base : -1;
+    if (grav_r) { grav_r[i * 3] = a[i].x; grav_r[i * 3 + 1] = a[i].y; grav_r[i * 3 + 2] = a[i].z; }
+    if (grav_m) grav_m[i] = a[i].w;
+    if (grav_q) {
+      grav_q[i * 5] = b[i].x; grav_q[i * 5 + 1] = b[i].y; grav_q[i * 5 + 2] = b[i].z;
+      grav_q[i * 5 + 3] = b[i].w; grav_q[i * 5 + 4] = cc[i].x;
+    }
+    if (dminsqd) dminsqd[i] = cc[i].y;
+    if (hydro_r) { hydro_r[i * 3] = ha[i].x; hydro_r[i * 3 + 1] = ha[i].y; hydro_r[i * 3 + 2] = ha[i].z; }
+    if (rmax) rmax[i] = ha[i].w;
+    if (hrangemax) hrangemax[i] = hr[i];
+  }
+  for (int l = 0; l <= c.info.ltot; ++l) {
+    if (first_cell) first_cell[l] = c.info.first_cell[l];
+    if (last_cell) last_cell[l] = c.info.last_cell[l];
+  }
+  return SEREN_GPU_OK;
+}
+
+int seren_gpu_last_step_stats(seren_gpu_ctx* h, double* stage_ms, int32_t* nlaunch) {
+  if (!h) return SEREN_GPU_ERR_ARG;
+  if (stage_ms)
+    for (int k = 0; k < 8; ++k) stage_ms[k] = h->c.stage_ms[k];
+  if (nlaunch) *nlaunch = h->c.nlaunch;
+  return SEREN_GPU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,134 @@
+// ctx.cuh - the device context behind one seren_gpu_ctx, and the launchers
+// each .cu file provides to the C ABI layer.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "../../include/seren_gpu.h"
+#include "common.cuh"
+
+namespace seren {
+
+// Scratch for the multi-level exclusive scan of int32 arrays.
+struct ScanScratch {
+  int* level_buf[4] = {nullptr, nullptr, nullptr, nullptr};  // block sums per level
+  int level_cap[4] = {0, 0, 0, 0};
+  int* total = nullptr;  // device int: total of the last scan
+};
+
+struct Ctx {
+  seren_gpu_params prm{};
+  int64_t pmax = 0;
+  int cmax = 0;          // 2*pmax, the reference's cmax_grav
+  int ptot = 0;
+  int dev = 0;
+  cudaStream_t st = nullptr;
+  std::string err;
+
+  // particles in tree order
+  double4* pm = nullptr;     // x, y, z, m
+  double2* hz = nullptr;     // h, zeta
+  double4* vel = nullptr;    // vx, vy, vz, 0
+  double* csq = nullptr;     // isothermal c_s^2 = Pconst*T
+  int* orig = nullptr;       // id of each slot in the first upload's order
+  double4* pm_alt = nullptr;
+  double2* hz_alt = nullptr;
+  double4* vel_alt = nullptr;
+  double* csq_alt = nullptr;
+  int* orig_alt = nullptr;
+  double* rho = nullptr;
+  double* omega = nullptr;
+  double* div_v = nullptr;
+  double* drhodt = nullptr;
+  double* press = nullptr;
+  double* sound = nullptr;
+  double* acc = nullptr;     // [ptot][3]
+  double* gpot = nullptr;
+  int* pptot = nullptr;
+  int* pplist = nullptr;     // [ptot][pp_limit]
+  int* act = nullptr;        // active list (0-based), when given
+  double* stage = nullptr;   // [pmax][6] device staging of host-layout arrays
+  int* istage = nullptr;     // [pmax*pp_limit] device staging of id arrays
+  double* h_pin = nullptr;   // pinned host staging, [pmax][6] doubles
+  int* hi_pin = nullptr;     // pinned host staging, ids
+
+  // build scratch
+  unsigned long long* keys = nullptr;
+  unsigned long long* keys_alt = nullptr;
+  int* idx = nullptr;
+  int* idx_alt = nullptr;
+  int* rs_hist = nullptr;     // [256][nblk]
+  double* bbox_part = nullptr;
+  int* branch = nullptr;      // branch cells of the level being split
+  int* branch_next = nullptr;
+  int* nchild = nullptr;      // children per branch cell
+  int* choff = nullptr;       // exclusive scan of nchild
+  int* cstart = nullptr;      // [nbranch][9] child range boundaries
+  int* bflag = nullptr;       // 1 for a branch child on the new level
+  int* bscan = nullptr;
+  ScanScratch scan;
+
+  // tree, breadth-first cell ids 0..ctot
+  int* leaf = nullptr;
+  int* nextcell = nullptr;
+  int* ifopen = nullptr;
+  int* pstart = nullptr;
+  int* pcount = nullptr;
+  int* parent = nullptr;
+  int* level = nullptr;
+  int4* link = nullptr;       // {leaf, nextcell, ifopen, pstart}, packed for walks
+  double4* gA = nullptr;      // gravity: COM x, y, z, m
+  double4* gB = nullptr;      // gravity: q1..q4 (xx, xy, yy, zx)
+  double2* gC = nullptr;      // gravity: q5 (zy), dminsqd
+  double4* hA = nullptr;      // hydro: bbox centre x, y, z, rmax
+  double* hrm = nullptr;      // hydro: hrangemax
+  double* hmax = nullptr;     // stock: max h in the cell (at stock time)
+  double4* bbmin = nullptr;
+  double4* bbmax = nullptr;
+  TreeInfo* d_info = nullptr;
+  TreeInfo info{};            // host mirror after a build
+  DevError* d_err = nullptr;
+  int* d_counts = nullptr;    // [16] int64 interaction counters (as 2 ints each)
+
+  // kernel tables
+  double4* tabA = nullptr;
+  double4* tabG = nullptr;
+
+  bool have_tree = false;
+  bool have_sph = false;
+  bool have_v = false;
+  bool have_csq = false;
+
+  // timing of the last force step
+  cudaEvent_t ev[10] = {};
+  double stage_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int nlaunch = 0;
+};
+
+// tree.cu
+int build_tree(Ctx& c);               // bbox, keys, sort, cells, leaf order, reorder
+void launch_unpack_parray(Ctx& c, const double* stage, int n);
+void launch_pack_parray(Ctx& c, double* stage, int n);
+void launch_stock(Ctx& c);            // BHgrav_stock + BHhydro_stock
+void launch_update_hmax(Ctx& c);      // BHhydro_update_hmax
+void launch_hguess(Ctx& c);           // BHhydro_hguess
+void scan_exclusive(Ctx& c, const int* in, int* out, int n);   // total -> c.scan.total
+int scan_scratch_alloc(ScanScratch& s, int nmax);
+
+// sph.cu
+void launch_gradh(Ctx& c, int nact);
+void launch_neib(Ctx& c, int nact);
+void launch_hydro(Ctx& c, int nact);
+void launch_thermal(Ctx& c);
+
+// gravity.cu
+void launch_grav(Ctx& c, int nact, int nsink, const double* d_sinks);
+void launch_sink_walk(Ctx& c, int nsink, const double* d_sinks, double* d_out /*[nsink][4]*/);
+
+// tables.cpp
+void make_kernel_tables(int kernel, std::vector<double>& w0, std::vector<double>& w1,
+                        std::vector<double>& w4, std::vector<double>& w5, std::vector<double>& w6,
+                        std::vector<double>& wh, std::vector<double>& wg);
+
+}  // namespace seren

@@ -1,0 +1,469 @@
+// gravity.cu - Barnes-Hut gravity walk with the geometric MAC, quadrupole
+// cell terms and the kernel-softened grad-h near field; direct sink gravity.
+//
+// Two arithmetic forms share one walk:
+//  * FP64: every cell and pair term is the reference expression
+//    (BHtree/BHgrav_accel.F90:146-226, gravity/gravity_gradh.F90:57-86) in
+//    FP64 with its association and no contraction.
+//  * mixed: the walk, the MAC test (drsqd > dminsqd) and the separations stay
+//    FP64, so exactly the same cells are accepted and the same pairs visited;
+//    the separation is then cast to FP32 and the cell/pair term evaluated in
+//    FP32 (rsqrtf, FMA), with the M4 softening kernel evaluated analytically at
+//    the centre of the reference's table bin; terms are summed in FP32 with
+//    Kahan compensation and added to the FP64 result once.
+#include "ctx.cuh"
+
+namespace seren {
+
+namespace {
+
+struct GravTree {
+  const int4* link;
+  const double4* gA;   // COM, m
+  const double4* gB;   // q1..q4
+  const double2* gC;   // q5, dminsqd
+  int ctot;
+};
+
+// ---------------------------------------------------------------------------
+// FP64 terms
+__device__ __forceinline__ void cell_term64(double d0, double d1, double d2, double drsqd,
+                                            const double4& a, const double4& q, double q5,
+                                            double& ax, double& ay, double& az, double& pot) {
+  const double invdrsqd = 1.0 / (drsqd + SMALL_NUMBER);
+  const double invdrmag = sqrt(invdrsqd);
+  const double mm = (a.w * invdrsqd) * invdrmag;
+  double t0 = -(mm * d0), t1 = -(mm * d1), t2 = -(mm * d2);
+  double dpot = a.w * invdrmag;
+  const double invdr5 = (invdrsqd * invdrsqd) * invdrmag;
+  const double q1 = q.x, q2 = q.y, q3 = q.z, q4 = q.w;
+  const double qscalar = (((q1 * d0) * d0 + (q3 * d1) * d1) - ((q1 + q3) * d2) * d2) +
+                         2.0 * ((((q2 * d0) * d1) + ((q4 * d0) * d2)) + ((q5 * d1) * d2));
+  t0 = (t0 + (((q1 * d0 + q2 * d1) + q4 * d2) * invdr5)) - ((((2.5 * qscalar) * d0) * invdr5) * invdrsqd);
+  t1 = (t1 + (((q2 * d0 + q3 * d1) + q5 * d2) * invdr5)) - ((((2.5 * qscalar) * d1) * invdr5) * invdrsqd);
+  t2 = (t2 + (((q4 * d0 + q5 * d1) - (q1 + q3) * d2) * invdr5)) - ((((2.5 * qscalar) * d2) * invdr5) * invdrsqd);
+  dpot = dpot + (0.5 * qscalar) * invdr5;
+  ax = ax + t0; ay = ay + t1; az = az + t2; pot = pot + dpot;
+}
+
+// gravity/gravity_gradh.F90:11-95, dr = rpp - rp
+__device__ __forceinline__ void pair_term64(double d0, double d1, double d2, double invhp, double zo_p,
+                                            double mq, double hq, double zq,
+                                            const double4* __restrict__ tabG, double& ax, double& ay,
+                                            double& az, double& pot) {
+  const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
+  const double drmag = sqrt(drsqd) + SMALL_NUMBER;
+  const double invdrmag = 1.0 / drmag;
+  double grav, dpot;
+  if (invdrmag > INVKERNRANGE * invhp) {
+    int kern = (int)((HALFKERNTOT * drmag) * invhp);
+    kern = min(kern, KERNTOT);
+    const double4 w = tabG[kern];
+    grav = (invhp * invhp) * (w.x + ((zo_p * w.y) * invhp) * invhp);
+    dpot = invhp * w.z;
+  } else {
+    grav = invdrmag * invdrmag;
+    dpot = invdrmag;
+  }
+  if (drmag < KERNRANGE * hq) {
+    const double invhq = 1.0 / hq;
+    int kern = (int)((HALFKERNTOT * drmag) * invhq);
+    kern = min(kern, KERNTOT);
+    const double4 w = tabG[kern];
+    grav = grav + (invhq * invhq) * (w.x + ((zq * w.y) * invhq) * invhq);
+    dpot = dpot + invhq * w.z;
+  } else {
+    grav = grav + invdrmag * invdrmag;
+    dpot = dpot + invdrmag;
+  }
+  const double f = ((0.5 * mq) * invdrmag) * grav;
+  ax = ax + f * d0; ay = ay + f * d1; az = az + f * d2;
+  pot = pot + (0.5 * mq) * dpot;
+}
+
+// gravity/gravity_meanh.F90:12-69
+__device__ __forceinline__ void meanh_term64(double d0, double d1, double d2, double hmean, double mq,
+                                             const double4* __restrict__ tabG, double& ax,
+                                             double& ay, double& az, double& pot) {
+  const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
+  const double drmag = sqrt(drsqd) + SMALL_NUMBER;
+  const double invdrmag = 1.0 / drmag;
+  double grav, dpot;
+  if (drmag < KERNRANGE * hmean) {
+    const double invhmean = 1.0 / hmean;
+    int kern = (int)((HALFKERNTOT * drmag) * invhmean);
+    kern = min(kern, KERNTOT);
+    const double4 w = tabG[kern];
+    grav = ((invdrmag * invhmean) * invhmean) * w.x;
+    dpot = invhmean * w.z;
+  } else {
+    grav = invdrmag * (invdrmag * invdrmag);
+    dpot = invdrmag;
+  }
+  const double f = mq * grav;
+  ax = ax + f * d0; ay = ay + f * d1; az = az + f * d2;
+  pot = pot + mq * dpot;
+}
+
+// ---------------------------------------------------------------------------
+// FP32 terms (mixed form)
+struct Kahan4 {
+  float s[4] = {0.f, 0.f, 0.f, 0.f};
+  float c[4] = {0.f, 0.f, 0.f, 0.f};
+  __device__ __forceinline__ void add(int k, float x) {
+    const float y = x - c[k];
+    const float t = s[k] + y;
+    c[k] = (t - s[k]) - y;
+    s[k] = t;
+  }
+  __device__ __forceinline__ double get(int k) const { return (double)s[k] - (double)c[k]; }
+};
+
+// M4 softened-gravity kernel functions (setup/kernel.F90:80-81, :99-102) at
+// the centre s = (2i+1)/KERNTOT of table bin i, in FP32.  Returns w5, w4, w6.
+__device__ __forceinline__ void m4_grav32(int i, float& w5, float& w4, float& w6) {
+  const float s = (float)(2 * i + 1) * 1.0e-4f;
+  const float s2 = s * s;
+  const float invpi = 0.318309886f;
+  if (i < KERNTOT / 2) {
+    // w5 = (4/3)s - 1.2 s^3 + 0.5 s^4 ; w4 = (-3 s + 2.25 s^2)/pi
+    // w6 = 1.4 - (2/3) s^2 + 0.3 s^4 - 0.1 s^5
+    w5 = s * fmaf(s2, fmaf(0.5f, s, -1.2f), 1.33333333f);
+    w4 = invpi * s * fmaf(2.25f, s, -3.0f);
+    w6 = fmaf(s2, fmaf(s2, fmaf(-0.1f, s, 0.3f), -0.66666667f), 1.4f);
+  } else {
+    // w5 = (8/3)s - 3 s^2 + 1.2 s^3 - (1/6) s^4 - 1/(15 s^2) ; w4 = -0.75 (2-s)^2 / pi
+    // w6 = -1/(15 s) + 1.6 - (4/3) s^2 + s^3 - 0.3 s^4 + (1/30) s^5
+    const float inv15s = __fdividef(1.0f, 15.0f * s);
+    w5 = s * fmaf(s, fmaf(s, fmaf(-0.16666667f, s, 1.2f), -3.0f), 2.66666667f) - inv15s / s;
+    const float sa = 2.0f - s;
+    w4 = -0.75f * invpi * sa * sa;
+    w6 = fmaf(s2, fmaf(s, fmaf(s, fmaf(0.033333333f, s, -0.3f), 1.0f), -1.33333333f), 1.6f) - inv15s;
+  }
+}
+
+__device__ __forceinline__ void cell_term32(float d0, float d1, float d2, float m, float q1, float q2,
+                                            float q3, float q4, float q5, Kahan4& acc) {
+  const float drsqd = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
+  const float invdrmag = rsqrtf(drsqd);
+  const float invdrsqd = invdrmag * invdrmag;
+  const float invdr3 = invdrsqd * invdrmag;
+  const float invdr5 = invdr3 * invdrsqd;
+  const float q6 = -(q1 + q3);
+  const float qx = fmaf(q4, d2, fmaf(q2, d1, q1 * d0));
+  const float qy = fmaf(q5, d2, fmaf(q3, d1, q2 * d0));
+  const float qz = fmaf(q6, d2, fmaf(q5, d1, q4 * d0));
+  const float qscalar = fmaf(qz, d2, fmaf(qy, d1, qx * d0));
+  const float g = fmaf(2.5f * qscalar, invdr5 * invdrsqd, m * invdr3);
+  acc.add(0, fmaf(qx, invdr5, -g * d0));
+  acc.add(1, fmaf(qy, invdr5, -g * d1));
+  acc.add(2, fmaf(qz, invdr5, -g * d2));
+  acc.add(3, fmaf(0.5f * qscalar, invdr5, m * invdrmag));
+}
+
+__device__ __forceinline__ void pair_term32(float d0, float d1, float d2, float invhp, float zo_p,
+                                            float mq, float hq, float zq, Kahan4& acc) {
+  const float drsqd = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
+  const float inv = rsqrtf(fmaxf(drsqd, 1.0e-30f));
+  const float drmag = drsqd * inv;
+  const float invdrmag = inv;
+  float grav, dpot;
+  if (drmag * invhp < KERNRANGE) {
+    const int kern = min((int)((5000.0f * drmag) * invhp), KERNTOT);
+    float w5, w4, w6;
+    m4_grav32(kern, w5, w4, w6);
+    grav = invhp * invhp * fmaf(zo_p * w4, invhp * invhp, w5);
+    dpot = invhp * w6;
+  } else {
+    grav = invdrmag * invdrmag;
+    dpot = invdrmag;
+  }
+  const float invhq = __frcp_rn(hq);
+  if (drmag < KERNRANGE * hq) {
+    const int kern = min((int)((5000.0f * drmag) * invhq), KERNTOT);
+    float w5, w4, w6;
+    m4_grav32(kern, w5, w4, w6);
+    grav = fmaf(invhq * invhq, fmaf(zq * w4, invhq * invhq, w5), grav);
+    dpot = fmaf(invhq, w6, dpot);
+  } else {
+    grav = fmaf(invdrmag, invdrmag, grav);
+    dpot = dpot + invdrmag;
+  }
+  const float f = 0.5f * mq * invdrmag * grav;
+  acc.add(0, f * d0);
+  acc.add(1, f * d1);
+  acc.add(2, f * d2);
+  acc.add(3, 0.5f * mq * dpot);
+}
+
+__device__ __forceinline__ void count_add(unsigned long long* counts, unsigned long long ncell,
+                                          unsigned long long npair) {
+  // warp-aggregated interaction counters
+  for (int o = 16; o > 0; o >>= 1) {
+    ncell += __shfl_down_sync(0xffffffffu, ncell, o);
+    npair += __shfl_down_sync(0xffffffffu, npair, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(counts + 0, ncell);
+    atomicAdd(counts + 1, npair);
+  }
+}
+
+// BHtree/BHgrav_accel.F90:21-348 for SPH particles, FP64 arithmetic
+__global__ void __launch_bounds__(128) k_grav64(int nact, const int* __restrict__ act,
+                                                const double4* __restrict__ pm,
+                                                const double2* __restrict__ hz, GravTree t,
+                                                const double4* __restrict__ tabG,
+                                                double* __restrict__ acc, double* __restrict__ gpot,
+                                                int nsink, const double* __restrict__ sinks,
+                                                DevError* err, unsigned long long* counts) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = i < nact;
+  const int p = live ? (act ? act[i] : i) : 0;
+  unsigned long long ncell = 0, npair = 0;
+  if (live) {
+    const double4 P = pm[p];
+    const double2 HZ = hz[p];
+    const double invhp = 1.0 / HZ.x;
+    const double zo_p = HZ.y;
+    double cx = 0.0, cy = 0.0, cz = 0.0, cp = 0.0;   // cell terms in walk order
+    double px = 0.0, py = 0.0, pz = 0.0, pp = 0.0;   // near-field terms in walk order
+    int c = 0, visits = 0;
+    const int cap = t.ctot + 2;
+    while (true) {
+      if (++visits > cap) {
+        set_error(err, SEREN_GPU_ERR_WALK, KID_GRAV, p, c);
+        break;
+      }
+      const int4 lk = t.link[c];
+      if (lk.x == 1) {                                                   // :128-136
+        const int q = lk.w;
+        if (q != p) {
+          const double4 Q = pm[q];
+          const double2 hq = hz[q];
+          pair_term64(Q.x - P.x, Q.y - P.y, Q.z - P.z, invhp, zo_p, Q.w, hq.x, hq.y, tabG, px, py, pz, pp);
+          ++npair;
+        }
+        c = lk.y;
+      } else {
+        const double4 a = t.gA[c];
+        const double d0 = P.x - a.x, d1 = P.y - a.y, d2 = P.z - a.z;        // :146-147
+        const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
+        const double2 cc = t.gC[c];
+        if (drsqd > cc.y) {                                              // :155
+          cell_term64(d0, d1, d2, drsqd, a, t.gB[c], cc.x, cx, cy, cz, cp);
+          ++ncell;
+          c = lk.y;
+        } else if (lk.x > 0) {                                           // :242-253
+          for (int k = 0; k < lk.x; ++k) {
+            const int q = lk.w + k;
+            if (q == p) continue;
+            const double4 Q = pm[q];
+            const double2 hq = hz[q];
+            pair_term64(Q.x - P.x, Q.y - P.y, Q.z - P.z, invhp, zo_p, Q.w, hq.x, hq.y, tabG, px, py, pz, pp);
+            ++npair;
+          }
+          c = lk.y;
+        } else if (lk.x == 0) {
+          c = lk.z;
+        } else {
+          c = lk.y;
+        }
+      }
+      if (c > t.ctot) break;
+    }
+    double* a = acc + (size_t)p * 3;
+    a[0] = a[0] + (cx + px);
+    a[1] = a[1] + (cy + py);
+    a[2] = a[2] + (cz + pz);
+    double pot = cp + pp;
+    if (nsink > 0) {                                   // sinks/direct_sink_gravity.F90:10-64
+      double sx = 0.0, sy = 0.0, sz = 0.0, sp = 0.0;
+      for (int s = 0; s < nsink; ++s) {
+        const double* sr = sinks + s * 5;
+        meanh_term64(sr[0] - P.x, sr[1] - P.y, sr[2] - P.z, 0.5 * (HZ.x + sr[4]), sr[3], tabG, sx,
+                     sy, sz, sp);
+      }
+      a[0] = a[0] + sx;
+      a[1] = a[1] + sy;
+      a[2] = a[2] + sz;
+      pot = pot + sp;
+    }
+    gpot[p] = pot;
+  }
+  count_add(counts, ncell, npair);
+}
+
+// the same walk, mixed-precision interaction arithmetic
+__global__ void __launch_bounds__(128) k_grav32(int nact, const int* __restrict__ act,
+                                                const double4* __restrict__ pm,
+                                                const double2* __restrict__ hz, GravTree t,
+                                                const double4* __restrict__ tabG,
+                                                double* __restrict__ acc, double* __restrict__ gpot,
+                                                int nsink, const double* __restrict__ sinks,
+                                                DevError* err, unsigned long long* counts) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = i < nact;
+  const int p = live ? (act ? act[i] : i) : 0;
+  unsigned long long ncell = 0, npair = 0;
+  if (live) {
+    const double4 P = pm[p];
+    const double2 HZ = hz[p];
+    const float invhp = (float)(1.0 / HZ.x);
+    const float zo_p = (float)HZ.y;
+    Kahan4 kc;
+    int c = 0, visits = 0;
+    const int cap = t.ctot + 2;
+    while (true) {
+      if (++visits > cap) {
+        set_error(err, SEREN_GPU_ERR_WALK, KID_GRAV_MIXED, p, c);
+        break;
+      }
+      const int4 lk = t.link[c];
+      if (lk.x == 1) {
+        const int q = lk.w;
+        if (q != p) {
+          const double4 Q = pm[q];
+          const double2 hq = hz[q];
+          pair_term32((float)(Q.x - P.x), (float)(Q.y - P.y), (float)(Q.z - P.z), invhp, zo_p,
+                      (float)Q.w, (float)hq.x, (float)hq.y, kc);
+          ++npair;
+        }
+        c = lk.y;
+      } else {
+        const double4 a = t.gA[c];
+        const double d0 = P.x - a.x, d1 = P.y - a.y, d2 = P.z - a.z;
+        const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
+        const double2 cc = t.gC[c];
+        if (drsqd > cc.y) {
+          const double4 q = t.gB[c];
+          cell_term32((float)d0, (float)d1, (float)d2, (float)a.w, (float)q.x, (float)q.y,
+                      (float)q.z, (float)q.w, (float)cc.x, kc);
+          ++ncell;
+          c = lk.y;
+        } else if (lk.x > 0) {
+          for (int k = 0; k < lk.x; ++k) {
+            const int q = lk.w + k;
+            if (q == p) continue;
+            const double4 Q = pm[q];
+            const double2 hq = hz[q];
+            pair_term32((float)(Q.x - P.x), (float)(Q.y - P.y), (float)(Q.z - P.z), invhp, zo_p,
+                        (float)Q.w, (float)hq.x, (float)hq.y, kc);
+            ++npair;
+          }
+          c = lk.y;
+        } else if (lk.x == 0) {
+          c = lk.z;
+        } else {
+          c = lk.y;
+        }
+      }
+      if (c > t.ctot) break;
+    }
+    double* a = acc + (size_t)p * 3;
+    a[0] = a[0] + kc.get(0);
+    a[1] = a[1] + kc.get(1);
+    a[2] = a[2] + kc.get(2);
+    double pot = kc.get(3);
+    if (nsink > 0) {
+      double sx = 0.0, sy = 0.0, sz = 0.0, sp = 0.0;
+      for (int s = 0; s < nsink; ++s) {
+        const double* sr = sinks + s * 5;
+        meanh_term64(sr[0] - P.x, sr[1] - P.y, sr[2] - P.z, 0.5 * (HZ.x + sr[4]), sr[3], tabG, sx,
+                     sy, sz, sp);
+      }
+      a[0] = a[0] + sx;
+      a[1] = a[1] + sy;
+      a[2] = a[2] + sz;
+      pot = pot + sp;
+    }
+    gpot[p] = pot;
+  }
+  count_add(counts, ncell, npair);
+}
+
+// sph_sim/sph_sink_forces.F90:49-110: BHgrav_accel(-s) with gravity_meanh
+// near field (BHgrav_accel.F90:299-314), then the other sinks directly.
+__global__ void k_sink_walk(int nsink, const double* __restrict__ sinks, const double4* __restrict__ pm,
+                            const double2* __restrict__ hz, GravTree t,
+                            const double4* __restrict__ tabG, double* __restrict__ out,
+                            DevError* err) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsink) return;
+  const double* sr = sinks + s * 5;
+  const double rx = sr[0], ry = sr[1], rz = sr[2];
+  const double invhp = 1.0 / sr[4];
+  const double hp = 1.0 / invhp;
+  double cx = 0.0, cy = 0.0, cz = 0.0, cp = 0.0, px = 0.0, py = 0.0, pz = 0.0, pp = 0.0;
+  int c = 0, visits = 0;
+  const int cap = t.ctot + 2;
+  while (true) {
+    if (++visits > cap) {
+      set_error(err, SEREN_GPU_ERR_WALK, KID_SINK, s, c);
+      break;
+    }
+    const int4 lk = t.link[c];
+    if (lk.x == 1) {
+      const double4 Q = pm[lk.w];
+      meanh_term64(Q.x - rx, Q.y - ry, Q.z - rz, 0.5 * (hp + hz[lk.w].x), Q.w, tabG, px, py, pz, pp);
+      c = lk.y;
+    } else {
+      const double4 a = t.gA[c];
+      const double d0 = rx - a.x, d1 = ry - a.y, d2 = rz - a.z;
+      const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
+      const double2 cc = t.gC[c];
+      if (drsqd > cc.y) {
+        cell_term64(d0, d1, d2, drsqd, a, t.gB[c], cc.x, cx, cy, cz, cp);
+        c = lk.y;
+      } else if (lk.x > 0) {
+        for (int k = 0; k < lk.x; ++k) {
+          const double4 Q = pm[lk.w + k];
+          meanh_term64(Q.x - rx, Q.y - ry, Q.z - rz, 0.5 * (hp + hz[lk.w + k].x), Q.w, tabG, px, py,
+                       pz, pp);
+        }
+        c = lk.y;
+      } else if (lk.x == 0) {
+        c = lk.z;
+      } else {
+        c = lk.y;
+      }
+    }
+    if (c > t.ctot) break;
+  }
+  double ax = cx + px, ay = cy + py, az = cz + pz, pot = cp + pp;
+  double sx = 0.0, sy = 0.0, sz = 0.0, sp = 0.0;
+  for (int ss = 0; ss < nsink; ++ss) {
+    if (ss == s) continue;
+    const double* o = sinks + ss * 5;
+    meanh_term64(o[0] - rx, o[1] - ry, o[2] - rz, 0.5 * (sr[4] + o[4]), o[3], tabG, sx, sy, sz, sp);
+  }
+  out[s * 4 + 0] = ax + sx;
+  out[s * 4 + 1] = ay + sy;
+  out[s * 4 + 2] = az + sz;
+  out[s * 4 + 3] = pot + sp;
+}
+
+inline int nb(long n, int t) { return (int)((n + t - 1) / t); }
+
+GravTree grav_tree(const Ctx& c) { return GravTree{c.link, c.gA, c.gB, c.gC, c.info.ctot}; }
+
+}  // namespace
+
+void launch_grav(Ctx& c, int nact, int nsink, const double* d_sinks) {
+  if (nact <= 0) return;
+  unsigned long long* counts = reinterpret_cast<unsigned long long*>(c.d_counts);
+  if (c.prm.precision == 0)
+    k_grav64<<<nb(nact, 128), 128, 0, c.st>>>(nact, c.act, c.pm, c.hz, grav_tree(c), c.tabG, c.acc,
+                                              c.gpot, nsink, d_sinks, c.d_err, counts);
+  else
+    k_grav32<<<nb(nact, 128), 128, 0, c.st>>>(nact, c.act, c.pm, c.hz, grav_tree(c), c.tabG, c.acc,
+                                              c.gpot, nsink, d_sinks, c.d_err, counts);
+}
+
+void launch_sink_walk(Ctx& c, int nsink, const double* d_sinks, double* d_out) {
+  if (nsink <= 0) return;
+  k_sink_walk<<<nb(nsink, 32), 32, 0, c.st>>>(nsink, d_sinks, c.pm, c.hz, grav_tree(c), c.tabG,
+                                              d_out, c.d_err);
+}
+
+}  // namespace seren

@@ -1,0 +1,82 @@
+"""ctypes binding of the CUDA library (the product).
+
+``GpuHotPath`` is a context of libseren_gpu.so with the reference-facing calls
+(tree_update, sph_update, get_neib, hydro_forces, grav_forces, sink_forces)
+plus the device-resident step (upload, force_step, drift, download).  Loading
+raises if the library is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .build import LIB
+from .cabi import HotPath, Params, SerenError, bind  # noqa: F401
+
+_lib = None
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int32)
+
+
+def library(build_if_missing: bool = True) -> C.CDLL:
+    """Load libseren_gpu.so (building it with nvcc first if it is missing)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            if not build_if_missing:
+                raise RuntimeError(f"{LIB} is missing: run python -m seren_b200.build")
+            from .build import build
+            build()
+        lib = bind(C.CDLL(LIB), "seren_gpu")
+        vp = C.c_void_p
+        for name, args in (("upload", [vp, C.c_int32, _dp, _dp, _dp]),
+                           ("force_step", [vp, C.c_int32]),
+                           ("drift", [vp, C.c_double]),
+                           ("download", [vp, _dp, _dp, _dp, _dp, _dp, _dp, _ip]),
+                           ("last_step_stats", [vp, _dp, _ip])):
+            fn = getattr(lib, f"seren_gpu_{name}")
+            fn.argtypes = args
+            fn.restype = C.c_int
+        _lib = lib
+    return _lib
+
+
+def _d(a):
+    return None if a is None else a.ctypes.data_as(_dp)
+
+
+class GpuHotPath(HotPath):
+    def __init__(self, pmax: int, params: Params):
+        super().__init__(library(), "seren_gpu", pmax, params)
+
+    # -- device-resident step -------------------------------------------------
+    def upload(self, parray, v, csq):
+        parray = np.ascontiguousarray(parray, dtype=np.float64)
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        csq = np.ascontiguousarray(csq, dtype=np.float64)
+        self._call("upload", self._ctx, parray.shape[0], _d(parray), _d(v), _d(csq))
+        self.ptot = parray.shape[0]
+
+    def force_step(self, first_call=False):
+        self._call("force_step", self._ctx, int(first_call))
+
+    def drift(self, dt: float):
+        self._call("drift", self._ctx, C.c_double(dt))
+
+    def download(self):
+        n = self.ptot
+        out = dict(parray=np.zeros((n, 6)), v=np.zeros((n, 3)), rho=np.zeros(n),
+                   omega=np.zeros(n), a=np.zeros((n, 3)), gpot=np.zeros(n),
+                   perm=np.zeros(n, dtype=np.int32))
+        self._call("download", self._ctx, _d(out["parray"]), _d(out["v"]), _d(out["rho"]),
+                   _d(out["omega"]), _d(out["a"]), _d(out["gpot"]),
+                   out["perm"].ctypes.data_as(_ip))
+        return out
+
+    def last_step_stats(self):
+        ms = (C.c_double * 8)()
+        nl = C.c_int32()
+        self._call("last_step_stats", self._ctx, ms, C.byref(nl))
+        return list(ms), nl.value
