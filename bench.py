@@ -1,0 +1,472 @@
+#!/usr/bin/env python
+"""Benchmark of the SEREN force hot path on B200: particle force evaluations/s.
+
+Workload: the turbulent molecular-cloud core (N = 4,194,304 particles uniform
+in a unit sphere, M = 1, G = 1, isothermal c_s = 0.2, divergence-free P(k) ~
+k^-4 velocity field at rms Mach 2), seeded synthetic data.  One step = one full
+force evaluation (tree build + reorder + stock, grad-h h/rho/Omega solve,
+hmax update, neighbour lists, isothermal thermal, hydro forces with MON97
+viscosity, Barnes-Hut gravity) followed by a drift r += v dt.  `value` is the
+mixed-precision (FP32 pair arithmetic) path with inputs resident in HBM; the
+FP64 path is timed on the same state for the speed-up and accuracy figures.
+`e2e` is the same metric through the host-buffer C ABI calls a Fortran caller
+makes (tree_update -> sph_update -> thermal on the host -> hydro_forces ->
+grav_forces), copies included.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = ("particle force evals/sec (grav+hydro) at 4M, FP32-comp vs FP64 on B200 at rms "
+          "err≤1e-3")
+UNIT = "particle evals/s"
+N_FULL = 4194304
+DT = 1.0e-3
+# algorithmic flops per interaction, counted from the reference expressions
+# (BHtree/BHgrav_accel.F90:146-226 quadrupole cell term; gravity/gravity_gradh.F90 pair)
+FLOPS_CELL = 75
+FLOPS_PAIR = 41
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--n", type=int, default=N_FULL, help="particle count (default 4,194,304)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample", type=int, default=0,
+                    help="active particles in the CPU sample (default N, or N/8 above 2^20)")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+def dist_init(n_gpus):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(ws, x):
+    if ws <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling in the background during a timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = max(smax, float(f[2]))
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def workload(n):
+    from seren_b200 import ics
+    t0 = time.time()
+    ic = ics.turbulent_core(n=n, seed=4, sound=0.2, mach=2.0, h_fac=1.2, thetamaxsqd=0.25)
+    log(f"[bench] workload {ic['name']} generated in {time.time() - t0:.1f}s")
+    return ic
+
+
+def params_for(ic, precision):
+    from seren_b200.cabi import Params
+    return Params.make(h_fac=ic["h_fac"], thetamaxsqd=ic["thetamaxsqd"], alpha=ic["alpha"],
+                       precision=precision)
+
+
+def run_resident(ic, precision, steps, warmup, ws):
+    """Device-resident steps; returns timing/stat dict and the final state."""
+    import torch
+
+    from seren_b200.gpu import GpuHotPath
+    n = ic["parray"].shape[0]
+    g = GpuHotPath(n, params_for(ic, precision))
+    g.upload(ic["parray"], ic["v"], ic["sound"] ** 2)
+    stream = torch.cuda.ExternalStream(g.stream())
+    g.force_step(first_call=True)
+    for _ in range(max(warmup, 1) - 1):
+        g.drift(DT)
+        g.force_step(first_call=False)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stage = np.zeros(8)
+    launches = 0
+    torch.cuda.synchronize()
+    barrier(ws)
+    torch.cuda.synchronize()
+    start.record(stream)
+    for _ in range(steps):
+        g.drift(DT)
+        launches += 1
+        g.force_step(first_call=False)
+        ms, nl, counts = g.last_step_stats()
+        stage += np.array(ms)
+        launches += nl
+    end.record(stream)
+    torch.cuda.synchronize()
+    barrier(ws)
+    total_ms = start.elapsed_time(end)
+    state = g.download()
+    res = dict(total_ms=total_ms, stage_ms=(stage / steps).tolist(), launches=launches,
+               counts=counts, ctx=g)
+    return res, state
+
+
+def run_e2e(ic, precision, steps, warmup, ws):
+    """Steps through the host-buffer C ABI, as the Fortran drivers call it, with
+    pinned host buffers; the host applies the permutation to its own arrays,
+    computes the isothermal thermal state and drifts."""
+    import ctypes as C
+
+    import torch
+
+    from seren_b200.gpu import GpuHotPath
+    n = ic["parray"].shape[0]
+    g = GpuHotPath(n, params_for(ic, precision))
+
+    def pinned(shape, dtype=np.float64):
+        t = torch.empty(shape, dtype=torch.float64 if dtype == np.float64 else torch.int32,
+                        pin_memory=True)
+        return t.numpy()
+
+    parray = pinned((n, 6)); parray[:] = ic["parray"]
+    v = pinned((n, 3)); v[:] = ic["v"]
+    v2 = pinned((n, 3))
+    sound = pinned((n,)); sound[:] = ic["sound"]
+    sound2 = pinned((n,))
+    press = pinned((n,))
+    rho = pinned((n,)); omega = pinned((n,)); div_v = pinned((n,)); drhodt = pinned((n,))
+    a = pinned((n, 3)); gpot = pinned((n,))
+    perm = pinned((n,), np.int32)
+    dp = C.POINTER(C.c_double)
+    ip = C.POINTER(C.c_int32)
+    P = lambda x: x.ctypes.data_as(dp)  # noqa: E731
+    ctx = g._ctx
+
+    def step(first):
+        nonlocal v, v2, sound, sound2
+        g._call("tree_update", ctx, n, P(parray), 1, 1, perm.ctypes.data_as(ip))
+        np.take(v, perm, axis=0, out=v2); v, v2 = v2, v
+        np.take(sound, perm, out=sound2); sound, sound2 = sound2, sound
+        g._call("sph_update", ctx, n, None, 0, P(parray), P(v), P(rho), P(omega), P(div_v),
+                P(drhodt), None, None, int(first))
+        np.multiply(sound, sound, out=press); press *= rho
+        g._call("hydro_forces", ctx, None, 0, P(press), P(sound), P(a))
+        g._call("grav_forces", ctx, None, 0, P(a), P(gpot), 0, None)
+        parray[:, 0:3] += v * DT
+
+    stream = torch.cuda.ExternalStream(g.stream())
+    for w in range(max(warmup, 1)):
+        step(w == 0)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    barrier(ws)
+    start.record(stream)
+    for _ in range(steps):
+        step(False)
+    end.record(stream)
+    torch.cuda.synchronize()
+    barrier(ws)
+    total_ms = start.elapsed_time(end)
+    h2d = n * (48 + 24 + 8 + 8 + 24)            # parray, v, press, sound, a (grav adds to it)
+    d2h = n * (48 + 4 + 16 + 32 + 24 + 24 + 8)  # parray+perm, h/zeta, rho..drhodt, a (hydro), a+gpot (grav)
+    g.close()
+    return dict(total_ms=total_ms, h2d=h2d, d2h=d2h)
+
+
+def traffic_per_launch(n):
+    """DRAM bytes of one gravity launch from the committed ncu summary, scaled
+    to n particles (profiles/gravity_mixed_ncu.txt, key dram_bytes_per_particle)."""
+    path = os.path.join(HERE, "profiles", "gravity_mixed_ncu.txt")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("dram_bytes_per_particle"):
+                    return float(line.split("=")[1].split()[0]) * n
+    except OSError:
+        pass
+    return None
+
+
+# ---------------------------------------------------------------------------
+def cpu_eval(ic_tree, sample, first_call=False):
+    """One force evaluation of the CPU oracle (the C++ FP64 restatement of the
+    reference) on all host cores.  The tree is built for all particles; grad-h,
+    neighbour lists, hydro and gravity run for `sample` random active particles
+    (all when sample >= N) and are scaled by N/sample."""
+    from oracle.oracle import Oracle, set_threads
+    cores = set_threads(os.cpu_count() or 1)
+    parray = ic_tree["parray"]
+    n = parray.shape[0]
+    o = Oracle(n, params_for(ic_tree, 0))
+    t0 = time.perf_counter()
+    po, perm = o.tree_update(parray)
+    t1 = time.perf_counter()
+    v = ic_tree["v"][perm]
+    sound = ic_tree["sound"][perm]
+    if sample >= n:
+        act = None
+    else:
+        rng = np.random.Generator(np.random.PCG64(12345))
+        act = np.sort(rng.choice(n, size=sample, replace=False)).astype(np.int32)
+    out = o.sph_update(po, v, first_call=first_call, acclist=act, lists=False)
+    press = sound * sound * out["rho"]
+    a = o.hydro_forces(press, sound, acclist=act)
+    a, gpot = o.grav_forces(a, acclist=act)
+    t2 = time.perf_counter()
+    frac = 1.0 if act is None else n / float(sample)
+    sec = (t1 - t0) + (t2 - t1) * frac
+    return dict(sec=sec, cores=cores, oracle=o, parray=out["parray"], perm=perm, a=a, gpot=gpot,
+                act=act)
+
+
+def accuracy_vs_direct(o, state_a, ids):
+    """rms and max |da|/|a| of accelerations against the FP64 direct sum
+    (sph/direct_sph_gravity.F90) for the particles ids (oracle order)."""
+    ad, _ = o.direct_gravity(ids)
+    err = np.linalg.norm(state_a - ad, axis=1) / np.linalg.norm(ad, axis=1)
+    return float(np.sqrt(np.mean(err ** 2))), float(err.max())
+
+
+# ---------------------------------------------------------------------------
+def main():
+    args = parse()
+    ws, rank, local = dist_init(args.gpus)
+    n = args.n
+    if args.impl == "reference":
+        return reference_arm(args, ws, rank, n)
+    import torch
+    torch.cuda.set_device(local)
+    ic = workload(n)
+    sampler = ClockSampler(local)
+    # mixed precision: the headline
+    sampler.start()
+    mixed, state_m = run_resident(ic, 1, args.steps, args.warmup, ws)
+    clocks = sampler.stop()
+    t_mixed = max_over_ranks(ws, mixed["total_ms"])
+    value = ws * n * args.steps / (t_mixed * 1e-3)
+    g = mixed["ctx"]
+    fp32_peak = g.fma_peak(1)
+    fp64_peak = g.fma_peak(0)
+    ncell, npair = mixed["counts"][0], mixed["counts"][1]
+    flops = FLOPS_CELL * ncell + FLOPS_PAIR * npair
+    grav_ms = mixed["stage_ms"][4]
+    achieved = flops / (grav_ms * 1e-3) / 1e12
+    g.close()
+    fp64 = None
+    acc = {}
+    if not args.no_fp64:
+        f64, state_d = run_resident(ic, 0, args.steps, args.warmup, ws)
+        f64["ctx"].close()
+        fp64 = dict(value=ws * n * args.steps / (max_over_ranks(ws, f64["total_ms"]) * 1e-3),
+                    ms_per_step=f64["total_ms"] / args.steps,
+                    stage_ms=[round(x, 3) for x in f64["stage_ms"][:6]])
+        am, ad = state_m["a"], state_d["a"]
+        # both runs start from the same state and drift identically, so the trees,
+        # the particle order and h agree; compare accelerations row by row
+        same = np.array_equal(state_m["perm"], state_d["perm"])
+        err = np.linalg.norm(am - ad, axis=1) / np.maximum(np.linalg.norm(ad, axis=1), 1e-300)
+        acc = dict(rms_vs_fp64=float(np.sqrt(np.mean(err ** 2))), max_vs_fp64=float(err.max()),
+                   same_order=bool(same))
+    e2e = None
+    if not args.no_e2e:
+        r = run_e2e(ic, 1, args.steps, args.warmup, ws)
+        e2e = dict(value=ws * n * args.steps / (max_over_ranks(ws, r["total_ms"]) * 1e-3),
+                   unit=UNIT, h2d_bytes_per_step=r["h2d"], d2h_bytes_per_step=r["d2h"],
+                   ms_per_step=r["total_ms"] / args.steps)
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        sample = args.cpu_sample or (n if n <= (1 << 20) else n // 8)
+        st = dict(state_m)
+        ic_cpu = dict(parray=st["parray"], v=st["v"], sound=np.sqrt(0.04) * np.ones(n),
+                      h_fac=ic["h_fac"], thetamaxsqd=ic["thetamaxsqd"], alpha=ic["alpha"])
+        r = cpu_eval(ic_cpu, sample)
+        cpu = dict(value=n / r["sec"], unit=UNIT, cores=r["cores"], kind="port",
+                   sample=(f"one force evaluation of the C++ FP64 restatement of the reference "
+                           f"(oracle/) on the state after the GPU run: tree build+stock of all "
+                           f"{n} particles, grad-h/neighbour lists/hydro/gravity for {sample} "
+                           f"random active particles, scaled by N/{sample}; "
+                           f"{r['sec']:.2f} s per evaluation"))
+        # accuracy of the GPU mixed result against the FP64 direct sum on a subset
+        # of the sampled particles (same state: the oracle rebuilt the same tree)
+        o = r["oracle"]
+        ids = r["act"][:: max(1, len(r["act"]) // 256)] if r["act"] is not None else \
+            np.arange(0, n, max(1, n // 256), dtype=np.int32)
+        ids = ids.astype(np.int32)
+        # the GPU state is in GPU tree order; the oracle reordered the same input
+        # with its own (identical) tree, so map GPU rows through the oracle perm
+        am = state_m["a"][r["perm"][ids]]
+        rms_d, max_d = accuracy_vs_direct(o, am, ids)
+        ao = r["a"][ids]
+        rms_t, max_t = accuracy_vs_direct(o, ao, ids)
+        acc.update(rms_vs_direct=rms_d, max_vs_direct=max_d, direct_subset=int(ids.size),
+                   oracle_tree_rms_vs_direct=rms_t)
+        o.close()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_mixed / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32+fp64",
+        "data": "synthetic (seeded turbulent uniform-sphere core, numpy PCG64)",
+        "config": {"workload": f"turbulent molecular-cloud core, N={n} per GPU, uniform sphere "
+                               "R=1 M=1 G=1, isothermal c_s=0.2, P(k)~k^-4 Mach 2, h_fac=1.2 "
+                               "(pp_gather 57), theta^2=0.25 quadrupole geometric MAC, "
+                               "MON97 alpha=1; step = full force evaluation + drift",
+                   "particles": n, "precision": "mixed (FP32 pair arithmetic, FP64 walk/MAC/"
+                   "grad-h)", "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
+                   "l2": "inputs larger than L2 (particles + tree ~1 GB resident)"},
+        "stage_ms": {k: round(x, 3) for k, x in zip(
+            ("tree", "gradh", "neib", "hydro", "gravity", "total"), mixed["stage_ms"][:6])},
+        "fp64": fp64,
+        "mixed_speedup_vs_fp64": (value / fp64["value"]) if fp64 else None,
+        "accuracy": acc,
+        "roofline": {"bound": "fp32", "kernel": "gravity walk (k_grav32)",
+                     "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                     "frac": achieved / fp32_peak, "traffic": traffic_per_launch(n),
+                     "flops_per_launch": flops, "cells": ncell, "pairs": npair,
+                     "launch_ms": grav_ms,
+                     "peak_source": "measured FP32 FMA throughput (seren_gpu_fma_peak); "
+                                    "MEASURED_PEAKS.json has no non-tensor FP32 figure",
+                     "fp64_peak": fp64_peak},
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": mixed["launches"],
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def reference_arm(args, ws, rank, n):
+    """The reference's CPU path (its C++ FP64 restatement in oracle/, since the
+    Fortran reference cannot be compiled here) on the host cores, rank 0 only."""
+    if rank != 0:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    ic = workload(n)
+    sample = args.cpu_sample or (n if n <= (1 << 20) else n // 32)
+    state = dict(parray=ic["parray"].copy(), v=ic["v"], sound=ic["sound"], h_fac=ic["h_fac"],
+                 thetamaxsqd=ic["thetamaxsqd"], alpha=ic["alpha"])
+    total = 0.0
+    cores = 1
+    for k in range(args.warmup + args.steps):
+        r = cpu_eval(state, sample, first_call=(k == 0))
+        cores = r["cores"]
+        # carry h and zeta forward in the oracle's tree order, then drift
+        state["parray"] = r["parray"]
+        state["v"] = state["v"][r["perm"]]
+        state["sound"] = state["sound"][r["perm"]]
+        state["parray"][:, 0:3] += state["v"] * DT
+        r["oracle"].close()
+        if k >= args.warmup:
+            total += r["sec"]
+    value = n * args.steps / total
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp64",
+        "data": "synthetic (seeded turbulent uniform-sphere core, numpy PCG64)",
+        "config": {"workload": f"turbulent molecular-cloud core, N={n}, as the GPU arm",
+                   "particles": n},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": (f"C++ FP64 restatement of the reference (oracle/; the Fortran "
+                                    f"reference has no compiler here): tree of all {n} particles, "
+                                    f"per-particle stages for {sample} random active particles "
+                                    f"scaled by N/{sample}, per step")},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

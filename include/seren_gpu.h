@@ -138,10 +138,22 @@ int seren_gpu_tree_export(seren_gpu_ctx* ctx, int32_t* ctot, int32_t* ltot,
                           double* dminsqd, double* hydro_r /*[ctot+1][3]*/,
                           double* rmax, double* hrangemax);
 
-/* Per-stage device time of the last seren_gpu_force_step (ms) and the
- * number of kernels it launched. */
+/* Per-stage device time of the last seren_gpu_force_step (ms: tree build +
+ * stock, grad-h, hmax update + neighbour lists, thermal + hydro, gravity,
+ * total), the number of kernels it launched, and the interaction counts of
+ * the last gravity call (counts[0] cell terms, counts[1] pair terms). */
 int seren_gpu_last_step_stats(seren_gpu_ctx* ctx, double* stage_ms /*[8]*/,
-                              int32_t* nlaunch);
+                              int32_t* nlaunch, int64_t* counts /*[8]*/);
+
+/* The CUDA stream every kernel of this context runs on (cudaStream_t), so a
+ * caller can order its own work and CUDA events against the library's. */
+int seren_gpu_get_stream(seren_gpu_ctx* ctx, void** stream);
+
+/* Measured FMA throughput of this GPU's FP32 (precision 1) or FP64
+ * (precision 0) pipe in TFLOP/s (2 flops per FMA), from a kernel of
+ * independent FMA chains over every SM; the roofline denominator of the
+ * pair-interaction kernels, which do not use tensor cores. */
+int seren_gpu_fma_peak(seren_gpu_ctx* ctx, int32_t precision, double* tflops);
 
 #ifdef __cplusplus
 }

@@ -100,6 +100,23 @@ __global__ void k_add_base(const int* __restrict__ src, int* __restrict__ dst, l
   if (i < n) dst[i] = src[i] + base;
 }
 
+// independent FMA chains for the pipe-throughput microbenchmark
+constexpr int FMA_CHAINS = 8;
+template <typename T>
+__global__ void k_fma_peak(T* out, int iters, T a, T b) {
+  T x[FMA_CHAINS];
+#pragma unroll
+  for (int k = 0; k < FMA_CHAINS; ++k) x[k] = (T)(threadIdx.x + k);
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < FMA_CHAINS; ++k) x[k] = fma(x[k], a, b);
+  }
+  T s = 0;
+#pragma unroll
+  for (int k = 0; k < FMA_CHAINS; ++k) s += x[k];
+  if (s == (T)-1.2345) out[0] = s;
+}
+
 __global__ void k_drift(int n, double4* __restrict__ pm, const double4* __restrict__ vel, double dt) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -239,7 +256,7 @@ int alloc_all(Ctx& c) {
 void reset_particles(Ctx& c, int ptot) {
   c.ptot = ptot;
   c.have_tree = c.have_sph = c.have_v = c.have_csq = false;
-  k_iota<<<nb(ptot, 256), 256, 0, c.st>>>(c.orig, ptot);
+  k_iota<<<nb(ptot, 256), 256, 0, c.st>>>(c.orig, ptot); ++c.nlaunch;
   cudaMemsetAsync(c.vel, 0, sizeof(double4) * ptot, c.st);
   cudaMemsetAsync(c.csq, 0, sizeof(double) * ptot, c.st);
   cudaMemsetAsync(c.pptot, 0, sizeof(int) * ptot, c.st);
@@ -307,7 +324,10 @@ int seren_gpu_tree_update(seren_gpu_ctx* h, int32_t ptot, double* parray, int32_
   if (do_build && !do_reorder)
     return fail(c, SEREN_GPU_ERR_ARG, "a build requires the particle reorder (REORDER=PARTICLES)");
   if (ptot != c.ptot) seren::reset_particles(c, ptot);
-  else if (do_build) seren::k_iota<<<nb(ptot, 256), 256, 0, c.st>>>(c.orig, ptot);
+  else if (do_build) {
+    seren::k_iota<<<nb(ptot, 256), 256, 0, c.st>>>(c.orig, ptot);
+    ++c.nlaunch;
+  }
   cudaMemcpyAsync(c.stage, parray, sizeof(double) * 6 * (size_t)ptot, cudaMemcpyHostToDevice, c.st);
   seren::launch_unpack_parray(c, c.stage, ptot);
   int rc = finish(c, "tree_update(upload)");
@@ -348,7 +368,7 @@ int seren_gpu_sph_update(seren_gpu_ctx* h, int32_t ptot, const int32_t* acclist,
   if (rc) return rc;
   if (!v) return fail(c, SEREN_GPU_ERR_ARG, "v is NULL");
   cudaMemcpyAsync(c.stage, v, sizeof(double) * 3 * (size_t)ptot, cudaMemcpyHostToDevice, c.st);
-  seren::k_unpack_v<<<nb(ptot, 256), 256, 0, c.st>>>(c.stage, ptot, c.vel);
+  seren::k_unpack_v<<<nb(ptot, 256), 256, 0, c.st>>>(c.stage, ptot, c.vel); ++c.nlaunch;
   c.have_v = true;
   int nact = 0;
   rc = seren::set_active(c, acclist, nacc, nact);
@@ -364,7 +384,7 @@ int seren_gpu_sph_update(seren_gpu_ctx* h, int32_t ptot, const int32_t* acclist,
   if (parray) {
     double* pin = seren::pinned(c, (size_t)2 * ptot);
     if (!pin) return fail(c, SEREN_GPU_ERR_CUDA, "pinned staging allocation failed");
-    seren::k_pack_hz<<<nb(ptot, 256), 256, 0, c.st>>>(c.hz, ptot, c.stage);
+    seren::k_pack_hz<<<nb(ptot, 256), 256, 0, c.st>>>(c.hz, ptot, c.stage); ++c.nlaunch;
     cudaMemcpyAsync(pin, c.stage, sizeof(double) * 2 * (size_t)ptot, cudaMemcpyDeviceToHost, c.st);
     cudaError_t e = cudaStreamSynchronize(c.st);
     if (e != cudaSuccess) return seren::cuda_fail(c, e, "sph_update(h)");
@@ -399,7 +419,7 @@ int seren_gpu_sph_update(seren_gpu_ctx* h, int32_t ptot, const int32_t* acclist,
       int* src = c.pplist;
       if (c.prm.index_base) {
         const long n = (long)ptot * L;
-        seren::k_add_base<<<nb(n, 256), 256, 0, c.st>>>(c.pplist, c.istage + ptot, n, c.prm.index_base);
+        seren::k_add_base<<<nb(n, 256), 256, 0, c.st>>>(c.pplist, c.istage + ptot, n, c.prm.index_base); ++c.nlaunch;
         src = c.istage + ptot;
       }
       if (!acclist) {
@@ -425,7 +445,7 @@ int seren_gpu_get_neib(seren_gpu_ctx* h, int32_t ptot, const int32_t* acclist, i
   if (rc) return rc;
   if (hh) {
     cudaMemcpyAsync(c.stage, hh, sizeof(double) * (size_t)ptot, cudaMemcpyHostToDevice, c.st);
-    seren::k_set_h<<<nb(ptot, 256), 256, 0, c.st>>>(c.stage, ptot, c.hz);
+    seren::k_set_h<<<nb(ptot, 256), 256, 0, c.st>>>(c.stage, ptot, c.hz); ++c.nlaunch;
   }
   int nact = 0;
   rc = seren::set_active(c, acclist, nacc, nact);
@@ -530,7 +550,7 @@ int seren_gpu_upload(seren_gpu_ctx* h, int32_t ptot, const double* parray, const
   int rc = finish(c, "upload(parray)");
   if (rc) return rc;
   cudaMemcpyAsync(c.stage, v, sizeof(double) * 3 * (size_t)ptot, cudaMemcpyHostToDevice, c.st);
-  seren::k_unpack_v<<<nb(ptot, 256), 256, 0, c.st>>>(c.stage, ptot, c.vel);
+  seren::k_unpack_v<<<nb(ptot, 256), 256, 0, c.st>>>(c.stage, ptot, c.vel); ++c.nlaunch;
   cudaMemcpyAsync(c.csq, csq, sizeof(double) * (size_t)ptot, cudaMemcpyHostToDevice, c.st);
   c.have_v = c.have_csq = true;
   return finish(c, "upload");
@@ -543,6 +563,7 @@ int seren_gpu_force_step(seren_gpu_ctx* h, int32_t first_call) {
     return fail(c, SEREN_GPU_ERR_STATE, "call seren_gpu_upload first");
   const int n = c.ptot;
   c.act = nullptr;
+  c.nlaunch = 0;
   cudaEventRecord(c.ev[0], c.st);
   int rc = seren::build_tree(c);
   if (rc) return rc;
@@ -562,6 +583,7 @@ int seren_gpu_force_step(seren_gpu_ctx* h, int32_t first_call) {
   cudaEventRecord(c.ev[5], c.st);
   rc = finish(c, "force_step");
   if (rc) return rc;
+  c.step_launches = c.nlaunch;
   c.have_sph = true;
   for (int k = 0; k < 5; ++k) {
     float ms = 0.f;
@@ -578,7 +600,7 @@ int seren_gpu_drift(seren_gpu_ctx* h, double dt) {
   if (!h) return SEREN_GPU_ERR_ARG;
   Ctx& c = h->c;
   if (!c.have_v) return fail(c, SEREN_GPU_ERR_STATE, "no velocities");
-  seren::k_drift<<<nb(c.ptot, 256), 256, 0, c.st>>>(c.ptot, c.pm, c.vel, dt);
+  seren::k_drift<<<nb(c.ptot, 256), 256, 0, c.st>>>(c.ptot, c.pm, c.vel, dt); ++c.nlaunch;
   return finish(c, "drift");
 }
 
@@ -595,7 +617,7 @@ int seren_gpu_download(seren_gpu_ctx* h, double* parray, double* v, double* rho,
     if (rc) return rc;
   }
   if (v) {
-    seren::k_pack_v<<<nb(n, 256), 256, 0, c.st>>>(c.stage, n, c.vel);
+    seren::k_pack_v<<<nb(n, 256), 256, 0, c.st>>>(c.stage, n, c.vel); ++c.nlaunch;
     cudaMemcpyAsync(v, c.stage, sizeof(double) * 3 * (size_t)n, cudaMemcpyDeviceToHost, c.st);
     int rc = finish(c, "download(v)");
     if (rc) return rc;
@@ -659,11 +681,49 @@ int seren_gpu_tree_export(seren_gpu_ctx* h, int32_t* ctot, int32_t* ltot, int32_
   return SEREN_GPU_OK;
 }
 
-int seren_gpu_last_step_stats(seren_gpu_ctx* h, double* stage_ms, int32_t* nlaunch) {
+int seren_gpu_last_step_stats(seren_gpu_ctx* h, double* stage_ms, int32_t* nlaunch,
+                              int64_t* counts) {
   if (!h) return SEREN_GPU_ERR_ARG;
+  Ctx& c = h->c;
   if (stage_ms)
-    for (int k = 0; k < 8; ++k) stage_ms[k] = h->c.stage_ms[k];
-  if (nlaunch) *nlaunch = h->c.nlaunch;
+    for (int k = 0; k < 8; ++k) stage_ms[k] = c.stage_ms[k];
+  if (nlaunch) *nlaunch = c.step_launches;
+  if (counts) {
+    unsigned long long cc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    cudaMemcpy(cc, c.d_counts, sizeof(cc), cudaMemcpyDeviceToHost);
+    for (int k = 0; k < 8; ++k) counts[k] = (int64_t)cc[k];
+  }
+  return SEREN_GPU_OK;
+}
+
+int seren_gpu_get_stream(seren_gpu_ctx* h, void** stream) {
+  if (!h || !stream) return SEREN_GPU_ERR_ARG;
+  *stream = (void*)h->c.st;
+  return SEREN_GPU_OK;
+}
+
+int seren_gpu_fma_peak(seren_gpu_ctx* h, int32_t precision, double* tflops) {
+  if (!h || !tflops || (precision != 0 && precision != 1)) return SEREN_GPU_ERR_ARG;
+  Ctx& c = h->c;
+  int nsm = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c.dev);
+  const int blocks = nsm * 4, threads = 256, iters = 2048;
+  float best = 1e30f;
+  for (int rep = 0; rep < 3; ++rep) {
+    cudaEventRecord(c.ev[8], c.st);
+    if (precision == 1)
+      seren::k_fma_peak<float><<<blocks, threads, 0, c.st>>>(reinterpret_cast<float*>(c.stage), iters, 0.999f, 1.0e-3f);
+    else
+      seren::k_fma_peak<double><<<blocks, threads, 0, c.st>>>(c.stage, iters, 0.999, 1.0e-3);
+    cudaEventRecord(c.ev[9], c.st);
+    int rc = finish(c, "fma_peak");
+    if (rc) return rc;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c.ev[8], c.ev[9]);
+    best = ms < best ? ms : best;
+  }
+  const double flops = 2.0 * seren::FMA_CHAINS * (double)iters * blocks * threads;
+  *tflops = flops / (best * 1e-3) / 1e12;
   return SEREN_GPU_OK;
 }
 

@@ -103,7 +103,8 @@ struct Ctx {
   // timing of the last force step
   cudaEvent_t ev[10] = {};
   double stage_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  int nlaunch = 0;
+  int nlaunch = 0;          // kernels launched since the counter was reset
+  int step_launches = 0;    // kernels of the last seren_gpu_force_step
 };
 
 // tree.cu

@@ -458,12 +458,13 @@ void launch_grav(Ctx& c, int nact, int nsink, const double* d_sinks) {
   else
     k_grav32<<<nb(nact, 128), 128, 0, c.st>>>(nact, c.act, c.pm, c.hz, grav_tree(c), c.tabG, c.acc,
                                               c.gpot, nsink, d_sinks, c.d_err, counts);
+  ++c.nlaunch;
 }
 
 void launch_sink_walk(Ctx& c, int nsink, const double* d_sinks, double* d_out) {
   if (nsink <= 0) return;
   k_sink_walk<<<nb(nsink, 32), 32, 0, c.st>>>(nsink, d_sinks, c.pm, c.hz, grav_tree(c), c.tabG,
-                                              d_out, c.d_err);
+                                              d_out, c.d_err); ++c.nlaunch;
 }
 
 }  // namespace seren

@@ -358,24 +358,24 @@ void launch_gradh(Ctx& c, int nact) {
   if (nact <= 0) return;
   k_gradh<<<nb(nact, 128), 128, 0, c.st>>>(nact, c.act, c.pm, c.hz, c.vel, c.rho, c.omega, c.div_v,
                                            c.drhodt, hydro_tree(c), c.tabA, c.prm.h_fac,
-                                           c.prm.pp_gather, c.info.rextent, c.d_err);
+                                           c.prm.pp_gather, c.info.rextent, c.d_err); ++c.nlaunch;
 }
 
 void launch_neib(Ctx& c, int nact) {
   if (nact <= 0) return;
   k_neib<<<nb(nact, 128), 128, 0, c.st>>>(nact, c.act, c.pm, c.hz, hydro_tree(c), c.prm.pp_limit,
-                                          c.pptot, c.pplist, c.d_err);
+                                          c.pptot, c.pplist, c.d_err); ++c.nlaunch;
 }
 
 void launch_hydro(Ctx& c, int nact) {
   if (nact <= 0) return;
   k_hydro<<<nb(nact, 128), 128, 0, c.st>>>(nact, c.act, c.pm, c.hz, c.vel, c.rho, c.omega, c.press,
                                            c.sound, c.pptot, c.pplist, c.prm.pp_limit,
-                                           hydro_tree(c), c.tabG, c.prm.alpha, c.acc, c.d_err);
+                                           hydro_tree(c), c.tabG, c.prm.alpha, c.acc, c.d_err); ++c.nlaunch;
 }
 
 void launch_thermal(Ctx& c) {
-  k_thermal<<<nb(c.ptot, 256), 256, 0, c.st>>>(c.ptot, c.csq, c.rho, c.press, c.sound);
+  k_thermal<<<nb(c.ptot, 256), 256, 0, c.st>>>(c.ptot, c.csq, c.rho, c.press, c.sound); ++c.nlaunch;
 }
 
 }  // namespace seren

@@ -561,13 +561,13 @@ int scan_scratch_alloc(ScanScratch& s, int nmax) {
 static void scan_rec(Ctx& c, const int* in, int* out, int n, int lv) {
   const int nblk = nb(n, SCAN_TILE);
   int* sums = c.scan.level_buf[lv];
-  k_scan_tile<<<nblk, SCAN_T, 0, c.st>>>(in, out, n, sums);
+  k_scan_tile<<<nblk, SCAN_T, 0, c.st>>>(in, out, n, sums); ++c.nlaunch;
   if (nblk == 1) {
-    k_copy_int<<<1, 1, 0, c.st>>>(sums, c.scan.total);
+    k_copy_int<<<1, 1, 0, c.st>>>(sums, c.scan.total); ++c.nlaunch;
     return;
   }
   scan_rec(c, sums, sums, nblk, lv + 1);
-  k_scan_add<<<nblk, SCAN_T, 0, c.st>>>(out, n, sums);
+  k_scan_add<<<nblk, SCAN_T, 0, c.st>>>(out, n, sums); ++c.nlaunch;
 }
 
 void scan_exclusive(Ctx& c, const int* in, int* out, int n) {
@@ -579,11 +579,11 @@ void scan_exclusive(Ctx& c, const int* in, int* out, int n) {
 }
 
 void launch_unpack_parray(Ctx& c, const double* stage, int n) {
-  k_unpack_parray<<<nb(n, 256), 256, 0, c.st>>>(stage, n, c.pm, c.hz, c.d_err);
+  k_unpack_parray<<<nb(n, 256), 256, 0, c.st>>>(stage, n, c.pm, c.hz, c.d_err); ++c.nlaunch;
 }
 
 void launch_pack_parray(Ctx& c, double* stage, int n) {
-  k_pack_parray<<<nb(n, 256), 256, 0, c.st>>>(stage, n, c.pm, c.hz);
+  k_pack_parray<<<nb(n, 256), 256, 0, c.st>>>(stage, n, c.pm, c.hz); ++c.nlaunch;
 }
 
 static int radix_sort(Ctx& c, int n) {
@@ -593,9 +593,9 @@ static int radix_sort(Ctx& c, int n) {
   int* va = c.idx;
   int* vb = c.idx_alt;
   for (int shift = 0; shift < 64; shift += 8) {
-    k_rs_hist<<<nblk, RS_T, 0, c.st>>>(ka, n, shift, c.rs_hist, nblk);
+    k_rs_hist<<<nblk, RS_T, 0, c.st>>>(ka, n, shift, c.rs_hist, nblk); ++c.nlaunch;
     scan_exclusive(c, c.rs_hist, c.rs_hist, 256 * nblk);
-    k_rs_scatter<<<nblk, RS_T, 0, c.st>>>(ka, va, kb, vb, n, shift, c.rs_hist, nblk);
+    k_rs_scatter<<<nblk, RS_T, 0, c.st>>>(ka, va, kb, vb, n, shift, c.rs_hist, nblk); ++c.nlaunch;
     std::swap(ka, kb);
     std::swap(va, vb);
   }
@@ -606,12 +606,12 @@ static int radix_sort(Ctx& c, int n) {
 int build_tree(Ctx& c) {
   const int n = c.ptot;
   const int bblk = std::min(nb(n, BB_T), 1184);
-  k_bbox_partial<<<bblk, BB_T, 0, c.st>>>(c.pm, n, c.bbox_part);
-  k_bbox_final<<<1, 1, 0, c.st>>>(c.bbox_part, bblk, c.d_info);
-  k_keys<<<nb(n, 256), 256, 0, c.st>>>(c.pm, n, c.d_info, c.keys, c.idx);
+  k_bbox_partial<<<bblk, BB_T, 0, c.st>>>(c.pm, n, c.bbox_part); ++c.nlaunch;
+  k_bbox_final<<<1, 1, 0, c.st>>>(c.bbox_part, bblk, c.d_info); ++c.nlaunch;
+  k_keys<<<nb(n, 256), 256, 0, c.st>>>(c.pm, n, c.d_info, c.keys, c.idx); ++c.nlaunch;
   radix_sort(c, n);
   k_root<<<1, 1, 0, c.st>>>(n, c.cmax, c.leaf, c.nextcell, c.ifopen, c.pstart, c.pcount, c.parent,
-                            c.level, c.branch, c.d_info);
+                            c.level, c.branch, c.d_info); ++c.nlaunch;
   int nbranch = 1, ctot = 0, lev = 0;
   int* br = c.branch;
   int* br_next = c.branch_next;
@@ -621,7 +621,7 @@ int build_tree(Ctx& c) {
       return SEREN_GPU_ERR_LMAX;
     }
     k_split<<<nb(nbranch, 128), 128, 0, c.st>>>(br, c.d_info, lev, c.pstart, c.pcount, c.keys,
-                                                c.nchild, c.cstart);
+                                                c.nchild, c.cstart); ++c.nlaunch;
     scan_exclusive(c, c.nchild, c.choff, nbranch);
     int nnew = 0;
     cudaMemcpyAsync(&nnew, c.scan.total, sizeof(int), cudaMemcpyDeviceToHost, c.st);
@@ -633,10 +633,10 @@ int build_tree(Ctx& c) {
     }
     k_emit<<<nb(nbranch, 128), 128, 0, c.st>>>(br, c.d_info, lev, c.choff, c.cstart, level_first,
                                                c.leaf, c.nextcell, c.ifopen, c.pstart, c.pcount,
-                                               c.parent, c.level, c.bflag);
+                                               c.parent, c.level, c.bflag); ++c.nlaunch;
     scan_exclusive(c, c.bflag, c.bscan, nnew);
-    k_next_branch<<<nb(nnew, 256), 256, 0, c.st>>>(c.bflag, c.bscan, nnew, level_first, br_next);
-    k_level_done<<<1, 1, 0, c.st>>>(c.d_info, lev, level_first, nnew, c.scan.total);
+    k_next_branch<<<nb(nnew, 256), 256, 0, c.st>>>(c.bflag, c.bscan, nnew, level_first, br_next); ++c.nlaunch;
+    k_level_done<<<1, 1, 0, c.st>>>(c.d_info, lev, level_first, nnew, c.scan.total); ++c.nlaunch;
     int nbn = 0;
     cudaMemcpyAsync(&nbn, c.scan.total, sizeof(int), cudaMemcpyDeviceToHost, c.st);
     if (cudaStreamSynchronize(c.st) != cudaSuccess) return SEREN_GPU_ERR_CUDA;
@@ -646,16 +646,16 @@ int build_tree(Ctx& c) {
     nbranch = nbn;
     if (nbranch == 0) break;
   }
-  k_leaf_order<<<nb(ctot + 1, 256), 256, 0, c.st>>>(c.leaf, c.pstart, ctot, c.idx);
+  k_leaf_order<<<nb(ctot + 1, 256), 256, 0, c.st>>>(c.leaf, c.pstart, ctot, c.idx); ++c.nlaunch;
   k_reorder<<<nb(n, 256), 256, 0, c.st>>>(c.idx, n, c.pm, c.hz, c.vel, c.csq, c.orig, c.pm_alt,
-                                           c.hz_alt, c.vel_alt, c.csq_alt, c.orig_alt);
+                                           c.hz_alt, c.vel_alt, c.csq_alt, c.orig_alt); ++c.nlaunch;
   std::swap(c.pm, c.pm_alt);
   std::swap(c.hz, c.hz_alt);
   std::swap(c.vel, c.vel_alt);
   std::swap(c.csq, c.csq_alt);
   std::swap(c.orig, c.orig_alt);
   k_pack_link<<<nb(ctot + 1, 256), 256, 0, c.st>>>(ctot, c.leaf, c.nextcell, c.ifopen, c.pstart,
-                                                   c.link);
+                                                   c.link); ++c.nlaunch;
   cudaMemcpyAsync(&c.info, c.d_info, sizeof(TreeInfo), cudaMemcpyDeviceToHost, c.st);
   if (cudaStreamSynchronize(c.st) != cudaSuccess) return SEREN_GPU_ERR_CUDA;
   c.have_tree = true;
@@ -669,7 +669,7 @@ void launch_stock(Ctx& c) {
     const int cnt = la - f + 1;
     if (cnt <= 0) continue;
     k_stock_level<<<nb(cnt, 128), 128, 0, c.st>>>(f, la, c.link, c.pm, c.hz, c.prm.thetamaxsqd, daux,
-                                                 c.gA, c.gB, c.gC, c.hA, c.hmax, c.bbmin, c.bbmax);
+                                                 c.gA, c.gB, c.gC, c.hA, c.hmax, c.bbmin, c.bbmax); ++c.nlaunch;
   }
 }
 
@@ -678,14 +678,14 @@ void launch_update_hmax(Ctx& c) {
     const int f = c.info.first_cell[l], la = c.info.last_cell[l];
     const int cnt = la - f + 1;
     if (cnt <= 0) continue;
-    k_hmax_level<<<nb(cnt, 128), 128, 0, c.st>>>(f, la, c.link, c.hz, c.hrm);
+    k_hmax_level<<<nb(cnt, 128), 128, 0, c.st>>>(f, la, c.link, c.hz, c.hrm); ++c.nlaunch;
   }
 }
 
 void launch_hguess(Ctx& c) {
   const int thresh = (int)(0.5 * (double)c.prm.pp_gather);
   k_hguess<<<nb(c.info.ctot + 1, 256), 256, 0, c.st>>>(c.info.ctot, c.link, c.pcount, c.parent,
-                                                       c.level, c.hA, thresh, c.hz);
+                                                       c.level, c.hA, thresh, c.hz); ++c.nlaunch;
 }
 
 }  // namespace seren

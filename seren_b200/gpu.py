@@ -35,7 +35,9 @@ def library(build_if_missing: bool = True) -> C.CDLL:
                            ("force_step", [vp, C.c_int32]),
                            ("drift", [vp, C.c_double]),
                            ("download", [vp, _dp, _dp, _dp, _dp, _dp, _dp, _ip]),
-                           ("last_step_stats", [vp, _dp, _ip])):
+                           ("last_step_stats", [vp, _dp, _ip, C.POINTER(C.c_int64)]),
+                           ("get_stream", [vp, C.POINTER(C.c_void_p)]),
+                           ("fma_peak", [vp, C.c_int32, _dp])):
             fn = getattr(lib, f"seren_gpu_{name}")
             fn.argtypes = args
             fn.restype = C.c_int
@@ -76,7 +78,22 @@ class GpuHotPath(HotPath):
         return out
 
     def last_step_stats(self):
+        """(stage milliseconds [8], kernel launches, interaction counts [8]) of the
+        last force_step; counts[0] cell terms, counts[1] pair terms."""
         ms = (C.c_double * 8)()
         nl = C.c_int32()
-        self._call("last_step_stats", self._ctx, ms, C.byref(nl))
-        return list(ms), nl.value
+        cnt = (C.c_int64 * 8)()
+        self._call("last_step_stats", self._ctx, ms, C.byref(nl), cnt)
+        return list(ms), nl.value, list(cnt)
+
+    def stream(self) -> int:
+        """The cudaStream_t (as an int) all kernels of this context run on."""
+        s = C.c_void_p()
+        self._call("get_stream", self._ctx, C.byref(s))
+        return int(s.value or 0)
+
+    def fma_peak(self, precision: int) -> float:
+        """Measured FMA throughput in TFLOP/s of the FP32 (1) or FP64 (0) pipe."""
+        t = C.c_double()
+        self._call("fma_peak", self._ctx, int(precision), C.byref(t))
+        return t.value

@@ -148,7 +148,7 @@ def turbulent_velocity(pos: np.ndarray, seed: int, ngrid: int = 128, index: floa
     vx = vx - kx * kdotv
     vy = vy - ky * kdotv
     vz = vz - kz * kdotv
-    grid = [np.fft.irfftn(c, s=(ng, ng, ng)) for c in (vx, vy, vz)]
+    grid = [np.fft.irfftn(c, s=(ng, ng, ng), axes=(0, 1, 2)) for c in (vx, vy, vz)]
     # trilinear interpolation on the periodic grid (cell-centred at (i+0.5)*dx - box/2)
     dx = box / ng
     g = (pos + 0.5 * box) / dx - 0.5

@@ -1,0 +1,178 @@
+"""The CPU oracle: kernel tables, tree structure, physical invariants of the
+reference's algorithm (the checks the reference's own physics relies on,
+since it ships no test vectors), and its error handling."""
+import numpy as np
+import pytest
+
+from oracle.oracle import KERNTOT, Oracle, kernel_tables
+from seren_b200 import ics
+from seren_b200.cabi import Params, SerenError
+from tests.helpers import case, params, rel_rows, run_pipeline
+
+S = (2.0 * np.arange(KERNTOT + 1) + 1.0) / KERNTOT
+
+
+def test_kernel_normalisation():
+    """Integral of W over 3-D space is 1 (setup/kernel.F90 M4, 3-D norm INVPI)."""
+    w0 = kernel_tables(0)[0]
+    ds = 2.0 / KERNTOT
+    integral = np.sum(4.0 * np.pi * S[:KERNTOT] ** 2 * w0[:KERNTOT]) * ds
+    assert abs(integral - 1.0) < 1e-6
+
+
+def test_kernel_identities():
+    t = kernel_tables(0)
+    w0, w1, w4, w5, w6, wh = t[0], t[1], t[4], t[5], t[6], t[7]
+    assert np.array_equal(w1, w4)                       # M4: gradient table used twice
+    # wh = -NDIM*w0 - s*w4 (kernel.F90:84, the commented identity)
+    assert np.max(np.abs(wh - (-3.0 * w0 - S * w4))) < 1e-12
+    # softened force and potential approach 1/s^2 and 1/s at s >= 2
+    assert abs(w5[KERNTOT] - 1.0 / S[KERNTOT] ** 2) < 1e-6
+    assert abs(w6[KERNTOT] - 1.0 / S[KERNTOT]) < 1e-6
+
+
+def test_thomas_couchman_table():
+    t0, t1 = kernel_tables(0), kernel_tables(1)
+    kerntc = int(KERNTOT / 3.0)
+    assert np.all(t1[1, :kerntc] == -1.0 * 0.318309886)
+    assert np.array_equal(t1[1, kerntc:], t0[1, kerntc:])
+    assert np.array_equal(np.delete(t1, 1, 0), np.delete(t0, 1, 0))
+
+
+def test_pp_gather():
+    assert ics.pp_gather_for(1.2) == 57          # initialize_seren_variables_1.F90:36
+    assert ics.pp_gather_for(ics.h_fac_for(50)) in (49, 50)
+
+
+@pytest.mark.parametrize("name", ["sphere4k", "plummer16k", "ragged777"])
+def test_tree_structure(name):
+    ic = case(name)
+    n = ic["parray"].shape[0]
+    o = Oracle(n, params(ic))
+    p, perm = o.tree_update(ic["parray"])
+    t = o.tree_export()
+    assert np.array_equal(np.sort(perm), np.arange(n))
+    assert np.array_equal(p, ic["parray"][perm])
+    leaf = t["leaf"]
+    assert leaf[0] == 0 and leaf.max() <= 8
+    # leaves in depth-first order list every particle once, in tree order 0..n-1
+    order = []
+    c = 0
+    while c <= t["ctot"]:
+        if leaf[c] > 0:
+            order.extend(t["plist"][c, :leaf[c]].tolist())
+            c = t["nextcell"][c]
+        else:
+            c = t["ifopen"][c]
+    assert order == list(range(n))
+    # levels partition the cell ids
+    assert t["first_cell"][0] == 0 and t["last_cell"][-1] == t["ctot"]
+    assert np.all(t["first_cell"][1:] == t["last_cell"][:-1] + 1)
+    # every cell mass is the sum of its particles; the root holds the total mass
+    assert abs(t["grav_m"][0] - ic["parray"][:, 3].sum()) < 1e-12
+
+
+def test_leaf_lists_keep_input_order():
+    """Within a leaf the reference keeps the particles' input order
+    (linked lists, BHgrav_build.F90:170-182)."""
+    ic = case("sphere4k")
+    o = Oracle(4096, params(ic))
+    _, perm = o.tree_update(ic["parray"])
+    t = o.tree_export()
+    for c in np.nonzero(t["leaf"] > 1)[0]:
+        ids = perm[t["plist"][c, :t["leaf"][c]]]
+        assert np.all(np.diff(ids) > 0)
+
+
+def test_hydro_conserves_momentum():
+    ic = case("turb20k")
+    o = Oracle(20000, params(ic))
+    r = run_pipeline(o, ic)
+    m = r["parray"][:, 3]
+    mom = np.abs((m[:, None] * r["a_hydro"]).sum(0))
+    scale = np.sum(m[:, None] * np.abs(r["a_hydro"]))
+    assert np.all(mom < 1e-13 * scale)
+
+
+def test_tree_tends_to_direct_sum():
+    """theta -> 0 opens every cell: the walk becomes direct_sph_gravity."""
+    ic = case("sphere4k")
+    o = Oracle(4096, params(ic, thetamaxsqd=1e-8))
+    r = run_pipeline(o, ic)
+    ids = np.arange(0, 4096, 7, dtype=np.int32)
+    ad, gd = o.direct_gravity(ids)
+    ag = r["a"] - r["a_hydro"]
+    assert rel_rows(ag[ids], ad).max() < 1e-12
+    assert rel_rows(r["gpot"][ids], gd).max() < 1e-12
+
+
+def test_tree_error_at_theta_half():
+    ic = case("sphere32k")
+    o = Oracle(32768, params(ic))
+    r = run_pipeline(o, ic)
+    ids = np.arange(0, 32768, 64, dtype=np.int32)
+    ad, _ = o.direct_gravity(ids)
+    err = rel_rows((r["a"] - r["a_hydro"])[ids], ad)
+    assert np.sqrt(np.mean(err ** 2)) < 5e-3
+
+
+def test_direct_sum_plummer_analytic():
+    """Direct-sum gravity of a Plummer sphere follows -M r / (r^2 + a^2)^1.5."""
+    ic = ics.plummer(n=8192, seed=21)
+    ic["sound"] = np.full(8192, 0.1)
+    o = Oracle(8192, params(ic))
+    r = run_pipeline(o, ic)
+    ids = np.arange(0, 8192, 8, dtype=np.int32)
+    ad, _ = o.direct_gravity(ids)
+    x = r["parray"][ids, :3]
+    rr = np.linalg.norm(x, axis=1)
+    sel = (rr > 0.3) & (rr < 3.0)
+    ana = rr[sel] / (rr[sel] ** 2 + 1.0) ** 1.5
+    ratio = np.linalg.norm(ad[sel], axis=1) / ana
+    assert abs(np.median(ratio) - 1.0) < 0.05
+
+
+def test_uniform_density():
+    """SPH density inside a uniform sphere is near 3M/(4 pi R^3); the Poisson
+    sampling and the self term bias it high by tens of per cent, not more."""
+    ic = case("sphere32k")
+    o = Oracle(32768, params(ic))
+    r = run_pipeline(o, ic)
+    rr = np.linalg.norm(r["parray"][:, :3], axis=1)
+    rho = r["sph"]["rho"][rr < 0.6]
+    ratio = np.median(rho) / (3.0 / (4.0 * np.pi))
+    assert 1.0 < ratio < 1.5
+    nn = r["sph"]["pptot"][rr < 0.6]
+    assert 40 < np.median(nn) < 80
+
+
+def test_error_codes():
+    ic = case("tiny100")
+    o = Oracle(50, params(ic))
+    with pytest.raises(SerenError) as e:
+        o.tree_update(ic["parray"])
+    assert e.value.code == 2                  # ptot > pmax: capacity
+    o = Oracle(100, params(ic))
+    bad = ic["parray"].copy()
+    bad[5, 1] = np.nan
+    with pytest.raises(SerenError) as e:
+        o.tree_update(bad)
+    assert e.value.code == 4                  # non-finite input
+    same = ic["parray"].copy()
+    same[:20, :3] = 0.25                      # 20 coincident particles: the tree cannot split them
+    with pytest.raises(SerenError) as e:
+        o.tree_update(same)
+    assert e.value.code == 3
+    with pytest.raises(SerenError):
+        Oracle(100, Params.make(h_fac=1.2, index_base=2))
+
+
+def test_too_few_particles_is_an_error():
+    """With fewer particles than pp_gather the reference grows h forever; the
+    restatement stops with ERR_WALK."""
+    ic = ics.uniform_sphere(n=40, seed=1)
+    o = Oracle(40, params(ic))
+    p, perm = o.tree_update(ic["parray"])
+    with pytest.raises(SerenError) as e:
+        o.sph_update(p, ic["v"][perm], first_call=True)
+    assert e.value.code == 5
