@@ -231,7 +231,8 @@ def run_e2e(ic, precision, steps, warmup, ws):
         np.take(sound, perm, out=sound2); sound, sound2 = sound2, sound
         g._call("sph_update", ctx, n, None, 0, P(parray), P(v), P(rho), P(omega), P(div_v),
                 P(drhodt), None, None, int(first))
-        np.multiply(sound, sound, out=press); press *= rho
+        np.multiply(sound, sound, out=press)
+        np.multiply(press, rho, out=press)
         g._call("hydro_forces", ctx, None, 0, P(press), P(sound), P(a))
         g._call("grav_forces", ctx, None, 0, P(a), P(gpot), 0, None)
         parray[:, 0:3] += v * DT
@@ -326,6 +327,8 @@ def main():
     clocks = sampler.stop()
     t_mixed = max_over_ranks(ws, mixed["total_ms"])
     value = ws * n * args.steps / (t_mixed * 1e-3)
+    log(f"[bench] mixed: {t_mixed / args.steps:.2f} ms/step, stages {mixed['stage_ms'][:6]}, "
+        f"launches {mixed['launches']}, counts {mixed['counts'][:2]}, clocks {clocks}")
     g = mixed["ctx"]
     fp32_peak = g.fma_peak(1)
     fp64_peak = g.fma_peak(0)
@@ -349,6 +352,7 @@ def main():
         err = np.linalg.norm(am - ad, axis=1) / np.maximum(np.linalg.norm(ad, axis=1), 1e-300)
         acc = dict(rms_vs_fp64=float(np.sqrt(np.mean(err ** 2))), max_vs_fp64=float(err.max()),
                    same_order=bool(same))
+        log(f"[bench] fp64: {fp64['ms_per_step']:.2f} ms/step, stages {fp64['stage_ms']}, {acc}")
     e2e = None
     if not args.no_e2e:
         r = run_e2e(ic, 1, args.steps, args.warmup, ws)

@@ -81,6 +81,8 @@ struct Ctx {
   double4* gA = nullptr;      // gravity: COM x, y, z, m
   double4* gB = nullptr;      // gravity: q1..q4 (xx, xy, yy, zx)
   double2* gC = nullptr;      // gravity: q5 (zy), dminsqd
+  float4* wA = nullptr;       // gravity walk: FP32 COM - root centre, upper MAC bracket
+  float* wLo = nullptr;       // gravity walk: lower MAC bracket
   double4* hA = nullptr;      // hydro: bbox centre x, y, z, rmax
   double* hrm = nullptr;      // hydro: hrangemax
   double* hmax = nullptr;     // stock: max h in the cell (at stock time)

@@ -209,163 +209,186 @@ __device__ __forceinline__ void count_add(unsigned long long* counts, unsigned l
   }
 }
 
-// BHtree/BHgrav_accel.F90:21-348 for SPH particles, FP64 arithmetic
-__global__ void __launch_bounds__(128) k_grav64(int nact, const int* __restrict__ act,
-                                                const double4* __restrict__ pm,
-                                                const double2* __restrict__ hz, GravTree t,
-                                                const double4* __restrict__ tabG,
-                                                double* __restrict__ acc, double* __restrict__ gpot,
-                                                int nsink, const double* __restrict__ sinks,
-                                                DevError* err, unsigned long long* counts) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool live = i < nact;
-  const int p = live ? (act ? act[i] : i) : 0;
-  unsigned long long ncell = 0, npair = 0;
-  if (live) {
-    const double4 P = pm[p];
-    const double2 HZ = hz[p];
-    const double invhp = 1.0 / HZ.x;
-    const double zo_p = HZ.y;
-    double cx = 0.0, cy = 0.0, cz = 0.0, cp = 0.0;   // cell terms in walk order
-    double px = 0.0, py = 0.0, pz = 0.0, pp = 0.0;   // near-field terms in walk order
-    int c = 0, visits = 0;
-    const int cap = t.ctot + 2;
-    while (true) {
-      if (++visits > cap) {
-        set_error(err, SEREN_GPU_ERR_WALK, KID_GRAV, p, c);
-        break;
-      }
-      const int4 lk = t.link[c];
-      if (lk.x == 1) {                                                   // :128-136
-        const int q = lk.w;
-        if (q != p) {
-          const double4 Q = pm[q];
-          const double2 hq = hz[q];
-          pair_term64(Q.x - P.x, Q.y - P.y, Q.z - P.z, invhp, zo_p, Q.w, hq.x, hq.y, tabG, px, py, pz, pp);
-          ++npair;
-        }
-        c = lk.y;
-      } else {
-        const double4 a = t.gA[c];
-        const double d0 = P.x - a.x, d1 = P.y - a.y, d2 = P.z - a.z;        // :146-147
-        const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
-        const double2 cc = t.gC[c];
-        if (drsqd > cc.y) {                                              // :155
-          cell_term64(d0, d1, d2, drsqd, a, t.gB[c], cc.x, cx, cy, cz, cp);
-          ++ncell;
-          c = lk.y;
-        } else if (lk.x > 0) {                                           // :242-253
-          for (int k = 0; k < lk.x; ++k) {
-            const int q = lk.w + k;
-            if (q == p) continue;
-            const double4 Q = pm[q];
-            const double2 hq = hz[q];
-            pair_term64(Q.x - P.x, Q.y - P.y, Q.z - P.z, invhp, zo_p, Q.w, hq.x, hq.y, tabG, px, py, pz, pp);
-            ++npair;
-          }
-          c = lk.y;
-        } else if (lk.x == 0) {
-          c = lk.z;
-        } else {
-          c = lk.y;
-        }
-      }
-      if (c > t.ctot) break;
-    }
-    double* a = acc + (size_t)p * 3;
-    a[0] = a[0] + (cx + px);
-    a[1] = a[1] + (cy + py);
-    a[2] = a[2] + (cz + pz);
-    double pot = cp + pp;
-    if (nsink > 0) {                                   // sinks/direct_sink_gravity.F90:10-64
-      double sx = 0.0, sy = 0.0, sz = 0.0, sp = 0.0;
-      for (int s = 0; s < nsink; ++s) {
-        const double* sr = sinks + s * 5;
-        meanh_term64(sr[0] - P.x, sr[1] - P.y, sr[2] - P.z, 0.5 * (HZ.x + sr[4]), sr[3], tabG, sx,
-                     sy, sz, sp);
-      }
-      a[0] = a[0] + sx;
-      a[1] = a[1] + sy;
-      a[2] = a[2] + sz;
-      pot = pot + sp;
-    }
-    gpot[p] = pot;
-  }
-  count_add(counts, ncell, npair);
-}
+// ---------------------------------------------------------------------------
+// Warp-cooperative walk.  One warp walks the tree once for 32 consecutive
+// particles (tree order: spatially adjacent) with the reference's per-particle
+// decisions intact: the walk position c is warp-uniform, each lane keeps a
+// skip marker (the nextcell of the highest cell it accepted while another lane
+// opened it; leaving any subtree lands exactly on its nextcell), and the MAC
+// test of each lane is the reference's drsqd > dminsqd.  That test runs first
+// in FP32 on root-relative coordinates against a bracket [lo, hi] around
+// dminsqd that covers the FP32 rounding; inside the bracket it is redone in
+// FP64 exactly as BHgrav_accel.F90:146-155 does, so every decision equals the
+// FP64 one.  Accepted cells and opened leaves go to per-warp lists in shared
+// memory with the mask of the lanes they belong to; a full list is flushed by
+// all lanes together (broadcast loads, per-lane predicate).
+constexpr int GW_THREADS = 128;
+constexpr int GW_WARPS = GW_THREADS / 32;
+constexpr int GW_CAP = 64;
+constexpr unsigned FULLMASK = 0xffffffffu;
 
-// the same walk, mixed-precision interaction arithmetic
-__global__ void __launch_bounds__(128) k_grav32(int nact, const int* __restrict__ act,
-                                                const double4* __restrict__ pm,
-                                                const double2* __restrict__ hz, GravTree t,
-                                                const double4* __restrict__ tabG,
-                                                double* __restrict__ acc, double* __restrict__ gpot,
-                                                int nsink, const double* __restrict__ sinks,
-                                                DevError* err, unsigned long long* counts) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+struct GravWalk {
+  const int4* link;
+  const float4* wA;     // FP32 COM relative to the root centre, hi bracket
+  const float* wLo;     // lo bracket
+  const double4* gA;
+  const double4* gB;
+  const double2* gC;
+  int ctot;
+  double rootx, rooty, rootz;
+};
+
+template <bool MIXED>
+__global__ void __launch_bounds__(GW_THREADS)
+k_grav_warp(int nact, const int* __restrict__ act, const double4* __restrict__ pm,
+            const double2* __restrict__ hz, GravWalk t, const double4* __restrict__ tabG,
+            double* __restrict__ acc, double* __restrict__ gpot, int nsink,
+            const double* __restrict__ sinks, DevError* err, unsigned long long* counts) {
+  __shared__ int s_cell[GW_WARPS][GW_CAP];
+  __shared__ unsigned s_cmask[GW_WARPS][GW_CAP];
+  __shared__ int s_pst[GW_WARPS][GW_CAP];
+  __shared__ unsigned s_pmask[GW_WARPS][GW_CAP];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int i = blockIdx.x * GW_THREADS + threadIdx.x;
   const bool live = i < nact;
-  const int p = live ? (act ? act[i] : i) : 0;
+  if (__ballot_sync(FULLMASK, live) == 0) return;       // whole warp past the end
+  const int p = live ? (act ? act[i] : i) : (act ? act[nact - 1] : nact - 1);
+  const double4 P = pm[p];
+  const double2 HZ = hz[p];
+  // warp reference point (lane 0 is live whenever any lane is)
+  const double rx = __shfl_sync(FULLMASK, P.x, 0);
+  const double ry = __shfl_sync(FULLMASK, P.y, 0);
+  const double rz = __shfl_sync(FULLMASK, P.z, 0);
+  const float px32 = (float)(P.x - t.rootx), py32 = (float)(P.y - t.rooty),
+              pz32 = (float)(P.z - t.rootz);
+  const float ux = (float)(P.x - rx), uy = (float)(P.y - ry), uz = (float)(P.z - rz);
+  const double invhp = 1.0 / HZ.x;
+  const double zo_p = HZ.y;
+  const float invhp32 = (float)invhp, zo32 = (float)zo_p;
+  Kahan4 kc;
+  double cx = 0.0, cy = 0.0, cz = 0.0, cp = 0.0, qx = 0.0, qy = 0.0, qz = 0.0, qp = 0.0;
   unsigned long long ncell = 0, npair = 0;
-  if (live) {
-    const double4 P = pm[p];
-    const double2 HZ = hz[p];
-    const float invhp = (float)(1.0 / HZ.x);
-    const float zo_p = (float)HZ.y;
-    Kahan4 kc;
-    int c = 0, visits = 0;
-    const int cap = t.ctot + 2;
-    while (true) {
-      if (++visits > cap) {
-        set_error(err, SEREN_GPU_ERR_WALK, KID_GRAV_MIXED, p, c);
-        break;
-      }
-      const int4 lk = t.link[c];
-      if (lk.x == 1) {
-        const int q = lk.w;
-        if (q != p) {
-          const double4 Q = pm[q];
-          const double2 hq = hz[q];
-          pair_term32((float)(Q.x - P.x), (float)(Q.y - P.y), (float)(Q.z - P.z), invhp, zo_p,
-                      (float)Q.w, (float)hq.x, (float)hq.y, kc);
-          ++npair;
-        }
-        c = lk.y;
-      } else {
-        const double4 a = t.gA[c];
-        const double d0 = P.x - a.x, d1 = P.y - a.y, d2 = P.z - a.z;
-        const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
-        const double2 cc = t.gC[c];
-        if (drsqd > cc.y) {
-          const double4 q = t.gB[c];
-          cell_term32((float)d0, (float)d1, (float)d2, (float)a.w, (float)q.x, (float)q.y,
-                      (float)q.z, (float)q.w, (float)cc.x, kc);
+  int skip = live ? -1 : -2;
+  int c = 0, visits = 0, nc = 0, np = 0;
+
+  auto flush_cells = [&]() {
+    __syncwarp();
+    for (int e = 0; e < nc; ++e) {
+      const int cid = s_cell[w][e];
+      const bool mine = (s_cmask[w][e] >> lane) & 1u;
+      const double4 a = t.gA[cid];
+      const double4 q = t.gB[cid];
+      const double q5 = t.gC[cid].x;
+      if (MIXED) {
+        const float fx = (float)(rx - a.x), fy = (float)(ry - a.y), fz = (float)(rz - a.z);
+        if (mine) {
+          cell_term32(ux + fx, uy + fy, uz + fz, (float)a.w, (float)q.x, (float)q.y, (float)q.z,
+                      (float)q.w, (float)q5, kc);
           ++ncell;
-          c = lk.y;
-        } else if (lk.x > 0) {
-          for (int k = 0; k < lk.x; ++k) {
-            const int q = lk.w + k;
-            if (q == p) continue;
-            const double4 Q = pm[q];
-            const double2 hq = hz[q];
-            pair_term32((float)(Q.x - P.x), (float)(Q.y - P.y), (float)(Q.z - P.z), invhp, zo_p,
-                        (float)Q.w, (float)hq.x, (float)hq.y, kc);
+        }
+      } else if (mine) {
+        const double d0 = P.x - a.x, d1 = P.y - a.y, d2 = P.z - a.z;
+        cell_term64(d0, d1, d2, (d0 * d0 + d1 * d1) + d2 * d2, a, q, q5, cx, cy, cz, cp);
+        ++ncell;
+      }
+    }
+    nc = 0;
+    __syncwarp();
+  };
+  auto flush_pairs = [&]() {
+    __syncwarp();
+    for (int e = 0; e < np; ++e) {
+      const int code = s_pst[w][e];
+      const bool mine = (s_pmask[w][e] >> lane) & 1u;
+      const int q0 = code >> 3, cnt = (code & 7) + 1;
+      for (int k = 0; k < cnt; ++k) {
+        const int q = q0 + k;
+        const double4 Q = pm[q];
+        const double2 H = hz[q];
+        if (MIXED) {
+          const float gx = (float)(Q.x - rx), gy = (float)(Q.y - ry), gz = (float)(Q.z - rz);
+          if (mine && q != p) {
+            pair_term32(gx - ux, gy - uy, gz - uz, invhp32, zo32, (float)Q.w, (float)H.x,
+                        (float)H.y, kc);
             ++npair;
           }
-          c = lk.y;
-        } else if (lk.x == 0) {
-          c = lk.z;
-        } else {
-          c = lk.y;
+        } else if (mine && q != p) {
+          pair_term64(Q.x - P.x, Q.y - P.y, Q.z - P.z, invhp, zo_p, Q.w, H.x, H.y, tabG, qx, qy,
+                      qz, qp);
+          ++npair;
         }
       }
-      if (c > t.ctot) break;
+    }
+    np = 0;
+    __syncwarp();
+  };
+
+  while (true) {
+    if (++visits > t.ctot + 2) {
+      if (lane == 0) set_error(err, SEREN_GPU_ERR_WALK, MIXED ? KID_GRAV_MIXED : KID_GRAV, p, c);
+      break;
+    }
+    const int4 lk = t.link[c];
+    if (skip == c) skip = -1;
+    const bool actv = skip == -1;
+    if (lk.x == 1) {                                         // BHgrav_accel.F90:128-136
+      const unsigned m = __ballot_sync(FULLMASK, actv && lk.w != p);
+      if (m) {
+        if (lane == 0) { s_pst[w][np] = lk.w * 8; s_pmask[w][np] = m; }
+        ++np;
+      }
+      c = lk.y;
+    } else {
+      bool accept = false;
+      if (actv) {
+        const float4 wa = t.wA[c];
+        const float d0 = px32 - wa.x, d1 = py32 - wa.y, d2 = pz32 - wa.z;
+        const float d2s = (d0 * d0 + d1 * d1) + d2 * d2;
+        if (d2s > wa.w) {
+          accept = true;
+        } else if (d2s >= t.wLo[c]) {                        // exact test, :146-155
+          const double4 a = t.gA[c];
+          const double e0 = P.x - a.x, e1 = P.y - a.y, e2 = P.z - a.z;
+          accept = ((e0 * e0 + e1 * e1) + e2 * e2) > t.gC[c].y;
+        }
+      }
+      const unsigned macc = __ballot_sync(FULLMASK, accept);
+      const unsigned mopn = __ballot_sync(FULLMASK, actv && !accept);
+      if (macc) {
+        if (lane == 0) { s_cell[w][nc] = c; s_cmask[w][nc] = macc; }
+        ++nc;
+      }
+      if (lk.x > 0) {                                        // :242-253
+        if (mopn) {
+          if (lane == 0) { s_pst[w][np] = lk.w * 8 + (lk.x - 1); s_pmask[w][np] = mopn; }
+          ++np;
+        }
+        c = lk.y;
+      } else if (lk.x == 0 && mopn) {
+        if (accept) skip = lk.y;
+        c = lk.z;
+      } else {
+        c = lk.y;
+      }
+    }
+    if (nc == GW_CAP) flush_cells();
+    if (np == GW_CAP) flush_pairs();
+    if (c > t.ctot) break;
+  }
+  flush_cells();
+  flush_pairs();
+  if (live) {
+    double ax, ay, az, pot;
+    if (MIXED) {
+      ax = kc.get(0); ay = kc.get(1); az = kc.get(2); pot = kc.get(3);
+    } else {
+      ax = cx + qx; ay = cy + qy; az = cz + qz; pot = cp + qp;
     }
     double* a = acc + (size_t)p * 3;
-    a[0] = a[0] + kc.get(0);
-    a[1] = a[1] + kc.get(1);
-    a[2] = a[2] + kc.get(2);
-    double pot = kc.get(3);
-    if (nsink > 0) {
+    a[0] = a[0] + ax;
+    a[1] = a[1] + ay;
+    a[2] = a[2] + az;
+    if (nsink > 0) {                                         // sinks/direct_sink_gravity.F90
       double sx = 0.0, sy = 0.0, sz = 0.0, sp = 0.0;
       for (int s = 0; s < nsink; ++s) {
         const double* sr = sinks + s * 5;
@@ -452,12 +475,14 @@ GravTree grav_tree(const Ctx& c) { return GravTree{c.link, c.gA, c.gB, c.gC, c.i
 void launch_grav(Ctx& c, int nact, int nsink, const double* d_sinks) {
   if (nact <= 0) return;
   unsigned long long* counts = reinterpret_cast<unsigned long long*>(c.d_counts);
+  const GravWalk gw{c.link, c.wA, c.wLo, c.gA, c.gB, c.gC, c.info.ctot,
+                    c.info.root[0], c.info.root[1], c.info.root[2]};
   if (c.prm.precision == 0)
-    k_grav64<<<nb(nact, 128), 128, 0, c.st>>>(nact, c.act, c.pm, c.hz, grav_tree(c), c.tabG, c.acc,
-                                              c.gpot, nsink, d_sinks, c.d_err, counts);
+    k_grav_warp<false><<<nb(nact, GW_THREADS), GW_THREADS, 0, c.st>>>(
+        nact, c.act, c.pm, c.hz, gw, c.tabG, c.acc, c.gpot, nsink, d_sinks, c.d_err, counts);
   else
-    k_grav32<<<nb(nact, 128), 128, 0, c.st>>>(nact, c.act, c.pm, c.hz, grav_tree(c), c.tabG, c.acc,
-                                              c.gpot, nsink, d_sinks, c.d_err, counts);
+    k_grav_warp<true><<<nb(nact, GW_THREADS), GW_THREADS, 0, c.st>>>(
+        nact, c.act, c.pm, c.hz, gw, c.tabG, c.acc, c.gpot, nsink, d_sinks, c.d_err, counts);
   ++c.nlaunch;
 }
 

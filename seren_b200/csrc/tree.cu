@@ -389,12 +389,19 @@ __global__ void k_pack_parray(double* __restrict__ st, int n, const double4* __r
 // BHgrav_stock.F90:11-358 (QUADRUPOLE, GEOMETRIC_MAC) and BHhydro_stock.F90,
 // one level at a time from the deepest up; a leaf's particles are the
 // contiguous range [pstart, pstart+leaf) in tree order.
+// It also writes the FP32 walk copy of each cell: COM relative to the root
+// centre and a bracket [lo, hi] around dminsqd wide enough to hold every FP32
+// rounding of the walk's prefilter test (coordinates rounded to within delta,
+// the difference, the squares and the sum); tests inside the bracket are
+// redone in FP64 by the walk.
 __global__ void k_stock_level(int cfirst, int clast, const int4* __restrict__ link,
                               const double4* __restrict__ pm, const double2* __restrict__ hz,
                               double thetamaxsqd, double daux, double4* __restrict__ gA,
                               double4* __restrict__ gB, double2* __restrict__ gC,
                               double4* __restrict__ hA, double* __restrict__ hmaxa,
-                              double4* __restrict__ bbmina, double4* __restrict__ bbmaxa) {
+                              double4* __restrict__ bbmina, double4* __restrict__ bbmaxa,
+                              double rootx, double rooty, double rootz, double delta,
+                              float4* __restrict__ wA, float* __restrict__ wLo) {
   const int c = cfirst + blockIdx.x * blockDim.x + threadIdx.x;
   if (c > clast) return;
   const int4 lk = link[c];
@@ -484,6 +491,12 @@ __global__ void k_stock_level(int cfirst, int clast, const int4* __restrict__ li
   gA[c] = make_double4(rc[0], rc[1], rc[2], mc);
   gB[c] = make_double4(qc[0], qc[1], qc[2], qc[3]);
   gC[c] = make_double2(qc[4], dminsqd);
+  {
+    const double marg = 2.0 * (8.0 * sqrt(dminsqd) * delta + 1.0e-6 * dminsqd + 16.0 * delta * delta);
+    wA[c] = make_float4((float)(rc[0] - rootx), (float)(rc[1] - rooty), (float)(rc[2] - rootz),
+                        __double2float_ru(dminsqd + marg));
+    wLo[c] = __double2float_rd(dminsqd - marg);
+  }
   hmaxa[c] = hmax;
   bbmina[c] = make_double4(bbmin[0], bbmin[1], bbmin[2], 0.0);
   bbmaxa[c] = make_double4(bbmax[0], bbmax[1], bbmax[2], 0.0);
@@ -664,12 +677,18 @@ int build_tree(Ctx& c) {
 
 void launch_stock(Ctx& c) {
   const double daux = 10.0 * pow(1.7976931348623157e308, -0.2);
+  // bound on the rounding of a coordinate relative to the root centre when
+  // cast to FP32: every position lies within cellsize (the root half width)
+  // of the centre on each axis, so half an ulp is below 2^-23 * cellsize
+  const double delta = ldexp(1.0, -22) * (c.info.cellsize > 0.0 ? c.info.cellsize : 1.0);
   for (int l = c.info.ltot; l >= 0; --l) {
     const int f = c.info.first_cell[l], la = c.info.last_cell[l];
     const int cnt = la - f + 1;
     if (cnt <= 0) continue;
     k_stock_level<<<nb(cnt, 128), 128, 0, c.st>>>(f, la, c.link, c.pm, c.hz, c.prm.thetamaxsqd, daux,
-                                                 c.gA, c.gB, c.gC, c.hA, c.hmax, c.bbmin, c.bbmax); ++c.nlaunch;
+                                                 c.gA, c.gB, c.gC, c.hA, c.hmax, c.bbmin, c.bbmax,
+                                                 c.info.root[0], c.info.root[1], c.info.root[2],
+                                                 delta, c.wA, c.wLo); ++c.nlaunch;
   }
 }
 
