@@ -302,12 +302,34 @@ def cpu_eval(ic_tree, sample, first_call=False):
                 act=act)
 
 
-def accuracy_vs_direct(o, state_a, ids):
-    """rms and max |da|/|a| of accelerations against the FP64 direct sum
-    (sph/direct_sph_gravity.F90) for the particles ids (oracle order)."""
+def gravity_accuracy(ic, parray, nsub=256):
+    """Gravity-only accelerations of the GPU (mixed and FP64 walks) and of the
+    oracle's tree walk on one state (parray: positions, masses, h, zeta), each
+    against the FP64 direct sum (sph/direct_sph_gravity.F90) of the oracle for
+    nsub particles: rms and max |da|/|a|."""
+    from oracle.oracle import Oracle
+    from seren_b200.gpu import GpuHotPath
+    n = parray.shape[0]
+    ids = np.arange(0, n, max(1, n // nsub), dtype=np.int32)[:nsub]
+    o = Oracle(n, params_for(ic, 0))
+    po, permo = o.tree_update(parray)
     ad, _ = o.direct_gravity(ids)
-    err = np.linalg.norm(state_a - ad, axis=1) / np.linalg.norm(ad, axis=1)
-    return float(np.sqrt(np.mean(err ** 2))), float(err.max())
+    at, _ = o.grav_forces(np.zeros((n, 3)), acclist=ids)
+
+    def stats(a):
+        err = np.linalg.norm(a - ad, axis=1) / np.linalg.norm(ad, axis=1)
+        return float(np.sqrt(np.mean(err ** 2))), float(err.max())
+    out = {"direct_subset": int(ids.size)}
+    out["oracle_tree_rms_vs_direct"], out["oracle_tree_max_vs_direct"] = stats(at[ids])
+    for prec, key in ((1, "mixed"), (0, "fp64")):
+        g = GpuHotPath(n, params_for(ic, prec))
+        pg, permg = g.tree_update(parray)
+        assert np.array_equal(permg, permo)
+        ag, _ = g.grav_forces(np.zeros((n, 3)))
+        g.close()
+        out[f"{key}_rms_vs_direct"], out[f"{key}_max_vs_direct"] = stats(ag[ids])
+    o.close()
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -372,21 +394,8 @@ def main():
                            f"{n} particles, grad-h/neighbour lists/hydro/gravity for {sample} "
                            f"random active particles, scaled by N/{sample}; "
                            f"{r['sec']:.2f} s per evaluation"))
-        # accuracy of the GPU mixed result against the FP64 direct sum on a subset
-        # of the sampled particles (same state: the oracle rebuilt the same tree)
-        o = r["oracle"]
-        ids = r["act"][:: max(1, len(r["act"]) // 256)] if r["act"] is not None else \
-            np.arange(0, n, max(1, n // 256), dtype=np.int32)
-        ids = ids.astype(np.int32)
-        # the GPU state is in GPU tree order; the oracle reordered the same input
-        # with its own (identical) tree, so map GPU rows through the oracle perm
-        am = state_m["a"][r["perm"][ids]]
-        rms_d, max_d = accuracy_vs_direct(o, am, ids)
-        ao = r["a"][ids]
-        rms_t, max_t = accuracy_vs_direct(o, ao, ids)
-        acc.update(rms_vs_direct=rms_d, max_vs_direct=max_d, direct_subset=int(ids.size),
-                   oracle_tree_rms_vs_direct=rms_t)
-        o.close()
+        r["oracle"].close()
+        acc.update(gravity_accuracy(ic, st["parray"]))
     if rank != 0:
         return
     line = {

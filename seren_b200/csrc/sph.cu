@@ -92,140 +92,328 @@ __device__ __forceinline__ bool walk_gather_scatter(const HydroTree& t, double r
   return true;
 }
 
-// sph/all_sph_gradh.F90:11-492 (GRAD_H_SPH, BH_TREE, GRAVITY)
-__global__ void __launch_bounds__(128) k_gradh(int nact, const int* __restrict__ act,
-                                               const double4* __restrict__ pm, double2* __restrict__ hz,
-                                               const double4* __restrict__ vel, double* __restrict__ rho,
-                                               double* __restrict__ omega, double* __restrict__ divv,
-                                               double* __restrict__ drhodt, HydroTree t,
-                                               const double4* __restrict__ tabA, double h_fac,
-                                               int pp_gather, double rextent, DevError* err) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nact) return;
-  const int p = act ? act[i] : i;
+// ---------------------------------------------------------------------------
+// grad-h solve, sph/all_sph_gradh.F90:11-492 (GRAD_H_SPH, BH_TREE, GRAVITY).
+//
+// Per-particle state of the iteration (:132-145) and its update after a
+// density pass (:238-285).  The omega sum of the iteration passes (:230, :238)
+// is never used after the loop (the final pass recomputes it), so the passes
+// accumulate the density only.
+struct GhState {
+  double hp, h_old, h_high, h_upper, h_lower, rho;
+  int iteration, pp_pot, ngrow;
+};
+
+__device__ __forceinline__ void gh_init(GhState& s, double h, double rextent) {
+  s.hp = h; s.h_old = h; s.h_high = 0.0; s.h_upper = rextent; s.h_lower = 0.0; s.rho = 0.0;
+  s.iteration = 0; s.pp_pot = 0; s.ngrow = 0;
+}
+
+// returns true when the iteration has ended (converged or given up)
+__device__ __forceinline__ bool gh_after_pass(GhState& s, double mp, double h_fac, double rextent,
+                                              double rt) {
+  s.rho = rt;
+  const double hcand = h_fac * pow(mp / rt, ONETHIRD);
+  if (fabs(s.hp - hcand) / s.hp < H_CON && s.iteration >= 1) return true;   // :246
+  double h_new;
+  if (s.iteration < GRADH_ITERATION_MAX) {
+    h_new = hcand;
+  } else if (s.iteration == GRADH_ITERATION_MAX) {
+    s.h_upper = rextent;
+    s.h_lower = 0.0;
+    h_new = 0.5 * (s.h_lower + s.h_upper);
+  } else if (s.iteration < 2 * GRADH_ITERATION_MAX) {
+    double fb;
+    if (rt > SMALL_NUMBER) fb = pow(s.hp, NDIMPR) - (pow(h_fac, NDIMPR) * mp) / rt;
+    else fb = 1.0;
+    if (fb > 0.0) s.h_upper = s.hp;
+    else s.h_lower = s.hp;
+    h_new = 0.5 * (s.h_lower + s.h_upper);
+  } else {
+    s.hp = s.h_old;
+    return true;
+  }
+  s.hp = h_new;
+  s.iteration = s.iteration + 1;
+  return false;
+}
+
+// one density term of an iteration pass (:218-230)
+__device__ __forceinline__ void gh_density_term(const double4& Q, double rx, double ry, double rz,
+                                                double hs, double ih, double hf,
+                                                const double4* __restrict__ tabA, double& rt) {
+  const double d0 = Q.x - rx, d1 = Q.y - ry, d2 = Q.z - rz;
+  const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
+  if (drsqd >= hs) return;
+  const double drmag = sqrt(drsqd) + SMALL_NUMBER;
+  const int kern = (int)((HALFKERNTOT * drmag) * ih);
+  if (kern >= KERNTOT) return;
+  rt = rt + (Q.w * hf) * tabA[kern].x;
+}
+
+// the final-pass sums (:360-425)
+struct GhFinal {
+  double rt, om, dv, zt;
+};
+
+__device__ __forceinline__ void gh_final_term(const double4& Q, const double4& V, double rx,
+                                              double ry, double rz, const double4& vp, double hs,
+                                              double ih, double hf,
+                                              const double4* __restrict__ tabA, GhFinal& f) {
+  const double d0 = Q.x - rx, d1 = Q.y - ry, d2 = Q.z - rz;
+  double drmag = (d0 * d0 + d1 * d1) + d2 * d2;
+  if (drmag > hs) return;
+  drmag = sqrt(drmag) + SMALL_NUMBER;
+  const int kern = (int)((HALFKERNTOT * drmag) * ih);
+  if (kern > KERNTOT) return;
+  const double dv0 = V.x - vp.x, dv1 = V.y - vp.y, dv2 = V.z - vp.z;
+  const double dvdr = (dv0 * d0 + dv1 * d1) + dv2 * d2;
+  const double4 w = tabA[kern];
+  f.rt = f.rt + (Q.w * hf) * w.x;
+  f.om = f.om + ((Q.w * hf) * ih) * w.y;
+  f.dv = f.dv - ((((Q.w * dvdr) * w.z) * hf) * ih) / drmag;
+  f.zt = f.zt + ((Q.w * ih) * ih) * w.w;
+}
+
+__device__ __forceinline__ void gh_store(int p, double mp, double hp, const GhFinal& f,
+                                         double2* __restrict__ hz, double* __restrict__ rho,
+                                         double* __restrict__ omega, double* __restrict__ divv,
+                                         double* __restrict__ drhodt, DevError* err) {
+  const double omega_f = 1.0 + ((hp * f.om) / (NDIMPR * f.rt));        // :428
+  const double div_v_p = f.dv / f.rt;
+  rho[p] = f.rt;                                                       // :436-442
+  omega[p] = omega_f;
+  divv[p] = div_v_p;
+  drhodt[p] = -((f.rt * div_v_p) / omega_f);
+  hz[p] = make_double2(hp, -((hp * f.zt) / ((NDIMPR * f.rt) * omega_f)));
+  if (hp < 0.0) set_error(err, SEREN_GPU_ERR_NEGATIVE_H, KID_GRADH, p, 0);
+}
+
+__device__ __forceinline__ void gh_final_init(GhFinal& f, double mp, double ih, double hf,
+                                              const double4& t0) {
+  f.rt = (mp * t0.x) * hf;                                             // :323-346
+  f.om = ((mp * hf) * ih) * t0.y;
+  f.dv = 0.0;
+  f.zt = ((mp * ih) * ih) * t0.w;
+}
+
+// The whole routine for one particle with its own walks: used when a warp's
+// shared candidate list overflows.
+__device__ void gradh_one(int p, const double4* __restrict__ pm, double2* __restrict__ hz,
+                          const double4* __restrict__ vel, double* __restrict__ rho,
+                          double* __restrict__ omega, double* __restrict__ divv,
+                          double* __restrict__ drhodt, const HydroTree& t,
+                          const double4* __restrict__ tabA, double h_fac, int pp_gather,
+                          double rextent, DevError* err) {
   const double4 P = pm[p];
   const double rx = P.x, ry = P.y, rz = P.z, mp = P.w;
-  double hp = hz[p].x;
   const double4 vp = vel[p];
   const double4 t0 = tabA[0];
-  double invhp, hfactor_p, hrangesqd;
-  int iteration = 0;
-  const double h_old = hp;
-  double h_new = hp;
-  double h_high = 0.0, h_upper = rextent, h_lower = 0.0;
-  int pp_pot = 0, ngrow = 0;
-  double rhotemp = 0.0, omega_p = 0.0;
+  GhState s;
+  gh_init(s, hz[p].x, rextent);
   while (true) {
     while (true) {                                                     // :154-191
-      if (hp > h_high) {
-        h_high = hp * HMULT;
+      if (s.hp > s.h_high) {
+        s.h_high = s.hp * HMULT;
         int cnt = 0;
-        if (!walk_gather(t, rx, ry, rz, KERNRANGE * h_high, err, p, [&](int) { ++cnt; })) return;
-        pp_pot = cnt;
+        if (!walk_gather(t, rx, ry, rz, KERNRANGE * s.h_high, err, p, [&](int) { ++cnt; })) return;
+        s.pp_pot = cnt;
       }
-      if (pp_pot < pp_gather) {
-        h_high = 0.0;
-        pp_pot = 0;
-        hp = hp * HMULT;
-        if (++ngrow > HGROW_CAP) {
+      if (s.pp_pot < pp_gather) {
+        s.h_high = 0.0;
+        s.pp_pot = 0;
+        s.hp = s.hp * HMULT;
+        if (++s.ngrow > HGROW_CAP) {
           set_error(err, SEREN_GPU_ERR_WALK, KID_GRADH, p, -1);
           return;
         }
       }
-      if (pp_pot > 0) break;
+      if (s.pp_pot > 0) break;
     }
-    h_new = hp;                                                        // :199-210
-    invhp = 1.0 / hp;
-    hfactor_p = pow(invhp, NDIMPR);
-    hrangesqd = (KERNRANGESQD * hp) * hp;
-    rhotemp = (mp * t0.x) * hfactor_p;
-    omega_p = ((mp * hfactor_p) * invhp) * t0.y;
-    const double hs = hrangesqd, ih = invhp, hf = hfactor_p;
-    double rt = rhotemp, om = omega_p;
-    walk_gather(t, rx, ry, rz, KERNRANGE * h_high, err, p, [&](int q) {  // :214-235
-      if (q == p) return;
-      const double4 Q = pm[q];
-      const double d0 = Q.x - rx, d1 = Q.y - ry, d2 = Q.z - rz;
-      const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
-      if (drsqd >= hs) return;
-      const double drmag = sqrt(drsqd) + SMALL_NUMBER;
-      const int kern = (int)((HALFKERNTOT * drmag) * ih);
-      if (kern >= KERNTOT) return;
-      const double4 w = tabA[kern];
-      rt = rt + (Q.w * hf) * w.x;
-      om = om + ((Q.w * hf) * ih) * w.y;
+    const double ih = 1.0 / s.hp;                                      // :199-210
+    const double hf = pow(ih, NDIMPR);
+    const double hs = (KERNRANGESQD * s.hp) * s.hp;
+    double rt = (mp * t0.x) * hf;
+    walk_gather(t, rx, ry, rz, KERNRANGE * s.h_high, err, p, [&](int q) {
+      if (q != p) gh_density_term(pm[q], rx, ry, rz, hs, ih, hf, tabA, rt);
     });
-    rhotemp = rt;
-    omega_p = 1.0 + ((hp * om) / (NDIMPR * rhotemp));                  // :238
-    const double hcand = h_fac * pow(mp / rhotemp, ONETHIRD);
-    if (fabs(hp - hcand) / hp < H_CON && iteration >= 1) break;        // :246
-    if (iteration < GRADH_ITERATION_MAX) {
-      h_new = hcand;
-    } else if (iteration == GRADH_ITERATION_MAX) {
-      h_upper = rextent;
-      h_lower = 0.0;
-      h_new = 0.5 * (h_lower + h_upper);
-    } else if (iteration < 2 * GRADH_ITERATION_MAX) {
-      double fb;
-      if (rhotemp > SMALL_NUMBER) fb = pow(hp, NDIMPR) - (pow(h_fac, NDIMPR) * mp) / rhotemp;
-      else fb = 1.0;
-      if (fb > 0.0) h_upper = hp;
-      else h_lower = hp;
-      h_new = 0.5 * (h_lower + h_upper);
-    } else {
-      h_new = h_old;
-      hp = h_new;
-      break;
-    }
-    hp = h_new;
-    iteration = iteration + 1;
+    if (gh_after_pass(s, mp, h_fac, rextent, rt)) break;
   }
-  hp = h_fac * pow(mp / rhotemp, ONETHIRD);                           // :317
-  invhp = 1.0 / hp;
-  hfactor_p = pow(invhp, NDIMPR);
-  hrangesqd = (KERNRANGESQD * hp) * hp;
-  double rt = (mp * t0.x) * hfactor_p;
-  double om = ((mp * hfactor_p) * invhp) * t0.y;
-  double dv_sum = 0.0;
-  double zt = ((mp * invhp) * invhp) * t0.w;
-  const double hs = hrangesqd, ih = invhp, hf = hfactor_p;
-  walk_gather(t, rx, ry, rz, KERNRANGE * h_high, err, p, [&](int q) {  // :360-425
-    if (q == p) return;
-    const double4 Q = pm[q];
-    const double d0 = Q.x - rx, d1 = Q.y - ry, d2 = Q.z - rz;
-    double drmag = (d0 * d0 + d1 * d1) + d2 * d2;
-    if (drmag > hs) return;
-    drmag = sqrt(drmag) + SMALL_NUMBER;
-    const int kern = (int)((HALFKERNTOT * drmag) * ih);
-    if (kern > KERNTOT) return;
-    const double4 V = vel[q];
-    const double dv0 = V.x - vp.x, dv1 = V.y - vp.y, dv2 = V.z - vp.z;
-    const double dvdr = (dv0 * d0 + dv1 * d1) + dv2 * d2;
-    const double4 w = tabA[kern];
-    rt = rt + (Q.w * hf) * w.x;
-    om = om + ((Q.w * hf) * ih) * w.y;
-    dv_sum = dv_sum - ((((Q.w * dvdr) * w.z) * hf) * ih) / drmag;
-    zt = zt + ((Q.w * ih) * ih) * w.w;
+  const double hp = h_fac * pow(mp / s.rho, ONETHIRD);                 // :317
+  const double ih = 1.0 / hp;
+  const double hf = pow(ih, NDIMPR);
+  const double hs = (KERNRANGESQD * hp) * hp;
+  GhFinal f;
+  gh_final_init(f, mp, ih, hf, t0);
+  walk_gather(t, rx, ry, rz, KERNRANGE * s.h_high, err, p, [&](int q) {
+    if (q != p) gh_final_term(pm[q], vel[q], rx, ry, rz, vp, hs, ih, hf, tabA, f);
   });
-  const double omega_f = 1.0 + ((hp * om) / (NDIMPR * rt));            // :428
-  const double div_v_p = dv_sum / rt;
-  rho[p] = rt;                                                         // :436-442
-  omega[p] = omega_f;
-  divv[p] = div_v_p;
-  drhodt[p] = -((rt * div_v_p) / omega_f);
-  hz[p] = make_double2(hp, -((hp * zt) / ((NDIMPR * rt) * omega_f)));
-  if (hp < 0.0) set_error(err, SEREN_GPU_ERR_NEGATIVE_H, KID_GRADH, p, 0);
+  gh_store(p, mp, hp, f, hz, rho, omega, divv, drhodt, err);
 }
 
-// sph/get_neib.F90:10-140
-__global__ void __launch_bounds__(128) k_neib(int nact, const int* __restrict__ act,
-                                              const double4* __restrict__ pm,
-                                              const double2* __restrict__ hz, HydroTree t, int L,
-                                              int* __restrict__ pptot, int* __restrict__ pplist,
-                                              DevError* err) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nact) return;
-  const int p = act ? act[i] : i;
+// ---------------------------------------------------------------------------
+// Warp-cooperative candidate walks.  The warp walks the hydro tree once for
+// its 32 particles, each lane with its own search test; the walk position is
+// warp-uniform and a lane that fails a branch cell's test skips that subtree
+// (its skip marker is the cell's nextcell), so a lane's bits select exactly the
+// leaves its own walk would open, in the same depth-first order.  Opened
+// leaves are stored once per warp as (pstart, count) with the lane mask.
+constexpr int SW_THREADS = 128;
+constexpr int SW_WARPS = SW_THREADS / 32;
+constexpr int SW_CAP = 256;
+constexpr unsigned FULL = 0xffffffffu;
+
+// test(h, c) -> bool is the lane's cell test; returns the entry count, or -1
+// when the list overflowed.  cnt accumulates the lane's candidate count.
+template <class Test>
+__device__ __forceinline__ int warp_walk(const HydroTree& t, bool part, int lane,
+                                         int* __restrict__ s_leaf, unsigned* __restrict__ s_mask,
+                                         int& cnt, DevError* err, int kid, int who, Test&& test) {
+  __syncwarp();
+  int c = 0, n = 0, visits = 0;
+  int skip = part ? -1 : -2;
+  cnt = 0;
+  while (true) {
+    if (++visits > t.ctot + 2) {
+      if (lane == 0) set_error(err, SEREN_GPU_ERR_WALK, kid, who, c);
+      return -1;
+    }
+    const int4 lk = t.link[c];
+    if (skip == c) skip = -1;
+    bool pass = false;
+    if (skip == -1) pass = test(t.hA[c], c);
+    const unsigned m = __ballot_sync(FULL, pass);
+    if (lk.x > 0) {
+      if (m) {
+        if (n == SW_CAP) return -1;
+        if (lane == 0) { s_leaf[n] = lk.w * 8 + (lk.x - 1); s_mask[n] = m; }
+        ++n;
+        if (pass) cnt += lk.x;
+      }
+      c = lk.y;
+    } else if (lk.x == 0 && m) {
+      if (skip == -1 && !pass) skip = lk.y;
+      c = lk.z;
+    } else {
+      c = lk.y;
+    }
+    if (c > t.ctot) break;
+  }
+  __syncwarp();
+  return n;
+}
+
+enum : int { GH_WALK = 0, GH_PASS = 1, GH_DONE = 2, GH_OFF = 3 };
+
+__global__ void __launch_bounds__(SW_THREADS) k_gradh_warp(
+    int nact, const int* __restrict__ act, const double4* __restrict__ pm, double2* __restrict__ hz,
+    const double4* __restrict__ vel, double* __restrict__ rho, double* __restrict__ omega,
+    double* __restrict__ divv, double* __restrict__ drhodt, HydroTree t,
+    const double4* __restrict__ tabA, double h_fac, int pp_gather, double rextent, DevError* err) {
+  __shared__ int s_leaf[SW_WARPS][SW_CAP];
+  __shared__ unsigned s_mask[SW_WARPS][SW_CAP];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int i = blockIdx.x * SW_THREADS + threadIdx.x;
+  const bool live = i < nact;
+  if (__ballot_sync(FULL, live) == 0) return;
+  const int p = live ? (act ? act[i] : i) : (act ? act[nact - 1] : nact - 1);
+  const double4 P = pm[p];
+  const double rx = P.x, ry = P.y, rz = P.z, mp = P.w;
+  const double4 t0 = tabA[0];
+  GhState s;
+  gh_init(s, hz[p].x, rextent);
+  int st = live ? GH_WALK : GH_OFF;
+  double R = -1.0;                 // search radius of the lane's current list
+  int nent = 0;
+  bool overflow = false;
+  auto gather_test = [&](const double4& h, int) {
+    const double d0 = h.x - rx, d1 = h.y - ry, d2 = h.z - rz;
+    const double tt = R + h.w;
+    return ((d0 * d0 + d1 * d1) + d2 * d2) <= tt * tt;
+  };
+  while (!overflow) {
+    while (__any_sync(FULL, st == GH_WALK)) {                          // :154-191
+      bool want = false;
+      if (st == GH_WALK && s.hp > s.h_high) {
+        s.h_high = s.hp * HMULT;
+        R = KERNRANGE * s.h_high;
+        want = true;
+      }
+      if (__any_sync(FULL, want)) {
+        int cnt = 0;
+        nent = warp_walk(t, R >= 0.0, lane, s_leaf[w], s_mask[w], cnt, err, KID_GRADH, p,
+                         gather_test);
+        if (nent < 0) { overflow = true; break; }
+        if (want) s.pp_pot = cnt;
+      }
+      if (st == GH_WALK) {
+        if (s.pp_pot < pp_gather) {
+          s.h_high = 0.0;
+          s.pp_pot = 0;
+          s.hp = s.hp * HMULT;
+          if (++s.ngrow > HGROW_CAP) {
+            set_error(err, SEREN_GPU_ERR_WALK, KID_GRADH, p, -1);
+            st = GH_OFF;
+            R = -1.0;
+          }
+        } else {
+          st = GH_PASS;
+        }
+      }
+    }
+    if (overflow || !__any_sync(FULL, st == GH_PASS)) break;
+    // density pass over the lane's candidates (:199-235)
+    const bool on = st == GH_PASS;
+    const double ih = on ? 1.0 / s.hp : 0.0;
+    const double hf = on ? pow(ih, NDIMPR) : 0.0;
+    const double hs = (KERNRANGESQD * s.hp) * s.hp;
+    double rt = (mp * t0.x) * hf;
+    for (int e = 0; e < nent; ++e) {
+      const int code = s_leaf[w][e];
+      const bool mine = on && ((s_mask[w][e] >> lane) & 1u);
+      const int q0 = code >> 3, n = (code & 7) + 1;
+      for (int k = 0; k < n; ++k) {
+        const int q = q0 + k;
+        const double4 Q = pm[q];
+        if (mine && q != p) gh_density_term(Q, rx, ry, rz, hs, ih, hf, tabA, rt);
+      }
+    }
+    if (on) st = gh_after_pass(s, mp, h_fac, rextent, rt) ? GH_DONE : GH_WALK;
+  }
+  if (overflow) {
+    if (live) gradh_one(p, pm, hz, vel, rho, omega, divv, drhodt, t, tabA, h_fac, pp_gather,
+                        rextent, err);
+    return;
+  }
+  // final pass over the same candidate list (:317-425)
+  const bool on = st == GH_DONE;
+  const double hp = on ? h_fac * pow(mp / s.rho, ONETHIRD) : 1.0;
+  const double ih = 1.0 / hp;
+  const double hf = on ? pow(ih, NDIMPR) : 0.0;
+  const double hs = (KERNRANGESQD * hp) * hp;
+  const double4 vp = vel[p];
+  GhFinal f;
+  gh_final_init(f, mp, ih, hf, t0);
+  for (int e = 0; e < nent; ++e) {
+    const int code = s_leaf[w][e];
+    const bool mine = on && ((s_mask[w][e] >> lane) & 1u);
+    const int q0 = code >> 3, n = (code & 7) + 1;
+    for (int k = 0; k < n; ++k) {
+      const int q = q0 + k;
+      const double4 Q = pm[q];
+      const double4 V = vel[q];
+      if (mine && q != p) gh_final_term(Q, V, rx, ry, rz, vp, hs, ih, hf, tabA, f);
+    }
+  }
+  if (on) gh_store(p, mp, hp, f, hz, rho, omega, divv, drhodt, err);
+}
+
+// ---------------------------------------------------------------------------
+// get_neib (sph/get_neib.F90:10-140): gather-or-scatter candidates
+// (BHhydro_walk.F90:37-43), kept if r^2 <= 4h_p^2 or r^2 <= 4h_pp^2, in order.
+__device__ void neib_one(int p, const double4* __restrict__ pm, const double2* __restrict__ hz,
+                         const HydroTree& t, int L, int* __restrict__ pptot,
+                         int* __restrict__ pplist, DevError* err) {
   const double4 P = pm[p];
   const double hp = hz[p].x;
   const double hsp = (KERNRANGESQD * hp) * hp;
@@ -244,6 +432,58 @@ __global__ void __launch_bounds__(128) k_neib(int nact, const int* __restrict__ 
     }
   });
   pptot[p] = cnt;
+}
+
+__global__ void __launch_bounds__(SW_THREADS) k_neib_warp(
+    int nact, const int* __restrict__ act, const double4* __restrict__ pm,
+    const double2* __restrict__ hz, HydroTree t, int L, int* __restrict__ pptot,
+    int* __restrict__ pplist, DevError* err) {
+  __shared__ int s_leaf[SW_WARPS][SW_CAP];
+  __shared__ unsigned s_mask[SW_WARPS][SW_CAP];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int i = blockIdx.x * SW_THREADS + threadIdx.x;
+  const bool live = i < nact;
+  if (__ballot_sync(FULL, live) == 0) return;
+  const int p = live ? (act ? act[i] : i) : (act ? act[nact - 1] : nact - 1);
+  const double4 P = pm[p];
+  const double hp = hz[p].x;
+  const double R = KERNRANGE * hp;
+  const double hsp = (KERNRANGESQD * hp) * hp;
+  int cnt = 0;
+  const int nent = warp_walk(t, live, lane, s_leaf[w], s_mask[w], cnt, err, KID_NEIB, p,
+                             [&](const double4& h, int c) {
+                               const double d0 = h.x - P.x, d1 = h.y - P.y, d2 = h.z - P.z;
+                               const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
+                               const double t1 = R + h.w;
+                               const double t2 = t.hrm[c] + h.w;
+                               return drsqd <= t1 * t1 || drsqd <= t2 * t2;
+                             });
+  if (nent < 0) {
+    if (live) neib_one(p, pm, hz, t, L, pptot, pplist, err);
+    return;
+  }
+  int* row = pplist + (size_t)p * L;
+  cnt = 0;
+  for (int e = 0; e < nent; ++e) {
+    const int code = s_leaf[w][e];
+    const bool mine = live && ((s_mask[w][e] >> lane) & 1u);
+    const int q0 = code >> 3, n = (code & 7) + 1;
+    for (int k = 0; k < n; ++k) {
+      const int q = q0 + k;
+      const double4 Q = pm[q];
+      const double hq = hz[q].x;
+      if (mine && q != p) {
+        const double hsq = (KERNRANGESQD * hq) * hq;
+        const double d0 = Q.x - P.x, d1 = Q.y - P.y, d2 = Q.z - P.z;
+        const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
+        if (drsqd <= hsp || drsqd <= hsq) {
+          if (cnt < L) row[cnt] = q;
+          ++cnt;
+        }
+      }
+    }
+  }
+  if (live) pptot[p] = cnt;
 }
 
 // sph/hydro_gradh.F90:9-339 (NEIGHBOUR_LISTS, ARTIFICIAL_VISCOSITY=MON97)
@@ -356,15 +596,15 @@ HydroTree hydro_tree(const Ctx& c) { return HydroTree{c.link, c.hA, c.hrm, c.inf
 
 void launch_gradh(Ctx& c, int nact) {
   if (nact <= 0) return;
-  k_gradh<<<nb(nact, 128), 128, 0, c.st>>>(nact, c.act, c.pm, c.hz, c.vel, c.rho, c.omega, c.div_v,
-                                           c.drhodt, hydro_tree(c), c.tabA, c.prm.h_fac,
-                                           c.prm.pp_gather, c.info.rextent, c.d_err); ++c.nlaunch;
+  k_gradh_warp<<<nb(nact, SW_THREADS), SW_THREADS, 0, c.st>>>(
+      nact, c.act, c.pm, c.hz, c.vel, c.rho, c.omega, c.div_v, c.drhodt, hydro_tree(c), c.tabA,
+      c.prm.h_fac, c.prm.pp_gather, c.info.rextent, c.d_err); ++c.nlaunch;
 }
 
 void launch_neib(Ctx& c, int nact) {
   if (nact <= 0) return;
-  k_neib<<<nb(nact, 128), 128, 0, c.st>>>(nact, c.act, c.pm, c.hz, hydro_tree(c), c.prm.pp_limit,
-                                          c.pptot, c.pplist, c.d_err); ++c.nlaunch;
+  k_neib_warp<<<nb(nact, SW_THREADS), SW_THREADS, 0, c.st>>>(
+      nact, c.act, c.pm, c.hz, hydro_tree(c), c.prm.pp_limit, c.pptot, c.pplist, c.d_err); ++c.nlaunch;
 }
 
 void launch_hydro(Ctx& c, int nact) {
