@@ -224,18 +224,28 @@ def run_e2e(ic, precision, steps, warmup, ws):
     P = lambda x: x.ctypes.data_as(dp)  # noqa: E731
     ctx = g._ctx
 
+    host_s = np.zeros(6)
+
     def step(first):
         nonlocal v, v2, sound, sound2
+        t0 = time.perf_counter()
         g._call("tree_update", ctx, n, P(parray), 1, 1, perm.ctypes.data_as(ip))
+        t1 = time.perf_counter()
         np.take(v, perm, axis=0, out=v2); v, v2 = v2, v
         np.take(sound, perm, out=sound2); sound, sound2 = sound2, sound
+        t2 = time.perf_counter()
         g._call("sph_update", ctx, n, None, 0, P(parray), P(v), P(rho), P(omega), P(div_v),
                 P(drhodt), None, None, int(first))
+        t3 = time.perf_counter()
         np.multiply(sound, sound, out=press)
         np.multiply(press, rho, out=press)
         g._call("hydro_forces", ctx, None, 0, P(press), P(sound), P(a))
+        t4 = time.perf_counter()
         g._call("grav_forces", ctx, None, 0, P(a), P(gpot), 0, None)
+        t5 = time.perf_counter()
         parray[:, 0:3] += v * DT
+        t6 = time.perf_counter()
+        host_s[:] += np.diff([t0, t1, t2, t3, t4, t5, t6])
 
     stream = torch.cuda.ExternalStream(g.stream())
     for w in range(max(warmup, 1)):
@@ -244,12 +254,17 @@ def run_e2e(ic, precision, steps, warmup, ws):
     torch.cuda.synchronize()
     barrier(ws)
     start.record(stream)
+    host_s[:] = 0.0
     for _ in range(steps):
         step(False)
     end.record(stream)
     torch.cuda.synchronize()
     barrier(ws)
     total_ms = start.elapsed_time(end)
+    log("[bench] e2e host ms/step: " + ", ".join(
+        f"{k} {1e3 * x / steps:.1f}" for k, x in zip(
+            ("tree_update", "host reorder", "sph_update", "thermal+hydro", "grav", "host drift"),
+            host_s)))
     h2d = n * (48 + 24 + 8 + 8 + 24)            # parray, v, press, sound, a (grav adds to it)
     d2h = n * (48 + 4 + 16 + 32 + 24 + 24 + 8)  # parray+perm, h/zeta, rho..drhodt, a (hydro), a+gpot (grav)
     g.close()

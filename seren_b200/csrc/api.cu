@@ -190,6 +190,7 @@ int check_tree(Ctx& c, int32_t ptot) {
 void free_all(Ctx& c) {
   void* ps[] = {c.pm, c.hz, c.vel, c.csq, c.orig, c.pm_alt, c.hz_alt, c.vel_alt, c.csq_alt,
                 c.orig_alt, c.rho, c.omega, c.div_v, c.drhodt, c.press, c.sound, c.acc, c.gpot,
+                c.pf, c.hf4,
                 c.pptot, c.pplist, c.stage, c.istage, c.keys, c.keys_alt, c.idx, c.idx_alt,
                 c.rs_hist, c.bbox_part, c.branch, c.branch_next, c.nchild, c.choff, c.cstart,
                 c.bflag, c.bscan, c.leaf, c.nextcell, c.ifopen, c.pstart, c.pcount, c.parent,
@@ -215,7 +216,8 @@ int alloc_all(Ctx& c) {
   bad |= alloc(c.pm_alt, P) | alloc(c.hz_alt, P) | alloc(c.vel_alt, P) | alloc(c.csq_alt, P) |
          alloc(c.orig_alt, P);
   bad |= alloc(c.rho, P) | alloc(c.omega, P) | alloc(c.div_v, P) | alloc(c.drhodt, P) |
-         alloc(c.press, P) | alloc(c.sound, P) | alloc(c.acc, 3 * P) | alloc(c.gpot, P);
+         alloc(c.press, P) | alloc(c.sound, P) | alloc(c.acc, 3 * P) | alloc(c.gpot, P) |
+         alloc(c.pf, P) | alloc(c.hf4, P);
   // stage: host-layout arrays and up to 1024 sinks; istage: active list + id arrays
   bad |= alloc(c.pptot, P) | alloc(c.pplist, P * L) | alloc(c.stage, std::max<size_t>(6 * P, 16384)) |
          alloc(c.istage, P * L + P);

@@ -45,6 +45,8 @@ struct Ctx {
   double* sound = nullptr;
   double* acc = nullptr;     // [ptot][3]
   double* gpot = nullptr;
+  double* pf = nullptr;      // hydro: press/rho/rho/omega per particle
+  double* hf4 = nullptr;     // hydro: (1/h)**(NDIM+1) per particle
   int* pptot = nullptr;
   int* pplist = nullptr;     // [ptot][pp_limit]
   int* act = nullptr;        // active list (0-based), when given

@@ -119,83 +119,6 @@ struct Kahan4 {
   __device__ __forceinline__ double get(int k) const { return (double)s[k] - (double)c[k]; }
 };
 
-// M4 softened-gravity kernel functions (setup/kernel.F90:80-81, :99-102) at
-// the centre s = (2i+1)/KERNTOT of table bin i, in FP32.  Returns w5, w4, w6.
-__device__ __forceinline__ void m4_grav32(int i, float& w5, float& w4, float& w6) {
-  const float s = (float)(2 * i + 1) * 1.0e-4f;
-  const float s2 = s * s;
-  const float invpi = 0.318309886f;
-  if (i < KERNTOT / 2) {
-    // w5 = (4/3)s - 1.2 s^3 + 0.5 s^4 ; w4 = (-3 s + 2.25 s^2)/pi
-    // w6 = 1.4 - (2/3) s^2 + 0.3 s^4 - 0.1 s^5
-    w5 = s * fmaf(s2, fmaf(0.5f, s, -1.2f), 1.33333333f);
-    w4 = invpi * s * fmaf(2.25f, s, -3.0f);
-    w6 = fmaf(s2, fmaf(s2, fmaf(-0.1f, s, 0.3f), -0.66666667f), 1.4f);
-  } else {
-    // w5 = (8/3)s - 3 s^2 + 1.2 s^3 - (1/6) s^4 - 1/(15 s^2) ; w4 = -0.75 (2-s)^2 / pi
-    // w6 = -1/(15 s) + 1.6 - (4/3) s^2 + s^3 - 0.3 s^4 + (1/30) s^5
-    const float inv15s = __fdividef(1.0f, 15.0f * s);
-    w5 = s * fmaf(s, fmaf(s, fmaf(-0.16666667f, s, 1.2f), -3.0f), 2.66666667f) - inv15s / s;
-    const float sa = 2.0f - s;
-    w4 = -0.75f * invpi * sa * sa;
-    w6 = fmaf(s2, fmaf(s, fmaf(s, fmaf(0.033333333f, s, -0.3f), 1.0f), -1.33333333f), 1.6f) - inv15s;
-  }
-}
-
-__device__ __forceinline__ void cell_term32(float d0, float d1, float d2, float m, float q1, float q2,
-                                            float q3, float q4, float q5, Kahan4& acc) {
-  const float drsqd = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
-  const float invdrmag = rsqrtf(drsqd);
-  const float invdrsqd = invdrmag * invdrmag;
-  const float invdr3 = invdrsqd * invdrmag;
-  const float invdr5 = invdr3 * invdrsqd;
-  const float q6 = -(q1 + q3);
-  const float qx = fmaf(q4, d2, fmaf(q2, d1, q1 * d0));
-  const float qy = fmaf(q5, d2, fmaf(q3, d1, q2 * d0));
-  const float qz = fmaf(q6, d2, fmaf(q5, d1, q4 * d0));
-  const float qscalar = fmaf(qz, d2, fmaf(qy, d1, qx * d0));
-  const float g = fmaf(2.5f * qscalar, invdr5 * invdrsqd, m * invdr3);
-  acc.add(0, fmaf(qx, invdr5, -g * d0));
-  acc.add(1, fmaf(qy, invdr5, -g * d1));
-  acc.add(2, fmaf(qz, invdr5, -g * d2));
-  acc.add(3, fmaf(0.5f * qscalar, invdr5, m * invdrmag));
-}
-
-__device__ __forceinline__ void pair_term32(float d0, float d1, float d2, float invhp, float zo_p,
-                                            float mq, float hq, float zq, Kahan4& acc) {
-  const float drsqd = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
-  const float inv = rsqrtf(fmaxf(drsqd, 1.0e-30f));
-  const float drmag = drsqd * inv;
-  const float invdrmag = inv;
-  float grav, dpot;
-  if (drmag * invhp < KERNRANGE) {
-    const int kern = min((int)((5000.0f * drmag) * invhp), KERNTOT);
-    float w5, w4, w6;
-    m4_grav32(kern, w5, w4, w6);
-    grav = invhp * invhp * fmaf(zo_p * w4, invhp * invhp, w5);
-    dpot = invhp * w6;
-  } else {
-    grav = invdrmag * invdrmag;
-    dpot = invdrmag;
-  }
-  const float invhq = __frcp_rn(hq);
-  if (drmag < KERNRANGE * hq) {
-    const int kern = min((int)((5000.0f * drmag) * invhq), KERNTOT);
-    float w5, w4, w6;
-    m4_grav32(kern, w5, w4, w6);
-    grav = fmaf(invhq * invhq, fmaf(zq * w4, invhq * invhq, w5), grav);
-    dpot = fmaf(invhq, w6, dpot);
-  } else {
-    grav = fmaf(invdrmag, invdrmag, grav);
-    dpot = dpot + invdrmag;
-  }
-  const float f = 0.5f * mq * invdrmag * grav;
-  acc.add(0, f * d0);
-  acc.add(1, f * d1);
-  acc.add(2, f * d2);
-  acc.add(3, 0.5f * mq * dpot);
-}
-
 __device__ __forceinline__ void count_add(unsigned long long* counts, unsigned long long ncell,
                                           unsigned long long npair) {
   // warp-aggregated interaction counters
@@ -224,7 +147,8 @@ __device__ __forceinline__ void count_add(unsigned long long* counts, unsigned l
 // all lanes together (broadcast loads, per-lane predicate).
 constexpr int GW_THREADS = 128;
 constexpr int GW_WARPS = GW_THREADS / 32;
-constexpr int GW_CAP = 64;
+constexpr int GW_CAP = 64;       // accepted-cell entries per warp list
+constexpr int GW_ITEMS = 128;    // near-field particle items per warp list
 constexpr unsigned FULLMASK = 0xffffffffu;
 
 struct GravWalk {
@@ -238,17 +162,112 @@ struct GravWalk {
   double rootx, rooty, rootz;
 };
 
+// M4 softened-gravity functions w5, w4, w6 (setup/kernel.F90:80-81, :99-102)
+// at the centre of the reference's table bin int(5000 r/h) (clamped to
+// KERNTOT), in FP32; both polynomial pieces are evaluated and selected so the
+// lanes of a warp do not diverge.
+__device__ __forceinline__ void m4_grav_bin(float x, float& w5, float& w4, float& w6) {
+  const float kf = fminf(floorf(5000.0f * x), (float)KERNTOT);
+  const float s = fmaf(kf, 2.0e-4f, 1.0e-4f);
+  const float s2 = s * s;
+  const float i5 = s * fmaf(s2, fmaf(0.5f, s, -1.2f), 1.33333333f);
+  const float i4 = 0.318309886f * s * fmaf(2.25f, s, -3.0f);
+  const float i6 = fmaf(s2, fmaf(s2, fmaf(-0.1f, s, 0.3f), -0.666666667f), 1.4f);
+  const float rs = __fdividef(1.0f, s);
+  const float o5 = s * fmaf(s, fmaf(s, fmaf(-0.166666667f, s, 1.2f), -3.0f), 2.66666667f) -
+                   0.0666666667f * rs * rs;
+  const float sa = 2.0f - s;
+  const float o4 = -0.238732415f * sa * sa;
+  const float o6 = fmaf(s2, fmaf(s, fmaf(s, fmaf(0.0333333333f, s, -0.3f), 1.0f), -1.33333333f),
+                        1.6f) - 0.0666666667f * rs;
+  const bool in = kf < 0.5f * (float)KERNTOT;
+  w5 = in ? i5 : o5;
+  w4 = in ? i4 : o4;
+  w6 = in ? i6 : o6;
+}
+
+// gravity_gradh.F90:57-86 in FP32, dr = rpp - rp, invhq precomputed
+__device__ __forceinline__ void pair32(float d0, float d1, float d2, float invhp, float zo_p,
+                                       float mq, float invhq, float zq, float& ax, float& ay,
+                                       float& az, float& ap) {
+  const float drsqd = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
+  const float inv = rsqrtf(fmaxf(drsqd, 1.0e-30f));
+  const float drmag = drsqd * inv;
+  float w5, w4, w6;
+  const float xp = drmag * invhp;
+  m4_grav_bin(xp, w5, w4, w6);
+  const float ihp2 = invhp * invhp;
+  const float inv2 = inv * inv;
+  float grav = xp < KERNRANGE ? ihp2 * fmaf(zo_p * w4, ihp2, w5) : inv2;
+  float dpot = xp < KERNRANGE ? invhp * w6 : inv;
+  const float xq = drmag * invhq;
+  m4_grav_bin(xq, w5, w4, w6);
+  const float ihq2 = invhq * invhq;
+  grav += xq < KERNRANGE ? ihq2 * fmaf(zq * w4, ihq2, w5) : inv2;
+  dpot += xq < KERNRANGE ? invhq * w6 : inv;
+  const float f = 0.5f * mq * inv * grav;
+  ax = fmaf(f, d0, ax);
+  ay = fmaf(f, d1, ay);
+  az = fmaf(f, d2, az);
+  ap = fmaf(0.5f * mq, dpot, ap);
+}
+
+// BHgrav_accel.F90:159-189 in FP32, dr = rp - rc
+__device__ __forceinline__ void cell32(float d0, float d1, float d2, const float4& a, const float4& q,
+                                       float q5, float& ax, float& ay, float& az, float& ap) {
+  const float drsqd = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
+  const float invdrmag = rsqrtf(drsqd);
+  const float invdrsqd = invdrmag * invdrmag;
+  const float invdr3 = invdrsqd * invdrmag;
+  const float invdr5 = invdr3 * invdrsqd;
+  const float qx = fmaf(q.w, d2, fmaf(q.y, d1, q.x * d0));
+  const float qy = fmaf(q5, d2, fmaf(q.z, d1, q.y * d0));
+  const float qz = fmaf(-(q.x + q.z), d2, fmaf(q5, d1, q.w * d0));
+  const float qscalar = fmaf(qz, d2, fmaf(qy, d1, qx * d0));
+  const float g = fmaf(2.5f * qscalar, invdr5 * invdrsqd, a.w * invdr3);
+  ax += fmaf(qx, invdr5, -g * d0);
+  ay += fmaf(qy, invdr5, -g * d1);
+  az += fmaf(qz, invdr5, -g * d2);
+  ap += fmaf(0.5f * qscalar, invdr5, a.w * invdrmag);
+}
+
+// Per-warp list records, prepared lane-parallel at flush time.
+template <bool MIXED>
+struct GwRec;
+template <>
+struct GwRec<true> {
+  float4 ca[GW_CAP];      // cell: (r_ref - COM) in FP32, m
+  float4 cb[GW_CAP];      // q1..q4
+  float cq5[GW_CAP];
+  int cid[GW_CAP];
+  unsigned cmask[GW_CAP];
+  float4 pa[GW_ITEMS];    // particle: (r_q - r_ref) in FP32, m
+  float2 pb[GW_ITEMS];    // 1/h, zeta
+  int qid[GW_ITEMS];
+  unsigned qmask[GW_ITEMS];
+};
+template <>
+struct GwRec<false> {
+  double4 ca[GW_CAP];     // COM, m
+  double4 cb[GW_CAP];
+  double cq5[GW_CAP];
+  int cid[GW_CAP];
+  unsigned cmask[GW_CAP];
+  double4 pa[GW_ITEMS];   // position, m
+  double2 pb[GW_ITEMS];   // h, zeta
+  int qid[GW_ITEMS];
+  unsigned qmask[GW_ITEMS];
+};
+
 template <bool MIXED>
 __global__ void __launch_bounds__(GW_THREADS)
 k_grav_warp(int nact, const int* __restrict__ act, const double4* __restrict__ pm,
             const double2* __restrict__ hz, GravWalk t, const double4* __restrict__ tabG,
             double* __restrict__ acc, double* __restrict__ gpot, int nsink,
             const double* __restrict__ sinks, DevError* err, unsigned long long* counts) {
-  __shared__ int s_cell[GW_WARPS][GW_CAP];
-  __shared__ unsigned s_cmask[GW_WARPS][GW_CAP];
-  __shared__ int s_pst[GW_WARPS][GW_CAP];
-  __shared__ unsigned s_pmask[GW_WARPS][GW_CAP];
+  __shared__ GwRec<MIXED> srec[GW_WARPS];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  GwRec<MIXED>& R = srec[w];
   const int i = blockIdx.x * GW_THREADS + threadIdx.x;
   const bool live = i < nact;
   if (__ballot_sync(FULLMASK, live) == 0) return;       // whole warp past the end
@@ -273,23 +292,44 @@ k_grav_warp(int nact, const int* __restrict__ act, const double4* __restrict__ p
 
   auto flush_cells = [&]() {
     __syncwarp();
-    for (int e = 0; e < nc; ++e) {
-      const int cid = s_cell[w][e];
-      const bool mine = (s_cmask[w][e] >> lane) & 1u;
+    for (int e = lane; e < nc; e += 32) {                    // lane-parallel preparation
+      const int cid = R.cid[e];
       const double4 a = t.gA[cid];
       const double4 q = t.gB[cid];
       const double q5 = t.gC[cid].x;
       if (MIXED) {
-        const float fx = (float)(rx - a.x), fy = (float)(ry - a.y), fz = (float)(rz - a.z);
-        if (mine) {
-          cell_term32(ux + fx, uy + fy, uz + fz, (float)a.w, (float)q.x, (float)q.y, (float)q.z,
-                      (float)q.w, (float)q5, kc);
+        reinterpret_cast<float4*>(R.ca)[e] =
+            make_float4((float)(rx - a.x), (float)(ry - a.y), (float)(rz - a.z), (float)a.w);
+        reinterpret_cast<float4*>(R.cb)[e] = make_float4((float)q.x, (float)q.y, (float)q.z, (float)q.w);
+        reinterpret_cast<float*>(R.cq5)[e] = (float)q5;
+      } else {
+        reinterpret_cast<double4*>(R.ca)[e] = a;
+        reinterpret_cast<double4*>(R.cb)[e] = q;
+        reinterpret_cast<double*>(R.cq5)[e] = q5;
+      }
+    }
+    __syncwarp();
+    if (MIXED) {
+      float sx = 0.f, sy = 0.f, sz = 0.f, sp = 0.f;
+      for (int e = 0; e < nc; ++e) {
+        if ((R.cmask[e] >> lane) & 1u) {
+          const float4 a = reinterpret_cast<const float4*>(R.ca)[e];
+          cell32(ux + a.x, uy + a.y, uz + a.z, a, reinterpret_cast<const float4*>(R.cb)[e],
+                 reinterpret_cast<const float*>(R.cq5)[e], sx, sy, sz, sp);
           ++ncell;
         }
-      } else if (mine) {
-        const double d0 = P.x - a.x, d1 = P.y - a.y, d2 = P.z - a.z;
-        cell_term64(d0, d1, d2, (d0 * d0 + d1 * d1) + d2 * d2, a, q, q5, cx, cy, cz, cp);
-        ++ncell;
+      }
+      kc.add(0, sx); kc.add(1, sy); kc.add(2, sz); kc.add(3, sp);
+    } else {
+      for (int e = 0; e < nc; ++e) {
+        if ((R.cmask[e] >> lane) & 1u) {
+          const double4 a = reinterpret_cast<const double4*>(R.ca)[e];
+          const double d0 = P.x - a.x, d1 = P.y - a.y, d2 = P.z - a.z;
+          cell_term64(d0, d1, d2, (d0 * d0 + d1 * d1) + d2 * d2, a,
+                      reinterpret_cast<const double4*>(R.cb)[e],
+                      reinterpret_cast<const double*>(R.cq5)[e], cx, cy, cz, cp);
+          ++ncell;
+        }
       }
     }
     nc = 0;
@@ -297,22 +337,36 @@ k_grav_warp(int nact, const int* __restrict__ act, const double4* __restrict__ p
   };
   auto flush_pairs = [&]() {
     __syncwarp();
-    for (int e = 0; e < np; ++e) {
-      const int code = s_pst[w][e];
-      const bool mine = (s_pmask[w][e] >> lane) & 1u;
-      const int q0 = code >> 3, cnt = (code & 7) + 1;
-      for (int k = 0; k < cnt; ++k) {
-        const int q = q0 + k;
-        const double4 Q = pm[q];
-        const double2 H = hz[q];
-        if (MIXED) {
-          const float gx = (float)(Q.x - rx), gy = (float)(Q.y - ry), gz = (float)(Q.z - rz);
-          if (mine && q != p) {
-            pair_term32(gx - ux, gy - uy, gz - uz, invhp32, zo32, (float)Q.w, (float)H.x,
-                        (float)H.y, kc);
-            ++npair;
-          }
-        } else if (mine && q != p) {
+    for (int e = lane; e < np; e += 32) {
+      const int q = R.qid[e];
+      const double4 Q = pm[q];
+      const double2 H = hz[q];
+      if (MIXED) {
+        reinterpret_cast<float4*>(R.pa)[e] =
+            make_float4((float)(Q.x - rx), (float)(Q.y - ry), (float)(Q.z - rz), (float)Q.w);
+        reinterpret_cast<float2*>(R.pb)[e] = make_float2((float)(1.0 / H.x), (float)H.y);
+      } else {
+        reinterpret_cast<double4*>(R.pa)[e] = Q;
+        reinterpret_cast<double2*>(R.pb)[e] = H;
+      }
+    }
+    __syncwarp();
+    if (MIXED) {
+      float sx = 0.f, sy = 0.f, sz = 0.f, sp = 0.f;
+      for (int e = 0; e < np; ++e) {
+        if (((R.qmask[e] >> lane) & 1u) && R.qid[e] != p) {
+          const float4 a = reinterpret_cast<const float4*>(R.pa)[e];
+          const float2 b = reinterpret_cast<const float2*>(R.pb)[e];
+          pair32(a.x - ux, a.y - uy, a.z - uz, invhp32, zo32, a.w, b.x, b.y, sx, sy, sz, sp);
+          ++npair;
+        }
+      }
+      kc.add(0, sx); kc.add(1, sy); kc.add(2, sz); kc.add(3, sp);
+    } else {
+      for (int e = 0; e < np; ++e) {
+        if (((R.qmask[e] >> lane) & 1u) && R.qid[e] != p) {
+          const double4 Q = reinterpret_cast<const double4*>(R.pa)[e];
+          const double2 H = reinterpret_cast<const double2*>(R.pb)[e];
           pair_term64(Q.x - P.x, Q.y - P.y, Q.z - P.z, invhp, zo_p, Q.w, H.x, H.y, tabG, qx, qy,
                       qz, qp);
           ++npair;
@@ -334,7 +388,7 @@ k_grav_warp(int nact, const int* __restrict__ act, const double4* __restrict__ p
     if (lk.x == 1) {                                         // BHgrav_accel.F90:128-136
       const unsigned m = __ballot_sync(FULLMASK, actv && lk.w != p);
       if (m) {
-        if (lane == 0) { s_pst[w][np] = lk.w * 8; s_pmask[w][np] = m; }
+        if (lane == 0) { R.qid[np] = lk.w; R.qmask[np] = m; }
         ++np;
       }
       c = lk.y;
@@ -355,13 +409,13 @@ k_grav_warp(int nact, const int* __restrict__ act, const double4* __restrict__ p
       const unsigned macc = __ballot_sync(FULLMASK, accept);
       const unsigned mopn = __ballot_sync(FULLMASK, actv && !accept);
       if (macc) {
-        if (lane == 0) { s_cell[w][nc] = c; s_cmask[w][nc] = macc; }
+        if (lane == 0) { R.cid[nc] = c; R.cmask[nc] = macc; }
         ++nc;
       }
       if (lk.x > 0) {                                        // :242-253
         if (mopn) {
-          if (lane == 0) { s_pst[w][np] = lk.w * 8 + (lk.x - 1); s_pmask[w][np] = mopn; }
-          ++np;
+          if (lane < lk.x) { R.qid[np + lane] = lk.w + lane; R.qmask[np + lane] = mopn; }
+          np += lk.x;
         }
         c = lk.y;
       } else if (lk.x == 0 && mopn) {
@@ -372,7 +426,7 @@ k_grav_warp(int nact, const int* __restrict__ act, const double4* __restrict__ p
       }
     }
     if (nc == GW_CAP) flush_cells();
-    if (np == GW_CAP) flush_pairs();
+    if (np > GW_ITEMS - LEAFMAX) flush_pairs();
     if (c > t.ctot) break;
   }
   flush_cells();
@@ -404,6 +458,7 @@ k_grav_warp(int nact, const int* __restrict__ act, const double4* __restrict__ p
   }
   count_add(counts, ncell, npair);
 }
+
 
 // sph_sim/sph_sink_forces.F90:49-110: BHgrav_accel(-s) with gravity_meanh
 // near field (BHgrav_accel.F90:299-314), then the other sinks directly.

@@ -486,48 +486,116 @@ __global__ void __launch_bounds__(SW_THREADS) k_neib_warp(
   if (live) pptot[p] = cnt;
 }
 
-// sph/hydro_gradh.F90:9-339 (NEIGHBOUR_LISTS, ARTIFICIAL_VISCOSITY=MON97)
+// sph/hydro_gradh.F90:9-339 (NEIGHBOUR_LISTS, ARTIFICIAL_VISCOSITY=MON97).
+// The per-particle factors press/rho/rho/omega (:96, :178) and
+// (1/h)**(NDIM+1) (:91, :196) are computed once per particle by k_hydro_prep
+// with the reference's expressions, so every pair reads them instead of
+// recomputing them (same values).
+__global__ void k_hydro_prep(int n, const double2* __restrict__ hz, const double* __restrict__ rho,
+                             const double* __restrict__ omega, const double* __restrict__ press,
+                             double* __restrict__ pf, double* __restrict__ hf4) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const double r = rho[p];
+  pf[p] = ((press[p] / r) / r) / omega[p];
+  hf4[p] = pow(1.0 / hz[p].x, NDIMPLUS1);
+}
+
+// M4 (or M4 Thomas-Couchman) gradient w1 (setup/kernel.F90:66-73, :93) at the
+// centre of table bin int(5000 r/h) in FP32, for the mixed form of the hydro
+// pair arithmetic.
+__device__ __forceinline__ float m4_w1_bin(float x, bool tc) {
+  const float kf = fminf(floorf(5000.0f * x), (float)KERNTOT);
+  const float s = fmaf(kf, 2.0e-4f, 1.0e-4f);
+  const float inner = (tc && kf < 3333.0f) ? -1.0f : s * fmaf(2.25f, s, -3.0f);
+  const float sa = 2.0f - s;
+  const float outer = -0.75f * sa * sa;
+  return 0.318309886f * (kf < 0.5f * (float)KERNTOT ? inner : outer);
+}
+
+template <bool MIXED>
 __global__ void __launch_bounds__(128) k_hydro(int nact, const int* __restrict__ act,
                                                const double4* __restrict__ pm,
                                                const double2* __restrict__ hz,
                                                const double4* __restrict__ vel,
                                                const double* __restrict__ rho,
-                                               const double* __restrict__ omega,
-                                               const double* __restrict__ press,
+                                               const double* __restrict__ pf,
+                                               const double* __restrict__ hf4,
                                                const double* __restrict__ sound,
                                                const int* __restrict__ pptot,
                                                const int* __restrict__ pplist, int L, HydroTree t,
                                                const double4* __restrict__ tabG, double alpha,
-                                               double* __restrict__ acc, DevError* err) {
+                                               bool tc, double* __restrict__ acc, DevError* err) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nact) return;
   const int p = act ? act[i] : i;
   const double4 P = pm[p];
   const double hp = hz[p].x;
   const double invhp = 1.0 / hp;
-  const double hfactor_p = pow(invhp, NDIMPLUS1);
+  const double hfactor_p = hf4[p];
   const double4 vp = vel[p];
   const double sound_p = sound[p];
   const double rho_p = rho[p];
-  const double pfactor_p = ((press[p] / rho_p) / rho_p) / omega[p];
+  const double pfactor_p = pf[p];
   const double beta = 2.0 * alpha;
   double at0 = 0.0, at1 = 0.0, at2 = 0.0, ad0 = 0.0, ad1 = 0.0, ad2 = 0.0;
+  // FP32 form
+  const float hp32 = (float)hp, invhp32 = (float)invhp, hf32 = (float)hfactor_p;
+  const float pf32 = (float)pfactor_p, c32 = (float)sound_p, rho32 = (float)rho_p;
+  const float alpha32 = (float)alpha, beta32 = (float)beta;
+  float f0 = 0.f, f1 = 0.f, f2 = 0.f, g0 = 0.f, g1 = 0.f, g2 = 0.f;
   auto pair = [&](int q) {
-    double wmean = 0.0;
-    const double rho_q = rho[q];
     const double4 Q = pm[q];
     const double hq = hz[q].x;
+    if (MIXED) {
+      const float u0 = (float)(Q.x - P.x), u1 = (float)(Q.y - P.y), u2 = (float)(Q.z - P.z);
+      const float hq32 = (float)hq;
+      const float r2 = fmaf(u2, u2, fmaf(u1, u1, u0 * u0));
+      if (r2 >= 4.0f * hp32 * hp32 && r2 >= 4.0f * hq32 * hq32) return;
+      const double4 V = vel[q];
+      const float dv0 = (float)(V.x - vp.x), dv1 = (float)(V.y - vp.y), dv2 = (float)(V.z - vp.z);
+      const float inv = rsqrtf(fmaxf(r2, 1.0e-30f));
+      const float drmag = r2 * inv;
+      const float dvdr = fmaf(dv2, u2, fmaf(dv1, u1, dv0 * u0));
+      const float e0 = u0 * inv, e1 = u1 * inv, e2 = u2 * inv;
+      const float invhq32 = __frcp_rn(hq32);
+      const float mq = (float)Q.w;
+      float wmean = 0.f, fsum = 0.f;
+      const float xp = drmag * invhp32;
+      if (xp < KERNRANGE) {
+        const float w1 = m4_w1_bin(xp, tc);
+        wmean = 0.5f * hf32 * w1;
+        fsum = mq * pf32 * hf32 * w1;
+      }
+      const float xq = drmag * invhq32;
+      if (xq < KERNRANGE) {
+        const float w1 = m4_w1_bin(xq, tc);
+        const float hfq = (float)hf4[q];
+        wmean = fmaf(0.5f * hfq, w1, wmean);
+        fsum = fmaf(mq * (float)pf[q] * hfq, w1, fsum);
+      }
+      f0 = fmaf(fsum, e0, f0); f1 = fmaf(fsum, e1, f1); f2 = fmaf(fsum, e2, f2);
+      if (dvdr < 0.0f) {
+        const float vsignal = c32 + (float)sound[q] - beta32 * dvdr * inv;
+        const float g = mq * alpha32 * vsignal * dvdr * inv * wmean *
+                        __frcp_rn(0.5f * (rho32 + (float)rho[q]));
+        g0 = fmaf(-g, e0, g0); g1 = fmaf(-g, e1, g1); g2 = fmaf(-g, e2, g2);
+      }
+      return;
+    }
+    double wmean = 0.0;
+    const double rho_q = rho[q];
     double u0 = Q.x - P.x, u1 = Q.y - P.y, u2 = Q.z - P.z;
     double drmag = (u0 * u0 + u1 * u1) + u2 * u2;
-    if (drmag >= (KERNRANGESQD * hp) * hp && drmag >= (KERNRANGESQD * hq) * hq) return;
+    if (drmag >= (KERNRANGESQD * hp) * hp && drmag >= (KERNRANGESQD * hq) * hq) return;  // :154
     drmag = sqrt(drmag) + SMALL_NUMBER;
     const double4 V = vel[q];
     const double dv0 = V.x - vp.x, dv1 = V.y - vp.y, dv2 = V.z - vp.z;
-    const double dvdr = (dv0 * u0 + dv1 * u1) + dv2 * u2;
+    const double dvdr = (dv0 * u0 + dv1 * u1) + dv2 * u2;                         // :157
     const double invdrmag = 1.0 / drmag;
     u0 = u0 * invdrmag; u1 = u1 * invdrmag; u2 = u2 * invdrmag;
-    const double pfactor_q = ((press[q] / rho_q) / rho_q) / omega[q];
-    if (drmag < KERNRANGE * hp) {
+    const double pfactor_q = pf[q];
+    if (drmag < KERNRANGE * hp) {                                                 // :181-192
       int kern = (int)((HALFKERNTOT * drmag) * invhp);
       kern = min(kern, KERNTOT);
       const double w1 = tabG[kern].w;
@@ -535,9 +603,9 @@ __global__ void __launch_bounds__(128) k_hydro(int nact, const int* __restrict__
       const double f = ((Q.w * pfactor_p) * hfactor_p) * w1;
       at0 = at0 + f * u0; at1 = at1 + f * u1; at2 = at2 + f * u2;
     }
-    if (drmag < KERNRANGE * hq) {
+    if (drmag < KERNRANGE * hq) {                                                 // :194-207
       const double invhq = 1.0 / hq;
-      const double hfq = pow(invhq, NDIMPLUS1);
+      const double hfq = hf4[q];
       int kern = (int)((HALFKERNTOT * drmag) * invhq);
       kern = min(kern, KERNTOT);
       const double w1 = tabG[kern].w;
@@ -545,8 +613,8 @@ __global__ void __launch_bounds__(128) k_hydro(int nact, const int* __restrict__
       const double f = ((Q.w * pfactor_q) * hfq) * w1;
       at0 = at0 + f * u0; at1 = at1 + f * u1; at2 = at2 + f * u2;
     }
-    const double rhomean = 0.5 * (rho_p + rho_q);
-    if (dvdr < 0.0) {
+    const double rhomean = 0.5 * (rho_p + rho_q);                                 // :213
+    if (dvdr < 0.0) {                                                             // :225-255
       const double vsignal = (sound_p + sound[q]) - ((beta * dvdr) * invdrmag);
       const double g = (((Q.w * alpha) * vsignal) * dvdr) * invdrmag;
       ad0 = ad0 - ((g * u0) * wmean) / rhomean;
@@ -572,9 +640,15 @@ __global__ void __launch_bounds__(128) k_hydro(int nact, const int* __restrict__
     });
   }
   double* a = acc + (size_t)p * 3;
-  a[0] = at0 + ad0;
-  a[1] = at1 + ad1;
-  a[2] = at2 + ad2;
+  if (MIXED) {
+    a[0] = (double)f0 + (double)g0;
+    a[1] = (double)f1 + (double)g1;
+    a[2] = (double)f2 + (double)g2;
+  } else {
+    a[0] = at0 + ad0;                                                            // :287, :297
+    a[1] = at1 + ad1;
+    a[2] = at2 + ad2;
+  }
 }
 
 // sph/thermal.F90:52-59 (ISOTHERMAL): press = Pconst*T*rho, sound = sqrt(press/rho)
@@ -609,9 +683,18 @@ void launch_neib(Ctx& c, int nact) {
 
 void launch_hydro(Ctx& c, int nact) {
   if (nact <= 0) return;
-  k_hydro<<<nb(nact, 128), 128, 0, c.st>>>(nact, c.act, c.pm, c.hz, c.vel, c.rho, c.omega, c.press,
-                                           c.sound, c.pptot, c.pplist, c.prm.pp_limit,
-                                           hydro_tree(c), c.tabG, c.prm.alpha, c.acc, c.d_err); ++c.nlaunch;
+  k_hydro_prep<<<nb(c.ptot, 256), 256, 0, c.st>>>(c.ptot, c.hz, c.rho, c.omega, c.press, c.pf,
+                                                  c.hf4);
+  ++c.nlaunch;
+  if (c.prm.precision == 0)
+    k_hydro<false><<<nb(nact, 128), 128, 0, c.st>>>(
+        nact, c.act, c.pm, c.hz, c.vel, c.rho, c.pf, c.hf4, c.sound, c.pptot, c.pplist,
+        c.prm.pp_limit, hydro_tree(c), c.tabG, c.prm.alpha, c.prm.kernel == 1, c.acc, c.d_err);
+  else
+    k_hydro<true><<<nb(nact, 128), 128, 0, c.st>>>(
+        nact, c.act, c.pm, c.hz, c.vel, c.rho, c.pf, c.hf4, c.sound, c.pptot, c.pplist,
+        c.prm.pp_limit, hydro_tree(c), c.tabG, c.prm.alpha, c.prm.kernel == 1, c.acc, c.d_err);
+  ++c.nlaunch;
 }
 
 void launch_thermal(Ctx& c) {

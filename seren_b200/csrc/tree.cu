@@ -104,14 +104,27 @@ __global__ void k_bbox_partial(const double4* __restrict__ pm, int n, double* __
 }
 
 __global__ void k_bbox_final(const double* __restrict__ part, int nblk, TreeInfo* info) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  double rmax[3] = {-BIG_NUMBER, -BIG_NUMBER, -BIG_NUMBER};
-  double rmin[3] = {BIG_NUMBER, BIG_NUMBER, BIG_NUMBER};
-  for (int b = 0; b < nblk; ++b)
+  __shared__ double s[6][BB_T];
+  double mx[3] = {-BIG_NUMBER, -BIG_NUMBER, -BIG_NUMBER};
+  double mn[3] = {BIG_NUMBER, BIG_NUMBER, BIG_NUMBER};
+  for (int b = threadIdx.x; b < nblk; b += BB_T)
     for (int k = 0; k < 3; ++k) {
-      rmax[k] = fmax(rmax[k], part[b * 6 + k]);
-      rmin[k] = fmin(rmin[k], part[b * 6 + 3 + k]);
+      mx[k] = fmax(mx[k], part[b * 6 + k]);
+      mn[k] = fmin(mn[k], part[b * 6 + 3 + k]);
     }
+  for (int k = 0; k < 3; ++k) { s[k][threadIdx.x] = mx[k]; s[3 + k][threadIdx.x] = mn[k]; }
+  __syncthreads();
+  for (int o = BB_T / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o)
+      for (int k = 0; k < 3; ++k) {
+        s[k][threadIdx.x] = fmax(s[k][threadIdx.x], s[k][threadIdx.x + o]);
+        s[3 + k][threadIdx.x] = fmin(s[3 + k][threadIdx.x], s[3 + k][threadIdx.x + o]);
+      }
+    __syncthreads();
+  }
+  if (threadIdx.x != 0) return;
+  const double rmax[3] = {s[0][0], s[1][0], s[2][0]};
+  const double rmin[3] = {s[3][0], s[4][0], s[5][0]};
   const double ext = fmax(fmax(rmax[0] - rmin[0], rmax[1] - rmin[1]), rmax[2] - rmin[2]);
   info->rextent = ext;
   info->cellsize = 0.5 * ext;
@@ -620,7 +633,7 @@ int build_tree(Ctx& c) {
   const int n = c.ptot;
   const int bblk = std::min(nb(n, BB_T), 1184);
   k_bbox_partial<<<bblk, BB_T, 0, c.st>>>(c.pm, n, c.bbox_part); ++c.nlaunch;
-  k_bbox_final<<<1, 1, 0, c.st>>>(c.bbox_part, bblk, c.d_info); ++c.nlaunch;
+  k_bbox_final<<<1, BB_T, 0, c.st>>>(c.bbox_part, bblk, c.d_info); ++c.nlaunch;
   k_keys<<<nb(n, 256), 256, 0, c.st>>>(c.pm, n, c.d_info, c.keys, c.idx); ++c.nlaunch;
   radix_sort(c, n);
   k_root<<<1, 1, 0, c.st>>>(n, c.cmax, c.leaf, c.nextcell, c.ifopen, c.pstart, c.pcount, c.parent,
