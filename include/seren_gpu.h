@@ -79,8 +79,10 @@ int seren_gpu_tree_update(seren_gpu_ctx* ctx, int32_t ptot, double* parray,
  * [BHhydro_hguess when first_call] -> all_sph_gradh for the active particles
  * -> BHhydro_update_hmax -> get_neib.  v is uploaded; parray columns h and
  * zeta, rho, omega, div_v and drhodt are written back for the active
- * particles.  pptot/pplist may be NULL (then the lists stay on the device for
- * seren_gpu_hydro_forces).  acclist == NULL means every particle is active. */
+ * particles (with every particle active, whole parray rows are written, their
+ * x, y, z, m being the ones uploaded by the last tree_update).  pptot/pplist
+ * may be NULL (then the lists stay on the device for seren_gpu_hydro_forces).
+ * acclist == NULL means every particle is active. */
 int seren_gpu_sph_update(seren_gpu_ctx* ctx, int32_t ptot, const int32_t* acclist,
                          int32_t nacc, double* parray, const double* v, double* rho,
                          double* omega, double* div_v, double* drhodt, int32_t* pptot,

@@ -384,7 +384,13 @@ int seren_gpu_sph_update(seren_gpu_ctx* h, int32_t ptot, const int32_t* acclist,
   if (rc) return rc;
   c.have_sph = true;
   // results back to the host arrays
-  if (parray) {
+  if (parray && acclist == nullptr) {
+    // every row changes: copy whole rows (positions and masses are the ones
+    // uploaded by the last tree_update) instead of scattering two columns
+    seren::launch_pack_parray(c, c.stage, ptot);
+    cudaMemcpyAsync(parray, c.stage, sizeof(double) * 6 * (size_t)ptot, cudaMemcpyDeviceToHost,
+                    c.st);
+  } else if (parray) {
     double* pin = seren::pinned(c, (size_t)2 * ptot);
     if (!pin) return fail(c, SEREN_GPU_ERR_CUDA, "pinned staging allocation failed");
     seren::k_pack_hz<<<nb(ptot, 256), 256, 0, c.st>>>(c.hz, ptot, c.stage); ++c.nlaunch;
@@ -567,6 +573,7 @@ int seren_gpu_force_step(seren_gpu_ctx* h, int32_t first_call) {
   const int n = c.ptot;
   c.act = nullptr;
   c.nlaunch = 0;
+  cudaMemsetAsync(c.d_counts, 0, sizeof(int) * 32, c.st);
   cudaEventRecord(c.ev[0], c.st);
   int rc = seren::build_tree(c);
   if (rc) return rc;
@@ -581,7 +588,6 @@ int seren_gpu_force_step(seren_gpu_ctx* h, int32_t first_call) {
   seren::launch_thermal(c);
   seren::launch_hydro(c, n);
   cudaEventRecord(c.ev[4], c.st);
-  cudaMemsetAsync(c.d_counts, 0, sizeof(int) * 32, c.st);
   seren::launch_grav(c, n, 0, nullptr);
   cudaEventRecord(c.ev[5], c.st);
   rc = finish(c, "force_step");

@@ -457,6 +457,7 @@ k_grav_warp(int nact, const int* __restrict__ act, const double4* __restrict__ p
     gpot[p] = pot;
   }
   count_add(counts, ncell, npair);
+  if (lane == 0) atomicAdd(counts + 2, (unsigned long long)visits);
 }
 
 

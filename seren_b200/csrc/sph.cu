@@ -268,12 +268,14 @@ constexpr unsigned FULL = 0xffffffffu;
 template <class Test>
 __device__ __forceinline__ int warp_walk(const HydroTree& t, bool part, int lane,
                                          int* __restrict__ s_leaf, unsigned* __restrict__ s_mask,
-                                         int& cnt, DevError* err, int kid, int who, Test&& test) {
+                                         int& cnt, unsigned long long& nvisit, DevError* err,
+                                         int kid, int who, Test&& test) {
   __syncwarp();
   int c = 0, n = 0, visits = 0;
   int skip = part ? -1 : -2;
   cnt = 0;
   while (true) {
+    ++nvisit;
     if (++visits > t.ctot + 2) {
       if (lane == 0) set_error(err, SEREN_GPU_ERR_WALK, kid, who, c);
       return -1;
@@ -309,7 +311,8 @@ __global__ void __launch_bounds__(SW_THREADS) k_gradh_warp(
     int nact, const int* __restrict__ act, const double4* __restrict__ pm, double2* __restrict__ hz,
     const double4* __restrict__ vel, double* __restrict__ rho, double* __restrict__ omega,
     double* __restrict__ divv, double* __restrict__ drhodt, HydroTree t,
-    const double4* __restrict__ tabA, double h_fac, int pp_gather, double rextent, DevError* err) {
+    const double4* __restrict__ tabA, double h_fac, int pp_gather, double rextent, DevError* err,
+    unsigned long long* counts) {
   __shared__ int s_leaf[SW_WARPS][SW_CAP];
   __shared__ unsigned s_mask[SW_WARPS][SW_CAP];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -320,6 +323,8 @@ __global__ void __launch_bounds__(SW_THREADS) k_gradh_warp(
   const double4 P = pm[p];
   const double rx = P.x, ry = P.y, rz = P.z, mp = P.w;
   const double4 t0 = tabA[0];
+  // warp-level work counters (walks, nodes visited, passes, candidates streamed)
+  unsigned long long nwalk = 0, nvisit = 0, npass = 0, ncand = 0;
   GhState s;
   gh_init(s, hz[p].x, rextent);
   int st = live ? GH_WALK : GH_OFF;
@@ -341,7 +346,8 @@ __global__ void __launch_bounds__(SW_THREADS) k_gradh_warp(
       }
       if (__any_sync(FULL, want)) {
         int cnt = 0;
-        nent = warp_walk(t, R >= 0.0, lane, s_leaf[w], s_mask[w], cnt, err, KID_GRADH, p,
+        ++nwalk;
+        nent = warp_walk(t, R >= 0.0, lane, s_leaf[w], s_mask[w], cnt, nvisit, err, KID_GRADH, p,
                          gather_test);
         if (nent < 0) { overflow = true; break; }
         if (want) s.pp_pot = cnt;
@@ -372,12 +378,20 @@ __global__ void __launch_bounds__(SW_THREADS) k_gradh_warp(
       const int code = s_leaf[w][e];
       const bool mine = on && ((s_mask[w][e] >> lane) & 1u);
       const int q0 = code >> 3, n = (code & 7) + 1;
-      for (int k = 0; k < n; ++k) {
-        const int q = q0 + k;
-        const double4 Q = pm[q];
-        if (mine && q != p) gh_density_term(Q, rx, ry, rz, hs, ih, hf, tabA, rt);
+      ncand += n;
+      // the leaf's particles are contiguous: issue four loads before using them
+      for (int k0 = 0; k0 < n; k0 += 4) {
+        double4 Q[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) Q[k] = pm[q0 + min(k0 + k, n - 1)];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const int q = q0 + k0 + k;
+          if (k0 + k < n && mine && q != p) gh_density_term(Q[k], rx, ry, rz, hs, ih, hf, tabA, rt);
+        }
       }
     }
+    ++npass;
     if (on) st = gh_after_pass(s, mp, h_fac, rextent, rt) ? GH_DONE : GH_WALK;
   }
   if (overflow) {
@@ -398,14 +412,29 @@ __global__ void __launch_bounds__(SW_THREADS) k_gradh_warp(
     const int code = s_leaf[w][e];
     const bool mine = on && ((s_mask[w][e] >> lane) & 1u);
     const int q0 = code >> 3, n = (code & 7) + 1;
-    for (int k = 0; k < n; ++k) {
-      const int q = q0 + k;
-      const double4 Q = pm[q];
-      const double4 V = vel[q];
-      if (mine && q != p) gh_final_term(Q, V, rx, ry, rz, vp, hs, ih, hf, tabA, f);
+    ncand += n;
+    for (int k0 = 0; k0 < n; k0 += 2) {
+      double4 Q[2], V[2];
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        Q[k] = pm[q0 + min(k0 + k, n - 1)];
+        V[k] = vel[q0 + min(k0 + k, n - 1)];
+      }
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const int q = q0 + k0 + k;
+        if (k0 + k < n && mine && q != p) gh_final_term(Q[k], V[k], rx, ry, rz, vp, hs, ih, hf, tabA, f);
+      }
     }
   }
+  ++npass;
   if (on) gh_store(p, mp, hp, f, hz, rho, omega, divv, drhodt, err);
+  if (lane == 0) {
+    atomicAdd(counts + 3, nwalk);
+    atomicAdd(counts + 4, nvisit);
+    atomicAdd(counts + 5, npass);
+    atomicAdd(counts + 6, ncand);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -437,7 +466,7 @@ __device__ void neib_one(int p, const double4* __restrict__ pm, const double2* _
 __global__ void __launch_bounds__(SW_THREADS) k_neib_warp(
     int nact, const int* __restrict__ act, const double4* __restrict__ pm,
     const double2* __restrict__ hz, HydroTree t, int L, int* __restrict__ pptot,
-    int* __restrict__ pplist, DevError* err) {
+    int* __restrict__ pplist, DevError* err, unsigned long long* counts) {
   __shared__ int s_leaf[SW_WARPS][SW_CAP];
   __shared__ unsigned s_mask[SW_WARPS][SW_CAP];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -450,7 +479,8 @@ __global__ void __launch_bounds__(SW_THREADS) k_neib_warp(
   const double R = KERNRANGE * hp;
   const double hsp = (KERNRANGESQD * hp) * hp;
   int cnt = 0;
-  const int nent = warp_walk(t, live, lane, s_leaf[w], s_mask[w], cnt, err, KID_NEIB, p,
+  unsigned long long nvisit = 0;
+  const int nent = warp_walk(t, live, lane, s_leaf[w], s_mask[w], cnt, nvisit, err, KID_NEIB, p,
                              [&](const double4& h, int c) {
                                const double d0 = h.x - P.x, d1 = h.y - P.y, d2 = h.z - P.z;
                                const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
@@ -484,6 +514,11 @@ __global__ void __launch_bounds__(SW_THREADS) k_neib_warp(
     }
   }
   if (live) pptot[p] = cnt;
+  if (lane == 0) {
+    unsigned long long ncand = 0;
+    for (int e = 0; e < nent; ++e) ncand += (s_leaf[w][e] & 7) + 1;
+    atomicAdd(counts + 7, ncand);
+  }
 }
 
 // sph/hydro_gradh.F90:9-339 (NEIGHBOUR_LISTS, ARTIFICIAL_VISCOSITY=MON97).
@@ -672,13 +707,17 @@ void launch_gradh(Ctx& c, int nact) {
   if (nact <= 0) return;
   k_gradh_warp<<<nb(nact, SW_THREADS), SW_THREADS, 0, c.st>>>(
       nact, c.act, c.pm, c.hz, c.vel, c.rho, c.omega, c.div_v, c.drhodt, hydro_tree(c), c.tabA,
-      c.prm.h_fac, c.prm.pp_gather, c.info.rextent, c.d_err); ++c.nlaunch;
+      c.prm.h_fac, c.prm.pp_gather, c.info.rextent, c.d_err,
+      reinterpret_cast<unsigned long long*>(c.d_counts));
+  ++c.nlaunch;
 }
 
 void launch_neib(Ctx& c, int nact) {
   if (nact <= 0) return;
   k_neib_warp<<<nb(nact, SW_THREADS), SW_THREADS, 0, c.st>>>(
-      nact, c.act, c.pm, c.hz, hydro_tree(c), c.prm.pp_limit, c.pptot, c.pplist, c.d_err); ++c.nlaunch;
+      nact, c.act, c.pm, c.hz, hydro_tree(c), c.prm.pp_limit, c.pptot, c.pplist, c.d_err,
+      reinterpret_cast<unsigned long long*>(c.d_counts));
+  ++c.nlaunch;
 }
 
 void launch_hydro(Ctx& c, int nact) {
