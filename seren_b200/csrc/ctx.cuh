@@ -87,6 +87,8 @@ struct Ctx {
   float* wLo = nullptr;       // gravity walk: lower MAC bracket
   double4* hA = nullptr;      // hydro: bbox centre x, y, z, rmax
   double* hrm = nullptr;      // hydro: hrangemax
+  float4* hA32 = nullptr;     // hydro walk: FP32 centre - root centre, rmax rounded up
+  float* hrm32 = nullptr;     // hydro walk: hrangemax rounded up
   double* hmax = nullptr;     // stock: max h in the cell (at stock time)
   double4* bbmin = nullptr;
   double4* bbmax = nullptr;

@@ -17,7 +17,11 @@ struct HydroTree {
   const int4* link;     // {leaf, nextcell, ifopen, pstart}
   const double4* hA;    // bbox centre, rmax
   const double* hrm;    // hrangemax
+  const float4* hA32;   // FP32 centre - root centre, rmax rounded up
+  const float* hrm32;   // hrangemax rounded up
   int ctot;
+  double rootx, rooty, rootz;
+  float delta;          // bound on the FP32 rounding of a root-relative coordinate
 };
 
 // BHtree/BHhydrowalk_hgather.F90:11-77 (gather test only).  f(q) is called
@@ -257,13 +261,32 @@ __device__ void gradh_one(int p, const double4* __restrict__ pm, double2* __rest
 // warp-uniform and a lane that fails a branch cell's test skips that subtree
 // (its skip marker is the cell's nextcell), so a lane's bits select exactly the
 // leaves its own walk would open, in the same depth-first order.  Opened
-// leaves are stored once per warp as (pstart, count) with the lane mask.
+// leaves are stored once per warp as (pstart, count) with the lane mask; each
+// lane then copies the leaves of its own bits into its own list, so every
+// pass over candidates runs over that particle's own candidates only, in the
+// reference's list order.
+//
+// Cell tests run first in FP32 on coordinates relative to the root centre:
+// test32() decides when the FP32 distance is outside a margin around the
+// threshold that covers every FP32 rounding involved (coordinates within
+// delta, the difference, the squares, the sum and the threshold itself), and
+// the test is redone in FP64 exactly as the reference writes it otherwise.
 constexpr int SW_THREADS = 128;
 constexpr int SW_WARPS = SW_THREADS / 32;
-constexpr int SW_CAP = 256;
+constexpr int SW_CAP = 256;      // union leaves per warp
+constexpr int OWN_CAP = 64;      // leaves per lane
 constexpr unsigned FULL = 0xffffffffu;
 
-// test(h, c) -> bool is the lane's cell test; returns the entry count, or -1
+// 1: d2 <= T^2 for sure, 0: d2 > T^2 for sure, -1: too close to tell in FP32
+__device__ __forceinline__ int test32(float d2, float T, float delta) {
+  const float T2 = T * T;
+  const float marg = fmaf(8.0f * delta, T, fmaf(16.0f * delta, delta, 1.0e-6f * T2));
+  if (d2 < T2 - marg) return 1;
+  if (d2 > T2 + marg) return 0;
+  return -1;
+}
+
+// test(c) -> bool is the lane's cell test; returns the entry count, or -1
 // when the list overflowed.  cnt accumulates the lane's candidate count.
 template <class Test>
 __device__ __forceinline__ int warp_walk(const HydroTree& t, bool part, int lane,
@@ -283,7 +306,7 @@ __device__ __forceinline__ int warp_walk(const HydroTree& t, bool part, int lane
     const int4 lk = t.link[c];
     if (skip == c) skip = -1;
     bool pass = false;
-    if (skip == -1) pass = test(t.hA[c], c);
+    if (skip == -1) pass = test(c);
     const unsigned m = __ballot_sync(FULL, pass);
     if (lk.x > 0) {
       if (m) {
@@ -305,6 +328,22 @@ __device__ __forceinline__ int warp_walk(const HydroTree& t, bool part, int lane
   return n;
 }
 
+// copy the union entries of this lane's bits into the lane's own list;
+// returns the lane's entry count (may exceed OWN_CAP: overflow)
+__device__ __forceinline__ int own_list(int nent, int lane, const int* __restrict__ s_leaf,
+                                        const unsigned* __restrict__ s_mask,
+                                        int (*__restrict__ own)[32]) {
+  int nown = 0;
+  for (int e = 0; e < nent; ++e) {
+    if ((s_mask[e] >> lane) & 1u) {
+      if (nown < OWN_CAP) own[nown][lane] = s_leaf[e];
+      ++nown;
+    }
+  }
+  __syncwarp();
+  return nown;
+}
+
 enum : int { GH_WALK = 0, GH_PASS = 1, GH_DONE = 2, GH_OFF = 3 };
 
 __global__ void __launch_bounds__(SW_THREADS) k_gradh_warp(
@@ -315,6 +354,7 @@ __global__ void __launch_bounds__(SW_THREADS) k_gradh_warp(
     unsigned long long* counts) {
   __shared__ int s_leaf[SW_WARPS][SW_CAP];
   __shared__ unsigned s_mask[SW_WARPS][SW_CAP];
+  __shared__ int s_own[SW_WARPS][OWN_CAP][32];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int i = blockIdx.x * SW_THREADS + threadIdx.x;
   const bool live = i < nact;
@@ -322,19 +362,26 @@ __global__ void __launch_bounds__(SW_THREADS) k_gradh_warp(
   const int p = live ? (act ? act[i] : i) : (act ? act[nact - 1] : nact - 1);
   const double4 P = pm[p];
   const double rx = P.x, ry = P.y, rz = P.z, mp = P.w;
+  const float px = (float)(rx - t.rootx), py = (float)(ry - t.rooty), pz = (float)(rz - t.rootz);
   const double4 t0 = tabA[0];
-  // warp-level work counters (walks, nodes visited, passes, candidates streamed)
+  // warp-level work counters (walks, nodes visited, passes, candidates)
   unsigned long long nwalk = 0, nvisit = 0, npass = 0, ncand = 0;
   GhState s;
   gh_init(s, hz[p].x, rextent);
   int st = live ? GH_WALK : GH_OFF;
   double R = -1.0;                 // search radius of the lane's current list
-  int nent = 0;
+  float R32 = -1.0f;
+  int nown = 0;
   bool overflow = false;
-  auto gather_test = [&](const double4& h, int) {
-    const double d0 = h.x - rx, d1 = h.y - ry, d2 = h.z - rz;
+  auto gather_test = [&](int c) {                      // BHhydrowalk_hgather.F90:36-40
+    const float4 h32 = t.hA32[c];
+    const float d0 = h32.x - px, d1 = h32.y - py, d2 = h32.z - pz;
+    const int r = test32((d0 * d0 + d1 * d1) + d2 * d2, R32 + h32.w, t.delta);
+    if (r >= 0) return r == 1;
+    const double4 h = t.hA[c];
+    const double e0 = h.x - rx, e1 = h.y - ry, e2 = h.z - rz;
     const double tt = R + h.w;
-    return ((d0 * d0 + d1 * d1) + d2 * d2) <= tt * tt;
+    return ((e0 * e0 + e1 * e1) + e2 * e2) <= tt * tt;
   };
   while (!overflow) {
     while (__any_sync(FULL, st == GH_WALK)) {                          // :154-191
@@ -342,14 +389,17 @@ __global__ void __launch_bounds__(SW_THREADS) k_gradh_warp(
       if (st == GH_WALK && s.hp > s.h_high) {
         s.h_high = s.hp * HMULT;
         R = KERNRANGE * s.h_high;
+        R32 = (float)R;
         want = true;
       }
       if (__any_sync(FULL, want)) {
         int cnt = 0;
         ++nwalk;
-        nent = warp_walk(t, R >= 0.0, lane, s_leaf[w], s_mask[w], cnt, nvisit, err, KID_GRADH, p,
-                         gather_test);
+        const int nent = warp_walk(t, R >= 0.0, lane, s_leaf[w], s_mask[w], cnt, nvisit, err,
+                                   KID_GRADH, p, gather_test);
         if (nent < 0) { overflow = true; break; }
+        nown = own_list(nent, lane, s_leaf[w], s_mask[w], s_own[w]);
+        if (__any_sync(FULL, nown > OWN_CAP)) { overflow = true; break; }
         if (want) s.pp_pot = cnt;
       }
       if (st == GH_WALK) {
@@ -361,6 +411,7 @@ __global__ void __launch_bounds__(SW_THREADS) k_gradh_warp(
             set_error(err, SEREN_GPU_ERR_WALK, KID_GRADH, p, -1);
             st = GH_OFF;
             R = -1.0;
+            R32 = -1.0f;
           }
         } else {
           st = GH_PASS;
@@ -368,67 +419,51 @@ __global__ void __launch_bounds__(SW_THREADS) k_gradh_warp(
       }
     }
     if (overflow || !__any_sync(FULL, st == GH_PASS)) break;
-    // density pass over the lane's candidates (:199-235)
-    const bool on = st == GH_PASS;
-    const double ih = on ? 1.0 / s.hp : 0.0;
-    const double hf = on ? pow(ih, NDIMPR) : 0.0;
-    const double hs = (KERNRANGESQD * s.hp) * s.hp;
-    double rt = (mp * t0.x) * hf;
-    for (int e = 0; e < nent; ++e) {
-      const int code = s_leaf[w][e];
-      const bool mine = on && ((s_mask[w][e] >> lane) & 1u);
-      const int q0 = code >> 3, n = (code & 7) + 1;
-      ncand += n;
-      // the leaf's particles are contiguous: issue four loads before using them
-      for (int k0 = 0; k0 < n; k0 += 4) {
-        double4 Q[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) Q[k] = pm[q0 + min(k0 + k, n - 1)];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          const int q = q0 + k0 + k;
-          if (k0 + k < n && mine && q != p) gh_density_term(Q[k], rx, ry, rz, hs, ih, hf, tabA, rt);
+    // density pass over the lane's own candidates (:199-235)
+    if (st == GH_PASS) {
+      const double ih = 1.0 / s.hp;
+      const double hf = pow(ih, NDIMPR);
+      const double hs = (KERNRANGESQD * s.hp) * s.hp;
+      double rt = (mp * t0.x) * hf;
+      for (int k = 0; k < nown; ++k) {
+        const int code = s_own[w][k][lane];
+        const int q0 = code >> 3, n = (code & 7) + 1;
+        ncand += n;
+        for (int j = 0; j < n; ++j) {
+          const int q = q0 + j;
+          if (q != p) gh_density_term(pm[q], rx, ry, rz, hs, ih, hf, tabA, rt);
         }
       }
+      st = gh_after_pass(s, mp, h_fac, rextent, rt) ? GH_DONE : GH_WALK;
     }
     ++npass;
-    if (on) st = gh_after_pass(s, mp, h_fac, rextent, rt) ? GH_DONE : GH_WALK;
   }
   if (overflow) {
     if (live) gradh_one(p, pm, hz, vel, rho, omega, divv, drhodt, t, tabA, h_fac, pp_gather,
                         rextent, err);
-    return;
-  }
-  // final pass over the same candidate list (:317-425)
-  const bool on = st == GH_DONE;
-  const double hp = on ? h_fac * pow(mp / s.rho, ONETHIRD) : 1.0;
-  const double ih = 1.0 / hp;
-  const double hf = on ? pow(ih, NDIMPR) : 0.0;
-  const double hs = (KERNRANGESQD * hp) * hp;
-  const double4 vp = vel[p];
-  GhFinal f;
-  gh_final_init(f, mp, ih, hf, t0);
-  for (int e = 0; e < nent; ++e) {
-    const int code = s_leaf[w][e];
-    const bool mine = on && ((s_mask[w][e] >> lane) & 1u);
-    const int q0 = code >> 3, n = (code & 7) + 1;
-    ncand += n;
-    for (int k0 = 0; k0 < n; k0 += 2) {
-      double4 Q[2], V[2];
-#pragma unroll
-      for (int k = 0; k < 2; ++k) {
-        Q[k] = pm[q0 + min(k0 + k, n - 1)];
-        V[k] = vel[q0 + min(k0 + k, n - 1)];
-      }
-#pragma unroll
-      for (int k = 0; k < 2; ++k) {
-        const int q = q0 + k0 + k;
-        if (k0 + k < n && mine && q != p) gh_final_term(Q[k], V[k], rx, ry, rz, vp, hs, ih, hf, tabA, f);
+  } else if (st == GH_DONE) {
+    // final pass over the same candidate list (:317-425)
+    const double hp = h_fac * pow(mp / s.rho, ONETHIRD);
+    const double ih = 1.0 / hp;
+    const double hf = pow(ih, NDIMPR);
+    const double hs = (KERNRANGESQD * hp) * hp;
+    const double4 vp = vel[p];
+    GhFinal f;
+    gh_final_init(f, mp, ih, hf, t0);
+    for (int k = 0; k < nown; ++k) {
+      const int code = s_own[w][k][lane];
+      const int q0 = code >> 3, n = (code & 7) + 1;
+      ncand += n;
+      for (int j = 0; j < n; ++j) {
+        const int q = q0 + j;
+        if (q != p) gh_final_term(pm[q], vel[q], rx, ry, rz, vp, hs, ih, hf, tabA, f);
       }
     }
+    gh_store(p, mp, hp, f, hz, rho, omega, divv, drhodt, err);
   }
   ++npass;
-  if (on) gh_store(p, mp, hp, f, hz, rho, omega, divv, drhodt, err);
+  // warp totals of the per-lane candidate counts
+  for (int o = 16; o > 0; o >>= 1) ncand += __shfl_down_sync(FULL, ncand, o);
   if (lane == 0) {
     atomicAdd(counts + 3, nwalk);
     atomicAdd(counts + 4, nvisit);
@@ -469,40 +504,54 @@ __global__ void __launch_bounds__(SW_THREADS) k_neib_warp(
     int* __restrict__ pplist, DevError* err, unsigned long long* counts) {
   __shared__ int s_leaf[SW_WARPS][SW_CAP];
   __shared__ unsigned s_mask[SW_WARPS][SW_CAP];
+  __shared__ int s_own[SW_WARPS][OWN_CAP][32];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int i = blockIdx.x * SW_THREADS + threadIdx.x;
   const bool live = i < nact;
   if (__ballot_sync(FULL, live) == 0) return;
   const int p = live ? (act ? act[i] : i) : (act ? act[nact - 1] : nact - 1);
   const double4 P = pm[p];
+  const float px = (float)(P.x - t.rootx), py = (float)(P.y - t.rooty), pz = (float)(P.z - t.rootz);
   const double hp = hz[p].x;
   const double R = KERNRANGE * hp;
+  const float R32 = (float)R;
   const double hsp = (KERNRANGESQD * hp) * hp;
   int cnt = 0;
   unsigned long long nvisit = 0;
   const int nent = warp_walk(t, live, lane, s_leaf[w], s_mask[w], cnt, nvisit, err, KID_NEIB, p,
-                             [&](const double4& h, int c) {
-                               const double d0 = h.x - P.x, d1 = h.y - P.y, d2 = h.z - P.z;
-                               const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
+                             [&](int c) {                   // BHhydro_walk.F90:37-43
+                               const float4 h32 = t.hA32[c];
+                               const float d0 = h32.x - px, d1 = h32.y - py, d2 = h32.z - pz;
+                               const float d2s = (d0 * d0 + d1 * d1) + d2 * d2;
+                               const int r1 = test32(d2s, R32 + h32.w, t.delta);
+                               const int r2 = test32(d2s, t.hrm32[c] + h32.w, t.delta);
+                               if (r1 == 1 || r2 == 1) return true;
+                               if (r1 == 0 && r2 == 0) return false;
+                               const double4 h = t.hA[c];
+                               const double e0 = h.x - P.x, e1 = h.y - P.y, e2 = h.z - P.z;
+                               const double drsqd = (e0 * e0 + e1 * e1) + e2 * e2;
                                const double t1 = R + h.w;
                                const double t2 = t.hrm[c] + h.w;
                                return drsqd <= t1 * t1 || drsqd <= t2 * t2;
                              });
-  if (nent < 0) {
+  const int nown = nent < 0 ? 0 : own_list(nent, lane, s_leaf[w], s_mask[w], s_own[w]);
+  if (nent < 0 || __any_sync(FULL, nown > OWN_CAP)) {
     if (live) neib_one(p, pm, hz, t, L, pptot, pplist, err);
     return;
   }
   int* row = pplist + (size_t)p * L;
+  unsigned long long ncand = 0;
   cnt = 0;
-  for (int e = 0; e < nent; ++e) {
-    const int code = s_leaf[w][e];
-    const bool mine = live && ((s_mask[w][e] >> lane) & 1u);
-    const int q0 = code >> 3, n = (code & 7) + 1;
-    for (int k = 0; k < n; ++k) {
-      const int q = q0 + k;
-      const double4 Q = pm[q];
-      const double hq = hz[q].x;
-      if (mine && q != p) {
+  if (live) {
+    for (int k = 0; k < nown; ++k) {
+      const int code = s_own[w][k][lane];
+      const int q0 = code >> 3, n = (code & 7) + 1;
+      ncand += n;
+      for (int j = 0; j < n; ++j) {
+        const int q = q0 + j;
+        if (q == p) continue;
+        const double4 Q = pm[q];
+        const double hq = hz[q].x;
         const double hsq = (KERNRANGESQD * hq) * hq;
         const double d0 = Q.x - P.x, d1 = Q.y - P.y, d2 = Q.z - P.z;
         const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
@@ -512,13 +561,10 @@ __global__ void __launch_bounds__(SW_THREADS) k_neib_warp(
         }
       }
     }
+    pptot[p] = cnt;
   }
-  if (live) pptot[p] = cnt;
-  if (lane == 0) {
-    unsigned long long ncand = 0;
-    for (int e = 0; e < nent; ++e) ncand += (s_leaf[w][e] & 7) + 1;
-    atomicAdd(counts + 7, ncand);
-  }
+  for (int o = 16; o > 0; o >>= 1) ncand += __shfl_down_sync(FULL, ncand, o);
+  if (lane == 0) atomicAdd(counts + 7, ncand);
 }
 
 // sph/hydro_gradh.F90:9-339 (NEIGHBOUR_LISTS, ARTIFICIAL_VISCOSITY=MON97).
@@ -699,7 +745,11 @@ __global__ void k_thermal(int n, const double* __restrict__ csq, const double* _
 
 inline int nb(long n, int t) { return (int)((n + t - 1) / t); }
 
-HydroTree hydro_tree(const Ctx& c) { return HydroTree{c.link, c.hA, c.hrm, c.info.ctot}; }
+HydroTree hydro_tree(const Ctx& c) {
+  const double delta = ldexp(1.0, -22) * (c.info.cellsize > 0.0 ? c.info.cellsize : 1.0);
+  return HydroTree{c.link, c.hA, c.hrm, c.hA32, c.hrm32, c.info.ctot, c.info.root[0],
+                   c.info.root[1], c.info.root[2], (float)delta};
+}
 
 }  // namespace
 

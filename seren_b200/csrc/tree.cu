@@ -414,7 +414,8 @@ __global__ void k_stock_level(int cfirst, int clast, const int4* __restrict__ li
                               double4* __restrict__ hA, double* __restrict__ hmaxa,
                               double4* __restrict__ bbmina, double4* __restrict__ bbmaxa,
                               double rootx, double rooty, double rootz, double delta,
-                              float4* __restrict__ wA, float* __restrict__ wLo) {
+                              float4* __restrict__ wA, float* __restrict__ wLo,
+                              float4* __restrict__ hA32) {
   const int c = cfirst + blockIdx.x * blockDim.x + threadIdx.x;
   if (c > clast) return;
   const int4 lk = link[c];
@@ -514,8 +515,9 @@ __global__ void k_stock_level(int cfirst, int clast, const int4* __restrict__ li
   bbmina[c] = make_double4(bbmin[0], bbmin[1], bbmin[2], 0.0);
   bbmaxa[c] = make_double4(bbmax[0], bbmax[1], bbmax[2], 0.0);
   // BHhydro_stock.F90:69-150: bounding-box centre and half diagonal
+  double4 hn;
   if (lk.x == 1) {
-    hA[c] = make_double4(rc[0], rc[1], rc[2], 0.0);
+    hn = make_double4(rc[0], rc[1], rc[2], 0.0);
   } else {
     double hc[3], diag = 0.0;
     for (int k = 0; k < 3; ++k) {
@@ -523,13 +525,17 @@ __global__ void k_stock_level(int cfirst, int clast, const int4* __restrict__ li
       const double hb = bbmax[k] - hc[k];
       diag = diag + hb * hb;
     }
-    hA[c] = make_double4(hc[0], hc[1], hc[2], sqrt(diag));
+    hn = make_double4(hc[0], hc[1], hc[2], sqrt(diag));
   }
+  hA[c] = hn;
+  hA32[c] = make_float4((float)(hn.x - rootx), (float)(hn.y - rooty), (float)(hn.z - rootz),
+                        __double2float_ru(hn.w));
 }
 
 // BHhydro_update_hmax.F90:29-88
 __global__ void k_hmax_level(int cfirst, int clast, const int4* __restrict__ link,
-                             const double2* __restrict__ hz, double* __restrict__ hrm) {
+                             const double2* __restrict__ hz, double* __restrict__ hrm,
+                             float* __restrict__ hrm32) {
   const int c = cfirst + blockIdx.x * blockDim.x + threadIdx.x;
   if (c > clast) return;
   const int4 lk = link[c];
@@ -548,6 +554,7 @@ __global__ void k_hmax_level(int cfirst, int clast, const int4* __restrict__ lin
     }
   }
   hrm[c] = hr;
+  hrm32[c] = __double2float_ru(hr);
 }
 
 // BHhydro_hguess.F90:106-155 (GRAD_H_SPH number criterion): the h of a
@@ -701,7 +708,7 @@ void launch_stock(Ctx& c) {
     k_stock_level<<<nb(cnt, 128), 128, 0, c.st>>>(f, la, c.link, c.pm, c.hz, c.prm.thetamaxsqd, daux,
                                                  c.gA, c.gB, c.gC, c.hA, c.hmax, c.bbmin, c.bbmax,
                                                  c.info.root[0], c.info.root[1], c.info.root[2],
-                                                 delta, c.wA, c.wLo); ++c.nlaunch;
+                                                 delta, c.wA, c.wLo, c.hA32); ++c.nlaunch;
   }
 }
 
@@ -710,7 +717,7 @@ void launch_update_hmax(Ctx& c) {
     const int f = c.info.first_cell[l], la = c.info.last_cell[l];
     const int cnt = la - f + 1;
     if (cnt <= 0) continue;
-    k_hmax_level<<<nb(cnt, 128), 128, 0, c.st>>>(f, la, c.link, c.hz, c.hrm); ++c.nlaunch;
+    k_hmax_level<<<nb(cnt, 128), 128, 0, c.st>>>(f, la, c.link, c.hz, c.hrm, c.hrm32); ++c.nlaunch;
   }
 }
 
