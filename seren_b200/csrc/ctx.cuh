@@ -79,6 +79,7 @@ struct Ctx {
   int* pcount = nullptr;
   int* parent = nullptr;
   int* level = nullptr;
+  int* nkids = nullptr;       // number of children (0 for leaves); they are ifopen..ifopen+n-1
   int4* link = nullptr;       // {leaf, nextcell, ifopen, pstart}, packed for walks
   double4* gA = nullptr;      // gravity: COM x, y, z, m
   double4* gB = nullptr;      // gravity: q1..q4 (xx, xy, yy, zx)
@@ -96,6 +97,7 @@ struct Ctx {
   TreeInfo info{};            // host mirror after a build
   DevError* d_err = nullptr;
   int* d_counts = nullptr;    // [16] int64 interaction counters (as 2 ints each)
+  int* work = nullptr;        // work counter of the persistent kernels
 
   // kernel tables
   double4* tabA = nullptr;

@@ -19,6 +19,7 @@ struct HydroTree {
   const double* hrm;    // hrangemax
   const float4* hA32;   // FP32 centre - root centre, rmax rounded up
   const float* hrm32;   // hrangemax rounded up
+  const int* nkids;     // children per cell (ids ifopen .. ifopen + nkids - 1)
   int ctot;
   double rootx, rooty, rootz;
   float delta;          // bound on the FP32 rounding of a root-relative coordinate
@@ -256,26 +257,33 @@ __device__ void gradh_one(int p, const double4* __restrict__ pm, double2* __rest
 }
 
 // ---------------------------------------------------------------------------
-// Warp-cooperative candidate walks.  The warp walks the hydro tree once for
-// its 32 particles, each lane with its own search test; the walk position is
-// warp-uniform and a lane that fails a branch cell's test skips that subtree
-// (its skip marker is the cell's nextcell), so a lane's bits select exactly the
-// leaves its own walk would open, in the same depth-first order.  Opened
-// leaves are stored once per warp as (pstart, count) with the lane mask; each
-// lane then copies the leaves of its own bits into its own list, so every
-// pass over candidates runs over that particle's own candidates only, in the
-// reference's list order.
+// Warp-per-particle search.  A warp takes one particle at a time: the walk of
+// the reference (BHhydrowalk_hgather / BHhydro_walk) runs breadth-first with
+// the lanes spread over the cells of each level, and the particle's candidates
+// are then processed 32 at a time (coalesced loads) with the per-lane partial
+// sums reduced at the end.  The set of opened leaves is exactly the
+// reference's (a leaf is reached only through cells that passed the test);
+// only the order of the floating-point sums differs.  Warps take chunks of
+// particles from a global counter.
 //
 // Cell tests run first in FP32 on coordinates relative to the root centre:
 // test32() decides when the FP32 distance is outside a margin around the
 // threshold that covers every FP32 rounding involved (coordinates within
 // delta, the difference, the squares, the sum and the threshold itself), and
 // the test is redone in FP64 exactly as the reference writes it otherwise.
-constexpr int SW_THREADS = 128;
-constexpr int SW_WARPS = SW_THREADS / 32;
-constexpr int SW_CAP = 256;      // union leaves per warp
-constexpr int OWN_CAP = 64;      // leaves per lane
+constexpr int WP_THREADS = 128;
+constexpr int WP_WARPS = WP_THREADS / 32;
+constexpr int WP_FCAP = 512;     // cells of one level of the walk
+constexpr int WP_LCAP = 256;     // opened leaves (a power of two: the sort pads to it)
+constexpr int WP_CCAP = 1024;    // candidate particles
+constexpr int WP_CHUNK = 8;      // particles per grab from the work counter
 constexpr unsigned FULL = 0xffffffffu;
+
+struct WpShared {
+  int front[2][WP_FCAP];
+  int leaves[WP_LCAP];
+  int cand[WP_CCAP];
+};
 
 // 1: d2 <= T^2 for sure, 0: d2 > T^2 for sure, -1: too close to tell in FP32
 __device__ __forceinline__ int test32(float d2, float T, float delta) {
@@ -286,189 +294,232 @@ __device__ __forceinline__ int test32(float d2, float T, float delta) {
   return -1;
 }
 
-// test(c) -> bool is the lane's cell test; returns the entry count, or -1
-// when the list overflowed.  cnt accumulates the lane's candidate count.
+__device__ __forceinline__ int warp_iscan(int v, int lane) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(FULL, v, o);
+    if (lane >= o) v += y;
+  }
+  return v;
+}
+
+// sum over the warp, the same value on every lane (lane 0's reduction)
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(FULL, v, o);
+  return __shfl_sync(FULL, v, 0);
+}
+
+// Breadth-first walk of one particle's search; returns the number of opened
+// leaves (codes pstart*8 + count-1 in s.leaves) or -1 when a buffer overflows;
+// cnt = the particles in the opened leaves.
 template <class Test>
-__device__ __forceinline__ int warp_walk(const HydroTree& t, bool part, int lane,
-                                         int* __restrict__ s_leaf, unsigned* __restrict__ s_mask,
-                                         int& cnt, unsigned long long& nvisit, DevError* err,
-                                         int kid, int who, Test&& test) {
+__device__ int wp_walk(const HydroTree& t, int lane, WpShared& s, int& cnt,
+                       unsigned long long& nvisit, Test&& test) {
+  int* fa = s.front[0];
+  int* fb = s.front[1];
   __syncwarp();
-  int c = 0, n = 0, visits = 0;
-  int skip = part ? -1 : -2;
-  cnt = 0;
-  while (true) {
-    ++nvisit;
-    if (++visits > t.ctot + 2) {
-      if (lane == 0) set_error(err, SEREN_GPU_ERR_WALK, kid, who, c);
-      return -1;
-    }
-    const int4 lk = t.link[c];
-    if (skip == c) skip = -1;
-    bool pass = false;
-    if (skip == -1) pass = test(c);
-    const unsigned m = __ballot_sync(FULL, pass);
-    if (lk.x > 0) {
-      if (m) {
-        if (n == SW_CAP) return -1;
-        if (lane == 0) { s_leaf[n] = lk.w * 8 + (lk.x - 1); s_mask[n] = m; }
-        ++n;
-        if (pass) cnt += lk.x;
+  if (lane == 0) fa[0] = 0;
+  __syncwarp();
+  int nf = 1, nleaf = 0, mine = 0;
+  bool over = false;
+  while (nf > 0) {
+    int nnext = 0;
+    for (int base = 0; base < nf; base += 32) {
+      const int idx = base + lane;
+      const bool valid = idx < nf;
+      const int c = valid ? fa[idx] : 0;
+      const bool pass = valid && test(c);
+      const int4 lk = t.link[c];
+      const bool isleaf = pass && lk.x > 0;
+      const bool isbr = pass && lk.x == 0;
+      const unsigned ml = __ballot_sync(FULL, isleaf);
+      if (isleaf) {
+        const int pos = nleaf + __popc(ml & ((1u << lane) - 1u));
+        if (pos < WP_LCAP) s.leaves[pos] = lk.w * 8 + (lk.x - 1);
+        mine += lk.x;
       }
-      c = lk.y;
-    } else if (lk.x == 0 && m) {
-      if (skip == -1 && !pass) skip = lk.y;
-      c = lk.z;
-    } else {
-      c = lk.y;
+      nleaf += __popc(ml);
+      const int nk = isbr ? t.nkids[c] : 0;
+      const int sc = warp_iscan(nk, lane);
+      if (isbr) {
+        const int o = nnext + sc - nk;
+        for (int j = 0; j < nk; ++j)
+          if (o + j < WP_FCAP) fb[o + j] = lk.z + j;
+      }
+      nnext += __shfl_sync(FULL, sc, 31);
     }
-    if (c > t.ctot) break;
+    nvisit += nf;
+    __syncwarp();
+    if (nnext > WP_FCAP) over = true;
+    int* tmp = fa;
+    fa = fb;
+    fb = tmp;
+    nf = over ? 0 : nnext;
   }
-  __syncwarp();
-  return n;
+  cnt = warp_iscan(mine, lane);
+  cnt = __shfl_sync(FULL, cnt, 31);
+  return (over || nleaf > WP_LCAP) ? -1 : nleaf;
 }
 
-// copy the union entries of this lane's bits into the lane's own list;
-// returns the lane's entry count (may exceed OWN_CAP: overflow)
-__device__ __forceinline__ int own_list(int nent, int lane, const int* __restrict__ s_leaf,
-                                        const unsigned* __restrict__ s_mask,
-                                        int (*__restrict__ own)[32]) {
-  int nown = 0;
-  for (int e = 0; e < nent; ++e) {
-    if ((s_mask[e] >> lane) & 1u) {
-      if (nown < OWN_CAP) own[nown][lane] = s_leaf[e];
-      ++nown;
-    }
+// leaves -> candidate particle ids, in leaf order; returns the count (may
+// exceed WP_CCAP: overflow)
+__device__ int wp_flatten(int nleaf, int lane, WpShared& s) {
+  int total = 0;
+  for (int base = 0; base < nleaf; base += 32) {
+    const int k = base + lane;
+    const int code = k < nleaf ? s.leaves[k] : 0;
+    const int n = k < nleaf ? (code & 7) + 1 : 0;
+    const int sc = warp_iscan(n, lane);
+    const int o = total + sc - n;
+    for (int j = 0; j < n; ++j)
+      if (o + j < WP_CCAP) s.cand[o + j] = (code >> 3) + j;
+    total += __shfl_sync(FULL, sc, 31);
   }
   __syncwarp();
-  return nown;
+  return total;
 }
 
-enum : int { GH_WALK = 0, GH_PASS = 1, GH_DONE = 2, GH_OFF = 3 };
+// ascending bitonic sort of s.leaves[0..n) (n <= WP_LCAP): depth-first leaf
+// order, which is the order of the reference's candidate lists
+__device__ void wp_sort_leaves(int n, int lane, WpShared& s) {
+  int N = 1;
+  while (N < n) N <<= 1;
+  for (int k = n + lane; k < N; k += 32) s.leaves[k] = 0x7fffffff;
+  __syncwarp();
+  for (int size = 2; size <= N; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int i = lane; i < (N >> 1); i += 32) {
+        const int lo = 2 * i - (i & (stride - 1));
+        const int hi = lo + stride;
+        const bool up = (lo & size) == 0;
+        const int x = s.leaves[lo], y = s.leaves[hi];
+        if ((x > y) == up) {
+          s.leaves[lo] = y;
+          s.leaves[hi] = x;
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
 
-__global__ void __launch_bounds__(SW_THREADS) k_gradh_warp(
+__device__ __forceinline__ int grab(int* work, int lane) {
+  int b = 0;
+  if (lane == 0) b = atomicAdd(work, WP_CHUNK);
+  return __shfl_sync(FULL, b, 0);
+}
+
+// sph/all_sph_gradh.F90:11-492, one warp per particle
+__global__ void __launch_bounds__(WP_THREADS) k_gradh_wp(
     int nact, const int* __restrict__ act, const double4* __restrict__ pm, double2* __restrict__ hz,
     const double4* __restrict__ vel, double* __restrict__ rho, double* __restrict__ omega,
     double* __restrict__ divv, double* __restrict__ drhodt, HydroTree t,
     const double4* __restrict__ tabA, double h_fac, int pp_gather, double rextent, DevError* err,
-    unsigned long long* counts) {
-  __shared__ int s_leaf[SW_WARPS][SW_CAP];
-  __shared__ unsigned s_mask[SW_WARPS][SW_CAP];
-  __shared__ int s_own[SW_WARPS][OWN_CAP][32];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int i = blockIdx.x * SW_THREADS + threadIdx.x;
-  const bool live = i < nact;
-  if (__ballot_sync(FULL, live) == 0) return;
-  const int p = live ? (act ? act[i] : i) : (act ? act[nact - 1] : nact - 1);
-  const double4 P = pm[p];
-  const double rx = P.x, ry = P.y, rz = P.z, mp = P.w;
-  const float px = (float)(rx - t.rootx), py = (float)(ry - t.rooty), pz = (float)(rz - t.rootz);
+    unsigned long long* counts, int* work) {
+  __shared__ WpShared sh[WP_WARPS];
+  const int lane = threadIdx.x & 31;
+  WpShared& S = sh[threadIdx.x >> 5];
   const double4 t0 = tabA[0];
-  // warp-level work counters (walks, nodes visited, passes, candidates)
-  unsigned long long nwalk = 0, nvisit = 0, npass = 0, ncand = 0;
-  GhState s;
-  gh_init(s, hz[p].x, rextent);
-  int st = live ? GH_WALK : GH_OFF;
-  double R = -1.0;                 // search radius of the lane's current list
-  float R32 = -1.0f;
-  int nown = 0;
-  bool overflow = false;
-  auto gather_test = [&](int c) {                      // BHhydrowalk_hgather.F90:36-40
-    const float4 h32 = t.hA32[c];
-    const float d0 = h32.x - px, d1 = h32.y - py, d2 = h32.z - pz;
-    const int r = test32((d0 * d0 + d1 * d1) + d2 * d2, R32 + h32.w, t.delta);
-    if (r >= 0) return r == 1;
-    const double4 h = t.hA[c];
-    const double e0 = h.x - rx, e1 = h.y - ry, e2 = h.z - rz;
-    const double tt = R + h.w;
-    return ((e0 * e0 + e1 * e1) + e2 * e2) <= tt * tt;
-  };
-  while (!overflow) {
-    while (__any_sync(FULL, st == GH_WALK)) {                          // :154-191
-      bool want = false;
-      if (st == GH_WALK && s.hp > s.h_high) {
-        s.h_high = s.hp * HMULT;
-        R = KERNRANGE * s.h_high;
-        R32 = (float)R;
-        want = true;
-      }
-      if (__any_sync(FULL, want)) {
-        int cnt = 0;
-        ++nwalk;
-        const int nent = warp_walk(t, R >= 0.0, lane, s_leaf[w], s_mask[w], cnt, nvisit, err,
-                                   KID_GRADH, p, gather_test);
-        if (nent < 0) { overflow = true; break; }
-        nown = own_list(nent, lane, s_leaf[w], s_mask[w], s_own[w]);
-        if (__any_sync(FULL, nown > OWN_CAP)) { overflow = true; break; }
-        if (want) s.pp_pot = cnt;
-      }
-      if (st == GH_WALK) {
-        if (s.pp_pot < pp_gather) {
-          s.h_high = 0.0;
-          s.pp_pot = 0;
-          s.hp = s.hp * HMULT;
-          if (++s.ngrow > HGROW_CAP) {
-            set_error(err, SEREN_GPU_ERR_WALK, KID_GRADH, p, -1);
-            st = GH_OFF;
-            R = -1.0;
-            R32 = -1.0f;
+  unsigned long long nwalk = 0, nvisit = 0, npass = 0, ncands = 0;
+  for (int base = grab(work, lane); base < nact; base = grab(work, lane)) {
+    const int end = min(base + WP_CHUNK, nact);
+    for (int i = base; i < end; ++i) {
+      const int p = act ? act[i] : i;
+      const double4 P = pm[p];
+      const double rx = P.x, ry = P.y, rz = P.z, mp = P.w;
+      const float px = (float)(rx - t.rootx), py = (float)(ry - t.rooty),
+                  pz = (float)(rz - t.rootz);
+      GhState s;
+      gh_init(s, hz[p].x, rextent);
+      double R = 0.0;
+      float R32 = 0.0f;
+      auto gather_test = [&](int c) {                 // BHhydrowalk_hgather.F90:36-40
+        const float4 h32 = t.hA32[c];
+        const float d0 = h32.x - px, d1 = h32.y - py, d2 = h32.z - pz;
+        const int r = test32((d0 * d0 + d1 * d1) + d2 * d2, R32 + h32.w, t.delta);
+        if (r >= 0) return r == 1;
+        const double4 h = t.hA[c];
+        const double e0 = h.x - rx, e1 = h.y - ry, e2 = h.z - rz;
+        const double tt = R + h.w;
+        return ((e0 * e0 + e1 * e1) + e2 * e2) <= tt * tt;
+      };
+      int ncand = 0;
+      bool over = false, bad = false;
+      while (true) {
+        while (true) {                                                 // :154-191
+          if (s.hp > s.h_high) {
+            s.h_high = s.hp * HMULT;
+            R = KERNRANGE * s.h_high;
+            R32 = (float)R;
+            int cnt = 0;
+            ++nwalk;
+            const int nl = wp_walk(t, lane, S, cnt, nvisit, gather_test);
+            if (nl < 0) { over = true; break; }
+            ncand = wp_flatten(nl, lane, S);
+            if (ncand > WP_CCAP) { over = true; break; }
+            s.pp_pot = cnt;
           }
-        } else {
-          st = GH_PASS;
+          if (s.pp_pot < pp_gather) {
+            s.h_high = 0.0;
+            s.pp_pot = 0;
+            s.hp = s.hp * HMULT;
+            if (++s.ngrow > HGROW_CAP) { bad = true; break; }
+          }
+          if (s.pp_pot > 0) break;
         }
+        if (over || bad) break;
+        const double ih = 1.0 / s.hp;                                  // :199-235
+        const double hf = pow(ih, NDIMPR);
+        const double hs = (KERNRANGESQD * s.hp) * s.hp;
+        double part = 0.0;
+        for (int k = lane; k < ncand; k += 32) {
+          const int q = S.cand[k];
+          if (q != p) gh_density_term(pm[q], rx, ry, rz, hs, ih, hf, tabA, part);
+        }
+        const double rt = (mp * t0.x) * hf + warp_sum(part);
+        ++npass;
+        ncands += ncand;
+        if (gh_after_pass(s, mp, h_fac, rextent, rt)) break;
       }
-    }
-    if (overflow || !__any_sync(FULL, st == GH_PASS)) break;
-    // density pass over the lane's own candidates (:199-235)
-    if (st == GH_PASS) {
-      const double ih = 1.0 / s.hp;
+      if (bad) {
+        if (lane == 0) set_error(err, SEREN_GPU_ERR_WALK, KID_GRADH, p, -1);
+        continue;
+      }
+      if (over) {
+        if (lane == 0)
+          gradh_one(p, pm, hz, vel, rho, omega, divv, drhodt, t, tabA, h_fac, pp_gather, rextent,
+                    err);
+        __syncwarp();
+        continue;
+      }
+      const double hp = h_fac * pow(mp / s.rho, ONETHIRD);            // :317-425
+      const double ih = 1.0 / hp;
       const double hf = pow(ih, NDIMPR);
-      const double hs = (KERNRANGESQD * s.hp) * s.hp;
-      double rt = (mp * t0.x) * hf;
-      for (int k = 0; k < nown; ++k) {
-        const int code = s_own[w][k][lane];
-        const int q0 = code >> 3, n = (code & 7) + 1;
-        ncand += n;
-        for (int j = 0; j < n; ++j) {
-          const int q = q0 + j;
-          if (q != p) gh_density_term(pm[q], rx, ry, rz, hs, ih, hf, tabA, rt);
-        }
-      }
-      st = gh_after_pass(s, mp, h_fac, rextent, rt) ? GH_DONE : GH_WALK;
-    }
-    ++npass;
-  }
-  if (overflow) {
-    if (live) gradh_one(p, pm, hz, vel, rho, omega, divv, drhodt, t, tabA, h_fac, pp_gather,
-                        rextent, err);
-  } else if (st == GH_DONE) {
-    // final pass over the same candidate list (:317-425)
-    const double hp = h_fac * pow(mp / s.rho, ONETHIRD);
-    const double ih = 1.0 / hp;
-    const double hf = pow(ih, NDIMPR);
-    const double hs = (KERNRANGESQD * hp) * hp;
-    const double4 vp = vel[p];
-    GhFinal f;
-    gh_final_init(f, mp, ih, hf, t0);
-    for (int k = 0; k < nown; ++k) {
-      const int code = s_own[w][k][lane];
-      const int q0 = code >> 3, n = (code & 7) + 1;
-      ncand += n;
-      for (int j = 0; j < n; ++j) {
-        const int q = q0 + j;
+      const double hs = (KERNRANGESQD * hp) * hp;
+      const double4 vp = vel[p];
+      GhFinal f;
+      f.rt = 0.0; f.om = 0.0; f.dv = 0.0; f.zt = 0.0;
+      for (int k = lane; k < ncand; k += 32) {
+        const int q = S.cand[k];
         if (q != p) gh_final_term(pm[q], vel[q], rx, ry, rz, vp, hs, ih, hf, tabA, f);
       }
+      GhFinal g;
+      gh_final_init(g, mp, ih, hf, t0);
+      g.rt = g.rt + warp_sum(f.rt);
+      g.om = g.om + warp_sum(f.om);
+      g.dv = g.dv + warp_sum(f.dv);
+      g.zt = g.zt + warp_sum(f.zt);
+      ++npass;
+      ncands += ncand;
+      if (lane == 0) gh_store(p, mp, hp, g, hz, rho, omega, divv, drhodt, err);
     }
-    gh_store(p, mp, hp, f, hz, rho, omega, divv, drhodt, err);
   }
-  ++npass;
-  // warp totals of the per-lane candidate counts
-  for (int o = 16; o > 0; o >>= 1) ncand += __shfl_down_sync(FULL, ncand, o);
   if (lane == 0) {
     atomicAdd(counts + 3, nwalk);
     atomicAdd(counts + 4, nvisit);
     atomicAdd(counts + 5, npass);
-    atomicAdd(counts + 6, ncand);
+    atomicAdd(counts + 6, ncands);
   }
 }
 
@@ -498,73 +549,78 @@ __device__ void neib_one(int p, const double4* __restrict__ pm, const double2* _
   pptot[p] = cnt;
 }
 
-__global__ void __launch_bounds__(SW_THREADS) k_neib_warp(
+__global__ void __launch_bounds__(WP_THREADS) k_neib_wp(
     int nact, const int* __restrict__ act, const double4* __restrict__ pm,
     const double2* __restrict__ hz, HydroTree t, int L, int* __restrict__ pptot,
-    int* __restrict__ pplist, DevError* err, unsigned long long* counts) {
-  __shared__ int s_leaf[SW_WARPS][SW_CAP];
-  __shared__ unsigned s_mask[SW_WARPS][SW_CAP];
-  __shared__ int s_own[SW_WARPS][OWN_CAP][32];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int i = blockIdx.x * SW_THREADS + threadIdx.x;
-  const bool live = i < nact;
-  if (__ballot_sync(FULL, live) == 0) return;
-  const int p = live ? (act ? act[i] : i) : (act ? act[nact - 1] : nact - 1);
-  const double4 P = pm[p];
-  const float px = (float)(P.x - t.rootx), py = (float)(P.y - t.rooty), pz = (float)(P.z - t.rootz);
-  const double hp = hz[p].x;
-  const double R = KERNRANGE * hp;
-  const float R32 = (float)R;
-  const double hsp = (KERNRANGESQD * hp) * hp;
-  int cnt = 0;
-  unsigned long long nvisit = 0;
-  const int nent = warp_walk(t, live, lane, s_leaf[w], s_mask[w], cnt, nvisit, err, KID_NEIB, p,
-                             [&](int c) {                   // BHhydro_walk.F90:37-43
-                               const float4 h32 = t.hA32[c];
-                               const float d0 = h32.x - px, d1 = h32.y - py, d2 = h32.z - pz;
-                               const float d2s = (d0 * d0 + d1 * d1) + d2 * d2;
-                               const int r1 = test32(d2s, R32 + h32.w, t.delta);
-                               const int r2 = test32(d2s, t.hrm32[c] + h32.w, t.delta);
-                               if (r1 == 1 || r2 == 1) return true;
-                               if (r1 == 0 && r2 == 0) return false;
-                               const double4 h = t.hA[c];
-                               const double e0 = h.x - P.x, e1 = h.y - P.y, e2 = h.z - P.z;
-                               const double drsqd = (e0 * e0 + e1 * e1) + e2 * e2;
-                               const double t1 = R + h.w;
-                               const double t2 = t.hrm[c] + h.w;
-                               return drsqd <= t1 * t1 || drsqd <= t2 * t2;
-                             });
-  const int nown = nent < 0 ? 0 : own_list(nent, lane, s_leaf[w], s_mask[w], s_own[w]);
-  if (nent < 0 || __any_sync(FULL, nown > OWN_CAP)) {
-    if (live) neib_one(p, pm, hz, t, L, pptot, pplist, err);
-    return;
-  }
-  int* row = pplist + (size_t)p * L;
-  unsigned long long ncand = 0;
-  cnt = 0;
-  if (live) {
-    for (int k = 0; k < nown; ++k) {
-      const int code = s_own[w][k][lane];
-      const int q0 = code >> 3, n = (code & 7) + 1;
-      ncand += n;
-      for (int j = 0; j < n; ++j) {
-        const int q = q0 + j;
-        if (q == p) continue;
-        const double4 Q = pm[q];
-        const double hq = hz[q].x;
-        const double hsq = (KERNRANGESQD * hq) * hq;
-        const double d0 = Q.x - P.x, d1 = Q.y - P.y, d2 = Q.z - P.z;
-        const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
-        if (drsqd <= hsp || drsqd <= hsq) {
-          if (cnt < L) row[cnt] = q;
-          ++cnt;
-        }
+    int* __restrict__ pplist, DevError* err, unsigned long long* counts, int* work) {
+  __shared__ WpShared sh[WP_WARPS];
+  const int lane = threadIdx.x & 31;
+  WpShared& S = sh[threadIdx.x >> 5];
+  unsigned long long nvisit = 0, ncands = 0;
+  for (int base = grab(work, lane); base < nact; base = grab(work, lane)) {
+    const int end = min(base + WP_CHUNK, nact);
+    for (int i = base; i < end; ++i) {
+      const int p = act ? act[i] : i;
+      const double4 P = pm[p];
+      const float px = (float)(P.x - t.rootx), py = (float)(P.y - t.rooty),
+                  pz = (float)(P.z - t.rootz);
+      const double hp = hz[p].x;
+      const double R = KERNRANGE * hp;
+      const float R32 = (float)R;
+      const double hsp = (KERNRANGESQD * hp) * hp;
+      int cnt = 0;
+      const int nl = wp_walk(t, lane, S, cnt, nvisit, [&](int c) {   // BHhydro_walk.F90:37-43
+        const float4 h32 = t.hA32[c];
+        const float d0 = h32.x - px, d1 = h32.y - py, d2 = h32.z - pz;
+        const float d2s = (d0 * d0 + d1 * d1) + d2 * d2;
+        const int r1 = test32(d2s, R32 + h32.w, t.delta);
+        const int r2 = test32(d2s, t.hrm32[c] + h32.w, t.delta);
+        if (r1 == 1 || r2 == 1) return true;
+        if (r1 == 0 && r2 == 0) return false;
+        const double4 h = t.hA[c];
+        const double e0 = h.x - P.x, e1 = h.y - P.y, e2 = h.z - P.z;
+        const double drsqd = (e0 * e0 + e1 * e1) + e2 * e2;
+        const double t1 = R + h.w;
+        const double t2 = t.hrm[c] + h.w;
+        return drsqd <= t1 * t1 || drsqd <= t2 * t2;
+      });
+      int ncand = -1;
+      if (nl >= 0) {
+        wp_sort_leaves(nl, lane, S);
+        ncand = wp_flatten(nl, lane, S);
       }
+      if (nl < 0 || ncand > WP_CCAP) {
+        if (lane == 0) neib_one(p, pm, hz, t, L, pptot, pplist, err);
+        __syncwarp();
+        continue;
+      }
+      ncands += ncand;
+      int* row = pplist + (size_t)p * L;
+      int kept = 0;
+      for (int b = 0; b < ncand; b += 32) {
+        const int k = b + lane;
+        const int q = k < ncand ? S.cand[k] : p;
+        bool keep = false;
+        if (q != p) {
+          const double4 Q = pm[q];
+          const double hq = hz[q].x;
+          const double hsq = (KERNRANGESQD * hq) * hq;
+          const double d0 = Q.x - P.x, d1 = Q.y - P.y, d2 = Q.z - P.z;
+          const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
+          keep = drsqd <= hsp || drsqd <= hsq;
+        }
+        const unsigned m = __ballot_sync(FULL, keep);
+        const int pos = kept + __popc(m & ((1u << lane) - 1u));
+        if (keep && pos < L) row[pos] = q;
+        kept += __popc(m);
+      }
+      if (lane == 0) pptot[p] = kept;
     }
-    pptot[p] = cnt;
   }
-  for (int o = 16; o > 0; o >>= 1) ncand += __shfl_down_sync(FULL, ncand, o);
-  if (lane == 0) atomicAdd(counts + 7, ncand);
+  if (lane == 0) {
+    atomicAdd(counts + 4, nvisit);
+    atomicAdd(counts + 7, ncands);
+  }
 }
 
 // sph/hydro_gradh.F90:9-339 (NEIGHBOUR_LISTS, ARTIFICIAL_VISCOSITY=MON97).
@@ -747,26 +803,36 @@ inline int nb(long n, int t) { return (int)((n + t - 1) / t); }
 
 HydroTree hydro_tree(const Ctx& c) {
   const double delta = ldexp(1.0, -22) * (c.info.cellsize > 0.0 ? c.info.cellsize : 1.0);
-  return HydroTree{c.link, c.hA, c.hrm, c.hA32, c.hrm32, c.info.ctot, c.info.root[0],
+  return HydroTree{c.link, c.hA, c.hrm, c.hA32, c.hrm32, c.nkids, c.info.ctot, c.info.root[0],
                    c.info.root[1], c.info.root[2], (float)delta};
 }
 
 }  // namespace
 
+// persistent grid of warps taking particle chunks from a counter
+static int wp_grid(const Ctx& c, int nact) {
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c.dev);
+  const int want = nb(nact, WP_CHUNK * WP_WARPS);
+  return want < nsm * 8 ? want : nsm * 8;
+}
+
 void launch_gradh(Ctx& c, int nact) {
   if (nact <= 0) return;
-  k_gradh_warp<<<nb(nact, SW_THREADS), SW_THREADS, 0, c.st>>>(
+  cudaMemsetAsync(c.work, 0, sizeof(int), c.st);
+  k_gradh_wp<<<wp_grid(c, nact), WP_THREADS, 0, c.st>>>(
       nact, c.act, c.pm, c.hz, c.vel, c.rho, c.omega, c.div_v, c.drhodt, hydro_tree(c), c.tabA,
       c.prm.h_fac, c.prm.pp_gather, c.info.rextent, c.d_err,
-      reinterpret_cast<unsigned long long*>(c.d_counts));
+      reinterpret_cast<unsigned long long*>(c.d_counts), c.work);
   ++c.nlaunch;
 }
 
 void launch_neib(Ctx& c, int nact) {
   if (nact <= 0) return;
-  k_neib_warp<<<nb(nact, SW_THREADS), SW_THREADS, 0, c.st>>>(
+  cudaMemsetAsync(c.work, 0, sizeof(int), c.st);
+  k_neib_wp<<<wp_grid(c, nact), WP_THREADS, 0, c.st>>>(
       nact, c.act, c.pm, c.hz, hydro_tree(c), c.prm.pp_limit, c.pptot, c.pplist, c.d_err,
-      reinterpret_cast<unsigned long long*>(c.d_counts));
+      reinterpret_cast<unsigned long long*>(c.d_counts), c.work);
   ++c.nlaunch;
 }
 

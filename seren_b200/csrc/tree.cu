@@ -287,7 +287,8 @@ __global__ void k_split(const int* __restrict__ branch, const TreeInfo* __restri
 __global__ void k_emit(const int* __restrict__ branch, const TreeInfo* __restrict__ info, int lev,
                        const int* __restrict__ choff, const int* __restrict__ cstart,
                        int level_first, int* leaf, int* nextcell, int* ifopen, int* pstart,
-                       int* pcount, int* parent, int* level, int* __restrict__ bflag) {
+                       int* pcount, int* parent, int* level, int* nkids,
+                       int* __restrict__ bflag) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= info->nbranch) return;
   const int b = branch[j];
@@ -306,12 +307,14 @@ __global__ void k_emit(const int* __restrict__ branch, const TreeInfo* __restric
     pcount[c] = cnt;
     parent[c] = b;
     level[c] = lev + 1;
+    nkids[c] = 0;
     bflag[c - level_first] = lf == 0 ? 1 : 0;
     if (prev >= 0) nextcell[prev] = c;
     prev = c;
   }
   nextcell[prev] = nextcell[b];
   ifopen[b] = first;
+  nkids[b] = k;
 }
 
 __global__ void k_next_branch(const int* __restrict__ bflag, const int* __restrict__ bscan, int nnew,
@@ -666,7 +669,7 @@ int build_tree(Ctx& c) {
     }
     k_emit<<<nb(nbranch, 128), 128, 0, c.st>>>(br, c.d_info, lev, c.choff, c.cstart, level_first,
                                                c.leaf, c.nextcell, c.ifopen, c.pstart, c.pcount,
-                                               c.parent, c.level, c.bflag); ++c.nlaunch;
+                                               c.parent, c.level, c.nkids, c.bflag); ++c.nlaunch;
     scan_exclusive(c, c.bflag, c.bscan, nnew);
     k_next_branch<<<nb(nnew, 256), 256, 0, c.st>>>(c.bflag, c.bscan, nnew, level_first, br_next); ++c.nlaunch;
     k_level_done<<<1, 1, 0, c.st>>>(c.d_info, lev, level_first, nnew, c.scan.total); ++c.nlaunch;
