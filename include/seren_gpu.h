@@ -142,10 +142,15 @@ int seren_gpu_tree_export(seren_gpu_ctx* ctx, int32_t* ctot, int32_t* ltot,
 
 /* Per-stage device time of the last seren_gpu_force_step (ms: tree build +
  * stock, grad-h, hmax update + neighbour lists, thermal + hydro, gravity,
- * total), the number of kernels it launched, and the interaction counts of
- * the last gravity call (counts[0] cell terms, counts[1] pair terms). */
+ * total), the number of kernels it launched, and the work counters of the
+ * last force evaluation (16 slots): gravity [0] cell terms, [1] pair terms,
+ * [2] walk entries (cell, lane mask), [8] deepest walk stack, [9] cell-list
+ * entries, [10] of them taken by all 32 lanes, [11] near-field list items,
+ * [12] of them for all 32 lanes; grad-h [3] walks, [4] cells visited (with
+ * the neighbour-list kernel), [5] passes, [6] candidates; neighbour lists
+ * [7] candidates. */
 int seren_gpu_last_step_stats(seren_gpu_ctx* ctx, double* stage_ms /*[8]*/,
-                              int32_t* nlaunch, int64_t* counts /*[8]*/);
+                              int32_t* nlaunch, int64_t* counts /*[16]*/);
 
 /* The CUDA stream every kernel of this context runs on (cudaStream_t), so a
  * caller can order its own work and CUDA events against the library's. */

@@ -194,7 +194,7 @@ void free_all(Ctx& c) {
                 c.pptot, c.pplist, c.stage, c.istage, c.keys, c.keys_alt, c.idx, c.idx_alt,
                 c.rs_hist, c.bbox_part, c.branch, c.branch_next, c.nchild, c.choff, c.cstart,
                 c.bflag, c.bscan, c.leaf, c.nextcell, c.ifopen, c.pstart, c.pcount, c.parent,
-                c.level, c.nkids, c.work, c.link, c.gA, c.gB, c.gC, c.wA, c.wLo, c.hA, c.hrm, c.hA32, c.hrm32, c.hmax, c.bbmin, c.bbmax, c.d_info,
+                c.level, c.nkids, c.work, c.wstack, c.link, c.gA, c.gB, c.gC, c.wA, c.wLo, c.hA, c.hrm, c.hA32, c.hrm32, c.hmax, c.bbmin, c.bbmax, c.d_info,
                 c.d_err, c.d_counts, c.tabA, c.tabG, c.scan.total, c.scan.level_buf[0],
                 c.scan.level_buf[1], c.scan.level_buf[2], c.scan.level_buf[3]};
   for (void* p : ps)
@@ -233,6 +233,9 @@ int alloc_all(Ctx& c) {
          alloc(c.hmax, C) | alloc(c.bbmin, C) | alloc(c.bbmax, C);
   bad |= alloc(c.d_info, 1) | alloc(c.d_err, 1) | alloc(c.d_counts, 32);
   bad |= alloc(c.tabA, KERNTOT + 1) | alloc(c.tabG, KERNTOT + 1);
+  c.wstack_slots = grav_walk_slots(c);
+  c.wstack_cap = grav_walk_stack_cap(c);
+  bad |= alloc(c.wstack, (size_t)c.wstack_slots * c.wstack_cap);
   if (bad) return -1;
   const size_t scan_n = std::max(std::max(256 * rsblk, C), P) + 16;
   if (scan_scratch_alloc(c.scan, (int)scan_n)) return -1;
@@ -700,9 +703,9 @@ int seren_gpu_last_step_stats(seren_gpu_ctx* h, double* stage_ms, int32_t* nlaun
     for (int k = 0; k < 8; ++k) stage_ms[k] = c.stage_ms[k];
   if (nlaunch) *nlaunch = c.step_launches;
   if (counts) {
-    unsigned long long cc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    unsigned long long cc[16] = {};
     cudaMemcpy(cc, c.d_counts, sizeof(cc), cudaMemcpyDeviceToHost);
-    for (int k = 0; k < 8; ++k) counts[k] = (int64_t)cc[k];
+    for (int k = 0; k < 16; ++k) counts[k] = (int64_t)cc[k];
   }
   return SEREN_GPU_OK;
 }

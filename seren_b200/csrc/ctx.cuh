@@ -98,6 +98,9 @@ struct Ctx {
   DevError* d_err = nullptr;
   int* d_counts = nullptr;    // [16] int64 interaction counters (as 2 ints each)
   int* work = nullptr;        // work counter of the persistent kernels
+  int2* wstack = nullptr;     // walk stacks, wstack_cap (cell, lane mask) entries per warp slot
+  int wstack_cap = 0;
+  int wstack_slots = 0;
 
   // kernel tables
   double4* tabA = nullptr;
@@ -134,6 +137,8 @@ void launch_thermal(Ctx& c);
 // gravity.cu
 void launch_grav(Ctx& c, int nact, int nsink, const double* d_sinks);
 void launch_sink_walk(Ctx& c, int nsink, const double* d_sinks, double* d_out /*[nsink][4]*/);
+int grav_walk_slots(const Ctx& c);      // resident warps of the gravity walk grid
+int grav_walk_stack_cap(const Ctx& c);  // stack entries per warp
 
 // tables.cpp
 void make_kernel_tables(int kernel, std::vector<double>& w0, std::vector<double>& w1,

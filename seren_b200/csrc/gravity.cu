@@ -11,6 +11,8 @@
 //    FP32 (rsqrtf, FMA), with the M4 softening kernel evaluated analytically at
 //    the centre of the reference's table bin; terms are summed in FP32 with
 //    Kahan compensation and added to the FP64 result once.
+#include <algorithm>
+
 #include "ctx.cuh"
 
 namespace seren {
@@ -133,32 +135,39 @@ __device__ __forceinline__ void count_add(unsigned long long* counts, unsigned l
 }
 
 // ---------------------------------------------------------------------------
-// Warp-cooperative walk.  One warp walks the tree once for 32 consecutive
-// particles (tree order: spatially adjacent) with the reference's per-particle
-// decisions intact: the walk position c is warp-uniform, each lane keeps a
-// skip marker (the nextcell of the highest cell it accepted while another lane
-// opened it; leaving any subtree lands exactly on its nextcell), and the MAC
-// test of each lane is the reference's drsqd > dminsqd.  That test runs first
+// Frontier walk.  One warp walks the tree for 32 consecutive active particles
+// (tree order: spatially adjacent) with the reference's per-particle decisions
+// intact.  The walk state is a per-warp stack of entries (cell, mask): the
+// cell, and the lanes whose walk reaches it (every ancestor was opened for
+// them).  Each step pops up to 32 entries; the lanes load those cells in
+// parallel, then every lane runs the reference's MAC test drsqd > dminsqd for
+// its own particle against each popped cell in its mask.  That test runs first
 // in FP32 on root-relative coordinates against a bracket [lo, hi] around
 // dminsqd that covers the FP32 rounding; inside the bracket it is redone in
 // FP64 exactly as BHgrav_accel.F90:146-155 does, so every decision equals the
-// FP64 one.  Accepted cells and opened leaves go to per-warp lists in shared
-// memory with the mask of the lanes they belong to; a full list is flushed by
-// all lanes together (broadcast loads, per-lane predicate).
+// FP64 one.  Accepted cells go to a cell list with the mask of lanes that took
+// them; opened leaves put their particles on a near-field list
+// (BHgrav_accel.F90:128-136, :242-253); opened branch cells push their children
+// with the mask of lanes that opened them.  Each cell is reached at most once
+// per group, so a group processes at most ctot+1 entries.  Full lists are
+// flushed by all lanes together (lane-parallel record preparation, then
+// broadcast loads and a per-lane predicate).
 constexpr int GW_THREADS = 128;
 constexpr int GW_WARPS = GW_THREADS / 32;
-constexpr int GW_CAP = 64;       // accepted-cell entries per warp list
-constexpr int GW_ITEMS = 128;    // near-field particle items per warp list
+constexpr int GW_STACK = 8192;   // frontier entries per warp (at most ctot+1 are ever live)
+constexpr int GW_PITEMS = 384;   // near-field (particle, mask) items per warp list
 constexpr unsigned FULLMASK = 0xffffffffu;
 
 struct GravWalk {
   const int4* link;
+  const int* nkids;     // children of a branch cell: ifopen .. ifopen+nkids-1
   const float4* wA;     // FP32 COM relative to the root centre, hi bracket
   const float* wLo;     // lo bracket
   const double4* gA;
   const double4* gB;
   const double2* gC;
   int ctot;
+  int scap;             // stack entries per warp
   double rootx, rooty, rootz;
 };
 
@@ -231,233 +240,297 @@ __device__ __forceinline__ void cell32(float d0, float d1, float d2, const float
   ap += fmaf(0.5f * qscalar, invdr5, a.w * invdrmag);
 }
 
-// Per-warp list records, prepared lane-parallel at flush time.
 template <bool MIXED>
-struct GwRec;
-template <>
-struct GwRec<true> {
-  float4 ca[GW_CAP];      // cell: (r_ref - COM) in FP32, m
-  float4 cb[GW_CAP];      // q1..q4
-  float cq5[GW_CAP];
-  int cid[GW_CAP];
-  unsigned cmask[GW_CAP];
-  float4 pa[GW_ITEMS];    // particle: (r_q - r_ref) in FP32, m
-  float2 pb[GW_ITEMS];    // 1/h, zeta
-  int qid[GW_ITEMS];
-  unsigned qmask[GW_ITEMS];
+struct GwTypes {
+  using R = float;
+  using R2 = float2;
+  using R4 = float4;
+  static constexpr int CAP = 96;   // accepted-cell entries per warp list
+  static constexpr int PREP = 128; // near-field records prepared per flush pass
 };
 template <>
-struct GwRec<false> {
-  double4 ca[GW_CAP];     // COM, m
-  double4 cb[GW_CAP];
-  double cq5[GW_CAP];
-  int cid[GW_CAP];
-  unsigned cmask[GW_CAP];
-  double4 pa[GW_ITEMS];   // position, m
-  double2 pb[GW_ITEMS];   // h, zeta
-  int qid[GW_ITEMS];
-  unsigned qmask[GW_ITEMS];
+struct GwTypes<false> {
+  using R = double;
+  using R2 = double2;
+  using R4 = double4;
+  static constexpr int CAP = 64;
+  static constexpr int PREP = 64;
 };
+
+// Per-warp shared state: interaction lists, prepared records, popped cells.
+template <bool MIXED>
+struct GwRec {
+  using T = GwTypes<MIXED>;
+  typename T::R4 ca[T::CAP];       // cell: mixed (r_ref - COM, m), FP64 (COM, m)
+  typename T::R4 cb[T::CAP];       // q1..q4
+  typename T::R cq5[T::CAP];
+  int cid[T::CAP];
+  unsigned cmask[T::CAP];
+  int qid[GW_PITEMS];
+  unsigned qmask[GW_PITEMS];
+  typename T::R4 pa[T::PREP];      // particle: mixed (r_q - r_ref, m), FP64 (r_q, m)
+  typename T::R2 pb[T::PREP];      // mixed (1/h, zeta), FP64 (h, zeta)
+  float4 fw[32];                   // popped cells: wA
+  float flo[32];                   // wLo
+  unsigned ftest[32];              // lanes that test the cell (0 for one-particle leaves)
+  int fcell[32];
+};
+
+__device__ __forceinline__ int warp_incl(int v, int lane) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(FULLMASK, v, o);
+    if (lane >= o) v += y;
+  }
+  return v;
+}
 
 template <bool MIXED>
 __global__ void __launch_bounds__(GW_THREADS)
-k_grav_warp(int nact, const int* __restrict__ act, const double4* __restrict__ pm,
+k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ pm,
             const double2* __restrict__ hz, GravWalk t, const double4* __restrict__ tabG,
             double* __restrict__ acc, double* __restrict__ gpot, int nsink,
-            const double* __restrict__ sinks, DevError* err, unsigned long long* counts) {
+            const double* __restrict__ sinks, int2* __restrict__ stacks, int* work,
+            DevError* err, unsigned long long* counts) {
+  using Cfg = GwTypes<MIXED>;
+  constexpr int CAP = Cfg::CAP;
   __shared__ GwRec<MIXED> srec[GW_WARPS];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   GwRec<MIXED>& R = srec[w];
-  const int i = blockIdx.x * GW_THREADS + threadIdx.x;
-  const bool live = i < nact;
-  if (__ballot_sync(FULLMASK, live) == 0) return;       // whole warp past the end
-  const int p = live ? (act ? act[i] : i) : (act ? act[nact - 1] : nact - 1);
-  const double4 P = pm[p];
-  const double2 HZ = hz[p];
-  // warp reference point (lane 0 is live whenever any lane is)
-  const double rx = __shfl_sync(FULLMASK, P.x, 0);
-  const double ry = __shfl_sync(FULLMASK, P.y, 0);
-  const double rz = __shfl_sync(FULLMASK, P.z, 0);
-  const float px32 = (float)(P.x - t.rootx), py32 = (float)(P.y - t.rooty),
-              pz32 = (float)(P.z - t.rootz);
-  const float ux = (float)(P.x - rx), uy = (float)(P.y - ry), uz = (float)(P.z - rz);
-  const double invhp = 1.0 / HZ.x;
-  const double zo_p = HZ.y;
-  const float invhp32 = (float)invhp, zo32 = (float)zo_p;
-  Kahan4 kc;
-  double cx = 0.0, cy = 0.0, cz = 0.0, cp = 0.0, qx = 0.0, qy = 0.0, qz = 0.0, qp = 0.0;
-  unsigned long long ncell = 0, npair = 0;
-  int skip = live ? -1 : -2;
-  int c = 0, visits = 0, nc = 0, np = 0;
-
-  auto flush_cells = [&]() {
-    __syncwarp();
-    for (int e = lane; e < nc; e += 32) {                    // lane-parallel preparation
-      const int cid = R.cid[e];
-      const double4 a = t.gA[cid];
-      const double4 q = t.gB[cid];
-      const double q5 = t.gC[cid].x;
-      if (MIXED) {
-        reinterpret_cast<float4*>(R.ca)[e] =
-            make_float4((float)(rx - a.x), (float)(ry - a.y), (float)(rz - a.z), (float)a.w);
-        reinterpret_cast<float4*>(R.cb)[e] = make_float4((float)q.x, (float)q.y, (float)q.z, (float)q.w);
-        reinterpret_cast<float*>(R.cq5)[e] = (float)q5;
-      } else {
-        reinterpret_cast<double4*>(R.ca)[e] = a;
-        reinterpret_cast<double4*>(R.cb)[e] = q;
-        reinterpret_cast<double*>(R.cq5)[e] = q5;
-      }
-    }
-    __syncwarp();
-    if (MIXED) {
-      float sx = 0.f, sy = 0.f, sz = 0.f, sp = 0.f;
-      for (int e = 0; e < nc; ++e) {
-        if ((R.cmask[e] >> lane) & 1u) {
-          const float4 a = reinterpret_cast<const float4*>(R.ca)[e];
-          cell32(ux + a.x, uy + a.y, uz + a.z, a, reinterpret_cast<const float4*>(R.cb)[e],
-                 reinterpret_cast<const float*>(R.cq5)[e], sx, sy, sz, sp);
-          ++ncell;
-        }
-      }
-      kc.add(0, sx); kc.add(1, sy); kc.add(2, sz); kc.add(3, sp);
-    } else {
-      for (int e = 0; e < nc; ++e) {
-        if ((R.cmask[e] >> lane) & 1u) {
-          const double4 a = reinterpret_cast<const double4*>(R.ca)[e];
-          const double d0 = P.x - a.x, d1 = P.y - a.y, d2 = P.z - a.z;
-          cell_term64(d0, d1, d2, (d0 * d0 + d1 * d1) + d2 * d2, a,
-                      reinterpret_cast<const double4*>(R.cb)[e],
-                      reinterpret_cast<const double*>(R.cq5)[e], cx, cy, cz, cp);
-          ++ncell;
-        }
-      }
-    }
-    nc = 0;
-    __syncwarp();
-  };
-  auto flush_pairs = [&]() {
-    __syncwarp();
-    for (int e = lane; e < np; e += 32) {
-      const int q = R.qid[e];
-      const double4 Q = pm[q];
-      const double2 H = hz[q];
-      if (MIXED) {
-        reinterpret_cast<float4*>(R.pa)[e] =
-            make_float4((float)(Q.x - rx), (float)(Q.y - ry), (float)(Q.z - rz), (float)Q.w);
-        reinterpret_cast<float2*>(R.pb)[e] = make_float2((float)(1.0 / H.x), (float)H.y);
-      } else {
-        reinterpret_cast<double4*>(R.pa)[e] = Q;
-        reinterpret_cast<double2*>(R.pb)[e] = H;
-      }
-    }
-    __syncwarp();
-    if (MIXED) {
-      float sx = 0.f, sy = 0.f, sz = 0.f, sp = 0.f;
-      for (int e = 0; e < np; ++e) {
-        if (((R.qmask[e] >> lane) & 1u) && R.qid[e] != p) {
-          const float4 a = reinterpret_cast<const float4*>(R.pa)[e];
-          const float2 b = reinterpret_cast<const float2*>(R.pb)[e];
-          pair32(a.x - ux, a.y - uy, a.z - uz, invhp32, zo32, a.w, b.x, b.y, sx, sy, sz, sp);
-          ++npair;
-        }
-      }
-      kc.add(0, sx); kc.add(1, sy); kc.add(2, sz); kc.add(3, sp);
-    } else {
-      for (int e = 0; e < np; ++e) {
-        if (((R.qmask[e] >> lane) & 1u) && R.qid[e] != p) {
-          const double4 Q = reinterpret_cast<const double4*>(R.pa)[e];
-          const double2 H = reinterpret_cast<const double2*>(R.pb)[e];
-          pair_term64(Q.x - P.x, Q.y - P.y, Q.z - P.z, invhp, zo_p, Q.w, H.x, H.y, tabG, qx, qy,
-                      qz, qp);
-          ++npair;
-        }
-      }
-    }
-    np = 0;
-    __syncwarp();
-  };
+  int2* const S = stacks + (size_t)(blockIdx.x * GW_WARPS + w) * t.scap;
+  const unsigned lt = (1u << lane) - 1u;
+  unsigned long long ncell = 0, npair = 0, nent = 0;
+  unsigned ce_all = 0, ce_full = 0, pi_all = 0, pi_full = 0;   // list fill statistics
+  int smax = 0;
 
   while (true) {
-    if (++visits > t.ctot + 2) {
-      if (lane == 0) set_error(err, SEREN_GPU_ERR_WALK, MIXED ? KID_GRAV_MIXED : KID_GRAV, p, c);
-      break;
-    }
-    const int4 lk = t.link[c];
-    if (skip == c) skip = -1;
-    const bool actv = skip == -1;
-    if (lk.x == 1) {                                         // BHgrav_accel.F90:128-136
-      const unsigned m = __ballot_sync(FULLMASK, actv && lk.w != p);
-      if (m) {
-        if (lane == 0) { R.qid[np] = lk.w; R.qmask[np] = m; }
-        ++np;
-      }
-      c = lk.y;
-    } else {
-      bool accept = false;
-      if (actv) {
-        const float4 wa = t.wA[c];
-        const float d0 = px32 - wa.x, d1 = py32 - wa.y, d2 = pz32 - wa.z;
-        const float d2s = (d0 * d0 + d1 * d1) + d2 * d2;
-        if (d2s > wa.w) {
-          accept = true;
-        } else if (d2s >= t.wLo[c]) {                        // exact test, :146-155
-          const double4 a = t.gA[c];
-          const double e0 = P.x - a.x, e1 = P.y - a.y, e2 = P.z - a.z;
-          accept = ((e0 * e0 + e1 * e1) + e2 * e2) > t.gC[c].y;
+    int g = 0;
+    if (lane == 0) g = atomicAdd(work, 1);
+    g = __shfl_sync(FULLMASK, g, 0);
+    if ((long long)g * 32 >= nact) break;
+    const int i = g * 32 + lane;
+    const bool live = i < nact;
+    const int p = live ? (act ? act[i] : i) : (act ? act[nact - 1] : nact - 1);
+    const double4 P = pm[p];
+    const double2 HZ = hz[p];
+    // warp reference point (lane 0 is always live)
+    const double rx = __shfl_sync(FULLMASK, P.x, 0);
+    const double ry = __shfl_sync(FULLMASK, P.y, 0);
+    const double rz = __shfl_sync(FULLMASK, P.z, 0);
+    const float px32 = (float)(P.x - t.rootx), py32 = (float)(P.y - t.rooty),
+                pz32 = (float)(P.z - t.rootz);
+    const float ux = (float)(P.x - rx), uy = (float)(P.y - ry), uz = (float)(P.z - rz);
+    const double invhp = 1.0 / HZ.x;
+    const double zo_p = HZ.y;
+    const float invhp32 = (float)invhp, zo32 = (float)zo_p;
+    Kahan4 kc;
+    double cx = 0.0, cy = 0.0, cz = 0.0, cp = 0.0, qx = 0.0, qy = 0.0, qz = 0.0, qp = 0.0;
+    int nc = 0, np = 0;
+
+    auto flush_cells = [&]() {
+      __syncwarp();
+      for (int e = lane; e < nc; e += 32) {                  // lane-parallel preparation
+        const int cid = R.cid[e];
+        const double4 a = t.gA[cid];
+        const double4 q = t.gB[cid];
+        const double q5 = t.gC[cid].x;
+        if constexpr (MIXED) {
+          R.ca[e] = make_float4((float)(rx - a.x), (float)(ry - a.y), (float)(rz - a.z), (float)a.w);
+          R.cb[e] = make_float4((float)q.x, (float)q.y, (float)q.z, (float)q.w);
+          R.cq5[e] = (float)q5;
+        } else {
+          R.ca[e] = a;
+          R.cb[e] = q;
+          R.cq5[e] = q5;
         }
       }
-      const unsigned macc = __ballot_sync(FULLMASK, accept);
-      const unsigned mopn = __ballot_sync(FULLMASK, actv && !accept);
-      if (macc) {
-        if (lane == 0) { R.cid[nc] = c; R.cmask[nc] = macc; }
-        ++nc;
-      }
-      if (lk.x > 0) {                                        // :242-253
-        if (mopn) {
-          if (lane < lk.x) { R.qid[np + lane] = lk.w + lane; R.qmask[np + lane] = mopn; }
-          np += lk.x;
+      __syncwarp();
+      if constexpr (MIXED) {
+        float sx = 0.f, sy = 0.f, sz = 0.f, sp = 0.f;
+        for (int e = 0; e < nc; ++e) {
+          if ((R.cmask[e] >> lane) & 1u) {
+            const float4 a = R.ca[e];
+            cell32(ux + a.x, uy + a.y, uz + a.z, a, R.cb[e], R.cq5[e], sx, sy, sz, sp);
+            ++ncell;
+          }
         }
-        c = lk.y;
-      } else if (lk.x == 0 && mopn) {
-        if (accept) skip = lk.y;
-        c = lk.z;
+        kc.add(0, sx); kc.add(1, sy); kc.add(2, sz); kc.add(3, sp);
       } else {
-        c = lk.y;
+        for (int e = 0; e < nc; ++e) {
+          if ((R.cmask[e] >> lane) & 1u) {
+            const double4 a = R.ca[e];
+            const double d0 = P.x - a.x, d1 = P.y - a.y, d2 = P.z - a.z;
+            cell_term64(d0, d1, d2, (d0 * d0 + d1 * d1) + d2 * d2, a, R.cb[e], R.cq5[e], cx, cy,
+                        cz, cp);
+            ++ncell;
+          }
+        }
       }
-    }
-    if (nc == GW_CAP) flush_cells();
-    if (np > GW_ITEMS - LEAFMAX) flush_pairs();
-    if (c > t.ctot) break;
-  }
-  flush_cells();
-  flush_pairs();
-  if (live) {
-    double ax, ay, az, pot;
-    if (MIXED) {
-      ax = kc.get(0); ay = kc.get(1); az = kc.get(2); pot = kc.get(3);
-    } else {
-      ax = cx + qx; ay = cy + qy; az = cz + qz; pot = cp + qp;
-    }
-    double* a = acc + (size_t)p * 3;
-    a[0] = a[0] + ax;
-    a[1] = a[1] + ay;
-    a[2] = a[2] + az;
-    if (nsink > 0) {                                         // sinks/direct_sink_gravity.F90
-      double sx = 0.0, sy = 0.0, sz = 0.0, sp = 0.0;
-      for (int s = 0; s < nsink; ++s) {
-        const double* sr = sinks + s * 5;
-        meanh_term64(sr[0] - P.x, sr[1] - P.y, sr[2] - P.z, 0.5 * (HZ.x + sr[4]), sr[3], tabG, sx,
-                     sy, sz, sp);
+      nc = 0;
+      __syncwarp();
+    };
+    auto flush_pairs = [&]() {
+      for (int b0 = 0; b0 < np; b0 += Cfg::PREP) {
+        const int nb = min(Cfg::PREP, np - b0);
+        __syncwarp();
+        for (int e = lane; e < nb; e += 32) {
+          const int q = R.qid[b0 + e];
+          const double4 Q = pm[q];
+          const double2 H = hz[q];
+          if constexpr (MIXED) {
+            R.pa[e] = make_float4((float)(Q.x - rx), (float)(Q.y - ry), (float)(Q.z - rz), (float)Q.w);
+            R.pb[e] = make_float2((float)(1.0 / H.x), (float)H.y);
+          } else {
+            R.pa[e] = Q;
+            R.pb[e] = H;
+          }
+        }
+        __syncwarp();
+        if constexpr (MIXED) {
+          float sx = 0.f, sy = 0.f, sz = 0.f, sp = 0.f;
+          for (int e = 0; e < nb; ++e) {
+            if (((R.qmask[b0 + e] >> lane) & 1u) && R.qid[b0 + e] != p) {
+              const float4 a = R.pa[e];
+              const float2 b = R.pb[e];
+              pair32(a.x - ux, a.y - uy, a.z - uz, invhp32, zo32, a.w, b.x, b.y, sx, sy, sz, sp);
+              ++npair;
+            }
+          }
+          kc.add(0, sx); kc.add(1, sy); kc.add(2, sz); kc.add(3, sp);
+        } else {
+          for (int e = 0; e < nb; ++e) {
+            if (((R.qmask[b0 + e] >> lane) & 1u) && R.qid[b0 + e] != p) {
+              const double4 Q = R.pa[e];
+              const double2 H = R.pb[e];
+              pair_term64(Q.x - P.x, Q.y - P.y, Q.z - P.z, invhp, zo_p, Q.w, H.x, H.y, tabG, qx,
+                          qy, qz, qp);
+              ++npair;
+            }
+          }
+        }
       }
-      a[0] = a[0] + sx;
-      a[1] = a[1] + sy;
-      a[2] = a[2] + sz;
-      pot = pot + sp;
+      np = 0;
+      __syncwarp();
+    };
+
+    const unsigned rootmask = __ballot_sync(FULLMASK, live);
+    if (lane == 0) S[0] = make_int2(0, (int)rootmask);
+    int sp = 1;
+    long long gent = 0;
+    while (sp > 0) {
+      __syncwarp();
+      const int k = min(32, sp);
+      sp -= k;
+      gent += k;
+      int cc = 0, nk = 0;
+      unsigned m = 0;
+      int4 lk = make_int4(-1, 0, 0, 0);
+      if (lane < k) {
+        const int2 ent = S[sp + lane];
+        cc = ent.x;
+        m = (unsigned)ent.y;
+        lk = t.link[cc];
+        if (lk.x != 1) {
+          R.fw[lane] = t.wA[cc];
+          R.flo[lane] = t.wLo[cc];
+          if (lk.x == 0) nk = t.nkids[cc];
+        }
+        R.ftest[lane] = lk.x == 1 ? 0u : m;
+        R.fcell[lane] = cc;
+      }
+      __syncwarp();
+      unsigned macc = 0;
+      for (int e = 0; e < k; ++e) {
+        const unsigned mt = R.ftest[e];
+        if (mt == 0u) continue;                              // warp-uniform
+        bool accept = false;
+        if ((mt >> lane) & 1u) {
+          const float4 wa = R.fw[e];
+          const float d0 = px32 - wa.x, d1 = py32 - wa.y, d2 = pz32 - wa.z;
+          const float d2s = (d0 * d0 + d1 * d1) + d2 * d2;
+          if (d2s > wa.w) {
+            accept = true;
+          } else if (d2s >= R.flo[e]) {                      // exact test, :146-155
+            const int ce = R.fcell[e];
+            const double4 a = t.gA[ce];
+            const double e0 = P.x - a.x, e1 = P.y - a.y, e2 = P.z - a.z;
+            accept = ((e0 * e0 + e1 * e1) + e2 * e2) > t.gC[ce].y;
+          }
+        }
+        const unsigned b = __ballot_sync(FULLMASK, accept);
+        if (lane == e) macc = b;
+      }
+      const unsigned mopn = m & ~macc;
+      // accepted cells
+      const unsigned bc = __ballot_sync(FULLMASK, macc != 0u);
+      if (macc != 0u) {
+        const int o = nc + __popc(bc & lt);
+        R.cid[o] = cc;
+        R.cmask[o] = macc;
+        ++ce_all;
+        ce_full += macc == rootmask;
+      }
+      nc += __popc(bc);
+      // opened leaves: their particles join the near-field list
+      const int npush = (lk.x > 0 && mopn != 0u) ? lk.x : 0;
+      pi_all += npush;
+      pi_full += mopn == rootmask ? npush : 0;
+      const int pin = warp_incl(npush, lane);
+      for (int q = 0; q < npush; ++q) {
+        R.qid[np + pin - npush + q] = lk.w + q;
+        R.qmask[np + pin - npush + q] = mopn;
+      }
+      np += __shfl_sync(FULLMASK, pin, 31);
+      // opened branch cells: children onto the stack
+      const int nch = (lk.x == 0 && mopn != 0u) ? nk : 0;
+      const int cin = warp_incl(nch, lane);
+      const int ctotal = __shfl_sync(FULLMASK, cin, 31);
+      if (sp + ctotal > t.scap || gent > (long long)t.ctot + 1) {
+        if (lane == 0) set_error(err, SEREN_GPU_ERR_WALK, MIXED ? KID_GRAV_MIXED : KID_GRAV, p, cc);
+        break;
+      }
+      for (int q = 0; q < nch; ++q) S[sp + cin - nch + q] = make_int2(lk.z + q, (int)mopn);
+      sp += ctotal;
+      smax = max(smax, sp);
+      if (nc > CAP - 32) flush_cells();
+      if (np > GW_PITEMS - 32 * LEAFMAX) flush_pairs();
     }
-    gpot[p] = pot;
+    nent += gent;
+    flush_cells();
+    flush_pairs();
+    if (live) {
+      double ax, ay, az, pot;
+      if constexpr (MIXED) {
+        ax = kc.get(0); ay = kc.get(1); az = kc.get(2); pot = kc.get(3);
+      } else {
+        ax = cx + qx; ay = cy + qy; az = cz + qz; pot = cp + qp;
+      }
+      double* a = acc + (size_t)p * 3;
+      a[0] = a[0] + ax;
+      a[1] = a[1] + ay;
+      a[2] = a[2] + az;
+      if (nsink > 0) {                                       // sinks/direct_sink_gravity.F90
+        double sx = 0.0, sy = 0.0, sz = 0.0, sp2 = 0.0;
+        for (int s = 0; s < nsink; ++s) {
+          const double* sr = sinks + s * 5;
+          meanh_term64(sr[0] - P.x, sr[1] - P.y, sr[2] - P.z, 0.5 * (HZ.x + sr[4]), sr[3], tabG,
+                       sx, sy, sz, sp2);
+        }
+        a[0] = a[0] + sx;
+        a[1] = a[1] + sy;
+        a[2] = a[2] + sz;
+        pot = pot + sp2;
+      }
+      gpot[p] = pot;
+    }
   }
   count_add(counts, ncell, npair);
-  if (lane == 0) atomicAdd(counts + 2, (unsigned long long)visits);
+  count_add(counts + 9, ce_all, ce_full);
+  count_add(counts + 11, pi_all, pi_full);
+  if (lane == 0) {
+    atomicAdd(counts + 2, nent);
+    atomicMax(counts + 8, (unsigned long long)smax);
+  }
 }
 
 
@@ -528,17 +601,49 @@ GravTree grav_tree(const Ctx& c) { return GravTree{c.link, c.gA, c.gB, c.gC, c.i
 
 }  // namespace
 
+static int grav_blocks_per_sm(int dev, bool mixed) {
+  static int occ[16][2] = {};
+  int dummy[2] = {0, 0};
+  int* o = dev >= 0 && dev < 16 ? occ[dev] : dummy;
+  int& r = o[mixed ? 1 : 0];
+  if (r == 0) {
+    if (mixed)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_grav_walk<true>, GW_THREADS, 0);
+    else
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_grav_walk<false>, GW_THREADS, 0);
+    if (r < 1) r = 1;
+  }
+  return r;
+}
+
+static int sm_count(const Ctx& c) {
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c.dev);
+  return nsm;
+}
+
+int grav_walk_slots(const Ctx& c) {
+  return sm_count(c) * std::max(grav_blocks_per_sm(c.dev, true), grav_blocks_per_sm(c.dev, false)) *
+         GW_WARPS;
+}
+
+int grav_walk_stack_cap(const Ctx& c) { return std::min(GW_STACK, c.cmax + 1); }
+
 void launch_grav(Ctx& c, int nact, int nsink, const double* d_sinks) {
   if (nact <= 0) return;
   unsigned long long* counts = reinterpret_cast<unsigned long long*>(c.d_counts);
-  const GravWalk gw{c.link, c.wA, c.wLo, c.gA, c.gB, c.gC, c.info.ctot,
+  const GravWalk gw{c.link, c.nkids, c.wA, c.wLo, c.gA, c.gB, c.gC, c.info.ctot, c.wstack_cap,
                     c.info.root[0], c.info.root[1], c.info.root[2]};
-  if (c.prm.precision == 0)
-    k_grav_warp<false><<<nb(nact, GW_THREADS), GW_THREADS, 0, c.st>>>(
-        nact, c.act, c.pm, c.hz, gw, c.tabG, c.acc, c.gpot, nsink, d_sinks, c.d_err, counts);
+  const bool mixed = c.prm.precision != 0;
+  const int groups = nb(nact, 32);
+  const int blocks = std::min(sm_count(c) * grav_blocks_per_sm(c.dev, mixed), nb(groups, GW_WARPS));
+  cudaMemsetAsync(c.work, 0, sizeof(int), c.st);
+  if (!mixed)
+    k_grav_walk<false><<<blocks, GW_THREADS, 0, c.st>>>(nact, c.act, c.pm, c.hz, gw, c.tabG,
+        c.acc, c.gpot, nsink, d_sinks, c.wstack, c.work, c.d_err, counts);
   else
-    k_grav_warp<true><<<nb(nact, GW_THREADS), GW_THREADS, 0, c.st>>>(
-        nact, c.act, c.pm, c.hz, gw, c.tabG, c.acc, c.gpot, nsink, d_sinks, c.d_err, counts);
+    k_grav_walk<true><<<blocks, GW_THREADS, 0, c.st>>>(nact, c.act, c.pm, c.hz, gw, c.tabG,
+        c.acc, c.gpot, nsink, d_sinks, c.wstack, c.work, c.d_err, counts);
   ++c.nlaunch;
 }
 

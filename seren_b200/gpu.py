@@ -78,11 +78,12 @@ class GpuHotPath(HotPath):
         return out
 
     def last_step_stats(self):
-        """(stage milliseconds [8], kernel launches, interaction counts [8]) of the
-        last force_step; counts[0] cell terms, counts[1] pair terms."""
+        """(stage milliseconds [8], kernel launches, work counters [16]) of the
+        last force_step; counts[0] cell terms, counts[1] pair terms (the slots
+        are listed at seren_gpu_last_step_stats)."""
         ms = (C.c_double * 8)()
         nl = C.c_int32()
-        cnt = (C.c_int64 * 8)()
+        cnt = (C.c_int64 * 16)()
         self._call("last_step_stats", self._ctx, ms, C.byref(nl), cnt)
         return list(ms), nl.value, list(cnt)
 

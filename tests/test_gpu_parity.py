@@ -92,7 +92,7 @@ def test_gravity_counts_equal_oracle(libs, name):
         o, g = _pair(libs, ic, precision=prec)
         ro = run_pipeline(o, ic)
         run_pipeline(g, ic)
-        cnt = (C.c_int64 * 8)()
+        cnt = (C.c_int64 * 16)()
         library().seren_gpu_last_step_stats(g._ctx, None, None, cnt)
         co = o.counts()
         assert cnt[0] == co["grav_cells"] and cnt[1] == co["grav_pairs"], (prec, list(cnt), co)
