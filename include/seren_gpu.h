@@ -162,6 +162,43 @@ int seren_gpu_get_stream(seren_gpu_ctx* ctx, void** stream);
  * pair-interaction kernels, which do not use tensor cores. */
 int seren_gpu_fma_peak(seren_gpu_ctx* ctx, int32_t precision, double* tflops);
 
+/* Hydro accelerations without a context and without allocating device memory.
+ * No counterpart in the reference: it serves callers that cannot call
+ * cudaMalloc, such as an application whose device memory belongs to its own
+ * pool allocator (a framework's caching allocator, a Fortran/OpenACC runtime
+ * that reserves the GPU up front) or that runs under a fixed memory budget.
+ * Such a caller cannot create a context, but it holds the particle state and
+ * the neighbour lists in device buffers of its own; this call runs the hydro
+ * kernel of seren_gpu_hydro_forces (grad-h pressure force and MON97
+ * viscosity, every particle active) on them.
+ *
+ * All pointers are DEVICE pointers, laid out like the host arrays above:
+ * parray[n][6], v[n][3], rho/omega/press/sound[n], pptot[n],
+ * pplist[n][pp_limit] with 0-based ids, output a[n][3] (overwritten).
+ * kernel and precision mean what they mean in seren_gpu_params.  stream is a
+ * cudaStream_t (NULL for the default stream); the call synchronises it.
+ *
+ * Limits: n <= SEREN_GPU_NOALLOC_PMAX (SEREN_GPU_ERR_CAPACITY beyond); every
+ * row must hold its whole neighbour list, 0 <= pptot <= pp_limit
+ * (SEREN_GPU_ERR_CAPACITY otherwise: the context entry point walks the tree
+ * for such rows, and there is no tree here); listed ids in 0..n-1
+ * (SEREN_GPU_ERR_ARG).  No message is kept: the return code is the report.
+ *
+ * Scratch: one fixed device array of 3.6 MiB (the kernel-layout copies of
+ * the particles, per-particle factors, kernel tables and an error block),
+ * held by every GPU that loads the library until the process exits.  The
+ * first call on a device looks up the array's address and uploads the kernel
+ * tables; make that first call before any stream capture.  Every call on a
+ * device shares the array and leaves its contents behind, so calls that
+ * overlap on the GPU (other streams, other host threads) race: serialise
+ * them. */
+#define SEREN_GPU_NOALLOC_PMAX 32768
+int seren_gpu_hydro_forces_noalloc(int32_t n, const double* parray, const double* v,
+                                   const double* rho, const double* omega, const double* press,
+                                   const double* sound, const int32_t* pptot,
+                                   const int32_t* pplist, int32_t pp_limit, int32_t kernel,
+                                   int32_t precision, double alpha, double* a, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -7,6 +7,9 @@
 // opened leaf's particles are consumed as they come, which visits candidates
 // in exactly the reference's list order (depth-first leaf order, particles in
 // leaf order), so every sum is accumulated in the reference's order.
+#include <mutex>
+#include <vector>
+
 #include "ctx.cuh"
 
 namespace seren {
@@ -857,3 +860,157 @@ void launch_thermal(Ctx& c) {
 }
 
 }  // namespace seren
+
+// ---------------------------------------------------------------------------
+// Hydro forces without a context and without allocation.
+//
+// Some callers cannot call cudaMalloc: an application whose device memory is
+// owned by its own pool allocator (a framework's caching allocator, or a
+// Fortran/OpenACC runtime that reserves the GPU's memory up front) or that runs
+// under a fixed device-memory budget.  Such a caller cannot create a context
+// (seren_gpu_create allocates the tree, lists and staging buffers), but it does
+// hold the particle arrays and neighbour lists in device buffers of its own.
+// seren_gpu_hydro_forces_noalloc runs the hydro kernel of
+// seren_gpu_hydro_forces on those buffers.  The kernel's scratch (the particle
+// arrays in the kernel's layout, the per-particle factors, the kernel tables
+// and the error block) lives in one file-scope device array of fixed size,
+// which every GPU that loads this library holds until the process exits.
+namespace seren {
+namespace {
+
+constexpr int NOALLOC_PMAX = SEREN_GPU_NOALLOC_PMAX;
+constexpr size_t NA_ERR = 0;                                     // DevError
+constexpr size_t NA_TAB = 32;                                    // 2 kernel tables (M4, M4TC)
+constexpr size_t NA_TABLEN = (size_t)(KERNTOT + 1) * 4;          // doubles per table
+constexpr size_t NA_PART = NA_TAB + ((2 * NA_TABLEN + 31) / 32) * 32;
+constexpr size_t NA_PM = NA_PART;                                // double4 per particle
+constexpr size_t NA_HZ = NA_PM + 4 * (size_t)NOALLOC_PMAX;       // double2
+constexpr size_t NA_VEL = NA_HZ + 2 * (size_t)NOALLOC_PMAX;      // double4
+constexpr size_t NA_PF = NA_VEL + 4 * (size_t)NOALLOC_PMAX;      // double
+constexpr size_t NA_HF4 = NA_PF + (size_t)NOALLOC_PMAX;          // double
+constexpr size_t NA_TOTAL = NA_HF4 + (size_t)NOALLOC_PMAX;       // 3.6 MiB in all
+
+static __device__ __align__(256) double g_noalloc_scratch[NA_TOTAL];
+
+// Copies the caller's rows into the kernel's layout and checks the lists:
+// 0 <= pptot <= pp_limit (rows the context entry point would complete with a
+// tree walk are refused here) and every listed id in 0..n-1.
+__global__ void k_noalloc_pack(int n, const double* __restrict__ parray,
+                               const double* __restrict__ v, const int* __restrict__ pptot,
+                               const int* __restrict__ pplist, int L, double4* __restrict__ pm,
+                               double2* __restrict__ hz, double4* __restrict__ vel,
+                               DevError* err) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double* r = parray + (size_t)i * 6;
+  pm[i] = make_double4(r[0], r[1], r[2], r[3]);
+  hz[i] = make_double2(r[4], r[5]);
+  const double* u = v + (size_t)i * 3;
+  vel[i] = make_double4(u[0], u[1], u[2], 0.0);
+  const int nn = pptot[i];
+  if (nn < 0 || nn > L) {
+    set_error(err, SEREN_GPU_ERR_CAPACITY, KID_HYDRO, i, nn);
+    return;
+  }
+  const int* row = pplist + (size_t)i * L;
+  for (int k = 0; k < nn; ++k) {
+    const int q = row[k];
+    if (q < 0 || q >= n) {
+      set_error(err, SEREN_GPU_ERR_ARG, KID_HYDRO, i, q);
+      return;
+    }
+  }
+}
+
+struct NoallocDevice {
+  bool ready = false;
+  double* base = nullptr;   // device address of g_noalloc_scratch
+};
+
+std::mutex g_noalloc_mutex;
+NoallocDevice g_noalloc_dev[64];
+
+// Once per device, with that device current: the device address of the
+// scratch array (the host-side name is only a stand-in) and the two kernel
+// tables, which stay in the array from then on.
+int noalloc_setup(int dev, double** base) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  NoallocDevice& d = g_noalloc_dev[dev];
+  if (d.ready) {
+    *base = d.base;
+    return SEREN_GPU_OK;
+  }
+  double* ptr = nullptr;
+  if (cudaGetSymbolAddress((void**)&ptr, g_noalloc_scratch) != cudaSuccess || !ptr)
+    return SEREN_GPU_ERR_CUDA;
+  for (int kernel = 0; kernel < 2; ++kernel) {
+    std::vector<double> w0, w1, w4, w5, w6, wh, wg;
+    make_kernel_tables(kernel, w0, w1, w4, w5, w6, wh, wg);
+    std::vector<double4> tg(KERNTOT + 1);
+    for (int i = 0; i <= KERNTOT; ++i) tg[i] = make_double4(w5[i], w4[i], w6[i], w1[i]);
+    if (cudaMemcpy(ptr + NA_TAB + kernel * NA_TABLEN, tg.data(), sizeof(double4) * tg.size(),
+                   cudaMemcpyHostToDevice) != cudaSuccess)
+      return SEREN_GPU_ERR_CUDA;
+  }
+  d.base = ptr;
+  d.ready = true;
+  *base = ptr;
+  return SEREN_GPU_OK;
+}
+
+int noalloc_status(cudaStream_t st, const DevError* d_err) {
+  DevError e{};
+  const cudaError_t rc1 = cudaMemcpyAsync(&e, d_err, sizeof(DevError), cudaMemcpyDeviceToHost, st);
+  const cudaError_t rc2 = cudaStreamSynchronize(st);
+  if (rc1 != cudaSuccess || rc2 != cudaSuccess || cudaGetLastError() != cudaSuccess)
+    return SEREN_GPU_ERR_CUDA;
+  return e.code;
+}
+
+}  // namespace
+}  // namespace seren
+
+extern "C" int seren_gpu_hydro_forces_noalloc(int32_t n, const double* parray, const double* v,
+                                              const double* rho, const double* omega,
+                                              const double* press, const double* sound,
+                                              const int32_t* pptot, const int32_t* pplist,
+                                              int32_t pp_limit, int32_t kernel, int32_t precision,
+                                              double alpha, double* a, void* stream) {
+  using namespace seren;
+  if (n < 0 || pp_limit < 1 || (kernel != 0 && kernel != 1) ||
+      (precision != 0 && precision != 1) || !(alpha >= 0.0))
+    return SEREN_GPU_ERR_ARG;
+  if (n > NOALLOC_PMAX) return SEREN_GPU_ERR_CAPACITY;
+  if (n == 0) return SEREN_GPU_OK;
+  if (!parray || !v || !rho || !omega || !press || !sound || !pptot || !pplist || !a)
+    return SEREN_GPU_ERR_ARG;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return SEREN_GPU_ERR_CUDA;
+  double* base = nullptr;
+  int rc = noalloc_setup(dev, &base);
+  if (rc) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  DevError* d_err = reinterpret_cast<DevError*>(base + NA_ERR);
+  double4* pm = reinterpret_cast<double4*>(base + NA_PM);
+  double2* hz = reinterpret_cast<double2*>(base + NA_HZ);
+  double4* vel = reinterpret_cast<double4*>(base + NA_VEL);
+  double* pf = base + NA_PF;
+  double* hf4 = base + NA_HF4;
+  const double4* tab = reinterpret_cast<const double4*>(base + NA_TAB + kernel * NA_TABLEN);
+  // the array keeps the previous call's contents: only the error block must start at zero
+  if (cudaMemsetAsync(d_err, 0, sizeof(DevError), st) != cudaSuccess) return SEREN_GPU_ERR_CUDA;
+  k_noalloc_pack<<<nb(n, 256), 256, 0, st>>>(n, parray, v, pptot, pplist, pp_limit, pm, hz, vel,
+                                              d_err);
+  if ((rc = noalloc_status(st, d_err))) return rc;
+  k_hydro_prep<<<nb(n, 256), 256, 0, st>>>(n, hz, rho, omega, press, pf, hf4);
+  const HydroTree none{};   // every row fits its list, so the kernel never walks a tree
+  if (precision == 0)
+    k_hydro<false><<<nb(n, 128), 128, 0, st>>>(n, nullptr, pm, hz, vel, rho, pf, hf4, sound,
+                                                 pptot, pplist, pp_limit, none, tab, alpha,
+                                                 kernel == 1, a, d_err);
+  else
+    k_hydro<true><<<nb(n, 128), 128, 0, st>>>(n, nullptr, pm, hz, vel, rho, pf, hf4, sound,
+                                                pptot, pplist, pp_limit, none, tab, alpha,
+                                                kernel == 1, a, d_err);
+  return noalloc_status(st, d_err);
+}
