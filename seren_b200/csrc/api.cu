@@ -233,7 +233,7 @@ int alloc_all(Ctx& c) {
          alloc(c.hmax, C) | alloc(c.bbmin, C) | alloc(c.bbmax, C);
   bad |= alloc(c.d_info, 1) | alloc(c.d_err, 1) | alloc(c.d_counts, 32);
   bad |= alloc(c.tabA, KERNTOT + 1) | alloc(c.tabG, KERNTOT + 1);
-  c.wstack_slots = grav_walk_slots(c);
+  c.wstack_slots = std::max(grav_walk_slots(c), hydro_walk_slots(c));
   c.wstack_cap = grav_walk_stack_cap(c);
   bad |= alloc(c.wstack, (size_t)c.wstack_slots * c.wstack_cap);
   if (bad) return -1;

@@ -133,6 +133,7 @@ void launch_gradh(Ctx& c, int nact);
 void launch_neib(Ctx& c, int nact);
 void launch_hydro(Ctx& c, int nact);
 void launch_thermal(Ctx& c);
+int hydro_walk_slots(const Ctx& c);     // resident warps of the grad-h / neighbour grids
 
 // gravity.cu
 void launch_grav(Ctx& c, int nact, int nsink, const double* d_sinks);

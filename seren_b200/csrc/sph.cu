@@ -1,16 +1,20 @@
 // sph.cu - grad-h smoothing length / density solve, neighbour lists, grad-h
 // hydro forces with MON97 viscosity, and the isothermal equation of state.
 //
-// One thread owns one active particle and follows its reference routine step
-// by step.  The candidate lists of the reference (BHhydrowalk_hgather,
-// BHhydro_walk) are never materialised: the stackless walk is re-run and each
-// opened leaf's particles are consumed as they come, which visits candidates
-// in exactly the reference's list order (depth-first leaf order, particles in
-// leaf order), so every sum is accumulated in the reference's order.
+// grad-h and the neighbour lists run on group walks: a warp walks the tree
+// for 32 neighbouring particles at once with each lane's own test, so every
+// lane opens exactly the leaves of its own reference walk (BHhydrowalk_hgather,
+// BHhydro_walk); the lanes then run their reference routines over the shared
+// list of opened leaves.  Neighbour lists come out in the reference's order
+// (depth-first leaf order, particles in leaf order); density sums only differ
+// from the reference's in the order of their terms.  The hydro force kernel
+// gives one thread to one particle and follows hydro_gradh step by step.
+#include <algorithm>
 #include <mutex>
 #include <vector>
 
 #include "ctx.cuh"
+#include "kernel_fns.h"
 
 namespace seren {
 
@@ -260,33 +264,12 @@ __device__ void gradh_one(int p, const double4* __restrict__ pm, double2* __rest
 }
 
 // ---------------------------------------------------------------------------
-// Warp-per-particle search.  A warp takes one particle at a time: the walk of
-// the reference (BHhydrowalk_hgather / BHhydro_walk) runs breadth-first with
-// the lanes spread over the cells of each level, and the particle's candidates
-// are then processed 32 at a time (coalesced loads) with the per-lane partial
-// sums reduced at the end.  The set of opened leaves is exactly the
-// reference's (a leaf is reached only through cells that passed the test);
-// only the order of the floating-point sums differs.  Warps take chunks of
-// particles from a global counter.
-//
 // Cell tests run first in FP32 on coordinates relative to the root centre:
 // test32() decides when the FP32 distance is outside a margin around the
 // threshold that covers every FP32 rounding involved (coordinates within
 // delta, the difference, the squares, the sum and the threshold itself), and
 // the test is redone in FP64 exactly as the reference writes it otherwise.
-constexpr int WP_THREADS = 128;
-constexpr int WP_WARPS = WP_THREADS / 32;
-constexpr int WP_FCAP = 512;     // cells of one level of the walk
-constexpr int WP_LCAP = 256;     // opened leaves (a power of two: the sort pads to it)
-constexpr int WP_CCAP = 1024;    // candidate particles
-constexpr int WP_CHUNK = 8;      // particles per grab from the work counter
 constexpr unsigned FULL = 0xffffffffu;
-
-struct WpShared {
-  int front[2][WP_FCAP];
-  int leaves[WP_LCAP];
-  int cand[WP_CCAP];
-};
 
 // 1: d2 <= T^2 for sure, 0: d2 > T^2 for sure, -1: too close to tell in FP32
 __device__ __forceinline__ int test32(float d2, float T, float delta) {
@@ -304,226 +287,6 @@ __device__ __forceinline__ int warp_iscan(int v, int lane) {
     if (lane >= o) v += y;
   }
   return v;
-}
-
-// sum over the warp, the same value on every lane (lane 0's reduction)
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(FULL, v, o);
-  return __shfl_sync(FULL, v, 0);
-}
-
-// Breadth-first walk of one particle's search; returns the number of opened
-// leaves (codes pstart*8 + count-1 in s.leaves) or -1 when a buffer overflows;
-// cnt = the particles in the opened leaves.
-template <class Test>
-__device__ int wp_walk(const HydroTree& t, int lane, WpShared& s, int& cnt,
-                       unsigned long long& nvisit, Test&& test) {
-  int* fa = s.front[0];
-  int* fb = s.front[1];
-  __syncwarp();
-  if (lane == 0) fa[0] = 0;
-  __syncwarp();
-  int nf = 1, nleaf = 0, mine = 0;
-  bool over = false;
-  while (nf > 0) {
-    int nnext = 0;
-    for (int base = 0; base < nf; base += 32) {
-      const int idx = base + lane;
-      const bool valid = idx < nf;
-      const int c = valid ? fa[idx] : 0;
-      const bool pass = valid && test(c);
-      const int4 lk = t.link[c];
-      const bool isleaf = pass && lk.x > 0;
-      const bool isbr = pass && lk.x == 0;
-      const unsigned ml = __ballot_sync(FULL, isleaf);
-      if (isleaf) {
-        const int pos = nleaf + __popc(ml & ((1u << lane) - 1u));
-        if (pos < WP_LCAP) s.leaves[pos] = lk.w * 8 + (lk.x - 1);
-        mine += lk.x;
-      }
-      nleaf += __popc(ml);
-      const int nk = isbr ? t.nkids[c] : 0;
-      const int sc = warp_iscan(nk, lane);
-      if (isbr) {
-        const int o = nnext + sc - nk;
-        for (int j = 0; j < nk; ++j)
-          if (o + j < WP_FCAP) fb[o + j] = lk.z + j;
-      }
-      nnext += __shfl_sync(FULL, sc, 31);
-    }
-    nvisit += nf;
-    __syncwarp();
-    if (nnext > WP_FCAP) over = true;
-    int* tmp = fa;
-    fa = fb;
-    fb = tmp;
-    nf = over ? 0 : nnext;
-  }
-  cnt = warp_iscan(mine, lane);
-  cnt = __shfl_sync(FULL, cnt, 31);
-  return (over || nleaf > WP_LCAP) ? -1 : nleaf;
-}
-
-// leaves -> candidate particle ids, in leaf order; returns the count (may
-// exceed WP_CCAP: overflow)
-__device__ int wp_flatten(int nleaf, int lane, WpShared& s) {
-  int total = 0;
-  for (int base = 0; base < nleaf; base += 32) {
-    const int k = base + lane;
-    const int code = k < nleaf ? s.leaves[k] : 0;
-    const int n = k < nleaf ? (code & 7) + 1 : 0;
-    const int sc = warp_iscan(n, lane);
-    const int o = total + sc - n;
-    for (int j = 0; j < n; ++j)
-      if (o + j < WP_CCAP) s.cand[o + j] = (code >> 3) + j;
-    total += __shfl_sync(FULL, sc, 31);
-  }
-  __syncwarp();
-  return total;
-}
-
-// ascending bitonic sort of s.leaves[0..n) (n <= WP_LCAP): depth-first leaf
-// order, which is the order of the reference's candidate lists
-__device__ void wp_sort_leaves(int n, int lane, WpShared& s) {
-  int N = 1;
-  while (N < n) N <<= 1;
-  for (int k = n + lane; k < N; k += 32) s.leaves[k] = 0x7fffffff;
-  __syncwarp();
-  for (int size = 2; size <= N; size <<= 1) {
-    for (int stride = size >> 1; stride > 0; stride >>= 1) {
-      for (int i = lane; i < (N >> 1); i += 32) {
-        const int lo = 2 * i - (i & (stride - 1));
-        const int hi = lo + stride;
-        const bool up = (lo & size) == 0;
-        const int x = s.leaves[lo], y = s.leaves[hi];
-        if ((x > y) == up) {
-          s.leaves[lo] = y;
-          s.leaves[hi] = x;
-        }
-      }
-      __syncwarp();
-    }
-  }
-}
-
-__device__ __forceinline__ int grab(int* work, int lane) {
-  int b = 0;
-  if (lane == 0) b = atomicAdd(work, WP_CHUNK);
-  return __shfl_sync(FULL, b, 0);
-}
-
-// sph/all_sph_gradh.F90:11-492, one warp per particle
-__global__ void __launch_bounds__(WP_THREADS) k_gradh_wp(
-    int nact, const int* __restrict__ act, const double4* __restrict__ pm, double2* __restrict__ hz,
-    const double4* __restrict__ vel, double* __restrict__ rho, double* __restrict__ omega,
-    double* __restrict__ divv, double* __restrict__ drhodt, HydroTree t,
-    const double4* __restrict__ tabA, double h_fac, int pp_gather, double rextent, DevError* err,
-    unsigned long long* counts, int* work) {
-  __shared__ WpShared sh[WP_WARPS];
-  const int lane = threadIdx.x & 31;
-  WpShared& S = sh[threadIdx.x >> 5];
-  const double4 t0 = tabA[0];
-  unsigned long long nwalk = 0, nvisit = 0, npass = 0, ncands = 0;
-  for (int base = grab(work, lane); base < nact; base = grab(work, lane)) {
-    const int end = min(base + WP_CHUNK, nact);
-    for (int i = base; i < end; ++i) {
-      const int p = act ? act[i] : i;
-      const double4 P = pm[p];
-      const double rx = P.x, ry = P.y, rz = P.z, mp = P.w;
-      const float px = (float)(rx - t.rootx), py = (float)(ry - t.rooty),
-                  pz = (float)(rz - t.rootz);
-      GhState s;
-      gh_init(s, hz[p].x, rextent);
-      double R = 0.0;
-      float R32 = 0.0f;
-      auto gather_test = [&](int c) {                 // BHhydrowalk_hgather.F90:36-40
-        const float4 h32 = t.hA32[c];
-        const float d0 = h32.x - px, d1 = h32.y - py, d2 = h32.z - pz;
-        const int r = test32((d0 * d0 + d1 * d1) + d2 * d2, R32 + h32.w, t.delta);
-        if (r >= 0) return r == 1;
-        const double4 h = t.hA[c];
-        const double e0 = h.x - rx, e1 = h.y - ry, e2 = h.z - rz;
-        const double tt = R + h.w;
-        return ((e0 * e0 + e1 * e1) + e2 * e2) <= tt * tt;
-      };
-      int ncand = 0;
-      bool over = false, bad = false;
-      while (true) {
-        while (true) {                                                 // :154-191
-          if (s.hp > s.h_high) {
-            s.h_high = s.hp * HMULT;
-            R = KERNRANGE * s.h_high;
-            R32 = (float)R;
-            int cnt = 0;
-            ++nwalk;
-            const int nl = wp_walk(t, lane, S, cnt, nvisit, gather_test);
-            if (nl < 0) { over = true; break; }
-            ncand = wp_flatten(nl, lane, S);
-            if (ncand > WP_CCAP) { over = true; break; }
-            s.pp_pot = cnt;
-          }
-          if (s.pp_pot < pp_gather) {
-            s.h_high = 0.0;
-            s.pp_pot = 0;
-            s.hp = s.hp * HMULT;
-            if (++s.ngrow > HGROW_CAP) { bad = true; break; }
-          }
-          if (s.pp_pot > 0) break;
-        }
-        if (over || bad) break;
-        const double ih = 1.0 / s.hp;                                  // :199-235
-        const double hf = pow(ih, NDIMPR);
-        const double hs = (KERNRANGESQD * s.hp) * s.hp;
-        double part = 0.0;
-        for (int k = lane; k < ncand; k += 32) {
-          const int q = S.cand[k];
-          if (q != p) gh_density_term(pm[q], rx, ry, rz, hs, ih, hf, tabA, part);
-        }
-        const double rt = (mp * t0.x) * hf + warp_sum(part);
-        ++npass;
-        ncands += ncand;
-        if (gh_after_pass(s, mp, h_fac, rextent, rt)) break;
-      }
-      if (bad) {
-        if (lane == 0) set_error(err, SEREN_GPU_ERR_WALK, KID_GRADH, p, -1);
-        continue;
-      }
-      if (over) {
-        if (lane == 0)
-          gradh_one(p, pm, hz, vel, rho, omega, divv, drhodt, t, tabA, h_fac, pp_gather, rextent,
-                    err);
-        __syncwarp();
-        continue;
-      }
-      const double hp = h_fac * pow(mp / s.rho, ONETHIRD);            // :317-425
-      const double ih = 1.0 / hp;
-      const double hf = pow(ih, NDIMPR);
-      const double hs = (KERNRANGESQD * hp) * hp;
-      const double4 vp = vel[p];
-      GhFinal f;
-      f.rt = 0.0; f.om = 0.0; f.dv = 0.0; f.zt = 0.0;
-      for (int k = lane; k < ncand; k += 32) {
-        const int q = S.cand[k];
-        if (q != p) gh_final_term(pm[q], vel[q], rx, ry, rz, vp, hs, ih, hf, tabA, f);
-      }
-      GhFinal g;
-      gh_final_init(g, mp, ih, hf, t0);
-      g.rt = g.rt + warp_sum(f.rt);
-      g.om = g.om + warp_sum(f.om);
-      g.dv = g.dv + warp_sum(f.dv);
-      g.zt = g.zt + warp_sum(f.zt);
-      ++npass;
-      ncands += ncand;
-      if (lane == 0) gh_store(p, mp, hp, g, hz, rho, omega, divv, drhodt, err);
-    }
-  }
-  if (lane == 0) {
-    atomicAdd(counts + 3, nwalk);
-    atomicAdd(counts + 4, nvisit);
-    atomicAdd(counts + 5, npass);
-    atomicAdd(counts + 6, ncands);
-  }
 }
 
 // ---------------------------------------------------------------------------
@@ -552,78 +315,433 @@ __device__ void neib_one(int p, const double4* __restrict__ pm, const double2* _
   pptot[p] = cnt;
 }
 
-__global__ void __launch_bounds__(WP_THREADS) k_neib_wp(
+// ---------------------------------------------------------------------------
+// Group search.  A warp takes 32 consecutive active particles (tree order:
+// spatially adjacent) and walks the tree for all of them at once: the walk
+// state is a per-warp stack of (cell, mask) entries, the mask holding the
+// lanes whose own walk reaches the cell; each step pops up to 32 entries,
+// loads those cells in parallel, and every lane in an entry's mask runs its
+// own particle's test on it (test32 in FP32, exact FP64 otherwise).  A cell
+// that passes for some lanes is opened for exactly those lanes, so the leaves
+// each lane opens are exactly those of its own reference walk.  Opened leaves
+// go to a per-warp list of (leaf, mask) entries; the passes over the
+// candidates then run once per entry for the whole warp (uniform loads of the
+// leaf's particles), each lane adding the terms of the particles whose entry
+// holds its bit.
+constexpr int GR_THREADS = 128;
+constexpr int GR_WARPS = GR_THREADS / 32;
+constexpr int GR_LCAP = 512;     // (leaf, mask) entries per warp
+
+struct GrShared {
+  int code[GR_LCAP];       // leaf: pstart*8 + count-1
+  unsigned mask[GR_LCAP];  // lanes whose walk opened the leaf
+  float4 fa[32];           // popped cells: hA32
+  float fh[32];            // hrm32
+  unsigned fm[32];         // lanes whose walk reaches the cell
+  int fc[32];
+  int cq[32];              // staged candidates: particle
+  unsigned cm[32];         //   lanes that take it
+  double4 cp[32];          //   position, mass
+  double4 cv[32];          //   velocity (final pass)
+};
+
+// Walk for the lanes in `lanes`, appending the opened leaves to R.code/R.mask
+// from nent on.  test(e) is this lane's test of popped cell e (R.fa[e],
+// R.fh[e], R.fc[e]).  Returns the new entry count, or -1 when the list or the
+// stack would overflow (nothing beyond the old count is then valid).
+template <class Test>
+__device__ int gr_walk(const HydroTree& t, unsigned lanes, int2* S, int scap, GrShared& R,
+                       int lane, int nent, unsigned long long& nvisit, Test&& test) {
+  const unsigned lt = (1u << lane) - 1u;
+  __syncwarp();
+  if (lane == 0) S[0] = make_int2(0, (int)lanes);
+  int sp = 1;
+  long long gent = 0;
+  while (sp > 0) {
+    __syncwarp();
+    const int k = min(32, sp);
+    sp -= k;
+    gent += k;
+    int nk = 0;
+    unsigned m = 0;
+    int4 lk = make_int4(-1, 0, 0, 0);
+    if (lane < k) {
+      const int2 ent = S[sp + lane];
+      const int cc = ent.x;
+      m = (unsigned)ent.y;
+      lk = t.link[cc];
+      R.fa[lane] = t.hA32[cc];
+      R.fh[lane] = t.hrm32[cc];
+      R.fm[lane] = m;
+      R.fc[lane] = cc;
+      if (lk.x == 0) nk = t.nkids[cc];
+    }
+    __syncwarp();
+    unsigned mpass = 0;
+    for (int e = 0; e < k; ++e) {
+      const bool pass = ((R.fm[e] >> lane) & 1u) && test(e);
+      const unsigned b = __ballot_sync(FULL, pass);
+      if (lane == e) mpass = b;
+    }
+    nvisit += k;
+    const bool isleaf = lk.x > 0 && mpass != 0u;              // candidates of the lanes in mpass
+    const unsigned bl = __ballot_sync(FULL, isleaf);
+    if (nent + __popc(bl) > GR_LCAP) return -1;
+    if (isleaf) {
+      const int o = nent + __popc(bl & lt);
+      R.code[o] = lk.w * 8 + (lk.x - 1);
+      R.mask[o] = mpass;
+    }
+    nent += __popc(bl);
+    const int nch = (lk.x == 0 && mpass != 0u) ? nk : 0;      // opened for the lanes in mpass
+    const int cin = warp_iscan(nch, lane);
+    const int ctotal = __shfl_sync(FULL, cin, 31);
+    if (sp + ctotal > scap || gent > (long long)t.ctot + 1) return -1;
+    for (int q = 0; q < nch; ++q) S[sp + cin - nch + q] = make_int2(lk.z + q, (int)mpass);
+    sp += ctotal;
+  }
+  __syncwarp();
+  return nent;
+}
+
+// Clears the bits of `lanes` from the list and drops emptied entries (order kept).
+__device__ int gr_drop(GrShared& R, int nent, unsigned lanes, int lane) {
+  const unsigned lt = (1u << lane) - 1u;
+  __syncwarp();
+  int out = 0;
+  for (int base = 0; base < nent; base += 32) {
+    const int e = base + lane;
+    int code = 0;
+    unsigned m = 0;
+    if (e < nent) {
+      code = R.code[e];
+      m = R.mask[e] & ~lanes;
+    }
+    const unsigned b = __ballot_sync(FULL, m != 0u);
+    __syncwarp();
+    if (m != 0u) {
+      const int o = out + __popc(b & lt);
+      R.code[o] = code;
+      R.mask[o] = m;
+    }
+    out += __popc(b);
+  }
+  __syncwarp();
+  return out;
+}
+
+// particles in the leaves holding bit `bit` (the reference's pp_pot)
+__device__ __forceinline__ int gr_count(const GrShared& R, int nent, unsigned bit) {
+  int n = 0;
+  for (int e = 0; e < nent; ++e)
+    if (R.mask[e] & bit) n += (R.code[e] & 7) + 1;
+  return n;
+}
+
+// ascending bitonic sort of the entries by leaf (depth-first leaf order, the
+// order of the reference's candidate lists), masks carried along
+__device__ void gr_sort(GrShared& R, int n, int lane) {
+  int N = 1;
+  while (N < n) N <<= 1;
+  for (int k = n + lane; k < N; k += 32) {
+    R.code[k] = 0x7fffffff;
+    R.mask[k] = 0u;
+  }
+  __syncwarp();
+  for (int size = 2; size <= N; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int i = lane; i < (N >> 1); i += 32) {
+        const int lo = 2 * i - (i & (stride - 1));
+        const int hi = lo + stride;
+        const bool up = (lo & size) == 0;
+        const int x = R.code[lo], y = R.code[hi];
+        if ((x > y) == up) {
+          const unsigned mx = R.mask[lo], my = R.mask[hi];
+          R.code[lo] = y; R.code[hi] = x;
+          R.mask[lo] = my; R.mask[hi] = mx;
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+// Stages the candidates of the next entries from e0 whose mask meets A, up to
+// 32 particles (whole leaves), into R.cq/R.cm and, through load(slot, q), the
+// particle data: one particle per lane, loaded in parallel.  Returns the count
+// and advances e0.
+template <class Load>
+__device__ int gr_stage(GrShared& R, int& e0, int nent, unsigned A, int lane, Load&& load) {
+  const int e = e0 + lane;
+  int cnt = 0, code = 0;
+  unsigned m = 0;
+  if (e < nent) {
+    m = R.mask[e] & A;
+    code = R.code[e];
+    cnt = m != 0u ? (code & 7) + 1 : 0;
+  }
+  const int inc = warp_iscan(cnt, lane);
+  const unsigned take = __ballot_sync(FULL, e < nent && inc <= 32);   // a prefix of the lanes
+  const int ntake = __popc(take);
+  const int total = ntake > 0 ? __shfl_sync(FULL, inc, ntake - 1) : 0;
+  __syncwarp();
+  if (((take >> lane) & 1u) && cnt > 0) {
+    const int o = inc - cnt;
+    for (int k = 0; k < cnt; ++k) {
+      R.cq[o + k] = (code >> 3) + k;
+      R.cm[o + k] = m;
+    }
+  }
+  e0 += ntake;
+  __syncwarp();
+  if (lane < total) load(lane, R.cq[lane]);
+  __syncwarp();
+  return total;
+}
+
+// gh_density_term and gh_final_term with the kernel bins evaluated in place
+// (kernel_fns.h, the same values as the tables)
+__device__ __forceinline__ void gh_density_term_k(const double4& Q, double rx, double ry,
+                                                  double rz, double hs, double ih, double hf,
+                                                  double& rt) {
+  const double d0 = Q.x - rx, d1 = Q.y - ry, d2 = Q.z - rz;
+  const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
+  if (drsqd >= hs) return;
+  const double drmag = sqrt(drsqd) + SMALL_NUMBER;
+  const int kern = (int)((HALFKERNTOT * drmag) * ih);
+  if (kern >= KERNTOT) return;
+  rt = rt + (Q.w * hf) * kfn::w0(kern);
+}
+
+__device__ __forceinline__ void gh_final_term_k(const double4& Q, const double4& V, double rx,
+                                                double ry, double rz, const double4& vp,
+                                                double hs, double ih, double hf, GhFinal& f) {
+  const double d0 = Q.x - rx, d1 = Q.y - ry, d2 = Q.z - rz;
+  double drmag = (d0 * d0 + d1 * d1) + d2 * d2;
+  if (drmag > hs) return;
+  drmag = sqrt(drmag) + SMALL_NUMBER;
+  const int kern = (int)((HALFKERNTOT * drmag) * ih);
+  if (kern > KERNTOT) return;
+  const double dv0 = V.x - vp.x, dv1 = V.y - vp.y, dv2 = V.z - vp.z;
+  const double dvdr = (dv0 * d0 + dv1 * d1) + dv2 * d2;
+  f.rt = f.rt + (Q.w * hf) * kfn::w0(kern);
+  f.om = f.om + ((Q.w * hf) * ih) * kfn::wh(kern);
+  f.dv = f.dv - ((((Q.w * dvdr) * kfn::w4(kern)) * hf) * ih) / drmag;
+  f.zt = f.zt + ((Q.w * ih) * ih) * kfn::wg(kern);
+}
+
+__device__ __forceinline__ int gr_next(int* work, int lane) {
+  int g = 0;
+  if (lane == 0) g = atomicAdd(work, 1);
+  return __shfl_sync(FULL, g, 0);
+}
+
+// sph/all_sph_gradh.F90:11-492 for 32 particles per warp.  Each lane runs its
+// particle's iteration (:132-285) on its own bits of the shared list; lanes
+// whose h outgrows their last walk (:154-191) are walked again together, their
+// old bits cleared first.
+__global__ void __launch_bounds__(GR_THREADS) k_gradh_grp(
+    int nact, const int* __restrict__ act, const double4* __restrict__ pm, double2* __restrict__ hz,
+    const double4* __restrict__ vel, double* __restrict__ rho, double* __restrict__ omega,
+    double* __restrict__ divv, double* __restrict__ drhodt, HydroTree t,
+    const double4* __restrict__ tabA, double h_fac, int pp_gather, double rextent,
+    int2* __restrict__ stacks, int scap, DevError* err, unsigned long long* counts, int* work) {
+  __shared__ GrShared sh[GR_WARPS];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  GrShared& R = sh[w];
+  int2* const S = stacks + (size_t)(blockIdx.x * GR_WARPS + w) * scap;
+  const unsigned bit = 1u << lane;
+  const double4 t0 = tabA[0];
+  unsigned long long nwalk = 0, nvisit = 0, npass = 0, ncands = 0;
+  for (int g = gr_next(work, lane); (long long)g * 32 < nact; g = gr_next(work, lane)) {
+    const int i = g * 32 + lane;
+    const bool live = i < nact;
+    const int p = live ? (act ? act[i] : i) : (act ? act[nact - 1] : nact - 1);
+    const double4 P = pm[p];
+    const double rx = P.x, ry = P.y, rz = P.z, mp = P.w;
+    const float px = (float)(rx - t.rootx), py = (float)(ry - t.rooty), pz = (float)(rz - t.rootz);
+    GhState s;
+    gh_init(s, hz[p].x, rextent);
+    double Rw = 0.0;
+    float R32 = 0.0f;
+    auto gather_test = [&](int e) {                    // BHhydrowalk_hgather.F90:36-40
+      const float4 h32 = R.fa[e];
+      const float d0 = h32.x - px, d1 = h32.y - py, d2 = h32.z - pz;
+      const int r = test32((d0 * d0 + d1 * d1) + d2 * d2, R32 + h32.w, t.delta);
+      if (r >= 0) return r == 1;
+      const double4 h = t.hA[R.fc[e]];
+      const double e0 = h.x - rx, e1 = h.y - ry, e2 = h.z - rz;
+      const double tt = Rw + h.w;
+      return ((e0 * e0 + e1 * e1) + e2 * e2) <= tt * tt;
+    };
+    bool active = live;        // still iterating
+    bool ok = live;            // ends with the final pass
+    bool single = false;       // list overflow: this lane runs gradh_one
+    int nent = 0;
+    while (__any_sync(FULL, active)) {
+      while (true) {                                                   // :154-191
+        const bool need = active && s.hp > s.h_high;
+        const unsigned W = __ballot_sync(FULL, need);
+        if (W) {
+          if (need) {
+            s.h_high = s.hp * HMULT;
+            Rw = KERNRANGE * s.h_high;
+            R32 = (float)Rw;
+            ++nwalk;
+          }
+          nent = gr_drop(R, nent, W, lane);
+          const int ne = gr_walk(t, W, S, scap, R, lane, nent, nvisit, gather_test);
+          if (ne < 0) {
+            if (need) { single = true; active = false; ok = false; }
+          } else {
+            nent = ne;
+            if (need) s.pp_pot = gr_count(R, nent, bit);
+          }
+        }
+        if (active && s.pp_pot < pp_gather) {
+          s.h_high = 0.0;
+          s.pp_pot = 0;
+          s.hp = s.hp * HMULT;
+          if (++s.ngrow > HGROW_CAP) {
+            set_error(err, SEREN_GPU_ERR_WALK, KID_GRADH, p, -1);
+            active = false;
+            ok = false;
+          }
+        }
+        if (!__any_sync(FULL, active && s.pp_pot == 0)) break;
+      }
+      const unsigned A = __ballot_sync(FULL, active);
+      if (A == 0u) break;
+      const double ih = 1.0 / s.hp;                                    // :199-235
+      const double hf = pow(ih, NDIMPR);
+      const double hs = (KERNRANGESQD * s.hp) * s.hp;
+      double rt = (mp * t0.x) * hf;
+      for (int e0 = 0; e0 < nent;) {
+        const int nc = gr_stage(R, e0, nent, A, lane, [&](int j, int q) { R.cp[j] = pm[q]; });
+        for (int j = 0; j < nc; ++j) {
+          const double4 Q = R.cp[j];
+          if ((R.cm[j] & bit) && R.cq[j] != p) gh_density_term_k(Q, rx, ry, rz, hs, ih, hf, rt);
+        }
+      }
+      if (active) {
+        ++npass;
+        ncands += s.pp_pot;
+        if (gh_after_pass(s, mp, h_fac, rextent, rt)) active = false;
+      }
+    }
+    // final pass (:317-425) on each lane's last candidate list
+    const unsigned F = __ballot_sync(FULL, ok);
+    const double hp = h_fac * pow(mp / s.rho, ONETHIRD);
+    const double ih = 1.0 / hp;
+    const double hf = pow(ih, NDIMPR);
+    const double hs = (KERNRANGESQD * hp) * hp;
+    const double4 vp = vel[p];
+    GhFinal f;
+    gh_final_init(f, mp, ih, hf, t0);
+    for (int e0 = 0; e0 < nent;) {
+      const int nc = gr_stage(R, e0, nent, F, lane, [&](int j, int q) {
+        R.cp[j] = pm[q];
+        R.cv[j] = vel[q];
+      });
+      for (int j = 0; j < nc; ++j) {
+        const double4 Q = R.cp[j];
+        const double4 V = R.cv[j];
+        if ((R.cm[j] & bit) && R.cq[j] != p) gh_final_term_k(Q, V, rx, ry, rz, vp, hs, ih, hf, f);
+      }
+    }
+    if (ok) {
+      ++npass;
+      ncands += s.pp_pot;
+      gh_store(p, mp, hp, f, hz, rho, omega, divv, drhodt, err);
+    }
+    if (single)
+      gradh_one(p, pm, hz, vel, rho, omega, divv, drhodt, t, tabA, h_fac, pp_gather, rextent, err);
+    __syncwarp();
+  }
+  atomicAdd(counts + 3, nwalk);
+  atomicAdd(counts + 5, npass);
+  atomicAdd(counts + 6, ncands);
+  if (lane == 0) atomicAdd(counts + 4, nvisit);
+}
+
+// get_neib (sph/get_neib.F90:10-140) for 32 particles per warp: one group walk
+// with each lane's gather-or-scatter test (BHhydro_walk.F90:37-43), the opened
+// leaves sorted into depth-first order, then each lane keeps the candidates
+// with r^2 <= 4h_p^2 or r^2 <= 4h_pp^2 in that order.
+__global__ void __launch_bounds__(GR_THREADS) k_neib_grp(
     int nact, const int* __restrict__ act, const double4* __restrict__ pm,
     const double2* __restrict__ hz, HydroTree t, int L, int* __restrict__ pptot,
-    int* __restrict__ pplist, DevError* err, unsigned long long* counts, int* work) {
-  __shared__ WpShared sh[WP_WARPS];
-  const int lane = threadIdx.x & 31;
-  WpShared& S = sh[threadIdx.x >> 5];
+    int* __restrict__ pplist, int2* __restrict__ stacks, int scap, DevError* err,
+    unsigned long long* counts, int* work) {
+  __shared__ GrShared sh[GR_WARPS];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  GrShared& R = sh[w];
+  int2* const S = stacks + (size_t)(blockIdx.x * GR_WARPS + w) * scap;
+  const unsigned bit = 1u << lane;
   unsigned long long nvisit = 0, ncands = 0;
-  for (int base = grab(work, lane); base < nact; base = grab(work, lane)) {
-    const int end = min(base + WP_CHUNK, nact);
-    for (int i = base; i < end; ++i) {
-      const int p = act ? act[i] : i;
-      const double4 P = pm[p];
-      const float px = (float)(P.x - t.rootx), py = (float)(P.y - t.rooty),
-                  pz = (float)(P.z - t.rootz);
-      const double hp = hz[p].x;
-      const double R = KERNRANGE * hp;
-      const float R32 = (float)R;
-      const double hsp = (KERNRANGESQD * hp) * hp;
-      int cnt = 0;
-      const int nl = wp_walk(t, lane, S, cnt, nvisit, [&](int c) {   // BHhydro_walk.F90:37-43
-        const float4 h32 = t.hA32[c];
-        const float d0 = h32.x - px, d1 = h32.y - py, d2 = h32.z - pz;
-        const float d2s = (d0 * d0 + d1 * d1) + d2 * d2;
-        const int r1 = test32(d2s, R32 + h32.w, t.delta);
-        const int r2 = test32(d2s, t.hrm32[c] + h32.w, t.delta);
-        if (r1 == 1 || r2 == 1) return true;
-        if (r1 == 0 && r2 == 0) return false;
-        const double4 h = t.hA[c];
-        const double e0 = h.x - P.x, e1 = h.y - P.y, e2 = h.z - P.z;
-        const double drsqd = (e0 * e0 + e1 * e1) + e2 * e2;
-        const double t1 = R + h.w;
-        const double t2 = t.hrm[c] + h.w;
-        return drsqd <= t1 * t1 || drsqd <= t2 * t2;
+  for (int g = gr_next(work, lane); (long long)g * 32 < nact; g = gr_next(work, lane)) {
+    const int i = g * 32 + lane;
+    const bool live = i < nact;
+    const int p = live ? (act ? act[i] : i) : (act ? act[nact - 1] : nact - 1);
+    const double4 P = pm[p];
+    const float px = (float)(P.x - t.rootx), py = (float)(P.y - t.rooty),
+                pz = (float)(P.z - t.rootz);
+    const double hp = hz[p].x;
+    const double Rw = KERNRANGE * hp;
+    const float R32 = (float)Rw;
+    const double hsp = (KERNRANGESQD * hp) * hp;
+    const unsigned lanes = __ballot_sync(FULL, live);
+    const int nent = gr_walk(t, lanes, S, scap, R, lane, 0, nvisit, [&](int e) {
+      const float4 h32 = R.fa[e];
+      const float d0 = h32.x - px, d1 = h32.y - py, d2 = h32.z - pz;
+      const float d2s = (d0 * d0 + d1 * d1) + d2 * d2;
+      const int r1 = test32(d2s, R32 + h32.w, t.delta);
+      const int r2 = test32(d2s, R.fh[e] + h32.w, t.delta);
+      if (r1 == 1 || r2 == 1) return true;
+      if (r1 == 0 && r2 == 0) return false;
+      const int c = R.fc[e];
+      const double4 h = t.hA[c];
+      const double e0 = h.x - P.x, e1 = h.y - P.y, e2 = h.z - P.z;
+      const double drsqd = (e0 * e0 + e1 * e1) + e2 * e2;
+      const double t1 = Rw + h.w;
+      const double t2 = t.hrm[c] + h.w;
+      return drsqd <= t1 * t1 || drsqd <= t2 * t2;
+    });
+    if (nent < 0) {
+      if (live) neib_one(p, pm, hz, t, L, pptot, pplist, err);
+      __syncwarp();
+      continue;
+    }
+    gr_sort(R, nent, lane);
+    int* row = pplist + (size_t)p * L;
+    int kept = 0;
+    for (int e0 = 0; e0 < nent;) {
+      const int nc = gr_stage(R, e0, nent, lanes, lane, [&](int j, int q) {
+        R.cp[j] = pm[q];
+        R.cv[j].x = hz[q].x;
       });
-      int ncand = -1;
-      if (nl >= 0) {
-        wp_sort_leaves(nl, lane, S);
-        ncand = wp_flatten(nl, lane, S);
-      }
-      if (nl < 0 || ncand > WP_CCAP) {
-        if (lane == 0) neib_one(p, pm, hz, t, L, pptot, pplist, err);
-        __syncwarp();
-        continue;
-      }
-      ncands += ncand;
-      int* row = pplist + (size_t)p * L;
-      int kept = 0;
-      for (int b = 0; b < ncand; b += 32) {
-        const int k = b + lane;
-        const int q = k < ncand ? S.cand[k] : p;
-        bool keep = false;
-        if (q != p) {
-          const double4 Q = pm[q];
-          const double hq = hz[q].x;
+      for (int j = 0; j < nc; ++j) {
+        const int q = R.cq[j];
+        const bool mine = (R.cm[j] & bit) != 0u;
+        ncands += mine ? 1 : 0;
+        if (mine && q != p) {
+          const double4 Q = R.cp[j];
+          const double hq = R.cv[j].x;
           const double hsq = (KERNRANGESQD * hq) * hq;
           const double d0 = Q.x - P.x, d1 = Q.y - P.y, d2 = Q.z - P.z;
           const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
-          keep = drsqd <= hsp || drsqd <= hsq;
+          if (drsqd <= hsp || drsqd <= hsq) {
+            if (kept < L) row[kept] = q;
+            ++kept;
+          }
         }
-        const unsigned m = __ballot_sync(FULL, keep);
-        const int pos = kept + __popc(m & ((1u << lane) - 1u));
-        if (keep && pos < L) row[pos] = q;
-        kept += __popc(m);
       }
-      if (lane == 0) pptot[p] = kept;
     }
+    if (live) pptot[p] = kept;
+    __syncwarp();
   }
-  if (lane == 0) {
-    atomicAdd(counts + 4, nvisit);
-    atomicAdd(counts + 7, ncands);
-  }
+  atomicAdd(counts + 7, ncands);
+  if (lane == 0) atomicAdd(counts + 4, nvisit);
 }
 
 // sph/hydro_gradh.F90:9-339 (NEIGHBOUR_LISTS, ARTIFICIAL_VISCOSITY=MON97).
@@ -812,20 +930,47 @@ HydroTree hydro_tree(const Ctx& c) {
 
 }  // namespace
 
-// persistent grid of warps taking particle chunks from a counter
-static int wp_grid(const Ctx& c, int nact) {
+// Resident blocks per SM of the group-walk kernels on device dev.
+static int gr_blocks_per_sm(int dev, int which) {
+  static int occ[16][2] = {};
+  int dummy[2] = {0, 0};
+  int* o = dev >= 0 && dev < 16 ? occ[dev] : dummy;
+  int& r = o[which];
+  if (r == 0) {
+    if (which == 0)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_gradh_grp, GR_THREADS, 0);
+    else
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_neib_grp, GR_THREADS, 0);
+    if (r < 1) r = 1;
+  }
+  return r;
+}
+
+static int sm_count(const Ctx& c) {
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c.dev);
-  const int want = nb(nact, WP_CHUNK * WP_WARPS);
-  return want < nsm * 8 ? want : nsm * 8;
+  return nsm;
+}
+
+int hydro_walk_slots(const Ctx& c) {
+  return sm_count(c) * std::max(gr_blocks_per_sm(c.dev, 0), gr_blocks_per_sm(c.dev, 1)) *
+         GR_WARPS;
+}
+
+// persistent grid of warps taking 32-particle groups from a counter, no more
+// warps than there are walk stacks
+static int gr_grid(const Ctx& c, int nact, int which) {
+  const int groups = nb(nact, 32);
+  int blocks = std::min(sm_count(c) * gr_blocks_per_sm(c.dev, which), nb(groups, GR_WARPS));
+  return std::max(1, std::min(blocks, c.wstack_slots / GR_WARPS));
 }
 
 void launch_gradh(Ctx& c, int nact) {
   if (nact <= 0) return;
   cudaMemsetAsync(c.work, 0, sizeof(int), c.st);
-  k_gradh_wp<<<wp_grid(c, nact), WP_THREADS, 0, c.st>>>(
+  k_gradh_grp<<<gr_grid(c, nact, 0), GR_THREADS, 0, c.st>>>(
       nact, c.act, c.pm, c.hz, c.vel, c.rho, c.omega, c.div_v, c.drhodt, hydro_tree(c), c.tabA,
-      c.prm.h_fac, c.prm.pp_gather, c.info.rextent, c.d_err,
+      c.prm.h_fac, c.prm.pp_gather, c.info.rextent, c.wstack, c.wstack_cap, c.d_err,
       reinterpret_cast<unsigned long long*>(c.d_counts), c.work);
   ++c.nlaunch;
 }
@@ -833,9 +978,9 @@ void launch_gradh(Ctx& c, int nact) {
 void launch_neib(Ctx& c, int nact) {
   if (nact <= 0) return;
   cudaMemsetAsync(c.work, 0, sizeof(int), c.st);
-  k_neib_wp<<<wp_grid(c, nact), WP_THREADS, 0, c.st>>>(
-      nact, c.act, c.pm, c.hz, hydro_tree(c), c.prm.pp_limit, c.pptot, c.pplist, c.d_err,
-      reinterpret_cast<unsigned long long*>(c.d_counts), c.work);
+  k_neib_grp<<<gr_grid(c, nact, 1), GR_THREADS, 0, c.st>>>(
+      nact, c.act, c.pm, c.hz, hydro_tree(c), c.prm.pp_limit, c.pptot, c.pplist, c.wstack,
+      c.wstack_cap, c.d_err, reinterpret_cast<unsigned long long*>(c.d_counts), c.work);
   ++c.nlaunch;
 }
 
