@@ -324,13 +324,15 @@ __device__ void neib_one(int p, const double4* __restrict__ pm, const double2* _
 // own particle's test on it (test32 in FP32, exact FP64 otherwise).  A cell
 // that passes for some lanes is opened for exactly those lanes, so the leaves
 // each lane opens are exactly those of its own reference walk.  Opened leaves
-// go to a per-warp list of (leaf, mask) entries; the passes over the
-// candidates then run once per entry for the whole warp (uniform loads of the
-// leaf's particles), each lane adding the terms of the particles whose entry
-// holds its bit.
+// go to a per-warp list of (leaf, mask) entries, and each lane keeps the
+// indices of its own entries.  The passes over the candidates then take the
+// particles one at a time: the warp flattens that particle's entries into its
+// candidate list and the 32 lanes share out the candidates (independent
+// loads), the partial sums reduced across the warp at the end.
 constexpr int GR_THREADS = 128;
 constexpr int GR_WARPS = GR_THREADS / 32;
 constexpr int GR_LCAP = 512;     // (leaf, mask) entries per warp
+constexpr int GR_PL = 64;        // entries in one lane's own list
 
 struct GrShared {
   int code[GR_LCAP];       // leaf: pstart*8 + count-1
@@ -339,10 +341,8 @@ struct GrShared {
   float fh[32];            // hrm32
   unsigned fm[32];         // lanes whose walk reaches the cell
   int fc[32];
-  int cq[32];              // staged candidates: particle
-  unsigned cm[32];         //   lanes that take it
-  double4 cp[32];          //   position, mass
-  double4 cv[32];          //   velocity (final pass)
+  unsigned short li[GR_PL][32];  // each lane's own entries, in list order
+  int cand[GR_PL * LEAFMAX];     // one particle's candidates
 };
 
 // Walk for the lanes in `lanes`, appending the opened leaves to R.code/R.mask
@@ -404,40 +404,6 @@ __device__ int gr_walk(const HydroTree& t, unsigned lanes, int2* S, int scap, Gr
   return nent;
 }
 
-// Clears the bits of `lanes` from the list and drops emptied entries (order kept).
-__device__ int gr_drop(GrShared& R, int nent, unsigned lanes, int lane) {
-  const unsigned lt = (1u << lane) - 1u;
-  __syncwarp();
-  int out = 0;
-  for (int base = 0; base < nent; base += 32) {
-    const int e = base + lane;
-    int code = 0;
-    unsigned m = 0;
-    if (e < nent) {
-      code = R.code[e];
-      m = R.mask[e] & ~lanes;
-    }
-    const unsigned b = __ballot_sync(FULL, m != 0u);
-    __syncwarp();
-    if (m != 0u) {
-      const int o = out + __popc(b & lt);
-      R.code[o] = code;
-      R.mask[o] = m;
-    }
-    out += __popc(b);
-  }
-  __syncwarp();
-  return out;
-}
-
-// particles in the leaves holding bit `bit` (the reference's pp_pot)
-__device__ __forceinline__ int gr_count(const GrShared& R, int nent, unsigned bit) {
-  int n = 0;
-  for (int e = 0; e < nent; ++e)
-    if (R.mask[e] & bit) n += (R.code[e] & 7) + 1;
-  return n;
-}
-
 // ascending bitonic sort of the entries by leaf (depth-first leaf order, the
 // order of the reference's candidate lists), masks carried along
 __device__ void gr_sort(GrShared& R, int n, int lane) {
@@ -464,39 +430,6 @@ __device__ void gr_sort(GrShared& R, int n, int lane) {
       __syncwarp();
     }
   }
-}
-
-// Stages the candidates of the next entries from e0 whose mask meets A, up to
-// 32 particles (whole leaves), into R.cq/R.cm and, through load(slot, q), the
-// particle data: one particle per lane, loaded in parallel.  Returns the count
-// and advances e0.
-template <class Load>
-__device__ int gr_stage(GrShared& R, int& e0, int nent, unsigned A, int lane, Load&& load) {
-  const int e = e0 + lane;
-  int cnt = 0, code = 0;
-  unsigned m = 0;
-  if (e < nent) {
-    m = R.mask[e] & A;
-    code = R.code[e];
-    cnt = m != 0u ? (code & 7) + 1 : 0;
-  }
-  const int inc = warp_iscan(cnt, lane);
-  const unsigned take = __ballot_sync(FULL, e < nent && inc <= 32);   // a prefix of the lanes
-  const int ntake = __popc(take);
-  const int total = ntake > 0 ? __shfl_sync(FULL, inc, ntake - 1) : 0;
-  __syncwarp();
-  if (((take >> lane) & 1u) && cnt > 0) {
-    const int o = inc - cnt;
-    for (int k = 0; k < cnt; ++k) {
-      R.cq[o + k] = (code >> 3) + k;
-      R.cm[o + k] = m;
-    }
-  }
-  e0 += ntake;
-  __syncwarp();
-  if (lane < total) load(lane, R.cq[lane]);
-  __syncwarp();
-  return total;
 }
 
 // gh_density_term and gh_final_term with the kernel bins evaluated in place
@@ -530,42 +463,300 @@ __device__ __forceinline__ void gh_final_term_k(const double4& Q, const double4&
   f.zt = f.zt + ((Q.w * ih) * ih) * kfn::wg(kern);
 }
 
+// This lane's entries (those holding its bit) in list order into R.li; the
+// count, or -1 when there are more than GR_PL.
+__device__ __forceinline__ int gr_lane_list(GrShared& R, int nent, unsigned bit, int lane) {
+  int n = 0;
+  for (int e = 0; e < nent; ++e) {
+    if (R.mask[e] & bit) {
+      if (n < GR_PL) R.li[n][lane] = (unsigned short)e;
+      ++n;
+    }
+  }
+  __syncwarp();
+  return n > GR_PL ? -1 : n;
+}
+
+// The candidates of lane j's n own entries, in order, into R.cand; the count.
+__device__ int gr_flatten(GrShared& R, int j, int n, int lane) {
+  int total = 0;
+  __syncwarp();
+  for (int base = 0; base < n; base += 32) {
+    const int t = base + lane;
+    int code = 0, c = 0;
+    if (t < n) {
+      code = R.code[R.li[t][j]];
+      c = (code & 7) + 1;
+    }
+    const int inc = warp_iscan(c, lane);
+    const int o = total + inc - c;
+    for (int k = 0; k < c; ++k) R.cand[o + k] = (code >> 3) + k;
+    total += __shfl_sync(FULL, inc, 31);
+  }
+  __syncwarp();
+  return total;
+}
+
+// sum over the warp, the same value on every lane
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(FULL, v, o);
+  return __shfl_sync(FULL, v, 0);
+}
+
 __device__ __forceinline__ int gr_next(int* work, int lane) {
   int g = 0;
   if (lane == 0) g = atomicAdd(work, 1);
   return __shfl_sync(FULL, g, 0);
 }
 
-// sph/all_sph_gradh.F90:11-492 for 32 particles per warp.  Each lane runs its
-// particle's iteration (:132-285) on its own bits of the shared list; lanes
-// whose h outgrows their last walk (:154-191) are walked again together, their
-// old bits cleared first.
-__global__ void __launch_bounds__(GR_THREADS) k_gradh_grp(
-    int nact, const int* __restrict__ act, const double4* __restrict__ pm, double2* __restrict__ hz,
+// ---------------------------------------------------------------------------
+// Warp-per-particle search for the few particles the group path hands back.
+constexpr int WP_THREADS = 128;
+constexpr int WP_WARPS = WP_THREADS / 32;
+constexpr int WP_FCAP = 512;     // cells of one level of the walk
+constexpr int WP_LCAP = 256;     // opened leaves (a power of two: the sort pads to it)
+constexpr int WP_CCAP = 1024;    // candidate particles
+
+struct WpShared {
+  int front[2][WP_FCAP];
+  int leaves[WP_LCAP];
+  int cand[WP_CCAP];
+};
+
+// Breadth-first walk of one particle's search; returns the number of opened
+// leaves (codes pstart*8 + count-1 in s.leaves) or -1 when a buffer overflows;
+// cnt = the particles in the opened leaves.
+template <class Test>
+__device__ int wp_walk(const HydroTree& t, int lane, WpShared& s, int& cnt,
+                       unsigned long long& nvisit, Test&& test) {
+  int* fa = s.front[0];
+  int* fb = s.front[1];
+  __syncwarp();
+  if (lane == 0) fa[0] = 0;
+  __syncwarp();
+  int nf = 1, nleaf = 0, mine = 0;
+  bool over = false;
+  while (nf > 0) {
+    int nnext = 0;
+    for (int base = 0; base < nf; base += 32) {
+      const int idx = base + lane;
+      const bool valid = idx < nf;
+      const int c = valid ? fa[idx] : 0;
+      const bool pass = valid && test(c);
+      const int4 lk = t.link[c];
+      const bool isleaf = pass && lk.x > 0;
+      const bool isbr = pass && lk.x == 0;
+      const unsigned ml = __ballot_sync(FULL, isleaf);
+      if (isleaf) {
+        const int pos = nleaf + __popc(ml & ((1u << lane) - 1u));
+        if (pos < WP_LCAP) s.leaves[pos] = lk.w * 8 + (lk.x - 1);
+        mine += lk.x;
+      }
+      nleaf += __popc(ml);
+      const int nk = isbr ? t.nkids[c] : 0;
+      const int sc = warp_iscan(nk, lane);
+      if (isbr) {
+        const int o = nnext + sc - nk;
+        for (int j = 0; j < nk; ++j)
+          if (o + j < WP_FCAP) fb[o + j] = lk.z + j;
+      }
+      nnext += __shfl_sync(FULL, sc, 31);
+    }
+    nvisit += nf;
+    __syncwarp();
+    if (nnext > WP_FCAP) over = true;
+    int* tmp = fa;
+    fa = fb;
+    fb = tmp;
+    nf = over ? 0 : nnext;
+  }
+  cnt = warp_iscan(mine, lane);
+  cnt = __shfl_sync(FULL, cnt, 31);
+  return (over || nleaf > WP_LCAP) ? -1 : nleaf;
+}
+
+// leaves -> candidate particle ids, in leaf order; returns the count (may
+// exceed WP_CCAP: overflow)
+__device__ int wp_flatten(int nleaf, int lane, WpShared& s) {
+  int total = 0;
+  for (int base = 0; base < nleaf; base += 32) {
+    const int k = base + lane;
+    const int code = k < nleaf ? s.leaves[k] : 0;
+    const int n = k < nleaf ? (code & 7) + 1 : 0;
+    const int sc = warp_iscan(n, lane);
+    const int o = total + sc - n;
+    for (int j = 0; j < n; ++j)
+      if (o + j < WP_CCAP) s.cand[o + j] = (code >> 3) + j;
+    total += __shfl_sync(FULL, sc, 31);
+  }
+  __syncwarp();
+  return total;
+}
+
+// sph/all_sph_gradh.F90:11-492 with one warp per particle and walks of its
+// own, for the particles k_gradh_pass hands back (redo[0..*nredo)): each walk
+// runs breadth-first with the lanes spread over the cells of a level, and the
+// candidates are processed 32 at a time with the partial sums reduced at the
+// end; when its own buffers overflow, one lane runs gradh_one.
+__global__ void __launch_bounds__(WP_THREADS) k_gradh_redo(
+    const int* __restrict__ act, const int* __restrict__ nredo,
+    const double4* __restrict__ pm, double2* __restrict__ hz,
     const double4* __restrict__ vel, double* __restrict__ rho, double* __restrict__ omega,
     double* __restrict__ divv, double* __restrict__ drhodt, HydroTree t,
-    const double4* __restrict__ tabA, double h_fac, int pp_gather, double rextent,
-    int2* __restrict__ stacks, int scap, DevError* err, unsigned long long* counts, int* work) {
-  __shared__ GrShared sh[GR_WARPS];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  GrShared& R = sh[w];
-  int2* const S = stacks + (size_t)(blockIdx.x * GR_WARPS + w) * scap;
-  const unsigned bit = 1u << lane;
+    const double4* __restrict__ tabA, double h_fac, int pp_gather, double rextent, DevError* err,
+    unsigned long long* counts) {
+  __shared__ WpShared sh[WP_WARPS];
+  const int lane = threadIdx.x & 31;
+  WpShared& S = sh[threadIdx.x >> 5];
   const double4 t0 = tabA[0];
   unsigned long long nwalk = 0, nvisit = 0, npass = 0, ncands = 0;
+  const int nact = *nredo;
+  for (int i = blockIdx.x * WP_WARPS + (threadIdx.x >> 5); i < nact; i += gridDim.x * WP_WARPS) {
+    {
+      const int p = act[i];
+      const double4 P = pm[p];
+      const double rx = P.x, ry = P.y, rz = P.z, mp = P.w;
+      const float px = (float)(rx - t.rootx), py = (float)(ry - t.rooty),
+                  pz = (float)(rz - t.rootz);
+      GhState s;
+      gh_init(s, hz[p].x, rextent);
+      double R = 0.0;
+      float R32 = 0.0f;
+      auto gather_test = [&](int c) {                 // BHhydrowalk_hgather.F90:36-40
+        const float4 h32 = t.hA32[c];
+        const float d0 = h32.x - px, d1 = h32.y - py, d2 = h32.z - pz;
+        const int r = test32((d0 * d0 + d1 * d1) + d2 * d2, R32 + h32.w, t.delta);
+        if (r >= 0) return r == 1;
+        const double4 h = t.hA[c];
+        const double e0 = h.x - rx, e1 = h.y - ry, e2 = h.z - rz;
+        const double tt = R + h.w;
+        return ((e0 * e0 + e1 * e1) + e2 * e2) <= tt * tt;
+      };
+      int ncand = 0;
+      bool over = false, bad = false;
+      while (true) {
+        while (true) {                                                 // :154-191
+          if (s.hp > s.h_high) {
+            s.h_high = s.hp * HMULT;
+            R = KERNRANGE * s.h_high;
+            R32 = (float)R;
+            int cnt = 0;
+            ++nwalk;
+            const int nl = wp_walk(t, lane, S, cnt, nvisit, gather_test);
+            if (nl < 0) { over = true; break; }
+            ncand = wp_flatten(nl, lane, S);
+            if (ncand > WP_CCAP) { over = true; break; }
+            s.pp_pot = cnt;
+          }
+          if (s.pp_pot < pp_gather) {
+            s.h_high = 0.0;
+            s.pp_pot = 0;
+            s.hp = s.hp * HMULT;
+            if (++s.ngrow > HGROW_CAP) { bad = true; break; }
+          }
+          if (s.pp_pot > 0) break;
+        }
+        if (over || bad) break;
+        const double ih = 1.0 / s.hp;                                  // :199-235
+        const double hf = pow(ih, NDIMPR);
+        const double hs = (KERNRANGESQD * s.hp) * s.hp;
+        double part = 0.0;
+        for (int k = lane; k < ncand; k += 32) {
+          const int q = S.cand[k];
+          if (q != p) gh_density_term(pm[q], rx, ry, rz, hs, ih, hf, tabA, part);
+        }
+        const double rt = (mp * t0.x) * hf + warp_sum(part);
+        ++npass;
+        ncands += ncand;
+        if (gh_after_pass(s, mp, h_fac, rextent, rt)) break;
+      }
+      if (bad) {
+        if (lane == 0) set_error(err, SEREN_GPU_ERR_WALK, KID_GRADH, p, -1);
+        continue;
+      }
+      if (over) {
+        if (lane == 0)
+          gradh_one(p, pm, hz, vel, rho, omega, divv, drhodt, t, tabA, h_fac, pp_gather, rextent,
+                    err);
+        __syncwarp();
+        continue;
+      }
+      const double hp = h_fac * pow(mp / s.rho, ONETHIRD);            // :317-425
+      const double ih = 1.0 / hp;
+      const double hf = pow(ih, NDIMPR);
+      const double hs = (KERNRANGESQD * hp) * hp;
+      const double4 vp = vel[p];
+      GhFinal f;
+      f.rt = 0.0; f.om = 0.0; f.dv = 0.0; f.zt = 0.0;
+      for (int k = lane; k < ncand; k += 32) {
+        const int q = S.cand[k];
+        if (q != p) gh_final_term(pm[q], vel[q], rx, ry, rz, vp, hs, ih, hf, tabA, f);
+      }
+      GhFinal g;
+      gh_final_init(g, mp, ih, hf, t0);
+      g.rt = g.rt + warp_sum(f.rt);
+      g.om = g.om + warp_sum(f.om);
+      g.dv = g.dv + warp_sum(f.dv);
+      g.zt = g.zt + warp_sum(f.zt);
+      ++npass;
+      ncands += ncand;
+      if (lane == 0) gh_store(p, mp, hp, g, hz, rho, omega, divv, drhodt, err);
+    }
+  }
+  if (lane == 0) {
+    atomicAdd(counts + 3, nwalk);
+    atomicAdd(counts + 4, nvisit);
+    atomicAdd(counts + 5, npass);
+    atomicAdd(counts + 6, ncands);
+  }
+}
+
+
+// sph/all_sph_gradh.F90:11-492 in two kernels.
+//
+// k_gradh_walk: the first neighbour walk of every active particle
+// (:154-170, BHhydrowalk_hgather at h_high = h*HMULT), 32 particles per warp
+// on a group walk; each particle's opened leaves go to its own row of
+// c.leaves (GH_LEAVES codes pstart*8 + count-1, in walk order) and their
+// number to c.nleaf (-1 when the row or the walk overflows).
+//
+// k_gradh_pass: one warp per particle.  The warp flattens the particle's row
+// into its candidate list once, then runs the reference's iteration on it
+// (:154-285): density passes with the 32 lanes sharing out the candidates and
+// the sums reduced across the warp, then the final pass (:317-425).  The
+// reference leaves this path only to grow h (pp_pot < pp_gather) or to walk
+// again (h > h_high); a particle that needs either, or whose row overflowed,
+// is redone from the start by gradh_one, which follows the reference's loop
+// with walks of its own and so takes the same steps (k_gradh_redo, one warp
+// per such particle).
+constexpr int GH_LEAVES = 128;   // opened leaves kept per particle
+
+__global__ void __launch_bounds__(GR_THREADS) k_gradh_walk(
+    int nact, const int* __restrict__ act, const double4* __restrict__ pm,
+    const double2* __restrict__ hz, HydroTree t, int* __restrict__ leaves,
+    int* __restrict__ nleaf, int2* __restrict__ stacks, int scap, unsigned long long* counts,
+    int* work) {
+  extern __shared__ __align__(16) unsigned char gr_smem[];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  GrShared& R = reinterpret_cast<GrShared*>(gr_smem)[w];
+  int2* const S = stacks + (size_t)(blockIdx.x * GR_WARPS + w) * scap;
+  const unsigned bit = 1u << lane;
+  unsigned long long nvisit = 0;
+  unsigned nwalk = 0;
   for (int g = gr_next(work, lane); (long long)g * 32 < nact; g = gr_next(work, lane)) {
     const int i = g * 32 + lane;
     const bool live = i < nact;
     const int p = live ? (act ? act[i] : i) : (act ? act[nact - 1] : nact - 1);
     const double4 P = pm[p];
-    const double rx = P.x, ry = P.y, rz = P.z, mp = P.w;
+    const double rx = P.x, ry = P.y, rz = P.z;
     const float px = (float)(rx - t.rootx), py = (float)(ry - t.rooty), pz = (float)(rz - t.rootz);
-    GhState s;
-    gh_init(s, hz[p].x, rextent);
-    double Rw = 0.0;
-    float R32 = 0.0f;
-    auto gather_test = [&](int e) {                    // BHhydrowalk_hgather.F90:36-40
-      const float4 h32 = R.fa[e];
+    const double Rw = KERNRANGE * (hz[p].x * HMULT);                  // :157-158
+    const float R32 = (float)Rw;
+    const unsigned lanes = __ballot_sync(FULL, live);
+    nwalk += live ? 1u : 0u;
+    const int nent = gr_walk(t, lanes, S, scap, R, lane, 0, nvisit, [&](int e) {
+      const float4 h32 = R.fa[e];                      // BHhydrowalk_hgather.F90:36-40
       const float d0 = h32.x - px, d1 = h32.y - py, d2 = h32.z - pz;
       const int r = test32((d0 * d0 + d1 * d1) + d2 * d2, R32 + h32.w, t.delta);
       if (r >= 0) return r == 1;
@@ -573,112 +764,136 @@ __global__ void __launch_bounds__(GR_THREADS) k_gradh_grp(
       const double e0 = h.x - rx, e1 = h.y - ry, e2 = h.z - rz;
       const double tt = Rw + h.w;
       return ((e0 * e0 + e1 * e1) + e2 * e2) <= tt * tt;
-    };
-    bool active = live;        // still iterating
-    bool ok = live;            // ends with the final pass
-    bool single = false;       // list overflow: this lane runs gradh_one
-    int nent = 0;
-    while (__any_sync(FULL, active)) {
-      while (true) {                                                   // :154-191
-        const bool need = active && s.hp > s.h_high;
-        const unsigned W = __ballot_sync(FULL, need);
-        if (W) {
-          if (need) {
-            s.h_high = s.hp * HMULT;
-            Rw = KERNRANGE * s.h_high;
-            R32 = (float)Rw;
-            ++nwalk;
-          }
-          nent = gr_drop(R, nent, W, lane);
-          const int ne = gr_walk(t, W, S, scap, R, lane, nent, nvisit, gather_test);
-          if (ne < 0) {
-            if (need) { single = true; active = false; ok = false; }
-          } else {
-            nent = ne;
-            if (need) s.pp_pot = gr_count(R, nent, bit);
-          }
+    });
+    int n = -1;
+    if (nent >= 0) {
+      n = 0;
+      int* row = leaves + (size_t)p * GH_LEAVES;
+      for (int e = 0; e < nent; ++e) {
+        if (R.mask[e] & bit) {
+          if (n < GH_LEAVES) row[n] = R.code[e];
+          ++n;
         }
-        if (active && s.pp_pot < pp_gather) {
-          s.h_high = 0.0;
-          s.pp_pot = 0;
-          s.hp = s.hp * HMULT;
-          if (++s.ngrow > HGROW_CAP) {
-            set_error(err, SEREN_GPU_ERR_WALK, KID_GRADH, p, -1);
-            active = false;
-            ok = false;
-          }
-        }
-        if (!__any_sync(FULL, active && s.pp_pot == 0)) break;
       }
-      const unsigned A = __ballot_sync(FULL, active);
-      if (A == 0u) break;
+      if (n > GH_LEAVES) n = -1;
+    }
+    if (live) nleaf[p] = n;
+    __syncwarp();
+  }
+  atomicAdd(counts + 3, (unsigned long long)nwalk);
+  if (lane == 0) atomicAdd(counts + 4, nvisit);
+}
+
+constexpr int GP_THREADS = 128;
+constexpr int GP_WARPS = GP_THREADS / 32;
+
+__global__ void __launch_bounds__(GP_THREADS) k_gradh_pass(
+    int nact, const int* __restrict__ act, const double4* __restrict__ pm, double2* __restrict__ hz,
+    const double4* __restrict__ vel, double* __restrict__ rho, double* __restrict__ omega,
+    double* __restrict__ divv, double* __restrict__ drhodt, HydroTree t,
+    const double4* __restrict__ tabA, double h_fac, int pp_gather, double rextent,
+    const int* __restrict__ leaves, const int* __restrict__ nleaf, int* __restrict__ redo,
+    int* __restrict__ nredo, DevError* err, unsigned long long* counts) {
+  __shared__ int cand_all[GP_WARPS][GH_LEAVES * LEAFMAX];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int* cand = cand_all[w];
+  const double4 t0 = tabA[0];
+  unsigned long long npass = 0, ncands = 0, niter = 0, nsingle = 0;
+  for (int i = blockIdx.x * GP_WARPS + w; i < nact; i += gridDim.x * GP_WARPS) {
+  const int p = act ? act[i] : i;
+  const int n = nleaf[p];
+  bool single = n < 0;
+  if (!single) {
+    // flatten the row: candidates in walk order (:172-191)
+    int total = 0;
+    for (int base = 0; base < n; base += 32) {
+      const int k = base + lane;
+      int code = 0, c = 0;
+      if (k < n) {
+        code = leaves[(size_t)p * GH_LEAVES + k];
+        c = (code & 7) + 1;
+      }
+      const int inc = warp_iscan(c, lane);
+      const int o = total + inc - c;
+      for (int j = 0; j < c; ++j) cand[o + j] = (code >> 3) + j;
+      total += __shfl_sync(FULL, inc, 31);
+    }
+    __syncwarp();
+    const double4 P = pm[p];
+    const double rx = P.x, ry = P.y, rz = P.z, mp = P.w;
+    GhState s;
+    gh_init(s, hz[p].x, rextent);
+    s.h_high = s.hp * HMULT;
+    s.pp_pot = total;
+    if (s.pp_pot < pp_gather) single = true;           // :175-181 would grow h
+    while (!single) {
       const double ih = 1.0 / s.hp;                                    // :199-235
       const double hf = pow(ih, NDIMPR);
       const double hs = (KERNRANGESQD * s.hp) * s.hp;
-      double rt = (mp * t0.x) * hf;
-      for (int e0 = 0; e0 < nent;) {
-        const int nc = gr_stage(R, e0, nent, A, lane, [&](int j, int q) { R.cp[j] = pm[q]; });
-        for (int j = 0; j < nc; ++j) {
-          const double4 Q = R.cp[j];
-          if ((R.cm[j] & bit) && R.cq[j] != p) gh_density_term_k(Q, rx, ry, rz, hs, ih, hf, rt);
-        }
+      double part = 0.0;
+      for (int k = lane; k < total; k += 32) {
+        const int q = cand[k];
+        if (q != p) gh_density_term_k(pm[q], rx, ry, rz, hs, ih, hf, part);
       }
-      if (active) {
-        ++npass;
-        ncands += s.pp_pot;
-        if (gh_after_pass(s, mp, h_fac, rextent, rt)) active = false;
-      }
-    }
-    // final pass (:317-425) on each lane's last candidate list
-    const unsigned F = __ballot_sync(FULL, ok);
-    const double hp = h_fac * pow(mp / s.rho, ONETHIRD);
-    const double ih = 1.0 / hp;
-    const double hf = pow(ih, NDIMPR);
-    const double hs = (KERNRANGESQD * hp) * hp;
-    const double4 vp = vel[p];
-    GhFinal f;
-    gh_final_init(f, mp, ih, hf, t0);
-    for (int e0 = 0; e0 < nent;) {
-      const int nc = gr_stage(R, e0, nent, F, lane, [&](int j, int q) {
-        R.cp[j] = pm[q];
-        R.cv[j] = vel[q];
-      });
-      for (int j = 0; j < nc; ++j) {
-        const double4 Q = R.cp[j];
-        const double4 V = R.cv[j];
-        if ((R.cm[j] & bit) && R.cq[j] != p) gh_final_term_k(Q, V, rx, ry, rz, vp, hs, ih, hf, f);
-      }
-    }
-    if (ok) {
+      niter += (total + 31) >> 5;
       ++npass;
-      ncands += s.pp_pot;
-      gh_store(p, mp, hp, f, hz, rho, omega, divv, drhodt, err);
+      ncands += total;
+      if (gh_after_pass(s, mp, h_fac, rextent, (mp * t0.x) * hf + warp_sum(part))) break;
+      if (s.hp > s.h_high) single = true;               // :154-170 would walk again
     }
-    if (single)
-      gradh_one(p, pm, hz, vel, rho, omega, divv, drhodt, t, tabA, h_fac, pp_gather, rextent, err);
-    __syncwarp();
+    if (!single) {
+      const double hp = h_fac * pow(mp / s.rho, ONETHIRD);             // :317-425
+      const double ih = 1.0 / hp;
+      const double hf = pow(ih, NDIMPR);
+      const double hs = (KERNRANGESQD * hp) * hp;
+      const double4 vp = vel[p];
+      GhFinal f;
+      f.rt = 0.0; f.om = 0.0; f.dv = 0.0; f.zt = 0.0;
+      for (int k = lane; k < total; k += 32) {
+        const int q = cand[k];
+        if (q != p) gh_final_term_k(pm[q], vel[q], rx, ry, rz, vp, hs, ih, hf, f);
+      }
+      niter += (total + 31) >> 5;
+      ++npass;
+      ncands += total;
+      GhFinal g;
+      gh_final_init(g, mp, ih, hf, t0);
+      g.rt = g.rt + warp_sum(f.rt);
+      g.om = g.om + warp_sum(f.om);
+      g.dv = g.dv + warp_sum(f.dv);
+      g.zt = g.zt + warp_sum(f.zt);
+      if (lane == 0) gh_store(p, mp, hp, g, hz, rho, omega, divv, drhodt, err);
+    }
   }
-  atomicAdd(counts + 3, nwalk);
-  atomicAdd(counts + 5, npass);
-  atomicAdd(counts + 6, ncands);
-  if (lane == 0) atomicAdd(counts + 4, nvisit);
+  if (single && lane == 0) redo[atomicAdd(nredo, 1)] = p;
+  nsingle += single ? 1 : 0;
+  __syncwarp();
+  }
+  if (lane == 0) {
+    atomicAdd(counts + 5, npass);
+    atomicAdd(counts + 6, ncands);
+    atomicAdd(counts + 13, niter);
+    atomicAdd(counts + 15, nsingle);
+  }
 }
 
 // get_neib (sph/get_neib.F90:10-140) for 32 particles per warp: one group walk
 // with each lane's gather-or-scatter test (BHhydro_walk.F90:37-43), the opened
-// leaves sorted into depth-first order, then each lane keeps the candidates
-// with r^2 <= 4h_p^2 or r^2 <= 4h_pp^2 in that order.
+// leaves sorted into depth-first order; then, particle by particle, the warp
+// keeps the candidates with r^2 <= 4h_p^2 or r^2 <= 4h_pp^2 in that order and
+// writes the row with coalesced stores.
 __global__ void __launch_bounds__(GR_THREADS) k_neib_grp(
     int nact, const int* __restrict__ act, const double4* __restrict__ pm,
     const double2* __restrict__ hz, HydroTree t, int L, int* __restrict__ pptot,
     int* __restrict__ pplist, int2* __restrict__ stacks, int scap, DevError* err,
     unsigned long long* counts, int* work) {
-  __shared__ GrShared sh[GR_WARPS];
+  extern __shared__ __align__(16) unsigned char gr_smem[];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  GrShared& R = sh[w];
+  GrShared& R = reinterpret_cast<GrShared*>(gr_smem)[w];
   int2* const S = stacks + (size_t)(blockIdx.x * GR_WARPS + w) * scap;
   const unsigned bit = 1u << lane;
-  unsigned long long nvisit = 0, ncands = 0;
+  const unsigned lt = bit - 1u;
+  unsigned long long nvisit = 0, ncands = 0, niter = 0;
   for (int g = gr_next(work, lane); (long long)g * 32 < nact; g = gr_next(work, lane)) {
     const int i = g * 32 + lane;
     const bool live = i < nact;
@@ -707,41 +922,49 @@ __global__ void __launch_bounds__(GR_THREADS) k_neib_grp(
       const double t2 = t.hrm[c] + h.w;
       return drsqd <= t1 * t1 || drsqd <= t2 * t2;
     });
-    if (nent < 0) {
-      if (live) neib_one(p, pm, hz, t, L, pptot, pplist, err);
-      __syncwarp();
-      continue;
+    int myn = -1;
+    if (nent >= 0) {
+      gr_sort(R, nent, lane);
+      myn = gr_lane_list(R, nent, bit, lane);
     }
-    gr_sort(R, nent, lane);
-    int* row = pplist + (size_t)p * L;
-    int kept = 0;
-    for (int e0 = 0; e0 < nent;) {
-      const int nc = gr_stage(R, e0, nent, lanes, lane, [&](int j, int q) {
-        R.cp[j] = pm[q];
-        R.cv[j].x = hz[q].x;
-      });
-      for (int j = 0; j < nc; ++j) {
-        const int q = R.cq[j];
-        const bool mine = (R.cm[j] & bit) != 0u;
-        ncands += mine ? 1 : 0;
-        if (mine && q != p) {
-          const double4 Q = R.cp[j];
-          const double hq = R.cv[j].x;
+    const unsigned G = __ballot_sync(FULL, live && myn >= 0);
+    for (unsigned todo = G; todo != 0u; todo &= todo - 1u) {
+      const int j = __ffs(todo) - 1;
+      const double xj = __shfl_sync(FULL, P.x, j), yj = __shfl_sync(FULL, P.y, j),
+                   zj = __shfl_sync(FULL, P.z, j), hsj = __shfl_sync(FULL, hsp, j);
+      const int pj = __shfl_sync(FULL, p, j);
+      const int nc = gr_flatten(R, j, __shfl_sync(FULL, myn, j), lane);
+      int* row = pplist + (size_t)pj * L;
+      int kept = 0;
+      for (int b = 0; b < nc; b += 32) {
+        const int k = b + lane;
+        const int q = k < nc ? R.cand[k] : pj;
+        bool keep = false;
+        if (q != pj) {
+          const double4 Q = pm[q];
+          const double hq = hz[q].x;
           const double hsq = (KERNRANGESQD * hq) * hq;
-          const double d0 = Q.x - P.x, d1 = Q.y - P.y, d2 = Q.z - P.z;
+          const double d0 = Q.x - xj, d1 = Q.y - yj, d2 = Q.z - zj;
           const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
-          if (drsqd <= hsp || drsqd <= hsq) {
-            if (kept < L) row[kept] = q;
-            ++kept;
-          }
+          keep = drsqd <= hsj || drsqd <= hsq;
         }
+        const unsigned m = __ballot_sync(FULL, keep);
+        const int pos = kept + __popc(m & lt);
+        if (keep && pos < L) row[pos] = q;
+        kept += __popc(m);
       }
+      niter += (nc + 31) >> 5;
+      ncands += nc;
+      if (lane == 0) pptot[pj] = kept;
     }
-    if (live) pptot[p] = kept;
+    if (live && myn < 0) neib_one(p, pm, hz, t, L, pptot, pplist, err);   // list overflow
     __syncwarp();
   }
-  atomicAdd(counts + 7, ncands);
-  if (lane == 0) atomicAdd(counts + 4, nvisit);
+  if (lane == 0) {
+    atomicAdd(counts + 4, nvisit);
+    atomicAdd(counts + 7, ncands);
+    atomicAdd(counts + 14, niter);
+  }
 }
 
 // sph/hydro_gradh.F90:9-339 (NEIGHBOUR_LISTS, ARTIFICIAL_VISCOSITY=MON97).
@@ -930,17 +1153,23 @@ HydroTree hydro_tree(const Ctx& c) {
 
 }  // namespace
 
-// Resident blocks per SM of the group-walk kernels on device dev.
+constexpr size_t GR_SMEM = sizeof(GrShared) * GR_WARPS;
+
+// Resident blocks per SM of the group-walk kernels on device dev (their
+// dynamic shared-memory limit is raised on first use per device).
 static int gr_blocks_per_sm(int dev, int which) {
   static int occ[16][2] = {};
   int dummy[2] = {0, 0};
   int* o = dev >= 0 && dev < 16 ? occ[dev] : dummy;
   int& r = o[which];
   if (r == 0) {
-    if (which == 0)
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_gradh_grp, GR_THREADS, 0);
-    else
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_neib_grp, GR_THREADS, 0);
+    if (which == 0) {
+      cudaFuncSetAttribute(k_gradh_walk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GR_SMEM);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_gradh_walk, GR_THREADS, GR_SMEM);
+    } else {
+      cudaFuncSetAttribute(k_neib_grp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GR_SMEM);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_neib_grp, GR_THREADS, GR_SMEM);
+    }
     if (r < 1) r = 1;
   }
   return r;
@@ -967,18 +1196,33 @@ static int gr_grid(const Ctx& c, int nact, int which) {
 
 void launch_gradh(Ctx& c, int nact) {
   if (nact <= 0) return;
+  unsigned long long* counts = reinterpret_cast<unsigned long long*>(c.d_counts);
+  const HydroTree t = hydro_tree(c);
   cudaMemsetAsync(c.work, 0, sizeof(int), c.st);
-  k_gradh_grp<<<gr_grid(c, nact, 0), GR_THREADS, 0, c.st>>>(
-      nact, c.act, c.pm, c.hz, c.vel, c.rho, c.omega, c.div_v, c.drhodt, hydro_tree(c), c.tabA,
-      c.prm.h_fac, c.prm.pp_gather, c.info.rextent, c.wstack, c.wstack_cap, c.d_err,
-      reinterpret_cast<unsigned long long*>(c.d_counts), c.work);
-  ++c.nlaunch;
+  k_gradh_walk<<<gr_grid(c, nact, 0), GR_THREADS, GR_SMEM, c.st>>>(
+      nact, c.act, c.pm, c.hz, t, c.leaves, c.nleaf, c.wstack, c.wstack_cap, counts, c.work);
+  static int occ[16] = {};
+  int& o = occ[c.dev >= 0 && c.dev < 16 ? c.dev : 0];
+  if (o == 0) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_gradh_pass, GP_THREADS, 0);
+    if (o < 1) o = 1;
+  }
+  const int blocks = std::min(sm_count(c) * o, nb(nact, GP_WARPS));
+  cudaMemsetAsync(c.work + 1, 0, sizeof(int), c.st);
+  k_gradh_pass<<<blocks, GP_THREADS, 0, c.st>>>(
+      nact, c.act, c.pm, c.hz, c.vel, c.rho, c.omega, c.div_v, c.drhodt, t, c.tabA,
+      c.prm.h_fac, c.prm.pp_gather, c.info.rextent, c.leaves, c.nleaf, c.redo, c.work + 1,
+      c.d_err, counts);
+  k_gradh_redo<<<sm_count(c) * 2, WP_THREADS, 0, c.st>>>(
+      c.redo, c.work + 1, c.pm, c.hz, c.vel, c.rho, c.omega, c.div_v, c.drhodt, t, c.tabA,
+      c.prm.h_fac, c.prm.pp_gather, c.info.rextent, c.d_err, counts);
+  c.nlaunch += 3;
 }
 
 void launch_neib(Ctx& c, int nact) {
   if (nact <= 0) return;
   cudaMemsetAsync(c.work, 0, sizeof(int), c.st);
-  k_neib_grp<<<gr_grid(c, nact, 1), GR_THREADS, 0, c.st>>>(
+  k_neib_grp<<<gr_grid(c, nact, 1), GR_THREADS, GR_SMEM, c.st>>>(
       nact, c.act, c.pm, c.hz, hydro_tree(c), c.prm.pp_limit, c.pptot, c.pplist, c.wstack,
       c.wstack_cap, c.d_err, reinterpret_cast<unsigned long long*>(c.d_counts), c.work);
   ++c.nlaunch;
