@@ -100,6 +100,7 @@ struct Ctx {
   int* work = nullptr;        // work counter of the persistent kernels
   int* leaves = nullptr;      // [pmax][128] opened leaves of each particle's grad-h walk
   int* nleaf = nullptr;       // their number (-1: overflow)
+  int* npot = nullptr;        // [pmax] particles in those leaves (pp_pot)
   int* redo = nullptr;        // [pmax] particles whose grad-h is redone alone; count in work[1]
   int2* wstack = nullptr;     // walk stacks, wstack_cap (cell, lane mask) entries per warp slot
   int wstack_cap = 0;

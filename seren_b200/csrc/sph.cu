@@ -721,10 +721,10 @@ __global__ void __launch_bounds__(WP_THREADS) k_gradh_redo(
 // c.leaves (GH_LEAVES codes pstart*8 + count-1, in walk order) and their
 // number to c.nleaf (-1 when the row or the walk overflows).
 //
-// k_gradh_pass: one warp per particle.  The warp flattens the particle's row
-// into its candidate list once, then runs the reference's iteration on it
-// (:154-285): density passes with the 32 lanes sharing out the candidates and
-// the sums reduced across the warp, then the final pass (:317-425).  The
+// k_gradh_pass: 32 particles per warp, each lane holding its particle's state;
+// the reference's iteration (:154-285) and final pass (:317-425) run with the
+// candidates of one particle at a time (its row flattened) shared out over the
+// lanes and the sums reduced across the warp.  The
 // reference leaves this path only to grow h (pp_pot < pp_gather) or to walk
 // again (h > h_high); a particle that needs either, or whose row overflowed,
 // is redone from the start by gradh_one, which follows the reference's loop
@@ -735,8 +735,8 @@ constexpr int GH_LEAVES = 128;   // opened leaves kept per particle
 __global__ void __launch_bounds__(GR_THREADS) k_gradh_walk(
     int nact, const int* __restrict__ act, const double4* __restrict__ pm,
     const double2* __restrict__ hz, HydroTree t, int* __restrict__ leaves,
-    int* __restrict__ nleaf, int2* __restrict__ stacks, int scap, unsigned long long* counts,
-    int* work) {
+    int* __restrict__ nleaf, int* __restrict__ npot, int2* __restrict__ stacks, int scap,
+    unsigned long long* counts, int* work) {
   extern __shared__ __align__(16) unsigned char gr_smem[];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   GrShared& R = reinterpret_cast<GrShared*>(gr_smem)[w];
@@ -765,19 +765,24 @@ __global__ void __launch_bounds__(GR_THREADS) k_gradh_walk(
       const double tt = Rw + h.w;
       return ((e0 * e0 + e1 * e1) + e2 * e2) <= tt * tt;
     });
-    int n = -1;
+    int n = -1, pot = 0;
     if (nent >= 0) {
       n = 0;
       int* row = leaves + (size_t)p * GH_LEAVES;
       for (int e = 0; e < nent; ++e) {
         if (R.mask[e] & bit) {
-          if (n < GH_LEAVES) row[n] = R.code[e];
+          const int code = R.code[e];
+          if (n < GH_LEAVES) row[n] = code;
           ++n;
+          pot += (code & 7) + 1;                        // pp_pot, :168
         }
       }
       if (n > GH_LEAVES) n = -1;
     }
-    if (live) nleaf[p] = n;
+    if (live) {
+      nleaf[p] = n;
+      npot[p] = pot;
+    }
     __syncwarp();
   }
   atomicAdd(counts + 3, (unsigned long long)nwalk);
@@ -787,94 +792,143 @@ __global__ void __launch_bounds__(GR_THREADS) k_gradh_walk(
 constexpr int GP_THREADS = 128;
 constexpr int GP_WARPS = GP_THREADS / 32;
 
+// A particle's row of opened leaves flattened into its candidates, in order;
+// returns the count.
+__device__ __forceinline__ int gp_flatten(const int* __restrict__ row, int n, int* cand,
+                                          int lane) {
+  int total = 0;
+  __syncwarp();
+  for (int base = 0; base < n; base += 32) {
+    const int k = base + lane;
+    int code = 0, c = 0;
+    if (k < n) {
+      code = row[k];
+      c = (code & 7) + 1;
+    }
+    const int inc = warp_iscan(c, lane);
+    const int o = total + inc - c;
+    for (int j = 0; j < c; ++j) cand[o + j] = (code >> 3) + j;
+    total += __shfl_sync(FULL, inc, 31);
+  }
+  __syncwarp();
+  return total;
+}
+
+// 32 consecutive particles per warp: each lane holds its particle's iteration
+// state, so the per-particle arithmetic of a pass (h, its powers, the update
+// of :238-285) runs once per lane for all 32; each particle's candidates are
+// shared out over the 32 lanes in turn.
 __global__ void __launch_bounds__(GP_THREADS) k_gradh_pass(
     int nact, const int* __restrict__ act, const double4* __restrict__ pm, double2* __restrict__ hz,
     const double4* __restrict__ vel, double* __restrict__ rho, double* __restrict__ omega,
-    double* __restrict__ divv, double* __restrict__ drhodt, HydroTree t,
-    const double4* __restrict__ tabA, double h_fac, int pp_gather, double rextent,
-    const int* __restrict__ leaves, const int* __restrict__ nleaf, int* __restrict__ redo,
+    double* __restrict__ divv, double* __restrict__ drhodt, const double4* __restrict__ tabA,
+    double h_fac, int pp_gather, double rextent, const int* __restrict__ leaves,
+    const int* __restrict__ nleaf, const int* __restrict__ npot, int* __restrict__ redo,
     int* __restrict__ nredo, DevError* err, unsigned long long* counts) {
   __shared__ int cand_all[GP_WARPS][GH_LEAVES * LEAFMAX];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   int* cand = cand_all[w];
   const double4 t0 = tabA[0];
   unsigned long long npass = 0, ncands = 0, niter = 0, nsingle = 0;
-  for (int i = blockIdx.x * GP_WARPS + w; i < nact; i += gridDim.x * GP_WARPS) {
-  const int p = act ? act[i] : i;
-  const int n = nleaf[p];
-  bool single = n < 0;
-  if (!single) {
-    // flatten the row: candidates in walk order (:172-191)
-    int total = 0;
-    for (int base = 0; base < n; base += 32) {
-      const int k = base + lane;
-      int code = 0, c = 0;
-      if (k < n) {
-        code = leaves[(size_t)p * GH_LEAVES + k];
-        c = (code & 7) + 1;
-      }
-      const int inc = warp_iscan(c, lane);
-      const int o = total + inc - c;
-      for (int j = 0; j < c; ++j) cand[o + j] = (code >> 3) + j;
-      total += __shfl_sync(FULL, inc, 31);
-    }
-    __syncwarp();
+  for (int g = blockIdx.x * GP_WARPS + w; (long long)g * 32 < nact; g += gridDim.x * GP_WARPS) {
+    const int i = g * 32 + lane;
+    const bool live = i < nact;
+    const int p = live ? (act ? act[i] : i) : (act ? act[nact - 1] : nact - 1);
+    const int n = live ? nleaf[p] : 0;
     const double4 P = pm[p];
     const double rx = P.x, ry = P.y, rz = P.z, mp = P.w;
     GhState s;
     gh_init(s, hz[p].x, rextent);
-    s.h_high = s.hp * HMULT;
-    s.pp_pot = total;
-    if (s.pp_pot < pp_gather) single = true;           // :175-181 would grow h
-    while (!single) {
+    s.h_high = s.hp * HMULT;                                           // :157-170
+    s.pp_pot = n >= 0 ? npot[p] : 0;
+    bool single = live && (n < 0 || s.pp_pot < pp_gather);             // :175-181 would grow h
+    bool active = live && !single;
+    double rt = 0.0;
+    while (true) {
+      const unsigned A = __ballot_sync(FULL, active);
+      if (A == 0u) break;
       const double ih = 1.0 / s.hp;                                    // :199-235
       const double hf = pow(ih, NDIMPR);
       const double hs = (KERNRANGESQD * s.hp) * s.hp;
-      double part = 0.0;
-      for (int k = lane; k < total; k += 32) {
-        const int q = cand[k];
-        if (q != p) gh_density_term_k(pm[q], rx, ry, rz, hs, ih, hf, part);
+      for (unsigned todo = A; todo != 0u; todo &= todo - 1u) {
+        const int j = __ffs(todo) - 1;
+        const double xj = __shfl_sync(FULL, rx, j), yj = __shfl_sync(FULL, ry, j),
+                     zj = __shfl_sync(FULL, rz, j);
+        const double hsj = __shfl_sync(FULL, hs, j), ihj = __shfl_sync(FULL, ih, j),
+                     hfj = __shfl_sync(FULL, hf, j);
+        const int pj = __shfl_sync(FULL, p, j);
+        const int nc = gp_flatten(leaves + (size_t)pj * GH_LEAVES, __shfl_sync(FULL, n, j), cand,
+                                  lane);
+        double part = 0.0;
+        for (int k = lane; k < nc; k += 32) {
+          const int q = cand[k];
+          if (q != pj) gh_density_term_k(pm[q], xj, yj, zj, hsj, ihj, hfj, part);
+        }
+        niter += (nc + 31) >> 5;
+        const double sum = warp_sum(part);
+        if (lane == j) rt = sum;
       }
-      niter += (total + 31) >> 5;
-      ++npass;
-      ncands += total;
-      if (gh_after_pass(s, mp, h_fac, rextent, (mp * t0.x) * hf + warp_sum(part))) break;
-      if (s.hp > s.h_high) single = true;               // :154-170 would walk again
-    }
-    if (!single) {
-      const double hp = h_fac * pow(mp / s.rho, ONETHIRD);             // :317-425
-      const double ih = 1.0 / hp;
-      const double hf = pow(ih, NDIMPR);
-      const double hs = (KERNRANGESQD * hp) * hp;
-      const double4 vp = vel[p];
-      GhFinal f;
-      f.rt = 0.0; f.om = 0.0; f.dv = 0.0; f.zt = 0.0;
-      for (int k = lane; k < total; k += 32) {
-        const int q = cand[k];
-        if (q != p) gh_final_term_k(pm[q], vel[q], rx, ry, rz, vp, hs, ih, hf, f);
+      if (active) {
+        ++npass;
+        ncands += s.pp_pot;
+        if (gh_after_pass(s, mp, h_fac, rextent, (mp * t0.x) * hf + rt)) active = false;
+        else if (s.hp > s.h_high) {                                    // :154-170 would walk again
+          single = true;
+          active = false;
+        }
       }
-      niter += (total + 31) >> 5;
+    }
+    // final pass (:317-425)
+    const bool ok = live && !single;
+    const unsigned F = __ballot_sync(FULL, ok);
+    const double hp = h_fac * pow(mp / s.rho, ONETHIRD);
+    const double ih = 1.0 / hp;
+    const double hf = pow(ih, NDIMPR);
+    const double hs = (KERNRANGESQD * hp) * hp;
+    const double4 vp = vel[p];
+    GhFinal f;
+    gh_final_init(f, mp, ih, hf, t0);
+    for (unsigned todo = F; todo != 0u; todo &= todo - 1u) {
+      const int j = __ffs(todo) - 1;
+      const double xj = __shfl_sync(FULL, rx, j), yj = __shfl_sync(FULL, ry, j),
+                   zj = __shfl_sync(FULL, rz, j);
+      const double hsj = __shfl_sync(FULL, hs, j), ihj = __shfl_sync(FULL, ih, j),
+                   hfj = __shfl_sync(FULL, hf, j);
+      const double4 vj = make_double4(__shfl_sync(FULL, vp.x, j), __shfl_sync(FULL, vp.y, j),
+                                      __shfl_sync(FULL, vp.z, j), 0.0);
+      const int pj = __shfl_sync(FULL, p, j);
+      const int nc = gp_flatten(leaves + (size_t)pj * GH_LEAVES, __shfl_sync(FULL, n, j), cand,
+                                lane);
+      GhFinal part;
+      part.rt = 0.0; part.om = 0.0; part.dv = 0.0; part.zt = 0.0;
+      for (int k = lane; k < nc; k += 32) {
+        const int q = cand[k];
+        if (q != pj) gh_final_term_k(pm[q], vel[q], xj, yj, zj, vj, hsj, ihj, hfj, part);
+      }
+      niter += (nc + 31) >> 5;
+      const double srt = warp_sum(part.rt), som = warp_sum(part.om), sdv = warp_sum(part.dv),
+                   szt = warp_sum(part.zt);
+      if (lane == j) {
+        f.rt = f.rt + srt;
+        f.om = f.om + som;
+        f.dv = f.dv + sdv;
+        f.zt = f.zt + szt;
+      }
+    }
+    if (ok) {
       ++npass;
-      ncands += total;
-      GhFinal g;
-      gh_final_init(g, mp, ih, hf, t0);
-      g.rt = g.rt + warp_sum(f.rt);
-      g.om = g.om + warp_sum(f.om);
-      g.dv = g.dv + warp_sum(f.dv);
-      g.zt = g.zt + warp_sum(f.zt);
-      if (lane == 0) gh_store(p, mp, hp, g, hz, rho, omega, divv, drhodt, err);
+      ncands += s.pp_pot;
+      gh_store(p, mp, hp, f, hz, rho, omega, divv, drhodt, err);
+    }
+    if (single) {
+      ++nsingle;
+      redo[atomicAdd(nredo, 1)] = p;
     }
   }
-  if (single && lane == 0) redo[atomicAdd(nredo, 1)] = p;
-  nsingle += single ? 1 : 0;
-  __syncwarp();
-  }
-  if (lane == 0) {
-    atomicAdd(counts + 5, npass);
-    atomicAdd(counts + 6, ncands);
-    atomicAdd(counts + 13, niter);
-    atomicAdd(counts + 15, nsingle);
-  }
+  atomicAdd(counts + 5, npass);
+  atomicAdd(counts + 6, ncands);
+  atomicAdd(counts + 15, nsingle);
+  if (lane == 0) atomicAdd(counts + 13, niter);
 }
 
 // get_neib (sph/get_neib.F90:10-140) for 32 particles per warp: one group walk
@@ -1200,19 +1254,20 @@ void launch_gradh(Ctx& c, int nact) {
   const HydroTree t = hydro_tree(c);
   cudaMemsetAsync(c.work, 0, sizeof(int), c.st);
   k_gradh_walk<<<gr_grid(c, nact, 0), GR_THREADS, GR_SMEM, c.st>>>(
-      nact, c.act, c.pm, c.hz, t, c.leaves, c.nleaf, c.wstack, c.wstack_cap, counts, c.work);
+      nact, c.act, c.pm, c.hz, t, c.leaves, c.nleaf, c.npot, c.wstack, c.wstack_cap, counts,
+      c.work);
   static int occ[16] = {};
   int& o = occ[c.dev >= 0 && c.dev < 16 ? c.dev : 0];
   if (o == 0) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_gradh_pass, GP_THREADS, 0);
     if (o < 1) o = 1;
   }
-  const int blocks = std::min(sm_count(c) * o, nb(nact, GP_WARPS));
+  const int blocks = std::min(sm_count(c) * o, nb(nb(nact, 32), GP_WARPS));
   cudaMemsetAsync(c.work + 1, 0, sizeof(int), c.st);
   k_gradh_pass<<<blocks, GP_THREADS, 0, c.st>>>(
-      nact, c.act, c.pm, c.hz, c.vel, c.rho, c.omega, c.div_v, c.drhodt, t, c.tabA,
-      c.prm.h_fac, c.prm.pp_gather, c.info.rextent, c.leaves, c.nleaf, c.redo, c.work + 1,
-      c.d_err, counts);
+      nact, c.act, c.pm, c.hz, c.vel, c.rho, c.omega, c.div_v, c.drhodt, c.tabA, c.prm.h_fac,
+      c.prm.pp_gather, c.info.rextent, c.leaves, c.nleaf, c.npot, c.redo, c.work + 1, c.d_err,
+      counts);
   k_gradh_redo<<<sm_count(c) * 2, WP_THREADS, 0, c.st>>>(
       c.redo, c.work + 1, c.pm, c.hz, c.vel, c.rho, c.omega, c.div_v, c.drhodt, t, c.tabA,
       c.prm.h_fac, c.prm.pp_gather, c.info.rextent, c.d_err, counts);
