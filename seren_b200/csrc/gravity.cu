@@ -221,6 +221,20 @@ __device__ __forceinline__ void pair32(float d0, float d1, float d2, float invhp
   ap = fmaf(0.5f * mq, dpot, ap);
 }
 
+// pair32 when r >= 2h_p and r >= 2h_q: both kernel branches are Newtonian
+// (the same operations pair32 performs for such a pair)
+__device__ __forceinline__ void pair32_far(float d0, float d1, float d2, float inv, float mq,
+                                           float& ax, float& ay, float& az, float& ap) {
+  const float inv2 = inv * inv;
+  const float grav = inv2 + inv2;
+  const float dpot = inv + inv;
+  const float f = 0.5f * mq * inv * grav;
+  ax = fmaf(f, d0, ax);
+  ay = fmaf(f, d1, ay);
+  az = fmaf(f, d2, az);
+  ap = fmaf(0.5f * mq, dpot, ap);
+}
+
 // BHgrav_accel.F90:159-189 in FP32, dr = rp - rc
 __device__ __forceinline__ void cell32(float d0, float d1, float d2, const float4& a, const float4& q,
                                        float q5, float& ax, float& ay, float& az, float& ap) {
@@ -389,10 +403,22 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
         if constexpr (MIXED) {
           float sx = 0.f, sy = 0.f, sz = 0.f, sp = 0.f;
           for (int e = 0; e < nb; ++e) {
-            if (((R.qmask[b0 + e] >> lane) & 1u) && R.qid[b0 + e] != p) {
-              const float4 a = R.pa[e];
-              const float2 b = R.pb[e];
-              pair32(a.x - ux, a.y - uy, a.z - uz, invhp32, zo32, a.w, b.x, b.y, sx, sy, sz, sp);
+            const bool on = ((R.qmask[b0 + e] >> lane) & 1u) && R.qid[b0 + e] != p;
+            const float4 a = R.pa[e];
+            const float2 b = R.pb[e];
+            const float d0 = a.x - ux, d1 = a.y - uy, d2 = a.z - uz;
+            const float drsqd = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
+            const float inv = rsqrtf(fmaxf(drsqd, 1.0e-30f));
+            const float drmag = drsqd * inv;
+            // pair32's own branch tests: the kernel is needed only inside 2h of either particle
+            const bool soft = on && (drmag * invhp32 < KERNRANGE || drmag * b.x < KERNRANGE);
+            if (__any_sync(FULLMASK, soft)) {
+              if (on) {
+                pair32(d0, d1, d2, invhp32, zo32, a.w, b.x, b.y, sx, sy, sz, sp);
+                ++npair;
+              }
+            } else if (on) {
+              pair32_far(d0, d1, d2, inv, a.w, sx, sy, sz, sp);
               ++npair;
             }
           }

@@ -463,6 +463,25 @@ __device__ __forceinline__ void gh_final_term_k(const double4& Q, const double4&
   f.zt = f.zt + ((Q.w * ih) * ih) * kfn::wg(kern);
 }
 
+// The density term of one candidate without branches: the value
+// gh_density_term_k adds when the candidate counts (r^2 < 4h^2 and its bin
+// below KERNTOT), 0 otherwise, so that the terms of several candidates can be
+// evaluated side by side.
+__device__ __forceinline__ double gh_density_sel(const double4& Q, double rx, double ry,
+                                                 double rz, double hs, double ih, double hf) {
+  const double d0 = Q.x - rx, d1 = Q.y - ry, d2 = Q.z - rz;
+  const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
+  const bool in = drsqd < hs;
+  const double drmag = sqrt(in ? drsqd : 0.0) + SMALL_NUMBER;
+  const int kern = (int)((HALFKERNTOT * drmag) * ih);
+  const int kc = in ? kern : 0;
+  const double s = kfn::bin_s(kc);
+  const double wi = ((1.0 - (1.5 * s) * s) + 0.75 * kfn::pw3(s)) * kfn::INVPI;
+  const double wo = (0.25 * kfn::pw3(2.0 - s)) * kfn::INVPI;
+  const double w = kc < kfn::KERN1 ? wi : wo;
+  return (in && kern < KERNTOT) ? (Q.w * hf) * w : 0.0;
+}
+
 // This lane's entries (those holding its bit) in list order into R.li; the
 // count, or -1 when there are more than GR_PL.
 __device__ __forceinline__ int gr_lane_list(GrShared& R, int nent, unsigned bit, int lane) {
@@ -859,13 +878,19 @@ __global__ void __launch_bounds__(GP_THREADS) k_gradh_pass(
         const int pj = __shfl_sync(FULL, p, j);
         const int nc = gp_flatten(leaves + (size_t)pj * GH_LEAVES, __shfl_sync(FULL, n, j), cand,
                                   lane);
-        double part = 0.0;
-        for (int k = lane; k < nc; k += 32) {
-          const int q = cand[k];
-          if (q != pj) gh_density_term_k(pm[q], xj, yj, zj, hsj, ihj, hfj, part);
+        double part0 = 0.0, part1 = 0.0;            // two candidates per lane at a time
+        for (int k = lane; k < nc; k += 64) {
+          const int q0 = cand[k];
+          const int q1 = k + 32 < nc ? cand[k + 32] : pj;
+          const double4 Q0 = pm[q0];
+          const double4 Q1 = pm[q1];
+          const double w0 = gh_density_sel(Q0, xj, yj, zj, hsj, ihj, hfj);
+          const double w1 = gh_density_sel(Q1, xj, yj, zj, hsj, ihj, hfj);
+          part0 = q0 != pj ? part0 + w0 : part0;
+          part1 = q1 != pj ? part1 + w1 : part1;
         }
         niter += (nc + 31) >> 5;
-        const double sum = warp_sum(part);
+        const double sum = warp_sum(part0 + part1);
         if (lane == j) rt = sum;
       }
       if (active) {
