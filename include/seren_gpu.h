@@ -148,8 +148,9 @@ int seren_gpu_tree_export(seren_gpu_ctx* ctx, int32_t* ctot, int32_t* ltot,
  * entries, [10] of them taken by all 32 lanes, [11] near-field list items,
  * [12] of them for all 32 lanes; grad-h [3] walks, [4] walk entries (with
  * the neighbour-list kernel), [5] passes, [6] candidates, [13] warp
- * iterations over candidates, [15] passes over the union list (a lane's own
- * list overflowed); neighbour lists [7] candidates, [14] warp iterations. */
+ * iterations over candidates; neighbour lists [7] candidates, [14] warp
+ * iterations; [15] particles handed to a single-particle path (grad-h
+ * re-walks and overflows, neighbour-row overflows). */
 int seren_gpu_last_step_stats(seren_gpu_ctx* ctx, double* stage_ms /*[8]*/,
                               int32_t* nlaunch, int64_t* counts /*[16]*/);
 

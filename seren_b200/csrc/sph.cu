@@ -324,15 +324,11 @@ __device__ void neib_one(int p, const double4* __restrict__ pm, const double2* _
 // own particle's test on it (test32 in FP32, exact FP64 otherwise).  A cell
 // that passes for some lanes is opened for exactly those lanes, so the leaves
 // each lane opens are exactly those of its own reference walk.  Opened leaves
-// go to a per-warp list of (leaf, mask) entries, and each lane keeps the
-// indices of its own entries.  The passes over the candidates then take the
-// particles one at a time: the warp flattens that particle's entries into its
-// candidate list and the 32 lanes share out the candidates (independent
-// loads), the partial sums reduced across the warp at the end.
+// go to a per-warp list of (leaf, mask) entries, from which each particle's
+// own leaves are written to its row in global memory for the pass kernels.
 constexpr int GR_THREADS = 128;
 constexpr int GR_WARPS = GR_THREADS / 32;
 constexpr int GR_LCAP = 512;     // (leaf, mask) entries per warp
-constexpr int GR_PL = 64;        // entries in one lane's own list
 
 struct GrShared {
   int code[GR_LCAP];       // leaf: pstart*8 + count-1
@@ -341,8 +337,6 @@ struct GrShared {
   float fh[32];            // hrm32
   unsigned fm[32];         // lanes whose walk reaches the cell
   int fc[32];
-  unsigned short li[GR_PL][32];  // each lane's own entries, in list order
-  int cand[GR_PL * LEAFMAX];     // one particle's candidates
 };
 
 // Walk for the lanes in `lanes`, appending the opened leaves to R.code/R.mask
@@ -432,20 +426,8 @@ __device__ void gr_sort(GrShared& R, int n, int lane) {
   }
 }
 
-// gh_density_term and gh_final_term with the kernel bins evaluated in place
-// (kernel_fns.h, the same values as the tables)
-__device__ __forceinline__ void gh_density_term_k(const double4& Q, double rx, double ry,
-                                                  double rz, double hs, double ih, double hf,
-                                                  double& rt) {
-  const double d0 = Q.x - rx, d1 = Q.y - ry, d2 = Q.z - rz;
-  const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
-  if (drsqd >= hs) return;
-  const double drmag = sqrt(drsqd) + SMALL_NUMBER;
-  const int kern = (int)((HALFKERNTOT * drmag) * ih);
-  if (kern >= KERNTOT) return;
-  rt = rt + (Q.w * hf) * kfn::w0(kern);
-}
-
+// gh_final_term with the kernel bins evaluated in place (kernel_fns.h, the
+// same values as the tables)
 __device__ __forceinline__ void gh_final_term_k(const double4& Q, const double4& V, double rx,
                                                 double ry, double rz, const double4& vp,
                                                 double hs, double ih, double hf, GhFinal& f) {
@@ -480,40 +462,6 @@ __device__ __forceinline__ double gh_density_sel(const double4& Q, double rx, do
   const double wo = (0.25 * kfn::pw3(2.0 - s)) * kfn::INVPI;
   const double w = kc < kfn::KERN1 ? wi : wo;
   return (in && kern < KERNTOT) ? (Q.w * hf) * w : 0.0;
-}
-
-// This lane's entries (those holding its bit) in list order into R.li; the
-// count, or -1 when there are more than GR_PL.
-__device__ __forceinline__ int gr_lane_list(GrShared& R, int nent, unsigned bit, int lane) {
-  int n = 0;
-  for (int e = 0; e < nent; ++e) {
-    if (R.mask[e] & bit) {
-      if (n < GR_PL) R.li[n][lane] = (unsigned short)e;
-      ++n;
-    }
-  }
-  __syncwarp();
-  return n > GR_PL ? -1 : n;
-}
-
-// The candidates of lane j's n own entries, in order, into R.cand; the count.
-__device__ int gr_flatten(GrShared& R, int j, int n, int lane) {
-  int total = 0;
-  __syncwarp();
-  for (int base = 0; base < n; base += 32) {
-    const int t = base + lane;
-    int code = 0, c = 0;
-    if (t < n) {
-      code = R.code[R.li[t][j]];
-      c = (code & 7) + 1;
-    }
-    const int inc = warp_iscan(c, lane);
-    const int o = total + inc - c;
-    for (int k = 0; k < c; ++k) R.cand[o + k] = (code >> 3) + k;
-    total += __shfl_sync(FULL, inc, 31);
-  }
-  __syncwarp();
-  return total;
 }
 
 // sum over the warp, the same value on every lane
@@ -956,23 +904,29 @@ __global__ void __launch_bounds__(GP_THREADS) k_gradh_pass(
   if (lane == 0) atomicAdd(counts + 13, niter);
 }
 
-// get_neib (sph/get_neib.F90:10-140) for 32 particles per warp: one group walk
-// with each lane's gather-or-scatter test (BHhydro_walk.F90:37-43), the opened
-// leaves sorted into depth-first order; then, particle by particle, the warp
-// keeps the candidates with r^2 <= 4h_p^2 or r^2 <= 4h_pp^2 in that order and
-// writes the row with coalesced stores.
-__global__ void __launch_bounds__(GR_THREADS) k_neib_grp(
+// get_neib (sph/get_neib.F90:10-140) in two kernels.
+//
+// k_neib_walk: 32 particles per warp on one group walk with each lane's
+// gather-or-scatter test (BHhydro_walk.F90:37-43); the opened leaves are sorted
+// into depth-first order (the order of the reference's candidate lists) and
+// each particle's go to its own row of c.leaves, their number to c.nleaf (-1
+// when the row or the walk overflows).
+//
+// k_neib_rows: 32 particles per warp; for each particle in turn the warp
+// flattens its row, keeps the candidates with r^2 <= 4h_p^2 or r^2 <= 4h_pp^2
+// in that order and writes them with coalesced stores.  A particle whose row
+// overflowed gets its list from neib_one.
+__global__ void __launch_bounds__(GR_THREADS) k_neib_walk(
     int nact, const int* __restrict__ act, const double4* __restrict__ pm,
-    const double2* __restrict__ hz, HydroTree t, int L, int* __restrict__ pptot,
-    int* __restrict__ pplist, int2* __restrict__ stacks, int scap, DevError* err,
-    unsigned long long* counts, int* work) {
+    const double2* __restrict__ hz, HydroTree t, int* __restrict__ leaves,
+    int* __restrict__ nleaf, int2* __restrict__ stacks, int scap, unsigned long long* counts,
+    int* work) {
   extern __shared__ __align__(16) unsigned char gr_smem[];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   GrShared& R = reinterpret_cast<GrShared*>(gr_smem)[w];
   int2* const S = stacks + (size_t)(blockIdx.x * GR_WARPS + w) * scap;
   const unsigned bit = 1u << lane;
-  const unsigned lt = bit - 1u;
-  unsigned long long nvisit = 0, ncands = 0, niter = 0;
+  unsigned long long nvisit = 0;
   for (int g = gr_next(work, lane); (long long)g * 32 < nact; g = gr_next(work, lane)) {
     const int i = g * 32 + lane;
     const bool live = i < nact;
@@ -980,10 +934,8 @@ __global__ void __launch_bounds__(GR_THREADS) k_neib_grp(
     const double4 P = pm[p];
     const float px = (float)(P.x - t.rootx), py = (float)(P.y - t.rooty),
                 pz = (float)(P.z - t.rootz);
-    const double hp = hz[p].x;
-    const double Rw = KERNRANGE * hp;
+    const double Rw = KERNRANGE * hz[p].x;
     const float R32 = (float)Rw;
-    const double hsp = (KERNRANGESQD * hp) * hp;
     const unsigned lanes = __ballot_sync(FULL, live);
     const int nent = gr_walk(t, lanes, S, scap, R, lane, 0, nvisit, [&](int e) {
       const float4 h32 = R.fa[e];
@@ -1001,23 +953,56 @@ __global__ void __launch_bounds__(GR_THREADS) k_neib_grp(
       const double t2 = t.hrm[c] + h.w;
       return drsqd <= t1 * t1 || drsqd <= t2 * t2;
     });
-    int myn = -1;
+    int n = -1;
     if (nent >= 0) {
       gr_sort(R, nent, lane);
-      myn = gr_lane_list(R, nent, bit, lane);
+      n = 0;
+      int* row = leaves + (size_t)p * GH_LEAVES;
+      for (int e = 0; e < nent; ++e) {
+        if (R.mask[e] & bit) {
+          if (n < GH_LEAVES) row[n] = R.code[e];
+          ++n;
+        }
+      }
+      if (n > GH_LEAVES) n = -1;
     }
-    const unsigned G = __ballot_sync(FULL, live && myn >= 0);
+    if (live) nleaf[p] = n;
+    __syncwarp();
+  }
+  if (lane == 0) atomicAdd(counts + 4, nvisit);
+}
+
+__global__ void __launch_bounds__(GP_THREADS) k_neib_rows(
+    int nact, const int* __restrict__ act, const double4* __restrict__ pm,
+    const double2* __restrict__ hz, HydroTree t, int L, const int* __restrict__ leaves,
+    const int* __restrict__ nleaf, int* __restrict__ pptot, int* __restrict__ pplist,
+    DevError* err, unsigned long long* counts) {
+  __shared__ int cand_all[GP_WARPS][GH_LEAVES * LEAFMAX];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int* cand = cand_all[w];
+  const unsigned lt = (1u << lane) - 1u;
+  unsigned long long ncands = 0, niter = 0, nsingle = 0;
+  for (int g = blockIdx.x * GP_WARPS + w; (long long)g * 32 < nact; g += gridDim.x * GP_WARPS) {
+    const int i = g * 32 + lane;
+    const bool live = i < nact;
+    const int p = live ? (act ? act[i] : i) : (act ? act[nact - 1] : nact - 1);
+    const int n = live ? nleaf[p] : 0;
+    const double4 P = pm[p];
+    const double hp = hz[p].x;
+    const double hsp = (KERNRANGESQD * hp) * hp;
+    const unsigned G = __ballot_sync(FULL, live && n >= 0);
     for (unsigned todo = G; todo != 0u; todo &= todo - 1u) {
       const int j = __ffs(todo) - 1;
       const double xj = __shfl_sync(FULL, P.x, j), yj = __shfl_sync(FULL, P.y, j),
                    zj = __shfl_sync(FULL, P.z, j), hsj = __shfl_sync(FULL, hsp, j);
       const int pj = __shfl_sync(FULL, p, j);
-      const int nc = gr_flatten(R, j, __shfl_sync(FULL, myn, j), lane);
+      const int nc = gp_flatten(leaves + (size_t)pj * GH_LEAVES, __shfl_sync(FULL, n, j), cand,
+                                lane);
       int* row = pplist + (size_t)pj * L;
       int kept = 0;
       for (int b = 0; b < nc; b += 32) {
         const int k = b + lane;
-        const int q = k < nc ? R.cand[k] : pj;
+        const int q = k < nc ? cand[k] : pj;
         bool keep = false;
         if (q != pj) {
           const double4 Q = pm[q];
@@ -1036,11 +1021,14 @@ __global__ void __launch_bounds__(GR_THREADS) k_neib_grp(
       ncands += nc;
       if (lane == 0) pptot[pj] = kept;
     }
-    if (live && myn < 0) neib_one(p, pm, hz, t, L, pptot, pplist, err);   // list overflow
+    if (live && n < 0) {
+      ++nsingle;
+      neib_one(p, pm, hz, t, L, pptot, pplist, err);
+    }
     __syncwarp();
   }
+  atomicAdd(counts + 15, nsingle);
   if (lane == 0) {
-    atomicAdd(counts + 4, nvisit);
     atomicAdd(counts + 7, ncands);
     atomicAdd(counts + 14, niter);
   }
@@ -1246,8 +1234,8 @@ static int gr_blocks_per_sm(int dev, int which) {
       cudaFuncSetAttribute(k_gradh_walk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GR_SMEM);
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_gradh_walk, GR_THREADS, GR_SMEM);
     } else {
-      cudaFuncSetAttribute(k_neib_grp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GR_SMEM);
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_neib_grp, GR_THREADS, GR_SMEM);
+      cudaFuncSetAttribute(k_neib_walk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GR_SMEM);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_neib_walk, GR_THREADS, GR_SMEM);
     }
     if (r < 1) r = 1;
   }
@@ -1301,11 +1289,22 @@ void launch_gradh(Ctx& c, int nact) {
 
 void launch_neib(Ctx& c, int nact) {
   if (nact <= 0) return;
+  unsigned long long* counts = reinterpret_cast<unsigned long long*>(c.d_counts);
+  const HydroTree t = hydro_tree(c);
   cudaMemsetAsync(c.work, 0, sizeof(int), c.st);
-  k_neib_grp<<<gr_grid(c, nact, 1), GR_THREADS, GR_SMEM, c.st>>>(
-      nact, c.act, c.pm, c.hz, hydro_tree(c), c.prm.pp_limit, c.pptot, c.pplist, c.wstack,
-      c.wstack_cap, c.d_err, reinterpret_cast<unsigned long long*>(c.d_counts), c.work);
-  ++c.nlaunch;
+  k_neib_walk<<<gr_grid(c, nact, 1), GR_THREADS, GR_SMEM, c.st>>>(
+      nact, c.act, c.pm, c.hz, t, c.leaves, c.nleaf, c.wstack, c.wstack_cap, counts, c.work);
+  static int occ[16] = {};
+  int& o = occ[c.dev >= 0 && c.dev < 16 ? c.dev : 0];
+  if (o == 0) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_neib_rows, GP_THREADS, 0);
+    if (o < 1) o = 1;
+  }
+  const int blocks = std::min(sm_count(c) * o, nb(nb(nact, 32), GP_WARPS));
+  k_neib_rows<<<blocks, GP_THREADS, 0, c.st>>>(nact, c.act, c.pm, c.hz, t, c.prm.pp_limit,
+                                               c.leaves, c.nleaf, c.pptot, c.pplist, c.d_err,
+                                               counts);
+  c.nlaunch += 2;
 }
 
 void launch_hydro(Ctx& c, int nact) {
