@@ -426,44 +426,6 @@ __device__ void gr_sort(GrShared& R, int n, int lane) {
   }
 }
 
-// gh_final_term with the kernel bins evaluated in place (kernel_fns.h, the
-// same values as the tables)
-__device__ __forceinline__ void gh_final_term_k(const double4& Q, const double4& V, double rx,
-                                                double ry, double rz, const double4& vp,
-                                                double hs, double ih, double hf, GhFinal& f) {
-  const double d0 = Q.x - rx, d1 = Q.y - ry, d2 = Q.z - rz;
-  double drmag = (d0 * d0 + d1 * d1) + d2 * d2;
-  if (drmag > hs) return;
-  drmag = sqrt(drmag) + SMALL_NUMBER;
-  const int kern = (int)((HALFKERNTOT * drmag) * ih);
-  if (kern > KERNTOT) return;
-  const double dv0 = V.x - vp.x, dv1 = V.y - vp.y, dv2 = V.z - vp.z;
-  const double dvdr = (dv0 * d0 + dv1 * d1) + dv2 * d2;
-  f.rt = f.rt + (Q.w * hf) * kfn::w0(kern);
-  f.om = f.om + ((Q.w * hf) * ih) * kfn::wh(kern);
-  f.dv = f.dv - ((((Q.w * dvdr) * kfn::w4(kern)) * hf) * ih) / drmag;
-  f.zt = f.zt + ((Q.w * ih) * ih) * kfn::wg(kern);
-}
-
-// The density term of one candidate without branches: the value
-// gh_density_term_k adds when the candidate counts (r^2 < 4h^2 and its bin
-// below KERNTOT), 0 otherwise, so that the terms of several candidates can be
-// evaluated side by side.
-__device__ __forceinline__ double gh_density_sel(const double4& Q, double rx, double ry,
-                                                 double rz, double hs, double ih, double hf) {
-  const double d0 = Q.x - rx, d1 = Q.y - ry, d2 = Q.z - rz;
-  const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
-  const bool in = drsqd < hs;
-  const double drmag = sqrt(in ? drsqd : 0.0) + SMALL_NUMBER;
-  const int kern = (int)((HALFKERNTOT * drmag) * ih);
-  const int kc = in ? kern : 0;
-  const double s = kfn::bin_s(kc);
-  const double wi = ((1.0 - (1.5 * s) * s) + 0.75 * kfn::pw3(s)) * kfn::INVPI;
-  const double wo = (0.25 * kfn::pw3(2.0 - s)) * kfn::INVPI;
-  const double w = kc < kfn::KERN1 ? wi : wo;
-  return (in && kern < KERNTOT) ? (Q.w * hf) * w : 0.0;
-}
-
 // sum over the warp, the same value on every lane
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -758,6 +720,29 @@ __global__ void __launch_bounds__(GR_THREADS) k_gradh_walk(
 
 constexpr int GP_THREADS = 128;
 constexpr int GP_WARPS = GP_THREADS / 32;
+constexpr int GP_INB = 128;      // packed in-range candidates per warp
+
+// The density term (:218-230) and the final-pass terms (:360-425) of one
+// candidate inside 2h, from its r^2, mass and dv.dr (the same operations as
+// gh_density_term and gh_final_term).
+__device__ __forceinline__ void gh_density_in(double d2, double m, double ih, double hf,
+                                              double& rt) {
+  const double drmag = sqrt(d2) + SMALL_NUMBER;
+  const int kern = (int)((HALFKERNTOT * drmag) * ih);
+  if (kern >= KERNTOT) return;
+  rt = rt + (m * hf) * kfn::w0(kern);
+}
+
+__device__ __forceinline__ void gh_final_in(double d2, double m, double dvdr, double ih,
+                                            double hf, GhFinal& f) {
+  const double drmag = sqrt(d2) + SMALL_NUMBER;
+  const int kern = (int)((HALFKERNTOT * drmag) * ih);
+  if (kern > KERNTOT) return;
+  f.rt = f.rt + (m * hf) * kfn::w0(kern);
+  f.om = f.om + ((m * hf) * ih) * kfn::wh(kern);
+  f.dv = f.dv - ((((m * dvdr) * kfn::w4(kern)) * hf) * ih) / drmag;
+  f.zt = f.zt + ((m * ih) * ih) * kfn::wg(kern);
+}
 
 // A particle's row of opened leaves flattened into its candidates, in order;
 // returns the count.
@@ -793,8 +778,13 @@ __global__ void __launch_bounds__(GP_THREADS) k_gradh_pass(
     const int* __restrict__ nleaf, const int* __restrict__ npot, int* __restrict__ redo,
     int* __restrict__ nredo, DevError* err, unsigned long long* counts) {
   __shared__ int cand_all[GP_WARPS][GH_LEAVES * LEAFMAX];
+  __shared__ double inb_all[GP_WARPS][3][GP_INB];   // candidates inside 2h: r^2, m, dv.dr
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   int* cand = cand_all[w];
+  double* ind2 = inb_all[w][0];
+  double* inm = inb_all[w][1];
+  double* indv = inb_all[w][2];
+  const unsigned lt = (1u << lane) - 1u;
   const double4 t0 = tabA[0];
   unsigned long long npass = 0, ncands = 0, niter = 0, nsingle = 0;
   for (int g = blockIdx.x * GP_WARPS + w; (long long)g * 32 < nact; g += gridDim.x * GP_WARPS) {
@@ -826,19 +816,33 @@ __global__ void __launch_bounds__(GP_THREADS) k_gradh_pass(
         const int pj = __shfl_sync(FULL, p, j);
         const int nc = gp_flatten(leaves + (size_t)pj * GH_LEAVES, __shfl_sync(FULL, n, j), cand,
                                   lane);
-        double part0 = 0.0, part1 = 0.0;            // two candidates per lane at a time
-        for (int k = lane; k < nc; k += 64) {
-          const int q0 = cand[k];
-          const int q1 = k + 32 < nc ? cand[k + 32] : pj;
-          const double4 Q0 = pm[q0];
-          const double4 Q1 = pm[q1];
-          const double w0 = gh_density_sel(Q0, xj, yj, zj, hsj, ihj, hfj);
-          const double w1 = gh_density_sel(Q1, xj, yj, zj, hsj, ihj, hfj);
-          part0 = q0 != pj ? part0 + w0 : part0;
-          part1 = q1 != pj ? part1 + w1 : part1;
+        // r^2 of every candidate; those inside 2h (:218) are packed into the
+        // buffer, whose terms are then evaluated 32 at a time
+        double part = 0.0;
+        int nin = 0;
+        for (int b = 0; b < nc; b += 32) {
+          const int k = b + lane;
+          const int q = k < nc ? cand[k] : pj;
+          const double4 Q = pm[q];
+          const double d0 = Q.x - xj, d1 = Q.y - yj, d2 = Q.z - zj;
+          const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
+          const bool in = q != pj && drsqd < hsj;
+          const unsigned m = __ballot_sync(FULL, in);
+          if (in) {
+            const int o = nin + __popc(m & lt);
+            ind2[o] = drsqd;
+            inm[o] = Q.w;
+          }
+          nin += __popc(m);
+          if (nin > GP_INB - 32 || b + 32 >= nc) {
+            __syncwarp();
+            for (int t = lane; t < nin; t += 32) gh_density_in(ind2[t], inm[t], ihj, hfj, part);
+            nin = 0;
+            __syncwarp();
+          }
         }
         niter += (nc + 31) >> 5;
-        const double sum = warp_sum(part0 + part1);
+        const double sum = warp_sum(part);
         if (lane == j) rt = sum;
       }
       if (active) {
@@ -874,9 +878,31 @@ __global__ void __launch_bounds__(GP_THREADS) k_gradh_pass(
                                 lane);
       GhFinal part;
       part.rt = 0.0; part.om = 0.0; part.dv = 0.0; part.zt = 0.0;
-      for (int k = lane; k < nc; k += 32) {
-        const int q = cand[k];
-        if (q != pj) gh_final_term_k(pm[q], vel[q], xj, yj, zj, vj, hsj, ihj, hfj, part);
+      int nin = 0;
+      for (int b = 0; b < nc; b += 32) {
+        const int k = b + lane;
+        const int q = k < nc ? cand[k] : pj;
+        const double4 Q = pm[q];
+        const double d0 = Q.x - xj, d1 = Q.y - yj, d2 = Q.z - zj;
+        const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
+        const bool in = q != pj && drsqd <= hsj;                      // :360
+        const unsigned m = __ballot_sync(FULL, in);
+        if (in) {
+          const double4 V = vel[q];
+          const double dv0 = V.x - vj.x, dv1 = V.y - vj.y, dv2 = V.z - vj.z;
+          const int o = nin + __popc(m & lt);
+          ind2[o] = drsqd;
+          inm[o] = Q.w;
+          indv[o] = (dv0 * d0 + dv1 * d1) + dv2 * d2;
+        }
+        nin += __popc(m);
+        if (nin > GP_INB - 32 || b + 32 >= nc) {
+          __syncwarp();
+          for (int t = lane; t < nin; t += 32)
+            gh_final_in(ind2[t], inm[t], indv[t], ihj, hfj, part);
+          nin = 0;
+          __syncwarp();
+        }
       }
       niter += (nc + 31) >> 5;
       const double srt = warp_sum(part.rt), som = warp_sum(part.om), sdv = warp_sum(part.dv),
