@@ -820,21 +820,28 @@ __global__ void __launch_bounds__(GP_THREADS) k_gradh_pass(
         // buffer, whose terms are then evaluated 32 at a time
         double part = 0.0;
         int nin = 0;
-        for (int b = 0; b < nc; b += 32) {
-          const int k = b + lane;
-          const int q = k < nc ? cand[k] : pj;
-          const double4 Q = pm[q];
-          const double d0 = Q.x - xj, d1 = Q.y - yj, d2 = Q.z - zj;
-          const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
-          const bool in = q != pj && drsqd < hsj;
-          const unsigned m = __ballot_sync(FULL, in);
-          if (in) {
-            const int o = nin + __popc(m & lt);
-            ind2[o] = drsqd;
-            inm[o] = Q.w;
+        for (int b = 0; b < nc; b += 64) {           // two chunks of candidates in flight
+          const int k0 = b + lane, k1 = b + 32 + lane;
+          const int q0 = k0 < nc ? cand[k0] : pj;
+          const int q1 = k1 < nc ? cand[k1] : pj;
+          const double4 Q0 = pm[q0];
+          const double4 Q1 = pm[q1];
+#pragma unroll
+          for (int u = 0; u < 2; ++u) {
+            const double4 Q = u == 0 ? Q0 : Q1;
+            const int q = u == 0 ? q0 : q1;
+            const double d0 = Q.x - xj, d1 = Q.y - yj, d2 = Q.z - zj;
+            const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
+            const bool in = q != pj && drsqd < hsj;
+            const unsigned m = __ballot_sync(FULL, in);
+            if (in) {
+              const int o = nin + __popc(m & lt);
+              ind2[o] = drsqd;
+              inm[o] = Q.w;
+            }
+            nin += __popc(m);
           }
-          nin += __popc(m);
-          if (nin > GP_INB - 32 || b + 32 >= nc) {
+          if (nin > GP_INB - 64 || b + 64 >= nc) {
             __syncwarp();
             for (int t = lane; t < nin; t += 32) gh_density_in(ind2[t], inm[t], ihj, hfj, part);
             nin = 0;
