@@ -770,7 +770,7 @@ __device__ __forceinline__ int gp_flatten(const int* __restrict__ row, int n, in
 // state, so the per-particle arithmetic of a pass (h, its powers, the update
 // of :238-285) runs once per lane for all 32; each particle's candidates are
 // shared out over the 32 lanes in turn.
-__global__ void __launch_bounds__(GP_THREADS) k_gradh_pass(
+__global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
     int nact, const int* __restrict__ act, const double4* __restrict__ pm, double2* __restrict__ hz,
     const double4* __restrict__ vel, double* __restrict__ rho, double* __restrict__ omega,
     double* __restrict__ divv, double* __restrict__ drhodt, const double4* __restrict__ tabA,
