@@ -1095,7 +1095,7 @@ __device__ __forceinline__ float m4_w1_bin(float x, bool tc) {
 }
 
 template <bool MIXED>
-__global__ void __launch_bounds__(128) k_hydro(int nact, const int* __restrict__ act,
+__global__ void __launch_bounds__(128, 8) k_hydro(int nact, const int* __restrict__ act,
                                                const double4* __restrict__ pm,
                                                const double2* __restrict__ hz,
                                                const double4* __restrict__ vel,
