@@ -55,6 +55,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=("core", "batched"), default="core",
+                    help="core: the turbulent core at N (default); batched: 256 independent "
+                         "clouds shared out across the ranks")
     ap.add_argument("--cpu-sample", type=int, default=0,
                     help="active particles in the CPU sample (default N, or N/8 above 2^20)")
     return ap.parse_args()
@@ -349,12 +352,72 @@ def gravity_accuracy(ic, parray, nsub=256):
 
 
 # ---------------------------------------------------------------------------
+def batched_main(args, ws, rank, local):
+    """256 independent clouds (N_i log-uniform in [8192, 262144], about 12M
+    particles): each rank takes its longest-processing-time share and keeps
+    one device-resident context per cloud; a step is a drift and force
+    evaluation of every cloud.  Total work is fixed, so scaling is strong."""
+    import torch
+
+    from seren_b200 import ics
+    from seren_b200.batch import CloudBatch, lpt_partition
+    torch.cuda.set_device(local)
+    clouds = ics.batched_clouds()
+    ns = [c["parray"].shape[0] for c in clouds]
+    mine = lpt_partition(ns, ws)[rank]
+    b = CloudBatch([clouds[i] for i in mine], precision=1)
+    del clouds
+    b.step(first_call=True)
+    for _ in range(max(args.warmup, 1) - 1):
+        b.step(dt=DT)
+    sampler = ClockSampler(local)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches = 0
+    torch.cuda.synchronize()
+    barrier(ws)
+    torch.cuda.synchronize()
+    sampler.start()
+    start.record()
+    for _ in range(args.steps):
+        launches += b.step(dt=DT)          # each context's calls synchronise their stream
+    end.record()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    barrier(ws)
+    t = max_over_ranks(ws, start.elapsed_time(end))
+    b.close()
+    total = sum(ns)
+    value = total * args.steps / (t * 1e-3)
+    log(f"[bench] batched: rank {rank} {len(mine)} clouds, {b.n} particles; "
+        f"{t / args.steps:.2f} ms/step (max over ranks)")
+    if rank != 0:
+        return
+    print(json.dumps({
+        "metric": "particle force evals/sec (grav+hydro), 256 independent clouds",
+        "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t / args.steps, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "fp32+fp64",
+        "data": "synthetic (256 seeded uniform-sphere clouds, numpy PCG64, seeds 1000+i)",
+        "config": {"workload": f"batched clouds: 256 uniform spheres, N_i log-uniform in "
+                               f"[8192, 262144] (total {total}), c_s ~ U[0.05, 0.3], "
+                               "h_fac=1.2, theta^2=0.25, MON97 alpha=1; each cloud its own tree; "
+                               "step = drift + full force evaluation of every cloud",
+                   "particles": total, "precision": "mixed (FP32 pair arithmetic, FP64 walk/"
+                   "MAC/grad-h)", "parallelism": f"clouds sharded over {ws} ranks "
+                   "(longest-processing-time on N log N), no exchange",
+                   "l2": "inputs larger than L2"},
+        "e2e": None, "cpu_baseline": None, "roofline": None,
+        "gpu_launches": launches, "clocks": clocks}), flush=True)
+
+
 def main():
     args = parse()
     ws, rank, local = dist_init(args.gpus)
     n = args.n
     if args.impl == "reference":
         return reference_arm(args, ws, rank, n)
+    if args.workload == "batched":
+        return batched_main(args, ws, rank, local)
     import torch
     torch.cuda.set_device(local)
     ic = workload(n)
@@ -431,7 +494,7 @@ def main():
         "fp64": fp64,
         "mixed_speedup_vs_fp64": (value / fp64["value"]) if fp64 else None,
         "accuracy": acc,
-        "roofline": {"bound": "fp32", "kernel": "gravity walk (k_grav32)",
+        "roofline": {"bound": "fp32", "kernel": "gravity walk (k_grav_walk<true>)",
                      "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                      "frac": achieved / fp32_peak, "traffic": traffic_per_launch(n),
                      "flops_per_launch": flops, "cells": ncell, "pairs": npair,
