@@ -51,13 +51,17 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--n", type=int, default=N_FULL, help="particle count (default 4,194,304)")
+    ap.add_argument("--n", type=int, default=0,
+                    help="particle count (default: 4,194,304 for core, 1,048,576 for plummer, "
+                         "8,388,608 for disc)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=("core", "batched"), default="core",
-                    help="core: the turbulent core at N (default); batched: 256 independent "
-                         "clouds shared out across the ranks")
+    ap.add_argument("--workload", choices=("core", "plummer", "disc", "batched"), default="core",
+                    help="core: the turbulent core (default, the headline); plummer: Plummer "
+                         "sphere, gravity accuracy over theta^2 in {0.09, 0.25, 0.49}; disc: "
+                         "protostellar disc around a sink; batched: 256 independent clouds "
+                         "shared out across the ranks")
     ap.add_argument("--cpu-sample", type=int, default=0,
                     help="active particles in the CPU sample (default N, or N/8 above 2^20)")
     return ap.parse_args()
@@ -145,12 +149,42 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-def workload(n):
+WORKLOAD_N = {"core": N_FULL, "plummer": 1048576, "disc": 8388608}
+
+
+def workload(n, kind="core"):
+    """Seeded synthetic inputs with the configs' shapes and distributions."""
     from seren_b200 import ics
     t0 = time.time()
-    ic = ics.turbulent_core(n=n, seed=4, sound=0.2, mach=2.0, h_fac=1.2, thetamaxsqd=0.25)
+    if kind == "plummer":
+        ic = ics.plummer(n=n, seed=2, thetamaxsqd=0.25)
+    elif kind == "disc":
+        ic = ics.protostellar_disc(n=n, seed=5)
+    else:
+        ic = ics.turbulent_core(n=n, seed=4, sound=0.2, mach=2.0, h_fac=1.2, thetamaxsqd=0.25)
     log(f"[bench] workload {ic['name']} generated in {time.time() - t0:.1f}s")
     return ic
+
+
+def workload_info(kind, n):
+    """(metric, data, config workload text) of a workload."""
+    if kind == "plummer":
+        return ("particle force evals/sec (grav+hydro), Plummer sphere N=1M",
+                "synthetic (seeded Plummer sphere, numpy PCG64)",
+                f"Plummer sphere a=1 M=1, N={n} per GPU, radii redrawn beyond 20a, AHW velocities, "
+                "h_fac for 50 neighbours, c_s=0 (gravity only), theta^2=0.25 (sweep 0.09/0.25/0.49 "
+                "in theta_sweep); step = full force evaluation + drift")
+    if kind == "disc":
+        return ("particle force evals/sec (grav+hydro), protostellar disc N=8M with a sink",
+                "synthetic (seeded protostellar disc, numpy PCG64)",
+                f"protostellar disc, N={n} per GPU, M_disc=0.1 on R in [0.1, 10] (R uniform), "
+                "H=0.05R, c_s=0.05 R^-0.25, Keplerian + pressure correction, one sink M=1 "
+                "h=0.05 at the origin (sink-gas forces FP64 direct), h_fac=1.2, theta^2=0.25; "
+                "step = full force evaluation + drift")
+    return (METRIC, "synthetic (seeded turbulent uniform-sphere core, numpy PCG64)",
+            f"turbulent molecular-cloud core, N={n} per GPU, uniform sphere R=1 M=1 G=1, "
+            "isothermal c_s=0.2, P(k)~k^-4 Mach 2, h_fac=1.2 (pp_gather 57), theta^2=0.25 "
+            "quadrupole geometric MAC, MON97 alpha=1; step = full force evaluation + drift")
 
 
 def params_for(ic, precision):
@@ -167,6 +201,8 @@ def run_resident(ic, precision, steps, warmup, ws):
     n = ic["parray"].shape[0]
     g = GpuHotPath(n, params_for(ic, precision))
     g.upload(ic["parray"], ic["v"], ic["sound"] ** 2)
+    if ic.get("sink") is not None:
+        g.set_sinks(ic["sink"])
     stream = torch.cuda.ExternalStream(g.stream())
     g.force_step(first_call=True)
     for _ in range(max(warmup, 1) - 1):
@@ -413,14 +449,23 @@ def batched_main(args, ws, rank, local):
 def main():
     args = parse()
     ws, rank, local = dist_init(args.gpus)
-    n = args.n
+    if args.workload == "batched":
+        if args.impl == "reference":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the reference arm times "
+                                  "the core workload only"}), flush=True)
+            return
+        return batched_main(args, ws, rank, local)
+    n = args.n or WORKLOAD_N[args.workload]
     if args.impl == "reference":
         return reference_arm(args, ws, rank, n)
-    if args.workload == "batched":
-        return batched_main(args, ws, rank, local)
     import torch
     torch.cuda.set_device(local)
-    ic = workload(n)
+    ic = workload(n, args.workload)
+    metric, data, wdesc = workload_info(args.workload, n)
+    if args.workload != "core":        # the e2e and CPU legs belong to the headline workload
+        args.no_e2e = True
+        args.no_cpu_baseline = True
     sampler = ClockSampler(local)
     # mixed precision: the headline
     sampler.start()
@@ -474,18 +519,29 @@ def main():
                            f"random active particles, scaled by N/{sample}; "
                            f"{r['sec']:.2f} s per evaluation"))
         r["oracle"].close()
-        acc.update(gravity_accuracy(ic, st["parray"]))
+    if rank == 0 and ws == 1:
+        acc.update(gravity_accuracy(ic, state_m["parray"],
+                                    nsub=4096 if args.workload == "plummer" else 256))
+    sweep = None
+    if args.workload == "plummer" and rank == 0 and ws == 1:
+        sweep = {}
+        for th in (0.09, 0.25, 0.49):
+            ic_th = dict(ic, thetamaxsqd=th)
+            r_th, st_th = run_resident(ic_th, 1, 2, 2, ws)
+            r_th["ctx"].close()
+            a_th = gravity_accuracy(ic_th, st_th["parray"], nsub=4096)
+            sweep[str(th)] = dict(gravity_ms=round(r_th["stage_ms"][4], 3),
+                                  step_ms=round(r_th["total_ms"] / 2, 3),
+                                  cells=r_th["counts"][0], pairs=r_th["counts"][1], **a_th)
+            log(f"[bench] theta^2={th}: {sweep[str(th)]}")
     if rank != 0:
         return
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "metric": metric, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_mixed / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "fp32+fp64",
-        "data": "synthetic (seeded turbulent uniform-sphere core, numpy PCG64)",
-        "config": {"workload": f"turbulent molecular-cloud core, N={n} per GPU, uniform sphere "
-                               "R=1 M=1 G=1, isothermal c_s=0.2, P(k)~k^-4 Mach 2, h_fac=1.2 "
-                               "(pp_gather 57), theta^2=0.25 quadrupole geometric MAC, "
-                               "MON97 alpha=1; step = full force evaluation + drift",
+        "data": data,
+        "config": {"workload": wdesc,
                    "particles": n, "precision": "mixed (FP32 pair arithmetic, FP64 walk/MAC/"
                    "grad-h)", "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
                    "l2": "inputs larger than L2 (particles + tree ~1 GB resident)"},
@@ -494,6 +550,7 @@ def main():
         "fp64": fp64,
         "mixed_speedup_vs_fp64": (value / fp64["value"]) if fp64 else None,
         "accuracy": acc,
+        "theta_sweep": sweep,
         "roofline": {"bound": "fp32", "kernel": "gravity walk (k_grav_walk<true>)",
                      "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                      "frac": achieved / fp32_peak, "traffic": traffic_per_launch(n),
@@ -521,7 +578,8 @@ def reference_arm(args, ws, rank, n):
             import torch.distributed as dist
             dist.destroy_process_group()
         return
-    ic = workload(n)
+    ic = workload(n, args.workload)
+    metric, data, wdesc = workload_info(args.workload, n)
     sample = args.cpu_sample or (n if n <= (1 << 20) else n // 32)
     state = dict(parray=ic["parray"].copy(), v=ic["v"], sound=ic["sound"], h_fac=ic["h_fac"],
                  thetamaxsqd=ic["thetamaxsqd"], alpha=ic["alpha"])
@@ -540,12 +598,10 @@ def reference_arm(args, ws, rank, n):
             total += r["sec"]
     value = n * args.steps / total
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "metric": metric, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp64",
-        "data": "synthetic (seeded turbulent uniform-sphere core, numpy PCG64)",
-        "config": {"workload": f"turbulent molecular-cloud core, N={n}, as the GPU arm",
-                   "particles": n},
+        "data": data, "config": {"workload": wdesc, "particles": n},
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": (f"C++ FP64 restatement of the reference (oracle/; the Fortran "

@@ -125,6 +125,11 @@ int seren_gpu_upload(seren_gpu_ctx* ctx, int32_t ptot, const double* parray,
                      const double* v, const double* csq);
 int seren_gpu_force_step(seren_gpu_ctx* ctx, int32_t first_call);
 int seren_gpu_drift(seren_gpu_ctx* ctx, double dt);
+/* Sinks for the device-resident step: from the next seren_gpu_force_step on,
+ * its gravity adds direct_sink_gravity (sinks/direct_sink_gravity.F90:10-64)
+ * for sink_rmh[s] = {x, y, z, m, h}, as seren_gpu_grav_forces does with
+ * nsink > 0 (at most 1024 sinks; nsink = 0 removes them). */
+int seren_gpu_set_sinks(seren_gpu_ctx* ctx, int32_t nsink, const double* sink_rmh);
 int seren_gpu_download(seren_gpu_ctx* ctx, double* parray, double* v, double* rho,
                        double* omega, double* a, double* gpot, int32_t* perm_total);
 

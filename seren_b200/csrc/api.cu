@@ -194,7 +194,7 @@ void free_all(Ctx& c) {
                 c.pptot, c.pplist, c.stage, c.istage, c.keys, c.keys_alt, c.idx, c.idx_alt,
                 c.rs_hist, c.bbox_part, c.branch, c.branch_next, c.nchild, c.choff, c.cstart,
                 c.bflag, c.bscan, c.leaf, c.nextcell, c.ifopen, c.pstart, c.pcount, c.parent,
-                c.level, c.nkids, c.work, c.wstack, c.leaves, c.nleaf, c.npot, c.redo, c.link, c.gA, c.gB, c.gC, c.wA, c.wLo, c.hA, c.hrm, c.hA32, c.hrm32, c.hmax, c.bbmin, c.bbmax, c.d_info,
+                c.level, c.nkids, c.work, c.sinks, c.wstack, c.leaves, c.nleaf, c.npot, c.redo, c.wide, c.link, c.gA, c.gB, c.gC, c.wA, c.wLo, c.hA, c.hrm, c.hA32, c.hrm32, c.hmax, c.bbmin, c.bbmax, c.d_info,
                 c.d_err, c.d_counts, c.tabA, c.tabG, c.scan.total, c.scan.level_buf[0],
                 c.scan.level_buf[1], c.scan.level_buf[2], c.scan.level_buf[3]};
   for (void* p : ps)
@@ -228,11 +228,11 @@ int alloc_all(Ctx& c) {
   bad |= alloc(c.leaf, C) | alloc(c.nextcell, C) | alloc(c.ifopen, C) | alloc(c.pstart, C) |
          alloc(c.pcount, C) | alloc(c.parent, C) | alloc(c.level, C) | alloc(c.link, C);
   bad |= alloc(c.hA32, C) | alloc(c.hrm32, C) | alloc(c.nkids, C) | alloc(c.work, 4);
-  bad |= alloc(c.leaves, P * 128) | alloc(c.nleaf, P) | alloc(c.npot, P) | alloc(c.redo, P);
+  bad |= alloc(c.leaves, P * 256) | alloc(c.nleaf, P) | alloc(c.npot, P) | alloc(c.redo, P) | alloc(c.wide, P);
   bad |= alloc(c.gA, C) | alloc(c.gB, C) | alloc(c.gC, C) | alloc(c.wA, C) | alloc(c.wLo, C) |
          alloc(c.hA, C) | alloc(c.hrm, C) |
          alloc(c.hmax, C) | alloc(c.bbmin, C) | alloc(c.bbmax, C);
-  bad |= alloc(c.d_info, 1) | alloc(c.d_err, 1) | alloc(c.d_counts, 32);
+  bad |= alloc(c.d_info, 1) | alloc(c.d_err, 1) | alloc(c.d_counts, 32) | alloc(c.sinks, 5 * 1024);
   bad |= alloc(c.tabA, KERNTOT + 1) | alloc(c.tabG, KERNTOT + 1);
   c.wstack_slots = std::max(grav_walk_slots(c), hydro_walk_slots(c));
   c.wstack_cap = grav_walk_stack_cap(c);
@@ -594,7 +594,7 @@ int seren_gpu_force_step(seren_gpu_ctx* h, int32_t first_call) {
   seren::launch_thermal(c);
   seren::launch_hydro(c, n);
   cudaEventRecord(c.ev[4], c.st);
-  seren::launch_grav(c, n, 0, nullptr);
+  seren::launch_grav(c, n, c.nsink, c.nsink > 0 ? c.sinks : nullptr);
   cudaEventRecord(c.ev[5], c.st);
   rc = finish(c, "force_step");
   if (rc) return rc;
@@ -609,6 +609,17 @@ int seren_gpu_force_step(seren_gpu_ctx* h, int32_t first_call) {
   cudaEventElapsedTime(&tot, c.ev[0], c.ev[5]);
   c.stage_ms[5] = tot;
   return SEREN_GPU_OK;
+}
+
+int seren_gpu_set_sinks(seren_gpu_ctx* h, int32_t nsink, const double* sink_rmh) {
+  if (!h) return SEREN_GPU_ERR_ARG;
+  Ctx& c = h->c;
+  if (nsink < 0 || nsink > 1024 || (nsink > 0 && !sink_rmh))
+    return fail(c, SEREN_GPU_ERR_ARG, "set_sinks: 0 <= nsink <= 1024 with sink_rmh given");
+  if (nsink > 0)
+    cudaMemcpyAsync(c.sinks, sink_rmh, sizeof(double) * 5 * nsink, cudaMemcpyHostToDevice, c.st);
+  c.nsink = nsink;
+  return finish(c, "set_sinks");
 }
 
 int seren_gpu_drift(seren_gpu_ctx* h, double dt) {

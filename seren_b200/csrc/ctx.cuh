@@ -98,10 +98,13 @@ struct Ctx {
   DevError* d_err = nullptr;
   int* d_counts = nullptr;    // [16] int64 interaction counters (as 2 ints each)
   int* work = nullptr;        // work counter of the persistent kernels
-  int* leaves = nullptr;      // [pmax][128] opened leaves of each particle's grad-h walk
+  double* sinks = nullptr;    // [1024][5] sinks of the device-resident step (x, y, z, m, h)
+  int nsink = 0;
+  int* leaves = nullptr;      // [pmax][256] opened leaves of each particle's grad-h walk
   int* nleaf = nullptr;       // their number (-1: overflow)
   int* npot = nullptr;        // [pmax] particles in those leaves (pp_pot)
-  int* redo = nullptr;        // [pmax] particles whose grad-h is redone alone; count in work[1]
+  int* redo = nullptr;
+  int* wide = nullptr;        // [pmax] particles whose grad-h walks cover most of the tree; count in work[2]        // [pmax] particles whose grad-h is redone alone; count in work[1]
   int2* wstack = nullptr;     // walk stacks, wstack_cap (cell, lane mask) entries per warp slot
   int wstack_cap = 0;
   int wstack_slots = 0;

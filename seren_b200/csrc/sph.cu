@@ -32,42 +32,6 @@ struct HydroTree {
   float delta;          // bound on the FP32 rounding of a root-relative coordinate
 };
 
-// BHtree/BHhydrowalk_hgather.F90:11-77 (gather test only).  f(q) is called
-// for every particle of every opened leaf.  Returns false when the walk
-// exceeded its cap (a corrupt tree), after flagging the error.
-template <class F>
-__device__ __forceinline__ bool walk_gather(const HydroTree& t, double rx, double ry, double rz,
-                                            double hrange, DevError* err, int who, F&& f) {
-  int c = 0;
-  int visits = 0;
-  const int cap = t.ctot + 2;
-  while (true) {
-    if (++visits > cap) {
-      set_error(err, SEREN_GPU_ERR_WALK, KID_GRADH, who, c);
-      return false;
-    }
-    const double4 h = t.hA[c];
-    const int4 lk = t.link[c];
-    const double d0 = h.x - rx, d1 = h.y - ry, d2 = h.z - rz;
-    const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
-    const double tt = hrange + h.w;
-    if (drsqd <= tt * tt) {
-      if (lk.x > 0) {
-        for (int i = 0; i < lk.x; ++i) f(lk.w + i);
-        c = lk.y;
-      } else if (lk.x == 0) {
-        c = lk.z;
-      } else {
-        c = lk.y;
-      }
-    } else {
-      c = lk.y;
-    }
-    if (c > t.ctot) break;
-  }
-  return true;
-}
-
 // BHtree/BHhydro_walk.F90:9-80 (gather or scatter test)
 template <class F>
 __device__ __forceinline__ bool walk_gather_scatter(const HydroTree& t, double rx, double ry,
@@ -150,42 +114,10 @@ __device__ __forceinline__ bool gh_after_pass(GhState& s, double mp, double h_fa
   return false;
 }
 
-// one density term of an iteration pass (:218-230)
-__device__ __forceinline__ void gh_density_term(const double4& Q, double rx, double ry, double rz,
-                                                double hs, double ih, double hf,
-                                                const double4* __restrict__ tabA, double& rt) {
-  const double d0 = Q.x - rx, d1 = Q.y - ry, d2 = Q.z - rz;
-  const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
-  if (drsqd >= hs) return;
-  const double drmag = sqrt(drsqd) + SMALL_NUMBER;
-  const int kern = (int)((HALFKERNTOT * drmag) * ih);
-  if (kern >= KERNTOT) return;
-  rt = rt + (Q.w * hf) * tabA[kern].x;
-}
-
 // the final-pass sums (:360-425)
 struct GhFinal {
   double rt, om, dv, zt;
 };
-
-__device__ __forceinline__ void gh_final_term(const double4& Q, const double4& V, double rx,
-                                              double ry, double rz, const double4& vp, double hs,
-                                              double ih, double hf,
-                                              const double4* __restrict__ tabA, GhFinal& f) {
-  const double d0 = Q.x - rx, d1 = Q.y - ry, d2 = Q.z - rz;
-  double drmag = (d0 * d0 + d1 * d1) + d2 * d2;
-  if (drmag > hs) return;
-  drmag = sqrt(drmag) + SMALL_NUMBER;
-  const int kern = (int)((HALFKERNTOT * drmag) * ih);
-  if (kern > KERNTOT) return;
-  const double dv0 = V.x - vp.x, dv1 = V.y - vp.y, dv2 = V.z - vp.z;
-  const double dvdr = (dv0 * d0 + dv1 * d1) + dv2 * d2;
-  const double4 w = tabA[kern];
-  f.rt = f.rt + (Q.w * hf) * w.x;
-  f.om = f.om + ((Q.w * hf) * ih) * w.y;
-  f.dv = f.dv - ((((Q.w * dvdr) * w.z) * hf) * ih) / drmag;
-  f.zt = f.zt + ((Q.w * ih) * ih) * w.w;
-}
 
 __device__ __forceinline__ void gh_store(int p, double mp, double hp, const GhFinal& f,
                                          double2* __restrict__ hz, double* __restrict__ rho,
@@ -207,60 +139,6 @@ __device__ __forceinline__ void gh_final_init(GhFinal& f, double mp, double ih, 
   f.om = ((mp * hf) * ih) * t0.y;
   f.dv = 0.0;
   f.zt = ((mp * ih) * ih) * t0.w;
-}
-
-// The whole routine for one particle with its own walks: used when a warp's
-// shared candidate list overflows.
-__device__ void gradh_one(int p, const double4* __restrict__ pm, double2* __restrict__ hz,
-                          const double4* __restrict__ vel, double* __restrict__ rho,
-                          double* __restrict__ omega, double* __restrict__ divv,
-                          double* __restrict__ drhodt, const HydroTree& t,
-                          const double4* __restrict__ tabA, double h_fac, int pp_gather,
-                          double rextent, DevError* err) {
-  const double4 P = pm[p];
-  const double rx = P.x, ry = P.y, rz = P.z, mp = P.w;
-  const double4 vp = vel[p];
-  const double4 t0 = tabA[0];
-  GhState s;
-  gh_init(s, hz[p].x, rextent);
-  while (true) {
-    while (true) {                                                     // :154-191
-      if (s.hp > s.h_high) {
-        s.h_high = s.hp * HMULT;
-        int cnt = 0;
-        if (!walk_gather(t, rx, ry, rz, KERNRANGE * s.h_high, err, p, [&](int) { ++cnt; })) return;
-        s.pp_pot = cnt;
-      }
-      if (s.pp_pot < pp_gather) {
-        s.h_high = 0.0;
-        s.pp_pot = 0;
-        s.hp = s.hp * HMULT;
-        if (++s.ngrow > HGROW_CAP) {
-          set_error(err, SEREN_GPU_ERR_WALK, KID_GRADH, p, -1);
-          return;
-        }
-      }
-      if (s.pp_pot > 0) break;
-    }
-    const double ih = 1.0 / s.hp;                                      // :199-210
-    const double hf = pow(ih, NDIMPR);
-    const double hs = (KERNRANGESQD * s.hp) * s.hp;
-    double rt = (mp * t0.x) * hf;
-    walk_gather(t, rx, ry, rz, KERNRANGE * s.h_high, err, p, [&](int q) {
-      if (q != p) gh_density_term(pm[q], rx, ry, rz, hs, ih, hf, tabA, rt);
-    });
-    if (gh_after_pass(s, mp, h_fac, rextent, rt)) break;
-  }
-  const double hp = h_fac * pow(mp / s.rho, ONETHIRD);                 // :317
-  const double ih = 1.0 / hp;
-  const double hf = pow(ih, NDIMPR);
-  const double hs = (KERNRANGESQD * hp) * hp;
-  GhFinal f;
-  gh_final_init(f, mp, ih, hf, t0);
-  walk_gather(t, rx, ry, rz, KERNRANGE * s.h_high, err, p, [&](int q) {
-    if (q != p) gh_final_term(pm[q], vel[q], rx, ry, rz, vp, hs, ih, hf, tabA, f);
-  });
-  gh_store(p, mp, hp, f, hz, rho, omega, divv, drhodt, err);
 }
 
 // ---------------------------------------------------------------------------
@@ -439,209 +317,6 @@ __device__ __forceinline__ int gr_next(int* work, int lane) {
   return __shfl_sync(FULL, g, 0);
 }
 
-// ---------------------------------------------------------------------------
-// Warp-per-particle search for the few particles the group path hands back.
-constexpr int WP_THREADS = 128;
-constexpr int WP_WARPS = WP_THREADS / 32;
-constexpr int WP_FCAP = 512;     // cells of one level of the walk
-constexpr int WP_LCAP = 256;     // opened leaves (a power of two: the sort pads to it)
-constexpr int WP_CCAP = 1024;    // candidate particles
-
-struct WpShared {
-  int front[2][WP_FCAP];
-  int leaves[WP_LCAP];
-  int cand[WP_CCAP];
-};
-
-// Breadth-first walk of one particle's search; returns the number of opened
-// leaves (codes pstart*8 + count-1 in s.leaves) or -1 when a buffer overflows;
-// cnt = the particles in the opened leaves.
-template <class Test>
-__device__ int wp_walk(const HydroTree& t, int lane, WpShared& s, int& cnt,
-                       unsigned long long& nvisit, Test&& test) {
-  int* fa = s.front[0];
-  int* fb = s.front[1];
-  __syncwarp();
-  if (lane == 0) fa[0] = 0;
-  __syncwarp();
-  int nf = 1, nleaf = 0, mine = 0;
-  bool over = false;
-  while (nf > 0) {
-    int nnext = 0;
-    for (int base = 0; base < nf; base += 32) {
-      const int idx = base + lane;
-      const bool valid = idx < nf;
-      const int c = valid ? fa[idx] : 0;
-      const bool pass = valid && test(c);
-      const int4 lk = t.link[c];
-      const bool isleaf = pass && lk.x > 0;
-      const bool isbr = pass && lk.x == 0;
-      const unsigned ml = __ballot_sync(FULL, isleaf);
-      if (isleaf) {
-        const int pos = nleaf + __popc(ml & ((1u << lane) - 1u));
-        if (pos < WP_LCAP) s.leaves[pos] = lk.w * 8 + (lk.x - 1);
-        mine += lk.x;
-      }
-      nleaf += __popc(ml);
-      const int nk = isbr ? t.nkids[c] : 0;
-      const int sc = warp_iscan(nk, lane);
-      if (isbr) {
-        const int o = nnext + sc - nk;
-        for (int j = 0; j < nk; ++j)
-          if (o + j < WP_FCAP) fb[o + j] = lk.z + j;
-      }
-      nnext += __shfl_sync(FULL, sc, 31);
-    }
-    nvisit += nf;
-    __syncwarp();
-    if (nnext > WP_FCAP) over = true;
-    int* tmp = fa;
-    fa = fb;
-    fb = tmp;
-    nf = over ? 0 : nnext;
-  }
-  cnt = warp_iscan(mine, lane);
-  cnt = __shfl_sync(FULL, cnt, 31);
-  return (over || nleaf > WP_LCAP) ? -1 : nleaf;
-}
-
-// leaves -> candidate particle ids, in leaf order; returns the count (may
-// exceed WP_CCAP: overflow)
-__device__ int wp_flatten(int nleaf, int lane, WpShared& s) {
-  int total = 0;
-  for (int base = 0; base < nleaf; base += 32) {
-    const int k = base + lane;
-    const int code = k < nleaf ? s.leaves[k] : 0;
-    const int n = k < nleaf ? (code & 7) + 1 : 0;
-    const int sc = warp_iscan(n, lane);
-    const int o = total + sc - n;
-    for (int j = 0; j < n; ++j)
-      if (o + j < WP_CCAP) s.cand[o + j] = (code >> 3) + j;
-    total += __shfl_sync(FULL, sc, 31);
-  }
-  __syncwarp();
-  return total;
-}
-
-// sph/all_sph_gradh.F90:11-492 with one warp per particle and walks of its
-// own, for the particles k_gradh_pass hands back (redo[0..*nredo)): each walk
-// runs breadth-first with the lanes spread over the cells of a level, and the
-// candidates are processed 32 at a time with the partial sums reduced at the
-// end; when its own buffers overflow, one lane runs gradh_one.
-__global__ void __launch_bounds__(WP_THREADS) k_gradh_redo(
-    const int* __restrict__ act, const int* __restrict__ nredo,
-    const double4* __restrict__ pm, double2* __restrict__ hz,
-    const double4* __restrict__ vel, double* __restrict__ rho, double* __restrict__ omega,
-    double* __restrict__ divv, double* __restrict__ drhodt, HydroTree t,
-    const double4* __restrict__ tabA, double h_fac, int pp_gather, double rextent, DevError* err,
-    unsigned long long* counts) {
-  __shared__ WpShared sh[WP_WARPS];
-  const int lane = threadIdx.x & 31;
-  WpShared& S = sh[threadIdx.x >> 5];
-  const double4 t0 = tabA[0];
-  unsigned long long nwalk = 0, nvisit = 0, npass = 0, ncands = 0;
-  const int nact = *nredo;
-  for (int i = blockIdx.x * WP_WARPS + (threadIdx.x >> 5); i < nact; i += gridDim.x * WP_WARPS) {
-    {
-      const int p = act[i];
-      const double4 P = pm[p];
-      const double rx = P.x, ry = P.y, rz = P.z, mp = P.w;
-      const float px = (float)(rx - t.rootx), py = (float)(ry - t.rooty),
-                  pz = (float)(rz - t.rootz);
-      GhState s;
-      gh_init(s, hz[p].x, rextent);
-      double R = 0.0;
-      float R32 = 0.0f;
-      auto gather_test = [&](int c) {                 // BHhydrowalk_hgather.F90:36-40
-        const float4 h32 = t.hA32[c];
-        const float d0 = h32.x - px, d1 = h32.y - py, d2 = h32.z - pz;
-        const int r = test32((d0 * d0 + d1 * d1) + d2 * d2, R32 + h32.w, t.delta);
-        if (r >= 0) return r == 1;
-        const double4 h = t.hA[c];
-        const double e0 = h.x - rx, e1 = h.y - ry, e2 = h.z - rz;
-        const double tt = R + h.w;
-        return ((e0 * e0 + e1 * e1) + e2 * e2) <= tt * tt;
-      };
-      int ncand = 0;
-      bool over = false, bad = false;
-      while (true) {
-        while (true) {                                                 // :154-191
-          if (s.hp > s.h_high) {
-            s.h_high = s.hp * HMULT;
-            R = KERNRANGE * s.h_high;
-            R32 = (float)R;
-            int cnt = 0;
-            ++nwalk;
-            const int nl = wp_walk(t, lane, S, cnt, nvisit, gather_test);
-            if (nl < 0) { over = true; break; }
-            ncand = wp_flatten(nl, lane, S);
-            if (ncand > WP_CCAP) { over = true; break; }
-            s.pp_pot = cnt;
-          }
-          if (s.pp_pot < pp_gather) {
-            s.h_high = 0.0;
-            s.pp_pot = 0;
-            s.hp = s.hp * HMULT;
-            if (++s.ngrow > HGROW_CAP) { bad = true; break; }
-          }
-          if (s.pp_pot > 0) break;
-        }
-        if (over || bad) break;
-        const double ih = 1.0 / s.hp;                                  // :199-235
-        const double hf = pow(ih, NDIMPR);
-        const double hs = (KERNRANGESQD * s.hp) * s.hp;
-        double part = 0.0;
-        for (int k = lane; k < ncand; k += 32) {
-          const int q = S.cand[k];
-          if (q != p) gh_density_term(pm[q], rx, ry, rz, hs, ih, hf, tabA, part);
-        }
-        const double rt = (mp * t0.x) * hf + warp_sum(part);
-        ++npass;
-        ncands += ncand;
-        if (gh_after_pass(s, mp, h_fac, rextent, rt)) break;
-      }
-      if (bad) {
-        if (lane == 0) set_error(err, SEREN_GPU_ERR_WALK, KID_GRADH, p, -1);
-        continue;
-      }
-      if (over) {
-        if (lane == 0)
-          gradh_one(p, pm, hz, vel, rho, omega, divv, drhodt, t, tabA, h_fac, pp_gather, rextent,
-                    err);
-        __syncwarp();
-        continue;
-      }
-      const double hp = h_fac * pow(mp / s.rho, ONETHIRD);            // :317-425
-      const double ih = 1.0 / hp;
-      const double hf = pow(ih, NDIMPR);
-      const double hs = (KERNRANGESQD * hp) * hp;
-      const double4 vp = vel[p];
-      GhFinal f;
-      f.rt = 0.0; f.om = 0.0; f.dv = 0.0; f.zt = 0.0;
-      for (int k = lane; k < ncand; k += 32) {
-        const int q = S.cand[k];
-        if (q != p) gh_final_term(pm[q], vel[q], rx, ry, rz, vp, hs, ih, hf, tabA, f);
-      }
-      GhFinal g;
-      gh_final_init(g, mp, ih, hf, t0);
-      g.rt = g.rt + warp_sum(f.rt);
-      g.om = g.om + warp_sum(f.om);
-      g.dv = g.dv + warp_sum(f.dv);
-      g.zt = g.zt + warp_sum(f.zt);
-      ++npass;
-      ncands += ncand;
-      if (lane == 0) gh_store(p, mp, hp, g, hz, rho, omega, divv, drhodt, err);
-    }
-  }
-  if (lane == 0) {
-    atomicAdd(counts + 3, nwalk);
-    atomicAdd(counts + 4, nvisit);
-    atomicAdd(counts + 5, npass);
-    atomicAdd(counts + 6, ncands);
-  }
-}
-
-
 // sph/all_sph_gradh.F90:11-492 in two kernels.
 //
 // k_gradh_walk: the first neighbour walk of every active particle
@@ -653,13 +328,14 @@ __global__ void __launch_bounds__(WP_THREADS) k_gradh_redo(
 // k_gradh_pass: 32 particles per warp, each lane holding its particle's state;
 // the reference's iteration (:154-285) and final pass (:317-425) run with the
 // candidates of one particle at a time (its row flattened) shared out over the
-// lanes and the sums reduced across the warp.  The
-// reference leaves this path only to grow h (pp_pot < pp_gather) or to walk
-// again (h > h_high); a particle that needs either, or whose row overflowed,
-// is redone from the start by gradh_one, which follows the reference's loop
-// with walks of its own and so takes the same steps (k_gradh_redo, one warp
-// per such particle).
-constexpr int GH_LEAVES = 128;   // opened leaves kept per particle
+// lanes and the sums reduced across the warp.  The reference leaves this path
+// only to grow h (pp_pot < pp_gather) or to walk again (h > h_high); a
+// particle that needs either, or whose row overflowed, is redone from the
+// start with walks of its own, which take the reference's steps in the same
+// order: k_gradh_redo (one warp per particle, walk buffers in global scratch)
+// and, for walks too large for those buffers, k_gradh_wide (one block per
+// particle, walks split over subtrees).
+constexpr int GH_LEAVES = 256;   // opened leaves kept per particle
 
 __global__ void __launch_bounds__(GR_THREADS) k_gradh_walk(
     int nact, const int* __restrict__ act, const double4* __restrict__ pm,
@@ -721,10 +397,13 @@ __global__ void __launch_bounds__(GR_THREADS) k_gradh_walk(
 constexpr int GP_THREADS = 128;
 constexpr int GP_WARPS = GP_THREADS / 32;
 constexpr int GP_INB = 128;      // packed in-range candidates per warp
+constexpr int GP_SEG = 64;       // leaves of a row flattened at a time
 
 // The density term (:218-230) and the final-pass terms (:360-425) of one
-// candidate inside 2h, from its r^2, mass and dv.dr (the same operations as
-// gh_density_term and gh_final_term).
+// candidate inside 2h, from its r^2, mass and dv.dr, with the reference's
+// operations in its order; the kernel bin is int(5000 r/h) with
+// r = sqrt(r^2) + 1e-20, its value evaluated in place (kernel_fns.h, equal to
+// the table entry).
 __device__ __forceinline__ void gh_density_in(double d2, double m, double ih, double hf,
                                               double& rt) {
   const double drmag = sqrt(d2) + SMALL_NUMBER;
@@ -777,7 +456,7 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
     double h_fac, int pp_gather, double rextent, const int* __restrict__ leaves,
     const int* __restrict__ nleaf, const int* __restrict__ npot, int* __restrict__ redo,
     int* __restrict__ nredo, DevError* err, unsigned long long* counts) {
-  __shared__ int cand_all[GP_WARPS][GH_LEAVES * LEAFMAX];
+  __shared__ int cand_all[GP_WARPS][GP_SEG * LEAFMAX];
   __shared__ double inb_all[GP_WARPS][3][GP_INB];   // candidates inside 2h: r^2, m, dv.dr
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   int* cand = cand_all[w];
@@ -814,11 +493,13 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
         const double hsj = __shfl_sync(FULL, hs, j), ihj = __shfl_sync(FULL, ih, j),
                      hfj = __shfl_sync(FULL, hf, j);
         const int pj = __shfl_sync(FULL, p, j);
-        const int nc = gp_flatten(leaves + (size_t)pj * GH_LEAVES, __shfl_sync(FULL, n, j), cand,
-                                  lane);
+        const int nj = __shfl_sync(FULL, n, j);
         // r^2 of every candidate; those inside 2h (:218) are packed into the
         // buffer, whose terms are then evaluated 32 at a time
         double part = 0.0;
+        for (int s0 = 0; s0 < nj; s0 += GP_SEG) {     // the row, GP_SEG leaves at a time
+        const int nc = gp_flatten(leaves + (size_t)pj * GH_LEAVES + s0, min(GP_SEG, nj - s0),
+                                  cand, lane);
         int nin = 0;
         for (int b = 0; b < nc; b += 64) {           // two chunks of candidates in flight
           const int k0 = b + lane, k1 = b + 32 + lane;
@@ -849,6 +530,7 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
           }
         }
         niter += (nc + 31) >> 5;
+        }
         const double sum = warp_sum(part);
         if (lane == j) rt = sum;
       }
@@ -881,10 +563,12 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
       const double4 vj = make_double4(__shfl_sync(FULL, vp.x, j), __shfl_sync(FULL, vp.y, j),
                                       __shfl_sync(FULL, vp.z, j), 0.0);
       const int pj = __shfl_sync(FULL, p, j);
-      const int nc = gp_flatten(leaves + (size_t)pj * GH_LEAVES, __shfl_sync(FULL, n, j), cand,
-                                lane);
+      const int nj = __shfl_sync(FULL, n, j);
       GhFinal part;
       part.rt = 0.0; part.om = 0.0; part.dv = 0.0; part.zt = 0.0;
+      for (int s0 = 0; s0 < nj; s0 += GP_SEG) {       // the row, GP_SEG leaves at a time
+      const int nc = gp_flatten(leaves + (size_t)pj * GH_LEAVES + s0, min(GP_SEG, nj - s0),
+                                cand, lane);
       int nin = 0;
       for (int b = 0; b < nc; b += 32) {
         const int k = b + lane;
@@ -912,6 +596,7 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
         }
       }
       niter += (nc + 31) >> 5;
+      }
       const double srt = warp_sum(part.rt), som = warp_sum(part.om), sdv = warp_sum(part.dv),
                    szt = warp_sum(part.zt);
       if (lane == j) {
@@ -935,6 +620,336 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
   atomicAdd(counts + 6, ncands);
   atomicAdd(counts + 15, nsingle);
   if (lane == 0) atomicAdd(counts + 13, niter);
+}
+
+// ---------------------------------------------------------------------------
+// grad-h for the particles k_gradh_pass hands back (redo[0..*nredo)): one warp
+// per particle runs the reference's loop (:132-425) with walks of its own.  A
+// walk runs breadth-first with the lanes spread over the cells of a level; its
+// two frontiers and the opened leaves live in global scratch (three walk-stack
+// slots per warp, idle while this kernel runs), and the passes flatten the
+// leaves GP_SEG at a time and share the candidates out over the lanes.
+constexpr int RD_THREADS = 128;
+constexpr int RD_WARPS = RD_THREADS / 32;
+
+// Breadth-first walk of one particle's search (BHhydrowalk_hgather); returns
+// the number of opened leaves (codes pstart*8 + count-1 in leaves, in no
+// particular order) or -1 when a buffer of cap entries would overflow; cnt =
+// the particles in the opened leaves (pp_pot).
+template <class Test>
+__device__ int rd_walk(const HydroTree& t, int lane, int* fa, int* fb, int* leaves, int cap,
+                       int& cnt, unsigned long long& nvisit, Test&& test) {
+  __syncwarp();
+  if (lane == 0) fa[0] = 0;
+  __syncwarp();
+  int nf = 1, nleaf = 0, mine = 0;
+  while (nf > 0) {
+    int nnext = 0;
+    for (int base = 0; base < nf; base += 32) {
+      const int idx = base + lane;
+      const bool valid = idx < nf;
+      const int c = valid ? fa[idx] : 0;
+      const bool pass = valid && test(c);
+      const int4 lk = t.link[c];
+      const bool isleaf = pass && lk.x > 0;
+      const bool isbr = pass && lk.x == 0;
+      const unsigned ml = __ballot_sync(FULL, isleaf);
+      if (isleaf) {
+        const int pos = nleaf + __popc(ml & ((1u << lane) - 1u));
+        if (pos < cap) leaves[pos] = lk.w * 8 + (lk.x - 1);
+        mine += lk.x;
+      }
+      nleaf += __popc(ml);
+      const int nk = isbr ? t.nkids[c] : 0;
+      const int sc = warp_iscan(nk, lane);
+      if (isbr) {
+        const int o = nnext + sc - nk;
+        for (int j = 0; j < nk; ++j)
+          if (o + j < cap) fb[o + j] = lk.z + j;
+      }
+      nnext += __shfl_sync(FULL, sc, 31);
+    }
+    nvisit += nf;
+    __syncwarp();
+    if (nnext > cap || nleaf > cap) return -1;
+    int* tmp = fa;
+    fa = fb;
+    fb = tmp;
+    nf = nnext;
+  }
+  cnt = __shfl_sync(FULL, warp_iscan(mine, lane), 31);
+  return nleaf;
+}
+
+__global__ void __launch_bounds__(RD_THREADS) k_gradh_redo(
+    const int* __restrict__ redo, const int* __restrict__ nredo, const double4* __restrict__ pm,
+    double2* __restrict__ hz, const double4* __restrict__ vel, double* __restrict__ rho,
+    double* __restrict__ omega, double* __restrict__ divv, double* __restrict__ drhodt,
+    HydroTree t, const double4* __restrict__ tabA, double h_fac, int pp_gather, double rextent,
+    int* __restrict__ scratch, int cap, int* __restrict__ wide, int* __restrict__ nwide,
+    DevError* err, unsigned long long* counts) {
+  __shared__ int cand_all[RD_WARPS][GP_SEG * LEAFMAX];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int* cand = cand_all[w];
+  const int gw = blockIdx.x * RD_WARPS + w;
+  int* fa = scratch + (size_t)gw * 3 * cap;
+  int* fb = fa + cap;
+  int* lv = fb + cap;
+  const double4 t0 = tabA[0];
+  unsigned long long nwalk = 0, nvisit = 0, npass = 0, ncands = 0;
+  const int nr = *nredo;
+  for (int i = gw; i < nr; i += gridDim.x * RD_WARPS) {
+    const int p = redo[i];
+    const double4 P = pm[p];
+    const double rx = P.x, ry = P.y, rz = P.z, mp = P.w;
+    const float px = (float)(rx - t.rootx), py = (float)(ry - t.rooty), pz = (float)(rz - t.rootz);
+    GhState s;
+    gh_init(s, hz[p].x, rextent);
+    double Rw = 0.0;
+    float R32 = 0.0f;
+    auto gather_test = [&](int c) {                    // BHhydrowalk_hgather.F90:36-40
+      const float4 h32 = t.hA32[c];
+      const float d0 = h32.x - px, d1 = h32.y - py, d2 = h32.z - pz;
+      const int r = test32((d0 * d0 + d1 * d1) + d2 * d2, R32 + h32.w, t.delta);
+      if (r >= 0) return r == 1;
+      const double4 h = t.hA[c];
+      const double e0 = h.x - rx, e1 = h.y - ry, e2 = h.z - rz;
+      const double tt = Rw + h.w;
+      return ((e0 * e0 + e1 * e1) + e2 * e2) <= tt * tt;
+    };
+    int nl = 0;
+    bool over = false, bad = false;
+    while (true) {
+      while (true) {                                                   // :154-191
+        if (s.hp > s.h_high) {
+          s.h_high = s.hp * HMULT;
+          Rw = KERNRANGE * s.h_high;
+          R32 = (float)Rw;
+          int cnt = 0;
+          ++nwalk;
+          nl = rd_walk(t, lane, fa, fb, lv, cap, cnt, nvisit, gather_test);
+          if (nl < 0) { over = true; break; }
+          s.pp_pot = cnt;
+        }
+        if (s.pp_pot < pp_gather) {
+          s.h_high = 0.0;
+          s.pp_pot = 0;
+          s.hp = s.hp * HMULT;
+          if (++s.ngrow > HGROW_CAP) { bad = true; break; }
+        }
+        if (s.pp_pot > 0) break;
+      }
+      if (over || bad) break;
+      const double ih = 1.0 / s.hp;                                    // :199-235
+      const double hf = pow(ih, NDIMPR);
+      const double hs = (KERNRANGESQD * s.hp) * s.hp;
+      double part = 0.0;
+      for (int s0 = 0; s0 < nl; s0 += GP_SEG) {
+        const int nc = gp_flatten(lv + s0, min(GP_SEG, nl - s0), cand, lane);
+        for (int k = lane; k < nc; k += 32) {
+          const int q = cand[k];
+          const double4 Q = pm[q];
+          const double d0 = Q.x - rx, d1 = Q.y - ry, d2 = Q.z - rz;
+          const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
+          if (q != p && drsqd < hs) gh_density_in(drsqd, Q.w, ih, hf, part);
+        }
+      }
+      ++npass;
+      ncands += s.pp_pot;
+      if (gh_after_pass(s, mp, h_fac, rextent, (mp * t0.x) * hf + warp_sum(part))) break;
+    }
+    if (bad) {
+      if (lane == 0) set_error(err, SEREN_GPU_ERR_WALK, KID_GRADH, p, -1);
+      continue;
+    }
+    if (over) {                                        // more than cap leaves or cells a level
+      if (lane == 0) wide[atomicAdd(nwide, 1)] = p;    // k_gradh_wide starts it again
+      continue;
+    }
+    const double hp = h_fac * pow(mp / s.rho, ONETHIRD);              // :317-425
+    const double ih = 1.0 / hp;
+    const double hf = pow(ih, NDIMPR);
+    const double hs = (KERNRANGESQD * hp) * hp;
+    const double4 vp = vel[p];
+    GhFinal f;
+    f.rt = 0.0; f.om = 0.0; f.dv = 0.0; f.zt = 0.0;
+    for (int s0 = 0; s0 < nl; s0 += GP_SEG) {
+      const int nc = gp_flatten(lv + s0, min(GP_SEG, nl - s0), cand, lane);
+      for (int k = lane; k < nc; k += 32) {
+        const int q = cand[k];
+        const double4 Q = pm[q];
+        const double d0 = Q.x - rx, d1 = Q.y - ry, d2 = Q.z - rz;
+        const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
+        if (q == p || drsqd > hs) continue;
+        const double4 V = vel[q];
+        const double dv0 = V.x - vp.x, dv1 = V.y - vp.y, dv2 = V.z - vp.z;
+        gh_final_in(drsqd, Q.w, (dv0 * d0 + dv1 * d1) + dv2 * d2, ih, hf, f);
+      }
+    }
+    ++npass;
+    ncands += s.pp_pot;
+    GhFinal g;
+    gh_final_init(g, mp, ih, hf, t0);
+    g.rt = g.rt + warp_sum(f.rt);
+    g.om = g.om + warp_sum(f.om);
+    g.dv = g.dv + warp_sum(f.dv);
+    g.zt = g.zt + warp_sum(f.zt);
+    if (lane == 0) gh_store(p, mp, hp, g, hz, rho, omega, divv, drhodt, err);
+  }
+  if (lane == 0) {
+    atomicAdd(counts + 3, nwalk);
+    atomicAdd(counts + 4, nvisit);
+    atomicAdd(counts + 5, npass);
+    atomicAdd(counts + 6, ncands);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// grad-h for the particles whose walks outgrow the redo kernel's scratch (the
+// reference's bisection, :262-275, starts from h_upper = rextent, so its first
+// walks can cover the whole domain).  One block per particle runs the
+// reference's loop; every walk runs in parallel over a cover of the tree (the
+// cells of one level and the leaves above it): a thread takes a cover cell,
+// checks that each of its ancestors passes the particle's test (the reference
+// reaches a cell only through opened cells), then walks its subtree with the
+// reference's stackless loop.  Nothing is stored; each pass walks again with
+// the same radius, so it sees the same candidates.
+constexpr int GWD_THREADS = 256;
+
+template <class F>
+__device__ void wide_walk(const HydroTree& t, const int* __restrict__ parent,
+                          const int* __restrict__ level, int L, int c1, double rx, double ry,
+                          double rz, double hrange, DevError* err, int who, F&& f) {
+  auto pass = [&](int c) {                             // BHhydrowalk_hgather.F90:36-40
+    const double4 h = t.hA[c];
+    const double d0 = h.x - rx, d1 = h.y - ry, d2 = h.z - rz;
+    const double tt = hrange + h.w;
+    return ((d0 * d0 + d1 * d1) + d2 * d2) <= tt * tt;
+  };
+  for (int c = threadIdx.x; c <= c1; c += blockDim.x) {
+    const int lv = level[c];
+    const int4 lk = t.link[c];
+    if (!(lv == L || (lv < L && lk.x > 0))) continue;
+    bool reach = true;
+    for (int a = parent[c]; a >= 0 && reach; a = parent[a]) reach = pass(a);
+    if (!reach) continue;
+    const int stop = lk.y;
+    int cur = c, visits = 0;
+    while (true) {
+      if (++visits > t.ctot + 2) {
+        set_error(err, SEREN_GPU_ERR_WALK, KID_GRADH, who, cur);
+        break;
+      }
+      const int4 l2 = t.link[cur];
+      const bool ok = pass(cur);
+      if (ok && l2.x > 0) {
+        for (int k = 0; k < l2.x; ++k) f(l2.w + k);
+        cur = l2.y;
+      } else if (ok && l2.x == 0) {
+        cur = l2.z;
+      } else {
+        cur = l2.y;
+      }
+      if (cur == stop || cur > t.ctot) break;
+    }
+  }
+}
+
+// sum over the block, the same value on every thread
+__device__ double block_sum(double v, double* sh) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  v = warp_sum(v);
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  double r = 0.0;
+  for (int k = 0; k < (int)(blockDim.x >> 5); ++k) r += sh[k];
+  __syncthreads();
+  return r;
+}
+
+__global__ void __launch_bounds__(GWD_THREADS) k_gradh_wide(
+    const int* __restrict__ wide, const int* __restrict__ nwide, const double4* __restrict__ pm,
+    double2* __restrict__ hz, const double4* __restrict__ vel, double* __restrict__ rho,
+    double* __restrict__ omega, double* __restrict__ divv, double* __restrict__ drhodt,
+    HydroTree t, const int* __restrict__ parent, const int* __restrict__ level, int L, int c1,
+    const double4* __restrict__ tabA, double h_fac, int pp_gather, double rextent, DevError* err,
+    unsigned long long* counts) {
+  __shared__ double red[GWD_THREADS / 32];
+  const double4 t0 = tabA[0];
+  unsigned long long nwalk = 0, npass = 0;
+  const int nw = *nwide;
+  for (int i = blockIdx.x; i < nw; i += gridDim.x) {
+    const int p = wide[i];
+    const double4 P = pm[p];
+    const double rx = P.x, ry = P.y, rz = P.z, mp = P.w;
+    GhState s;
+    gh_init(s, hz[p].x, rextent);
+    bool bad = false;
+    while (true) {
+      while (true) {                                                   // :154-191
+        if (s.hp > s.h_high) {
+          s.h_high = s.hp * HMULT;
+          double cnt = 0.0;
+          wide_walk(t, parent, level, L, c1, rx, ry, rz, KERNRANGE * s.h_high, err, p,
+                    [&](int) { cnt += 1.0; });
+          s.pp_pot = (int)block_sum(cnt, red);
+          ++nwalk;
+        }
+        if (s.pp_pot < pp_gather) {
+          s.h_high = 0.0;
+          s.pp_pot = 0;
+          s.hp = s.hp * HMULT;
+          if (++s.ngrow > HGROW_CAP) { bad = true; break; }
+        }
+        if (s.pp_pot > 0) break;
+      }
+      if (bad) break;
+      const double ih = 1.0 / s.hp;                                    // :199-235
+      const double hf = pow(ih, NDIMPR);
+      const double hs = (KERNRANGESQD * s.hp) * s.hp;
+      double part = 0.0;
+      wide_walk(t, parent, level, L, c1, rx, ry, rz, KERNRANGE * s.h_high, err, p, [&](int q) {
+        const double4 Q = pm[q];
+        const double d0 = Q.x - rx, d1 = Q.y - ry, d2 = Q.z - rz;
+        const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
+        if (q != p && drsqd < hs) gh_density_in(drsqd, Q.w, ih, hf, part);
+      });
+      ++npass;
+      if (gh_after_pass(s, mp, h_fac, rextent, (mp * t0.x) * hf + block_sum(part, red))) break;
+    }
+    if (bad) {
+      if (threadIdx.x == 0) set_error(err, SEREN_GPU_ERR_WALK, KID_GRADH, p, -1);
+      continue;
+    }
+    const double hp = h_fac * pow(mp / s.rho, ONETHIRD);              // :317-425
+    const double ih = 1.0 / hp;
+    const double hf = pow(ih, NDIMPR);
+    const double hs = (KERNRANGESQD * hp) * hp;
+    const double4 vp = vel[p];
+    GhFinal f;
+    f.rt = 0.0; f.om = 0.0; f.dv = 0.0; f.zt = 0.0;
+    wide_walk(t, parent, level, L, c1, rx, ry, rz, KERNRANGE * s.h_high, err, p, [&](int q) {
+      const double4 Q = pm[q];
+      const double d0 = Q.x - rx, d1 = Q.y - ry, d2 = Q.z - rz;
+      const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
+      if (q == p || drsqd > hs) return;
+      const double4 V = vel[q];
+      const double dv0 = V.x - vp.x, dv1 = V.y - vp.y, dv2 = V.z - vp.z;
+      gh_final_in(drsqd, Q.w, (dv0 * d0 + dv1 * d1) + dv2 * d2, ih, hf, f);
+    });
+    ++npass;
+    GhFinal g;
+    gh_final_init(g, mp, ih, hf, t0);
+    g.rt = g.rt + block_sum(f.rt, red);
+    g.om = g.om + block_sum(f.om, red);
+    g.dv = g.dv + block_sum(f.dv, red);
+    g.zt = g.zt + block_sum(f.zt, red);
+    if (threadIdx.x == 0) gh_store(p, mp, hp, g, hz, rho, omega, divv, drhodt, err);
+  }
+  if (threadIdx.x == 0) {
+    atomicAdd(counts + 3, nwalk);
+    atomicAdd(counts + 5, npass);
+  }
 }
 
 // get_neib (sph/get_neib.F90:10-140) in two kernels.
@@ -1010,7 +1025,7 @@ __global__ void __launch_bounds__(GP_THREADS) k_neib_rows(
     const double2* __restrict__ hz, HydroTree t, int L, const int* __restrict__ leaves,
     const int* __restrict__ nleaf, int* __restrict__ pptot, int* __restrict__ pplist,
     DevError* err, unsigned long long* counts) {
-  __shared__ int cand_all[GP_WARPS][GH_LEAVES * LEAFMAX];
+  __shared__ int cand_all[GP_WARPS][GP_SEG * LEAFMAX];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   int* cand = cand_all[w];
   const unsigned lt = (1u << lane) - 1u;
@@ -1029,10 +1044,12 @@ __global__ void __launch_bounds__(GP_THREADS) k_neib_rows(
       const double xj = __shfl_sync(FULL, P.x, j), yj = __shfl_sync(FULL, P.y, j),
                    zj = __shfl_sync(FULL, P.z, j), hsj = __shfl_sync(FULL, hsp, j);
       const int pj = __shfl_sync(FULL, p, j);
-      const int nc = gp_flatten(leaves + (size_t)pj * GH_LEAVES, __shfl_sync(FULL, n, j), cand,
-                                lane);
+      const int nj = __shfl_sync(FULL, n, j);
       int* row = pplist + (size_t)pj * L;
       int kept = 0;
+      for (int s0 = 0; s0 < nj; s0 += GP_SEG) {       // the row, GP_SEG leaves at a time
+      const int nc = gp_flatten(leaves + (size_t)pj * GH_LEAVES + s0, min(GP_SEG, nj - s0),
+                                cand, lane);
       for (int b = 0; b < nc; b += 32) {
         const int k = b + lane;
         const int q = k < nc ? cand[k] : pj;
@@ -1052,6 +1069,7 @@ __global__ void __launch_bounds__(GP_THREADS) k_neib_rows(
       }
       niter += (nc + 31) >> 5;
       ncands += nc;
+      }
       if (lane == 0) pptot[pj] = kept;
     }
     if (live && n < 0) {
@@ -1309,15 +1327,28 @@ void launch_gradh(Ctx& c, int nact) {
     if (o < 1) o = 1;
   }
   const int blocks = std::min(sm_count(c) * o, nb(nb(nact, 32), GP_WARPS));
-  cudaMemsetAsync(c.work + 1, 0, sizeof(int), c.st);
+  cudaMemsetAsync(c.work + 1, 0, 2 * sizeof(int), c.st);
   k_gradh_pass<<<blocks, GP_THREADS, 0, c.st>>>(
       nact, c.act, c.pm, c.hz, c.vel, c.rho, c.omega, c.div_v, c.drhodt, c.tabA, c.prm.h_fac,
       c.prm.pp_gather, c.info.rextent, c.leaves, c.nleaf, c.npot, c.redo, c.work + 1, c.d_err,
       counts);
-  k_gradh_redo<<<sm_count(c) * 2, WP_THREADS, 0, c.st>>>(
+  // three walk-stack slots of scratch per redo warp
+  k_gradh_redo<<<std::max(1, (c.wstack_slots / 3) / RD_WARPS), RD_THREADS, 0, c.st>>>(
       c.redo, c.work + 1, c.pm, c.hz, c.vel, c.rho, c.omega, c.div_v, c.drhodt, t, c.tabA,
-      c.prm.h_fac, c.prm.pp_gather, c.info.rextent, c.d_err, counts);
-  c.nlaunch += 3;
+      c.prm.h_fac, c.prm.pp_gather, c.info.rextent, reinterpret_cast<int*>(c.wstack),
+      2 * c.wstack_cap, c.wide, c.work + 2, c.d_err, counts);
+  // a cover of the tree: the first level with at least 2 cells per thread, and the leaves above
+  int L = c.info.ltot;
+  for (int l = 0; l <= c.info.ltot; ++l)
+    if (c.info.last_cell[l] - c.info.first_cell[l] + 1 >= 2 * GWD_THREADS) {
+      L = l;
+      break;
+    }
+  k_gradh_wide<<<sm_count(c) * 2, GWD_THREADS, 0, c.st>>>(
+      c.wide, c.work + 2, c.pm, c.hz, c.vel, c.rho, c.omega, c.div_v, c.drhodt, t, c.parent,
+      c.level, L, c.info.last_cell[L], c.tabA, c.prm.h_fac, c.prm.pp_gather, c.info.rextent,
+      c.d_err, counts);
+  c.nlaunch += 4;
 }
 
 void launch_neib(Ctx& c, int nact) {

@@ -34,6 +34,7 @@ def library(build_if_missing: bool = True) -> C.CDLL:
         for name, args in (("upload", [vp, C.c_int32, _dp, _dp, _dp]),
                            ("force_step", [vp, C.c_int32]),
                            ("drift", [vp, C.c_double]),
+                           ("set_sinks", [vp, C.c_int32, _dp]),
                            ("download", [vp, _dp, _dp, _dp, _dp, _dp, _dp, _ip]),
                            ("last_step_stats", [vp, _dp, _ip, C.POINTER(C.c_int64)]),
                            ("get_stream", [vp, C.POINTER(C.c_void_p)]),
@@ -63,6 +64,12 @@ class GpuHotPath(HotPath):
 
     def force_step(self, first_call=False):
         self._call("force_step", self._ctx, int(first_call))
+
+    def set_sinks(self, sinks):
+        """Sinks ([nsink][5]: x, y, z, m, h) for the device-resident step."""
+        s = None if sinks is None else np.ascontiguousarray(np.atleast_2d(sinks), dtype=np.float64)
+        ns = 0 if s is None else s.shape[0]
+        self._call("set_sinks", self._ctx, ns, None if s is None else _d(s))
 
     def drift(self, dt: float):
         self._call("drift", self._ctx, C.c_double(dt))

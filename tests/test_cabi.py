@@ -38,7 +38,7 @@ def test_oracle_mirrors_the_abi():
     for n in declared():
         tail = n[len("seren_gpu_"):]
         if tail in ("upload", "force_step", "drift", "download", "last_step_stats",
-                    "get_stream", "fma_peak", "hydro_forces_noalloc"):
+                    "get_stream", "fma_peak", "hydro_forces_noalloc", "set_sinks"):
             continue          # device-resident path, device-buffer call, GPU-only introspection
         assert hasattr(lib, "seren_oracle_" + tail), tail
 

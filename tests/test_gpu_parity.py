@@ -210,3 +210,21 @@ def test_resident_step_matches_host_calls(libs):
     assert np.array_equal(st["parray"][:, 4], r["sph"]["parray"][:, 4])
     assert rel_rows(st["a"], r["a"]).max() < 1e-13
     assert np.array_equal(st["gpot"], r["gpot"])
+
+
+def test_resident_step_with_sink_matches_host_calls(libs):
+    """seren_gpu_set_sinks puts the sink-gas term of grav_forces into the
+    device-resident step."""
+    ic = case("disc12k")
+    Oracle, Gpu = libs
+    n = ic["parray"].shape[0]
+    g1 = Gpu(n, params(ic))
+    g2 = Gpu(n, params(ic))
+    r = run_pipeline(g1, ic, sinks=ic["sink"])
+    g2.upload(ic["parray"], ic["v"], ic["sound"] ** 2)
+    g2.set_sinks(ic["sink"])
+    g2.force_step(first_call=True)
+    st = g2.download()
+    assert np.array_equal(st["perm"], r["perm"])
+    assert rel_rows(st["a"], r["a"]).max() < 1e-13
+    assert np.array_equal(st["gpot"], r["gpot"])
