@@ -149,7 +149,8 @@ int seren_gpu_tree_export(seren_gpu_ctx* ctx, int32_t* ctot, int32_t* ltot,
  * stock, grad-h, hmax update + neighbour lists, thermal + hydro, gravity,
  * total), the number of kernels it launched, and the work counters of the
  * last force evaluation (16 slots): gravity [0] cell terms, [1] pair terms,
- * [2] walk entries (cell, lane mask), [8] deepest walk stack, [9] cell-list
+ * [2] walk entries (cell, lane mask), [8] grad-h particles whose walks
+ * needed a block each (k_gradh_wide), [9] cell-list
  * entries, [10] of them taken by all 32 lanes, [11] near-field list items,
  * [12] of them for all 32 lanes; grad-h [3] walks, [4] walk entries (with
  * the neighbour-list kernel), [5] passes, [6] candidates, [13] warp

@@ -104,7 +104,9 @@ struct Ctx {
   int* nleaf = nullptr;       // their number (-1: overflow)
   int* npot = nullptr;        // [pmax] particles in those leaves (pp_pot)
   int* redo = nullptr;
-  int* wide = nullptr;        // [pmax] particles whose grad-h walks cover most of the tree; count in work[2]        // [pmax] particles whose grad-h is redone alone; count in work[1]
+  int* wide = nullptr;        // [pmax] particles whose grad-h walks cover most of the tree; count in work[2]
+  void* wst = nullptr;        // state of a batch of those particles (sph.cu)
+  double* wacc = nullptr;     // their walk accumulators, 4 per particle        // [pmax] particles whose grad-h is redone alone; count in work[1]
   int2* wstack = nullptr;     // walk stacks, wstack_cap (cell, lane mask) entries per warp slot
   int wstack_cap = 0;
   int wstack_slots = 0;
@@ -141,6 +143,7 @@ void launch_neib(Ctx& c, int nact);
 void launch_hydro(Ctx& c, int nact);
 void launch_thermal(Ctx& c);
 int hydro_walk_slots(const Ctx& c);     // resident warps of the grad-h / neighbour grids
+int wide_scratch_alloc(Ctx& c);         // c.wst, c.wacc; 0 or -1
 
 // gravity.cu
 void launch_grav(Ctx& c, int nact, int nsink, const double* d_sinks);

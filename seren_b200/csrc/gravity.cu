@@ -315,7 +315,6 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
   const unsigned lt = (1u << lane) - 1u;
   unsigned long long ncell = 0, npair = 0, nent = 0;
   unsigned ce_all = 0, ce_full = 0, pi_all = 0, pi_full = 0;   // list fill statistics
-  int smax = 0;
 
   while (true) {
     int g = 0;
@@ -517,7 +516,6 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
       }
       for (int q = 0; q < nch; ++q) S[sp + cin - nch + q] = make_int2(lk.z + q, (int)mopn);
       sp += ctotal;
-      smax = max(smax, sp);
       if (nc > CAP - 32) flush_cells();
       if (np > GW_PITEMS - 32 * LEAFMAX) flush_pairs();
     }
@@ -553,10 +551,7 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
   count_add(counts, ncell, npair);
   count_add(counts + 9, ce_all, ce_full);
   count_add(counts + 11, pi_all, pi_full);
-  if (lane == 0) {
-    atomicAdd(counts + 2, nent);
-    atomicMax(counts + 8, (unsigned long long)smax);
-  }
+  if (lane == 0) atomicAdd(counts + 2, nent);
 }
 
 

@@ -804,57 +804,6 @@ __global__ void __launch_bounds__(RD_THREADS) k_gradh_redo(
   }
 }
 
-// ---------------------------------------------------------------------------
-// grad-h for the particles whose walks outgrow the redo kernel's scratch (the
-// reference's bisection, :262-275, starts from h_upper = rextent, so its first
-// walks can cover the whole domain).  One block per particle runs the
-// reference's loop; every walk runs in parallel over a cover of the tree (the
-// cells of one level and the leaves above it): a thread takes a cover cell,
-// checks that each of its ancestors passes the particle's test (the reference
-// reaches a cell only through opened cells), then walks its subtree with the
-// reference's stackless loop.  Nothing is stored; each pass walks again with
-// the same radius, so it sees the same candidates.
-constexpr int GWD_THREADS = 256;
-
-template <class F>
-__device__ void wide_walk(const HydroTree& t, const int* __restrict__ parent,
-                          const int* __restrict__ level, int L, int c1, double rx, double ry,
-                          double rz, double hrange, DevError* err, int who, F&& f) {
-  auto pass = [&](int c) {                             // BHhydrowalk_hgather.F90:36-40
-    const double4 h = t.hA[c];
-    const double d0 = h.x - rx, d1 = h.y - ry, d2 = h.z - rz;
-    const double tt = hrange + h.w;
-    return ((d0 * d0 + d1 * d1) + d2 * d2) <= tt * tt;
-  };
-  for (int c = threadIdx.x; c <= c1; c += blockDim.x) {
-    const int lv = level[c];
-    const int4 lk = t.link[c];
-    if (!(lv == L || (lv < L && lk.x > 0))) continue;
-    bool reach = true;
-    for (int a = parent[c]; a >= 0 && reach; a = parent[a]) reach = pass(a);
-    if (!reach) continue;
-    const int stop = lk.y;
-    int cur = c, visits = 0;
-    while (true) {
-      if (++visits > t.ctot + 2) {
-        set_error(err, SEREN_GPU_ERR_WALK, KID_GRADH, who, cur);
-        break;
-      }
-      const int4 l2 = t.link[cur];
-      const bool ok = pass(cur);
-      if (ok && l2.x > 0) {
-        for (int k = 0; k < l2.x; ++k) f(l2.w + k);
-        cur = l2.y;
-      } else if (ok && l2.x == 0) {
-        cur = l2.z;
-      } else {
-        cur = l2.y;
-      }
-      if (cur == stop || cur > t.ctot) break;
-    }
-  }
-}
-
 // sum over the block, the same value on every thread
 __device__ double block_sum(double v, double* sh) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -867,89 +816,211 @@ __device__ double block_sum(double v, double* sh) {
   return r;
 }
 
-__global__ void __launch_bounds__(GWD_THREADS) k_gradh_wide(
-    const int* __restrict__ wide, const int* __restrict__ nwide, const double4* __restrict__ pm,
-    double2* __restrict__ hz, const double4* __restrict__ vel, double* __restrict__ rho,
-    double* __restrict__ omega, double* __restrict__ divv, double* __restrict__ drhodt,
-    HydroTree t, const int* __restrict__ parent, const int* __restrict__ level, int L, int c1,
-    const double4* __restrict__ tabA, double h_fac, int pp_gather, double rextent, DevError* err,
-    unsigned long long* counts) {
-  __shared__ double red[GWD_THREADS / 32];
-  const double4 t0 = tabA[0];
-  unsigned long long nwalk = 0, npass = 0;
-  const int nw = *nwide;
-  for (int i = blockIdx.x; i < nw; i += gridDim.x) {
-    const int p = wide[i];
-    const double4 P = pm[p];
-    const double rx = P.x, ry = P.y, rz = P.z, mp = P.w;
-    GhState s;
-    gh_init(s, hz[p].x, rextent);
-    bool bad = false;
+// ---------------------------------------------------------------------------
+// grad-h for the particles whose walks outgrow the redo kernel's scratch (the
+// reference's bisection, :262-275, starts from h_upper = rextent, so its first
+// walks can cover most of the domain).  They are few, so every walk of every
+// such particle is spread over the whole GPU: the host runs rounds of
+//   k_wide_walk   - each (particle, slice) block walks a slice of a cover of
+//                   the tree (the cells of one level and the leaves above it):
+//                   a cover cell counts only when each ancestor passes the
+//                   particle's test (the reference reaches a cell only through
+//                   opened cells), its subtree is walked with the reference's
+//                   stackless loop, and the candidates' count or terms are
+//                   summed into the particle's accumulators;
+//   k_wide_update - each particle takes the reference's next step from them
+//                   (:154-191 walk / grow, :238-285 density update, :317-425
+//                   final pass) and says what its next walk must compute;
+// until no particle has a walk left.  Nothing is stored per candidate; every
+// walk of a pass uses the radius of the particle's last counting walk, so it
+// sees the same candidates.
+constexpr int WD_THREADS = 256;
+
+__global__ void k_flag_error(DevError* err, int code, int where) {
+  set_error(err, code, where, -1, -1);
+}
+
+constexpr int WD_SLICES = 64;    // blocks per particle and round
+constexpr int WD_BATCH = 1024;   // particles per batch of rounds
+
+enum WideJob : int { WJ_COUNT = 1, WJ_PASS = 2, WJ_FINAL = 3, WJ_DONE = 0 };
+
+struct WideState {
+  GhState s;
+  double4 P;        // position, mass
+  double4 v;        // velocity
+  double ih, hf, hs, hp;   // of the pass in progress
+  int p;
+  int job;          // WideJob
+};
+
+__global__ void k_wide_init(int n, const int* __restrict__ ids, const double4* __restrict__ pm,
+                            const double2* __restrict__ hz, const double4* __restrict__ vel,
+                            double rextent, WideState* __restrict__ ws,
+                            double* __restrict__ acc, unsigned long long* counts) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  atomicAdd(counts + 8, 1ull);
+  WideState& w = ws[i];
+  w.p = ids[i];
+  w.P = pm[w.p];
+  w.v = vel[w.p];
+  gh_init(w.s, hz[w.p].x, rextent);
+  w.job = WJ_COUNT;                 // hp > h_high = 0: the first walk (:154-170)
+  w.s.h_high = w.s.hp * HMULT;
+  for (int k = 0; k < 4; ++k) acc[4 * i + k] = 0.0;
+}
+
+// one walk per pending particle, WD_SLICES blocks each
+__global__ void __launch_bounds__(WD_THREADS) k_wide_walk(
+    int n, const WideState* __restrict__ ws, const double4* __restrict__ pm,
+    const double4* __restrict__ vel, HydroTree t, const int* __restrict__ parent,
+    const int* __restrict__ level, int L, int c1, double* __restrict__ acc, DevError* err) {
+  __shared__ double red[WD_THREADS / 32];
+  const int i = blockIdx.x / WD_SLICES, slice = blockIdx.x % WD_SLICES;
+  if (i >= n) return;
+  const WideState& w = ws[i];
+  const int job = w.job;
+  if (job == WJ_DONE) return;                                    // block-uniform
+  const int p = w.p;
+  const double rx = w.P.x, ry = w.P.y, rz = w.P.z;
+  const double hrange = KERNRANGE * w.s.h_high;
+  const double hs = w.hs, ih = w.ih, hf = w.hf;
+  const double4 vp = w.v;
+  auto pass = [&](int c) {                             // BHhydrowalk_hgather.F90:36-40
+    const double4 h = t.hA[c];
+    const double d0 = h.x - rx, d1 = h.y - ry, d2 = h.z - rz;
+    const double tt = hrange + h.w;
+    return ((d0 * d0 + d1 * d1) + d2 * d2) <= tt * tt;
+  };
+  double s0 = 0.0;
+  GhFinal f;
+  f.rt = 0.0; f.om = 0.0; f.dv = 0.0; f.zt = 0.0;
+  const int stride = WD_SLICES * WD_THREADS;
+  for (int c = slice * WD_THREADS + threadIdx.x; c <= c1; c += stride) {
+    const int lv = level[c];
+    const int4 lk = t.link[c];
+    if (!(lv == L || (lv < L && lk.x > 0))) continue;
+    bool reach = true;
+    for (int a = parent[c]; a >= 0 && reach; a = parent[a]) reach = pass(a);
+    if (!reach) continue;
+    const int stop = lk.y;
+    int cur = c, visits = 0;
     while (true) {
-      while (true) {                                                   // :154-191
-        if (s.hp > s.h_high) {
-          s.h_high = s.hp * HMULT;
-          double cnt = 0.0;
-          wide_walk(t, parent, level, L, c1, rx, ry, rz, KERNRANGE * s.h_high, err, p,
-                    [&](int) { cnt += 1.0; });
-          s.pp_pot = (int)block_sum(cnt, red);
-          ++nwalk;
-        }
-        if (s.pp_pot < pp_gather) {
-          s.h_high = 0.0;
-          s.pp_pot = 0;
-          s.hp = s.hp * HMULT;
-          if (++s.ngrow > HGROW_CAP) { bad = true; break; }
-        }
-        if (s.pp_pot > 0) break;
+      if (++visits > t.ctot + 2) {
+        set_error(err, SEREN_GPU_ERR_WALK, KID_GRADH, p, cur);
+        break;
       }
-      if (bad) break;
-      const double ih = 1.0 / s.hp;                                    // :199-235
-      const double hf = pow(ih, NDIMPR);
-      const double hs = (KERNRANGESQD * s.hp) * s.hp;
-      double part = 0.0;
-      wide_walk(t, parent, level, L, c1, rx, ry, rz, KERNRANGE * s.h_high, err, p, [&](int q) {
-        const double4 Q = pm[q];
-        const double d0 = Q.x - rx, d1 = Q.y - ry, d2 = Q.z - rz;
-        const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
-        if (q != p && drsqd < hs) gh_density_in(drsqd, Q.w, ih, hf, part);
-      });
-      ++npass;
-      if (gh_after_pass(s, mp, h_fac, rextent, (mp * t0.x) * hf + block_sum(part, red))) break;
+      const int4 l2 = t.link[cur];
+      const bool ok = pass(cur);
+      if (ok && l2.x > 0) {
+        for (int k = 0; k < l2.x; ++k) {
+          const int q = l2.w + k;
+          if (job == WJ_COUNT) {
+            s0 += 1.0;                                   // pp_pot counts every particle
+            continue;
+          }
+          if (q == p) continue;
+          const double4 Q = pm[q];
+          const double d0 = Q.x - rx, d1 = Q.y - ry, d2 = Q.z - rz;
+          const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
+          if (job == WJ_PASS) {
+            if (drsqd < hs) gh_density_in(drsqd, Q.w, ih, hf, s0);
+          } else if (drsqd <= hs) {
+            const double4 V = vel[q];
+            const double dv0 = V.x - vp.x, dv1 = V.y - vp.y, dv2 = V.z - vp.z;
+            gh_final_in(drsqd, Q.w, (dv0 * d0 + dv1 * d1) + dv2 * d2, ih, hf, f);
+          }
+        }
+        cur = l2.y;
+      } else if (ok && l2.x == 0) {
+        cur = l2.z;
+      } else {
+        cur = l2.y;
+      }
+      if (cur == stop || cur > t.ctot) break;
     }
-    if (bad) {
-      if (threadIdx.x == 0) set_error(err, SEREN_GPU_ERR_WALK, KID_GRADH, p, -1);
-      continue;
+  }
+  const double r0 = block_sum(job == WJ_FINAL ? f.rt : s0, red);
+  if (threadIdx.x == 0) atomicAdd(acc + 4 * i, r0);
+  if (job == WJ_FINAL) {
+    const double r1 = block_sum(f.om, red), r2 = block_sum(f.dv, red), r3 = block_sum(f.zt, red);
+    if (threadIdx.x == 0) {
+      atomicAdd(acc + 4 * i + 1, r1);
+      atomicAdd(acc + 4 * i + 2, r2);
+      atomicAdd(acc + 4 * i + 3, r3);
     }
-    const double hp = h_fac * pow(mp / s.rho, ONETHIRD);              // :317-425
-    const double ih = 1.0 / hp;
-    const double hf = pow(ih, NDIMPR);
-    const double hs = (KERNRANGESQD * hp) * hp;
-    const double4 vp = vel[p];
-    GhFinal f;
-    f.rt = 0.0; f.om = 0.0; f.dv = 0.0; f.zt = 0.0;
-    wide_walk(t, parent, level, L, c1, rx, ry, rz, KERNRANGE * s.h_high, err, p, [&](int q) {
-      const double4 Q = pm[q];
-      const double d0 = Q.x - rx, d1 = Q.y - ry, d2 = Q.z - rz;
-      const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
-      if (q == p || drsqd > hs) return;
-      const double4 V = vel[q];
-      const double dv0 = V.x - vp.x, dv1 = V.y - vp.y, dv2 = V.z - vp.z;
-      gh_final_in(drsqd, Q.w, (dv0 * d0 + dv1 * d1) + dv2 * d2, ih, hf, f);
-    });
-    ++npass;
+  }
+}
+
+// the reference's next step for each particle; *more = 1 while walks remain
+__global__ void k_wide_update(int n, WideState* __restrict__ ws, double* __restrict__ acc,
+                              const double4* __restrict__ tabA, double h_fac, int pp_gather,
+                              double rextent, double2* __restrict__ hz, double* __restrict__ rho,
+                              double* __restrict__ omega, double* __restrict__ divv,
+                              double* __restrict__ drhodt, int* __restrict__ more,
+                              DevError* err, unsigned long long* counts) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  WideState& w = ws[i];
+  if (w.job == WJ_DONE) return;
+  GhState& s = w.s;
+  const double mp = w.P.w;
+  const double4 t0 = tabA[0];
+  double* a = acc + 4 * i;
+  if (w.job == WJ_FINAL) {                                          // :426-442
     GhFinal g;
-    gh_final_init(g, mp, ih, hf, t0);
-    g.rt = g.rt + block_sum(f.rt, red);
-    g.om = g.om + block_sum(f.om, red);
-    g.dv = g.dv + block_sum(f.dv, red);
-    g.zt = g.zt + block_sum(f.zt, red);
-    if (threadIdx.x == 0) gh_store(p, mp, hp, g, hz, rho, omega, divv, drhodt, err);
+    gh_final_init(g, mp, w.ih, w.hf, t0);
+    g.rt = g.rt + a[0];
+    g.om = g.om + a[1];
+    g.dv = g.dv + a[2];
+    g.zt = g.zt + a[3];
+    gh_store(w.p, mp, w.hp, g, hz, rho, omega, divv, drhodt, err);
+    w.job = WJ_DONE;
+    atomicAdd(counts + 5, 1ull);
+    return;
   }
-  if (threadIdx.x == 0) {
-    atomicAdd(counts + 3, nwalk);
-    atomicAdd(counts + 5, npass);
+  if (w.job == WJ_COUNT) {
+    s.pp_pot = (int)a[0];
+    atomicAdd(counts + 3, 1ull);
+  } else {                                                          // WJ_PASS
+    atomicAdd(counts + 5, 1ull);
+    if (gh_after_pass(s, mp, h_fac, rextent, (mp * t0.x) * w.hf + a[0])) {
+      w.hp = h_fac * pow(mp / s.rho, ONETHIRD);                      // :317
+      w.ih = 1.0 / w.hp;
+      w.hf = pow(w.ih, NDIMPR);
+      w.hs = (KERNRANGESQD * w.hp) * w.hp;
+      w.job = WJ_FINAL;
+      a[0] = a[1] = a[2] = a[3] = 0.0;
+      *more = 1;
+      return;
+    }
   }
+  a[0] = a[1] = a[2] = a[3] = 0.0;
+  while (true) {                                                    // :154-191
+    if (s.hp > s.h_high) {
+      s.h_high = s.hp * HMULT;
+      w.job = WJ_COUNT;
+      *more = 1;
+      return;
+    }
+    if (s.pp_pot < pp_gather) {
+      s.h_high = 0.0;
+      s.pp_pot = 0;
+      s.hp = s.hp * HMULT;
+      if (++s.ngrow > HGROW_CAP) {
+        set_error(err, SEREN_GPU_ERR_WALK, KID_GRADH, w.p, -1);
+        w.job = WJ_DONE;
+        return;
+      }
+    }
+    if (s.pp_pot > 0) break;
+  }
+  w.ih = 1.0 / s.hp;                                                // :199-210
+  w.hf = pow(w.ih, NDIMPR);
+  w.hs = (KERNRANGESQD * s.hp) * s.hp;
+  w.job = WJ_PASS;
+  *more = 1;
 }
 
 // get_neib (sph/get_neib.F90:10-140) in two kernels.
@@ -1312,6 +1383,12 @@ static int gr_grid(const Ctx& c, int nact, int which) {
   return std::max(1, std::min(blocks, c.wstack_slots / GR_WARPS));
 }
 
+int wide_scratch_alloc(Ctx& c) {
+  if (cudaMalloc(&c.wst, sizeof(WideState) * WD_BATCH) != cudaSuccess) return -1;
+  if (cudaMalloc(&c.wacc, sizeof(double) * 4 * WD_BATCH) != cudaSuccess) return -1;
+  return 0;
+}
+
 void launch_gradh(Ctx& c, int nact) {
   if (nact <= 0) return;
   unsigned long long* counts = reinterpret_cast<unsigned long long*>(c.d_counts);
@@ -1337,18 +1414,46 @@ void launch_gradh(Ctx& c, int nact) {
       c.redo, c.work + 1, c.pm, c.hz, c.vel, c.rho, c.omega, c.div_v, c.drhodt, t, c.tabA,
       c.prm.h_fac, c.prm.pp_gather, c.info.rextent, reinterpret_cast<int*>(c.wstack),
       2 * c.wstack_cap, c.wide, c.work + 2, c.d_err, counts);
-  // a cover of the tree: the first level with at least 2 cells per thread, and the leaves above
-  int L = c.info.ltot;
-  for (int l = 0; l <= c.info.ltot; ++l)
-    if (c.info.last_cell[l] - c.info.first_cell[l] + 1 >= 2 * GWD_THREADS) {
-      L = l;
-      break;
+  // the particles whose walks outgrew the redo kernel's scratch: rounds of
+  // whole-GPU walks until each has taken its last step
+  int nwide = 0;
+  cudaMemcpyAsync(&nwide, c.work + 2, sizeof(int), cudaMemcpyDeviceToHost, c.st);
+  cudaStreamSynchronize(c.st);
+  if (nwide > 0) {
+    int L = c.info.ltot;                         // cover: a level with a cell per thread
+    for (int l = 0; l <= c.info.ltot; ++l)
+      if (c.info.last_cell[l] - c.info.first_cell[l] + 1 >= WD_SLICES * WD_THREADS) {
+        L = l;
+        break;
+      }
+    const int round_cap = 4 * GRADH_ITERATION_MAX + 2 * HGROW_CAP + 16;
+    for (int b0 = 0; b0 < nwide; b0 += WD_BATCH) {
+      const int n = std::min(WD_BATCH, nwide - b0);
+      k_wide_init<<<nb(n, 128), 128, 0, c.st>>>(n, c.wide + b0, c.pm, c.hz, c.vel,
+                                                  c.info.rextent, static_cast<WideState*>(c.wst), c.wacc, counts);
+      ++c.nlaunch;
+      for (int round = 0;; ++round) {
+        k_wide_walk<<<n * WD_SLICES, WD_THREADS, 0, c.st>>>(
+            n, static_cast<WideState*>(c.wst), c.pm, c.vel, t, c.parent, c.level, L,
+            c.info.last_cell[L], c.wacc,
+            c.d_err);
+        cudaMemsetAsync(c.work + 3, 0, sizeof(int), c.st);
+        k_wide_update<<<nb(n, 128), 128, 0, c.st>>>(
+            n, static_cast<WideState*>(c.wst), c.wacc, c.tabA, c.prm.h_fac, c.prm.pp_gather, c.info.rextent, c.hz, c.rho,
+            c.omega, c.div_v, c.drhodt, c.work + 3, c.d_err, counts);
+        c.nlaunch += 2;
+        int more = 0;
+        cudaMemcpyAsync(&more, c.work + 3, sizeof(int), cudaMemcpyDeviceToHost, c.st);
+        cudaStreamSynchronize(c.st);
+        if (!more) break;
+        if (round > round_cap) {               // cannot happen: each step is bounded
+          k_flag_error<<<1, 1, 0, c.st>>>(c.d_err, SEREN_GPU_ERR_WALK, KID_GRADH);
+          break;
+        }
+      }
     }
-  k_gradh_wide<<<sm_count(c) * 2, GWD_THREADS, 0, c.st>>>(
-      c.wide, c.work + 2, c.pm, c.hz, c.vel, c.rho, c.omega, c.div_v, c.drhodt, t, c.parent,
-      c.level, L, c.info.last_cell[L], c.tabA, c.prm.h_fac, c.prm.pp_gather, c.info.rextent,
-      c.d_err, counts);
-  c.nlaunch += 4;
+  }
+  c.nlaunch += 3;
 }
 
 void launch_neib(Ctx& c, int nact) {
