@@ -236,22 +236,25 @@ __device__ __forceinline__ void pair32_far(float d0, float d1, float d2, float i
 }
 
 // BHgrav_accel.F90:159-189 in FP32, dr = rp - rc
-__device__ __forceinline__ void cell32(float d0, float d1, float d2, const float4& a, const float4& q,
-                                       float q5, float& ax, float& ay, float& az, float& ap) {
+// q holds q1..q4, q5z (q5, -(q1 + q3)); m the cell mass
+__device__ __forceinline__ void cell32(float d0, float d1, float d2, float m, const float4& q,
+                                       const float2& q5z, float& ax, float& ay, float& az,
+                                       float& ap) {
   const float drsqd = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
   const float invdrmag = rsqrtf(drsqd);
   const float invdrsqd = invdrmag * invdrmag;
   const float invdr3 = invdrsqd * invdrmag;
   const float invdr5 = invdr3 * invdrsqd;
   const float qx = fmaf(q.w, d2, fmaf(q.y, d1, q.x * d0));
-  const float qy = fmaf(q5, d2, fmaf(q.z, d1, q.y * d0));
-  const float qz = fmaf(-(q.x + q.z), d2, fmaf(q5, d1, q.w * d0));
+  const float qy = fmaf(q5z.x, d2, fmaf(q.z, d1, q.y * d0));
+  const float qz = fmaf(q5z.y, d2, fmaf(q5z.x, d1, q.w * d0));
   const float qscalar = fmaf(qz, d2, fmaf(qy, d1, qx * d0));
-  const float g = fmaf(2.5f * qscalar, invdr5 * invdrsqd, a.w * invdr3);
-  ax += fmaf(qx, invdr5, -g * d0);
-  ay += fmaf(qy, invdr5, -g * d1);
-  az += fmaf(qz, invdr5, -g * d2);
-  ap += fmaf(0.5f * qscalar, invdr5, a.w * invdrmag);
+  // -(2.5 (dr.Q.dr) / r^7 + m / r^3)
+  const float ng = fmaf(-2.5f * qscalar, invdr5 * invdrsqd, -(m * invdr3));
+  ax = fmaf(ng, d0, fmaf(qx, invdr5, ax));
+  ay = fmaf(ng, d1, fmaf(qy, invdr5, ay));
+  az = fmaf(ng, d2, fmaf(qz, invdr5, az));
+  ap = fmaf(m, invdrmag, fmaf(0.5f * qscalar, invdr5, ap));
 }
 
 template <bool MIXED>
@@ -259,14 +262,16 @@ struct GwTypes {
   using R = float;
   using R2 = float2;
   using R4 = float4;
-  static constexpr int CAP = 96;   // accepted-cell entries per warp list
-  static constexpr int PREP = 128; // near-field records prepared per flush pass
+  using Q5 = float2;               // q5, -(q1 + q3)
+  static constexpr int CAP = 64;   // accepted-cell entries per warp list
+  static constexpr int PREP = 96;  // near-field records prepared per flush pass
 };
 template <>
 struct GwTypes<false> {
   using R = double;
   using R2 = double2;
   using R4 = double4;
+  using Q5 = double;
   static constexpr int CAP = 64;
   static constexpr int PREP = 64;
 };
@@ -277,7 +282,7 @@ struct GwRec {
   using T = GwTypes<MIXED>;
   typename T::R4 ca[T::CAP];       // cell: mixed (r_ref - COM, m), FP64 (COM, m)
   typename T::R4 cb[T::CAP];       // q1..q4
-  typename T::R cq5[T::CAP];
+  typename T::Q5 cq5[T::CAP];
   int cid[T::CAP];
   unsigned cmask[T::CAP];
   int qid[GW_PITEMS];
@@ -300,7 +305,7 @@ __device__ __forceinline__ int warp_incl(int v, int lane) {
 }
 
 template <bool MIXED>
-__global__ void __launch_bounds__(GW_THREADS)
+__global__ void __launch_bounds__(GW_THREADS, MIXED ? 6 : 4)
 k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ pm,
             const double2* __restrict__ hz, GravWalk t, const double4* __restrict__ tabG,
             double* __restrict__ acc, double* __restrict__ gpot, int nsink,
@@ -350,7 +355,7 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
         if constexpr (MIXED) {
           R.ca[e] = make_float4((float)(rx - a.x), (float)(ry - a.y), (float)(rz - a.z), (float)a.w);
           R.cb[e] = make_float4((float)q.x, (float)q.y, (float)q.z, (float)q.w);
-          R.cq5[e] = (float)q5;
+          R.cq5[e] = make_float2((float)q5, (float)(-(q.x + q.z)));
         } else {
           R.ca[e] = a;
           R.cb[e] = q;
@@ -360,13 +365,15 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
       __syncwarp();
       if constexpr (MIXED) {
         float sx = 0.f, sy = 0.f, sz = 0.f, sp = 0.f;
+        int mine = 0;
         for (int e = 0; e < nc; ++e) {
           if ((R.cmask[e] >> lane) & 1u) {
             const float4 a = R.ca[e];
-            cell32(ux + a.x, uy + a.y, uz + a.z, a, R.cb[e], R.cq5[e], sx, sy, sz, sp);
-            ++ncell;
+            cell32(ux + a.x, uy + a.y, uz + a.z, a.w, R.cb[e], R.cq5[e], sx, sy, sz, sp);
+            ++mine;
           }
         }
+        ncell += mine;
         kc.add(0, sx); kc.add(1, sy); kc.add(2, sz); kc.add(3, sp);
       } else {
         for (int e = 0; e < nc; ++e) {
