@@ -471,26 +471,41 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
         R.fcell[lane] = cc;
       }
       __syncwarp();
+      // each lane's MAC test on the popped cells, four at a time with their
+      // loads issued first; a lane inside the FP32 bracket takes the exact
+      // FP64 test (rare, a warp-uniform branch)
       unsigned macc = 0;
-      for (int e = 0; e < k; ++e) {
-        const unsigned mt = R.ftest[e];
-        if (mt == 0u) continue;                              // warp-uniform
-        bool accept = false;
-        if ((mt >> lane) & 1u) {
-          const float4 wa = R.fw[e];
-          const float d0 = px32 - wa.x, d1 = py32 - wa.y, d2 = pz32 - wa.z;
-          const float d2s = (d0 * d0 + d1 * d1) + d2 * d2;
-          if (d2s > wa.w) {
-            accept = true;
-          } else if (d2s >= R.flo[e]) {                      // exact test, :146-155
-            const int ce = R.fcell[e];
-            const double4 a = t.gA[ce];
-            const double e0 = P.x - a.x, e1 = P.y - a.y, e2 = P.z - a.z;
-            accept = ((e0 * e0 + e1 * e1) + e2 * e2) > t.gC[ce].y;
-          }
+      for (int e0 = 0; e0 < k; e0 += 4) {
+        float4 wa[4];
+        float lo[4];
+        unsigned mt[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int e = min(e0 + u, k - 1);
+          wa[u] = R.fw[e];
+          lo[u] = R.flo[e];
+          mt[u] = e0 + u < k ? R.ftest[e] : 0u;
         }
-        const unsigned b = __ballot_sync(FULLMASK, accept);
-        if (lane == e) macc = b;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const bool mine = (mt[u] >> lane) & 1u;
+          const float d0 = px32 - wa[u].x, d1 = py32 - wa[u].y, d2 = pz32 - wa[u].z;
+          const float d2s = (d0 * d0 + d1 * d1) + d2 * d2;
+          const bool hi = d2s > wa[u].w;
+          unsigned b = __ballot_sync(FULLMASK, mine && hi);
+          const bool amb = mine && !hi && d2s >= lo[u];
+          if (__any_sync(FULLMASK, amb)) {                   // exact test, :146-155
+            bool a2 = false;
+            if (amb) {
+              const int ce = R.fcell[e0 + u];
+              const double4 a = t.gA[ce];
+              const double e0d = P.x - a.x, e1d = P.y - a.y, e2d = P.z - a.z;
+              a2 = ((e0d * e0d + e1d * e1d) + e2d * e2d) > t.gC[ce].y;
+            }
+            b |= __ballot_sync(FULLMASK, a2);
+          }
+          if (lane == e0 + u) macc = b;
+        }
       }
       const unsigned mopn = m & ~macc;
       // accepted cells
