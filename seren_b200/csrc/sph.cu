@@ -1183,7 +1183,12 @@ __device__ __forceinline__ float m4_w1_bin(float x, bool tc) {
   return 0.318309886f * (kf < 0.5f * (float)KERNTOT ? inner : outer);
 }
 
-template <bool MIXED>
+constexpr int HY_SUB = 4;        // threads per particle in the mixed hydro kernel
+
+// SUB consecutive threads share one particle, each taking every SUB-th entry
+// of its neighbour list, and their sums are added at the end (SUB = 1 keeps the
+// reference's order of terms).
+template <bool MIXED, int SUB>
 __global__ void __launch_bounds__(128, 8) k_hydro(int nact, const int* __restrict__ act,
                                                const double4* __restrict__ pm,
                                                const double2* __restrict__ hz,
@@ -1196,9 +1201,11 @@ __global__ void __launch_bounds__(128, 8) k_hydro(int nact, const int* __restric
                                                const int* __restrict__ pplist, int L, HydroTree t,
                                                const double4* __restrict__ tabG, double alpha,
                                                bool tc, double* __restrict__ acc, DevError* err) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nact) return;
-  const int p = act ? act[i] : i;
+  const int gi = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = gi / SUB, sub = gi % SUB;
+  if (SUB == 1 && i >= nact) return;
+  const bool valid = i < nact;
+  const int p = valid ? (act ? act[i] : i) : 0;
   const double4 P = pm[p];
   const double hp = hz[p].x;
   const double invhp = 1.0 / hp;
@@ -1292,11 +1299,11 @@ __global__ void __launch_bounds__(128, 8) k_hydro(int nact, const int* __restric
       ad2 = ad2 - ((g * u2) * wmean) / rhomean;
     }
   };
-  const int nn = pptot[p];
+  const int nn = valid ? pptot[p] : 0;
   if (nn <= L) {
     const int* row = pplist + (size_t)p * L;
-    for (int k = 0; k < nn; ++k) pair(row[k]);
-  } else {
+    for (int k = sub; k < nn; k += SUB) pair(row[k]);
+  } else if (sub == 0) {
     // get_neib_on_fly (sph/get_neib_on_fly.F90:11-130): same test as get_neib
     const double hsp = (KERNRANGESQD * hp) * hp;
     walk_gather_scatter(t, P.x, P.y, P.z, KERNRANGE * hp, err, p, [&](int q) {
@@ -1308,6 +1315,18 @@ __global__ void __launch_bounds__(128, 8) k_hydro(int nact, const int* __restric
       const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
       if (drsqd <= hsp || drsqd <= hsq) pair(q);
     });
+  }
+  if (SUB > 1) {
+#pragma unroll
+    for (int o = SUB / 2; o > 0; o >>= 1) {
+      f0 += __shfl_xor_sync(0xffffffffu, f0, o);
+      f1 += __shfl_xor_sync(0xffffffffu, f1, o);
+      f2 += __shfl_xor_sync(0xffffffffu, f2, o);
+      g0 += __shfl_xor_sync(0xffffffffu, g0, o);
+      g1 += __shfl_xor_sync(0xffffffffu, g1, o);
+      g2 += __shfl_xor_sync(0xffffffffu, g2, o);
+    }
+    if (!valid || sub != 0) return;
   }
   double* a = acc + (size_t)p * 3;
   if (MIXED) {
@@ -1482,11 +1501,11 @@ void launch_hydro(Ctx& c, int nact) {
                                                   c.hf4);
   ++c.nlaunch;
   if (c.prm.precision == 0)
-    k_hydro<false><<<nb(nact, 128), 128, 0, c.st>>>(
+    k_hydro<false, 1><<<nb(nact, 128), 128, 0, c.st>>>(
         nact, c.act, c.pm, c.hz, c.vel, c.rho, c.pf, c.hf4, c.sound, c.pptot, c.pplist,
         c.prm.pp_limit, hydro_tree(c), c.tabG, c.prm.alpha, c.prm.kernel == 1, c.acc, c.d_err);
   else
-    k_hydro<true><<<nb(nact, 128), 128, 0, c.st>>>(
+    k_hydro<true, HY_SUB><<<nb((long)nact * HY_SUB, 128), 128, 0, c.st>>>(
         nact, c.act, c.pm, c.hz, c.vel, c.rho, c.pf, c.hf4, c.sound, c.pptot, c.pplist,
         c.prm.pp_limit, hydro_tree(c), c.tabG, c.prm.alpha, c.prm.kernel == 1, c.acc, c.d_err);
   ++c.nlaunch;
@@ -1642,11 +1661,11 @@ extern "C" int seren_gpu_hydro_forces_noalloc(int32_t n, const double* parray, c
   k_hydro_prep<<<nb(n, 256), 256, 0, st>>>(n, hz, rho, omega, press, pf, hf4);
   const HydroTree none{};   // every row fits its list, so the kernel never walks a tree
   if (precision == 0)
-    k_hydro<false><<<nb(n, 128), 128, 0, st>>>(n, nullptr, pm, hz, vel, rho, pf, hf4, sound,
+    k_hydro<false, 1><<<nb(n, 128), 128, 0, st>>>(n, nullptr, pm, hz, vel, rho, pf, hf4, sound,
                                                  pptot, pplist, pp_limit, none, tab, alpha,
                                                  kernel == 1, a, d_err);
   else
-    k_hydro<true><<<nb(n, 128), 128, 0, st>>>(n, nullptr, pm, hz, vel, rho, pf, hf4, sound,
+    k_hydro<true, HY_SUB><<<nb((long)n * HY_SUB, 128), 128, 0, st>>>(n, nullptr, pm, hz, vel, rho, pf, hf4, sound,
                                                 pptot, pplist, pp_limit, none, tab, alpha,
                                                 kernel == 1, a, d_err);
   return noalloc_status(st, d_err);
