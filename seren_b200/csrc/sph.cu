@@ -455,7 +455,8 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
     double* __restrict__ divv, double* __restrict__ drhodt, const double4* __restrict__ tabA,
     double h_fac, int pp_gather, double rextent, const int* __restrict__ leaves,
     const int* __restrict__ nleaf, const int* __restrict__ npot, int* __restrict__ redo,
-    int* __restrict__ nredo, DevError* err, unsigned long long* counts) {
+    int* __restrict__ nredo, int* __restrict__ prune, int L, DevError* err,
+    unsigned long long* counts) {
   __shared__ int cand_all[GP_WARPS][GP_SEG * LEAFMAX];
   __shared__ double inb_all[GP_WARPS][3][GP_INB];   // candidates inside 2h: r^2, m, dv.dr
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -479,6 +480,12 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
     s.pp_pot = n >= 0 ? npot[p] : 0;
     bool single = live && (n < 0 || s.pp_pot < pp_gather);             // :175-181 would grow h
     bool active = live && !single;
+    // The candidates within 2 h_high of the particle, recorded in its row of
+    // `prune` by the first pass: every later pass has h <= h_high (else the
+    // particle walks again), so they hold all the candidates it can count.
+    const double hh = (KERNRANGESQD * s.h_high) * s.h_high;
+    int npr = -1;
+    bool first = true;
     double rt = 0.0;
     while (true) {
       const unsigned A = __ballot_sync(FULL, active);
@@ -491,49 +498,69 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
         const double xj = __shfl_sync(FULL, rx, j), yj = __shfl_sync(FULL, ry, j),
                      zj = __shfl_sync(FULL, rz, j);
         const double hsj = __shfl_sync(FULL, hs, j), ihj = __shfl_sync(FULL, ih, j),
-                     hfj = __shfl_sync(FULL, hf, j);
+                     hfj = __shfl_sync(FULL, hf, j), hhj = __shfl_sync(FULL, hh, j);
         const int pj = __shfl_sync(FULL, p, j);
         const int nj = __shfl_sync(FULL, n, j);
+        const int nprj = __shfl_sync(FULL, npr, j);
+        int* prj = prune + (size_t)pj * L;
         // r^2 of every candidate; those inside 2h (:218) are packed into the
         // buffer, whose terms are then evaluated 32 at a time
         double part = 0.0;
-        for (int s0 = 0; s0 < nj; s0 += GP_SEG) {     // the row, GP_SEG leaves at a time
-        const int nc = gp_flatten(leaves + (size_t)pj * GH_LEAVES + s0, min(GP_SEG, nj - s0),
-                                  cand, lane);
-        int nin = 0;
-        for (int b = 0; b < nc; b += 64) {           // two chunks of candidates in flight
-          const int k0 = b + lane, k1 = b + 32 + lane;
-          const int q0 = k0 < nc ? cand[k0] : pj;
-          const int q1 = k1 < nc ? cand[k1] : pj;
-          const double4 Q0 = pm[q0];
-          const double4 Q1 = pm[q1];
+        int kept = 0;
+        auto chunks = [&](int nc, auto getq) {
+          int nin = 0;
+          for (int b = 0; b < nc; b += 64) {         // two chunks of candidates in flight
+            const int k0 = b + lane, k1 = b + 32 + lane;
+            const int q0 = k0 < nc ? getq(k0) : pj;
+            const int q1 = k1 < nc ? getq(k1) : pj;
+            const double4 Q0 = pm[q0];
+            const double4 Q1 = pm[q1];
 #pragma unroll
-          for (int u = 0; u < 2; ++u) {
-            const double4 Q = u == 0 ? Q0 : Q1;
-            const int q = u == 0 ? q0 : q1;
-            const double d0 = Q.x - xj, d1 = Q.y - yj, d2 = Q.z - zj;
-            const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
-            const bool in = q != pj && drsqd < hsj;
-            const unsigned m = __ballot_sync(FULL, in);
-            if (in) {
-              const int o = nin + __popc(m & lt);
-              ind2[o] = drsqd;
-              inm[o] = Q.w;
+            for (int u = 0; u < 2; ++u) {
+              const double4 Q = u == 0 ? Q0 : Q1;
+              const int q = u == 0 ? q0 : q1;
+              const double d0 = Q.x - xj, d1 = Q.y - yj, d2 = Q.z - zj;
+              const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
+              const bool in = q != pj && drsqd < hsj;
+              const unsigned m = __ballot_sync(FULL, in);
+              if (in) {
+                const int o = nin + __popc(m & lt);
+                ind2[o] = drsqd;
+                inm[o] = Q.w;
+              }
+              nin += __popc(m);
+              if (first) {                           // record the candidates within 2 h_high
+                const bool keep = q != pj && drsqd < hhj;
+                const unsigned mk = __ballot_sync(FULL, keep);
+                const int pos = kept + __popc(mk & lt);
+                if (keep && pos < L) prj[pos] = q;
+                kept += __popc(mk);
+              }
             }
-            nin += __popc(m);
+            if (nin > GP_INB - 64 || b + 64 >= nc) {
+              __syncwarp();
+              for (int t = lane; t < nin; t += 32) gh_density_in(ind2[t], inm[t], ihj, hfj, part);
+              nin = 0;
+              __syncwarp();
+            }
           }
-          if (nin > GP_INB - 64 || b + 64 >= nc) {
-            __syncwarp();
-            for (int t = lane; t < nin; t += 32) gh_density_in(ind2[t], inm[t], ihj, hfj, part);
-            nin = 0;
-            __syncwarp();
+          niter += (nc + 31) >> 5;
+        };
+        if (first || nprj < 0) {
+          for (int s0 = 0; s0 < nj; s0 += GP_SEG) {   // the row, GP_SEG leaves at a time
+            const int nc = gp_flatten(leaves + (size_t)pj * GH_LEAVES + s0,
+                                      min(GP_SEG, nj - s0), cand, lane);
+            chunks(nc, [&](int k) { return cand[k]; });
           }
+          if (first && lane == j) npr = kept <= L ? kept : -1;
+        } else {
+          chunks(nprj, [&](int k) { return prj[k]; });
         }
-        niter += (nc + 31) >> 5;
-        }
+        __syncwarp();
         const double sum = warp_sum(part);
         if (lane == j) rt = sum;
       }
+      first = false;
       if (active) {
         ++npass;
         ncands += s.pp_pot;
@@ -564,15 +591,17 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
                                       __shfl_sync(FULL, vp.z, j), 0.0);
       const int pj = __shfl_sync(FULL, p, j);
       const int nj = __shfl_sync(FULL, n, j);
+      // the recorded candidates serve when 2h < 2 h_high (those within 2h of the
+      // final h are among them)
+      const int nprj = __shfl_sync(FULL, (npr >= 0 && hp < s.h_high) ? npr : -1, j);
+      const int* prj = prune + (size_t)pj * L;
       GhFinal part;
       part.rt = 0.0; part.om = 0.0; part.dv = 0.0; part.zt = 0.0;
-      for (int s0 = 0; s0 < nj; s0 += GP_SEG) {       // the row, GP_SEG leaves at a time
-      const int nc = gp_flatten(leaves + (size_t)pj * GH_LEAVES + s0, min(GP_SEG, nj - s0),
-                                cand, lane);
+      auto fchunks = [&](int nc, auto getq) {
       int nin = 0;
       for (int b = 0; b < nc; b += 32) {
         const int k = b + lane;
-        const int q = k < nc ? cand[k] : pj;
+        const int q = k < nc ? getq(k) : pj;
         const double4 Q = pm[q];
         const double d0 = Q.x - xj, d1 = Q.y - yj, d2 = Q.z - zj;
         const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
@@ -596,6 +625,15 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
         }
       }
       niter += (nc + 31) >> 5;
+      };
+      if (nprj < 0) {
+        for (int s0 = 0; s0 < nj; s0 += GP_SEG) {     // the row, GP_SEG leaves at a time
+          const int nc = gp_flatten(leaves + (size_t)pj * GH_LEAVES + s0, min(GP_SEG, nj - s0),
+                                    cand, lane);
+          fchunks(nc, [&](int k) { return cand[k]; });
+        }
+      } else {
+        fchunks(nprj, [&](int k) { return prj[k]; });
       }
       const double srt = warp_sum(part.rt), som = warp_sum(part.om), sdv = warp_sum(part.dv),
                    szt = warp_sum(part.zt);
@@ -1426,8 +1464,8 @@ void launch_gradh(Ctx& c, int nact) {
   cudaMemsetAsync(c.work + 1, 0, 2 * sizeof(int), c.st);
   k_gradh_pass<<<blocks, GP_THREADS, 0, c.st>>>(
       nact, c.act, c.pm, c.hz, c.vel, c.rho, c.omega, c.div_v, c.drhodt, c.tabA, c.prm.h_fac,
-      c.prm.pp_gather, c.info.rextent, c.leaves, c.nleaf, c.npot, c.redo, c.work + 1, c.d_err,
-      counts);
+      c.prm.pp_gather, c.info.rextent, c.leaves, c.nleaf, c.npot, c.redo, c.work + 1,
+      c.pplist, c.prm.pp_limit, c.d_err, counts);
   // three walk-stack slots of scratch per redo warp
   k_gradh_redo<<<std::max(1, (c.wstack_slots / 3) / RD_WARPS), RD_THREADS, 0, c.st>>>(
       c.redo, c.work + 1, c.pm, c.hz, c.vel, c.rho, c.omega, c.div_v, c.drhodt, t, c.tabA,
