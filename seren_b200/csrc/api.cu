@@ -195,7 +195,7 @@ void free_all(Ctx& c) {
                 c.rs_hist, c.bbox_part, c.branch, c.branch_next, c.nchild, c.choff, c.cstart,
                 c.bflag, c.bscan, c.leaf, c.nextcell, c.ifopen, c.pstart, c.pcount, c.parent,
                 c.level, c.nkids, c.work, c.sinks, c.wstack, c.leaves, c.nleaf, c.npot, c.redo, c.wide, c.wst, c.wacc, c.link, c.gA, c.gB, c.gC, c.wA, c.wLo, c.hA, c.hrm, c.hA32, c.hrm32, c.hmax, c.bbmin, c.bbmax, c.d_info,
-                c.d_err, c.d_counts, c.tabA, c.tabG, c.scan.total, c.scan.level_buf[0],
+                c.d_err, c.d_counts, c.tabA, c.tabG, c.tabG32, c.scan.total, c.scan.level_buf[0],
                 c.scan.level_buf[1], c.scan.level_buf[2], c.scan.level_buf[3]};
   for (void* p : ps)
     if (p) cudaFree(p);
@@ -234,7 +234,7 @@ int alloc_all(Ctx& c) {
          alloc(c.hA, C) | alloc(c.hrm, C) |
          alloc(c.hmax, C) | alloc(c.bbmin, C) | alloc(c.bbmax, C);
   bad |= alloc(c.d_info, 1) | alloc(c.d_err, 1) | alloc(c.d_counts, 32) | alloc(c.sinks, 5 * 1024);
-  bad |= alloc(c.tabA, KERNTOT + 1) | alloc(c.tabG, KERNTOT + 1);
+  bad |= alloc(c.tabA, KERNTOT + 1) | alloc(c.tabG, KERNTOT + 1) | alloc(c.tabG32, KERNTOT + 1);
   c.wstack_slots = std::max(grav_walk_slots(c), hydro_walk_slots(c));
   c.wstack_cap = grav_walk_stack_cap(c);
   bad |= alloc(c.wstack, (size_t)c.wstack_slots * c.wstack_cap);
@@ -258,6 +258,12 @@ int alloc_all(Ctx& c) {
   if (cudaMemcpy(c.tabA, ta.data(), sizeof(double4) * ta.size(), cudaMemcpyHostToDevice) != cudaSuccess)
     return -1;
   if (cudaMemcpy(c.tabG, tg.data(), sizeof(double4) * tg.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+    return -1;
+  std::vector<float4> t32(KERNTOT + 1);
+  for (int i = 0; i <= KERNTOT; ++i)
+    t32[i] = make_float4((float)w5[i], (float)w4[i], (float)w6[i], 0.0f);
+  if (cudaMemcpy(c.tabG32, t32.data(), sizeof(float4) * t32.size(), cudaMemcpyHostToDevice) !=
+      cudaSuccess)
     return -1;
   return 0;
 }

@@ -114,6 +114,7 @@ struct Ctx {
   // kernel tables
   double4* tabA = nullptr;
   double4* tabG = nullptr;
+  float4* tabG32 = nullptr;   // FP32 w5, w4, w6 of tabG (mixed gravity)
 
   bool have_tree = false;
   bool have_sph = false;

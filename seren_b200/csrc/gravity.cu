@@ -8,8 +8,8 @@
 //  * mixed: the walk, the MAC test (drsqd > dminsqd) and the separations stay
 //    FP64, so exactly the same cells are accepted and the same pairs visited;
 //    the separation is then cast to FP32 and the cell/pair term evaluated in
-//    FP32 (rsqrtf, FMA), with the M4 softening kernel evaluated analytically at
-//    the centre of the reference's table bin; terms are summed in FP32 with
+//    FP32 (rsqrtf, FMA), with the M4 softening kernel read at the reference's
+//    table bin from an FP32 copy of its table; terms are summed in FP32 with
 //    Kahan compensation and added to the FP64 result once.
 #include <algorithm>
 
@@ -171,49 +171,28 @@ struct GravWalk {
   double rootx, rooty, rootz;
 };
 
-// M4 softened-gravity functions w5, w4, w6 (setup/kernel.F90:80-81, :99-102)
-// at the centre of the reference's table bin int(5000 r/h) (clamped to
-// KERNTOT), in FP32; both polynomial pieces are evaluated and selected so the
-// lanes of a warp do not diverge.
-__device__ __forceinline__ void m4_grav_bin(float x, float& w5, float& w4, float& w6) {
-  const float kf = fminf(floorf(5000.0f * x), (float)KERNTOT);
-  const float s = fmaf(kf, 2.0e-4f, 1.0e-4f);
-  const float s2 = s * s;
-  const float i5 = s * fmaf(s2, fmaf(0.5f, s, -1.2f), 1.33333333f);
-  const float i4 = 0.318309886f * s * fmaf(2.25f, s, -3.0f);
-  const float i6 = fmaf(s2, fmaf(s2, fmaf(-0.1f, s, 0.3f), -0.666666667f), 1.4f);
-  const float rs = __fdividef(1.0f, s);
-  const float o5 = s * fmaf(s, fmaf(s, fmaf(-0.166666667f, s, 1.2f), -3.0f), 2.66666667f) -
-                   0.0666666667f * rs * rs;
-  const float sa = 2.0f - s;
-  const float o4 = -0.238732415f * sa * sa;
-  const float o6 = fmaf(s2, fmaf(s, fmaf(s, fmaf(0.0333333333f, s, -0.3f), 1.0f), -1.33333333f),
-                        1.6f) - 0.0666666667f * rs;
-  const bool in = kf < 0.5f * (float)KERNTOT;
-  w5 = in ? i5 : o5;
-  w4 = in ? i4 : o4;
-  w6 = in ? i6 : o6;
-}
-
-// gravity_gradh.F90:57-86 in FP32, dr = rpp - rp, invhq precomputed
+// gravity_gradh.F90:57-86 in FP32, dr = rpp - rp, invhq precomputed.  The M4
+// softened-gravity functions w5, w4, w6 (setup/kernel.F90:80-81, :99-102) come
+// from an FP32 copy of the reference's table at bin int(5000 r/h), clamped to
+// KERNTOT (tab32[k] = w5, w4, w6).
 __device__ __forceinline__ void pair32(float d0, float d1, float d2, float invhp, float zo_p,
-                                       float mq, float invhq, float zq, float& ax, float& ay,
+                                       float mq, float invhq, float zq,
+                                       const float4* __restrict__ tab32, float& ax, float& ay,
                                        float& az, float& ap) {
   const float drsqd = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
   const float inv = rsqrtf(fmaxf(drsqd, 1.0e-30f));
   const float drmag = drsqd * inv;
-  float w5, w4, w6;
   const float xp = drmag * invhp;
-  m4_grav_bin(xp, w5, w4, w6);
+  const float xq = drmag * invhq;
+  const float4 wp = tab32[(int)fminf(5000.0f * xp, (float)KERNTOT)];
+  const float4 wq = tab32[(int)fminf(5000.0f * xq, (float)KERNTOT)];
   const float ihp2 = invhp * invhp;
   const float inv2 = inv * inv;
-  float grav = xp < KERNRANGE ? ihp2 * fmaf(zo_p * w4, ihp2, w5) : inv2;
-  float dpot = xp < KERNRANGE ? invhp * w6 : inv;
-  const float xq = drmag * invhq;
-  m4_grav_bin(xq, w5, w4, w6);
+  float grav = xp < KERNRANGE ? ihp2 * fmaf(zo_p * wp.y, ihp2, wp.x) : inv2;
+  float dpot = xp < KERNRANGE ? invhp * wp.z : inv;
   const float ihq2 = invhq * invhq;
-  grav += xq < KERNRANGE ? ihq2 * fmaf(zq * w4, ihq2, w5) : inv2;
-  dpot += xq < KERNRANGE ? invhq * w6 : inv;
+  grav += xq < KERNRANGE ? ihq2 * fmaf(zq * wq.y, ihq2, wq.x) : inv2;
+  dpot += xq < KERNRANGE ? invhq * wq.z : inv;
   const float f = 0.5f * mq * inv * grav;
   ax = fmaf(f, d0, ax);
   ay = fmaf(f, d1, ay);
@@ -308,9 +287,9 @@ template <bool MIXED>
 __global__ void __launch_bounds__(GW_THREADS, MIXED ? 6 : 4)
 k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ pm,
             const double2* __restrict__ hz, GravWalk t, const double4* __restrict__ tabG,
-            double* __restrict__ acc, double* __restrict__ gpot, int nsink,
-            const double* __restrict__ sinks, int2* __restrict__ stacks, int* work,
-            DevError* err, unsigned long long* counts) {
+            const float4* __restrict__ tab32, double* __restrict__ acc,
+            double* __restrict__ gpot, int nsink, const double* __restrict__ sinks,
+            int2* __restrict__ stacks, int* work, DevError* err, unsigned long long* counts) {
   using Cfg = GwTypes<MIXED>;
   constexpr int CAP = Cfg::CAP;
   __shared__ GwRec<MIXED> srec[GW_WARPS];
@@ -420,7 +399,7 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
             const bool soft = on && (drmag * invhp32 < KERNRANGE || drmag * b.x < KERNRANGE);
             if (__any_sync(FULLMASK, soft)) {
               if (on) {
-                pair32(d0, d1, d2, invhp32, zo32, a.w, b.x, b.y, sx, sy, sz, sp);
+                pair32(d0, d1, d2, invhp32, zo32, a.w, b.x, b.y, tab32, sx, sy, sz, sp);
                 ++npair;
               }
             } else if (on) {
@@ -683,10 +662,10 @@ void launch_grav(Ctx& c, int nact, int nsink, const double* d_sinks) {
   cudaMemsetAsync(c.work, 0, sizeof(int), c.st);
   if (!mixed)
     k_grav_walk<false><<<blocks, GW_THREADS, 0, c.st>>>(nact, c.act, c.pm, c.hz, gw, c.tabG,
-        c.acc, c.gpot, nsink, d_sinks, c.wstack, c.work, c.d_err, counts);
+        c.tabG32, c.acc, c.gpot, nsink, d_sinks, c.wstack, c.work, c.d_err, counts);
   else
     k_grav_walk<true><<<blocks, GW_THREADS, 0, c.st>>>(nact, c.act, c.pm, c.hz, gw, c.tabG,
-        c.acc, c.gpot, nsink, d_sinks, c.wstack, c.work, c.d_err, counts);
+        c.tabG32, c.acc, c.gpot, nsink, d_sinks, c.wstack, c.work, c.d_err, counts);
   ++c.nlaunch;
 }
 
