@@ -284,7 +284,7 @@ __device__ __forceinline__ int warp_incl(int v, int lane) {
 }
 
 template <bool MIXED>
-__global__ void __launch_bounds__(GW_THREADS, MIXED ? 6 : 4)
+__global__ void __launch_bounds__(GW_THREADS, MIXED ? 5 : 4)
 k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ pm,
             const double2* __restrict__ hz, GravWalk t, const double4* __restrict__ tabG,
             const float4* __restrict__ tab32, double* __restrict__ acc,
@@ -345,6 +345,7 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
       if constexpr (MIXED) {
         float sx = 0.f, sy = 0.f, sz = 0.f, sp = 0.f;
         int mine = 0;
+#pragma unroll 2
         for (int e = 0; e < nc; ++e) {
           if ((R.cmask[e] >> lane) & 1u) {
             const float4 a = R.ca[e];
@@ -387,6 +388,7 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
         __syncwarp();
         if constexpr (MIXED) {
           float sx = 0.f, sy = 0.f, sz = 0.f, sp = 0.f;
+#pragma unroll 2
           for (int e = 0; e < nb; ++e) {
             const bool on = ((R.qmask[b0 + e] >> lane) & 1u) && R.qid[b0 + e] != p;
             const float4 a = R.pa[e];

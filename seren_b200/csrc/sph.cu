@@ -11,6 +11,7 @@
 // gives one thread to one particle and follows hydro_gradh step by step.
 #include <algorithm>
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 #include "ctx.cuh"
@@ -445,10 +446,29 @@ __device__ __forceinline__ int gp_flatten(const int* __restrict__ row, int n, in
   return total;
 }
 
+constexpr int GP_PSEG = 32;      // k_gradh_pass: leaves of a row flattened at a time
+constexpr int GP_PINB = 128;     // k_gradh_pass: packed in-range candidates per warp
+
+template <int N>
+using ICst = std::integral_constant<int, N>;
+
+// k_gradh_pass's per-warp shared state: the group's per-particle values that
+// the candidate loops read for one particle at a time (broadcast loads), a
+// flattened row segment, and the packed in-range candidates.
+struct GpWarp {
+  double x[32], y[32], z[32];
+  double hs[32], ih[32], hf[32];   // (2h)^2, 1/h, 1/h^3 of the pass in progress
+  double hh[32];                   // (2 h_high)^2: radius of the recorded candidates
+  int p[32], n[32], npr[32];       // particle, leaves in its row, recorded candidates (-1: none)
+  int cand[GP_PSEG * LEAFMAX];
+  double d2[GP_PINB], m[GP_PINB], dv[GP_PINB];
+};
+
 // 32 consecutive particles per warp: each lane holds its particle's iteration
 // state, so the per-particle arithmetic of a pass (h, its powers, the update
 // of :238-285) runs once per lane for all 32; each particle's candidates are
-// shared out over the 32 lanes in turn.
+// shared out over the 32 lanes in turn, 32*U at a time with all their loads
+// issued together (U = 4 for the recorded candidates of the density passes).
 __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
     int nact, const int* __restrict__ act, const double4* __restrict__ pm, double2* __restrict__ hz,
     const double4* __restrict__ vel, double* __restrict__ rho, double* __restrict__ omega,
@@ -457,34 +477,133 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
     const int* __restrict__ nleaf, const int* __restrict__ npot, int* __restrict__ redo,
     int* __restrict__ nredo, int* __restrict__ prune, int L, DevError* err,
     unsigned long long* counts) {
-  __shared__ int cand_all[GP_WARPS][GP_SEG * LEAFMAX];
-  __shared__ double inb_all[GP_WARPS][3][GP_INB];   // candidates inside 2h: r^2, m, dv.dr
+  __shared__ GpWarp gpw[GP_WARPS];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  int* cand = cand_all[w];
-  double* ind2 = inb_all[w][0];
-  double* inm = inb_all[w][1];
-  double* indv = inb_all[w][2];
+  GpWarp& W = gpw[w];
   const unsigned lt = (1u << lane) - 1u;
-  const double4 t0 = tabA[0];
-  unsigned long long npass = 0, ncands = 0, niter = 0, nsingle = 0;
+  unsigned npass = 0, ncands = 0, niter = 0, nsingle = 0;
+
+  // Density sum (:211-235) of particle j over the candidates getq(0..nc): r^2
+  // of each; those inside 2h (:218) are packed into the buffer and their terms
+  // summed 32 at a time.  KEEP (first pass): the candidates within 2 h_high
+  // are recorded, in order, in j's row of `prune`.
+  auto dscan = [&](int j, int nc, auto getq, auto u_, auto keep_, int& kept, double& part) {
+    constexpr int U = decltype(u_)::value;
+    constexpr bool KEEP = decltype(keep_)::value;
+    const double xj = W.x[j], yj = W.y[j], zj = W.z[j], hsj = W.hs[j];
+    const int pj = W.p[j];
+    int nin = 0;
+    for (int b = 0; b < nc; b += 32 * U) {
+      int q[U];
+      double4 Q[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int k = b + 32 * u + lane;
+        q[u] = k < nc ? getq(k) : pj;
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) Q[u] = pm[q[u]];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const double d0 = Q[u].x - xj, d1 = Q[u].y - yj, d2 = Q[u].z - zj;
+        const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
+        const bool in = q[u] != pj && drsqd < hsj;
+        const unsigned mi = __ballot_sync(FULL, in);
+        if (in) {
+          const int o = nin + __popc(mi & lt);
+          W.d2[o] = drsqd;
+          W.m[o] = Q[u].w;
+        }
+        nin += __popc(mi);
+        if constexpr (KEEP) {
+          const bool keep = q[u] != pj && drsqd < W.hh[j];
+          const unsigned mk = __ballot_sync(FULL, keep);
+          const int pos = kept + __popc(mk & lt);
+          if (keep && pos < L) prune[(size_t)pj * L + pos] = q[u];
+          kept += __popc(mk);
+        }
+      }
+      if (nin > GP_PINB - 32 * U || b + 32 * U >= nc) {
+        __syncwarp();
+        const double ihj = W.ih[j], hfj = W.hf[j];
+        for (int t = lane; t < nin; t += 32) gh_density_in(W.d2[t], W.m[t], ihj, hfj, part);
+        nin = 0;
+        __syncwarp();
+      }
+    }
+    niter += (nc + 31) >> 5;
+  };
+
+  // Final-pass sums (:360-425) of particle j over the candidates getq(0..nc),
+  // its velocity vj
+  auto fscan = [&](int j, int nc, auto getq, auto u_, double vxj, double vyj, double vzj,
+                   GhFinal& part) {
+    constexpr int U = decltype(u_)::value;
+    const double xj = W.x[j], yj = W.y[j], zj = W.z[j], hsj = W.hs[j];
+    const int pj = W.p[j];
+    int nin = 0;
+    for (int b = 0; b < nc; b += 32 * U) {
+      int q[U];
+      double4 Q[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int k = b + 32 * u + lane;
+        q[u] = k < nc ? getq(k) : pj;
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) Q[u] = pm[q[u]];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const double d0 = Q[u].x - xj, d1 = Q[u].y - yj, d2 = Q[u].z - zj;
+        const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
+        const bool in = q[u] != pj && drsqd <= hsj;                   // :360
+        const unsigned mi = __ballot_sync(FULL, in);
+        if (in) {
+          const double4 V = vel[q[u]];
+          const double dv0 = V.x - vxj, dv1 = V.y - vyj, dv2 = V.z - vzj;
+          const int o = nin + __popc(mi & lt);
+          W.d2[o] = drsqd;
+          W.m[o] = Q[u].w;
+          W.dv[o] = (dv0 * d0 + dv1 * d1) + dv2 * d2;
+        }
+        nin += __popc(mi);
+      }
+      if (nin > GP_PINB - 32 * U || b + 32 * U >= nc) {
+        __syncwarp();
+        const double ihj = W.ih[j], hfj = W.hf[j];
+        for (int t = lane; t < nin; t += 32)
+          gh_final_in(W.d2[t], W.m[t], W.dv[t], ihj, hfj, part);
+        nin = 0;
+        __syncwarp();
+      }
+    }
+    niter += (nc + 31) >> 5;
+  };
+
   for (int g = blockIdx.x * GP_WARPS + w; (long long)g * 32 < nact; g += gridDim.x * GP_WARPS) {
     const int i = g * 32 + lane;
     const bool live = i < nact;
     const int p = live ? (act ? act[i] : i) : (act ? act[nact - 1] : nact - 1);
     const int n = live ? nleaf[p] : 0;
     const double4 P = pm[p];
-    const double rx = P.x, ry = P.y, rz = P.z, mp = P.w;
+    const double mp = P.w;
     GhState s;
     gh_init(s, hz[p].x, rextent);
     s.h_high = s.hp * HMULT;                                           // :157-170
     s.pp_pot = n >= 0 ? npot[p] : 0;
     bool single = live && (n < 0 || s.pp_pot < pp_gather);             // :175-181 would grow h
     bool active = live && !single;
+    __syncwarp();                                      // the previous group's reads are done
+    W.x[lane] = P.x;
+    W.y[lane] = P.y;
+    W.z[lane] = P.z;
     // The candidates within 2 h_high of the particle, recorded in its row of
     // `prune` by the first pass: every later pass has h <= h_high (else the
     // particle walks again), so they hold all the candidates it can count.
-    const double hh = (KERNRANGESQD * s.h_high) * s.h_high;
-    int npr = -1;
+    W.hh[lane] = (KERNRANGESQD * s.h_high) * s.h_high;
+    W.p[lane] = p;
+    W.n[lane] = n;
+    W.npr[lane] = -1;
     bool first = true;
     double rt = 0.0;
     while (true) {
@@ -492,71 +611,30 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
       if (A == 0u) break;
       const double ih = 1.0 / s.hp;                                    // :199-235
       const double hf = pow(ih, NDIMPR);
-      const double hs = (KERNRANGESQD * s.hp) * s.hp;
+      W.ih[lane] = ih;
+      W.hf[lane] = hf;
+      W.hs[lane] = (KERNRANGESQD * s.hp) * s.hp;
+      __syncwarp();
       for (unsigned todo = A; todo != 0u; todo &= todo - 1u) {
         const int j = __ffs(todo) - 1;
-        const double xj = __shfl_sync(FULL, rx, j), yj = __shfl_sync(FULL, ry, j),
-                     zj = __shfl_sync(FULL, rz, j);
-        const double hsj = __shfl_sync(FULL, hs, j), ihj = __shfl_sync(FULL, ih, j),
-                     hfj = __shfl_sync(FULL, hf, j), hhj = __shfl_sync(FULL, hh, j);
-        const int pj = __shfl_sync(FULL, p, j);
-        const int nj = __shfl_sync(FULL, n, j);
-        const int nprj = __shfl_sync(FULL, npr, j);
-        int* prj = prune + (size_t)pj * L;
-        // r^2 of every candidate; those inside 2h (:218) are packed into the
-        // buffer, whose terms are then evaluated 32 at a time
         double part = 0.0;
         int kept = 0;
-        auto chunks = [&](int nc, auto getq) {
-          int nin = 0;
-          for (int b = 0; b < nc; b += 64) {         // two chunks of candidates in flight
-            const int k0 = b + lane, k1 = b + 32 + lane;
-            const int q0 = k0 < nc ? getq(k0) : pj;
-            const int q1 = k1 < nc ? getq(k1) : pj;
-            const double4 Q0 = pm[q0];
-            const double4 Q1 = pm[q1];
-#pragma unroll
-            for (int u = 0; u < 2; ++u) {
-              const double4 Q = u == 0 ? Q0 : Q1;
-              const int q = u == 0 ? q0 : q1;
-              const double d0 = Q.x - xj, d1 = Q.y - yj, d2 = Q.z - zj;
-              const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
-              const bool in = q != pj && drsqd < hsj;
-              const unsigned m = __ballot_sync(FULL, in);
-              if (in) {
-                const int o = nin + __popc(m & lt);
-                ind2[o] = drsqd;
-                inm[o] = Q.w;
-              }
-              nin += __popc(m);
-              if (first) {                           // record the candidates within 2 h_high
-                const bool keep = q != pj && drsqd < hhj;
-                const unsigned mk = __ballot_sync(FULL, keep);
-                const int pos = kept + __popc(mk & lt);
-                if (keep && pos < L) prj[pos] = q;
-                kept += __popc(mk);
-              }
-            }
-            if (nin > GP_INB - 64 || b + 64 >= nc) {
-              __syncwarp();
-              for (int t = lane; t < nin; t += 32) gh_density_in(ind2[t], inm[t], ihj, hfj, part);
-              nin = 0;
-              __syncwarp();
-            }
-          }
-          niter += (nc + 31) >> 5;
-        };
+        const int nprj = W.npr[j];
         if (first || nprj < 0) {
-          for (int s0 = 0; s0 < nj; s0 += GP_SEG) {   // the row, GP_SEG leaves at a time
-            const int nc = gp_flatten(leaves + (size_t)pj * GH_LEAVES + s0,
-                                      min(GP_SEG, nj - s0), cand, lane);
-            chunks(nc, [&](int k) { return cand[k]; });
+          const int nj = W.n[j];
+          const int* row = leaves + (size_t)W.p[j] * GH_LEAVES;
+          for (int s0 = 0; s0 < nj; s0 += GP_PSEG) {   // the row, GP_PSEG leaves at a time
+            const int nc = gp_flatten(row + s0, min(GP_PSEG, nj - s0), W.cand, lane);
+            auto fromrow = [&](int k) { return W.cand[k]; };
+            if (first) dscan(j, nc, fromrow, ICst<2>{}, std::true_type{}, kept, part);
+            else dscan(j, nc, fromrow, ICst<2>{}, std::false_type{}, kept, part);
           }
-          if (first && lane == j) npr = kept <= L ? kept : -1;
+          if (first && lane == 0) W.npr[j] = kept <= L ? kept : -1;
         } else {
-          chunks(nprj, [&](int k) { return prj[k]; });
+          const int* prj = prune + (size_t)W.p[j] * L;
+          dscan(j, nprj, [&](int k) { return prj[k]; }, ICst<4>{}, std::false_type{}, kept,
+                part);
         }
-        __syncwarp();
         const double sum = warp_sum(part);
         if (lane == j) rt = sum;
       }
@@ -564,12 +642,13 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
       if (active) {
         ++npass;
         ncands += s.pp_pot;
-        if (gh_after_pass(s, mp, h_fac, rextent, (mp * t0.x) * hf + rt)) active = false;
+        if (gh_after_pass(s, mp, h_fac, rextent, (mp * tabA[0].x) * hf + rt)) active = false;
         else if (s.hp > s.h_high) {                                    // :154-170 would walk again
           single = true;
           active = false;
         }
       }
+      __syncwarp();
     }
     // final pass (:317-425)
     const bool ok = live && !single;
@@ -577,63 +656,33 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
     const double hp = h_fac * pow(mp / s.rho, ONETHIRD);
     const double ih = 1.0 / hp;
     const double hf = pow(ih, NDIMPR);
-    const double hs = (KERNRANGESQD * hp) * hp;
     const double4 vp = vel[p];
+    W.ih[lane] = ih;
+    W.hf[lane] = hf;
+    W.hs[lane] = (KERNRANGESQD * hp) * hp;
+    // the recorded candidates serve when 2h < 2 h_high (those within 2h of the
+    // final h are among them)
+    if (!(hp < s.h_high)) W.npr[lane] = -1;
+    __syncwarp();
     GhFinal f;
-    gh_final_init(f, mp, ih, hf, t0);
+    gh_final_init(f, mp, ih, hf, tabA[0]);
     for (unsigned todo = F; todo != 0u; todo &= todo - 1u) {
       const int j = __ffs(todo) - 1;
-      const double xj = __shfl_sync(FULL, rx, j), yj = __shfl_sync(FULL, ry, j),
-                   zj = __shfl_sync(FULL, rz, j);
-      const double hsj = __shfl_sync(FULL, hs, j), ihj = __shfl_sync(FULL, ih, j),
-                   hfj = __shfl_sync(FULL, hf, j);
-      const double4 vj = make_double4(__shfl_sync(FULL, vp.x, j), __shfl_sync(FULL, vp.y, j),
-                                      __shfl_sync(FULL, vp.z, j), 0.0);
-      const int pj = __shfl_sync(FULL, p, j);
-      const int nj = __shfl_sync(FULL, n, j);
-      // the recorded candidates serve when 2h < 2 h_high (those within 2h of the
-      // final h are among them)
-      const int nprj = __shfl_sync(FULL, (npr >= 0 && hp < s.h_high) ? npr : -1, j);
-      const int* prj = prune + (size_t)pj * L;
+      const double vxj = __shfl_sync(FULL, vp.x, j), vyj = __shfl_sync(FULL, vp.y, j),
+                   vzj = __shfl_sync(FULL, vp.z, j);
+      const int nprj = W.npr[j];
       GhFinal part;
       part.rt = 0.0; part.om = 0.0; part.dv = 0.0; part.zt = 0.0;
-      auto fchunks = [&](int nc, auto getq) {
-      int nin = 0;
-      for (int b = 0; b < nc; b += 32) {
-        const int k = b + lane;
-        const int q = k < nc ? getq(k) : pj;
-        const double4 Q = pm[q];
-        const double d0 = Q.x - xj, d1 = Q.y - yj, d2 = Q.z - zj;
-        const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
-        const bool in = q != pj && drsqd <= hsj;                      // :360
-        const unsigned m = __ballot_sync(FULL, in);
-        if (in) {
-          const double4 V = vel[q];
-          const double dv0 = V.x - vj.x, dv1 = V.y - vj.y, dv2 = V.z - vj.z;
-          const int o = nin + __popc(m & lt);
-          ind2[o] = drsqd;
-          inm[o] = Q.w;
-          indv[o] = (dv0 * d0 + dv1 * d1) + dv2 * d2;
-        }
-        nin += __popc(m);
-        if (nin > GP_INB - 32 || b + 32 >= nc) {
-          __syncwarp();
-          for (int t = lane; t < nin; t += 32)
-            gh_final_in(ind2[t], inm[t], indv[t], ihj, hfj, part);
-          nin = 0;
-          __syncwarp();
-        }
-      }
-      niter += (nc + 31) >> 5;
-      };
       if (nprj < 0) {
-        for (int s0 = 0; s0 < nj; s0 += GP_SEG) {     // the row, GP_SEG leaves at a time
-          const int nc = gp_flatten(leaves + (size_t)pj * GH_LEAVES + s0, min(GP_SEG, nj - s0),
-                                    cand, lane);
-          fchunks(nc, [&](int k) { return cand[k]; });
+        const int nj = W.n[j];
+        const int* row = leaves + (size_t)W.p[j] * GH_LEAVES;
+        for (int s0 = 0; s0 < nj; s0 += GP_PSEG) {     // the row, GP_PSEG leaves at a time
+          const int nc = gp_flatten(row + s0, min(GP_PSEG, nj - s0), W.cand, lane);
+          fscan(j, nc, [&](int k) { return W.cand[k]; }, ICst<1>{}, vxj, vyj, vzj, part);
         }
       } else {
-        fchunks(nprj, [&](int k) { return prj[k]; });
+        const int* prj = prune + (size_t)W.p[j] * L;
+        fscan(j, nprj, [&](int k) { return prj[k]; }, ICst<2>{}, vxj, vyj, vzj, part);
       }
       const double srt = warp_sum(part.rt), som = warp_sum(part.om), sdv = warp_sum(part.dv),
                    szt = warp_sum(part.zt);
@@ -654,10 +703,10 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
       redo[atomicAdd(nredo, 1)] = p;
     }
   }
-  atomicAdd(counts + 5, npass);
-  atomicAdd(counts + 6, ncands);
-  atomicAdd(counts + 15, nsingle);
-  if (lane == 0) atomicAdd(counts + 13, niter);
+  atomicAdd(counts + 5, (unsigned long long)npass);
+  atomicAdd(counts + 6, (unsigned long long)ncands);
+  atomicAdd(counts + 15, (unsigned long long)nsingle);
+  if (lane == 0) atomicAdd(counts + 13, (unsigned long long)niter);
 }
 
 // ---------------------------------------------------------------------------
