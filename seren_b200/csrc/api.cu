@@ -194,7 +194,7 @@ void free_all(Ctx& c) {
                 c.pptot, c.pplist, c.stage, c.istage, c.keys, c.keys_alt, c.idx, c.idx_alt,
                 c.rs_hist, c.bbox_part, c.branch, c.branch_next, c.nchild, c.choff, c.cstart,
                 c.bflag, c.bscan, c.leaf, c.nextcell, c.ifopen, c.pstart, c.pcount, c.parent,
-                c.level, c.nkids, c.work, c.sinks, c.wstack, c.leaves, c.nleaf, c.npot, c.redo, c.wide, c.wst, c.wacc, c.link, c.gA, c.gB, c.gC, c.wA, c.wLo, c.hA, c.hrm, c.hA32, c.hrm32, c.hmax, c.bbmin, c.bbmax, c.d_info,
+                c.level, c.nkids, c.work, c.sinks, c.wstack, c.leaves, c.nleaf, c.npot, c.redo, c.wide, c.wst, c.wacc, c.link, c.gA, c.gB, c.gC, c.wA, c.hN, c.hA, c.hrm, c.hA32, c.hrm32, c.hmax, c.bbmin, c.bbmax, c.d_info,
                 c.d_err, c.d_counts, c.tabA, c.tabG, c.tabG32, c.scan.total, c.scan.level_buf[0],
                 c.scan.level_buf[1], c.scan.level_buf[2], c.scan.level_buf[3]};
   for (void* p : ps)
@@ -230,7 +230,7 @@ int alloc_all(Ctx& c) {
   bad |= alloc(c.hA32, C) | alloc(c.hrm32, C) | alloc(c.nkids, C) | alloc(c.work, 4);
   bad |= alloc(c.leaves, P * 256) | alloc(c.nleaf, P) | alloc(c.npot, P) | alloc(c.redo, P) | alloc(c.wide, P);
   bad |= wide_scratch_alloc(c);
-  bad |= alloc(c.gA, C) | alloc(c.gB, C) | alloc(c.gC, C) | alloc(c.wA, C) | alloc(c.wLo, C) |
+  bad |= alloc(c.gA, C) | alloc(c.gB, C) | alloc(c.gC, C) | alloc(c.wA, 2 * C) | alloc(c.hN, 2 * C) |
          alloc(c.hA, C) | alloc(c.hrm, C) |
          alloc(c.hmax, C) | alloc(c.bbmin, C) | alloc(c.bbmax, C);
   bad |= alloc(c.d_info, 1) | alloc(c.d_err, 1) | alloc(c.d_counts, 32) | alloc(c.sinks, 5 * 1024);

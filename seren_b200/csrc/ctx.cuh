@@ -84,8 +84,15 @@ struct Ctx {
   double4* gA = nullptr;      // gravity: COM x, y, z, m
   double4* gB = nullptr;      // gravity: q1..q4 (xx, xy, yy, zx)
   double2* gC = nullptr;      // gravity: q5 (zy), dminsqd
-  float4* wA = nullptr;       // gravity walk: FP32 COM - root centre, upper MAC bracket
-  float* wLo = nullptr;       // gravity walk: lower MAC bracket
+  // gravity walk node, two float4 per cell (one 32-byte sector): FP32 COM -
+  // root centre and the upper MAC bracket; the lower bracket, then (as int
+  // bits) the first particle of a leaf or first child of a branch, and the
+  // leaf's particle count or minus the branch's number of children
+  float4* wA = nullptr;
+  // hydro walk node, two float4 per cell: hA32; hrm32, then (as int bits)
+  // the first particle of a leaf or first child of a branch, and the leaf's
+  // particle count or minus the branch's number of children
+  float4* hN = nullptr;
   double4* hA = nullptr;      // hydro: bbox centre x, y, z, rmax
   double* hrm = nullptr;      // hydro: hrangemax
   float4* hA32 = nullptr;     // hydro walk: FP32 centre - root centre, rmax rounded up

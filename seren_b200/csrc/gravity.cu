@@ -159,10 +159,10 @@ constexpr int GW_PITEMS = 384;   // near-field (particle, mask) items per warp l
 constexpr unsigned FULLMASK = 0xffffffffu;
 
 struct GravWalk {
-  const int4* link;
-  const int* nkids;     // children of a branch cell: ifopen .. ifopen+nkids-1
-  const float4* wA;     // FP32 COM relative to the root centre, hi bracket
-  const float* wLo;     // lo bracket
+  // two float4 per cell: (FP32 COM relative to the root centre, hi bracket),
+  // (lo bracket, first particle of a leaf / first child of a branch, leaf
+  // count / -children, 0) as int bits
+  const float4* wN;
   const double4* gA;
   const double4* gB;
   const double2* gC;
@@ -435,20 +435,18 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
       const int k = min(32, sp);
       sp -= k;
       gent += k;
-      int cc = 0, nk = 0;
+      int cc = 0, cnt = 0, base = 0;     // cnt: leaf particles, or -children of a branch
       unsigned m = 0;
-      int4 lk = make_int4(-1, 0, 0, 0);
       if (lane < k) {
         const int2 ent = S[sp + lane];
         cc = ent.x;
         m = (unsigned)ent.y;
-        lk = t.link[cc];
-        if (lk.x != 1) {
-          R.fw[lane] = t.wA[cc];
-          R.flo[lane] = t.wLo[cc];
-          if (lk.x == 0) nk = t.nkids[cc];
-        }
-        R.ftest[lane] = lk.x == 1 ? 0u : m;
+        const float4 na = t.wN[2 * cc], nb2 = t.wN[2 * cc + 1];
+        cnt = __float_as_int(nb2.z);
+        base = __float_as_int(nb2.y);
+        R.fw[lane] = na;
+        R.flo[lane] = nb2.x;
+        R.ftest[lane] = cnt == 1 ? 0u : m;
         R.fcell[lane] = cc;
       }
       __syncwarp();
@@ -471,7 +469,7 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
         for (int u = 0; u < 4; ++u) {
           const bool mine = (mt[u] >> lane) & 1u;
           const float d0 = px32 - wa[u].x, d1 = py32 - wa[u].y, d2 = pz32 - wa[u].z;
-          const float d2s = (d0 * d0 + d1 * d1) + d2 * d2;
+          const float d2s = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
           const bool hi = d2s > wa[u].w;
           unsigned b = __ballot_sync(FULLMASK, mine && hi);
           const bool amb = mine && !hi && d2s >= lo[u];
@@ -500,24 +498,24 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
       }
       nc += __popc(bc);
       // opened leaves: their particles join the near-field list
-      const int npush = (lk.x > 0 && mopn != 0u) ? lk.x : 0;
+      const int npush = (cnt > 0 && mopn != 0u) ? cnt : 0;
       pi_all += npush;
       pi_full += mopn == rootmask ? npush : 0;
       const int pin = warp_incl(npush, lane);
       for (int q = 0; q < npush; ++q) {
-        R.qid[np + pin - npush + q] = lk.w + q;
+        R.qid[np + pin - npush + q] = base + q;
         R.qmask[np + pin - npush + q] = mopn;
       }
       np += __shfl_sync(FULLMASK, pin, 31);
       // opened branch cells: children onto the stack
-      const int nch = (lk.x == 0 && mopn != 0u) ? nk : 0;
+      const int nch = (cnt < 0 && mopn != 0u) ? -cnt : 0;
       const int cin = warp_incl(nch, lane);
       const int ctotal = __shfl_sync(FULLMASK, cin, 31);
       if (sp + ctotal > t.scap || gent > (long long)t.ctot + 1) {
         if (lane == 0) set_error(err, SEREN_GPU_ERR_WALK, MIXED ? KID_GRAV_MIXED : KID_GRAV, p, cc);
         break;
       }
-      for (int q = 0; q < nch; ++q) S[sp + cin - nch + q] = make_int2(lk.z + q, (int)mopn);
+      for (int q = 0; q < nch; ++q) S[sp + cin - nch + q] = make_int2(base + q, (int)mopn);
       sp += ctotal;
       if (nc > CAP - 32) flush_cells();
       if (np > GW_PITEMS - 32 * LEAFMAX) flush_pairs();
@@ -656,7 +654,7 @@ int grav_walk_stack_cap(const Ctx& c) { return std::min(GW_STACK, c.cmax + 1); }
 void launch_grav(Ctx& c, int nact, int nsink, const double* d_sinks) {
   if (nact <= 0) return;
   unsigned long long* counts = reinterpret_cast<unsigned long long*>(c.d_counts);
-  const GravWalk gw{c.link, c.nkids, c.wA, c.wLo, c.gA, c.gB, c.gC, c.info.ctot, c.wstack_cap,
+  const GravWalk gw{c.wA, c.gA, c.gB, c.gC, c.info.ctot, c.wstack_cap,
                     c.info.root[0], c.info.root[1], c.info.root[2]};
   const bool mixed = c.prm.precision != 0;
   const int groups = nb(nact, 32);

@@ -28,6 +28,8 @@ struct HydroTree {
   const float4* hA32;   // FP32 centre - root centre, rmax rounded up
   const float* hrm32;   // hrangemax rounded up
   const int* nkids;     // children per cell (ids ifopen .. ifopen + nkids - 1)
+  const float4* hN;     // two per cell: hA32; hrm32, first particle / first child,
+                        // leaf count / -children (int bits)
   int ctot;
   double rootx, rooty, rootz;
   float delta;          // bound on the FP32 rounding of a root-relative coordinate
@@ -235,19 +237,19 @@ __device__ int gr_walk(const HydroTree& t, unsigned lanes, int2* S, int scap, Gr
     const int k = min(32, sp);
     sp -= k;
     gent += k;
-    int nk = 0;
+    int cnt = 0, base = 0;           // cnt: leaf particles, or -children of a branch
     unsigned m = 0;
-    int4 lk = make_int4(-1, 0, 0, 0);
     if (lane < k) {
       const int2 ent = S[sp + lane];
       const int cc = ent.x;
       m = (unsigned)ent.y;
-      lk = t.link[cc];
-      R.fa[lane] = t.hA32[cc];
-      R.fh[lane] = t.hrm32[cc];
+      const float4 na = t.hN[2 * cc], nb2 = t.hN[2 * cc + 1];
+      cnt = __float_as_int(nb2.z);
+      base = __float_as_int(nb2.y);
+      R.fa[lane] = na;
+      R.fh[lane] = nb2.x;
       R.fm[lane] = m;
       R.fc[lane] = cc;
-      if (lk.x == 0) nk = t.nkids[cc];
     }
     __syncwarp();
     unsigned mpass = 0;
@@ -257,20 +259,20 @@ __device__ int gr_walk(const HydroTree& t, unsigned lanes, int2* S, int scap, Gr
       if (lane == e) mpass = b;
     }
     nvisit += k;
-    const bool isleaf = lk.x > 0 && mpass != 0u;              // candidates of the lanes in mpass
+    const bool isleaf = cnt > 0 && mpass != 0u;               // candidates of the lanes in mpass
     const unsigned bl = __ballot_sync(FULL, isleaf);
     if (nent + __popc(bl) > GR_LCAP) return -1;
     if (isleaf) {
       const int o = nent + __popc(bl & lt);
-      R.code[o] = lk.w * 8 + (lk.x - 1);
+      R.code[o] = base * 8 + (cnt - 1);
       R.mask[o] = mpass;
     }
     nent += __popc(bl);
-    const int nch = (lk.x == 0 && mpass != 0u) ? nk : 0;      // opened for the lanes in mpass
+    const int nch = (cnt < 0 && mpass != 0u) ? -cnt : 0;      // opened for the lanes in mpass
     const int cin = warp_iscan(nch, lane);
     const int ctotal = __shfl_sync(FULL, cin, 31);
     if (sp + ctotal > scap || gent > (long long)t.ctot + 1) return -1;
-    for (int q = 0; q < nch; ++q) S[sp + cin - nch + q] = make_int2(lk.z + q, (int)mpass);
+    for (int q = 0; q < nch; ++q) S[sp + cin - nch + q] = make_int2(base + q, (int)mpass);
     sp += ctotal;
   }
   __syncwarp();
@@ -1442,7 +1444,7 @@ inline int nb(long n, int t) { return (int)((n + t - 1) / t); }
 
 HydroTree hydro_tree(const Ctx& c) {
   const double delta = ldexp(1.0, -22) * (c.info.cellsize > 0.0 ? c.info.cellsize : 1.0);
-  return HydroTree{c.link, c.hA, c.hrm, c.hA32, c.hrm32, c.nkids, c.info.ctot, c.info.root[0],
+  return HydroTree{c.link, c.hA, c.hrm, c.hA32, c.hrm32, c.nkids, c.hN, c.info.ctot, c.info.root[0],
                    c.info.root[1], c.info.root[2], (float)delta};
 }
 

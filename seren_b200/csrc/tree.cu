@@ -417,8 +417,8 @@ __global__ void k_stock_level(int cfirst, int clast, const int4* __restrict__ li
                               double4* __restrict__ hA, double* __restrict__ hmaxa,
                               double4* __restrict__ bbmina, double4* __restrict__ bbmaxa,
                               double rootx, double rooty, double rootz, double delta,
-                              float4* __restrict__ wA, float* __restrict__ wLo,
-                              float4* __restrict__ hA32) {
+                              const int* __restrict__ nkids, float4* __restrict__ wA,
+                              float4* __restrict__ hA32, float4* __restrict__ hN) {
   const int c = cfirst + blockIdx.x * blockDim.x + threadIdx.x;
   if (c > clast) return;
   const int4 lk = link[c];
@@ -510,9 +510,11 @@ __global__ void k_stock_level(int cfirst, int clast, const int4* __restrict__ li
   gC[c] = make_double2(qc[4], dminsqd);
   {
     const double marg = 2.0 * (8.0 * sqrt(dminsqd) * delta + 1.0e-6 * dminsqd + 16.0 * delta * delta);
-    wA[c] = make_float4((float)(rc[0] - rootx), (float)(rc[1] - rooty), (float)(rc[2] - rootz),
-                        __double2float_ru(dminsqd + marg));
-    wLo[c] = __double2float_rd(dminsqd - marg);
+    wA[2 * c] = make_float4((float)(rc[0] - rootx), (float)(rc[1] - rooty),
+                            (float)(rc[2] - rootz), __double2float_ru(dminsqd + marg));
+    wA[2 * c + 1] = make_float4(__double2float_rd(dminsqd - marg),
+                                __int_as_float(lk.x > 0 ? lk.w : lk.z),
+                                __int_as_float(lk.x > 0 ? lk.x : -nkids[c]), 0.0f);
   }
   hmaxa[c] = hmax;
   bbmina[c] = make_double4(bbmin[0], bbmin[1], bbmin[2], 0.0);
@@ -531,14 +533,18 @@ __global__ void k_stock_level(int cfirst, int clast, const int4* __restrict__ li
     hn = make_double4(hc[0], hc[1], hc[2], sqrt(diag));
   }
   hA[c] = hn;
-  hA32[c] = make_float4((float)(hn.x - rootx), (float)(hn.y - rooty), (float)(hn.z - rootz),
-                        __double2float_ru(hn.w));
+  const float4 h32 = make_float4((float)(hn.x - rootx), (float)(hn.y - rooty),
+                                 (float)(hn.z - rootz), __double2float_ru(hn.w));
+  hA32[c] = h32;
+  hN[2 * c] = h32;
+  hN[2 * c + 1] = make_float4(0.0f, __int_as_float(lk.x > 0 ? lk.w : lk.z),
+                              __int_as_float(lk.x > 0 ? lk.x : -nkids[c]), 0.0f);
 }
 
 // BHhydro_update_hmax.F90:29-88
 __global__ void k_hmax_level(int cfirst, int clast, const int4* __restrict__ link,
                              const double2* __restrict__ hz, double* __restrict__ hrm,
-                             float* __restrict__ hrm32) {
+                             float* __restrict__ hrm32, float4* __restrict__ hN) {
   const int c = cfirst + blockIdx.x * blockDim.x + threadIdx.x;
   if (c > clast) return;
   const int4 lk = link[c];
@@ -558,6 +564,7 @@ __global__ void k_hmax_level(int cfirst, int clast, const int4* __restrict__ lin
   }
   hrm[c] = hr;
   hrm32[c] = __double2float_ru(hr);
+  reinterpret_cast<float*>(hN)[8 * (size_t)c + 4] = hrm32[c];
 }
 
 // BHhydro_hguess.F90:106-155 (GRAD_H_SPH number criterion): the h of a
@@ -711,7 +718,7 @@ void launch_stock(Ctx& c) {
     k_stock_level<<<nb(cnt, 128), 128, 0, c.st>>>(f, la, c.link, c.pm, c.hz, c.prm.thetamaxsqd, daux,
                                                  c.gA, c.gB, c.gC, c.hA, c.hmax, c.bbmin, c.bbmax,
                                                  c.info.root[0], c.info.root[1], c.info.root[2],
-                                                 delta, c.wA, c.wLo, c.hA32); ++c.nlaunch;
+                                                 delta, c.nkids, c.wA, c.hA32, c.hN); ++c.nlaunch;
   }
 }
 
@@ -720,7 +727,7 @@ void launch_update_hmax(Ctx& c) {
     const int f = c.info.first_cell[l], la = c.info.last_cell[l];
     const int cnt = la - f + 1;
     if (cnt <= 0) continue;
-    k_hmax_level<<<nb(cnt, 128), 128, 0, c.st>>>(f, la, c.link, c.hz, c.hrm, c.hrm32); ++c.nlaunch;
+    k_hmax_level<<<nb(cnt, 128), 128, 0, c.st>>>(f, la, c.link, c.hz, c.hrm, c.hrm32, c.hN); ++c.nlaunch;
   }
 }
 
