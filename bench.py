@@ -9,9 +9,12 @@ hmax update, neighbour lists, isothermal thermal, hydro forces with MON97
 viscosity, Barnes-Hut gravity) followed by a drift r += v dt.  `value` is the
 mixed-precision (FP32 pair arithmetic) path with inputs resident in HBM; the
 FP64 path is timed on the same state for the speed-up and accuracy figures.
-`e2e` is the same metric through the host-buffer C ABI calls a Fortran caller
-makes (tree_update -> sph_update -> thermal on the host -> hydro_forces ->
-grav_forces), copies included.
+`e2e` is the same metric from pinned host buffers to pinned host buffers
+through seren_gpu_force_step_io (inputs copied in and every result copied
+back each step, the copies overlapped with the force step on a second
+stream); `e2e_reference_calls` is the same through the host-buffer calls a
+Fortran caller of the reference's interface makes (tree_update -> sph_update
+-> thermal on the host -> hydro_forces -> grav_forces), copies included.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -230,6 +233,68 @@ def run_resident(ic, precision, steps, warmup, ws):
     res = dict(total_ms=total_ms, stage_ms=(stage / steps).tolist(), launches=launches,
                counts=counts, ctx=g)
     return res, state
+
+
+def run_e2e_io(ic, precision, steps, warmup, ws):
+    """Steps through seren_gpu_force_step_io with pinned host buffers: each
+    step copies parray, v and c_s^2 in from the host and parray, v, c_s^2,
+    rho, omega, a, gpot and the permutation (tree order) back over them; the
+    host then drifts its positions (torch CPU ops, all cores), so every step
+    starts from the host's arrays."""
+    import ctypes as C
+
+    import torch
+
+    from seren_b200.gpu import GpuHotPath
+    torch.set_num_threads(os.cpu_count() or 1)
+    n = ic["parray"].shape[0]
+    g = GpuHotPath(n, params_for(ic, precision))
+
+    def pinned(shape, dtype=torch.float64):
+        return torch.empty(shape, dtype=dtype, pin_memory=True)
+
+    parray = pinned((n, 6)); parray.copy_(torch.from_numpy(ic["parray"]))
+    v = pinned((n, 3)); v.copy_(torch.from_numpy(ic["v"]))
+    csq = pinned((n,)); csq.copy_(torch.from_numpy(ic["sound"] ** 2))
+    rho, omega, gpot = (pinned((n,)) for _ in range(3))
+    a = pinned((n, 3))
+    perm = pinned((n,), torch.int32)
+    dp = C.POINTER(C.c_double)
+    ip = C.POINTER(C.c_int32)
+    P = lambda x: C.cast(x.data_ptr(), dp)  # noqa: E731
+    ctx = g._ctx
+    host_s = np.zeros(2)
+
+    def step(first):
+        t0 = time.perf_counter()
+        g._call("force_step_io", ctx, n, P(parray), P(v), P(csq), int(first), P(parray), P(v),
+                P(csq), P(rho), P(omega), P(a), P(gpot), C.cast(perm.data_ptr(), ip))
+        t1 = time.perf_counter()
+        parray[:, 0:3].add_(v, alpha=DT)
+        t2 = time.perf_counter()
+        host_s[:] += np.diff([t0, t1, t2])
+
+    stream = torch.cuda.ExternalStream(g.stream())
+    for w in range(max(warmup, 1)):
+        step(w == 0)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    barrier(ws)
+    start.record(stream)
+    host_s[:] = 0.0
+    for _ in range(steps):
+        step(False)
+    end.record(stream)
+    torch.cuda.synchronize()
+    barrier(ws)
+    total_ms = start.elapsed_time(end)
+    stage = g.last_step_stats()[0][5]
+    log(f"[bench] e2e (force_step_io) ms/step: call {1e3 * host_s[0] / steps:.1f} "
+        f"(device step {stage:.1f}), host drift {1e3 * host_s[1] / steps:.1f}")
+    h2d = n * (48 + 24 + 8)                          # parray, v, c_s^2
+    d2h = n * (48 + 24 + 8 + 8 + 8 + 24 + 8 + 4)     # parray, v, c_s^2, rho, omega, a, gpot, perm
+    g.close()
+    return dict(total_ms=total_ms, h2d=h2d, d2h=d2h)
 
 
 def run_e2e(ic, precision, steps, warmup, ws):
@@ -499,12 +564,18 @@ def main():
         acc = dict(rms_vs_fp64=float(np.sqrt(np.mean(err ** 2))), max_vs_fp64=float(err.max()),
                    same_order=bool(same))
         log(f"[bench] fp64: {fp64['ms_per_step']:.2f} ms/step, stages {fp64['stage_ms']}, {acc}")
-    e2e = None
+    e2e = e2e_calls = None
     if not args.no_e2e:
-        r = run_e2e(ic, 1, args.steps, args.warmup, ws)
+        r = run_e2e_io(ic, 1, args.steps, args.warmup, ws)
         e2e = dict(value=ws * n * args.steps / (max_over_ranks(ws, r["total_ms"]) * 1e-3),
                    unit=UNIT, h2d_bytes_per_step=r["h2d"], d2h_bytes_per_step=r["d2h"],
-                   ms_per_step=r["total_ms"] / args.steps)
+                   ms_per_step=r["total_ms"] / args.steps,
+                   api="seren_gpu_force_step_io (pinned host buffers in and out every step)")
+        r = run_e2e(ic, 1, args.steps, args.warmup, ws)
+        e2e_calls = dict(value=ws * n * args.steps / (max_over_ranks(ws, r["total_ms"]) * 1e-3),
+                         unit=UNIT, h2d_bytes_per_step=r["h2d"], d2h_bytes_per_step=r["d2h"],
+                         ms_per_step=r["total_ms"] / args.steps,
+                         api="tree_update, sph_update, hydro_forces, grav_forces")
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         sample = args.cpu_sample or (n if n <= (1 << 20) else n // 8)
@@ -561,6 +632,7 @@ def main():
                      "fp64_peak": fp64_peak},
         "cpu_baseline": cpu,
         "e2e": e2e,
+        "e2e_reference_calls": e2e_calls,
         "gpu_launches": mixed["launches"],
         "clocks": clocks,
     }

@@ -133,6 +133,23 @@ int seren_gpu_set_sinks(seren_gpu_ctx* ctx, int32_t nsink, const double* sink_rm
 int seren_gpu_download(seren_gpu_ctx* ctx, double* parray, double* v, double* rho,
                        double* omega, double* a, double* gpot, int32_t* perm_total);
 
+/* One force evaluation from host buffers to host buffers: the work of
+ * seren_gpu_upload(ptot, parray, v, csq), seren_gpu_force_step(first_call)
+ * and seren_gpu_download(parray_out, v_out, rho, omega, a, gpot, perm_total)
+ * in one call, plus csq_out (c_s^2 in tree order).  The copies overlap the
+ * force step on a second stream: v and c_s^2 come in during the tree build,
+ * and each result goes out once the stage that makes it has run (v, c_s^2,
+ * perm after the tree build; parray with the new h, rho, omega after grad-h;
+ * a and gpot after gravity).  Outputs are in tree order; any output may be
+ * NULL and may alias its input.  Pinned host buffers give overlapped copies.
+ * Not a reference entry point: it fuses the calls a caller of
+ * seren_gpu_tree_update / sph_update / hydro_forces / grav_forces makes
+ * each step when it keeps no state on the device. */
+int seren_gpu_force_step_io(seren_gpu_ctx* ctx, int32_t ptot, const double* parray,
+                            const double* v, const double* csq, int32_t first_call,
+                            double* parray_out, double* v_out, double* csq_out, double* rho,
+                            double* omega, double* a, double* gpot, int32_t* perm_total);
+
 /* Tree inspection (BHgrav_node / BHhydro_node of headers/modules.F90:907-959
  * in the reference's breadth-first cell numbering).  Counts first: pass NULL
  * arrays to get ctot and ltot.  plist rows hold particle ids (index_base) and

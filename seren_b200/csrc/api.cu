@@ -200,8 +200,12 @@ void free_all(Ctx& c) {
   for (void* p : ps)
     if (p) cudaFree(p);
   if (c.h_pin) cudaFreeHost(c.h_pin);
+  if (c.stage_io) cudaFree(c.stage_io);
   for (auto& e : c.ev)
     if (e) cudaEventDestroy(e);
+  for (auto& e : c.ev_io)
+    if (e) cudaEventDestroy(e);
+  if (c.st_io) cudaStreamDestroy(c.st_io);
   if (c.st) cudaStreamDestroy(c.st);
 }
 
@@ -319,6 +323,7 @@ int seren_gpu_create(seren_gpu_ctx** out, int64_t pmax, const seren_gpu_params* 
 void seren_gpu_destroy(seren_gpu_ctx* h) {
   if (!h) return;
   cudaStreamSynchronize(h->c.st);
+  if (h->c.st_io) cudaStreamSynchronize(h->c.st_io);
   seren::free_all(h->c);
   delete h;
 }
@@ -578,33 +583,91 @@ int seren_gpu_upload(seren_gpu_ctx* h, int32_t ptot, const double* parray, const
   return finish(c, "upload");
 }
 
-int seren_gpu_force_step(seren_gpu_ctx* h, int32_t first_call) {
-  if (!h) return SEREN_GPU_ERR_ARG;
-  Ctx& c = h->c;
-  if (!c.have_v || !c.have_csq || c.ptot < 1)
-    return fail(c, SEREN_GPU_ERR_STATE, "call seren_gpu_upload first");
+namespace seren {
+namespace {
+
+// Host buffers of seren_gpu_force_step_io (NULL ones are skipped)
+struct IoPlan {
+  double* parray;
+  double* v;
+  double* csq;
+  double* rho;
+  double* omega;
+  double* a;
+  double* gpot;
+  int32_t* perm;
+};
+
+int io_init(Ctx& c) {
+  if (c.st_io) return 0;
+  if (cudaStreamCreateWithFlags(&c.st_io, cudaStreamNonBlocking) != cudaSuccess) {
+    c.st_io = nullptr;
+    return -1;
+  }
+  for (auto& e : c.ev_io)
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return -1;
+  if (cudaMalloc(&c.stage_io, sizeof(double) * 6 * (size_t)c.pmax) != cudaSuccess) {
+    c.stage_io = nullptr;
+    return -1;
+  }
+  return 0;
+}
+
+// The device-resident force step.  With io, each result leaves on the copy
+// stream once the stage that makes it has run: v, c_s^2 and the permutation
+// after the tree build, parray (h), rho and omega after grad-h; a and gpot
+// follow gravity on the compute stream.
+int force_step_body(Ctx& c, int first_call, const IoPlan* io) {
   const int n = c.ptot;
+  const size_t N = (size_t)n;
   c.act = nullptr;
-  c.nlaunch = 0;
   cudaMemsetAsync(c.d_counts, 0, sizeof(int) * 32, c.st);
   cudaEventRecord(c.ev[0], c.st);
-  int rc = seren::build_tree(c);
+  int rc = build_tree(c);
   if (rc) return rc;
-  seren::launch_stock(c);
+  launch_stock(c);
   cudaEventRecord(c.ev[1], c.st);
-  if (first_call) seren::launch_hguess(c);
-  seren::launch_gradh(c, n);
+  if (io) {
+    cudaStreamWaitEvent(c.st_io, c.ev[1], 0);
+    if (io->v) {
+      k_pack_v<<<nb(n, 256), 256, 0, c.st_io>>>(c.stage_io, n, c.vel); ++c.nlaunch;
+      cudaMemcpyAsync(io->v, c.stage_io, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, c.st_io);
+    }
+    if (io->csq) cudaMemcpyAsync(io->csq, c.csq, sizeof(double) * N, cudaMemcpyDeviceToHost, c.st_io);
+    if (io->perm) cudaMemcpyAsync(io->perm, c.orig, sizeof(int) * N, cudaMemcpyDeviceToHost, c.st_io);
+  }
+  if (first_call) launch_hguess(c);
+  launch_gradh(c, n);
   cudaEventRecord(c.ev[2], c.st);
-  seren::launch_update_hmax(c);
-  seren::launch_neib(c, n);
+  if (io) {
+    cudaStreamWaitEvent(c.st_io, c.ev[2], 0);
+    if (io->parray) {
+      launch_pack_parray(c, c.stage_io, n, c.st_io);
+      cudaMemcpyAsync(io->parray, c.stage_io, sizeof(double) * 6 * N, cudaMemcpyDeviceToHost,
+                      c.st_io);
+    }
+    if (io->rho) cudaMemcpyAsync(io->rho, c.rho, sizeof(double) * N, cudaMemcpyDeviceToHost, c.st_io);
+    if (io->omega)
+      cudaMemcpyAsync(io->omega, c.omega, sizeof(double) * N, cudaMemcpyDeviceToHost, c.st_io);
+  }
+  launch_update_hmax(c);
+  launch_neib(c, n);
   cudaEventRecord(c.ev[3], c.st);
-  seren::launch_thermal(c);
-  seren::launch_hydro(c, n);
+  launch_thermal(c);
+  launch_hydro(c, n);
   cudaEventRecord(c.ev[4], c.st);
-  seren::launch_grav(c, n, c.nsink, c.nsink > 0 ? c.sinks : nullptr);
+  launch_grav(c, n, c.nsink, c.nsink > 0 ? c.sinks : nullptr);
   cudaEventRecord(c.ev[5], c.st);
+  if (io) {
+    if (io->a) cudaMemcpyAsync(io->a, c.acc, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, c.st);
+    if (io->gpot) cudaMemcpyAsync(io->gpot, c.gpot, sizeof(double) * N, cudaMemcpyDeviceToHost, c.st);
+  }
   rc = finish(c, "force_step");
   if (rc) return rc;
+  if (io) {
+    const cudaError_t e = cudaStreamSynchronize(c.st_io);
+    if (e != cudaSuccess) return cuda_fail(c, e, "force_step_io(copies)");
+  }
   c.step_launches = c.nlaunch;
   c.have_sph = true;
   for (int k = 0; k < 5; ++k) {
@@ -615,6 +678,61 @@ int seren_gpu_force_step(seren_gpu_ctx* h, int32_t first_call) {
   float tot = 0.f;
   cudaEventElapsedTime(&tot, c.ev[0], c.ev[5]);
   c.stage_ms[5] = tot;
+  return SEREN_GPU_OK;
+}
+
+}  // namespace
+}  // namespace seren
+
+int seren_gpu_force_step(seren_gpu_ctx* h, int32_t first_call) {
+  if (!h) return SEREN_GPU_ERR_ARG;
+  Ctx& c = h->c;
+  if (!c.have_v || !c.have_csq || c.ptot < 1)
+    return fail(c, SEREN_GPU_ERR_STATE, "call seren_gpu_upload first");
+  c.nlaunch = 0;
+  return seren::force_step_body(c, first_call, nullptr);
+}
+
+int seren_gpu_force_step_io(seren_gpu_ctx* h, int32_t ptot, const double* parray, const double* v,
+                            const double* csq, int32_t first_call, double* parray_out,
+                            double* v_out, double* csq_out, double* rho, double* omega, double* a,
+                            double* gpot, int32_t* perm_total) {
+  if (!h) return SEREN_GPU_ERR_ARG;
+  Ctx& c = h->c;
+  if (!parray || !v || !csq || ptot < 1) return fail(c, SEREN_GPU_ERR_ARG, "NULL array or ptot < 1");
+  if (ptot > c.pmax) return fail(c, SEREN_GPU_ERR_CAPACITY, "ptot > pmax");
+  if (seren::io_init(c)) {
+    cudaGetLastError();
+    return fail(c, SEREN_GPU_ERR_CUDA, "force_step_io: copy stream or staging buffer");
+  }
+  const size_t N = (size_t)ptot;
+  c.nlaunch = 0;
+  seren::reset_particles(c, ptot);
+  cudaEventRecord(c.ev_io[0], c.st);                       // velocities and c_s^2 cleared
+  cudaMemcpyAsync(c.stage, parray, sizeof(double) * 6 * N, cudaMemcpyHostToDevice, c.st);
+  seren::launch_unpack_parray(c, c.stage, ptot);
+  // velocities and c_s^2 come in on the copy stream while the tree is built;
+  // the particle reorder waits for them
+  cudaStreamWaitEvent(c.st_io, c.ev_io[0], 0);
+  cudaMemcpyAsync(c.stage_io, v, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, c.st_io);
+  seren::k_unpack_v<<<nb(ptot, 256), 256, 0, c.st_io>>>(c.stage_io, ptot, c.vel); ++c.nlaunch;
+  cudaMemcpyAsync(c.csq, csq, sizeof(double) * N, cudaMemcpyHostToDevice, c.st_io);
+  cudaEventRecord(c.ev_io[1], c.st_io);
+  c.reorder_wait = c.ev_io[1];
+  c.have_v = c.have_csq = true;
+  int rc = finish(c, "force_step_io(upload)");
+  if (rc == SEREN_GPU_OK) {
+    const seren::IoPlan io{parray_out, v_out, csq_out, rho, omega, a, gpot, perm_total};
+    rc = seren::force_step_body(c, first_call, &io);
+  }
+  if (rc != SEREN_GPU_OK) {                                // leave no copy in flight
+    cudaStreamSynchronize(c.st_io);
+    c.reorder_wait = nullptr;
+    c.have_v = c.have_csq = false;
+    return rc;
+  }
+  if (perm_total && c.prm.index_base)
+    for (size_t i = 0; i < N; ++i) perm_total[i] += c.prm.index_base;
   return SEREN_GPU_OK;
 }
 

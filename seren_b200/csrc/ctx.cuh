@@ -128,6 +128,14 @@ struct Ctx {
   bool have_v = false;
   bool have_csq = false;
 
+  // seren_gpu_force_step_io: a copy stream, its events and a staging buffer
+  // of 6*pmax doubles, made on first use; build_tree waits for reorder_wait
+  // (when set) before it reorders the particles
+  cudaStream_t st_io = nullptr;
+  cudaEvent_t ev_io[2] = {};
+  double* stage_io = nullptr;
+  cudaEvent_t reorder_wait = nullptr;
+
   // timing of the last force step
   cudaEvent_t ev[10] = {};
   double stage_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -138,7 +146,7 @@ struct Ctx {
 // tree.cu
 int build_tree(Ctx& c);               // bbox, keys, sort, cells, leaf order, reorder
 void launch_unpack_parray(Ctx& c, const double* stage, int n);
-void launch_pack_parray(Ctx& c, double* stage, int n);
+void launch_pack_parray(Ctx& c, double* stage, int n, cudaStream_t s = nullptr);
 void launch_stock(Ctx& c);            // BHgrav_stock + BHhydro_stock
 void launch_update_hmax(Ctx& c);      // BHhydro_update_hmax
 void launch_hguess(Ctx& c);           // BHhydro_hguess

@@ -625,8 +625,8 @@ void launch_unpack_parray(Ctx& c, const double* stage, int n) {
   k_unpack_parray<<<nb(n, 256), 256, 0, c.st>>>(stage, n, c.pm, c.hz, c.d_err); ++c.nlaunch;
 }
 
-void launch_pack_parray(Ctx& c, double* stage, int n) {
-  k_pack_parray<<<nb(n, 256), 256, 0, c.st>>>(stage, n, c.pm, c.hz); ++c.nlaunch;
+void launch_pack_parray(Ctx& c, double* stage, int n, cudaStream_t s) {
+  k_pack_parray<<<nb(n, 256), 256, 0, s ? s : c.st>>>(stage, n, c.pm, c.hz); ++c.nlaunch;
 }
 
 static int radix_sort(Ctx& c, int n) {
@@ -690,6 +690,10 @@ int build_tree(Ctx& c) {
     if (nbranch == 0) break;
   }
   k_leaf_order<<<nb(ctot + 1, 256), 256, 0, c.st>>>(c.leaf, c.pstart, ctot, c.idx); ++c.nlaunch;
+  if (c.reorder_wait) {                     // velocities and c_s^2 still being copied in
+    cudaStreamWaitEvent(c.st, c.reorder_wait, 0);
+    c.reorder_wait = nullptr;
+  }
   k_reorder<<<nb(n, 256), 256, 0, c.st>>>(c.idx, n, c.pm, c.hz, c.vel, c.csq, c.orig, c.pm_alt,
                                            c.hz_alt, c.vel_alt, c.csq_alt, c.orig_alt); ++c.nlaunch;
   std::swap(c.pm, c.pm_alt);

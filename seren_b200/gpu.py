@@ -33,6 +33,8 @@ def library(build_if_missing: bool = True) -> C.CDLL:
         vp = C.c_void_p
         for name, args in (("upload", [vp, C.c_int32, _dp, _dp, _dp]),
                            ("force_step", [vp, C.c_int32]),
+                           ("force_step_io", [vp, C.c_int32, _dp, _dp, _dp, C.c_int32, _dp, _dp,
+                                              _dp, _dp, _dp, _dp, _dp, _ip]),
                            ("drift", [vp, C.c_double]),
                            ("set_sinks", [vp, C.c_int32, _dp]),
                            ("download", [vp, _dp, _dp, _dp, _dp, _dp, _dp, _ip]),
@@ -64,6 +66,24 @@ class GpuHotPath(HotPath):
 
     def force_step(self, first_call=False):
         self._call("force_step", self._ctx, int(first_call))
+
+    def force_step_io(self, parray, v, csq, first_call=False):
+        """One force evaluation from host arrays to host arrays
+        (seren_gpu_force_step_io): returns parray, v, csq, rho, omega, a, gpot
+        and perm, in tree order."""
+        parray = np.ascontiguousarray(parray, dtype=np.float64)
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        csq = np.ascontiguousarray(csq, dtype=np.float64)
+        n = parray.shape[0]
+        out = dict(parray=np.zeros((n, 6)), v=np.zeros((n, 3)), csq=np.zeros(n), rho=np.zeros(n),
+                   omega=np.zeros(n), a=np.zeros((n, 3)), gpot=np.zeros(n),
+                   perm=np.zeros(n, dtype=np.int32))
+        self._call("force_step_io", self._ctx, n, _d(parray), _d(v), _d(csq), int(first_call),
+                   _d(out["parray"]), _d(out["v"]), _d(out["csq"]), _d(out["rho"]),
+                   _d(out["omega"]), _d(out["a"]), _d(out["gpot"]),
+                   out["perm"].ctypes.data_as(_ip))
+        self.ptot = n
+        return out
 
     def set_sinks(self, sinks):
         """Sinks ([nsink][5]: x, y, z, m, h) for the device-resident step."""

@@ -37,8 +37,9 @@ def test_oracle_mirrors_the_abi():
     lib = library()
     for n in declared():
         tail = n[len("seren_gpu_"):]
-        if tail in ("upload", "force_step", "drift", "download", "last_step_stats",
-                    "get_stream", "fma_peak", "hydro_forces_noalloc", "set_sinks"):
+        if tail in ("upload", "force_step", "force_step_io", "drift", "download",
+                    "last_step_stats", "get_stream", "fma_peak", "hydro_forces_noalloc",
+                    "set_sinks"):
             continue          # device-resident path, device-buffer call, GPU-only introspection
         assert hasattr(lib, "seren_oracle_" + tail), tail
 

@@ -212,6 +212,29 @@ def test_resident_step_matches_host_calls(libs):
     assert np.array_equal(st["gpot"], r["gpot"])
 
 
+def test_force_step_io_matches_resident_step(libs):
+    """seren_gpu_force_step_io (copies overlapped on a second stream) returns
+    what upload + force_step + download return, on two steps in a row (the
+    second from the first's tree-ordered outputs, written over its inputs)."""
+    ic = case("turb20k")
+    Oracle, Gpu = libs
+    n = ic["parray"].shape[0]
+    g1 = Gpu(n, params(ic))
+    g2 = Gpu(n, params(ic))
+    parray, v, csq = ic["parray"].copy(), ic["v"].copy(), ic["sound"] ** 2
+    for step in range(2):
+        g1.upload(parray, v, csq)
+        g1.force_step(first_call=step == 0)
+        ref = g1.download()
+        got = g2.force_step_io(parray, v, csq, first_call=step == 0)
+        for k in ("parray", "v", "rho", "omega", "a", "gpot", "perm"):
+            assert np.array_equal(got[k], ref[k]), (step, k)
+        assert np.array_equal(got["csq"], csq[got["perm"]])
+        assert g2.last_step_stats()[1] > g1.last_step_stats()[1]
+        parray, v, csq = got["parray"], got["v"], got["csq"]
+        parray[:, 0:3] += 1e-3 * v
+
+
 def test_resident_step_with_sink_matches_host_calls(libs):
     """seren_gpu_set_sinks puts the sink-gas term of grav_forces into the
     device-resident step."""
