@@ -272,6 +272,7 @@ struct GwRec {
   float flo[32];                   // wLo
   unsigned ftest[32];              // lanes that test the cell (0 for one-particle leaves)
   int fcell[32];
+  int fund[32];                    // popped cells the group test leaves undecided
 };
 
 __device__ __forceinline__ int warp_incl(int v, int lane) {
@@ -317,6 +318,18 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
     const float px32 = (float)(P.x - t.rootx), py32 = (float)(P.y - t.rooty),
                 pz32 = (float)(P.z - t.rootz);
     const float ux = (float)(P.x - rx), uy = (float)(P.y - ry), uz = (float)(P.z - rz);
+    // the group's bounding sphere in the walk's FP32 coordinates: centre lane
+    // 0, radius the farthest live lane's distance, rounded up
+    const float gx = __shfl_sync(FULLMASK, px32, 0), gy = __shfl_sync(FULLMASK, py32, 0),
+                gz = __shfl_sync(FULLMASK, pz32, 0);
+    float grad;
+    {
+      const float e0 = px32 - gx, e1 = py32 - gy, e2 = pz32 - gz;
+      float r2 = live ? fmaf(e2, e2, fmaf(e1, e1, e0 * e0)) : 0.0f;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) r2 = fmaxf(r2, __shfl_xor_sync(FULLMASK, r2, o));
+      grad = sqrtf(r2) * 1.00001f;
+    }
     const double invhp = 1.0 / HZ.x;
     const double zo_p = HZ.y;
     const float invhp32 = (float)invhp, zo32 = (float)zo_p;
@@ -437,6 +450,13 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
       gent += k;
       int cc = 0, cnt = 0, base = 0;     // cnt: leaf particles, or -children of a branch
       unsigned m = 0;
+      // group test of the popped cell: 1 when every lane's FP32 prefilter
+      // would pass it (d2s > hi: nearest possible lane beyond the bracket),
+      // 2 when none would reach the bracket (d2s < lo for the farthest
+      // possible lane, or a one-particle leaf, which has no MAC test), 0 when
+      // each lane tests it; margins of 1e-5 cover every FP32 rounding, so the
+      // decisions are the per-lane ones
+      int dec = 0;
       if (lane < k) {
         const int2 ent = S[sp + lane];
         cc = ent.x;
@@ -448,22 +468,36 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
         R.flo[lane] = nb2.x;
         R.ftest[lane] = cnt == 1 ? 0u : m;
         R.fcell[lane] = cc;
+        if (cnt == 1) {
+          dec = 2;
+        } else {
+          const float e0 = gx - na.x, e1 = gy - na.y, e2 = gz - na.z;
+          const float D = sqrtf(fmaf(e2, e2, fmaf(e1, e1, e0 * e0)));
+          const float dn = fmaf(D, 0.99999f, -grad);      // at most the nearest lane's distance
+          const float df = fmaf(D, 1.00001f, grad);       // at least the farthest lane's
+          if (dn > 0.0f && (dn * dn) * 0.99999f > na.w) dec = 1;
+          else if ((df * df) * 1.00001f < nb2.x) dec = 2;
+        }
       }
+      unsigned macc = dec == 1 ? m : 0u;
+      const unsigned und = __ballot_sync(FULLMASK, lane < k && dec == 0);
+      if (lane < k && dec == 0) R.fund[__popc(und & lt)] = lane;
       __syncwarp();
-      // each lane's MAC test on the popped cells, four at a time with their
+      // each lane's MAC test on the undecided cells, four at a time with their
       // loads issued first; a lane inside the FP32 bracket takes the exact
       // FP64 test (rare, a warp-uniform branch)
-      unsigned macc = 0;
-      for (int e0 = 0; e0 < k; e0 += 4) {
+      const int ku = __popc(und);
+      for (int e0 = 0; e0 < ku; e0 += 4) {
+        int ie[4];
         float4 wa[4];
         float lo[4];
         unsigned mt[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-          const int e = min(e0 + u, k - 1);
-          wa[u] = R.fw[e];
-          lo[u] = R.flo[e];
-          mt[u] = e0 + u < k ? R.ftest[e] : 0u;
+          ie[u] = R.fund[min(e0 + u, ku - 1)];
+          wa[u] = R.fw[ie[u]];
+          lo[u] = R.flo[ie[u]];
+          mt[u] = e0 + u < ku ? R.ftest[ie[u]] : 0u;
         }
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
@@ -476,14 +510,14 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
           if (__any_sync(FULLMASK, amb)) {                   // exact test, :146-155
             bool a2 = false;
             if (amb) {
-              const int ce = R.fcell[e0 + u];
+              const int ce = R.fcell[ie[u]];
               const double4 a = t.gA[ce];
               const double e0d = P.x - a.x, e1d = P.y - a.y, e2d = P.z - a.z;
               a2 = ((e0d * e0d + e1d * e1d) + e2d * e2d) > t.gC[ce].y;
             }
             b |= __ballot_sync(FULLMASK, a2);
           }
-          if (lane == e0 + u) macc = b;
+          if (e0 + u < ku && lane == ie[u]) macc = b;
         }
       }
       const unsigned mopn = m & ~macc;
