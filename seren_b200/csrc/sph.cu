@@ -218,15 +218,63 @@ struct GrShared {
   float fh[32];            // hrm32
   unsigned fm[32];         // lanes whose walk reaches the cell
   int fc[32];
+  int fu[32];              // popped cells the group test leaves undecided
 };
 
+// A group's bounding sphere in the walks' FP32 root-relative coordinates:
+// centre lane 0, radius the farthest live lane's distance (rounded up), and
+// the least and largest search radius over its live lanes.
+struct GrGroup {
+  float x, y, z, r, rmin, rmax;
+};
+
+__device__ __forceinline__ GrGroup gr_group(float px, float py, float pz, float R, bool live) {
+  GrGroup g;
+  g.x = __shfl_sync(0xffffffffu, px, 0);
+  g.y = __shfl_sync(0xffffffffu, py, 0);
+  g.z = __shfl_sync(0xffffffffu, pz, 0);
+  const float e0 = px - g.x, e1 = py - g.y, e2 = pz - g.z;
+  float r2 = live ? fmaf(e2, e2, fmaf(e1, e1, e0 * e0)) : 0.0f;
+  float lo = live ? R : 3.0e38f, hi = live ? R : 0.0f;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    r2 = fmaxf(r2, __shfl_xor_sync(0xffffffffu, r2, o));
+    lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+  g.r = sqrtf(r2) * 1.00001f;
+  g.rmin = lo;
+  g.rmax = hi;
+  return g;
+}
+
+// Group test of a popped cell (FP32 centre c.xyz, rmax c.w rounded up) for
+// searches where a lane passes when its distance is at most its radius + c.w:
+// 1 when the group's farthest possible point is within rlo + c.w (rlo: the
+// least radius of any lane), 2 when its nearest possible point is beyond
+// rhi + c.w (rhi: the largest), else 0.  The margin covers the FP32 rounding
+// of coordinates (delta each), radii and arithmetic, so a decision is the
+// exact FP64 one of every lane.
+__device__ __forceinline__ int gr_decide(const GrGroup& g, const float4& c, float rlo, float rhi,
+                                         float delta) {
+  const float e0 = c.x - g.x, e1 = c.y - g.y, e2 = c.z - g.z;
+  const float D = sqrtf(fmaf(e2, e2, fmaf(e1, e1, e0 * e0)));
+  const float mg = fmaf(1.0e-5f, D + g.r + rhi + c.w, 4.0f * delta);
+  if (D + g.r + mg < rlo + c.w) return 1;
+  if (D - g.r - mg > rhi + c.w) return 2;
+  return 0;
+}
+
 // Walk for the lanes in `lanes`, appending the opened leaves to R.code/R.mask
-// from nent on.  test(e) is this lane's test of popped cell e (R.fa[e],
-// R.fh[e], R.fc[e]).  Returns the new entry count, or -1 when the list or the
-// stack would overflow (nothing beyond the old count is then valid).
-template <class Test>
+// from nent on.  gtest(hA32, hrm32) is the group test of a popped cell (1: it
+// passes for every lane, 2: for none, 0: undecided); test(e) is this lane's
+// test of undecided popped cell e (R.fa[e], R.fh[e], R.fc[e]).  Returns the
+// new entry count, or -1 when the list or the stack would overflow (nothing
+// beyond the old count is then valid).
+template <class GTest, class Test>
 __device__ int gr_walk(const HydroTree& t, unsigned lanes, int2* S, int scap, GrShared& R,
-                       int lane, int nent, unsigned long long& nvisit, Test&& test) {
+                       int lane, int nent, unsigned long long& nvisit, GTest&& gtest,
+                       Test&& test) {
   const unsigned lt = (1u << lane) - 1u;
   __syncwarp();
   if (lane == 0) S[0] = make_int2(0, (int)lanes);
@@ -239,6 +287,7 @@ __device__ int gr_walk(const HydroTree& t, unsigned lanes, int2* S, int scap, Gr
     gent += k;
     int cnt = 0, base = 0;           // cnt: leaf particles, or -children of a branch
     unsigned m = 0;
+    int dec = 0;
     if (lane < k) {
       const int2 ent = S[sp + lane];
       const int cc = ent.x;
@@ -250,10 +299,14 @@ __device__ int gr_walk(const HydroTree& t, unsigned lanes, int2* S, int scap, Gr
       R.fh[lane] = nb2.x;
       R.fm[lane] = m;
       R.fc[lane] = cc;
+      dec = gtest(na, nb2.x);
     }
+    unsigned mpass = dec == 1 ? m : 0u;
+    const unsigned und = __ballot_sync(FULL, lane < k && dec == 0);
+    if (lane < k && dec == 0) R.fu[__popc(und & lt)] = lane;
     __syncwarp();
-    unsigned mpass = 0;
-    for (int e = 0; e < k; ++e) {
+    for (unsigned u = und; u != 0u; u &= u - 1u) {         // the undecided cells, lane by lane
+      const int e = __ffs(u) - 1;
       const bool pass = ((R.fm[e] >> lane) & 1u) && test(e);
       const unsigned b = __ballot_sync(FULL, pass);
       if (lane == e) mpass = b;
@@ -363,7 +416,10 @@ __global__ void __launch_bounds__(GR_THREADS) k_gradh_walk(
     const float R32 = (float)Rw;
     const unsigned lanes = __ballot_sync(FULL, live);
     nwalk += live ? 1u : 0u;
-    const int nent = gr_walk(t, lanes, S, scap, R, lane, 0, nvisit, [&](int e) {
+    const GrGroup grp = gr_group(px, py, pz, R32, live);
+    const int nent = gr_walk(t, lanes, S, scap, R, lane, 0, nvisit, [&](const float4& c, float) {
+      return gr_decide(grp, c, grp.rmin, grp.rmax, t.delta);
+    }, [&](int e) {
       const float4 h32 = R.fa[e];                      // BHhydrowalk_hgather.F90:36-40
       const float d0 = h32.x - px, d1 = h32.y - py, d2 = h32.z - pz;
       const int r = test32((d0 * d0 + d1 * d1) + d2 * d2, R32 + h32.w, t.delta);
@@ -1145,7 +1201,12 @@ __global__ void __launch_bounds__(GR_THREADS) k_neib_walk(
     const double Rw = KERNRANGE * hz[p].x;
     const float R32 = (float)Rw;
     const unsigned lanes = __ballot_sync(FULL, live);
-    const int nent = gr_walk(t, lanes, S, scap, R, lane, 0, nvisit, [&](int e) {
+    const GrGroup grp = gr_group(px, py, pz, R32, live);
+    const int nent = gr_walk(t, lanes, S, scap, R, lane, 0, nvisit, [&](const float4& c, float fh) {
+      // gather or scatter (BHhydro_walk.F90:37-43): a lane passes within
+      // max(its 2h, hrangemax) + rmax
+      return gr_decide(grp, c, fmaxf(grp.rmin, fh), fmaxf(grp.rmax, fh), t.delta);
+    }, [&](int e) {
       const float4 h32 = R.fa[e];
       const float d0 = h32.x - px, d1 = h32.y - py, d2 = h32.z - pz;
       const float d2s = (d0 * d0 + d1 * d1) + d2 * d2;
