@@ -598,6 +598,18 @@ struct IoPlan {
   int32_t* perm;
 };
 
+// the device address of a host buffer that is page-locked and mapped (as
+// pinned allocations are under unified addressing), else nullptr
+double* mapped_host(double* p) {
+  if (!p) return nullptr;
+  cudaPointerAttributes at{};
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return at.type == cudaMemoryTypeHost ? static_cast<double*>(at.devicePointer) : nullptr;
+}
+
 int io_init(Ctx& c) {
   if (c.st_io) return 0;
   if (cudaStreamCreateWithFlags(&c.st_io, cudaStreamNonBlocking) != cudaSuccess) {
@@ -626,6 +638,7 @@ int force_step_body(Ctx& c, int first_call, const IoPlan* io) {
   int rc = build_tree(c);
   if (rc) return rc;
   launch_stock(c);
+  finish_reorder(c);
   cudaEventRecord(c.ev[1], c.st);
   if (io) {
     cudaStreamWaitEvent(c.st_io, c.ev[1], 0);
@@ -656,11 +669,17 @@ int force_step_body(Ctx& c, int first_call, const IoPlan* io) {
   launch_thermal(c);
   launch_hydro(c, n);
   cudaEventRecord(c.ev[4], c.st);
-  launch_grav(c, n, c.nsink, c.nsink > 0 ? c.sinks : nullptr);
+  // a and gpot go straight to mapped (pinned) host buffers from the gravity
+  // kernel, else they are copied after it
+  double* amap = io ? mapped_host(io->a) : nullptr;
+  double* gmap = io ? mapped_host(io->gpot) : nullptr;
+  launch_grav(c, n, c.nsink, c.nsink > 0 ? c.sinks : nullptr, amap, gmap);
   cudaEventRecord(c.ev[5], c.st);
   if (io) {
-    if (io->a) cudaMemcpyAsync(io->a, c.acc, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, c.st);
-    if (io->gpot) cudaMemcpyAsync(io->gpot, c.gpot, sizeof(double) * N, cudaMemcpyDeviceToHost, c.st);
+    if (io->a && !amap)
+      cudaMemcpyAsync(io->a, c.acc, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, c.st);
+    if (io->gpot && !gmap)
+      cudaMemcpyAsync(io->gpot, c.gpot, sizeof(double) * N, cudaMemcpyDeviceToHost, c.st);
   }
   rc = finish(c, "force_step");
   if (rc) return rc;
@@ -728,6 +747,7 @@ int seren_gpu_force_step_io(seren_gpu_ctx* h, int32_t ptot, const double* parray
   if (rc != SEREN_GPU_OK) {                                // leave no copy in flight
     cudaStreamSynchronize(c.st_io);
     c.reorder_wait = nullptr;
+    c.reorder_late = false;
     c.have_v = c.have_csq = false;
     return rc;
   }

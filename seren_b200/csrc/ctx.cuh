@@ -135,6 +135,7 @@ struct Ctx {
   cudaEvent_t ev_io[2] = {};
   double* stage_io = nullptr;
   cudaEvent_t reorder_wait = nullptr;
+  bool reorder_late = false;    // v and c_s^2 still to reorder (finish_reorder)
 
   // timing of the last force step
   cudaEvent_t ev[10] = {};
@@ -145,6 +146,7 @@ struct Ctx {
 
 // tree.cu
 int build_tree(Ctx& c);               // bbox, keys, sort, cells, leaf order, reorder
+void finish_reorder(Ctx& c);          // the deferred v, c_s^2 reorder (reorder_wait set)
 void launch_unpack_parray(Ctx& c, const double* stage, int n);
 void launch_pack_parray(Ctx& c, double* stage, int n, cudaStream_t s = nullptr);
 void launch_stock(Ctx& c);            // BHgrav_stock + BHhydro_stock
@@ -162,7 +164,10 @@ int hydro_walk_slots(const Ctx& c);     // resident warps of the grad-h / neighb
 int wide_scratch_alloc(Ctx& c);         // c.wst, c.wacc; 0 or -1
 
 // gravity.cu
-void launch_grav(Ctx& c, int nact, int nsink, const double* d_sinks);
+// amap/gmap (optional): host buffers mapped into the device address space
+// that receive a and gpot of each particle as soon as its group is done
+void launch_grav(Ctx& c, int nact, int nsink, const double* d_sinks, double* amap = nullptr,
+                 double* gmap = nullptr);
 void launch_sink_walk(Ctx& c, int nsink, const double* d_sinks, double* d_out /*[nsink][4]*/);
 int grav_walk_slots(const Ctx& c);      // resident warps of the gravity walk grid
 int grav_walk_stack_cap(const Ctx& c);  // stack entries per warp

@@ -289,7 +289,8 @@ __global__ void __launch_bounds__(GW_THREADS, MIXED ? 5 : 4)
 k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ pm,
             const double2* __restrict__ hz, GravWalk t, const double4* __restrict__ tabG,
             const float4* __restrict__ tab32, double* __restrict__ acc,
-            double* __restrict__ gpot, int nsink, const double* __restrict__ sinks,
+            double* __restrict__ gpot, double* __restrict__ amap, double* __restrict__ gmap,
+            int nsink, const double* __restrict__ sinks,
             int2* __restrict__ stacks, int* work, DevError* err, unsigned long long* counts) {
   using Cfg = GwTypes<MIXED>;
   constexpr int CAP = Cfg::CAP;
@@ -581,6 +582,14 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
         pot = pot + sp2;
       }
       gpot[p] = pot;
+      // host buffers mapped into the device address space: the results
+      // cross PCIe while the other groups still compute
+      if (amap) {
+        amap[(size_t)p * 3] = a[0];
+        amap[(size_t)p * 3 + 1] = a[1];
+        amap[(size_t)p * 3 + 2] = a[2];
+      }
+      if (gmap) gmap[p] = pot;
     }
   }
   count_add(counts, ncell, npair);
@@ -685,7 +694,8 @@ int grav_walk_slots(const Ctx& c) {
 
 int grav_walk_stack_cap(const Ctx& c) { return std::min(GW_STACK, c.cmax + 1); }
 
-void launch_grav(Ctx& c, int nact, int nsink, const double* d_sinks) {
+void launch_grav(Ctx& c, int nact, int nsink, const double* d_sinks, double* amap,
+                 double* gmap) {
   if (nact <= 0) return;
   unsigned long long* counts = reinterpret_cast<unsigned long long*>(c.d_counts);
   const GravWalk gw{c.wA, c.gA, c.gB, c.gC, c.info.ctot, c.wstack_cap,
@@ -696,10 +706,10 @@ void launch_grav(Ctx& c, int nact, int nsink, const double* d_sinks) {
   cudaMemsetAsync(c.work, 0, sizeof(int), c.st);
   if (!mixed)
     k_grav_walk<false><<<blocks, GW_THREADS, 0, c.st>>>(nact, c.act, c.pm, c.hz, gw, c.tabG,
-        c.tabG32, c.acc, c.gpot, nsink, d_sinks, c.wstack, c.work, c.d_err, counts);
+        c.tabG32, c.acc, c.gpot, amap, gmap, nsink, d_sinks, c.wstack, c.work, c.d_err, counts);
   else
     k_grav_walk<true><<<blocks, GW_THREADS, 0, c.st>>>(nact, c.act, c.pm, c.hz, gw, c.tabG,
-        c.tabG32, c.acc, c.gpot, nsink, d_sinks, c.wstack, c.work, c.d_err, counts);
+        c.tabG32, c.acc, c.gpot, amap, gmap, nsink, d_sinks, c.wstack, c.work, c.d_err, counts);
   ++c.nlaunch;
 }
 

@@ -371,6 +371,29 @@ __global__ void k_reorder(const int* __restrict__ perm, int n, const double4* __
   orig2[i] = orig[p];
 }
 
+// the reorder without v and c_s^2 (still being copied in: finish_reorder)
+__global__ void k_reorder_pos(const int* __restrict__ perm, int n, const double4* __restrict__ pm,
+                              const double2* __restrict__ hz, const int* __restrict__ orig,
+                              double4* __restrict__ pm2, double2* __restrict__ hz2,
+                              int* __restrict__ orig2) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int p = perm[i];
+  pm2[i] = pm[p];
+  hz2[i] = hz[p];
+  orig2[i] = orig[p];
+}
+
+__global__ void k_reorder_vc(const int* __restrict__ perm, int n, const double4* __restrict__ vel,
+                             const double* __restrict__ csq, double4* __restrict__ vel2,
+                             double* __restrict__ csq2) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int p = perm[i];
+  vel2[i] = vel[p];
+  csq2[i] = csq[p];
+}
+
 __global__ void k_pack_link(int ctot, const int* __restrict__ leaf, const int* __restrict__ nextcell,
                             const int* __restrict__ ifopen, const int* __restrict__ pstart,
                             int4* __restrict__ link) {
@@ -621,6 +644,17 @@ void scan_exclusive(Ctx& c, const int* in, int* out, int n) {
   scan_rec(c, in, out, n, 0);
 }
 
+void finish_reorder(Ctx& c) {
+  if (!c.reorder_late) return;
+  cudaStreamWaitEvent(c.st, c.reorder_wait, 0);
+  k_reorder_vc<<<nb(c.ptot, 256), 256, 0, c.st>>>(c.idx, c.ptot, c.vel, c.csq, c.vel_alt,
+                                                   c.csq_alt); ++c.nlaunch;
+  std::swap(c.vel, c.vel_alt);
+  std::swap(c.csq, c.csq_alt);
+  c.reorder_late = false;
+  c.reorder_wait = nullptr;
+}
+
 void launch_unpack_parray(Ctx& c, const double* stage, int n) {
   k_unpack_parray<<<nb(n, 256), 256, 0, c.st>>>(stage, n, c.pm, c.hz, c.d_err); ++c.nlaunch;
 }
@@ -691,15 +725,17 @@ int build_tree(Ctx& c) {
   }
   k_leaf_order<<<nb(ctot + 1, 256), 256, 0, c.st>>>(c.leaf, c.pstart, ctot, c.idx); ++c.nlaunch;
   if (c.reorder_wait) {                     // velocities and c_s^2 still being copied in
-    cudaStreamWaitEvent(c.st, c.reorder_wait, 0);
-    c.reorder_wait = nullptr;
+    k_reorder_pos<<<nb(n, 256), 256, 0, c.st>>>(c.idx, n, c.pm, c.hz, c.orig, c.pm_alt, c.hz_alt,
+                                                 c.orig_alt); ++c.nlaunch;
+    c.reorder_late = true;
+  } else {
+    k_reorder<<<nb(n, 256), 256, 0, c.st>>>(c.idx, n, c.pm, c.hz, c.vel, c.csq, c.orig, c.pm_alt,
+                                             c.hz_alt, c.vel_alt, c.csq_alt, c.orig_alt); ++c.nlaunch;
+    std::swap(c.vel, c.vel_alt);
+    std::swap(c.csq, c.csq_alt);
   }
-  k_reorder<<<nb(n, 256), 256, 0, c.st>>>(c.idx, n, c.pm, c.hz, c.vel, c.csq, c.orig, c.pm_alt,
-                                           c.hz_alt, c.vel_alt, c.csq_alt, c.orig_alt); ++c.nlaunch;
   std::swap(c.pm, c.pm_alt);
   std::swap(c.hz, c.hz_alt);
-  std::swap(c.vel, c.vel_alt);
-  std::swap(c.csq, c.csq_alt);
   std::swap(c.orig, c.orig_alt);
   k_pack_link<<<nb(ctot + 1, 256), 256, 0, c.st>>>(ctot, c.leaf, c.nextcell, c.ifopen, c.pstart,
                                                    c.link); ++c.nlaunch;

@@ -235,6 +235,44 @@ def test_force_step_io_matches_resident_step(libs):
         parray[:, 0:3] += 1e-3 * v
 
 
+def test_force_step_io_pinned_buffers(libs):
+    """With page-locked host buffers seren_gpu_force_step_io writes a and gpot
+    from the gravity kernel straight into them (mapped) and defers the v, c_s^2
+    reorder; the results equal the resident step's."""
+    import ctypes as C
+
+    import torch
+    ic = case("turb20k")
+    Oracle, Gpu = libs
+    n = ic["parray"].shape[0]
+    g1 = Gpu(n, params(ic))
+    g2 = Gpu(n, params(ic))
+    g1.upload(ic["parray"], ic["v"], ic["sound"] ** 2)
+    g1.force_step(first_call=True)
+    ref = g1.download()
+
+    def pinned(a, dtype=torch.float64):
+        t = torch.empty(a.shape, dtype=dtype, pin_memory=True)
+        t.copy_(torch.from_numpy(np.ascontiguousarray(a)))
+        return t
+
+    dp, ip = C.POINTER(C.c_double), C.POINTER(C.c_int32)
+    P = lambda t: C.cast(t.data_ptr(), dp)  # noqa: E731
+    parray, v, csq = pinned(ic["parray"]), pinned(ic["v"]), pinned(ic["sound"] ** 2)
+    out = {k: pinned(np.zeros(shape)) for k, shape in
+           (("rho", (n,)), ("omega", (n,)), ("a", (n, 3)), ("gpot", (n,)))}
+    perm = pinned(np.zeros(n, dtype=np.int32), torch.int32)
+    g2._call("force_step_io", g2._ctx, n, P(parray), P(v), P(csq), 1, P(parray), P(v), P(csq),
+             P(out["rho"]), P(out["omega"]), P(out["a"]), P(out["gpot"]),
+             C.cast(perm.data_ptr(), ip))
+    assert np.array_equal(perm.numpy(), ref["perm"])
+    assert np.array_equal(parray.numpy(), ref["parray"])
+    assert np.array_equal(v.numpy(), ref["v"])
+    for k in ("rho", "omega", "a", "gpot"):
+        assert np.array_equal(out[k].numpy(), ref[k]), k
+    assert np.array_equal(csq.numpy(), (ic["sound"] ** 2)[ref["perm"]])
+
+
 def test_resident_step_with_sink_matches_host_calls(libs):
     """seren_gpu_set_sinks puts the sink-gas term of grav_forces into the
     device-resident step."""
