@@ -288,9 +288,9 @@ def run_e2e_io(ic, precision, steps, warmup, ws):
     torch.cuda.synchronize()
     barrier(ws)
     total_ms = start.elapsed_time(end)
-    stage = g.last_step_stats()[0][5]
+    stages = g.last_step_stats()[0][:6]
     log(f"[bench] e2e (force_step_io) ms/step: call {1e3 * host_s[0] / steps:.1f} "
-        f"(device step {stage:.1f}), host drift {1e3 * host_s[1] / steps:.1f}")
+        f"(device stages {[round(x, 2) for x in stages]}), host drift {1e3 * host_s[1] / steps:.1f}")
     h2d = n * (48 + 24 + 8)                          # parray, v, c_s^2
     d2h = n * (48 + 24 + 8 + 8 + 8 + 24 + 8 + 4)     # parray, v, c_s^2, rho, omega, a, gpot, perm
     g.close()

@@ -638,22 +638,22 @@ int force_step_body(Ctx& c, int first_call, const IoPlan* io) {
   int rc = build_tree(c);
   if (rc) return rc;
   launch_stock(c);
-  finish_reorder(c);
   cudaEventRecord(c.ev[1], c.st);
-  if (io) {
+  if (io && io->perm) {
     cudaStreamWaitEvent(c.st_io, c.ev[1], 0);
+    cudaMemcpyAsync(io->perm, c.orig, sizeof(int) * N, cudaMemcpyDeviceToHost, c.st_io);
+  }
+  if (first_call) launch_hguess(c);
+  launch_gradh(c, n);                         // runs finish_reorder before its passes
+  finish_reorder(c);
+  cudaEventRecord(c.ev[2], c.st);
+  if (io) {
+    cudaStreamWaitEvent(c.st_io, c.ev[2], 0);
     if (io->v) {
       k_pack_v<<<nb(n, 256), 256, 0, c.st_io>>>(c.stage_io, n, c.vel); ++c.nlaunch;
       cudaMemcpyAsync(io->v, c.stage_io, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, c.st_io);
     }
     if (io->csq) cudaMemcpyAsync(io->csq, c.csq, sizeof(double) * N, cudaMemcpyDeviceToHost, c.st_io);
-    if (io->perm) cudaMemcpyAsync(io->perm, c.orig, sizeof(int) * N, cudaMemcpyDeviceToHost, c.st_io);
-  }
-  if (first_call) launch_hguess(c);
-  launch_gradh(c, n);
-  cudaEventRecord(c.ev[2], c.st);
-  if (io) {
-    cudaStreamWaitEvent(c.st_io, c.ev[2], 0);
     if (io->parray) {
       launch_pack_parray(c, c.stage_io, n, c.st_io);
       cudaMemcpyAsync(io->parray, c.stage_io, sizeof(double) * 6 * N, cudaMemcpyDeviceToHost,
@@ -727,11 +727,11 @@ int seren_gpu_force_step_io(seren_gpu_ctx* h, int32_t ptot, const double* parray
   const size_t N = (size_t)ptot;
   c.nlaunch = 0;
   seren::reset_particles(c, ptot);
-  cudaEventRecord(c.ev_io[0], c.st);                       // velocities and c_s^2 cleared
   cudaMemcpyAsync(c.stage, parray, sizeof(double) * 6 * N, cudaMemcpyHostToDevice, c.st);
   seren::launch_unpack_parray(c, c.stage, ptot);
+  cudaEventRecord(c.ev_io[0], c.st);         // v, c_s^2 cleared; parray in (the link is free)
   // velocities and c_s^2 come in on the copy stream while the tree is built;
-  // the particle reorder waits for them
+  // their reorder waits for them after the stock
   cudaStreamWaitEvent(c.st_io, c.ev_io[0], 0);
   cudaMemcpyAsync(c.stage_io, v, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, c.st_io);
   seren::k_unpack_v<<<nb(ptot, 256), 256, 0, c.st_io>>>(c.stage_io, ptot, c.vel); ++c.nlaunch;

@@ -1566,6 +1566,7 @@ void launch_gradh(Ctx& c, int nact) {
   k_gradh_walk<<<gr_grid(c, nact, 0), GR_THREADS, GR_SMEM, c.st>>>(
       nact, c.act, c.pm, c.hz, t, c.leaves, c.nleaf, c.npot, c.wstack, c.wstack_cap, counts,
       c.work);
+  finish_reorder(c);            // velocities still arriving: the passes need them from here on
   static int occ[16] = {};
   int& o = occ[c.dev >= 0 && c.dev < 16 ? c.dev : 0];
   if (o == 0) {
