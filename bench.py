@@ -12,7 +12,7 @@ FP64 path is timed on the same state for the speed-up and accuracy figures.
 `e2e` is the same metric from pinned host buffers to pinned host buffers
 through seren_gpu_force_step_io (inputs copied in and every result copied
 back each step, the copies overlapped with the force step on a second
-stream); `e2e_reference_calls` is the same through the host-buffer calls a
+stream; the host's drift between calls is not timed); `e2e_reference_calls` is the same through the host-buffer calls a
 Fortran caller of the reference's interface makes (tree_update -> sph_update
 -> thermal on the host -> hydro_forces -> grav_forces), copies included.
 
@@ -237,10 +237,11 @@ def run_resident(ic, precision, steps, warmup, ws):
 
 def run_e2e_io(ic, precision, steps, warmup, ws):
     """Steps through seren_gpu_force_step_io with pinned host buffers: each
-    step copies parray, v and c_s^2 in from the host and parray, v, c_s^2,
+    call copies parray, v and c_s^2 in from the host and parray, v, c_s^2,
     rho, omega, a, gpot and the permutation (tree order) back over them; the
-    host then drifts its positions (torch CPU ops, all cores), so every step
-    starts from the host's arrays."""
+    host then drifts its positions (torch CPU ops, all cores, not timed), so
+    every call starts from the host's arrays.  The time is the sum over the
+    timed calls of CUDA events recorded around each call."""
     import ctypes as C
 
     import torch
@@ -265,32 +266,39 @@ def run_e2e_io(ic, precision, steps, warmup, ws):
     ctx = g._ctx
     host_s = np.zeros(2)
 
-    def step(first):
+    stream = torch.cuda.ExternalStream(g.stream())
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(max(steps, 1))]
+
+    def step(first, k=None):
+        # the call is timed with events on the library's stream around it (it
+        # returns with every copy done); the host's drift between calls is not
         t0 = time.perf_counter()
+        if k is not None:
+            ev[k][0].record(stream)
         g._call("force_step_io", ctx, n, P(parray), P(v), P(csq), int(first), P(parray), P(v),
                 P(csq), P(rho), P(omega), P(a), P(gpot), C.cast(perm.data_ptr(), ip))
+        if k is not None:
+            ev[k][1].record(stream)
         t1 = time.perf_counter()
         parray[:, 0:3].add_(v, alpha=DT)
         t2 = time.perf_counter()
         host_s[:] += np.diff([t0, t1, t2])
 
-    stream = torch.cuda.ExternalStream(g.stream())
     for w in range(max(warmup, 1)):
         step(w == 0)
-    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     barrier(ws)
-    start.record(stream)
     host_s[:] = 0.0
-    for _ in range(steps):
-        step(False)
-    end.record(stream)
+    for k in range(steps):
+        step(False, k)
     torch.cuda.synchronize()
     barrier(ws)
-    total_ms = start.elapsed_time(end)
+    total_ms = sum(e0.elapsed_time(e1) for e0, e1 in ev[:steps])
     stages = g.last_step_stats()[0][:6]
-    log(f"[bench] e2e (force_step_io) ms/step: call {1e3 * host_s[0] / steps:.1f} "
-        f"(device stages {[round(x, 2) for x in stages]}), host drift {1e3 * host_s[1] / steps:.1f}")
+    log(f"[bench] e2e (force_step_io) ms/step: call {total_ms / steps:.1f} by events, "
+        f"{1e3 * host_s[0] / steps:.1f} by host clock (device stages "
+        f"{[round(x, 2) for x in stages]}); host drift between calls {1e3 * host_s[1] / steps:.1f}")
     h2d = n * (48 + 24 + 8)                          # parray, v, c_s^2
     d2h = n * (48 + 24 + 8 + 8 + 8 + 24 + 8 + 4)     # parray, v, c_s^2, rho, omega, a, gpot, perm
     g.close()

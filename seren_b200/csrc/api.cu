@@ -282,6 +282,33 @@ void reset_particles(Ctx& c, int ptot) {
   cudaMemsetAsync(c.pptot, 0, sizeof(int) * ptot, c.st);
 }
 
+// the device address of a host buffer that is page-locked and mapped (as
+// pinned allocations are under unified addressing), else nullptr
+double* mapped_host(double* p) {
+  if (!p) return nullptr;
+  cudaPointerAttributes at{};
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return at.type == cudaMemoryTypeHost ? static_cast<double*>(at.devicePointer) : nullptr;
+}
+
+int io_init(Ctx& c) {
+  if (c.st_io) return 0;
+  if (cudaStreamCreateWithFlags(&c.st_io, cudaStreamNonBlocking) != cudaSuccess) {
+    c.st_io = nullptr;
+    return -1;
+  }
+  for (auto& e : c.ev_io)
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return -1;
+  if (cudaMalloc(&c.stage_io, sizeof(double) * 6 * (size_t)c.pmax) != cudaSuccess) {
+    c.stage_io = nullptr;
+    return -1;
+  }
+  return 0;
+}
+
 }  // namespace
 }  // namespace seren
 
@@ -388,26 +415,64 @@ int seren_gpu_sph_update(seren_gpu_ctx* h, int32_t ptot, const int32_t* acclist,
   int rc = seren::check_tree(c, ptot);
   if (rc) return rc;
   if (!v) return fail(c, SEREN_GPU_ERR_ARG, "v is NULL");
-  cudaMemcpyAsync(c.stage, v, sizeof(double) * 3 * (size_t)ptot, cudaMemcpyHostToDevice, c.st);
-  seren::k_unpack_v<<<nb(ptot, 256), 256, 0, c.st>>>(c.stage, ptot, c.vel); ++c.nlaunch;
+  const size_t N = (size_t)ptot;
+  // every particle active: v comes in on the copy stream while the grad-h
+  // walk runs (its passes wait for it), and the results of grad-h go back on
+  // it while the neighbour lists are built
+  const bool overlap = acclist == nullptr && seren::io_init(c) == 0;
+  cudaGetLastError();
+  if (overlap) {
+    cudaEventRecord(c.ev_io[0], c.st);
+    cudaStreamWaitEvent(c.st_io, c.ev_io[0], 0);
+    cudaMemcpyAsync(c.stage_io, v, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, c.st_io);
+    seren::k_unpack_v<<<nb(ptot, 256), 256, 0, c.st_io>>>(c.stage_io, ptot, c.vel); ++c.nlaunch;
+    cudaEventRecord(c.ev_io[1], c.st_io);
+    c.vel_wait = c.ev_io[1];
+  } else {
+    cudaMemcpyAsync(c.stage, v, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, c.st);
+    seren::k_unpack_v<<<nb(ptot, 256), 256, 0, c.st>>>(c.stage, ptot, c.vel); ++c.nlaunch;
+  }
   c.have_v = true;
+  auto drain = [&](int code) {                // no copy left in flight on an error
+    if (overlap) cudaStreamSynchronize(c.st_io);
+    c.vel_wait = nullptr;
+    return code;
+  };
   int nact = 0;
   rc = seren::set_active(c, acclist, nacc, nact);
-  if (rc) return rc;
+  if (rc) return drain(rc);
   if (first_call) seren::launch_hguess(c);
   seren::launch_gradh(c, nact);
+  seren::finish_reorder(c);
+  if (overlap) {
+    cudaEventRecord(c.ev_io[2], c.st);
+    cudaStreamWaitEvent(c.st_io, c.ev_io[2], 0);
+    if (parray) {
+      // every row changes: copy whole rows (positions and masses are the ones
+      // uploaded by the last tree_update) instead of scattering two columns
+      seren::launch_pack_parray(c, c.stage_io, ptot, c.st_io);
+      cudaMemcpyAsync(parray, c.stage_io, sizeof(double) * 6 * N, cudaMemcpyDeviceToHost, c.st_io);
+    }
+    if (rho) cudaMemcpyAsync(rho, c.rho, sizeof(double) * N, cudaMemcpyDeviceToHost, c.st_io);
+    if (omega) cudaMemcpyAsync(omega, c.omega, sizeof(double) * N, cudaMemcpyDeviceToHost, c.st_io);
+    if (div_v) cudaMemcpyAsync(div_v, c.div_v, sizeof(double) * N, cudaMemcpyDeviceToHost, c.st_io);
+    if (drhodt)
+      cudaMemcpyAsync(drhodt, c.drhodt, sizeof(double) * N, cudaMemcpyDeviceToHost, c.st_io);
+  }
   seren::launch_update_hmax(c);
   seren::launch_neib(c, nact);
   rc = finish(c, "sph_update");
-  if (rc) return rc;
+  if (rc) return drain(rc);
+  if (overlap) {
+    const cudaError_t e = cudaStreamSynchronize(c.st_io);
+    if (e != cudaSuccess) return seren::cuda_fail(c, e, "sph_update(copies)");
+  }
   c.have_sph = true;
-  // results back to the host arrays
-  if (parray && acclist == nullptr) {
-    // every row changes: copy whole rows (positions and masses are the ones
-    // uploaded by the last tree_update) instead of scattering two columns
+  // results back to the host arrays (the overlapped path has sent them)
+  if (overlap) {
+  } else if (parray && acclist == nullptr) {
     seren::launch_pack_parray(c, c.stage, ptot);
-    cudaMemcpyAsync(parray, c.stage, sizeof(double) * 6 * (size_t)ptot, cudaMemcpyDeviceToHost,
-                    c.st);
+    cudaMemcpyAsync(parray, c.stage, sizeof(double) * 6 * N, cudaMemcpyDeviceToHost, c.st);
   } else if (parray) {
     double* pin = seren::pinned(c, (size_t)2 * ptot);
     if (!pin) return fail(c, SEREN_GPU_ERR_CUDA, "pinned staging allocation failed");
@@ -425,10 +490,12 @@ int seren_gpu_sph_update(seren_gpu_ctx* h, int32_t ptot, const int32_t* acclist,
       parray[p * 6 + 5] = pin[p * 2 + 1];
     }
   }
-  if (rho && (rc = seren::d2h_rows(c, rho, c.rho, 1, acclist, nact))) return rc;
-  if (omega && (rc = seren::d2h_rows(c, omega, c.omega, 1, acclist, nact))) return rc;
-  if (div_v && (rc = seren::d2h_rows(c, div_v, c.div_v, 1, acclist, nact))) return rc;
-  if (drhodt && (rc = seren::d2h_rows(c, drhodt, c.drhodt, 1, acclist, nact))) return rc;
+  if (!overlap) {
+    if (rho && (rc = seren::d2h_rows(c, rho, c.rho, 1, acclist, nact))) return rc;
+    if (omega && (rc = seren::d2h_rows(c, omega, c.omega, 1, acclist, nact))) return rc;
+    if (div_v && (rc = seren::d2h_rows(c, div_v, c.div_v, 1, acclist, nact))) return rc;
+    if (drhodt && (rc = seren::d2h_rows(c, drhodt, c.drhodt, 1, acclist, nact))) return rc;
+  }
   if (pptot || pplist) {
     const int L = c.prm.pp_limit;
     std::vector<int> tot(ptot);
@@ -511,9 +578,11 @@ int seren_gpu_hydro_forces(seren_gpu_ctx* h, const int32_t* acclist, int32_t nac
   int nact = 0;
   int rc = seren::set_active(c, acclist, nacc, nact);
   if (rc) return rc;
-  seren::launch_hydro(c, nact);
+  // every particle active and a page-locked: the kernel writes a straight to it
+  double* amap = acclist == nullptr ? seren::mapped_host(a) : nullptr;
+  seren::launch_hydro(c, nact, amap);
   rc = finish(c, "hydro_forces");
-  if (rc) return rc;
+  if (rc || amap) return rc;
   if ((rc = seren::d2h_rows(c, a, c.acc, 3, acclist, nact))) return rc;
   return finish(c, "hydro_forces(copy back)");
 }
@@ -527,7 +596,13 @@ int seren_gpu_grav_forces(seren_gpu_ctx* h, const int32_t* acclist, int32_t nacc
     return fail(c, SEREN_GPU_ERR_ARG, "bad arguments");
   if (nsink > 1024) return fail(c, SEREN_GPU_ERR_ARG, "nsink > 1024");
   const int ptot = c.ptot;
-  cudaMemcpyAsync(c.acc, a, sizeof(double) * 3 * (size_t)ptot, cudaMemcpyHostToDevice, c.st);
+  // every particle active and a, gpot page-locked: the kernel reads the
+  // acceleration to add to from a and writes a and gpot straight back
+  double* amap = acclist == nullptr ? seren::mapped_host(a) : nullptr;
+  double* gmap = amap ? seren::mapped_host(gpot) : nullptr;
+  if (!gmap) amap = nullptr;
+  if (!amap)
+    cudaMemcpyAsync(c.acc, a, sizeof(double) * 3 * (size_t)ptot, cudaMemcpyHostToDevice, c.st);
   double* d_sinks = c.stage;
   if (nsink > 0)
     cudaMemcpyAsync(d_sinks, sink_rmh, sizeof(double) * 5 * nsink, cudaMemcpyHostToDevice, c.st);
@@ -535,9 +610,9 @@ int seren_gpu_grav_forces(seren_gpu_ctx* h, const int32_t* acclist, int32_t nacc
   int rc = seren::set_active(c, acclist, nacc, nact);
   if (rc) return rc;
   cudaMemsetAsync(c.d_counts, 0, sizeof(int) * 32, c.st);
-  seren::launch_grav(c, nact, nsink, d_sinks);
+  seren::launch_grav(c, nact, nsink, d_sinks, amap, gmap, amap);
   rc = finish(c, "grav_forces");
-  if (rc) return rc;
+  if (rc || amap) return rc;
   if ((rc = seren::d2h_rows(c, a, c.acc, 3, acclist, nact))) return rc;
   if ((rc = seren::d2h_rows(c, gpot, c.gpot, 1, acclist, nact))) return rc;
   return finish(c, "grav_forces(copy back)");
@@ -597,33 +672,6 @@ struct IoPlan {
   double* gpot;
   int32_t* perm;
 };
-
-// the device address of a host buffer that is page-locked and mapped (as
-// pinned allocations are under unified addressing), else nullptr
-double* mapped_host(double* p) {
-  if (!p) return nullptr;
-  cudaPointerAttributes at{};
-  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
-    cudaGetLastError();
-    return nullptr;
-  }
-  return at.type == cudaMemoryTypeHost ? static_cast<double*>(at.devicePointer) : nullptr;
-}
-
-int io_init(Ctx& c) {
-  if (c.st_io) return 0;
-  if (cudaStreamCreateWithFlags(&c.st_io, cudaStreamNonBlocking) != cudaSuccess) {
-    c.st_io = nullptr;
-    return -1;
-  }
-  for (auto& e : c.ev_io)
-    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return -1;
-  if (cudaMalloc(&c.stage_io, sizeof(double) * 6 * (size_t)c.pmax) != cudaSuccess) {
-    c.stage_io = nullptr;
-    return -1;
-  }
-  return 0;
-}
 
 // The device-resident force step.  With io, each result leaves on the copy
 // stream once the stage that makes it has run: v, c_s^2 and the permutation

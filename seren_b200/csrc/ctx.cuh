@@ -132,10 +132,11 @@ struct Ctx {
   // of 6*pmax doubles, made on first use; build_tree waits for reorder_wait
   // (when set) before it reorders the particles
   cudaStream_t st_io = nullptr;
-  cudaEvent_t ev_io[2] = {};
+  cudaEvent_t ev_io[3] = {};
   double* stage_io = nullptr;
   cudaEvent_t reorder_wait = nullptr;
   bool reorder_late = false;    // v and c_s^2 still to reorder (finish_reorder)
+  cudaEvent_t vel_wait = nullptr;   // velocities still being copied in (finish_reorder waits)
 
   // timing of the last force step
   cudaEvent_t ev[10] = {};
@@ -158,16 +159,17 @@ int scan_scratch_alloc(ScanScratch& s, int nmax);
 // sph.cu
 void launch_gradh(Ctx& c, int nact);
 void launch_neib(Ctx& c, int nact);
-void launch_hydro(Ctx& c, int nact);
+void launch_hydro(Ctx& c, int nact, double* amap = nullptr);   // amap: mapped host a (optional)
 void launch_thermal(Ctx& c);
 int hydro_walk_slots(const Ctx& c);     // resident warps of the grad-h / neighbour grids
 int wide_scratch_alloc(Ctx& c);         // c.wst, c.wacc; 0 or -1
 
 // gravity.cu
 // amap/gmap (optional): host buffers mapped into the device address space
-// that receive a and gpot of each particle as soon as its group is done
+// that receive a and gpot of each particle as soon as its group is done;
+// abase (optional): where the acceleration gravity adds to is read (else acc)
 void launch_grav(Ctx& c, int nact, int nsink, const double* d_sinks, double* amap = nullptr,
-                 double* gmap = nullptr);
+                 double* gmap = nullptr, const double* abase = nullptr);
 void launch_sink_walk(Ctx& c, int nsink, const double* d_sinks, double* d_out /*[nsink][4]*/);
 int grav_walk_slots(const Ctx& c);      // resident warps of the gravity walk grid
 int grav_walk_stack_cap(const Ctx& c);  // stack entries per warp

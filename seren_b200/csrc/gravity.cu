@@ -289,7 +289,7 @@ __global__ void __launch_bounds__(GW_THREADS, MIXED ? 5 : 4)
 k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ pm,
             const double2* __restrict__ hz, GravWalk t, const double4* __restrict__ tabG,
             const float4* __restrict__ tab32, double* __restrict__ acc,
-            double* __restrict__ gpot, double* __restrict__ amap, double* __restrict__ gmap,
+            double* __restrict__ gpot, const double* abase, double* amap, double* __restrict__ gmap,
             int nsink, const double* __restrict__ sinks,
             int2* __restrict__ stacks, int* work, DevError* err, unsigned long long* counts) {
   using Cfg = GwTypes<MIXED>;
@@ -566,9 +566,11 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
         ax = cx + qx; ay = cy + qy; az = cz + qz; pot = cp + qp;
       }
       double* a = acc + (size_t)p * 3;
-      a[0] = a[0] + ax;
-      a[1] = a[1] + ay;
-      a[2] = a[2] + az;
+      // the acceleration gravity adds to: acc, or a mapped host buffer
+      const double* ab = abase ? abase + (size_t)p * 3 : a;
+      a[0] = ab[0] + ax;
+      a[1] = ab[1] + ay;
+      a[2] = ab[2] + az;
       if (nsink > 0) {                                       // sinks/direct_sink_gravity.F90
         double sx = 0.0, sy = 0.0, sz = 0.0, sp2 = 0.0;
         for (int s = 0; s < nsink; ++s) {
@@ -695,7 +697,7 @@ int grav_walk_slots(const Ctx& c) {
 int grav_walk_stack_cap(const Ctx& c) { return std::min(GW_STACK, c.cmax + 1); }
 
 void launch_grav(Ctx& c, int nact, int nsink, const double* d_sinks, double* amap,
-                 double* gmap) {
+                 double* gmap, const double* abase) {
   if (nact <= 0) return;
   unsigned long long* counts = reinterpret_cast<unsigned long long*>(c.d_counts);
   const GravWalk gw{c.wA, c.gA, c.gB, c.gC, c.info.ctot, c.wstack_cap,
@@ -706,10 +708,12 @@ void launch_grav(Ctx& c, int nact, int nsink, const double* d_sinks, double* ama
   cudaMemsetAsync(c.work, 0, sizeof(int), c.st);
   if (!mixed)
     k_grav_walk<false><<<blocks, GW_THREADS, 0, c.st>>>(nact, c.act, c.pm, c.hz, gw, c.tabG,
-        c.tabG32, c.acc, c.gpot, amap, gmap, nsink, d_sinks, c.wstack, c.work, c.d_err, counts);
+        c.tabG32, c.acc, c.gpot, abase, amap, gmap, nsink, d_sinks, c.wstack, c.work, c.d_err,
+        counts);
   else
     k_grav_walk<true><<<blocks, GW_THREADS, 0, c.st>>>(nact, c.act, c.pm, c.hz, gw, c.tabG,
-        c.tabG32, c.acc, c.gpot, amap, gmap, nsink, d_sinks, c.wstack, c.work, c.d_err, counts);
+        c.tabG32, c.acc, c.gpot, abase, amap, gmap, nsink, d_sinks, c.wstack, c.work, c.d_err,
+        counts);
   ++c.nlaunch;
 }
 

@@ -1350,7 +1350,8 @@ __global__ void __launch_bounds__(128, 8) k_hydro(int nact, const int* __restric
                                                const int* __restrict__ pptot,
                                                const int* __restrict__ pplist, int L, HydroTree t,
                                                const double4* __restrict__ tabG, double alpha,
-                                               bool tc, double* __restrict__ acc, DevError* err) {
+                                               bool tc, double* __restrict__ acc,
+                                               double* __restrict__ amap, DevError* err) {
   const int gi = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = gi / SUB, sub = gi % SUB;
   if (SUB == 1 && i >= nact) return;
@@ -1478,15 +1479,24 @@ __global__ void __launch_bounds__(128, 8) k_hydro(int nact, const int* __restric
     }
     if (!valid || sub != 0) return;
   }
-  double* a = acc + (size_t)p * 3;
+  double r0, r1, r2;
   if (MIXED) {
-    a[0] = (double)f0 + (double)g0;
-    a[1] = (double)f1 + (double)g1;
-    a[2] = (double)f2 + (double)g2;
+    r0 = (double)f0 + (double)g0;
+    r1 = (double)f1 + (double)g1;
+    r2 = (double)f2 + (double)g2;
   } else {
-    a[0] = at0 + ad0;                                                            // :287, :297
-    a[1] = at1 + ad1;
-    a[2] = at2 + ad2;
+    r0 = at0 + ad0;                                                              // :287, :297
+    r1 = at1 + ad1;
+    r2 = at2 + ad2;
+  }
+  double* a = acc + (size_t)p * 3;
+  a[0] = r0;
+  a[1] = r1;
+  a[2] = r2;
+  if (amap) {                                  // a mapped host buffer: straight over PCIe
+    amap[(size_t)p * 3] = r0;
+    amap[(size_t)p * 3 + 1] = r1;
+    amap[(size_t)p * 3 + 2] = r2;
   }
 }
 
@@ -1646,7 +1656,7 @@ void launch_neib(Ctx& c, int nact) {
   c.nlaunch += 2;
 }
 
-void launch_hydro(Ctx& c, int nact) {
+void launch_hydro(Ctx& c, int nact, double* amap) {
   if (nact <= 0) return;
   k_hydro_prep<<<nb(c.ptot, 256), 256, 0, c.st>>>(c.ptot, c.hz, c.rho, c.omega, c.press, c.pf,
                                                   c.hf4);
@@ -1654,11 +1664,13 @@ void launch_hydro(Ctx& c, int nact) {
   if (c.prm.precision == 0)
     k_hydro<false, 1><<<nb(nact, 128), 128, 0, c.st>>>(
         nact, c.act, c.pm, c.hz, c.vel, c.rho, c.pf, c.hf4, c.sound, c.pptot, c.pplist,
-        c.prm.pp_limit, hydro_tree(c), c.tabG, c.prm.alpha, c.prm.kernel == 1, c.acc, c.d_err);
+        c.prm.pp_limit, hydro_tree(c), c.tabG, c.prm.alpha, c.prm.kernel == 1, c.acc, amap,
+        c.d_err);
   else
     k_hydro<true, HY_SUB><<<nb((long)nact * HY_SUB, 128), 128, 0, c.st>>>(
         nact, c.act, c.pm, c.hz, c.vel, c.rho, c.pf, c.hf4, c.sound, c.pptot, c.pplist,
-        c.prm.pp_limit, hydro_tree(c), c.tabG, c.prm.alpha, c.prm.kernel == 1, c.acc, c.d_err);
+        c.prm.pp_limit, hydro_tree(c), c.tabG, c.prm.alpha, c.prm.kernel == 1, c.acc, amap,
+        c.d_err);
   ++c.nlaunch;
 }
 
@@ -1814,10 +1826,10 @@ extern "C" int seren_gpu_hydro_forces_noalloc(int32_t n, const double* parray, c
   if (precision == 0)
     k_hydro<false, 1><<<nb(n, 128), 128, 0, st>>>(n, nullptr, pm, hz, vel, rho, pf, hf4, sound,
                                                  pptot, pplist, pp_limit, none, tab, alpha,
-                                                 kernel == 1, a, d_err);
+                                                 kernel == 1, a, nullptr, d_err);
   else
     k_hydro<true, HY_SUB><<<nb((long)n * HY_SUB, 128), 128, 0, st>>>(n, nullptr, pm, hz, vel, rho, pf, hf4, sound,
                                                 pptot, pplist, pp_limit, none, tab, alpha,
-                                                kernel == 1, a, d_err);
+                                                kernel == 1, a, nullptr, d_err);
   return noalloc_status(st, d_err);
 }

@@ -645,6 +645,10 @@ void scan_exclusive(Ctx& c, const int* in, int* out, int n) {
 }
 
 void finish_reorder(Ctx& c) {
+  if (c.vel_wait) {
+    cudaStreamWaitEvent(c.st, c.vel_wait, 0);
+    c.vel_wait = nullptr;
+  }
   if (!c.reorder_late) return;
   cudaStreamWaitEvent(c.st, c.reorder_wait, 0);
   k_reorder_vc<<<nb(c.ptot, 256), 256, 0, c.st>>>(c.idx, c.ptot, c.vel, c.csq, c.vel_alt,

@@ -273,6 +273,58 @@ def test_force_step_io_pinned_buffers(libs):
     assert np.array_equal(csq.numpy(), (ic["sound"] ** 2)[ref["perm"]])
 
 
+def test_host_calls_with_pinned_buffers(libs):
+    """With page-locked buffers the reference-shaped calls overlap their copies
+    (sph_update) or map the buffers (hydro_forces writes a, grav_forces reads
+    and writes a and gpot, straight from the kernels); the results equal the
+    ones from pageable buffers."""
+    import ctypes as C
+
+    import torch
+    ic = case("turb20k")
+    Oracle, Gpu = libs
+    n = ic["parray"].shape[0]
+    prm = params(ic)
+    g1 = Gpu(n, prm)
+    g2 = Gpu(n, prm)
+    r = run_pipeline(g1, ic)
+
+    def pinned(a, dtype=torch.float64):
+        t = torch.empty(a.shape, dtype=dtype, pin_memory=True)
+        t.copy_(torch.from_numpy(np.ascontiguousarray(a)))
+        return t
+
+    dp, ip = C.POINTER(C.c_double), C.POINTER(C.c_int32)
+    P = lambda t: C.cast(t.data_ptr(), dp)  # noqa: E731
+    I = lambda t: C.cast(t.data_ptr(), ip)  # noqa: E731,E741
+    parray = pinned(ic["parray"])
+    perm = pinned(np.zeros(n, dtype=np.int32), torch.int32)
+    g2._call("tree_update", g2._ctx, n, P(parray), 1, 1, I(perm))
+    pm = perm.numpy().copy()
+    v = pinned(ic["v"][pm])
+    L = prm.pp_limit
+    out = {k: pinned(np.zeros(n)) for k in ("rho", "omega", "div_v", "drhodt")}
+    pptot = pinned(np.zeros(n, dtype=np.int32), torch.int32)
+    pplist = pinned(np.full((n, L), -1, dtype=np.int32), torch.int32)
+    g2._call("sph_update", g2._ctx, n, None, 0, P(parray), P(v), P(out["rho"]), P(out["omega"]),
+             P(out["div_v"]), P(out["drhodt"]), I(pptot), I(pplist), 1)
+    sound = ic["sound"][pm]
+    press = pinned(sound * sound * out["rho"].numpy())
+    a = pinned(np.zeros((n, 3)))
+    g2._call("hydro_forces", g2._ctx, None, 0, P(press), P(pinned(sound)), P(a))
+    a_hydro = a.numpy().copy()
+    gpot = pinned(np.zeros(n))
+    g2._call("grav_forces", g2._ctx, None, 0, P(a), P(gpot), 0, None)
+    assert np.array_equal(pm, r["perm"])
+    assert np.array_equal(parray.numpy(), r["sph"]["parray"])
+    for k in ("rho", "omega", "div_v", "drhodt"):
+        assert np.array_equal(out[k].numpy(), r["sph"][k]), k
+    assert lists_equal(pptot.numpy(), pplist.numpy(), r["sph"]["pptot"], r["sph"]["pplist"], L)
+    assert np.array_equal(a_hydro, r["a_hydro"])
+    assert np.array_equal(a.numpy(), r["a"])
+    assert np.array_equal(gpot.numpy(), r["gpot"])
+
+
 def test_resident_step_with_sink_matches_host_calls(libs):
     """seren_gpu_set_sinks puts the sink-gas term of grav_forces into the
     device-resident step."""
