@@ -200,6 +200,7 @@ void free_all(Ctx& c) {
   for (void* p : ps)
     if (p) cudaFree(p);
   if (c.h_pin) cudaFreeHost(c.h_pin);
+  if (c.h_map) cudaFreeHost(c.h_map);
   if (c.stage_io) cudaFree(c.stage_io);
   for (auto& e : c.ev)
     if (e) cudaEventDestroy(e);
@@ -663,6 +664,8 @@ namespace {
 
 // Host buffers of seren_gpu_force_step_io (NULL ones are skipped)
 struct IoPlan {
+  const double* v_in;      // velocities and c_s^2 to copy in after the tree build
+  const double* csq_in;
   double* parray;
   double* v;
   double* csq;
@@ -687,9 +690,15 @@ int force_step_body(Ctx& c, int first_call, const IoPlan* io) {
   if (rc) return rc;
   launch_stock(c);
   cudaEventRecord(c.ev[1], c.st);
-  if (io && io->perm) {
+  if (io) {
+    // v and c_s^2 come in on the copy stream while the grad-h walk runs (the
+    // tree build has the device to itself); the passes wait for them
     cudaStreamWaitEvent(c.st_io, c.ev[1], 0);
-    cudaMemcpyAsync(io->perm, c.orig, sizeof(int) * N, cudaMemcpyDeviceToHost, c.st_io);
+    cudaMemcpyAsync(c.stage_io, io->v_in, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, c.st_io);
+    k_unpack_v<<<nb(n, 256), 256, 0, c.st_io>>>(c.stage_io, n, c.vel); ++c.nlaunch;
+    cudaMemcpyAsync(c.csq, io->csq_in, sizeof(double) * N, cudaMemcpyHostToDevice, c.st_io);
+    cudaEventRecord(c.ev_io[1], c.st_io);
+    if (io->perm) cudaMemcpyAsync(io->perm, c.orig, sizeof(int) * N, cudaMemcpyDeviceToHost, c.st_io);
   }
   if (first_call) launch_hguess(c);
   launch_gradh(c, n);                         // runs finish_reorder before its passes
@@ -777,19 +786,14 @@ int seren_gpu_force_step_io(seren_gpu_ctx* h, int32_t ptot, const double* parray
   seren::reset_particles(c, ptot);
   cudaMemcpyAsync(c.stage, parray, sizeof(double) * 6 * N, cudaMemcpyHostToDevice, c.st);
   seren::launch_unpack_parray(c, c.stage, ptot);
-  cudaEventRecord(c.ev_io[0], c.st);         // v, c_s^2 cleared; parray in (the link is free)
-  // velocities and c_s^2 come in on the copy stream while the tree is built;
-  // their reorder waits for them after the stock
-  cudaStreamWaitEvent(c.st_io, c.ev_io[0], 0);
-  cudaMemcpyAsync(c.stage_io, v, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, c.st_io);
-  seren::k_unpack_v<<<nb(ptot, 256), 256, 0, c.st_io>>>(c.stage_io, ptot, c.vel); ++c.nlaunch;
-  cudaMemcpyAsync(c.csq, csq, sizeof(double) * N, cudaMemcpyHostToDevice, c.st_io);
-  cudaEventRecord(c.ev_io[1], c.st_io);
+  // velocities and c_s^2 arrive after the tree build (force_step_body), in
+  // upload order in vel / csq; the tree build reorders the rest and leaves
+  // them to finish_reorder, which waits for the copy
   c.reorder_wait = c.ev_io[1];
   c.have_v = c.have_csq = true;
   int rc = finish(c, "force_step_io(upload)");
   if (rc == SEREN_GPU_OK) {
-    const seren::IoPlan io{parray_out, v_out, csq_out, rho, omega, a, gpot, perm_total};
+    const seren::IoPlan io{v, csq, parray_out, v_out, csq_out, rho, omega, a, gpot, perm_total};
     rc = seren::force_step_body(c, first_call, &io);
   }
   if (rc != SEREN_GPU_OK) {                                // leave no copy in flight

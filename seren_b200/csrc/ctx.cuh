@@ -53,6 +53,10 @@ struct Ctx {
   double* stage = nullptr;   // [pmax][6] device staging of host-layout arrays
   int* istage = nullptr;     // [pmax*pp_limit] device staging of id arrays
   double* h_pin = nullptr;   // pinned host staging, [pmax][6] doubles
+  // mapped page-locked host words the device writes small results into
+  // (read_dev): no copy-engine transfer, so they never queue behind bulk copies
+  int* h_map = nullptr;
+  int* d_map = nullptr;
   int* hi_pin = nullptr;     // pinned host staging, ids
 
   // build scratch
@@ -148,6 +152,9 @@ struct Ctx {
 // tree.cu
 int build_tree(Ctx& c);               // bbox, keys, sort, cells, leaf order, reorder
 void finish_reorder(Ctx& c);          // the deferred v, c_s^2 reorder (reorder_wait set)
+// copy `bytes` (a multiple of 4, at most 1 KiB) of device memory to the host
+// through the mapped words, after the work queued on c.st; 0 or an error code
+int read_dev(Ctx& c, const void* dsrc, void* hdst, size_t bytes);
 void launch_unpack_parray(Ctx& c, const double* stage, int n);
 void launch_pack_parray(Ctx& c, double* stage, int n, cudaStream_t s = nullptr);
 void launch_stock(Ctx& c);            // BHgrav_stock + BHhydro_stock

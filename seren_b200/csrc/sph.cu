@@ -1597,8 +1597,7 @@ void launch_gradh(Ctx& c, int nact) {
   // the particles whose walks outgrew the redo kernel's scratch: rounds of
   // whole-GPU walks until each has taken its last step
   int nwide = 0;
-  cudaMemcpyAsync(&nwide, c.work + 2, sizeof(int), cudaMemcpyDeviceToHost, c.st);
-  cudaStreamSynchronize(c.st);
+  read_dev(c, c.work + 2, &nwide, sizeof(int));
   if (nwide > 0) {
     int L = c.info.ltot;                         // cover: a level with a cell per thread
     for (int l = 0; l <= c.info.ltot; ++l)
@@ -1623,8 +1622,7 @@ void launch_gradh(Ctx& c, int nact) {
             c.omega, c.div_v, c.drhodt, c.work + 3, c.d_err, counts);
         c.nlaunch += 2;
         int more = 0;
-        cudaMemcpyAsync(&more, c.work + 3, sizeof(int), cudaMemcpyDeviceToHost, c.st);
-        cudaStreamSynchronize(c.st);
+        read_dev(c, c.work + 3, &more, sizeof(int));
         if (!more) break;
         if (round > round_cap) {               // cannot happen: each step is bounded
           k_flag_error<<<1, 1, 0, c.st>>>(c.d_err, SEREN_GPU_ERR_WALK, KID_GRADH);

@@ -12,6 +12,7 @@
 // prefix, emitted level by level in breadth-first order, and each leaf's
 // particles are put back into input-index order.
 #include <cstdio>
+#include <cstring>
 
 #include "ctx.cuh"
 
@@ -644,6 +645,33 @@ void scan_exclusive(Ctx& c, const int* in, int* out, int n) {
   scan_rec(c, in, out, n, 0);
 }
 
+__global__ void k_publish(const int* __restrict__ src, int n, volatile int* dst) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+}
+
+int read_dev(Ctx& c, const void* dsrc, void* hdst, size_t bytes) {
+  if (bytes % 4 != 0 || bytes > 1024) return SEREN_GPU_ERR_ARG;
+  if (c.h_map == nullptr) {
+    void* h = nullptr;
+    void* d = nullptr;
+    if (cudaHostAlloc(&h, 1024, cudaHostAllocMapped) != cudaSuccess ||
+        cudaHostGetDevicePointer(&d, h, 0) != cudaSuccess) {
+      if (h) cudaFreeHost(h);
+      cudaGetLastError();
+      // no mapped memory: an ordinary copy
+      cudaMemcpyAsync(hdst, dsrc, bytes, cudaMemcpyDeviceToHost, c.st);
+      return cudaStreamSynchronize(c.st) == cudaSuccess ? SEREN_GPU_OK : SEREN_GPU_ERR_CUDA;
+    }
+    c.h_map = static_cast<int*>(h);
+    c.d_map = static_cast<int*>(d);
+  }
+  k_publish<<<1, 128, 0, c.st>>>(static_cast<const int*>(dsrc), (int)(bytes / 4), c.d_map);
+  ++c.nlaunch;
+  if (cudaStreamSynchronize(c.st) != cudaSuccess) return SEREN_GPU_ERR_CUDA;
+  std::memcpy(hdst, const_cast<const int*>(c.h_map), bytes);
+  return SEREN_GPU_OK;
+}
+
 void finish_reorder(Ctx& c) {
   if (c.vel_wait) {
     cudaStreamWaitEvent(c.st, c.vel_wait, 0);
@@ -705,8 +733,7 @@ int build_tree(Ctx& c) {
                                                 c.nchild, c.cstart); ++c.nlaunch;
     scan_exclusive(c, c.nchild, c.choff, nbranch);
     int nnew = 0;
-    cudaMemcpyAsync(&nnew, c.scan.total, sizeof(int), cudaMemcpyDeviceToHost, c.st);
-    if (cudaStreamSynchronize(c.st) != cudaSuccess) return SEREN_GPU_ERR_CUDA;
+    if (read_dev(c, c.scan.total, &nnew, sizeof(int))) return SEREN_GPU_ERR_CUDA;
     const int level_first = ctot + 1;
     if ((long)ctot + nnew > (long)c.cmax) {
       c.err = "cell count exceeds cmax = 2*pmax";
@@ -719,8 +746,7 @@ int build_tree(Ctx& c) {
     k_next_branch<<<nb(nnew, 256), 256, 0, c.st>>>(c.bflag, c.bscan, nnew, level_first, br_next); ++c.nlaunch;
     k_level_done<<<1, 1, 0, c.st>>>(c.d_info, lev, level_first, nnew, c.scan.total); ++c.nlaunch;
     int nbn = 0;
-    cudaMemcpyAsync(&nbn, c.scan.total, sizeof(int), cudaMemcpyDeviceToHost, c.st);
-    if (cudaStreamSynchronize(c.st) != cudaSuccess) return SEREN_GPU_ERR_CUDA;
+    if (read_dev(c, c.scan.total, &nbn, sizeof(int))) return SEREN_GPU_ERR_CUDA;
     ctot += nnew;
     ++lev;
     std::swap(br, br_next);
@@ -743,8 +769,8 @@ int build_tree(Ctx& c) {
   std::swap(c.orig, c.orig_alt);
   k_pack_link<<<nb(ctot + 1, 256), 256, 0, c.st>>>(ctot, c.leaf, c.nextcell, c.ifopen, c.pstart,
                                                    c.link); ++c.nlaunch;
-  cudaMemcpyAsync(&c.info, c.d_info, sizeof(TreeInfo), cudaMemcpyDeviceToHost, c.st);
-  if (cudaStreamSynchronize(c.st) != cudaSuccess) return SEREN_GPU_ERR_CUDA;
+  static_assert(sizeof(TreeInfo) % 4 == 0 && sizeof(TreeInfo) <= 1024, "TreeInfo through read_dev");
+  if (read_dev(c, c.d_info, &c.info, sizeof(TreeInfo))) return SEREN_GPU_ERR_CUDA;
   c.have_tree = true;
   return SEREN_GPU_OK;
 }
