@@ -534,7 +534,7 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
     double h_fac, int pp_gather, double rextent, const int* __restrict__ leaves,
     const int* __restrict__ nleaf, const int* __restrict__ npot, int* __restrict__ redo,
     int* __restrict__ nredo, int* __restrict__ prune, int L, DevError* err,
-    unsigned long long* counts) {
+    unsigned long long* counts, int* work) {
   __shared__ GpWarp gpw[GP_WARPS];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   GpWarp& W = gpw[w];
@@ -638,7 +638,7 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
     niter += (nc + 31) >> 5;
   };
 
-  for (int g = blockIdx.x * GP_WARPS + w; (long long)g * 32 < nact; g += gridDim.x * GP_WARPS) {
+  for (int g = gr_next(work, lane); (long long)g * 32 < nact; g = gr_next(work, lane)) {
     const int i = g * 32 + lane;
     const bool live = i < nact;
     const int p = live ? (act ? act[i] : i) : (act ? act[nact - 1] : nact - 1);
@@ -1245,13 +1245,13 @@ __global__ void __launch_bounds__(GP_THREADS) k_neib_rows(
     int nact, const int* __restrict__ act, const double4* __restrict__ pm,
     const double2* __restrict__ hz, HydroTree t, int L, const int* __restrict__ leaves,
     const int* __restrict__ nleaf, int* __restrict__ pptot, int* __restrict__ pplist,
-    DevError* err, unsigned long long* counts) {
+    DevError* err, unsigned long long* counts, int* work) {
   __shared__ int cand_all[GP_WARPS][GP_SEG * LEAFMAX];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   int* cand = cand_all[w];
   const unsigned lt = (1u << lane) - 1u;
   unsigned long long ncands = 0, niter = 0, nsingle = 0;
-  for (int g = blockIdx.x * GP_WARPS + w; (long long)g * 32 < nact; g += gridDim.x * GP_WARPS) {
+  for (int g = gr_next(work, lane); (long long)g * 32 < nact; g = gr_next(work, lane)) {
     const int i = g * 32 + lane;
     const bool live = i < nact;
     const int p = live ? (act ? act[i] : i) : (act ? act[nact - 1] : nact - 1);
@@ -1584,11 +1584,11 @@ void launch_gradh(Ctx& c, int nact) {
     if (o < 1) o = 1;
   }
   const int blocks = std::min(sm_count(c) * o, nb(nb(nact, 32), GP_WARPS));
-  cudaMemsetAsync(c.work + 1, 0, 2 * sizeof(int), c.st);
+  cudaMemsetAsync(c.work, 0, 3 * sizeof(int), c.st);     // group counter, nredo, nwide
   k_gradh_pass<<<blocks, GP_THREADS, 0, c.st>>>(
       nact, c.act, c.pm, c.hz, c.vel, c.rho, c.omega, c.div_v, c.drhodt, c.tabA, c.prm.h_fac,
       c.prm.pp_gather, c.info.rextent, c.leaves, c.nleaf, c.npot, c.redo, c.work + 1,
-      c.pplist, c.prm.pp_limit, c.d_err, counts);
+      c.pplist, c.prm.pp_limit, c.d_err, counts, c.work);
   // three walk-stack slots of scratch per redo warp
   k_gradh_redo<<<std::max(1, (c.wstack_slots / 3) / RD_WARPS), RD_THREADS, 0, c.st>>>(
       c.redo, c.work + 1, c.pm, c.hz, c.vel, c.rho, c.omega, c.div_v, c.drhodt, t, c.tabA,
@@ -1648,9 +1648,10 @@ void launch_neib(Ctx& c, int nact) {
     if (o < 1) o = 1;
   }
   const int blocks = std::min(sm_count(c) * o, nb(nb(nact, 32), GP_WARPS));
+  cudaMemsetAsync(c.work, 0, sizeof(int), c.st);          // group counter
   k_neib_rows<<<blocks, GP_THREADS, 0, c.st>>>(nact, c.act, c.pm, c.hz, t, c.prm.pp_limit,
                                                c.leaves, c.nleaf, c.pptot, c.pplist, c.d_err,
-                                               counts);
+                                               counts, c.work);
   c.nlaunch += 2;
 }
 
