@@ -346,6 +346,7 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
         const double4 q = t.gB[cid];
         const double q5 = t.gC[cid].x;
         if constexpr (MIXED) {
+          ncell += __popc(R.cmask[e]);                       // the terms this entry gives
           R.ca[e] = make_float4((float)(rx - a.x), (float)(ry - a.y), (float)(rz - a.z), (float)a.w);
           R.cb[e] = make_float4((float)q.x, (float)q.y, (float)q.z, (float)q.w);
           R.cq5[e] = make_float2((float)q5, (float)(-(q.x + q.z)));
@@ -358,16 +359,13 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
       __syncwarp();
       if constexpr (MIXED) {
         float sx = 0.f, sy = 0.f, sz = 0.f, sp = 0.f;
-        int mine = 0;
 #pragma unroll 2
         for (int e = 0; e < nc; ++e) {
           if ((R.cmask[e] >> lane) & 1u) {
             const float4 a = R.ca[e];
             cell32(ux + a.x, uy + a.y, uz + a.z, a.w, R.cb[e], R.cq5[e], sx, sy, sz, sp);
-            ++mine;
           }
         }
-        ncell += mine;
         kc.add(0, sx); kc.add(1, sy); kc.add(2, sz); kc.add(3, sp);
       } else {
         for (int e = 0; e < nc; ++e) {
@@ -392,6 +390,9 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
           const double4 Q = pm[q];
           const double2 H = hz[q];
           if constexpr (MIXED) {
+            // the pairs this item gives (each lane's own particle, one item
+            // of its list, is taken off at the end of the group)
+            npair += __popc(R.qmask[b0 + e]);
             R.pa[e] = make_float4((float)(Q.x - rx), (float)(Q.y - ry), (float)(Q.z - rz), (float)Q.w);
             R.pb[e] = make_float2((float)(1.0 / H.x), (float)H.y);
           } else {
@@ -414,13 +415,9 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
             // pair32's own branch tests: the kernel is needed only inside 2h of either particle
             const bool soft = on && (drmag * invhp32 < KERNRANGE || drmag * b.x < KERNRANGE);
             if (__any_sync(FULLMASK, soft)) {
-              if (on) {
-                pair32(d0, d1, d2, invhp32, zo32, a.w, b.x, b.y, tab32, sx, sy, sz, sp);
-                ++npair;
-              }
+              if (on) pair32(d0, d1, d2, invhp32, zo32, a.w, b.x, b.y, tab32, sx, sy, sz, sp);
             } else if (on) {
               pair32_far(d0, d1, d2, inv, a.w, sx, sy, sz, sp);
-              ++npair;
             }
           }
           kc.add(0, sx); kc.add(1, sy); kc.add(2, sz); kc.add(3, sp);
@@ -558,6 +555,7 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
     nent += gent;
     flush_cells();
     flush_pairs();
+    if constexpr (MIXED) npair -= live ? 1u : 0u;           // the lane's own particle
     if (live) {
       double ax, ay, az, pot;
       if constexpr (MIXED) {
