@@ -1016,6 +1016,15 @@ __global__ void k_wide_init(int n, const int* __restrict__ ids, const double4* _
   for (int k = 0; k < 4; ++k) acc[4 * i + k] = 0.0;
 }
 
+// A pass at h <= h_high (every density pass; the final pass when its h is
+// below h_high) counts exactly the particles within 2h: each lies in a leaf
+// the walk at h_high opened, since the bounding sphere of every cell that
+// holds it holds it.  Those passes run over all particles (k_wide_brute);
+// k_wide_walk keeps the walks that count candidates and the other final passes.
+__device__ __forceinline__ bool wide_brute(const WideState& w) {
+  return w.job == WJ_PASS || (w.job == WJ_FINAL && w.hp < w.s.h_high);
+}
+
 // one walk per pending particle, WD_SLICES blocks each
 __global__ void __launch_bounds__(WD_THREADS) k_wide_walk(
     int n, const WideState* __restrict__ ws, const double4* __restrict__ pm,
@@ -1026,7 +1035,7 @@ __global__ void __launch_bounds__(WD_THREADS) k_wide_walk(
   if (i >= n) return;
   const WideState& w = ws[i];
   const int job = w.job;
-  if (job == WJ_DONE) return;                                    // block-uniform
+  if (job == WJ_DONE || wide_brute(w)) return;                   // block-uniform
   const int p = w.p;
   const double rx = w.P.x, ry = w.P.y, rz = w.P.z;
   const double hrange = KERNRANGE * w.s.h_high;
@@ -1094,6 +1103,66 @@ __global__ void __launch_bounds__(WD_THREADS) k_wide_walk(
       atomicAdd(acc + 4 * i + 1, r1);
       atomicAdd(acc + 4 * i + 2, r2);
       atomicAdd(acc + 4 * i + 3, r3);
+    }
+  }
+}
+
+// the passes wide_brute() selects: each block takes WD_THREADS * BR_Q
+// particles and adds their terms of every such pass (same terms and tests as
+// the walk's candidates give)
+constexpr int BR_Q = 4;          // particles per thread
+__global__ void __launch_bounds__(WD_THREADS) k_wide_brute(int n, const WideState* __restrict__ ws,
+                                                           int ptot, const double4* __restrict__ pm,
+                                                           const double4* __restrict__ vel,
+                                                           double* __restrict__ acc) {
+  __shared__ double red[WD_THREADS / 32];
+  int qi[BR_Q];
+  double4 Q[BR_Q];
+#pragma unroll
+  for (int k = 0; k < BR_Q; ++k) {
+    const long q = (long)blockIdx.x * (WD_THREADS * BR_Q) + k * WD_THREADS + threadIdx.x;
+    qi[k] = q < ptot ? (int)q : -1;
+    Q[k] = q < ptot ? pm[q] : make_double4(0.0, 0.0, 0.0, 0.0);
+  }
+  for (int i = 0; i < n; ++i) {
+    const WideState& w = ws[i];
+    if (!wide_brute(w)) continue;                                 // block-uniform
+    const int p = w.p;
+    const double rx = w.P.x, ry = w.P.y, rz = w.P.z;
+    const double hs = w.hs, ih = w.ih, hf = w.hf;
+    if (w.job == WJ_PASS) {                                       // :211-235
+      double s0 = 0.0;
+#pragma unroll
+      for (int k = 0; k < BR_Q; ++k) {
+        if (qi[k] < 0 || qi[k] == p) continue;
+        const double d0 = Q[k].x - rx, d1 = Q[k].y - ry, d2 = Q[k].z - rz;
+        const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
+        if (drsqd < hs) gh_density_in(drsqd, Q[k].w, ih, hf, s0);
+      }
+      const double r0 = block_sum(s0, red);
+      if (threadIdx.x == 0 && r0 != 0.0) atomicAdd(acc + 4 * i, r0);
+    } else {                                                      // :360-425
+      const double4 vp = w.v;
+      GhFinal f;
+      f.rt = 0.0; f.om = 0.0; f.dv = 0.0; f.zt = 0.0;
+#pragma unroll
+      for (int k = 0; k < BR_Q; ++k) {
+        if (qi[k] < 0 || qi[k] == p) continue;
+        const double d0 = Q[k].x - rx, d1 = Q[k].y - ry, d2 = Q[k].z - rz;
+        const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
+        if (drsqd > hs) continue;
+        const double4 V = vel[qi[k]];
+        const double dv0 = V.x - vp.x, dv1 = V.y - vp.y, dv2 = V.z - vp.z;
+        gh_final_in(drsqd, Q[k].w, (dv0 * d0 + dv1 * d1) + dv2 * d2, ih, hf, f);
+      }
+      const double r0 = block_sum(f.rt, red), r1 = block_sum(f.om, red),
+                   r2 = block_sum(f.dv, red), r3 = block_sum(f.zt, red);
+      if (threadIdx.x == 0) {
+        if (r0 != 0.0) atomicAdd(acc + 4 * i, r0);
+        if (r1 != 0.0) atomicAdd(acc + 4 * i + 1, r1);
+        if (r2 != 0.0) atomicAdd(acc + 4 * i + 2, r2);
+        if (r3 != 0.0) atomicAdd(acc + 4 * i + 3, r3);
+      }
     }
   }
 }
@@ -1616,6 +1685,9 @@ void launch_gradh(Ctx& c, int nact) {
             n, static_cast<WideState*>(c.wst), c.pm, c.vel, t, c.parent, c.level, L,
             c.info.last_cell[L], c.wacc,
             c.d_err);
+        k_wide_brute<<<nb(c.ptot, WD_THREADS * BR_Q), WD_THREADS, 0, c.st>>>(
+            n, static_cast<WideState*>(c.wst), c.ptot, c.pm, c.vel, c.wacc);
+        ++c.nlaunch;
         cudaMemsetAsync(c.work + 3, 0, sizeof(int), c.st);
         k_wide_update<<<nb(n, 128), 128, 0, c.st>>>(
             n, static_cast<WideState*>(c.wst), c.wacc, c.tabA, c.prm.h_fac, c.prm.pp_gather, c.info.rextent, c.hz, c.rho,
