@@ -50,7 +50,10 @@ typedef struct {
   int32_t leafmax;     /* must be 8 (LEAFMAX)                                    */
   int32_t lmax;        /* maximum tree level, <= 30 (LMAX)                       */
   int32_t index_base;  /* 1: Fortran ids (1..ptot); 0: C ids (0..ptot-1)         */
-  int32_t reserved;
+  int32_t redo_cap;    /* 0: default; n > 0: a grad-h redo walk that needs more than n
+                          frontier cells or leaves moves to the whole-GPU path (results
+                          unchanged; small n exercises that path in tests). The CPU
+                          oracle ignores it.                                        */
   double h_fac;        /* h = h_fac*(m/rho)^(1/3)                                */
   double thetamaxsqd;  /* geometric MAC opening angle squared                    */
   double alpha;        /* artificial viscosity alpha (beta is always 2*alpha)    */

@@ -28,15 +28,15 @@ class Params(C.Structure):
     _fields_ = [("ndim", C.c_int32), ("kernel", C.c_int32), ("visc", C.c_int32),
                 ("precision", C.c_int32), ("pp_gather", C.c_int32), ("pp_limit", C.c_int32),
                 ("leafmax", C.c_int32), ("lmax", C.c_int32), ("index_base", C.c_int32),
-                ("reserved", C.c_int32), ("h_fac", C.c_double), ("thetamaxsqd", C.c_double),
+                ("redo_cap", C.c_int32), ("h_fac", C.c_double), ("thetamaxsqd", C.c_double),
                 ("alpha", C.c_double), ("alpha_min", C.c_double)]
 
     @classmethod
     def make(cls, h_fac=1.2, thetamaxsqd=0.25, alpha=1.0, precision=0, kernel=0,
-             pp_gather=None, index_base=0, lmax=30):
+             pp_gather=None, index_base=0, lmax=30, redo_cap=0):
         from .ics import pp_gather_for
         ppg = pp_gather_for(h_fac) if pp_gather is None else int(pp_gather)
-        return cls(3, kernel, 0, precision, ppg, 2 * ppg, 8, lmax, index_base, 0,
+        return cls(3, kernel, 0, precision, ppg, 2 * ppg, 8, lmax, index_base, int(redo_cap),
                    float(h_fac), float(thetamaxsqd), float(alpha), 0.1)
 
 

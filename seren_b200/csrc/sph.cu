@@ -1662,7 +1662,8 @@ void launch_gradh(Ctx& c, int nact) {
   k_gradh_redo<<<std::max(1, (c.wstack_slots / 3) / RD_WARPS), RD_THREADS, 0, c.st>>>(
       c.redo, c.work + 1, c.pm, c.hz, c.vel, c.rho, c.omega, c.div_v, c.drhodt, t, c.tabA,
       c.prm.h_fac, c.prm.pp_gather, c.info.rextent, reinterpret_cast<int*>(c.wstack),
-      2 * c.wstack_cap, c.wide, c.work + 2, c.d_err, counts);
+      c.prm.redo_cap > 0 ? std::min(c.prm.redo_cap, 2 * c.wstack_cap) : 2 * c.wstack_cap,
+      c.wide, c.work + 2, c.d_err, counts);
   // the particles whose walks outgrew the redo kernel's scratch: rounds of
   // whole-GPU walks until each has taken its last step
   int nwide = 0;

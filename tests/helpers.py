@@ -32,11 +32,11 @@ def case(name: str):
     return ic
 
 
-def params(ic, precision=0, index_base=0, kernel=0, thetamaxsqd=None):
+def params(ic, precision=0, index_base=0, kernel=0, thetamaxsqd=None, redo_cap=0):
     return Params.make(h_fac=ic["h_fac"],
                        thetamaxsqd=ic["thetamaxsqd"] if thetamaxsqd is None else thetamaxsqd,
                        alpha=ic["alpha"], precision=precision, index_base=index_base,
-                       kernel=kernel)
+                       kernel=kernel, redo_cap=redo_cap)
 
 
 def run_pipeline(hp, ic, first_call=True, sinks=None):

@@ -67,6 +67,32 @@ def test_full_evaluation_fp64(libs, name):
     assert rel_rows(rg["gpot"], ro["gpot"]).max() < TOL
 
 
+def test_whole_gpu_gradh_path_matches_oracle(libs):
+    """With a tiny redo scratch (redo_cap) the particles that grad-h hands to
+    the redo kernel on the first call (h guess) go on to the whole-GPU path:
+    counting walks over subtrees, passes over all particles.  The results are
+    still the oracle's."""
+    ic = case("turb20k")
+    o, g = _pair(libs, ic, redo_cap=8)
+    ro = run_pipeline(o, ic)
+    rg = run_pipeline(g, ic)
+    so, sg = ro["sph"], rg["sph"]
+    assert rel_rows(sg["parray"][:, 4], so["parray"][:, 4]).max() < TOL
+    for k in ("rho", "omega"):
+        assert rel_rows(sg[k], so[k]).max() < TOL, k
+    for k in ("div_v", "drhodt"):
+        assert rel_scaled(sg[k], so[k]) < TOL, k
+    L = g.params.pp_limit
+    assert lists_equal(so["pptot"], so["pplist"], sg["pptot"], sg["pplist"], L)
+    assert rel_rows(rg["a"], ro["a"]).max() < 1e-11
+    Oracle, Gpu = libs
+    n = ic["parray"].shape[0]
+    g2 = Gpu(n, params(ic, redo_cap=8))
+    g2.upload(ic["parray"], ic["v"], ic["sound"] ** 2)
+    g2.force_step(first_call=True)
+    assert g2.last_step_stats()[2][8] > 0           # particles on the whole-GPU path
+
+
 @pytest.mark.parametrize("name", ["sphere4k", "plummer16k", "disc12k"])
 def test_neighbour_lists_at_oracle_h(libs, name):
     """get_neib at the same h is bit-exact (sph/get_neib.F90:83-118)."""
