@@ -455,7 +455,6 @@ __global__ void __launch_bounds__(GR_THREADS) k_gradh_walk(
 
 constexpr int GP_THREADS = 128;
 constexpr int GP_WARPS = GP_THREADS / 32;
-constexpr int GP_INB = 128;      // packed in-range candidates per warp
 constexpr int GP_SEG = 64;       // leaves of a row flattened at a time
 
 // The density term (:218-230) and the final-pass terms (:360-425) of one
