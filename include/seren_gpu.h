@@ -128,6 +128,27 @@ int seren_gpu_upload(seren_gpu_ctx* ctx, int32_t ptot, const double* parray,
                      const double* v, const double* csq);
 int seren_gpu_force_step(seren_gpu_ctx* ctx, int32_t first_call);
 int seren_gpu_drift(seren_gpu_ctx* ctx, double dt);
+/* Per-particle timesteps on the state of the last force evaluation
+ * (timestep/timestep_size.F90:52-120 with HYDRO and MON97 viscosity,
+ * beta = 2*alpha, no internal energy):
+ *   dt_p = min(accel_mult*sqrt(h/(|a| + 1e-20)),
+ *              courant_mult*h/(c + h|div v| + 0.6*(alpha*c + beta*h|div v|))).
+ * *dt_min receives the least of them (the global step of
+ * sph_sim/sph_timesteps.F90:58-66); dt (may be NULL) every dt_p, in tree
+ * order.  Not a reference entry point: it replaces the loop that calls
+ * timestep_size for every particle. */
+int seren_gpu_timestep(seren_gpu_ctx* ctx, double courant_mult, double accel_mult,
+                       double* dt_min, double* dt);
+/* One step of the reference's second-order Runge-Kutta scheme
+ * (advance/advance_runge_kutta.F90:40-72) for all particles on one timestep
+ * level, kept on the device: r_half = r + v*dt/2, v_half = v + a*dt/2; the
+ * forces at the half step; r' = r + v_half*dt, v' = v + a_half*dt; the forces
+ * at the end, so the state is at t + dt with its accelerations, ready for
+ * seren_gpu_timestep.  Two force evaluations, each as seren_gpu_force_step
+ * (tree rebuilt; the step's state follows the particle reorder).  Needs
+ * seren_gpu_upload and one seren_gpu_force_step first.  Not a reference
+ * entry point: it replaces sph_advance's per-particle loop for one level. */
+int seren_gpu_rk2_step(seren_gpu_ctx* ctx, double dt);
 /* Sinks for the device-resident step: from the next seren_gpu_force_step on,
  * its gravity adds direct_sink_gravity (sinks/direct_sink_gravity.F90:10-64)
  * for sink_rmh[s] = {x, y, z, m, h}, as seren_gpu_grav_forces does with

@@ -72,6 +72,36 @@ def kernel_tables(kernel: int = 0) -> np.ndarray:
     return t
 
 
+def timestep_sizes(h, a, div_v, sound, alpha, courant_mult=0.2, accel_mult=0.5):
+    """Per-particle timesteps, timestep/timestep_size.F90:52-120 (HYDRO,
+    ARTIFICIAL_VISCOSITY with beta = 2 alpha, no internal energy), in FP64 with
+    the Fortran expressions' order of operations:
+    tacc = accel_mult*sqrt(h/(|a| + 1e-20)) (:95-96),
+    tcour = courant_mult*h/(c + h|div v| + 0.6(alpha c + beta h|div v|)) (:103-105,
+    TVISC_FAC = 0.6 from headers/macros.h:133), dt = min(tacc, tcour)."""
+    a = np.asarray(a, dtype=np.float64).reshape(-1, 3)
+    h = np.asarray(h, dtype=np.float64)
+    dv = np.abs(np.asarray(div_v, dtype=np.float64))
+    c = np.asarray(sound, dtype=np.float64)
+    beta = 2.0 * alpha
+    amag = np.sqrt((a[:, 0] * a[:, 0] + a[:, 1] * a[:, 1]) + a[:, 2] * a[:, 2])
+    tacc = accel_mult * np.sqrt(h / (amag + 1.0e-20))
+    tcour = (courant_mult * h) / ((c + h * dv) + 0.6 * (alpha * c + (beta * h) * dv))
+    return np.minimum(tacc, tcour)
+
+
+def rk2_half(r, v, a, dt):
+    """advance/advance_runge_kutta.F90:40-54 at the half step (dt = step/2):
+    r + v dt, v + a dt."""
+    return r + v * dt, v + a * dt
+
+
+def rk2_full(r_old, v_old, v_half, a_half, dt):
+    """advance/advance_runge_kutta.F90:56-69 at the end of the step: r_old +
+    v_half dt, v_old + a dt."""
+    return r_old + v_half * dt, v_old + a_half * dt
+
+
 class Oracle(HotPath):
     def __init__(self, pmax: int, params: Params):
         super().__init__(library(), "seren_oracle", pmax, params)

@@ -117,6 +117,63 @@ __global__ void k_fma_peak(T* out, int iters, T a, T b) {
   if (s == (T)-1.2345) out[0] = s;
 }
 
+// timestep/timestep_size.F90:52-120 (HYDRO, ARTIFICIAL_VISCOSITY, no internal
+// energy): dt = min(accel_mult sqrt(h / (|a| + 1e-20)),
+// courant_mult h / (c + h|div v| + 0.6 (alpha c + beta h|div v|))), and the
+// least over the particles (positive doubles order as their bit patterns)
+__global__ void k_timestep(int n, const double2* __restrict__ hz, const double* __restrict__ acc,
+                           const double* __restrict__ div_v, const double* __restrict__ sound,
+                           double alpha, double beta, double courant_mult, double accel_mult,
+                           double* __restrict__ dt_out, unsigned long long* __restrict__ dt_min) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  double dt = 1.0e300;
+  if (i < n) {
+    const double a0 = acc[3 * i], a1 = acc[3 * i + 1], a2 = acc[3 * i + 2];
+    const double hp = hz[i].x;
+    const double dv = fabs(div_v[i]);
+    const double vsignal = sound[i];
+    const double amag = sqrt((a0 * a0 + a1 * a1) + a2 * a2);
+    const double tacc = accel_mult * sqrt(hp / (amag + 1.0e-20));
+    const double tcour = (courant_mult * hp) /
+                         ((vsignal + hp * dv) + 0.6 * (alpha * vsignal + (beta * hp) * dv));
+    dt = fmin(tacc, tcour);
+    dt_out[i] = dt;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) dt = fmin(dt, __shfl_xor_sync(0xffffffffu, dt, o));
+  if ((threadIdx.x & 31) == 0) atomicMin(dt_min, (unsigned long long)__double_as_longlong(dt));
+}
+
+// advance/advance_runge_kutta.F90:40-72, one timestep level: the first half
+// (dt = step/2) keeps r_old, v_old and v_half; the second (dt = step) uses them
+__global__ void k_rk_half(int n, double4* __restrict__ pm, double4* __restrict__ vel,
+                          const double* __restrict__ acc, double4* __restrict__ r_old,
+                          double4* __restrict__ v_old, double4* __restrict__ v_half, double dt) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double4 r = pm[i], v = vel[i];
+  r_old[i] = r;
+  v_old[i] = v;
+  const double4 rp = make_double4(r.x + v.x * dt, r.y + v.y * dt, r.z + v.z * dt, r.w);
+  const double4 vp = make_double4(v.x + acc[3 * i] * dt, v.y + acc[3 * i + 1] * dt,
+                                  v.z + acc[3 * i + 2] * dt, 0.0);
+  pm[i] = rp;
+  vel[i] = vp;
+  v_half[i] = vp;
+}
+
+__global__ void k_rk_full(int n, double4* __restrict__ pm, double4* __restrict__ vel,
+                          const double* __restrict__ acc, const double4* __restrict__ r_old,
+                          const double4* __restrict__ v_old, const double4* __restrict__ v_half,
+                          double dt) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double4 r = r_old[i], v = v_old[i], vh = v_half[i];
+  pm[i] = make_double4(r.x + vh.x * dt, r.y + vh.y * dt, r.z + vh.z * dt, pm[i].w);
+  vel[i] = make_double4(v.x + acc[3 * i] * dt, v.y + acc[3 * i + 1] * dt,
+                        v.z + acc[3 * i + 2] * dt, 0.0);
+}
+
 __global__ void k_drift(int n, double4* __restrict__ pm, const double4* __restrict__ vel, double dt) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -202,6 +259,8 @@ void free_all(Ctx& c) {
   if (c.h_pin) cudaFreeHost(c.h_pin);
   if (c.h_map) cudaFreeHost(c.h_map);
   if (c.stage_io) cudaFree(c.stage_io);
+  for (double4* p : {c.r_old, c.v_old, c.v_half, c.r_old_alt, c.v_old_alt, c.v_half_alt})
+    if (p) cudaFree(p);
   for (auto& e : c.ev)
     if (e) cudaEventDestroy(e);
   for (auto& e : c.ev_io)
@@ -817,6 +876,59 @@ int seren_gpu_set_sinks(seren_gpu_ctx* h, int32_t nsink, const double* sink_rmh)
     cudaMemcpyAsync(c.sinks, sink_rmh, sizeof(double) * 5 * nsink, cudaMemcpyHostToDevice, c.st);
   c.nsink = nsink;
   return finish(c, "set_sinks");
+}
+
+int seren_gpu_timestep(seren_gpu_ctx* h, double courant_mult, double accel_mult, double* dt_min,
+                       double* dt) {
+  if (!h) return SEREN_GPU_ERR_ARG;
+  Ctx& c = h->c;
+  if (!dt_min || !(courant_mult > 0.0) || !(accel_mult > 0.0))
+    return fail(c, SEREN_GPU_ERR_ARG, "timestep: dt_min NULL or a multiplier not positive");
+  if (!c.have_sph || c.ptot < 1) return fail(c, SEREN_GPU_ERR_STATE, "no forces yet");
+  const int n = c.ptot;
+  double* d_dt = c.stage;                                  // [n] steps, then the least
+  unsigned long long* d_min = reinterpret_cast<unsigned long long*>(c.stage + n);
+  static const unsigned long long inf_bits = 0x7ff0000000000000ull;
+  cudaMemcpyAsync(d_min, &inf_bits, sizeof(inf_bits), cudaMemcpyHostToDevice, c.st);
+  seren::k_timestep<<<nb(n, 256), 256, 0, c.st>>>(n, c.hz, c.acc, c.div_v, c.sound, c.prm.alpha,
+                                                   2.0 * c.prm.alpha, courant_mult, accel_mult,
+                                                   d_dt, d_min);
+  ++c.nlaunch;
+  if (seren::read_dev(c, d_min, dt_min, sizeof(double))) return finish(c, "timestep");
+  if (dt) cudaMemcpyAsync(dt, d_dt, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, c.st);
+  return finish(c, "timestep");
+}
+
+int seren_gpu_rk2_step(seren_gpu_ctx* h, double dt) {
+  if (!h) return SEREN_GPU_ERR_ARG;
+  Ctx& c = h->c;
+  if (!(dt > 0.0) || !std::isfinite(dt)) return fail(c, SEREN_GPU_ERR_ARG, "rk2_step: dt not positive");
+  if (!c.have_v || !c.have_csq || !c.have_sph || c.ptot < 1)
+    return fail(c, SEREN_GPU_ERR_STATE, "rk2_step: call seren_gpu_upload and seren_gpu_force_step first");
+  if (!c.r_old) {
+    const size_t P = (size_t)c.pmax;
+    for (double4** p : {&c.r_old, &c.v_old, &c.v_half, &c.r_old_alt, &c.v_old_alt, &c.v_half_alt})
+      if (cudaMalloc(p, sizeof(double4) * P) != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        for (double4** q : {&c.r_old, &c.v_old, &c.v_half, &c.r_old_alt, &c.v_old_alt, &c.v_half_alt})
+          if (*q) { cudaFree(*q); *q = nullptr; }
+        return fail(c, SEREN_GPU_ERR_CUDA, "rk2_step: state allocation failed");
+      }
+  }
+  const int n = c.ptot;
+  c.nlaunch = 0;
+  // first half (advance_runge_kutta.F90:40-54) with the forces at the start
+  seren::k_rk_half<<<nb(n, 256), 256, 0, c.st>>>(n, c.pm, c.vel, c.acc, c.r_old, c.v_old,
+                                                  c.v_half, 0.5 * dt);
+  ++c.nlaunch;
+  int rc = seren::force_step_body(c, 0, nullptr);             // forces at the half step
+  if (rc) return rc;
+  // second half (:56-69) from the start with v_half and the half-step forces
+  seren::k_rk_full<<<nb(n, 256), 256, 0, c.st>>>(n, c.pm, c.vel, c.acc, c.r_old, c.v_old,
+                                                  c.v_half, dt);
+  ++c.nlaunch;
+  return seren::force_step_body(c, 0, nullptr);               // forces at the end
 }
 
 int seren_gpu_drift(seren_gpu_ctx* h, double dt) {

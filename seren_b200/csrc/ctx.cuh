@@ -44,6 +44,15 @@ struct Ctx {
   double* press = nullptr;
   double* sound = nullptr;
   double* acc = nullptr;     // [ptot][3]
+  // second-order Runge-Kutta state (seren_gpu_rk2_step), made on first use and
+  // reordered with the particles: positions and velocities at the start of
+  // the step and the velocities at its half
+  double4* r_old = nullptr;
+  double4* v_old = nullptr;
+  double4* v_half = nullptr;
+  double4* r_old_alt = nullptr;
+  double4* v_old_alt = nullptr;
+  double4* v_half_alt = nullptr;
   double* gpot = nullptr;
   double* pf = nullptr;      // hydro: press/rho/rho/omega per particle
   double* hf4 = nullptr;     // hydro: (1/h)**(NDIM+1) per particle

@@ -395,6 +395,18 @@ __global__ void k_reorder_vc(const int* __restrict__ perm, int n, const double4*
   csq2[i] = csq[p];
 }
 
+__global__ void k_reorder_rk(const int* __restrict__ perm, int n, const double4* __restrict__ a,
+                             const double4* __restrict__ b, const double4* __restrict__ c,
+                             double4* __restrict__ a2, double4* __restrict__ b2,
+                             double4* __restrict__ c2) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int p = perm[i];
+  a2[i] = a[p];
+  b2[i] = b[p];
+  c2[i] = c[p];
+}
+
 __global__ void k_pack_link(int ctot, const int* __restrict__ leaf, const int* __restrict__ nextcell,
                             const int* __restrict__ ifopen, const int* __restrict__ pstart,
                             int4* __restrict__ link) {
@@ -767,6 +779,13 @@ int build_tree(Ctx& c) {
   std::swap(c.pm, c.pm_alt);
   std::swap(c.hz, c.hz_alt);
   std::swap(c.orig, c.orig_alt);
+  if (c.r_old) {                            // Runge-Kutta state follows the particles
+    k_reorder_rk<<<nb(n, 256), 256, 0, c.st>>>(c.idx, n, c.r_old, c.v_old, c.v_half, c.r_old_alt,
+                                                c.v_old_alt, c.v_half_alt); ++c.nlaunch;
+    std::swap(c.r_old, c.r_old_alt);
+    std::swap(c.v_old, c.v_old_alt);
+    std::swap(c.v_half, c.v_half_alt);
+  }
   k_pack_link<<<nb(ctot + 1, 256), 256, 0, c.st>>>(ctot, c.leaf, c.nextcell, c.ifopen, c.pstart,
                                                    c.link); ++c.nlaunch;
   static_assert(sizeof(TreeInfo) % 4 == 0 && sizeof(TreeInfo) <= 1024, "TreeInfo through read_dev");

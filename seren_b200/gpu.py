@@ -36,6 +36,8 @@ def library(build_if_missing: bool = True) -> C.CDLL:
                            ("force_step_io", [vp, C.c_int32, _dp, _dp, _dp, C.c_int32, _dp, _dp,
                                               _dp, _dp, _dp, _dp, _dp, _ip]),
                            ("drift", [vp, C.c_double]),
+                           ("timestep", [vp, C.c_double, C.c_double, _dp, _dp]),
+                           ("rk2_step", [vp, C.c_double]),
                            ("set_sinks", [vp, C.c_int32, _dp]),
                            ("download", [vp, _dp, _dp, _dp, _dp, _dp, _dp, _ip]),
                            ("last_step_stats", [vp, _dp, _ip, C.POINTER(C.c_int64)]),
@@ -93,6 +95,20 @@ class GpuHotPath(HotPath):
 
     def drift(self, dt: float):
         self._call("drift", self._ctx, C.c_double(dt))
+
+    def timestep(self, courant_mult=0.2, accel_mult=0.5, per_particle=False):
+        """Least particle timestep (seren_gpu_timestep) of the last force
+        evaluation; with per_particle, also every particle's (tree order)."""
+        dmin = C.c_double()
+        dt = np.zeros(self.ptot) if per_particle else None
+        self._call("timestep", self._ctx, C.c_double(courant_mult), C.c_double(accel_mult),
+                   C.byref(dmin), _d(dt))
+        return (dmin.value, dt) if per_particle else dmin.value
+
+    def rk2_step(self, dt: float):
+        """One second-order Runge-Kutta step of dt on the device
+        (seren_gpu_rk2_step): two force evaluations."""
+        self._call("rk2_step", self._ctx, C.c_double(dt))
 
     def download(self):
         n = self.ptot

@@ -367,3 +367,44 @@ def test_resident_step_with_sink_matches_host_calls(libs):
     assert np.array_equal(st["perm"], r["perm"])
     assert rel_rows(st["a"], r["a"]).max() < 1e-13
     assert np.array_equal(st["gpot"], r["gpot"])
+
+
+def test_timestep_and_rk2_step_match_oracle(libs):
+    """seren_gpu_timestep equals timestep_size.F90 on the oracle's state, and
+    one device-resident second-order Runge-Kutta step (two force evaluations,
+    the particles reordered at each tree build) equals the oracle's forces
+    driven through the same step with advance_runge_kutta.F90's updates."""
+    from oracle.oracle import rk2_full, rk2_half, timestep_sizes
+    ic = case("turb20k")
+    o, g = _pair(libs, ic)
+    n = ic["parray"].shape[0]
+    # start: forces and timesteps
+    g.upload(ic["parray"], ic["v"], ic["sound"] ** 2)
+    g.force_step(first_call=True)
+    dt_min, dt_g = g.timestep(0.2, 0.5, per_particle=True)
+    r0 = run_pipeline(o, ic)
+    p0, perm0 = r0["sph"]["parray"], r0["perm"]
+    dt_o = timestep_sizes(p0[:, 4], r0["a"], r0["sph"]["div_v"], r0["sound"], ic["alpha"])
+    assert np.array_equal(g.download()["perm"], perm0)
+    assert rel_rows(dt_g, dt_o).max() < 1e-11
+    assert dt_min == dt_g.min()
+    dt = dt_min
+    g.rk2_step(dt)
+    st = g.download()
+    # the oracle through the same step: half step, forces, full step, forces
+    v0 = ic["v"][perm0]
+    rh, vh = rk2_half(p0[:, 0:3], v0, r0["a"], 0.5 * dt)
+    ph = p0.copy()
+    ph[:, 0:3] = rh
+    r1 = run_pipeline(o, dict(ic, parray=ph, v=vh, sound=r0["sound"]), first_call=False)
+    perm1 = r1["perm"]                                   # tree order 1 -> tree order 0
+    x1, v1 = rk2_full(p0[perm1, 0:3], v0[perm1], vh[perm1], r1["a"], dt)
+    p1 = r1["sph"]["parray"].copy()
+    p1[:, 0:3] = x1
+    r2 = run_pipeline(o, dict(ic, parray=p1, v=v1, sound=r1["sound"]), first_call=False)
+    perm2 = r2["perm"]
+    assert np.array_equal(st["perm"], perm0[perm1[perm2]])
+    assert np.abs(st["parray"][:, 0:3] - r2["parray"][:, 0:3]).max() < 1e-12
+    assert rel_rows(st["v"], v1[perm2]).max() < 1e-10
+    assert rel_rows(st["parray"][:, 4], r2["sph"]["parray"][:, 4]).max() < 1e-10
+    assert rel_rows(st["a"], r2["a"]).max() < 1e-9

@@ -176,3 +176,26 @@ def test_too_few_particles_is_an_error():
     with pytest.raises(SerenError) as e:
         o.sph_update(p, ic["v"][perm], first_call=True)
     assert e.value.code == 5
+
+
+def test_timestep_sizes_formula():
+    """timestep_size.F90:95-105 on hand numbers: h = 0.1, a = (3, 4, 0), c = 1,
+    div v = -2, alpha = 1 (beta = 2): tacc = 0.5 sqrt(0.1/5), tcour =
+    0.2*0.1/((1 + 0.2) + 0.6 (1 + 0.4)) = 0.02/2.04, dt = the smaller."""
+    from oracle.oracle import timestep_sizes
+    dt = timestep_sizes([0.1, 0.1], [[3.0, 4.0, 0.0], [0.0, 0.0, 1e-8]], [-2.0, 0.0], [1.0, 1.0],
+                        1.0)
+    assert abs(dt[0] - 0.02 / 2.04) < 1e-15
+    # with |a| tiny and div v = 0 the Courant limit 0.2*0.1/(1 + 0.6) holds
+    assert abs(dt[1] - 0.02 / 1.6) < 1e-15
+
+
+def test_rk2_steps():
+    """advance_runge_kutta.F90:40-69: half step with the start forces, full
+    step from the start with the half-step velocity and forces."""
+    from oracle.oracle import rk2_full, rk2_half
+    r, v, a = np.array([[1.0, 0.0, 0.0]]), np.array([[0.0, 1.0, 0.0]]), np.array([[-1.0, 0.0, 0.0]])
+    rh, vh = rk2_half(r, v, a, 0.05)
+    assert np.allclose(rh, [[1.0, 0.05, 0.0]]) and np.allclose(vh, [[-0.05, 1.0, 0.0]])
+    r1, v1 = rk2_full(r, v, vh, -rh, 0.1)
+    assert np.allclose(r1, [[1.0 - 0.005, 0.1, 0.0]]) and np.allclose(v1, [[-0.1, 0.995, 0.0]])
