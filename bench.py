@@ -235,6 +235,40 @@ def run_resident(ic, precision, steps, warmup, ws):
     return res, state
 
 
+def run_rk2(ic, precision, steps, warmup, ws):
+    """Device-resident integration: seren_gpu_timestep then seren_gpu_rk2_step
+    (two force evaluations) per step, from the state after one force step;
+    timed with CUDA events on the library's stream, max over ranks."""
+    import torch
+
+    from seren_b200.gpu import GpuHotPath
+    n = ic["parray"].shape[0]
+    g = GpuHotPath(n, params_for(ic, precision))
+    g.upload(ic["parray"], ic["v"], ic["sound"] ** 2)
+    stream = torch.cuda.ExternalStream(g.stream())
+    g.force_step(first_call=True)
+    dts = []
+    for _ in range(max(warmup, 1)):
+        g.rk2_step(g.timestep())
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    barrier(ws)
+    start.record(stream)
+    for _ in range(steps):
+        dt = g.timestep()
+        dts.append(dt)
+        g.rk2_step(dt)
+    end.record(stream)
+    torch.cuda.synchronize()
+    barrier(ws)
+    total_ms = max_over_ranks(ws, start.elapsed_time(end))
+    g.close()
+    return dict(ms_per_step=total_ms / steps, force_evals_per_step=2,
+                value=ws * 2 * n * steps / (total_ms * 1e-3), unit=UNIT,
+                dt=[float(x) for x in dts],
+                api="seren_gpu_timestep + seren_gpu_rk2_step (courant 0.2, accel 0.5)")
+
+
 def run_e2e_io(ic, precision, steps, warmup, ws):
     """Steps through seren_gpu_force_step_io with pinned host buffers: each
     call copies parray, v and c_s^2 in from the host and parray, v, c_s^2,
@@ -572,6 +606,10 @@ def main():
         acc = dict(rms_vs_fp64=float(np.sqrt(np.mean(err ** 2))), max_vs_fp64=float(err.max()),
                    same_order=bool(same))
         log(f"[bench] fp64: {fp64['ms_per_step']:.2f} ms/step, stages {fp64['stage_ms']}, {acc}")
+    rk2 = None
+    if args.workload == "core":
+        rk2 = run_rk2(ic, 1, args.steps, args.warmup, ws)
+        log(f"[bench] rk2 step: {rk2['ms_per_step']:.2f} ms (two force evaluations), dt {rk2['dt']}")
     e2e = e2e_calls = None
     if not args.no_e2e:
         r = run_e2e_io(ic, 1, args.steps, args.warmup, ws)
@@ -641,6 +679,7 @@ def main():
         "cpu_baseline": cpu,
         "e2e": e2e,
         "e2e_reference_calls": e2e_calls,
+        "rk2_step": rk2,
         "gpu_launches": mixed["launches"],
         "clocks": clocks,
     }
