@@ -2,7 +2,9 @@
 
 The product is the CUDA library ``seren_b200/_build/libseren_gpu.so`` with the C
 ABI declared in ``include/seren_gpu.h``; ``seren_b200.gpu`` is its ctypes
-binding and ``seren_b200.ics`` generates the seeded synthetic workloads.
+binding, ``seren_b200.ics`` generates the seeded synthetic workloads and
+``seren_b200.snapshot`` reads and writes SEREN binary snapshots.
 """
 from .ics import (batched_clouds, h_fac_for, plummer, pp_gather_for,  # noqa: F401
                   protostellar_disc, turbulent_core, uniform_sphere)
+from .snapshot import read_seren_unform, to_hot_path, write_seren_unform  # noqa: F401,E402
