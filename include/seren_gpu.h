@@ -149,6 +149,20 @@ int seren_gpu_timestep(seren_gpu_ctx* ctx, double courant_mult, double accel_mul
  * seren_gpu_upload and one seren_gpu_force_step first.  Not a reference
  * entry point: it replaces sph_advance's per-particle loop for one level. */
 int seren_gpu_rk2_step(seren_gpu_ctx* ctx, double dt);
+/* Sinks that seren_gpu_rk2_step moves with the gas (sinks/advance_sink_RK.F90:
+ * 22-51, same step; their accelerations are sph_sink_forces.F90:49-110 on each
+ * step's trees): velocities [nsink][3] and radii for the sinks last given to
+ * seren_gpu_set_sinks (which stops their motion until this is called again). */
+int seren_gpu_set_sink_motion(seren_gpu_ctx* ctx, int32_t nsink, const double* sink_v,
+                              const double* sink_radius);
+/* The sinks' current state (any pointer may be NULL): x, y, z, m, h
+ * [nsink][5], v [nsink][3], acceleration [nsink][3] and potential. */
+int seren_gpu_get_sinks(seren_gpu_ctx* ctx, int32_t nsink, double* sink_rmh, double* sink_v,
+                        double* sink_a, double* sink_gpot);
+/* The least sink timestep (sinks/sink_timestep.F90:28-52: sink_mult times
+ * sqrt(radius/|a|) and radius/|v|, and the sink-sink crossing times), which
+ * sph_sim/sph_timesteps.F90:69-74 folds into the global minimum. */
+int seren_gpu_sink_timestep(seren_gpu_ctx* ctx, double sink_mult, double* dt_min);
 /* Sinks for the device-resident step: from the next seren_gpu_force_step on,
  * its gravity adds direct_sink_gravity (sinks/direct_sink_gravity.F90:10-64)
  * for sink_rmh[s] = {x, y, z, m, h}, as seren_gpu_grav_forces does with

@@ -90,6 +90,32 @@ def timestep_sizes(h, a, div_v, sound, alpha, courant_mult=0.2, accel_mult=0.5):
     return np.minimum(tacc, tcour)
 
 
+def sink_timesteps(rmh, v, a, radius, sink_mult=0.5):
+    """sinks/sink_timestep.F90:28-52 for every sink: min(sink_mult
+    sqrt(radius/(|a| + 1e-20)), sink_mult radius/(|v| + 1e-20)) and, with more
+    than one sink, sink_mult max(½(radius + radius'), distance)/(|v - v'| + 1e-20)
+    for every other sink."""
+    rmh, v, a = (np.asarray(x, np.float64).reshape(len(radius), -1) for x in (rmh, v, a))
+    radius = np.asarray(radius, np.float64)
+    out = np.zeros(len(radius))
+    for s in range(len(radius)):
+        acc = np.sqrt((a[s, 0] * a[s, 0] + a[s, 1] * a[s, 1]) + a[s, 2] * a[s, 2])
+        vel = np.sqrt((v[s, 0] * v[s, 0] + v[s, 1] * v[s, 1]) + v[s, 2] * v[s, 2])
+        dt = min(sink_mult * np.sqrt(radius[s] / (acc + 1.0e-20)),
+                 (sink_mult * radius[s]) / (vel + 1.0e-20))
+        for ss in range(len(radius)):
+            if ss == s:
+                continue
+            d = rmh[ss, 0:3] - rmh[s, 0:3]
+            dist = max(0.5 * (radius[s] + radius[ss]),
+                       np.sqrt((d[0] * d[0] + d[1] * d[1]) + d[2] * d[2]))
+            e = v[s] - v[ss]
+            dt = min(dt, (sink_mult * dist) / (np.sqrt((e[0] * e[0] + e[1] * e[1]) + e[2] * e[2]) +
+                                               1.0e-20))
+        out[s] = dt
+    return out
+
+
 def rk2_half(r, v, a, dt):
     """advance/advance_runge_kutta.F90:40-54 at the half step (dt = step/2):
     r + v dt, v + a dt."""

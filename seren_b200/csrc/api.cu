@@ -252,7 +252,7 @@ void free_all(Ctx& c) {
                 c.rs_hist, c.bbox_part, c.branch, c.branch_next, c.nchild, c.choff, c.cstart,
                 c.bflag, c.bscan, c.leaf, c.nextcell, c.ifopen, c.pstart, c.pcount, c.parent,
                 c.level, c.nkids, c.work, c.sinks, c.wstack, c.leaves, c.nleaf, c.npot, c.redo, c.wide, c.wst, c.wacc, c.link, c.gA, c.gB, c.gC, c.wA, c.hN, c.hA, c.hrm, c.hA32, c.hrm32, c.hmax, c.bbmin, c.bbmax, c.d_info,
-                c.d_err, c.d_counts, c.tabA, c.tabG, c.tabG32, c.scan.total, c.scan.level_buf[0],
+                c.d_err, c.d_counts, c.sink_out, c.tabA, c.tabG, c.tabG32, c.scan.total, c.scan.level_buf[0],
                 c.scan.level_buf[1], c.scan.level_buf[2], c.scan.level_buf[3]};
   for (void* p : ps)
     if (p) cudaFree(p);
@@ -297,7 +297,8 @@ int alloc_all(Ctx& c) {
   bad |= alloc(c.gA, C) | alloc(c.gB, C) | alloc(c.gC, C) | alloc(c.wA, 2 * C) | alloc(c.hN, 2 * C) |
          alloc(c.hA, C) | alloc(c.hrm, C) |
          alloc(c.hmax, C) | alloc(c.bbmin, C) | alloc(c.bbmax, C);
-  bad |= alloc(c.d_info, 1) | alloc(c.d_err, 1) | alloc(c.d_counts, 32) | alloc(c.sinks, 5 * 1024);
+  bad |= alloc(c.d_info, 1) | alloc(c.d_err, 1) | alloc(c.d_counts, 32) | alloc(c.sinks, 5 * 1024) |
+         alloc(c.sink_out, 4 * 1024);
   bad |= alloc(c.tabA, KERNTOT + 1) | alloc(c.tabG, KERNTOT + 1) | alloc(c.tabG32, KERNTOT + 1);
   c.wstack_slots = std::max(grav_walk_slots(c), hydro_walk_slots(c));
   c.wstack_cap = grav_walk_stack_cap(c);
@@ -743,6 +744,7 @@ int force_step_body(Ctx& c, int first_call, const IoPlan* io) {
   const int n = c.ptot;
   const size_t N = (size_t)n;
   c.act = nullptr;
+  c.sink_a_valid = false;                    // a new tree: the sinks' accelerations are stale
   cudaMemsetAsync(c.d_counts, 0, sizeof(int) * 32, c.st);
   cudaEventRecord(c.ev[0], c.st);
   int rc = build_tree(c);
@@ -875,7 +877,115 @@ int seren_gpu_set_sinks(seren_gpu_ctx* h, int32_t nsink, const double* sink_rmh)
   if (nsink > 0)
     cudaMemcpyAsync(c.sinks, sink_rmh, sizeof(double) * 5 * nsink, cudaMemcpyHostToDevice, c.st);
   c.nsink = nsink;
+  c.sink_rmh.assign(sink_rmh, sink_rmh + 5 * (size_t)nsink);
+  c.sink_move = false;                       // velocities again with seren_gpu_set_sink_motion
+  c.sink_a_valid = false;
   return finish(c, "set_sinks");
+}
+
+namespace seren {
+namespace {
+
+// the sinks' accelerations and potentials (sph_sink_forces.F90:49-110) on the
+// current tree, into the host copies
+int sink_accels(Ctx& c) {
+  launch_sink_walk(c, c.nsink, c.sinks, c.sink_out);
+  std::vector<double> out((size_t)c.nsink * 4);
+  cudaMemcpyAsync(out.data(), c.sink_out, sizeof(double) * out.size(), cudaMemcpyDeviceToHost, c.st);
+  const int rc = finish(c, "sink accelerations");
+  if (rc) return rc;
+  c.sink_a.resize((size_t)c.nsink * 3);
+  c.sink_pot.resize((size_t)c.nsink);
+  for (int s = 0; s < c.nsink; ++s) {
+    for (int k = 0; k < 3; ++k) c.sink_a[s * 3 + k] = out[s * 4 + k];
+    c.sink_pot[s] = out[s * 4 + 3];
+  }
+  c.sink_a_valid = true;
+  return SEREN_GPU_OK;
+}
+
+int sink_upload(Ctx& c) {
+  cudaMemcpyAsync(c.sinks, c.sink_rmh.data(), sizeof(double) * 5 * (size_t)c.nsink,
+                  cudaMemcpyHostToDevice, c.st);
+  return SEREN_GPU_OK;
+}
+
+}  // namespace
+}  // namespace seren
+
+int seren_gpu_set_sink_motion(seren_gpu_ctx* h, int32_t nsink, const double* sink_v,
+                              const double* sink_radius) {
+  if (!h) return SEREN_GPU_ERR_ARG;
+  Ctx& c = h->c;
+  if (nsink < 1 || nsink != c.nsink || !sink_v || !sink_radius)
+    return fail(c, SEREN_GPU_ERR_ARG, "set_sink_motion: nsink as in seren_gpu_set_sinks, arrays given");
+  c.sink_v.assign(sink_v, sink_v + 3 * (size_t)nsink);
+  c.sink_radius.assign(sink_radius, sink_radius + (size_t)nsink);
+  c.sink_move = true;
+  return SEREN_GPU_OK;
+}
+
+int seren_gpu_get_sinks(seren_gpu_ctx* h, int32_t nsink, double* sink_rmh, double* sink_v,
+                        double* sink_a, double* sink_gpot) {
+  if (!h) return SEREN_GPU_ERR_ARG;
+  Ctx& c = h->c;
+  if (nsink < 1 || nsink != c.nsink) return fail(c, SEREN_GPU_ERR_ARG, "get_sinks: nsink differs");
+  if ((sink_a || sink_gpot) && !c.sink_a_valid) {
+    if (!c.have_tree) return fail(c, SEREN_GPU_ERR_STATE, "get_sinks: no tree for the accelerations");
+    const int rc = seren::sink_accels(c);
+    if (rc) return rc;
+  }
+  const size_t n = (size_t)nsink;
+  if (sink_rmh) std::memcpy(sink_rmh, c.sink_rmh.data(), sizeof(double) * 5 * n);
+  if (sink_v) {
+    if (c.sink_v.size() < 3 * n) return fail(c, SEREN_GPU_ERR_STATE, "get_sinks: no sink velocities");
+    std::memcpy(sink_v, c.sink_v.data(), sizeof(double) * 3 * n);
+  }
+  if (sink_a) std::memcpy(sink_a, c.sink_a.data(), sizeof(double) * 3 * n);
+  if (sink_gpot) std::memcpy(sink_gpot, c.sink_pot.data(), sizeof(double) * n);
+  return SEREN_GPU_OK;
+}
+
+int seren_gpu_sink_timestep(seren_gpu_ctx* h, double sink_mult, double* dt_min) {
+  if (!h) return SEREN_GPU_ERR_ARG;
+  Ctx& c = h->c;
+  if (!dt_min || !(sink_mult > 0.0)) return fail(c, SEREN_GPU_ERR_ARG, "sink_timestep: bad arguments");
+  if (!c.sink_move) return fail(c, SEREN_GPU_ERR_STATE, "sink_timestep: call seren_gpu_set_sink_motion");
+  if (!c.sink_a_valid) {
+    if (!c.have_tree) return fail(c, SEREN_GPU_ERR_STATE, "sink_timestep: no tree");
+    const int rc = seren::sink_accels(c);
+    if (rc) return rc;
+  }
+  // sinks/sink_timestep.F90:28-52, the least over the sinks (sph_timesteps.F90:69-74)
+  double best = 1.0e300;
+  for (int s = 0; s < c.nsink; ++s) {
+    const double rads = c.sink_radius[s];
+    const double* as = &c.sink_a[s * 3];
+    const double* vs = &c.sink_v[s * 3];
+    const double* rs = &c.sink_rmh[s * 5];
+    const double acc_mag = std::sqrt((as[0] * as[0] + as[1] * as[1]) + as[2] * as[2]);
+    double vel_mag = std::sqrt((vs[0] * vs[0] + vs[1] * vs[1]) + vs[2] * vs[2]);
+    const double dt1 = sink_mult * std::sqrt(rads / (acc_mag + 1.0e-20));
+    double dt2 = (sink_mult * rads) / (vel_mag + 1.0e-20);
+    double dt = std::min(dt1, dt2);
+    if (c.nsink > 1) {
+      for (int ss = 0; ss < c.nsink; ++ss) {
+        if (ss == s) continue;
+        const double* rss = &c.sink_rmh[ss * 5];
+        const double d0 = rss[0] - rs[0], d1 = rss[1] - rs[1], d2 = rss[2] - rs[2];
+        const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
+        const double dist = std::max(0.5 * (rads + c.sink_radius[ss]), std::sqrt(drsqd));
+        const double* vss = &c.sink_v[ss * 3];
+        const double e0 = vs[0] - vss[0], e1 = vs[1] - vss[1], e2 = vs[2] - vss[2];
+        vel_mag = std::sqrt((e0 * e0 + e1 * e1) + e2 * e2);
+        dt2 = (sink_mult * dist) / (vel_mag + 1.0e-20);
+        dt = std::min(dt, dt2);
+      }
+    }
+    best = std::min(best, dt);
+  }
+  *dt_min = best;
+  return SEREN_GPU_OK;
 }
 
 int seren_gpu_timestep(seren_gpu_ctx* h, double courant_mult, double accel_mult, double* dt_min,
@@ -918,17 +1028,48 @@ int seren_gpu_rk2_step(seren_gpu_ctx* h, double dt) {
   }
   const int n = c.ptot;
   c.nlaunch = 0;
+  // sinks set in motion move with the same scheme (sinks/advance_sink_RK.F90:22-51)
+  const bool sinks = c.sink_move && c.nsink > 0;
+  int rc = SEREN_GPU_OK;
+  if (sinks && !c.sink_a_valid && (rc = seren::sink_accels(c))) return rc;
+  const size_t ns = (size_t)c.nsink;
   // first half (advance_runge_kutta.F90:40-54) with the forces at the start
   seren::k_rk_half<<<nb(n, 256), 256, 0, c.st>>>(n, c.pm, c.vel, c.acc, c.r_old, c.v_old,
                                                   c.v_half, 0.5 * dt);
   ++c.nlaunch;
-  int rc = seren::force_step_body(c, 0, nullptr);             // forces at the half step
+  if (sinks) {
+    c.sink_rold.resize(3 * ns);
+    c.sink_vold.resize(3 * ns);
+    c.sink_vhalf.resize(3 * ns);
+    const double hdt = 0.5 * dt;
+    for (size_t s = 0; s < ns; ++s)
+      for (int k = 0; k < 3; ++k) {
+        c.sink_rold[s * 3 + k] = c.sink_rmh[s * 5 + k];
+        c.sink_vold[s * 3 + k] = c.sink_v[s * 3 + k];
+        c.sink_rmh[s * 5 + k] = c.sink_rold[s * 3 + k] + c.sink_vold[s * 3 + k] * hdt;
+        c.sink_v[s * 3 + k] = c.sink_vold[s * 3 + k] + c.sink_a[s * 3 + k] * hdt;
+        c.sink_vhalf[s * 3 + k] = c.sink_v[s * 3 + k];
+      }
+    seren::sink_upload(c);
+  }
+  rc = seren::force_step_body(c, 0, nullptr);                 // forces at the half step
   if (rc) return rc;
+  if (sinks && (rc = seren::sink_accels(c))) return rc;
   // second half (:56-69) from the start with v_half and the half-step forces
   seren::k_rk_full<<<nb(n, 256), 256, 0, c.st>>>(n, c.pm, c.vel, c.acc, c.r_old, c.v_old,
                                                   c.v_half, dt);
   ++c.nlaunch;
-  return seren::force_step_body(c, 0, nullptr);               // forces at the end
+  if (sinks) {
+    for (size_t s = 0; s < ns; ++s)
+      for (int k = 0; k < 3; ++k) {
+        c.sink_rmh[s * 5 + k] = c.sink_rold[s * 3 + k] + c.sink_vhalf[s * 3 + k] * dt;
+        c.sink_v[s * 3 + k] = c.sink_vold[s * 3 + k] + c.sink_a[s * 3 + k] * dt;
+      }
+    seren::sink_upload(c);
+  }
+  rc = seren::force_step_body(c, 0, nullptr);                 // forces at the end
+  if (rc) return rc;
+  return sinks ? seren::sink_accels(c) : SEREN_GPU_OK;
 }
 
 int seren_gpu_drift(seren_gpu_ctx* h, double dt) {

@@ -120,6 +120,14 @@ struct Ctx {
   int* work = nullptr;        // work counter of the persistent kernels
   double* sinks = nullptr;    // [1024][5] sinks of the device-resident step (x, y, z, m, h)
   int nsink = 0;
+  double* sink_out = nullptr; // [1024][4] sink accelerations and potentials of the last walk
+  // sinks that seren_gpu_rk2_step moves (seren_gpu_set_sink_motion): host
+  // copies of their state, [nsink][5] x y z m h, [nsink][3] v and a, radius,
+  // potential, and the Runge-Kutta start and half-step values
+  bool sink_move = false;
+  bool sink_a_valid = false;
+  std::vector<double> sink_rmh, sink_v, sink_a, sink_pot, sink_radius, sink_rold, sink_vold,
+      sink_vhalf;
   int* leaves = nullptr;      // [pmax][256] opened leaves of each particle's grad-h walk
   int* nleaf = nullptr;       // their number (-1: overflow)
   int* npot = nullptr;        // [pmax] particles in those leaves (pp_pot)

@@ -38,6 +38,9 @@ def library(build_if_missing: bool = True) -> C.CDLL:
                            ("drift", [vp, C.c_double]),
                            ("timestep", [vp, C.c_double, C.c_double, _dp, _dp]),
                            ("rk2_step", [vp, C.c_double]),
+                           ("set_sink_motion", [vp, C.c_int32, _dp, _dp]),
+                           ("get_sinks", [vp, C.c_int32, _dp, _dp, _dp, _dp]),
+                           ("sink_timestep", [vp, C.c_double, _dp]),
                            ("set_sinks", [vp, C.c_int32, _dp]),
                            ("download", [vp, _dp, _dp, _dp, _dp, _dp, _dp, _ip]),
                            ("last_step_stats", [vp, _dp, _ip, C.POINTER(C.c_int64)]),
@@ -92,6 +95,27 @@ class GpuHotPath(HotPath):
         s = None if sinks is None else np.ascontiguousarray(np.atleast_2d(sinks), dtype=np.float64)
         ns = 0 if s is None else s.shape[0]
         self._call("set_sinks", self._ctx, ns, None if s is None else _d(s))
+        self.nsink = ns
+
+    def set_sink_motion(self, v, radius):
+        """Velocities [nsink][3] and radii of the sinks, which rk2_step then
+        moves with the gas."""
+        v = np.ascontiguousarray(np.atleast_2d(v), dtype=np.float64)
+        radius = np.ascontiguousarray(np.atleast_1d(radius), dtype=np.float64)
+        self._call("set_sink_motion", self._ctx, v.shape[0], _d(v), _d(radius))
+
+    def get_sinks(self):
+        ns = self.nsink
+        out = dict(rmh=np.zeros((ns, 5)), v=np.zeros((ns, 3)), a=np.zeros((ns, 3)),
+                   gpot=np.zeros(ns))
+        self._call("get_sinks", self._ctx, ns, _d(out["rmh"]), _d(out["v"]), _d(out["a"]),
+                   _d(out["gpot"]))
+        return out
+
+    def sink_timestep(self, sink_mult=0.5):
+        d = C.c_double()
+        self._call("sink_timestep", self._ctx, C.c_double(sink_mult), C.byref(d))
+        return d.value
 
     def drift(self, dt: float):
         self._call("drift", self._ctx, C.c_double(dt))

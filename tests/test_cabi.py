@@ -39,7 +39,8 @@ def test_oracle_mirrors_the_abi():
         tail = n[len("seren_gpu_"):]
         if tail in ("upload", "force_step", "force_step_io", "drift", "download",
                     "last_step_stats", "get_stream", "fma_peak", "hydro_forces_noalloc",
-                    "set_sinks", "timestep", "rk2_step"):
+                    "set_sinks", "timestep", "rk2_step", "set_sink_motion", "get_sinks",
+                    "sink_timestep"):
             continue          # device-resident path (timestep / rk2: numpy restatements in
                               # oracle.py), device-buffer call, GPU-only introspection
         assert hasattr(lib, "seren_oracle_" + tail), tail
