@@ -269,7 +269,7 @@ struct GwRec {
   typename T::R4 pa[T::PREP];      // particle: mixed (r_q - r_ref, m), FP64 (r_q, m)
   typename T::R2 pb[T::PREP];      // mixed (1/h, zeta), FP64 (h, zeta)
   float4 fw[32];                   // popped cells: wA
-  float flo[32];                   // wLo
+  float flo[32];                   // lower MAC bracket
   unsigned ftest[32];              // lanes that test the cell (0 for one-particle leaves)
   int fcell[32];
   int fund[32];                    // popped cells the group test leaves undecided
