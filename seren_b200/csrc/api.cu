@@ -246,7 +246,8 @@ int check_tree(Ctx& c, int32_t ptot) {
 
 void free_all(Ctx& c) {
   void* ps[] = {c.pm, c.hz, c.vel, c.csq, c.orig, c.pm_alt, c.hz_alt, c.vel_alt, c.csq_alt,
-                c.orig_alt, c.rho, c.omega, c.div_v, c.drhodt, c.press, c.sound, c.acc, c.gpot,
+                c.orig_alt, c.rho, c.omega, c.div_v, c.drhodt, c.rho_alt, c.omega_alt, c.div_v_alt,
+                c.drhodt_alt, c.press, c.sound, c.acc, c.gpot,
                 c.pf, c.hf4,
                 c.pptot, c.pplist, c.stage, c.istage, c.keys, c.keys_alt, c.idx, c.idx_alt,
                 c.rs_hist, c.bbox_part, c.branch, c.branch_next, c.nchild, c.choff, c.cstart,
@@ -279,6 +280,8 @@ int alloc_all(Ctx& c) {
   bad |= alloc(c.pm, P) | alloc(c.hz, P) | alloc(c.vel, P) | alloc(c.csq, P) | alloc(c.orig, P);
   bad |= alloc(c.pm_alt, P) | alloc(c.hz_alt, P) | alloc(c.vel_alt, P) | alloc(c.csq_alt, P) |
          alloc(c.orig_alt, P);
+  bad |= alloc(c.rho_alt, P) | alloc(c.omega_alt, P) | alloc(c.div_v_alt, P) |
+         alloc(c.drhodt_alt, P);
   bad |= alloc(c.rho, P) | alloc(c.omega, P) | alloc(c.div_v, P) | alloc(c.drhodt, P) |
          alloc(c.press, P) | alloc(c.sound, P) | alloc(c.acc, 3 * P) | alloc(c.gpot, P) |
          alloc(c.pf, P) | alloc(c.hf4, P);

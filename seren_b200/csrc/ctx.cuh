@@ -41,6 +41,12 @@ struct Ctx {
   double* omega = nullptr;
   double* div_v = nullptr;
   double* drhodt = nullptr;
+  // reorder targets of rho, omega, div_v, drhodt: a tree build permutes them
+  // with the particles, as main/reorder_array.F90 does the host's arrays
+  double* rho_alt = nullptr;
+  double* omega_alt = nullptr;
+  double* div_v_alt = nullptr;
+  double* drhodt_alt = nullptr;
   double* press = nullptr;
   double* sound = nullptr;
   double* acc = nullptr;     // [ptot][3]

@@ -395,6 +395,20 @@ __global__ void k_reorder_vc(const int* __restrict__ perm, int n, const double4*
   csq2[i] = csq[p];
 }
 
+__global__ void k_reorder_sph(const int* __restrict__ perm, int n, const double* __restrict__ a,
+                              const double* __restrict__ b, const double* __restrict__ c,
+                              const double* __restrict__ d, double* __restrict__ a2,
+                              double* __restrict__ b2, double* __restrict__ c2,
+                              double* __restrict__ d2) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int p = perm[i];
+  a2[i] = a[p];
+  b2[i] = b[p];
+  c2[i] = c[p];
+  d2[i] = d[p];
+}
+
 __global__ void k_reorder_rk(const int* __restrict__ perm, int n, const double4* __restrict__ a,
                              const double4* __restrict__ b, const double4* __restrict__ c,
                              double4* __restrict__ a2, double4* __restrict__ b2,
@@ -779,6 +793,15 @@ int build_tree(Ctx& c) {
   std::swap(c.pm, c.pm_alt);
   std::swap(c.hz, c.hz_alt);
   std::swap(c.orig, c.orig_alt);
+  // rho, omega, div v, drho/dt of the last evaluation follow the particles
+  // (main/reorder_array.F90): particles left out of an active subset keep theirs
+  k_reorder_sph<<<nb(n, 256), 256, 0, c.st>>>(c.idx, n, c.rho, c.omega, c.div_v, c.drhodt,
+                                               c.rho_alt, c.omega_alt, c.div_v_alt,
+                                               c.drhodt_alt); ++c.nlaunch;
+  std::swap(c.rho, c.rho_alt);
+  std::swap(c.omega, c.omega_alt);
+  std::swap(c.div_v, c.div_v_alt);
+  std::swap(c.drhodt, c.drhodt_alt);
   if (c.r_old) {                            // Runge-Kutta state follows the particles
     k_reorder_rk<<<nb(n, 256), 256, 0, c.st>>>(c.idx, n, c.r_old, c.v_old, c.v_half, c.r_old_alt,
                                                 c.v_old_alt, c.v_half_alt); ++c.nlaunch;

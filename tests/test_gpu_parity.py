@@ -463,3 +463,43 @@ def test_rk2_step_with_a_moving_sink_matches_oracle(libs):
     assert np.abs(s1["rmh"][:, 0:3] - sx1).max() < 1e-13
     assert rel_rows(s1["v"], sv1).max() < 1e-11
     assert rel_rows(s1["a"], sa1).max() < 1e-9
+
+
+def test_active_subset_after_a_rebuild(libs):
+    """Block-timestep use of the reference-shaped calls: after a first full
+    evaluation the particles move, the tree is rebuilt (the host permutes its
+    arrays), and only every third particle is updated.  The inactive particles'
+    rho, omega (the neighbours' values the active particles' hydro reads) must
+    follow the reorder, as main/reorder_array.F90 permutes them."""
+    ic = case("turb20k")
+    o, g = _pair(libs, ic)
+    n = ic["parray"].shape[0]
+    r0 = run_pipeline(o, ic)
+    rg0 = run_pipeline(g, ic)
+    assert np.array_equal(r0["perm"], rg0["perm"])
+    p1 = r0["sph"]["parray"].copy()
+    v0 = ic["v"][r0["perm"]]
+    p1[:, 0:3] += 2e-3 * v0
+    po, permo = o.tree_update(p1)
+    pg, permg = g.tree_update(p1)
+    assert np.array_equal(permo, permg)
+    v1 = v0[permo]
+    act = np.arange(0, n, 3, dtype=np.int32)
+    so = o.sph_update(po, v1, acclist=act)
+    sg = g.sph_update(pg, v1, acclist=act)
+    for k in ("rho", "omega"):
+        assert rel_rows(sg[k][act], so[k][act]).max() < TOL, k
+    for k in ("div_v", "drhodt"):                   # they pass through zero
+        assert rel_scaled(sg[k][act], so[k][act]) < TOL, k
+    assert rel_rows(sg["parray"][act, 4], so["parray"][act, 4]).max() < TOL
+    # the host's rho: the previous values, permuted, with the active rows new
+    rho = r0["sph"]["rho"][permo].copy()
+    rho[act] = so["rho"][act]
+    sound = r0["sound"][permo]
+    press = sound * sound * rho
+    ao = o.hydro_forces(press, sound, acclist=act)
+    ag = g.hydro_forces(press, sound, acclist=act)
+    assert rel_scaled(ag[act], ao[act]) < TOL
+    go, _ = o.grav_forces(ao, acclist=act)
+    gg, _ = g.grav_forces(ag, acclist=act)
+    assert rel_rows(gg[act], go[act]).max() < 1e-11
