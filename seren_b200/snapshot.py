@@ -1,7 +1,9 @@
 """SEREN binary snapshots (format id SERENBINARYDUMPV2) read and written in
 the layout of io/write_data_seren_unform.F90 and io/read_data_seren_unform.F90,
-so that snapshots of the Fortran code can feed the GPU path and its results
-can be read back by the Fortran tools.
+and DRAGON snapshots (binary and ASCII, io/read_data_dragon_unform.F90,
+io/read_data_dragon_form.F90 and their writers), so that snapshots of the
+Fortran code can feed the GPU path and its results can be read back by the
+Fortran tools.
 
 The files are Fortran unformatted sequential files: every record is framed by
 a 4-byte length before and after it; a record longer than 2**31 - 9 bytes is
@@ -280,3 +282,282 @@ def to_hot_path(snap: Dict):
     if snap.get("sinks"):
         sinks = np.array([[*s["r"][0:3], s["m"], s["h"]] for s in snap["sinks"]])
     return parray, v, sinks
+
+
+# ---------------------------------------------------------------------------
+# DRAGON snapshots
+#
+# Layout (write_data_dragon_unform.F90:44-271, write_data_dragon_form.F90:34-171):
+#   idata(20) int | rdata(50) real | positions (NDIM per particle) |
+#   velocities (VDIM per particle) | temperatures | h | rho | m | types (int) |
+#   particle ids (int, PARTICLE_ID builds only)
+# with ptot + stot entries in every per-particle block, the sinks last.  In the
+# binary file each block is one Fortran record (reals of kind PR); in the ASCII
+# file every value or particle vector is one list-directed record (line).
+# idata(1) = entries, idata(2) = nsteps, idata(3) = gas entries, idata(4) =
+# snapshot, idata(20) = pgas_orig; rdata(1) = time, rdata(2) = lastsnap,
+# rdata(50) = mgas_orig.  Types: 1 gas, 6 boundary, 9 intercloud, 10 dark
+# matter (ASCII reader only), -1 sink, 0 accreted (dropped), 4 split (refused).
+
+DRAGON_GAS, DRAGON_BOUNDARY, DRAGON_ICM, DRAGON_CDM = 1, 6, 9, 10
+DRAGON_SINK, DRAGON_DEAD, DRAGON_SPLIT = -1, 0, 4
+_KERNRANGE = 2.0                 # sink radius = KERNRANGE * h for DRAGON sinks
+_DRAGON_TRESTR = 1000.0          # write_data_dragon_unform.F90:31-32 (cgs)
+_DRAGON_RHORESTR = 1.0e-13
+
+
+def _dragon_assemble(idata, rdata, pos, vel, temp, h, rho, m, ptype, ids, with_cdm: bool,
+                     rounding=None) -> Dict:
+    """Sort DRAGON entries into SEREN's particle order: boundary, intercloud,
+    gas (and dark matter for the ASCII reader), each in file order; sinks
+    apart; accreted entries dropped (read_data_dragon_unform.F90:91-116 and
+    135-343, read_data_dragon_form.F90:81-113 and 143-371).  Without ids, a
+    particle's porig is its 1-based position in the file, as the reference
+    sets it when no restart log exists."""
+    ntot = int(idata[0])
+    ptype = np.asarray(ptype).astype(np.int64)
+    counts = {t: int(np.count_nonzero(ptype == t)) for t in
+              (DRAGON_SINK, DRAGON_DEAD, DRAGON_GAS, DRAGON_SPLIT, DRAGON_BOUNDARY, DRAGON_ICM,
+               DRAGON_CDM)}
+    stot, pdead = counts[DRAGON_SINK], counts[DRAGON_DEAD]
+    ptot = ntot - (stot + pdead)
+    if counts[DRAGON_SPLIT] != 0:
+        raise ValueError("particle splitting not supported (DRAGON type 4)")
+    kinds = [DRAGON_BOUNDARY, DRAGON_ICM, DRAGON_GAS] + ([DRAGON_CDM] if with_cdm else [])
+    if ptot != sum(counts[t] for t in kinds):
+        raise ValueError("particles do not add up (types other than "
+                         + ", ".join(str(t) for t in kinds) + ", -1 and 0 present)")
+    order = np.concatenate([np.flatnonzero(ptype == t) for t in kinds]) if ptot else \
+        np.zeros(0, np.int64)
+    sk = np.flatnonzero(ptype == DRAGON_SINK)
+    rnd = (lambda a: a) if rounding is None else rounding
+    out: Dict = dict(format_id="DRAGON", idata=np.asarray(idata), rdata=np.asarray(rdata),
+                     ptot=ptot, stot=stot, pdead=pdead, pboundary=counts[DRAGON_BOUNDARY],
+                     picm=counts[DRAGON_ICM], pgas=counts[DRAGON_GAS],
+                     pcdm=counts[DRAGON_CDM] if with_cdm else 0,
+                     nsteps=int(idata[1]), snapshot=int(idata[3]), pgas_orig=int(idata[19]),
+                     time=float(rnd(rdata[0])), lastsnap=float(rnd(rdata[1])),
+                     mgas_orig=float(rnd(rdata[49])))
+    out["r"] = pos[order].astype(np.float64)
+    out["v"] = vel[order].astype(np.float64)
+    out["temp"] = temp[order].astype(np.float64)
+    out["h"] = h[order].astype(np.float64)
+    out["rho"] = rho[order].astype(np.float64)
+    out["m"] = m[order].astype(np.float64)
+    out["ptype"] = ptype[order].astype(np.int32)
+    out["porig"] = (np.asarray(ids)[order].astype(np.int32) if ids is not None
+                    else (order + 1).astype(np.int32))
+    # sink fields the DRAGON format does not hold take the reader's defaults
+    # (read_data_dragon_unform.F90:341-349)
+    out["sinks"] = [dict(r=pos[s].astype(np.float64), v=vel[s].astype(np.float64),
+                         m=float(m[s]), h=float(h[s]), radius=_KERNRANGE * float(h[s]),
+                         accrete=True, static=False) for s in sk]
+    return out
+
+
+def read_dragon_unform(path: str, ids: bool = False, ndim: int = 3) -> Dict:
+    """A binary DRAGON snapshot (read_data_dragon_unform.F90:9-364) as a dict
+    with the keys of read_seren_unform's particle blocks (r, v, temp, h, rho,
+    m, porig, ptype), the counts and the sinks.  The real kind (4 or 8 bytes)
+    is taken from the length of the rdata record.  ids=True reads porig from
+    the id record (a PARTICLE_ID build restarting a run); otherwise porig is
+    the file position.  Dark-matter entries (type 10) are refused, as this
+    reader of the reference counts no dark matter."""
+    with open(path, "rb") as f:
+        rec = _read_record(f)
+        if len(rec) != 80:
+            raise ValueError(f"not a DRAGON snapshot (idata record of {len(rec)} bytes)")
+        idata = np.frombuffer(rec, "<i4").copy()
+        rec = _read_record(f)
+        if len(rec) not in (200, 400):
+            raise ValueError(f"not a DRAGON snapshot (rdata record of {len(rec)} bytes)")
+        real = np.dtype("<f4") if len(rec) == 200 else np.dtype("<f8")
+        rdata = np.frombuffer(rec, real).copy()
+        n = int(idata[0])
+        if n < 0:
+            raise ValueError("negative particle count in a DRAGON header")
+
+        def block(dt, comp):
+            a = np.frombuffer(_read_record(f), dt)
+            if a.size != n * comp:
+                raise ValueError(f"DRAGON block holds {a.size} values, expected {n * comp}")
+            return a.reshape(n, comp) if comp > 1 else a.copy()
+
+        pos = block(real, ndim)
+        vel = block(real, ndim)
+        temp, h, rho, m = (block(real, 1) for _ in range(4))
+        ptype = block("<i4", 1)
+        idv = block("<i4", 1) if ids else None
+    return _dragon_assemble(idata, rdata, pos, vel, temp, h, rho, m, ptype, idv,
+                            with_cdm=False)
+
+
+class _ListDirected:
+    """Fortran list-directed input over a text file: every read statement
+    starts on a new record (line), takes values from as many lines as it
+    needs and drops the rest of its last line; values are separated by
+    blanks or commas; r*c repeats c r times; D exponents are accepted."""
+
+    def __init__(self, text: str):
+        self.lines = text.splitlines()
+        self.i = 0
+
+    def read(self, n: int) -> List[str]:
+        vals: List[str] = []
+        while len(vals) < n:
+            if self.i >= len(self.lines):
+                raise EOFError("end of file in a list-directed read")
+            line = self.lines[self.i]
+            self.i += 1
+            for tok in line.replace(",", " ").split():
+                if "*" in tok:
+                    k, _, v = tok.partition("*")
+                    vals.extend([v] * int(k))
+                else:
+                    vals.append(tok)
+        return vals[:n]
+
+    def reals(self, n: int) -> List[float]:
+        return [float(t.replace("D", "E").replace("d", "e")) for t in self.read(n)]
+
+
+def read_dragon_form(path: str, ids: bool = False, ndim: int = 3) -> Dict:
+    """An ASCII DRAGON snapshot (read_data_dragon_form.F90:9-396) as a dict
+    like read_dragon_unform's.  The reference reads every real value of this
+    format into a single-precision variable, so positions, velocities, h, rho,
+    m, temperatures and the header times come back rounded to float32 and
+    widened again, as in the reference; types are read as reals and
+    truncated.  Dark matter (type 10) is accepted and placed after the gas."""
+    with open(path, "r") as f:
+        rd = _ListDirected(f.read())
+    idata = np.array([int(rd.read(1)[0]) for _ in range(20)], np.int64)
+    rdata = np.array([rd.reals(1)[0] for _ in range(50)], np.float64).astype(np.float32)
+    n = int(idata[0])
+    if n < 0:
+        raise ValueError("negative particle count in a DRAGON header")
+    sp = np.float32
+    pos = np.array([rd.reals(ndim) for _ in range(n)], np.float64).reshape(n, ndim).astype(sp)
+    vel = np.array([rd.reals(ndim) for _ in range(n)], np.float64).reshape(n, ndim).astype(sp)
+    temp, h, rho, m = (np.array([rd.reals(1)[0] for _ in range(n)], np.float64).astype(sp)
+                       for _ in range(4))
+    ptype = np.trunc(np.array([rd.reals(1)[0] for _ in range(n)], np.float64).astype(sp))
+    idv = None
+    if ids:
+        idv = np.array([int(rd.read(1)[0]) for _ in range(n)], np.int64)
+    return _dragon_assemble(idata, rdata.astype(np.float64), pos, vel, temp, h, rho, m,
+                            ptype.astype(np.int64), idv, with_cdm=True)
+
+
+def _dragon_columns(r, m, h, v, rho, temp, ptype, porig, sinks, scales):
+    r = np.asarray(r, np.float64).reshape(-1, 3)
+    n = r.shape[0]
+    v = np.asarray(v, np.float64).reshape(n, 3)
+    m, h, rho = (np.asarray(x, np.float64).reshape(n) for x in (m, h, rho))
+    temp = np.zeros(n) if temp is None else np.asarray(temp, np.float64).reshape(n)
+    ptype = np.full(n, DRAGON_GAS, np.int32) if ptype is None else \
+        np.asarray(ptype, np.int32).reshape(n)
+    porig = np.arange(1, n + 1, dtype=np.int32) if porig is None else \
+        np.asarray(porig, np.int32).reshape(n)
+    sinks = sinks or []
+    rs, vs, ms, rhos = scales["rscale"], scales["vscale"], scales["mscale"], scales["rhoscale"]
+    cols = dict(r=r * rs, v=v * vs, temp=temp, h=h * rs, rho=rho * rhos, m=m * ms, ptype=ptype,
+                porig=porig)
+    if sinks:
+        cols["r"] = np.vstack([cols["r"], [np.asarray(s["r"], np.float64) * rs for s in sinks]])
+        cols["v"] = np.vstack([cols["v"], [np.asarray(s.get("v", (0.0, 0.0, 0.0)), np.float64)
+                                           * vs for s in sinks]])
+        cols["temp"] = np.concatenate([cols["temp"], np.zeros(len(sinks))])
+        cols["h"] = np.concatenate([cols["h"], [s["h"] * rs for s in sinks]])
+        cols["rho"] = np.concatenate([cols["rho"], np.full(len(sinks),
+                                                           scales["rhosink"] * rhos)])
+        cols["m"] = np.concatenate([cols["m"], [s["m"] * ms for s in sinks]])
+        cols["ptype"] = np.concatenate([cols["ptype"], np.full(len(sinks), DRAGON_SINK,
+                                                               np.int32)])
+        cols["porig"] = np.concatenate([cols["porig"], np.zeros(len(sinks), np.int32)])
+    return n, len(sinks), cols
+
+
+def _dragon_header(entries, gas_entries, nsteps, snapshot, pgas_orig, time, lastsnap,
+                   mgas_orig, tscale, mscale):
+    idata = np.zeros(20, np.int64)
+    idata[0], idata[1], idata[2], idata[3], idata[19] = (entries, nsteps, gas_entries, snapshot,
+                                                         pgas_orig)
+    rdata = np.zeros(50, np.float64)
+    rdata[0], rdata[1], rdata[49] = time * tscale, lastsnap * tscale, mgas_orig * mscale
+    return idata, rdata
+
+
+def write_dragon_unform(path: str, r, m, h, v, rho, temp=None, ptype=None, porig=None,
+                        sinks: Optional[List[Dict]] = None, pr: int = 4, ids: bool = False,
+                        time: float = 0.0, lastsnap: float = 0.0, snapshot: int = 0,
+                        nsteps: int = 0, pgas_orig: Optional[int] = None,
+                        mgas_orig: Optional[float] = None, rhosink: float = 0.0,
+                        rscale: float = 1.0, vscale: float = 1.0, mscale: float = 1.0,
+                        rhoscale: float = 1.0, tscale: float = 1.0) -> int:
+    """Write a binary DRAGON snapshot as write_data_dragon_unform.F90 does,
+    including its density-temperature cut: only particles with
+    rho * rhoscale > 1e-13 or temp < 1000 are written (:57-67), then the sinks
+    (type -1, temperature 0, density rhosink).  Particles must come in SEREN's
+    order (boundary, intercloud, gas); their types are written for the kept
+    particles in that order (the reference offsets the intercloud and gas types
+    by the uncut boundary and intercloud counts, which is the same whenever
+    the cut keeps every boundary and intercloud particle).  ids=True adds the
+    id record of a PARTICLE_ID build.  Returns the number of particles kept."""
+    if pr not in (4, 8):
+        raise ValueError("pr must be 4 or 8")
+    real = np.dtype("<f4") if pr == 4 else np.dtype("<f8")
+    sc = dict(rscale=rscale, vscale=vscale, mscale=mscale, rhoscale=rhoscale, rhosink=rhosink)
+    n, stot, c = _dragon_columns(r, m, h, v, rho, temp, ptype, porig, sinks, sc)
+    keep = np.concatenate([(c["rho"][:n] > _DRAGON_RHORESTR) | (c["temp"][:n] < _DRAGON_TRESTR),
+                           np.ones(stot, bool)])
+    kept = int(np.count_nonzero(keep[:n]))
+    mg = float(np.sum(np.asarray(m, np.float64))) if mgas_orig is None else mgas_orig
+    idata, rdata = _dragon_header(kept + stot, kept, nsteps, snapshot,
+                                  n if pgas_orig is None else pgas_orig, time, lastsnap, mg,
+                                  tscale, mscale)
+    with open(path, "wb") as f:
+        _write_record(f, idata.astype("<i4").tobytes())
+        _write_record(f, rdata.astype(real).tobytes())
+        for k in ("r", "v", "temp", "h", "rho", "m"):
+            _write_record(f, c[k][keep].astype(real).tobytes())
+        _write_record(f, c["ptype"][keep].astype("<i4").tobytes())
+        if ids:
+            _write_record(f, c["porig"][keep].astype("<i4").tobytes())
+    return kept
+
+
+def _fort_real(x: float, pr: int) -> str:
+    return f"{x: .9E}" if pr == 4 else f"{x: .17E}"
+
+
+def write_dragon_form(path: str, r, m, h, v, rho, temp=None, ptype=None, porig=None,
+                      sinks: Optional[List[Dict]] = None, pr: int = 8, ids: bool = False,
+                      time: float = 0.0, lastsnap: float = 0.0, snapshot: int = 0,
+                      nsteps: int = 0, pgas_orig: Optional[int] = None,
+                      mgas_orig: Optional[float] = None, rhosink: float = 0.0,
+                      rscale: float = 1.0, vscale: float = 1.0, mscale: float = 1.0,
+                      rhoscale: float = 1.0, tscale: float = 1.0) -> None:
+    """Write an ASCII DRAGON snapshot as write_data_dragon_form.F90 does
+    (every particle, no density-temperature cut; one value or one particle
+    vector per line; sinks last).  Reals are printed with enough digits to
+    read back exactly at real kind pr."""
+    if pr not in (4, 8):
+        raise ValueError("pr must be 4 or 8")
+    sc = dict(rscale=rscale, vscale=vscale, mscale=mscale, rhoscale=rhoscale, rhosink=rhosink)
+    n, stot, c = _dragon_columns(r, m, h, v, rho, temp, ptype, porig, sinks, sc)
+    mg = float(np.sum(np.asarray(m, np.float64))) if mgas_orig is None else mgas_orig
+    idata, rdata = _dragon_header(n + stot, n, nsteps, snapshot, n if pgas_orig is None
+                                  else pgas_orig, time, lastsnap, mg, tscale, mscale)
+    cast = (lambda a: np.asarray(a, np.float64).astype(np.float32)) if pr == 4 else \
+        (lambda a: np.asarray(a, np.float64))
+    out: List[str] = [f"{int(x):12d}" for x in idata]
+    out += [_fort_real(float(x), pr) for x in cast(rdata)]
+    for k in ("r", "v"):
+        out += [" ".join(_fort_real(float(x), pr) for x in row) for row in cast(c[k])]
+    for k in ("temp", "h", "rho", "m"):
+        out += [_fort_real(float(x), pr) for x in cast(c[k])]
+    out += [f"{int(x):12d}" for x in c["ptype"]]
+    if ids:
+        out += [f"{int(x):12d}" for x in c["porig"]]
+    with open(path, "w") as f:
+        f.write("\n".join(out) + "\n")
