@@ -163,6 +163,24 @@ int seren_gpu_get_sinks(seren_gpu_ctx* ctx, int32_t nsink, double* sink_rmh, dou
  * sqrt(radius/|a|) and radius/|v|, and the sink-sink crossing times), which
  * sph_sim/sph_timesteps.F90:69-74 folds into the global minimum. */
 int seren_gpu_sink_timestep(seren_gpu_ctx* ctx, double sink_mult, double* dt_min);
+/* Sink accretion on the device-resident particles, replacing
+ * sinks/accrete_particles.F90:14-365 with main/remove_from_list.F90:10-96
+ * (called by sinks/sink_update.F90:24 after the step's advance).  Each particle
+ * inside the radius of an accreting sink (accrete[s] != 0; NULL: every sink)
+ * goes to the nearest one; with energy_accrete it must also be bound to it
+ * (kinetic energy of the reduced mass below m_p times the pair potential of
+ * gravity/gravity_gradh.F90, called as the reference calls it).  An accreting
+ * sink takes the mass of its particles, moves to their common centre of mass,
+ * velocity and mass-weighted acceleration, and sink_angmom[s] (when given,
+ * [nsink][3], added to) takes the angular momentum about the new centre of
+ * mass.  The accreted particles leave the device arrays, the others keep their
+ * order; naccreted[s] (when given) counts them per sink, *ptot_out (when
+ * given) is the new particle count.  Needs seren_gpu_set_sinks,
+ * seren_gpu_set_sink_motion and a force step; afterwards the next force step
+ * builds a new tree (calls that reuse the tree fail until then). */
+int seren_gpu_accrete(seren_gpu_ctx* ctx, int32_t nsink, const int32_t* accrete,
+                      int32_t energy_accrete, double* sink_angmom, int32_t* naccreted,
+                      int32_t* ptot_out);
 /* Sinks for the device-resident step: from the next seren_gpu_force_step on,
  * its gravity adds direct_sink_gravity (sinks/direct_sink_gravity.F90:10-64)
  * for sink_rmh[s] = {x, y, z, m, h}, as seren_gpu_grav_forces does with

@@ -8,6 +8,7 @@ unpinned: the reference ships no golden vectors and cannot be compiled here.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 import subprocess
 
@@ -114,6 +115,114 @@ def sink_timesteps(rmh, v, a, radius, sink_mult=0.5):
                                                1.0e-20))
         out[s] = dt
     return out
+
+
+def _accrete_pot(d, invhp, hq, mq, w6):
+    """gravity/gravity_gradh.F90:11-95, the potential only (zeta/omega = 0);
+    accrete_particles.F90:178-180 passes the sink's 1/h as hq."""
+    drsqd = (d[0] * d[0] + d[1] * d[1]) + d[2] * d[2]
+    drmag = math.sqrt(drsqd) + 1.0e-20
+    invdrmag = 1.0 / drmag
+    if invdrmag > 0.5 * invhp:
+        kern = min(int((5000.0 * drmag) * invhp), KERNTOT)
+        dpot = invhp * w6[kern]
+    else:
+        dpot = invdrmag
+    if drmag < 2.0 * hq:
+        invhq = 1.0 / hq
+        kern = min(int((5000.0 * drmag) * invhq), KERNTOT)
+        dpot = dpot + invhq * w6[kern]
+    else:
+        dpot = dpot + invdrmag
+    return (0.5 * mq) * dpot
+
+
+def accrete_particles(r, m, h, v, a, sink_rmh, sink_v, sink_a, sink_radius, accrete=None,
+                      energy_accrete=False):
+    """sinks/accrete_particles.F90:14-365 and main/remove_from_list.F90:10-96
+    for particles r [N,3], m, h, v, a [N,3] (all gas) and sinks rmh [S,5] (x,
+    y, z, m, h), v, a [S,3], radius [S].  Every particle inside an accreting
+    sink's radius goes to the nearest such sink (:83-108; a later sink only
+    when strictly nearer); with energy_accrete it must be bound to it
+    (:147-190).  Each sink with accreted particles takes their mass and moves
+    to the centre of mass, velocity and mass-weighted acceleration, summed in
+    particle order, and gains the angular momentum about that centre
+    (:225-285).  Returns dead (sink per particle, -1 kept), keep (kept
+    particles in order), count per sink, the new sink rmh, v, a and the
+    angular momentum added to each sink."""
+    r, v, a = (np.asarray(x, np.float64).reshape(-1, 3) for x in (r, v, a))
+    m, h = (np.asarray(x, np.float64).ravel() for x in (m, h))
+    rmh = np.array(sink_rmh, np.float64).reshape(-1, 5)
+    sv = np.array(sink_v, np.float64).reshape(-1, 3)
+    sa = np.array(sink_a, np.float64).reshape(-1, 3)
+    rad = np.asarray(sink_radius, np.float64).ravel()
+    ns, n = rmh.shape[0], r.shape[0]
+    acc = [True] * ns if accrete is None else [bool(x) for x in accrete]
+    w6 = kernel_tables()[6].tolist()
+    dead = [-1] * n
+    for p in range(n):
+        rp = r[p].tolist()
+        flag, best = -1, 0.0
+        for s in range(ns):
+            if not acc[s]:
+                continue
+            d = [rp[k] - float(rmh[s, k]) for k in range(3)]
+            drsqd = (d[0] * d[0] + d[1] * d[1]) + d[2] * d[2]
+            rads = float(rad[s])
+            if drsqd < rads * rads and (flag == -1 or drsqd < best):
+                flag, best = s, drsqd
+        if flag < 0:
+            continue
+        if energy_accrete:
+            ms, mp = float(rmh[flag, 3]), float(m[p])
+            e = [float(sv[flag, k]) - float(v[p, k]) for k in range(3)]
+            reduced_mass = (ms * mp) / (ms + mp)
+            dpotp = _accrete_pot([float(rmh[flag, k]) - rp[k] for k in range(3)], 1.0 / float(h[p]),
+                                 1.0 / float(rmh[flag, 4]), ms, w6)
+            total = ((0.5 * reduced_mass) * ((e[0] * e[0] + e[1] * e[1]) + e[2] * e[2])) - dpotp * mp
+            if not total < 0.0:
+                continue
+        dead[p] = flag
+    new_rmh, new_v, new_a = rmh.copy(), sv.copy(), sa.copy()
+    angmom = np.zeros((ns, 3))
+    count = np.zeros(ns, np.int64)
+    for s in range(ns):
+        if not acc[s]:
+            continue
+        mine = [p for p in range(n) if dead[p] == s]
+        if not mine:
+            continue
+        ms = float(rmh[s, 3])
+        rs, vs = rmh[s, 0:3].tolist(), sv[s].tolist()
+        mt = ms
+        rc = [ms * x for x in rs]
+        vc = [ms * x for x in vs]
+        ac = [ms * x for x in sa[s].tolist()]
+        for p in mine:
+            mp = float(m[p])
+            mt = mt + mp
+            for k in range(3):
+                rc[k] = rc[k] + mp * float(r[p, k])
+                vc[k] = vc[k] + mp * float(v[p, k])
+                ac[k] = ac[k] + mp * float(a[p, k])
+        rc = [x / mt for x in rc]
+        vc = [x / mt for x in vc]
+        ac = [x / mt for x in ac]
+        L = [0.0, 0.0, 0.0]
+
+        def add(L, mq, d, e):
+            return [(L[0] + (mq * d[1]) * e[2]) - (mq * d[2]) * e[1],
+                    (L[1] + (mq * d[2]) * e[0]) - (mq * d[0]) * e[2],
+                    (L[2] + (mq * d[0]) * e[1]) - (mq * d[1]) * e[0]]
+        L = add(L, ms, [rs[k] - rc[k] for k in range(3)], [vs[k] - vc[k] for k in range(3)])
+        for p in mine:
+            L = add(L, float(m[p]), [rc[k] - float(r[p, k]) for k in range(3)],
+                    [vc[k] - float(v[p, k]) for k in range(3)])
+        new_rmh[s, 0:3], new_rmh[s, 3] = rc, mt
+        new_v[s], new_a[s], angmom[s], count[s] = vc, ac, L, len(mine)
+    keep = np.array([p for p in range(n) if dead[p] < 0], np.int64)
+    return dict(dead=np.array(dead, np.int64), keep=keep, count=count, rmh=new_rmh, v=new_v,
+                a=new_a, angmom=angmom)
 
 
 def rk2_half(r, v, a, dt):

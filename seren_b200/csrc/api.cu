@@ -262,6 +262,8 @@ void free_all(Ctx& c) {
   if (c.stage_io) cudaFree(c.stage_io);
   for (double4* p : {c.r_old, c.v_old, c.v_half, c.r_old_alt, c.v_old_alt, c.v_half_alt})
     if (p) cudaFree(p);
+  for (void* p : {(void*)c.acc_sinks, (void*)c.acc_out, (void*)c.acc_ws})
+    if (p) cudaFree(p);
   for (auto& e : c.ev)
     if (e) cudaEventDestroy(e);
   for (auto& e : c.ev_io)
@@ -634,7 +636,8 @@ int seren_gpu_hydro_forces(seren_gpu_ctx* h, const int32_t* acclist, int32_t nac
                            const double* press, const double* sound, double* a) {
   if (!h) return SEREN_GPU_ERR_ARG;
   Ctx& c = h->c;
-  if (!c.have_sph) return fail(c, SEREN_GPU_ERR_STATE, "call seren_gpu_sph_update first");
+  if (!c.have_sph || !c.have_tree)
+    return fail(c, SEREN_GPU_ERR_STATE, "call seren_gpu_sph_update first");
   if (!press || !sound || !a) return fail(c, SEREN_GPU_ERR_ARG, "NULL array");
   const int ptot = c.ptot;
   cudaMemcpyAsync(c.press, press, sizeof(double) * ptot, cudaMemcpyHostToDevice, c.st);
@@ -1073,6 +1076,84 @@ int seren_gpu_rk2_step(seren_gpu_ctx* h, double dt) {
   rc = seren::force_step_body(c, 0, nullptr);                 // forces at the end
   if (rc) return rc;
   return sinks ? seren::sink_accels(c) : SEREN_GPU_OK;
+}
+
+int seren_gpu_accrete(seren_gpu_ctx* h, int32_t nsink, const int32_t* accrete,
+                      int32_t energy_accrete, double* sink_angmom, int32_t* naccreted,
+                      int32_t* ptot_out) {
+  if (!h) return SEREN_GPU_ERR_ARG;
+  Ctx& c = h->c;
+  if (nsink < 1 || nsink != c.nsink)
+    return fail(c, SEREN_GPU_ERR_ARG, "accrete: nsink as in seren_gpu_set_sinks");
+  if (!c.sink_move)
+    return fail(c, SEREN_GPU_ERR_STATE, "accrete: call seren_gpu_set_sink_motion");
+  if (!c.have_v || !c.have_sph || c.ptot < 1)
+    return fail(c, SEREN_GPU_ERR_STATE, "accrete: call seren_gpu_force_step first");
+  if (!c.sink_a_valid) {
+    if (!c.have_tree) return fail(c, SEREN_GPU_ERR_STATE, "accrete: no tree for the sinks' accelerations");
+    const int rc = seren::sink_accels(c);
+    if (rc) return rc;
+  }
+  if (!c.acc_ws) {
+    const size_t P = (size_t)c.pmax;
+    if (cudaMalloc(&c.acc_sinks, sizeof(double) * seren::ACC_STRIDE * 1024) != cudaSuccess ||
+        cudaMalloc(&c.acc_out, sizeof(double) * seren::ACC_STRIDE * 1024) != cudaSuccess ||
+        cudaMalloc(&c.acc_ws, sizeof(int) * 4 * P) != cudaSuccess) {
+      cudaGetLastError();
+      for (void** p : {(void**)&c.acc_sinks, (void**)&c.acc_out, (void**)&c.acc_ws})
+        if (*p) { cudaFree(*p); *p = nullptr; }
+      return fail(c, SEREN_GPU_ERR_CUDA, "accrete: scratch allocation failed");
+    }
+  }
+  const int ns = nsink;
+  const int S = seren::ACC_STRIDE;
+  std::vector<double> rec((size_t)ns * S, 0.0);
+  for (int s = 0; s < ns; ++s) {
+    double* R = &rec[(size_t)s * S];
+    for (int k = 0; k < 5; ++k) R[k] = c.sink_rmh[s * 5 + k];
+    R[5] = c.sink_radius[s];
+    R[6] = (!accrete || accrete[s]) ? 1.0 : 0.0;
+    for (int k = 0; k < 3; ++k) {
+      R[7 + k] = c.sink_v[s * 3 + k];
+      R[10 + k] = c.sink_a[s * 3 + k];
+    }
+  }
+  cudaMemcpyAsync(c.acc_sinks, rec.data(), sizeof(double) * rec.size(), cudaMemcpyHostToDevice, c.st);
+  c.nlaunch = 0;
+  std::vector<double> out;
+  int ndead = 0;
+  int rc = seren::launch_accrete(c, ns, energy_accrete ? 1 : 0, out, ndead);
+  if (rc) return finish(c, "accrete");
+  rc = finish(c, "accrete");
+  if (rc) return rc;
+  if (naccreted)
+    for (int s = 0; s < ns; ++s) naccreted[s] = 0;
+  if (ndead > 0) {
+    // accrete_particles.F90:264-285: the new sink state; rold and vold (the
+    // Runge-Kutta start values) are the new position and velocity
+    for (int s = 0; s < ns; ++s) {
+      const double* O = &out[(size_t)s * S];
+      const int cnt = (int)O[15];
+      if (naccreted) naccreted[s] = cnt;
+      if (cnt <= 0) continue;
+      c.sink_rmh[s * 5 + 3] = O[0];
+      for (int k = 0; k < 3; ++k) {
+        c.sink_rmh[s * 5 + k] = O[1 + k];
+        c.sink_v[s * 3 + k] = O[4 + k];
+        c.sink_a[s * 3 + k] = O[7 + k];
+        if (c.sink_rold.size() == 3 * (size_t)ns) c.sink_rold[s * 3 + k] = O[1 + k];
+        if (c.sink_vold.size() == 3 * (size_t)ns) c.sink_vold[s * 3 + k] = O[4 + k];
+        if (sink_angmom) sink_angmom[s * 3 + k] = sink_angmom[s * 3 + k] + O[10 + k];
+      }
+    }
+    rc = seren::sink_upload(c);
+    if (rc) return rc;
+    // the tree and neighbour lists index the old arrays: the next force step
+    // builds a new tree (accrete_particles.F90:330, nstock = nsteps)
+    c.have_tree = false;
+  }
+  if (ptot_out) *ptot_out = c.ptot;
+  return SEREN_GPU_OK;
 }
 
 int seren_gpu_drift(seren_gpu_ctx* h, double dt) {

@@ -137,10 +137,10 @@ struct Ctx {
   int* leaves = nullptr;      // [pmax][256] opened leaves of each particle's grad-h walk
   int* nleaf = nullptr;       // their number (-1: overflow)
   int* npot = nullptr;        // [pmax] particles in those leaves (pp_pot)
-  int* redo = nullptr;
+  int* redo = nullptr;        // [pmax] particles whose grad-h is redone alone; count in work[1]
   int* wide = nullptr;        // [pmax] particles whose grad-h walks cover most of the tree; count in work[2]
   void* wst = nullptr;        // state of a batch of those particles (sph.cu)
-  double* wacc = nullptr;     // their walk accumulators, 4 per particle        // [pmax] particles whose grad-h is redone alone; count in work[1]
+  double* wacc = nullptr;     // their walk accumulators, 4 per particle
   int2* wstack = nullptr;     // walk stacks, wstack_cap (cell, lane mask) entries per warp slot
   int wstack_cap = 0;
   int wstack_slots = 0;
@@ -149,6 +149,13 @@ struct Ctx {
   double4* tabA = nullptr;
   double4* tabG = nullptr;
   float4* tabG32 = nullptr;   // FP32 w5, w4, w6 of tabG (mixed gravity)
+
+  // sink accretion (seren_gpu_accrete), made on first use: sink records and
+  // results, ACC_STRIDE doubles per sink for up to 1024 sinks, and 4 * pmax ints
+  // of scratch (sinks.cu)
+  double* acc_sinks = nullptr;
+  double* acc_out = nullptr;
+  int* acc_ws = nullptr;
 
   bool have_tree = false;
   bool have_sph = false;
@@ -203,6 +210,13 @@ void launch_grav(Ctx& c, int nact, int nsink, const double* d_sinks, double* ama
 void launch_sink_walk(Ctx& c, int nsink, const double* d_sinks, double* d_out /*[nsink][4]*/);
 int grav_walk_slots(const Ctx& c);      // resident warps of the gravity walk grid
 int grav_walk_stack_cap(const Ctx& c);  // stack entries per warp
+
+// sinks.cu
+constexpr int ACC_STRIDE = 16;
+// accrete_particles + remove_from_list on the device-resident particles with
+// the sinks in c.acc_sinks: ndead particles accreted (0: nothing changed); when
+// ndead > 0, out holds ACC_STRIDE doubles per sink and c.ptot is the kept count
+int launch_accrete(Ctx& c, int nsink, int energy, std::vector<double>& out, int& ndead);
 
 // tables.cpp
 void make_kernel_tables(int kernel, std::vector<double>& w0, std::vector<double>& w1,

@@ -41,6 +41,7 @@ def library(build_if_missing: bool = True) -> C.CDLL:
                            ("set_sink_motion", [vp, C.c_int32, _dp, _dp]),
                            ("get_sinks", [vp, C.c_int32, _dp, _dp, _dp, _dp]),
                            ("sink_timestep", [vp, C.c_double, _dp]),
+                           ("accrete", [vp, C.c_int32, _ip, C.c_int32, _dp, _ip, _ip]),
                            ("set_sinks", [vp, C.c_int32, _dp]),
                            ("download", [vp, _dp, _dp, _dp, _dp, _dp, _dp, _ip]),
                            ("last_step_stats", [vp, _dp, _ip, C.POINTER(C.c_int64)]),
@@ -116,6 +117,27 @@ class GpuHotPath(HotPath):
         d = C.c_double()
         self._call("sink_timestep", self._ctx, C.c_double(sink_mult), C.byref(d))
         return d.value
+
+    def accrete(self, energy_accrete=False, accrete=None, angmom=None):
+        """Sink accretion and removal of the accreted particles
+        (seren_gpu_accrete).  accrete: per-sink flags (None: every sink);
+        angmom [nsink][3] is added to in place when given.  Returns the number
+        accreted by each sink; self.ptot becomes the kept count."""
+        ns = self.nsink
+        flags = None if accrete is None else \
+            np.ascontiguousarray(np.atleast_1d(accrete), dtype=np.int32)
+        if flags is not None and flags.size != ns:
+            raise ValueError("one accrete flag per sink")
+        if angmom is not None and (angmom.dtype != np.float64 or angmom.shape != (ns, 3) or
+                                   not angmom.flags.c_contiguous):
+            raise ValueError("angmom must be a C-contiguous float64 array [nsink][3]")
+        cnt = np.zeros(ns, np.int32)
+        ptot = C.c_int32()
+        self._call("accrete", self._ctx, ns, None if flags is None else flags.ctypes.data_as(_ip),
+                   1 if energy_accrete else 0, _d(angmom), cnt.ctypes.data_as(_ip),
+                   C.byref(ptot))
+        self.ptot = ptot.value
+        return cnt
 
     def drift(self, dt: float):
         self._call("drift", self._ctx, C.c_double(dt))

@@ -199,3 +199,49 @@ def test_rk2_steps():
     assert np.allclose(rh, [[1.0, 0.05, 0.0]]) and np.allclose(vh, [[-0.05, 1.0, 0.0]])
     r1, v1 = rk2_full(r, v, vh, -rh, 0.1)
     assert np.allclose(r1, [[1.0 - 0.005, 0.1, 0.0]]) and np.allclose(v1, [[-0.1, 0.995, 0.0]])
+
+
+def test_accretion_conserves_mass_momentum_and_angular_momentum():
+    """The accretion restatement (accrete_particles.F90) against invariants that
+    do not depend on its loops: each accreted particle lies inside its sink's
+    radius and no accreting sink is nearer; mass, momentum, mass-weighted
+    acceleration and angular momentum about the origin (sink orbital part plus
+    the spin added) are conserved; a sink that does not accrete takes nothing;
+    without the energy test every particle inside a radius is taken."""
+    from oracle.oracle import accrete_particles
+    rng = np.random.default_rng(11)
+    n = 3000
+    r = rng.uniform(-1, 1, (n, 3))
+    v = rng.normal(0, 0.5, (n, 3))
+    a = rng.normal(0, 1.0, (n, 3))
+    m = rng.uniform(0.5, 1.5, n) / n
+    h = rng.uniform(0.05, 0.1, n)
+    rmh = np.array([[0.0, 0.0, 0.0, 0.05, 0.05], [0.25, 0.0, 0.0, 0.03, 0.04],
+                    [-0.5, 0.5, 0.2, 0.02, 0.05]])
+    sv = np.array([[0.1, 0.0, 0.0], [0.0, -0.2, 0.1], [0.0, 0.0, 0.3]])
+    sa = rng.normal(0, 1.0, (3, 3))
+    rad = np.array([0.3, 0.2, 0.25])
+    flags = [1, 1, 0]
+    w = accrete_particles(r, m, h, v, a, rmh, sv, sa, rad, accrete=flags, energy_accrete=True)
+    allin = accrete_particles(r, m, h, v, a, rmh, sv, sa, rad, accrete=flags)
+    d2 = ((r[:, None, :] - rmh[None, :, 0:3]) ** 2).sum(-1)
+    inside = (d2 < rad[None, :] ** 2) & (np.array(flags, bool)[None, :])
+    assert (allin["dead"] >= 0).sum() == inside.any(1).sum()
+    assert 0 < (w["dead"] >= 0).sum() < (allin["dead"] >= 0).sum()
+    for q in np.flatnonzero(w["dead"] >= 0):
+        s = w["dead"][q]
+        assert inside[q, s] and d2[q, s] == d2[q, inside[q]].min()
+    assert w["count"][2] == 0 and np.array_equal(w["rmh"][2], rmh[2])
+    for s in (0, 1):
+        mine = w["dead"] == s
+        mt = rmh[s, 3] + m[mine].sum()
+        assert np.isclose(w["rmh"][s, 3], mt, rtol=1e-14)
+        p0 = rmh[s, 3] * sv[s] + (m[mine, None] * v[mine]).sum(0)
+        assert np.allclose(w["rmh"][s, 3] * w["v"][s], p0, rtol=1e-12, atol=1e-15)
+        f0 = rmh[s, 3] * sa[s] + (m[mine, None] * a[mine]).sum(0)
+        assert np.allclose(w["rmh"][s, 3] * w["a"][s], f0, rtol=1e-12, atol=1e-15)
+        L0 = rmh[s, 3] * np.cross(rmh[s, 0:3], sv[s]) + (m[mine, None] *
+                                                          np.cross(r[mine], v[mine])).sum(0)
+        L1 = w["rmh"][s, 3] * np.cross(w["rmh"][s, 0:3], w["v"][s]) + w["angmom"][s]
+        assert np.allclose(L1, L0, rtol=1e-10, atol=1e-15)
+    assert np.array_equal(w["keep"], np.flatnonzero(w["dead"] < 0))
