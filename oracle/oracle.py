@@ -119,7 +119,7 @@ def sink_timesteps(rmh, v, a, radius, sink_mult=0.5):
 
 def _accrete_pot(d, invhp, hq, mq, w6):
     """gravity/gravity_gradh.F90:11-95, the potential only (zeta/omega = 0);
-    accrete_particles.F90:178-180 passes the sink's 1/h as hq."""
+    accrete_particles.F90:186-188 passes the sink's 1/h as hq."""
     drsqd = (d[0] * d[0] + d[1] * d[1]) + d[2] * d[2]
     drmag = math.sqrt(drsqd) + 1.0e-20
     invdrmag = 1.0 / drmag
@@ -142,12 +142,12 @@ def accrete_particles(r, m, h, v, a, sink_rmh, sink_v, sink_a, sink_radius, accr
     """sinks/accrete_particles.F90:14-365 and main/remove_from_list.F90:10-96
     for particles r [N,3], m, h, v, a [N,3] (all gas) and sinks rmh [S,5] (x,
     y, z, m, h), v, a [S,3], radius [S].  Every particle inside an accreting
-    sink's radius goes to the nearest such sink (:83-108; a later sink only
+    sink's radius goes to the nearest such sink (:82-106; a later sink only
     when strictly nearer); with energy_accrete it must be bound to it
-    (:147-190).  Each sink with accreted particles takes their mass and moves
+    (:165-205).  Each sink with accreted particles takes their mass and moves
     to the centre of mass, velocity and mass-weighted acceleration, summed in
     particle order, and gains the angular momentum about that centre
-    (:225-285).  Returns dead (sink per particle, -1 kept), keep (kept
+    (:233-281).  Returns dead (sink per particle, -1 kept), keep (kept
     particles in order), count per sink, the new sink rmh, v, a and the
     angular momentum added to each sink."""
     r, v, a = (np.asarray(x, np.float64).reshape(-1, 3) for x in (r, v, a))

@@ -23,7 +23,7 @@ namespace {
 inline int nb(long n, int t) { return (int)((n + t - 1) / t); }
 
 // gravity/gravity_gradh.F90:11-95, the potential only, with zeta/omega = 0, as
-// accrete_particles.F90:178-180 calls it: the sink's 1/h is passed where the
+// accrete_particles.F90:186-188 calls it: the sink's 1/h is passed where the
 // routine takes the second body's h (hq below is that value)
 __device__ __forceinline__ double accrete_pot(double d0, double d1, double d2, double invhp,
                                               double hq, double mq,
@@ -50,8 +50,8 @@ __device__ __forceinline__ double accrete_pot(double d0, double d1, double d2, d
   return (0.5 * mq) * dpot;
 }
 
-// accrete_particles.F90:83-108 (nearest accreting sink whose radius holds the
-// particle; a later sink wins only when strictly nearer) and :147-190 (the
+// accrete_particles.F90:82-106 (nearest accreting sink whose radius holds the
+// particle; a later sink wins only when strictly nearer) and :165-205 (the
 // energy test); dead[p] = that sink when the particle is accreted, else -1
 __global__ void k_acc_flag(int n, int ns, int energy, const double4* __restrict__ pm,
                            const double2* __restrict__ hz, const double4* __restrict__ vel,
@@ -108,7 +108,7 @@ __global__ void k_acc_lists(int n, const int* __restrict__ dead, const int* __re
     live[p - pos[p]] = p;
 }
 
-// accrete_particles.F90:125-285 for one sink per warp: the sums over its
+// accrete_particles.F90:128-281 for one sink per warp: the sums over its
 // accreted particles in index order, the new centre of mass, velocity and
 // acceleration, and the angular momentum about the new centre of mass of the
 // old sink and of each accreted particle
