@@ -181,6 +181,45 @@ int seren_gpu_sink_timestep(seren_gpu_ctx* ctx, double sink_mult, double* dt_min
 int seren_gpu_accrete(seren_gpu_ctx* ctx, int32_t nsink, const int32_t* accrete,
                       int32_t energy_accrete, double* sink_angmom, int32_t* naccreted,
                       int32_t* ptot_out);
+
+/* Options of the sink search (setup/default_parameters.F90:120-129; the
+ * logical ones 0 or 1).  sinkrad is the new sink's radius, in units of the
+ * particle's h when hmult_sinkrad (the reference's SINK_RADIUS = HMULT). */
+typedef struct {
+  double rhosink;
+  double sinkrad;
+  int32_t hmult_sinkrad;
+  int32_t rho_search;
+  int32_t potmin_search;
+  int32_t hill_sphere_search;
+  int32_t div_v_search;
+  int32_t div_a_search;
+  int32_t timescale_search;
+  int32_t reserved;        /* 0 */
+} seren_gpu_sink_search_params;
+
+/* Sink search and creation on the device-resident particles, replacing
+ * sinks/sink_search.F90:11-433 with sinks/create_sink.F90:11-268 (called by
+ * sinks/sink_update.F90:16-20 every nsearchstep steps).  Candidates: rho >=
+ * rhosink (rho_search), a minimum of the potential over the gather
+ * neighbours (potmin_search), not within 2 radii of a sink, the Hill test
+ * (hill_sphere_search; it reads accelerations that only the reference's
+ * DEBUG_FORCES builds fill, and so rejects nothing, as there), div v and div
+ * a of the neighbours within max(sinkrad, 2h) not positive, and the timescale
+ * test (timescale_search).  When a candidate passes, the densest candidate
+ * of the last test loop becomes a sink (as the reference picks it) with the
+ * particles within the sink radius of it: mass, centre of mass, velocity,
+ * acceleration, h = radius/2, and its angular momentum in sink_angmom[3]
+ * (when given).  Those particles leave the device arrays (the rest keep
+ * their order); the new sink is appended to the sinks (seren_gpu_get_sinks)
+ * and moves with seren_gpu_rk2_step.  *created is 1 or 0, *psink_id the id
+ * (index_base) of the particle it was made from, *nremoved the particles
+ * removed, *ptot_out the particles left (each may be NULL).  Needs a force
+ * step on the current positions (the walk uses its tree); with sinks, their
+ * motion set.  Afterwards the next force step builds a new tree. */
+int seren_gpu_sink_search(seren_gpu_ctx* ctx, const seren_gpu_sink_search_params* prm,
+                          int32_t* created, int32_t* psink_id, double* sink_angmom,
+                          int32_t* nremoved, int32_t* ptot_out);
 /* Sinks for the device-resident step: from the next seren_gpu_force_step on,
  * its gravity adds direct_sink_gravity (sinks/direct_sink_gravity.F90:10-64)
  * for sink_rmh[s] = {x, y, z, m, h}, as seren_gpu_grav_forces does with

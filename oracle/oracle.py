@@ -225,6 +225,180 @@ def accrete_particles(r, m, h, v, a, sink_rmh, sink_v, sink_a, sink_radius, accr
                 a=new_a, angmom=angmom)
 
 
+def _is_potmin(r, h, gpot, p):
+    """sph/all_sph_gradh.F90:355-471: the particle's -gpot is below every
+    gather neighbour's (within 2h, kernel bin <= KERNTOT) and below 0."""
+    hp = float(h[p])
+    invhp = 1.0 / hp
+    dr = r - r[p]
+    drsqd = (dr[:, 0] * dr[:, 0] + dr[:, 1] * dr[:, 1]) + dr[:, 2] * dr[:, 2]
+    near = drsqd <= (4.0 * hp) * hp
+    near[p] = False
+    drmag = np.sqrt(drsqd[near]) + 1.0e-20
+    ok = ((5000.0 * drmag) * invhp).astype(np.int64) <= KERNTOT
+    gmin = 0.0
+    if ok.any():
+        gmin = min(0.0, float(np.min(-gpot[near][ok])))
+    return gmin > -float(gpot[p])
+
+
+def sink_search(r, m, h, v, a, rho, gpot, sink_rmh, sink_v, sink_a, sink_radius,
+                rhosink, sinkrad, hmult_sinkrad=False, rho_search=True, potmin_search=True,
+                hill_sphere_search=True, div_v_search=True, div_a_search=True,
+                timescale_search=False):
+    """sinks/sink_search.F90:11-433 and sinks/create_sink.F90:11-268 on
+    particles in tree order (r [N,3], m, h, v [N,3], a [N,3], rho, gpot) with
+    existing sinks (rmh [S,5], v, a [S,3], radius [S]).  Returns psink (-1: no sink made), the
+    candidates in density order with their flags, and for a new sink its
+    state (m, r, v, a, h, radius, angmom), the removed particles (psink and
+    its neighbours within the sink radius, in index order) and the kept ones.
+    Kept as the reference has them: the Hill test reads the particles' a_grav
+    and the sinks' agrav, which only DEBUG_FORCES builds fill
+    (sph_sim/sph_grav_forces.F90:128-130; otherwise zero, so the test never
+    rejects); div a divides by the
+    dot product of the relative acceleration and separation; the particle
+    made a sink is the one the last candidate loop visited last (:420-426
+    assign psink = p), which can be a candidate that failed that loop's
+    test when a lower-density one passed."""
+    r, v, a = (np.asarray(x, np.float64).reshape(-1, 3) for x in (r, v, a))
+    m, h, rho, gpot = (np.asarray(x, np.float64).ravel() for x in (m, h, rho, gpot))
+    rmh = np.array(sink_rmh, np.float64).reshape(-1, 5)
+    sv = np.array(sink_v, np.float64).reshape(-1, 3)
+    sa = np.array(sink_a, np.float64).reshape(-1, 3)
+    srad = np.asarray(sink_radius, np.float64).ravel()
+    n, stot = r.shape[0], rmh.shape[0]
+    t = kernel_tables()
+    w0, w1, w4 = t[0].tolist(), t[1].tolist(), t[4].tolist()
+    out = dict(psink=-1, candidates=[], flags=[])
+    cand = [p for p in range(n)
+            if not (rho_search and rho[p] < rhosink)
+            and not (potmin_search and not _is_potmin(r, h, gpot, p))]
+    if not cand:
+        return out
+    cand.sort(key=lambda p: float(rho[p]))          # stable, as insertion_sort_real
+    k = len(cand)
+    flag = [True] * k
+    srho = [float(rho[p]) for p in cand]
+    if stot > 0:                                    # :158-200
+        for i, p in enumerate(cand):
+            rp = r[p].tolist()
+            for s in range(stot):
+                dr = [float(rmh[s, c]) - rp[c] for c in range(3)]
+                drsqd = (dr[0] * dr[0] + dr[1] * dr[1]) + dr[2] * dr[2]
+                if drsqd < (2.0 * float(srad[s])) * (2.0 * float(srad[s])):
+                    flag[i] = False
+                if hill_sphere_search:
+                    da = [0.0, 0.0, 0.0]                # sink agrav - particle a_grav
+                    dadr = (da[0] * dr[0] + da[1] * dr[1]) + da[2] * dr[2]
+                    rho_hill = -(3.0 * dadr) / ((4.0 * 3.1415926536) * drsqd)
+                    if srho[i] < 3.0 * rho_hill:
+                        flag[i] = False
+    last = -1                                       # the last candidate a loop visits
+    div_v = [0.0] * k
+    for i, p in enumerate(cand):                    # :212-303
+        if not flag[i]:
+            continue
+        last = i
+        rp, vp, ap = r[p].tolist(), v[p].tolist(), a[p].tolist()
+        hp = float(h[p])
+        hrange = max(sinkrad * hp, 2.0 * hp) if hmult_sinkrad else max(sinkrad, 2.0 * hp)
+        hrangesqd = hrange * hrange
+        invhp = 2.0 / hrange
+        hfactor = math.pow(invhp, 3.0)
+        d = r - r[p]
+        dsq = (d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2]
+        rhotemp = (float(m[p]) * w0[0]) * hfactor
+        dv_p, da_p, curl = 0.0, 0.0, [0.0, 0.0, 0.0]
+        for pp in np.flatnonzero(dsq <= hrangesqd).tolist():
+            if pp == p:
+                continue
+            dr = d[pp].tolist()
+            drmag = math.sqrt(float(dsq[pp])) + 1.0e-20
+            invdrmag = 1.0 / drmag
+            kern = int((5000.0 * drmag) * invhp)
+            if kern > KERNTOT:
+                continue
+            mpp = float(m[pp])
+            dv = [float(v[pp, c]) - vp[c] for c in range(3)]
+            dvdr = (dv[0] * dr[0] + dv[1] * dr[1]) + dv[2] * dr[2]
+            rhotemp = rhotemp + (mpp * hfactor) * w0[kern]
+            dv_p = dv_p - ((((mpp * dvdr) * w4[kern]) * hfactor) * invhp) * invdrmag
+            dadr = ((float(a[pp, 0]) - ap[0]) * dr[0] + (float(a[pp, 1]) - ap[1]) * dr[1]) + \
+                (float(a[pp, 2]) - ap[2]) * dr[2]
+            da_p = da_p - ((((mpp * w4[kern]) * hfactor) * invhp) / dadr) * invdrmag
+            x = [dv[1] * dr[2] - dv[2] * dr[1], dv[2] * dr[0] - dv[0] * dr[2],
+                 dv[0] * dr[1] - dv[1] * dr[0]]
+            curl = [curl[c] - ((((mpp * x[c]) * invdrmag) * w1[kern]) * hfactor) * invhp
+                    for c in range(3)]
+        div_v[i] = dv_p / rhotemp
+        if div_a_search and da_p / rhotemp > 0.0:
+            flag[i] = False
+        if div_v_search and div_v[i] > 0.0:
+            flag[i] = False
+    if stot > 0:                                    # :311-410, only tacc1 and tcond1 decide
+        last = -1
+        for i, p in enumerate(cand):
+            if not flag[i]:
+                continue
+            last = i
+            rp, vp = r[p].tolist(), v[p].tolist()
+            for s in range(stot):
+                dr = [float(rmh[s, c]) - rp[c] for c in range(3)]
+                drmag = math.sqrt((dr[0] * dr[0] + dr[1] * dr[1]) + dr[2] * dr[2]) + 1.0e-20
+                du = [dr[c] / drmag for c in range(3)]
+                dv = [float(sv[s, c]) - vp[c] for c in range(3)]
+                drad = drmag - 2.0 * float(srad[s])
+                vrad = (dv[0] * du[0] + dv[1] * du[1]) + dv[2] * du[2]
+                tacc1 = -drad / vrad
+                tcond1 = -1.0 / div_v[i]
+                if timescale_search and tcond1 > tacc1:
+                    flag[i] = False
+    out["candidates"], out["flags"] = cand, flag
+    if not any(flag) or last < 0:
+        return out
+    psink = cand[last]
+    out["psink"] = psink
+    # create_sink.F90:70-230
+    rp, vp = r[psink].tolist(), v[psink].tolist()
+    mp, hp = float(m[psink]), float(h[psink])
+    msink = mp
+    rs = [mp * x for x in rp]
+    vs = [mp * x for x in vp]
+    asn = [mp * x for x in a[psink].tolist()]
+    rads = sinkrad * hp if hmult_sinkrad else sinkrad
+    hh = 0.5 * rads
+    d = r - r[psink]
+    dsq = (d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2]
+    neib = [pp for pp in np.flatnonzero(dsq <= (4.0 * hh) * hh).tolist() if pp != psink]
+    for pp in neib:
+        mpp = float(m[pp])
+        msink = msink + mpp
+        for c in range(3):
+            rs[c] = rs[c] + mpp * float(r[pp, c])
+            vs[c] = vs[c] + mpp * float(v[pp, c])
+            asn[c] = asn[c] + mpp * float(a[pp, c])
+    rs = [x / msink for x in rs]
+    vs = [x / msink for x in vs]
+    asn = [x / msink for x in asn]
+    dr = [rs[c] - rp[c] for c in range(3)]
+    dv = [vs[c] - vp[c] for c in range(3)]
+    L = [(mp * dr[1]) * dv[2] - (mp * dr[2]) * dv[1], (mp * dr[2]) * dv[0] - (mp * dr[0]) * dv[2],
+         (mp * dr[0]) * dv[1] - (mp * dr[1]) * dv[0]]
+    for pp in neib:
+        mpp = float(m[pp])
+        dv = [vs[c] - float(v[pp, c]) for c in range(3)]
+        dr = [rs[c] - float(r[pp, c]) for c in range(3)]
+        L = [(L[0] + (mpp * dr[1]) * dv[2]) - (mpp * dr[2]) * dv[1],
+             (L[1] + (mpp * dr[2]) * dv[0]) - (mpp * dr[0]) * dv[2],
+             (L[2] + (mpp * dr[0]) * dv[1]) - (mpp * dr[1]) * dv[0]]
+    removed = sorted(neib + [psink])
+    gone = set(removed)
+    out.update(m=msink, r=np.array(rs), v=np.array(vs), a=np.array(asn), h=0.5 * rads,
+               radius=rads, angmom=np.array(L), removed=np.array(removed, np.int64),
+               keep=np.array([p for p in range(n) if p not in gone], np.int64))
+    return out
+
+
 def rk2_half(r, v, a, dt):
     """advance/advance_runge_kutta.F90:40-54 at the half step (dt = step/2):
     r + v dt, v + a dt."""

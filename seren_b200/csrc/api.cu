@@ -910,6 +910,42 @@ int sink_accels(Ctx& c) {
   return SEREN_GPU_OK;
 }
 
+// the scratch of accretion and sink search, made on first use; 0 or -1
+int sink_scratch(Ctx& c) {
+  if (c.acc_ws) return 0;
+  const size_t P = (size_t)c.pmax;
+  if (cudaMalloc(&c.acc_sinks, sizeof(double) * ACC_STRIDE * 1024) != cudaSuccess ||
+      cudaMalloc(&c.acc_out, sizeof(double) * ACC_STRIDE * 1024) != cudaSuccess ||
+      cudaMalloc(&c.acc_ws, sizeof(int) * (4 * P + 16)) != cudaSuccess) {
+    cudaGetLastError();
+    for (void** p : {(void**)&c.acc_sinks, (void**)&c.acc_out, (void**)&c.acc_ws})
+      if (*p) { cudaFree(*p); *p = nullptr; }
+    return -1;
+  }
+  return 0;
+}
+
+// the sinks' records for the accretion and search kernels: x, y, z, m, h,
+// radius, accrete (1/0; accrete NULL: every sink), v, a
+void sink_records(Ctx& c, const int32_t* accrete) {
+  const int ns = c.nsink;
+  if (ns < 1) return;
+  const int S = ACC_STRIDE;
+  std::vector<double> rec((size_t)ns * S, 0.0);
+  for (int s = 0; s < ns; ++s) {
+    double* R = &rec[(size_t)s * S];
+    for (int k = 0; k < 5; ++k) R[k] = c.sink_rmh[s * 5 + k];
+    R[5] = c.sink_radius[s];
+    R[6] = (!accrete || accrete[s]) ? 1.0 : 0.0;
+    for (int k = 0; k < 3; ++k) {
+      R[7 + k] = c.sink_v[s * 3 + k];
+      R[10 + k] = c.sink_a[s * 3 + k];
+    }
+  }
+  cudaMemcpyAsync(c.acc_sinks, rec.data(), sizeof(double) * rec.size(), cudaMemcpyHostToDevice, c.st);
+  cudaStreamSynchronize(c.st);              // rec is a local vector
+}
+
 int sink_upload(Ctx& c) {
   cudaMemcpyAsync(c.sinks, c.sink_rmh.data(), sizeof(double) * 5 * (size_t)c.nsink,
                   cudaMemcpyHostToDevice, c.st);
@@ -1094,31 +1130,10 @@ int seren_gpu_accrete(seren_gpu_ctx* h, int32_t nsink, const int32_t* accrete,
     const int rc = seren::sink_accels(c);
     if (rc) return rc;
   }
-  if (!c.acc_ws) {
-    const size_t P = (size_t)c.pmax;
-    if (cudaMalloc(&c.acc_sinks, sizeof(double) * seren::ACC_STRIDE * 1024) != cudaSuccess ||
-        cudaMalloc(&c.acc_out, sizeof(double) * seren::ACC_STRIDE * 1024) != cudaSuccess ||
-        cudaMalloc(&c.acc_ws, sizeof(int) * 4 * P) != cudaSuccess) {
-      cudaGetLastError();
-      for (void** p : {(void**)&c.acc_sinks, (void**)&c.acc_out, (void**)&c.acc_ws})
-        if (*p) { cudaFree(*p); *p = nullptr; }
-      return fail(c, SEREN_GPU_ERR_CUDA, "accrete: scratch allocation failed");
-    }
-  }
+  if (seren::sink_scratch(c)) return fail(c, SEREN_GPU_ERR_CUDA, "accrete: scratch allocation failed");
   const int ns = nsink;
   const int S = seren::ACC_STRIDE;
-  std::vector<double> rec((size_t)ns * S, 0.0);
-  for (int s = 0; s < ns; ++s) {
-    double* R = &rec[(size_t)s * S];
-    for (int k = 0; k < 5; ++k) R[k] = c.sink_rmh[s * 5 + k];
-    R[5] = c.sink_radius[s];
-    R[6] = (!accrete || accrete[s]) ? 1.0 : 0.0;
-    for (int k = 0; k < 3; ++k) {
-      R[7 + k] = c.sink_v[s * 3 + k];
-      R[10 + k] = c.sink_a[s * 3 + k];
-    }
-  }
-  cudaMemcpyAsync(c.acc_sinks, rec.data(), sizeof(double) * rec.size(), cudaMemcpyHostToDevice, c.st);
+  seren::sink_records(c, accrete);
   c.nlaunch = 0;
   std::vector<double> out;
   int ndead = 0;
@@ -1151,6 +1166,67 @@ int seren_gpu_accrete(seren_gpu_ctx* h, int32_t nsink, const int32_t* accrete,
     // the tree and neighbour lists index the old arrays: the next force step
     // builds a new tree (accrete_particles.F90:330, nstock = nsteps)
     c.have_tree = false;
+  }
+  if (ptot_out) *ptot_out = c.ptot;
+  return SEREN_GPU_OK;
+}
+
+int seren_gpu_sink_search(seren_gpu_ctx* h, const seren_gpu_sink_search_params* prm,
+                          int32_t* created, int32_t* psink_id, double* sink_angmom,
+                          int32_t* nremoved, int32_t* ptot_out) {
+  if (!h) return SEREN_GPU_ERR_ARG;
+  Ctx& c = h->c;
+  if (!prm || !(prm->sinkrad > 0.0))
+    return fail(c, SEREN_GPU_ERR_ARG, "sink_search: parameters with sinkrad > 0");
+  if (!c.have_tree || !c.have_v || !c.have_sph || c.ptot < 1)
+    return fail(c, SEREN_GPU_ERR_STATE, "sink_search: call seren_gpu_force_step first");
+  if (c.nsink >= 1024) return fail(c, SEREN_GPU_ERR_CAPACITY, "sink_search: 1024 sinks already");
+  if (c.nsink > 0 && !c.sink_move)
+    return fail(c, SEREN_GPU_ERR_STATE, "sink_search: call seren_gpu_set_sink_motion");
+  if (c.nsink > 0 && !c.sink_a_valid) {
+    const int rc = seren::sink_accels(c);
+    if (rc) return rc;
+  }
+  if (seren::sink_scratch(c)) return fail(c, SEREN_GPU_ERR_CUDA, "sink_search: scratch allocation failed");
+  seren::sink_records(c, nullptr);
+  const seren::SinkSearchArgs sa{prm->rhosink, prm->sinkrad, prm->hmult_sinkrad != 0,
+                                 prm->rho_search != 0, prm->potmin_search != 0,
+                                 prm->hill_sphere_search != 0, prm->div_v_search != 0,
+                                 prm->div_a_search != 0, prm->timescale_search != 0};
+  c.nlaunch = 0;
+  int psink = -1, pid = -1, nrem = 0;
+  std::vector<double> out;
+  int rc = seren::launch_sink_search(c, c.nsink, sa, psink, pid, out, nrem);
+  if (rc) return finish(c, "sink_search");
+  rc = finish(c, "sink_search");
+  if (rc) return rc;
+  if (created) *created = psink >= 0 ? 1 : 0;
+  if (psink_id) *psink_id = psink >= 0 ? pid + c.prm.index_base : -1;
+  if (nremoved) *nremoved = nrem;
+  if (psink >= 0) {
+    // create_sink.F90:153-201: the new sink (accreting, h = radius / 2)
+    const double rads = out[13];
+    const bool first = c.nsink == 0;
+    const size_t ns = (size_t)c.nsink;
+    c.sink_rmh.resize(5 * ns);
+    c.sink_v.resize(3 * ns);
+    c.sink_a.resize(3 * ns);
+    c.sink_radius.resize(ns);
+    for (int k = 0; k < 3; ++k) c.sink_rmh.push_back(out[1 + k]);
+    c.sink_rmh.push_back(out[0]);
+    c.sink_rmh.push_back(seren::INVKERNRANGE * rads);
+    for (int k = 0; k < 3; ++k) c.sink_v.push_back(out[4 + k]);
+    for (int k = 0; k < 3; ++k) c.sink_a.push_back(out[7 + k]);
+    c.sink_radius.push_back(rads);
+    c.sink_pot.resize((size_t)c.nsink + 1, 0.0);
+    c.nsink += 1;
+    c.sink_move = true;
+    if (first) c.sink_a_valid = true;
+    if (sink_angmom)
+      for (int k = 0; k < 3; ++k) sink_angmom[k] = out[10 + k];
+    rc = seren::sink_upload(c);
+    if (rc) return rc;
+    c.have_tree = false;                     // create_sink.F90:255-256: nbuild = nstock = nsteps
   }
   if (ptot_out) *ptot_out = c.ptot;
   return SEREN_GPU_OK;

@@ -55,7 +55,8 @@ struct DevError {
 
 enum KernelId : int {
   KID_BBOX = 1, KID_KEYS, KID_SORT, KID_SPLIT, KID_EMIT, KID_REORDER, KID_STOCK, KID_HGUESS,
-  KID_GRADH, KID_HMAX, KID_NEIB, KID_HYDRO, KID_GRAV, KID_GRAV_MIXED, KID_SINK, KID_THERMAL
+  KID_GRADH, KID_HMAX, KID_NEIB, KID_HYDRO, KID_GRAV, KID_GRAV_MIXED, KID_SINK, KID_THERMAL,
+  KID_SINK_SEARCH
 };
 
 __device__ __forceinline__ void set_error(DevError* e, int code, int where, int index, int aux) {

@@ -150,9 +150,9 @@ struct Ctx {
   double4* tabG = nullptr;
   float4* tabG32 = nullptr;   // FP32 w5, w4, w6 of tabG (mixed gravity)
 
-  // sink accretion (seren_gpu_accrete), made on first use: sink records and
-  // results, ACC_STRIDE doubles per sink for up to 1024 sinks, and 4 * pmax ints
-  // of scratch (sinks.cu)
+  // sink accretion and search (seren_gpu_accrete, seren_gpu_sink_search), made
+  // on first use: sink records and results, ACC_STRIDE doubles per sink for up
+  // to 1024 sinks, and 4 * pmax + 16 ints of scratch (sinks.cu)
   double* acc_sinks = nullptr;
   double* acc_out = nullptr;
   int* acc_ws = nullptr;
@@ -213,6 +213,24 @@ int grav_walk_stack_cap(const Ctx& c);  // stack entries per warp
 
 // sinks.cu
 constexpr int ACC_STRIDE = 16;
+// the options of sinks/sink_search.F90 (setup/default_parameters.F90:120-129)
+struct SinkSearchArgs {
+  double rhosink;
+  double sinkrad;
+  int hmult_sinkrad;
+  int rho_search;
+  int potmin_search;
+  int hill_sphere_search;
+  int div_v_search;
+  int div_a_search;
+  int timescale_search;
+};
+// sink_search + create_sink on the device-resident particles with the sinks
+// in c.acc_sinks: psink = the particle made a sink (-1: none; psink_id its id),
+// out = {m, x, y, z, vx, vy, vz, ax, ay, az, Lx, Ly, Lz, radius}, nremoved
+// particles removed (psink and its neighbours); c.ptot is the kept count
+int launch_sink_search(Ctx& c, int nsink, const SinkSearchArgs& sa, int& psink, int& psink_id,
+                       std::vector<double>& out, int& nremoved);
 // accrete_particles + remove_from_list on the device-resident particles with
 // the sinks in c.acc_sinks: ndead particles accreted (0: nothing changed); when
 // ndead > 0, out holds ACC_STRIDE doubles per sink and c.ptot is the kept count

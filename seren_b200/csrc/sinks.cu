@@ -22,6 +22,8 @@ namespace {
 
 inline int nb(long n, int t) { return (int)((n + t - 1) / t); }
 
+constexpr double SINK_PI = 3.1415926536;   // the reference's PI (headers/macros.h)
+
 // gravity/gravity_gradh.F90:11-95, the potential only, with zeta/omega = 0, as
 // accrete_particles.F90:186-188 calls it: the sink's 1/h is passed where the
 // routine takes the second body's h (hq below is that value)
@@ -235,29 +237,327 @@ __global__ void k_acc_compact(const int* __restrict__ live, int n, const double4
   }
 }
 
+// ---------------------------------------------------------------------------
+// Sink search (sinks/sink_search.F90:11-433) and creation (sinks/create_sink.F90:11-268)
+
+// BHtree/BHhydrowalk_hgather.F90:11-77: the depth-first walk over the cells
+// whose hydro sphere (bbox centre, rmax) comes within hrange of r, calling f on
+// every particle of each opened leaf.  The tree build numbers particles depth
+// first, so f sees them in increasing index order, the order of the
+// reference's potential-neighbour list.  At most 2 (ctot + 1) steps; more
+// means broken links and sets the error flag.
+template <class F>
+__device__ void hgather_walk(double rx, double ry, double rz, double hrange, int ctot,
+                             const int4* __restrict__ link, const double4* __restrict__ hA,
+                             DevError* err, F&& f) {
+  int c = 0;
+  long steps = 0;
+  const long cap = 2L * (ctot + 1) + 2;
+  while (c >= 0 && c <= ctot) {
+    if (++steps > cap) {
+      set_error(err, SEREN_GPU_ERR_WALK, KID_SINK_SEARCH, c, ctot);
+      return;
+    }
+    const double4 H = hA[c];
+    const int4 L = link[c];                 // leaf, nextcell, ifopen, pstart
+    const double d0 = H.x - rx, d1 = H.y - ry, d2 = H.z - rz;
+    const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
+    const double maxdistsqd = (hrange + H.w) * (hrange + H.w);
+    if (drsqd <= maxdistsqd) {
+      if (L.x > 0) {
+        for (int i = 0; i < L.x; ++i) f(L.w + i);
+        c = L.y;
+      } else if (L.x == 0) {
+        c = L.z;
+      } else {
+        c = L.y;
+      }
+    } else {
+      c = L.y;
+    }
+  }
+}
+
+// candidates by density (sink_search.F90:71-76): flag[p] = 1 unless rho_search
+// and rho < rhosink
+__global__ void k_ss_mark(int n, int rho_search, double rhosink, const double* __restrict__ rho,
+                          int* __restrict__ flag, int* __restrict__ mark) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const int f = (rho_search && rho[p] < rhosink) ? 0 : 1;
+  flag[p] = f;
+  mark[p] = f;
+}
+
+__global__ void k_ss_list(int n, const int* __restrict__ flag, const int* __restrict__ pos,
+                          int* __restrict__ list) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < n && flag[p]) list[pos[p]] = p;
+}
+
+// Every test of sink_search.F90 for one candidate per thread: the potential
+// minimum (all_sph_gradh.F90:355-471 over the gather neighbours within 2h),
+// the existing sinks (:158-200; the Hill test reads a_grav and the sinks'
+// agrav, which only DEBUG_FORCES builds fill: zero, so it rejects nothing),
+// the smoothed density, div v, div a and curl v over the neighbours within
+// max(sinkrad, 2h) (:212-303, the reference's expressions in order; div a
+// divides by the relative acceleration along the separation, as there), and
+// the timescale test (:311-410).  entry[i]: the candidate is still flagged when
+// the last of those loops reaches it (the loop that leaves psink = p); fin[i]:
+// it passed every test.
+__global__ void k_ss_test(int n1, const int* __restrict__ list, const double4* __restrict__ pm,
+                          const double2* __restrict__ hz, const double4* __restrict__ vel,
+                          const double* __restrict__ acc, const double* __restrict__ rho,
+                          const double* __restrict__ gpot, int ctot,
+                          const int4* __restrict__ link, const double4* __restrict__ hA,
+                          const double4* __restrict__ tabA, const double4* __restrict__ tabG,
+                          int nsink, const double* __restrict__ sk, SinkSearchArgs sa,
+                          int* __restrict__ entry, int* __restrict__ fin, DevError* err) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n1) return;
+  const int p = list[i];
+  const double4 P = pm[p];
+  const double hp = hz[p].x;
+  if (sa.potmin_search) {
+    const double invhp = 1.0 / hp;
+    const double hrangesqd = (KERNRANGESQD * hp) * hp;
+    double gpotmin = 0.0;
+    hgather_walk(P.x, P.y, P.z, KERNRANGE * hp, ctot, link, hA, err, [&](int pp) {
+      if (pp == p) return;
+      const double4 Q = pm[pp];
+      const double d0 = Q.x - P.x, d1 = Q.y - P.y, d2 = Q.z - P.z;
+      const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
+      if (drsqd > hrangesqd) return;
+      const double drmag = sqrt(drsqd) + SMALL_NUMBER;
+      const int kern = (int)((HALFKERNTOT * drmag) * invhp);
+      if (kern > KERNTOT) return;
+      gpotmin = fmin(-gpot[pp], gpotmin);
+    });
+    if (!(gpotmin > -gpot[p])) {
+      entry[i] = 0;
+      fin[i] = 0;
+      return;
+    }
+  }
+  bool flag = true;
+  if (nsink > 0) {
+    const double rhop = rho[p];
+    for (int s = 0; s < nsink; ++s) {
+      const double* S = sk + (size_t)s * ACC_STRIDE;
+      const double d0 = S[0] - P.x, d1 = S[1] - P.y, d2 = S[2] - P.z;
+      const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
+      const double rr = 2.0 * S[5];
+      if (drsqd < rr * rr) flag = false;
+      if (sa.hill_sphere_search) {
+        const double e0 = 0.0, e1 = 0.0, e2 = 0.0;        // sink agrav - particle a_grav
+        const double dadr = (e0 * d0 + e1 * d1) + e2 * d2;
+        const double rho_hill = -(3.0 * dadr) / ((4.0 * SINK_PI) * drsqd);
+        if (rhop < 3.0 * rho_hill) flag = false;
+      }
+    }
+  }
+  bool at_last = flag;                                   // entering the hydro loop
+  double div_v = 0.0;
+  if (flag) {
+    const double4 V = vel[p];
+    const double ax = acc[3 * (size_t)p], ay = acc[3 * (size_t)p + 1], az = acc[3 * (size_t)p + 2];
+    const double hrange = sa.hmult_sinkrad ? fmax(sa.sinkrad * hp, KERNRANGE * hp)
+                                           : fmax(sa.sinkrad, KERNRANGE * hp);
+    const double hrangesqd = hrange * hrange;
+    const double invhp = KERNRANGE / hrange;
+    const double hfactor = pow(invhp, NDIMPR);
+    double rhotemp = (P.w * tabA[0].x) * hfactor;
+    double dvp = 0.0, dap = 0.0, c0 = 0.0, c1 = 0.0, c2 = 0.0;
+    hgather_walk(P.x, P.y, P.z, hrange, ctot, link, hA, err, [&](int pp) {
+      if (pp == p) return;
+      const double4 Q = pm[pp];
+      const double d0 = Q.x - P.x, d1 = Q.y - P.y, d2 = Q.z - P.z;
+      double drmag = (d0 * d0 + d1 * d1) + d2 * d2;
+      if (drmag > hrangesqd) return;
+      drmag = sqrt(drmag) + SMALL_NUMBER;
+      const double invdrmag = 1.0 / drmag;
+      const int kern = (int)((HALFKERNTOT * drmag) * invhp);
+      if (kern > KERNTOT) return;
+      const double mpp = Q.w;
+      const double4 W = vel[pp];
+      const double v0 = W.x - V.x, v1 = W.y - V.y, v2 = W.z - V.z;
+      const double dvdr = (v0 * d0 + v1 * d1) + v2 * d2;
+      const double4 TA = tabA[kern];                   // w0, wh, w4, wg
+      const double w1 = tabG[kern].w;
+      rhotemp = rhotemp + (mpp * hfactor) * TA.x;
+      dvp = dvp - ((((mpp * dvdr) * TA.z) * hfactor) * invhp) * invdrmag;
+      const double dadr = ((acc[3 * (size_t)pp] - ax) * d0 + (acc[3 * (size_t)pp + 1] - ay) * d1) +
+                          (acc[3 * (size_t)pp + 2] - az) * d2;
+      dap = dap - ((((mpp * TA.z) * hfactor) * invhp) / dadr) * invdrmag;
+      const double x0 = v1 * d2 - v2 * d1, x1 = v2 * d0 - v0 * d2, x2 = v0 * d1 - v1 * d0;
+      c0 = c0 - ((((mpp * x0) * invdrmag) * w1) * hfactor) * invhp;
+      c1 = c1 - ((((mpp * x1) * invdrmag) * w1) * hfactor) * invhp;
+      c2 = c2 - ((((mpp * x2) * invdrmag) * w1) * hfactor) * invhp;
+    });
+    div_v = dvp / rhotemp;
+    const double div_a = dap / rhotemp;
+    if (sa.div_a_search && div_a > 0.0) flag = false;
+    if (sa.div_v_search && div_v > 0.0) flag = false;
+  }
+  if (nsink > 0) {
+    at_last = flag;                                      // entering the timescale loop
+    if (flag) {
+      const double4 V = vel[p];
+      for (int s = 0; s < nsink; ++s) {
+        const double* S = sk + (size_t)s * ACC_STRIDE;
+        const double d0 = S[0] - P.x, d1 = S[1] - P.y, d2 = S[2] - P.z;
+        const double drmag = sqrt((d0 * d0 + d1 * d1) + d2 * d2) + SMALL_NUMBER;
+        const double u0 = d0 / drmag, u1 = d1 / drmag, u2 = d2 / drmag;
+        const double e0 = S[7] - V.x, e1 = S[8] - V.y, e2 = S[9] - V.z;
+        const double drad = drmag - 2.0 * S[5];
+        const double vrad = (e0 * u0 + e1 * u1) + e2 * u2;
+        const double tacc1 = -drad / vrad;
+        const double tcond1 = -1.0 / div_v;
+        if (sa.timescale_search && tcond1 > tacc1) flag = false;
+      }
+    }
+  }
+  entry[i] = at_last ? 1 : 0;
+  fin[i] = flag ? 1 : 0;
+}
+
+// sink_search.F90:420-428: the candidates were sorted by density (stable) and
+// the last loop left p at the densest candidate it visited (ties: the highest
+// index); a sink is made there when any candidate passed every test
+__global__ void k_ss_select(int n1, const int* __restrict__ list, const double* __restrict__ rho,
+                            const int* __restrict__ entry, const int* __restrict__ fin,
+                            int* __restrict__ out) {
+  __shared__ double br[1024];
+  __shared__ int bp[1024];
+  __shared__ int any;
+  const int t = threadIdx.x;
+  if (t == 0) any = 0;
+  __syncthreads();
+  double best = 0.0;
+  int bestp = -1;
+  int anyf = 0;
+  for (int i = t; i < n1; i += blockDim.x) {
+    anyf |= fin[i];
+    if (!entry[i]) continue;
+    const int p = list[i];
+    const double r = rho[p];
+    if (bestp < 0 || r > best || (r == best && p > bestp)) {
+      best = r;
+      bestp = p;
+    }
+  }
+  if (anyf) atomicOr(&any, 1);
+  br[t] = best;
+  bp[t] = bestp;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (t < w) {
+      const int q = bp[t + w];
+      if (q >= 0 && (bp[t] < 0 || br[t + w] > br[t] || (br[t + w] == br[t] && q > bp[t]))) {
+        br[t] = br[t + w];
+        bp[t] = q;
+      }
+    }
+    __syncthreads();
+  }
+  if (t == 0) out[0] = any ? bp[0] : -1;
+}
+
+// create_sink.F90:98-103: psink and the particles within the new sink's
+// radius of it (gather_neib_on_fly with h = rads/2: within (2h)^2 inclusive)
+__global__ void k_cs_mark(int n, int psink, double hrangesqd, const double4* __restrict__ pm,
+                          int* __restrict__ dead, int* __restrict__ mark) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const double4 S = pm[psink];
+  const double4 Q = pm[p];
+  const double d0 = Q.x - S.x, d1 = Q.y - S.y, d2 = Q.z - S.z;
+  const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
+  const int d = (p == psink || drsqd <= hrangesqd) ? 0 : -1;
+  dead[p] = d;
+  mark[p] = d >= 0 ? 1 : 0;
+}
+
+// create_sink.F90:70-150 in one warp: the new sink's mass, centre of mass,
+// velocity and acceleration from psink then its neighbours in index order, and
+// the angular momentum about the centre of mass; out = {m, x, y, z, vx, vy,
+// vz, ax, ay, az, Lx, Ly, Lz}
+__global__ void k_cs_sink(int psink, const int* __restrict__ dlist, int nd,
+                          const double4* __restrict__ pm, const double4* __restrict__ vel,
+                          const double* __restrict__ acc, double* __restrict__ out) {
+  const int lane = threadIdx.x;
+  const double4 P = pm[psink];
+  const double4 V = vel[psink];
+  const double mp = P.w;
+  double ms = mp;
+  double r0 = mp * P.x, r1 = mp * P.y, r2 = mp * P.z;
+  double v0 = mp * V.x, v1 = mp * V.y, v2 = mp * V.z;
+  double a0 = mp * acc[3 * (size_t)psink], a1 = mp * acc[3 * (size_t)psink + 1],
+         a2 = mp * acc[3 * (size_t)psink + 2];
+  for (int base = 0; base < nd; base += 32) {
+    const int i = base + lane;
+    const int q0 = i < nd ? dlist[i] : -1;
+    unsigned m = __ballot_sync(0xffffffffu, q0 >= 0 && q0 != psink);
+    while (m) {
+      const int j = __ffs(m) - 1;
+      m &= m - 1;
+      const int q = __shfl_sync(0xffffffffu, q0, j);
+      const double4 Q = pm[q];
+      const double4 W = vel[q];
+      const double* A = acc + 3 * (size_t)q;
+      const double mq = Q.w;
+      ms = ms + mq;
+      r0 = r0 + mq * Q.x; r1 = r1 + mq * Q.y; r2 = r2 + mq * Q.z;
+      v0 = v0 + mq * W.x; v1 = v1 + mq * W.y; v2 = v2 + mq * W.z;
+      a0 = a0 + mq * A[0]; a1 = a1 + mq * A[1]; a2 = a2 + mq * A[2];
+    }
+  }
+  r0 = r0 / ms; r1 = r1 / ms; r2 = r2 / ms;
+  v0 = v0 / ms; v1 = v1 / ms; v2 = v2 / ms;
+  a0 = a0 / ms; a1 = a1 / ms; a2 = a2 / ms;
+  // psink: dr = r_sink - r_p, dv = v_sink - v_p
+  double L0, L1, L2;
+  {
+    const double d0 = r0 - P.x, d1 = r1 - P.y, d2 = r2 - P.z;
+    const double e0 = v0 - V.x, e1 = v1 - V.y, e2 = v2 - V.z;
+    L0 = (mp * d1) * e2 - (mp * d2) * e1;
+    L1 = (mp * d2) * e0 - (mp * d0) * e2;
+    L2 = (mp * d0) * e1 - (mp * d1) * e0;
+  }
+  for (int base = 0; base < nd; base += 32) {
+    const int i = base + lane;
+    const int q0 = i < nd ? dlist[i] : -1;
+    unsigned m = __ballot_sync(0xffffffffu, q0 >= 0 && q0 != psink);
+    while (m) {
+      const int j = __ffs(m) - 1;
+      m &= m - 1;
+      const int q = __shfl_sync(0xffffffffu, q0, j);
+      const double4 Q = pm[q];
+      const double4 W = vel[q];
+      const double mq = Q.w;
+      const double d0 = r0 - Q.x, d1 = r1 - Q.y, d2 = r2 - Q.z;
+      const double e0 = v0 - W.x, e1 = v1 - W.y, e2 = v2 - W.z;
+      L0 = (L0 + (mq * d1) * e2) - (mq * d2) * e1;
+      L1 = (L1 + (mq * d2) * e0) - (mq * d0) * e2;
+      L2 = (L2 + (mq * d0) * e1) - (mq * d1) * e0;
+    }
+  }
+  if (lane == 0) {
+    out[0] = ms;
+    out[1] = r0; out[2] = r1; out[3] = r2;
+    out[4] = v0; out[5] = v1; out[6] = v2;
+    out[7] = a0; out[8] = a1; out[9] = a2;
+    out[10] = L0; out[11] = L1; out[12] = L2;
+  }
+}
+
 }  // namespace
 
-int launch_accrete(Ctx& c, int nsink, int energy, std::vector<double>& out, int& ndead) {
-  const int n = c.ptot;
+// remove_from_list.F90:46-62 on the device: the kept particles (live, in
+// index order) gathered into the spare buffers, which become the arrays; a and
+// gpot go through the staging buffer
+void remove_dead(Ctx& c, const int* live, int nlive) {
   const size_t P = (size_t)c.pmax;
-  int* dead = c.acc_ws;
-  int* mark = c.acc_ws + P;
-  int* dlist = c.acc_ws + 2 * P;
-  int* live = c.acc_ws + 3 * P;
-  ndead = 0;
-  k_acc_flag<<<nb(n, 256), 256, 0, c.st>>>(n, nsink, energy, c.pm, c.hz, c.vel, c.acc_sinks,
-                                            c.tabG, dead, mark); ++c.nlaunch;
-  scan_exclusive(c, mark, mark, n);
-  int rc = read_dev(c, c.scan.total, &ndead, sizeof(int));
-  if (rc) return rc;
-  if (ndead <= 0) return SEREN_GPU_OK;
-  k_acc_lists<<<nb(n, 256), 256, 0, c.st>>>(n, dead, mark, dlist, live); ++c.nlaunch;
-  k_acc_sinks<<<nsink, 32, 0, c.st>>>(nsink, c.acc_sinks, dlist, ndead, dead, c.pm, c.vel, c.acc,
-                                       c.acc_out); ++c.nlaunch;
-  out.assign((size_t)nsink * ACC_STRIDE, 0.0);
-  cudaMemcpyAsync(out.data(), c.acc_out, sizeof(double) * out.size(), cudaMemcpyDeviceToHost, c.st);
-  // the kept particles, gathered into the spare buffers; a and gpot through the staging buffer
-  const int nlive = n - ndead;
   double* acc2 = c.stage;
   double* gpot2 = c.stage + 3 * P;
   if (nlive > 0) {
@@ -284,6 +584,80 @@ int launch_accrete(Ctx& c, int nsink, int energy, std::vector<double>& out, int&
     std::swap(c.v_half, c.v_half_alt);
   }
   c.ptot = nlive;
+}
+
+int launch_accrete(Ctx& c, int nsink, int energy, std::vector<double>& out, int& ndead) {
+  const int n = c.ptot;
+  const size_t P = (size_t)c.pmax;
+  int* dead = c.acc_ws;
+  int* mark = c.acc_ws + P;
+  int* dlist = c.acc_ws + 2 * P;
+  int* live = c.acc_ws + 3 * P;
+  ndead = 0;
+  k_acc_flag<<<nb(n, 256), 256, 0, c.st>>>(n, nsink, energy, c.pm, c.hz, c.vel, c.acc_sinks,
+                                            c.tabG, dead, mark); ++c.nlaunch;
+  scan_exclusive(c, mark, mark, n);
+  int rc = read_dev(c, c.scan.total, &ndead, sizeof(int));
+  if (rc) return rc;
+  if (ndead <= 0) return SEREN_GPU_OK;
+  k_acc_lists<<<nb(n, 256), 256, 0, c.st>>>(n, dead, mark, dlist, live); ++c.nlaunch;
+  k_acc_sinks<<<nsink, 32, 0, c.st>>>(nsink, c.acc_sinks, dlist, ndead, dead, c.pm, c.vel, c.acc,
+                                       c.acc_out); ++c.nlaunch;
+  out.assign((size_t)nsink * ACC_STRIDE, 0.0);
+  cudaMemcpyAsync(out.data(), c.acc_out, sizeof(double) * out.size(), cudaMemcpyDeviceToHost, c.st);
+  remove_dead(c, live, n - ndead);
+  return SEREN_GPU_OK;
+}
+
+int launch_sink_search(Ctx& c, int nsink, const SinkSearchArgs& sa, int& psink, int& psink_id,
+                       std::vector<double>& out, int& nremoved) {
+  const int n = c.ptot;
+  const size_t P = (size_t)c.pmax;
+  int* flag = c.acc_ws;
+  int* mark = c.acc_ws + P;
+  int* list = c.acc_ws + 2 * P;
+  int* live = c.acc_ws + 3 * P;
+  psink = -1;
+  nremoved = 0;
+  k_ss_mark<<<nb(n, 256), 256, 0, c.st>>>(n, sa.rho_search, sa.rhosink, c.rho, flag, mark);
+  ++c.nlaunch;
+  scan_exclusive(c, mark, mark, n);
+  int n1 = 0;
+  int rc = read_dev(c, c.scan.total, &n1, sizeof(int));
+  if (rc) return rc;
+  if (n1 <= 0) return SEREN_GPU_OK;
+  k_ss_list<<<nb(n, 256), 256, 0, c.st>>>(n, flag, mark, list); ++c.nlaunch;
+  // per-candidate results in the first two scratch arrays (their flags are used up)
+  int* entry = flag;
+  int* fin = mark;
+  k_ss_test<<<nb(n1, 64), 64, 0, c.st>>>(n1, list, c.pm, c.hz, c.vel, c.acc, c.rho, c.gpot,
+                                          c.info.ctot, c.link, c.hA, c.tabA, c.tabG, nsink,
+                                          c.acc_sinks, sa, entry, fin, c.d_err); ++c.nlaunch;
+  k_ss_select<<<1, 1024, 0, c.st>>>(n1, list, c.rho, entry, fin, c.acc_ws + 4 * P); ++c.nlaunch;
+  rc = read_dev(c, c.acc_ws + 4 * P, &psink, sizeof(int));
+  if (rc) return rc;
+  if (psink < 0) return SEREN_GPU_OK;
+  // create_sink: psink and its neighbours within the sink radius leave
+  rc = read_dev(c, c.orig + psink, &psink_id, sizeof(int));
+  if (rc) return rc;
+  double2 hzp{0.0, 0.0};
+  if (sa.hmult_sinkrad && (rc = read_dev(c, c.hz + psink, &hzp, sizeof(double2)))) return rc;
+  const double rads = sa.hmult_sinkrad ? sa.sinkrad * hzp.x : sa.sinkrad;
+  const double hh = INVKERNRANGE * rads;
+  int* dead = c.acc_ws;
+  int* dlist = c.acc_ws + 2 * P;
+  k_cs_mark<<<nb(n, 256), 256, 0, c.st>>>(n, psink, (KERNRANGESQD * hh) * hh, c.pm, dead, mark);
+  ++c.nlaunch;
+  scan_exclusive(c, mark, mark, n);
+  rc = read_dev(c, c.scan.total, &nremoved, sizeof(int));
+  if (rc) return rc;
+  k_acc_lists<<<nb(n, 256), 256, 0, c.st>>>(n, dead, mark, dlist, live); ++c.nlaunch;
+  k_cs_sink<<<1, 32, 0, c.st>>>(psink, dlist, nremoved, c.pm, c.vel, c.acc, c.acc_out);
+  ++c.nlaunch;
+  out.assign(ACC_STRIDE, 0.0);
+  cudaMemcpyAsync(out.data(), c.acc_out, sizeof(double) * ACC_STRIDE, cudaMemcpyDeviceToHost, c.st);
+  out[13] = rads;
+  remove_dead(c, live, n - nremoved);
   return SEREN_GPU_OK;
 }
 

@@ -42,6 +42,7 @@ def library(build_if_missing: bool = True) -> C.CDLL:
                            ("get_sinks", [vp, C.c_int32, _dp, _dp, _dp, _dp]),
                            ("sink_timestep", [vp, C.c_double, _dp]),
                            ("accrete", [vp, C.c_int32, _ip, C.c_int32, _dp, _ip, _ip]),
+                           ("sink_search", [vp, C.c_void_p, _ip, _ip, _dp, _ip, _ip]),
                            ("set_sinks", [vp, C.c_int32, _dp]),
                            ("download", [vp, _dp, _dp, _dp, _dp, _dp, _dp, _ip]),
                            ("last_step_stats", [vp, _dp, _ip, C.POINTER(C.c_int64)]),
@@ -54,6 +55,14 @@ def library(build_if_missing: bool = True) -> C.CDLL:
     return _lib
 
 
+class SinkSearchParams(C.Structure):
+    """seren_gpu_sink_search_params of include/seren_gpu.h."""
+    _fields_ = [("rhosink", C.c_double), ("sinkrad", C.c_double)] + [
+        (n, C.c_int32) for n in ("hmult_sinkrad", "rho_search", "potmin_search",
+                                 "hill_sphere_search", "div_v_search", "div_a_search",
+                                 "timescale_search", "reserved")]
+
+
 def _d(a):
     return None if a is None else a.ctypes.data_as(_dp)
 
@@ -61,6 +70,7 @@ def _d(a):
 class GpuHotPath(HotPath):
     def __init__(self, pmax: int, params: Params):
         super().__init__(library(), "seren_gpu", pmax, params)
+        self.nsink = 0
 
     # -- device-resident step -------------------------------------------------
     def upload(self, parray, v, csq):
@@ -138,6 +148,26 @@ class GpuHotPath(HotPath):
                    C.byref(ptot))
         self.ptot = ptot.value
         return cnt
+
+    def sink_search(self, rhosink, sinkrad, hmult_sinkrad=False, rho_search=True,
+                    potmin_search=True, hill_sphere_search=True, div_v_search=True,
+                    div_a_search=True, timescale_search=False):
+        """Sink search and creation (seren_gpu_sink_search); the defaults are
+        the reference's (setup/default_parameters.F90:120-129).  Returns a
+        dict: created, psink_id, angmom [3], nremoved; self.nsink and
+        self.ptot follow."""
+        prm = SinkSearchParams(float(rhosink), float(sinkrad), int(hmult_sinkrad), int(rho_search),
+                               int(potmin_search), int(hill_sphere_search), int(div_v_search),
+                               int(div_a_search), int(timescale_search), 0)
+        created, pid, nrem, ptot = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
+        angmom = np.zeros(3)
+        self._call("sink_search", self._ctx, C.cast(C.byref(prm), C.c_void_p), C.byref(created),
+                   C.byref(pid), _d(angmom), C.byref(nrem), C.byref(ptot))
+        self.ptot = ptot.value
+        if created.value:
+            self.nsink += 1
+        return dict(created=bool(created.value), psink_id=pid.value, angmom=angmom,
+                    nremoved=nrem.value)
 
     def drift(self, dt: float):
         self._call("drift", self._ctx, C.c_double(dt))

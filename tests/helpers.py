@@ -25,6 +25,17 @@ def case(name: str):
     elif name == "ragged777":          # ragged size, not a multiple of any tile
         ic = ics.uniform_sphere(n=777, seed=3)
         ic["v"] = np.random.Generator(np.random.PCG64(9)).normal(0, 0.1, (777, 3))
+    elif name == "clumps12k":          # three dense Plummer clumps (sink search)
+        parts = []
+        for centre, seed in (((-1.0, 0.0, 0.0), 11), ((1.0, 0.0, 0.0), 12), ((0.0, 1.0, 0.2), 13)):
+            q = ics.plummer(n=4000, seed=seed, a=0.1, mass=1.0 / 3.0, rtrunc=1.0)
+            q["parray"][:, 0:3] += np.array(centre)
+            q["v"] *= 0.3
+            parts.append(q)
+        ic = dict(parts[0])
+        ic["parray"] = np.vstack([q["parray"] for q in parts])
+        ic["v"] = np.vstack([q["v"] for q in parts])
+        ic["sound"] = np.full(ic["parray"].shape[0], 0.1)
     elif name == "tiny100":            # just above pp_gather
         ic = ics.uniform_sphere(n=100, seed=5)
     else:

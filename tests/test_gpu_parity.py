@@ -552,3 +552,70 @@ def test_accretion_matches_oracle(libs, energy, flags):
     st2 = g.download()
     assert np.array_equal(np.sort(st2["perm"]), np.sort(st1["perm"]))
     assert np.isfinite(st2["a"]).all()
+
+
+def test_sink_search_matches_oracle(libs):
+    """Sink search and creation on the device (sink_search.F90, create_sink.F90)
+    against the oracle on the same state, three dense clumps: first with no
+    sink (the densest candidate fails div v / div a, a lighter one passes, and
+    the sink is made at the densest, as the reference's loop leaves it), then,
+    after a force step that includes the new sink, a second search with it in
+    place (overlap, Hill and timescale tests, the radius in units of h).  The
+    chosen particle, the new sink's mass, position, velocity, acceleration and
+    angular momentum (FP64 sums in index order: bit-exact) and the kept
+    particles in their order all match."""
+    from oracle.oracle import sink_search
+    ic = case("clumps12k")
+    _, g = _pair(libs, ic)
+    g.upload(ic["parray"], ic["v"], ic["sound"] ** 2)
+    g.force_step(first_call=True)
+    st = g.download()
+    p = st["parray"]
+    rhosink = float(np.percentile(st["rho"], 90))
+    none = (np.zeros((0, 5)), np.zeros((0, 3)), np.zeros((0, 3)), np.zeros(0))
+    want = sink_search(p[:, 0:3], p[:, 3], p[:, 4], st["v"], st["a"], st["rho"], st["gpot"],
+                       *none, rhosink=rhosink, sinkrad=0.05)
+    assert want["psink"] >= 0 and want["flags"][-1] is False
+    got = g.sink_search(rhosink, 0.05)
+    assert got["created"] and got["psink_id"] == st["perm"][want["psink"]]
+    assert got["nremoved"] == len(want["removed"]) and g.ptot == len(want["keep"])
+    assert np.array_equal(got["angmom"], want["angmom"])
+    s1 = g.get_sinks()
+    assert g.nsink == 1
+    assert np.array_equal(s1["rmh"][0], np.r_[want["r"], want["m"], want["h"]])
+    assert np.array_equal(s1["v"][0], want["v"]) and np.array_equal(s1["a"][0], want["a"])
+    st1 = g.download()
+    keep = want["keep"]
+    assert np.array_equal(st1["perm"], st["perm"][keep])
+    assert np.array_equal(st1["parray"], p[keep]) and np.array_equal(st1["v"], st["v"][keep])
+    # a second search with the sink in place (overlap, Hill and timescale loops)
+    g.force_step(first_call=False)
+    st2, s2 = g.download(), g.get_sinks()
+    p2 = st2["parray"]
+    args = dict(rhosink=rhosink, sinkrad=0.05, div_a_search=False)
+    want2 = sink_search(p2[:, 0:3], p2[:, 3], p2[:, 4], st2["v"], st2["a"], st2["rho"],
+                        st2["gpot"], s2["rmh"], s2["v"], s2["a"], np.full(1, 0.05), **args)
+    assert want2["psink"] >= 0
+    got2 = g.sink_search(**args)
+    assert got2["created"] and got2["psink_id"] == st2["perm"][want2["psink"]]
+    assert np.array_equal(got2["angmom"], want2["angmom"])
+    s3 = g.get_sinks()
+    assert g.nsink == 2 and np.array_equal(s3["rmh"][0], s2["rmh"][0])
+    assert np.array_equal(s3["rmh"][1], np.r_[want2["r"], want2["m"], want2["h"]])
+    assert np.array_equal(g.download()["perm"], st2["perm"][want2["keep"]])
+    # the radius in units of h and the timescale test
+    g.force_step(first_call=False)
+    st3, s3 = g.download(), g.get_sinks()
+    p3 = st3["parray"]
+    args = dict(rhosink=rhosink, sinkrad=0.6, hmult_sinkrad=True, timescale_search=True)
+    want3 = sink_search(p3[:, 0:3], p3[:, 3], p3[:, 4], st3["v"], st3["a"], st3["rho"],
+                        st3["gpot"], s3["rmh"], s3["v"], s3["a"], np.full(2, 0.05), **args)
+    got3 = g.sink_search(**args)
+    assert got3["created"] == (want3["psink"] >= 0)
+    if got3["created"]:
+        assert got3["psink_id"] == st3["perm"][want3["psink"]]
+        assert np.array_equal(got3["angmom"], want3["angmom"])
+    else:
+        assert g.ptot == p3.shape[0] and np.array_equal(g.download()["perm"], st3["perm"])
+    g.force_step(first_call=False)
+    assert np.isfinite(g.download()["a"]).all()

@@ -245,3 +245,43 @@ def test_accretion_conserves_mass_momentum_and_angular_momentum():
         L1 = w["rmh"][s, 3] * np.cross(w["rmh"][s, 0:3], w["v"][s]) + w["angmom"][s]
         assert np.allclose(L1, L0, rtol=1e-10, atol=1e-15)
     assert np.array_equal(w["keep"], np.flatnonzero(w["dead"] < 0))
+
+
+def test_sink_search_picks_as_the_reference_does():
+    """The sink search restatement (sink_search.F90, create_sink.F90) on three
+    dense clumps: the three potential minima are the candidates; with the
+    div v / div a tests the densest fails and a lighter one passes, and the
+    sink is made at the densest all the same (the last loop leaves psink at
+    the densest candidate it visited); the new sink holds the mass, centre of
+    mass and momentum of the particles it removes, and the angular momentum
+    about its centre."""
+    from oracle.oracle import sink_search
+    ic = case("clumps12k")
+    n = ic["parray"].shape[0]
+    o = Oracle(n, params(ic))
+    r = run_pipeline(o, ic)
+    p, rho, g = r["sph"]["parray"], r["sph"]["rho"], r["gpot"]
+    none = (np.zeros((0, 5)), np.zeros((0, 3)), np.zeros((0, 3)), np.zeros(0))
+    s = sink_search(p[:, 0:3], p[:, 3], p[:, 4], r["v"], r["a"], rho, g, *none,
+                    rhosink=np.percentile(rho, 90), sinkrad=0.05)
+    cand = s["candidates"]
+    assert len(cand) == 3 and list(np.argsort(rho[cand])) == [0, 1, 2]
+    assert s["flags"][2] is False and any(s["flags"])
+    assert s["psink"] == cand[2]
+    gone = s["removed"]
+    assert s["psink"] in gone and len(gone) > 100
+    d = np.sqrt(np.sum((p[gone, 0:3] - p[s["psink"], 0:3]) ** 2, axis=1))
+    assert d.max() <= 0.05 * (1 + 1e-12)
+    m = p[gone, 3]
+    assert np.isclose(s["m"], m.sum(), rtol=1e-14)
+    assert np.allclose(s["r"], (m[:, None] * p[gone, 0:3]).sum(0) / m.sum(), rtol=1e-12)
+    assert np.allclose(s["v"], (m[:, None] * r["v"][gone]).sum(0) / m.sum(), rtol=1e-12, atol=1e-15)
+    L = (m[:, None] * np.cross(p[gone, 0:3] - s["r"], r["v"][gone] - s["v"])).sum(0)
+    assert np.allclose(s["angmom"], L, rtol=1e-9, atol=1e-18)
+    assert s["h"] == 0.025 and s["radius"] == 0.05
+    assert np.array_equal(np.sort(np.concatenate([s["keep"], gone])), np.arange(n))
+    # no density or divergence tests: the densest candidate passes and is taken
+    s2 = sink_search(p[:, 0:3], p[:, 3], p[:, 4], r["v"], r["a"], rho, g, *none,
+                     rhosink=np.percentile(rho, 90), sinkrad=0.05, div_v_search=False,
+                     div_a_search=False)
+    assert s2["psink"] == cand[2] and all(s2["flags"])
