@@ -164,7 +164,7 @@ int seren_gpu_get_sinks(seren_gpu_ctx* ctx, int32_t nsink, double* sink_rmh, dou
  * sph_sim/sph_timesteps.F90:69-74 folds into the global minimum. */
 int seren_gpu_sink_timestep(seren_gpu_ctx* ctx, double sink_mult, double* dt_min);
 /* Sink accretion on the device-resident particles, replacing
- * sinks/accrete_particles.F90:14-365 with main/remove_from_list.F90:10-96
+ * sinks/accrete_particles.F90:16-365 with main/remove_from_list.F90:10-96
  * (called by sinks/sink_update.F90:24 after the step's advance).  Each particle
  * inside the radius of an accreting sink (accrete[s] != 0; NULL: every sink)
  * goes to the nearest one; with energy_accrete it must also be bound to it
@@ -199,7 +199,7 @@ typedef struct {
 } seren_gpu_sink_search_params;
 
 /* Sink search and creation on the device-resident particles, replacing
- * sinks/sink_search.F90:11-433 with sinks/create_sink.F90:11-268 (called by
+ * sinks/sink_search.F90:25-433 with sinks/create_sink.F90:11-268 (called by
  * sinks/sink_update.F90:16-20 every nsearchstep steps).  Candidates: rho >=
  * rhosink (rho_search), a minimum of the potential over the gather
  * neighbours (potmin_search), not within 2 radii of a sink, the Hill test

@@ -139,7 +139,7 @@ def _accrete_pot(d, invhp, hq, mq, w6):
 
 def accrete_particles(r, m, h, v, a, sink_rmh, sink_v, sink_a, sink_radius, accrete=None,
                       energy_accrete=False):
-    """sinks/accrete_particles.F90:14-365 and main/remove_from_list.F90:10-96
+    """sinks/accrete_particles.F90:16-365 and main/remove_from_list.F90:10-96
     for particles r [N,3], m, h, v, a [N,3] (all gas) and sinks rmh [S,5] (x,
     y, z, m, h), v, a [S,3], radius [S].  Every particle inside an accreting
     sink's radius goes to the nearest such sink (:82-106; a later sink only
@@ -246,7 +246,7 @@ def sink_search(r, m, h, v, a, rho, gpot, sink_rmh, sink_v, sink_a, sink_radius,
                 rhosink, sinkrad, hmult_sinkrad=False, rho_search=True, potmin_search=True,
                 hill_sphere_search=True, div_v_search=True, div_a_search=True,
                 timescale_search=False):
-    """sinks/sink_search.F90:11-433 and sinks/create_sink.F90:11-268 on
+    """sinks/sink_search.F90:25-433 and sinks/create_sink.F90:11-268 on
     particles in tree order (r [N,3], m, h, v [N,3], a [N,3], rho, gpot) with
     existing sinks (rmh [S,5], v, a [S,3], radius [S]).  Returns psink (-1: no sink made), the
     candidates in density order with their flags, and for a new sink its
@@ -257,7 +257,7 @@ def sink_search(r, m, h, v, a, rho, gpot, sink_rmh, sink_v, sink_a, sink_radius,
     (sph_sim/sph_grav_forces.F90:128-130; otherwise zero, so the test never
     rejects); div a divides by the
     dot product of the relative acceleration and separation; the particle
-    made a sink is the one the last candidate loop visited last (:420-426
+    made a sink is the one the last candidate loop visited last (:405-413
     assign psink = p), which can be a candidate that failed that loop's
     test when a lower-density one passed."""
     r, v, a = (np.asarray(x, np.float64).reshape(-1, 3) for x in (r, v, a))
@@ -279,7 +279,7 @@ def sink_search(r, m, h, v, a, rho, gpot, sink_rmh, sink_v, sink_a, sink_radius,
     k = len(cand)
     flag = [True] * k
     srho = [float(rho[p]) for p in cand]
-    if stot > 0:                                    # :158-200
+    if stot > 0:                                    # :155-200
         for i, p in enumerate(cand):
             rp = r[p].tolist()
             for s in range(stot):
@@ -295,7 +295,7 @@ def sink_search(r, m, h, v, a, rho, gpot, sink_rmh, sink_v, sink_a, sink_radius,
                         flag[i] = False
     last = -1                                       # the last candidate a loop visits
     div_v = [0.0] * k
-    for i, p in enumerate(cand):                    # :212-303
+    for i, p in enumerate(cand):                    # :221-300
         if not flag[i]:
             continue
         last = i
@@ -335,7 +335,7 @@ def sink_search(r, m, h, v, a, rho, gpot, sink_rmh, sink_v, sink_a, sink_radius,
             flag[i] = False
         if div_v_search and div_v[i] > 0.0:
             flag[i] = False
-    if stot > 0:                                    # :311-410, only tacc1 and tcond1 decide
+    if stot > 0:                                    # :328-400, only tacc1 and tcond1 decide
         last = -1
         for i, p in enumerate(cand):
             if not flag[i]:
@@ -358,7 +358,7 @@ def sink_search(r, m, h, v, a, rho, gpot, sink_rmh, sink_v, sink_a, sink_radius,
         return out
     psink = cand[last]
     out["psink"] = psink
-    # create_sink.F90:70-230
+    # create_sink.F90:64-244
     rp, vp = r[psink].tolist(), v[psink].tolist()
     mp, hp = float(m[psink]), float(h[psink])
     msink = mp

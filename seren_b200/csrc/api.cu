@@ -1204,7 +1204,7 @@ int seren_gpu_sink_search(seren_gpu_ctx* h, const seren_gpu_sink_search_params* 
   if (psink_id) *psink_id = psink >= 0 ? pid + c.prm.index_base : -1;
   if (nremoved) *nremoved = nrem;
   if (psink >= 0) {
-    // create_sink.F90:153-201: the new sink (accreting, h = radius / 2)
+    // create_sink.F90:160-201: the new sink (accreting, h = radius / 2)
     const double rads = out[13];
     const bool first = c.nsink == 0;
     const size_t ns = (size_t)c.nsink;
@@ -1226,7 +1226,7 @@ int seren_gpu_sink_search(seren_gpu_ctx* h, const seren_gpu_sink_search_params* 
       for (int k = 0; k < 3; ++k) sink_angmom[k] = out[10 + k];
     rc = seren::sink_upload(c);
     if (rc) return rc;
-    c.have_tree = false;                     // create_sink.F90:255-256: nbuild = nstock = nsteps
+    c.have_tree = false;                     // create_sink.F90:250-251: nbuild = nstock = nsteps
   }
   if (ptot_out) *ptot_out = c.ptot;
   return SEREN_GPU_OK;

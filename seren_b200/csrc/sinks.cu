@@ -1,4 +1,4 @@
-// Sink accretion on the device-resident particles: sinks/accrete_particles.F90:14-365
+// Sink accretion on the device-resident particles: sinks/accrete_particles.F90:16-365
 // (each gas particle inside the radius of an accreting sink is given to the nearest
 // such sink; when bound to it, or always without the energy test, its mass, momentum
 // and mass-weighted acceleration go to the sink, which moves to the new centre of mass
@@ -238,7 +238,7 @@ __global__ void k_acc_compact(const int* __restrict__ live, int n, const double4
 }
 
 // ---------------------------------------------------------------------------
-// Sink search (sinks/sink_search.F90:11-433) and creation (sinks/create_sink.F90:11-268)
+// Sink search (sinks/sink_search.F90:25-433) and creation (sinks/create_sink.F90:11-268)
 
 // BHtree/BHhydrowalk_hgather.F90:11-77: the depth-first walk over the cells
 // whose hydro sphere (bbox centre, rmax) comes within hrange of r, calling f on
@@ -278,7 +278,7 @@ __device__ void hgather_walk(double rx, double ry, double rz, double hrange, int
   }
 }
 
-// candidates by density (sink_search.F90:71-76): flag[p] = 1 unless rho_search
+// candidates by density (sink_search.F90:106-131): flag[p] = 1 unless rho_search
 // and rho < rhosink
 __global__ void k_ss_mark(int n, int rho_search, double rhosink, const double* __restrict__ rho,
                           int* __restrict__ flag, int* __restrict__ mark) {
@@ -297,12 +297,12 @@ __global__ void k_ss_list(int n, const int* __restrict__ flag, const int* __rest
 
 // Every test of sink_search.F90 for one candidate per thread: the potential
 // minimum (all_sph_gradh.F90:355-471 over the gather neighbours within 2h),
-// the existing sinks (:158-200; the Hill test reads a_grav and the sinks'
+// the existing sinks (:155-200; the Hill test reads a_grav and the sinks'
 // agrav, which only DEBUG_FORCES builds fill: zero, so it rejects nothing),
 // the smoothed density, div v, div a and curl v over the neighbours within
-// max(sinkrad, 2h) (:212-303, the reference's expressions in order; div a
+// max(sinkrad, 2h) (:221-300, the reference's expressions in order; div a
 // divides by the relative acceleration along the separation, as there), and
-// the timescale test (:311-410).  entry[i]: the candidate is still flagged when
+// the timescale test (:328-400).  entry[i]: the candidate is still flagged when
 // the last of those loops reaches it (the loop that leaves psink = p); fin[i]:
 // it passed every test.
 __global__ void k_ss_test(int n1, const int* __restrict__ list, const double4* __restrict__ pm,
@@ -421,7 +421,7 @@ __global__ void k_ss_test(int n1, const int* __restrict__ list, const double4* _
   fin[i] = flag ? 1 : 0;
 }
 
-// sink_search.F90:420-428: the candidates were sorted by density (stable) and
+// sink_search.F90:405-423: the candidates were sorted by density (stable) and
 // the last loop left p at the densest candidate it visited (ties: the highest
 // index); a sink is made there when any candidate passed every test
 __global__ void k_ss_select(int n1, const int* __restrict__ list, const double* __restrict__ rho,
@@ -463,7 +463,7 @@ __global__ void k_ss_select(int n1, const int* __restrict__ list, const double* 
   if (t == 0) out[0] = any ? bp[0] : -1;
 }
 
-// create_sink.F90:98-103: psink and the particles within the new sink's
+// create_sink.F90:88 and sph/gather_neib_on_fly.F90: psink and the particles within the new sink's
 // radius of it (gather_neib_on_fly with h = rads/2: within (2h)^2 inclusive)
 __global__ void k_cs_mark(int n, int psink, double hrangesqd, const double4* __restrict__ pm,
                           int* __restrict__ dead, int* __restrict__ mark) {
@@ -478,7 +478,7 @@ __global__ void k_cs_mark(int n, int psink, double hrangesqd, const double4* __r
   mark[p] = d >= 0 ? 1 : 0;
 }
 
-// create_sink.F90:70-150 in one warp: the new sink's mass, centre of mass,
+// create_sink.F90:64-150 in one warp: the new sink's mass, centre of mass,
 // velocity and acceleration from psink then its neighbours in index order, and
 // the angular momentum about the centre of mass; out = {m, x, y, z, vx, vy,
 // vz, ax, ay, az, Lx, Ly, Lz}
