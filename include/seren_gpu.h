@@ -225,6 +225,17 @@ int seren_gpu_sink_search(seren_gpu_ctx* ctx, const seren_gpu_sink_search_params
  * for sink_rmh[s] = {x, y, z, m, h}, as seren_gpu_grav_forces does with
  * nsink > 0 (at most 1024 sinks; nsink = 0 removes them). */
 int seren_gpu_set_sinks(seren_gpu_ctx* ctx, int32_t nsink, const double* sink_rmh);
+/* Build schedule of the device-resident force steps (seren_gpu_force_step and
+ * the evaluations inside seren_gpu_rk2_step), as main/tree_update.F90:26-88
+ * with the reference's nbuildstep (default there 8; here 1, a build every
+ * evaluation): the tree is built on the next evaluation and then every
+ * nbuildstep evaluations; in between the same cells are restocked at the new
+ * positions (BHgrav_stock, BHhydro_stock) and the particles keep their
+ * order.  A build also happens after an upload, on a first call, after
+ * accretion or sink creation, and when a particle has moved beyond twice
+ * the root cell's half width from its centre (the bound of the walks' FP32
+ * node records).  seren_gpu_force_step_io always builds. */
+int seren_gpu_set_build_step(seren_gpu_ctx* ctx, int32_t nbuildstep);
 int seren_gpu_download(seren_gpu_ctx* ctx, double* parray, double* v, double* rho,
                        double* omega, double* a, double* gpot, int32_t* perm_total);
 

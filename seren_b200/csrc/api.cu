@@ -753,9 +753,22 @@ int force_step_body(Ctx& c, int first_call, const IoPlan* io) {
   c.sink_a_valid = false;                    // a new tree: the sinks' accelerations are stale
   cudaMemsetAsync(c.d_counts, 0, sizeof(int) * 32, c.st);
   cudaEventRecord(c.ev[0], c.st);
-  int rc = build_tree(c);
-  if (rc) return rc;
-  launch_stock(c);
+  // main/tree_update.F90:26-88: a build every nbuildstep evaluations (and
+  // whenever there is no tree, on a first call, or from host buffers), a
+  // restock of the same cells in between
+  int rc = SEREN_GPU_OK;
+  if (io || first_call || !c.have_tree || c.since_build >= c.nbuildstep) {
+    rc = build_tree(c);
+    if (rc) return rc;
+    launch_stock(c);
+    c.since_build = 0;
+  } else {
+    bool rebuilt = false;
+    rc = restock(c, rebuilt);
+    if (rc) return rc;
+    if (rebuilt) c.since_build = 0;
+  }
+  ++c.since_build;
   cudaEventRecord(c.ev[1], c.st);
   if (io) {
     // v and c_s^2 come in on the copy stream while the grad-h walk runs (the
@@ -1229,6 +1242,15 @@ int seren_gpu_sink_search(seren_gpu_ctx* h, const seren_gpu_sink_search_params* 
     c.have_tree = false;                     // create_sink.F90:250-251: nbuild = nstock = nsteps
   }
   if (ptot_out) *ptot_out = c.ptot;
+  return SEREN_GPU_OK;
+}
+
+int seren_gpu_set_build_step(seren_gpu_ctx* h, int32_t nbuildstep) {
+  if (!h) return SEREN_GPU_ERR_ARG;
+  Ctx& c = h->c;
+  if (nbuildstep < 1) return fail(c, SEREN_GPU_ERR_ARG, "set_build_step: nbuildstep >= 1");
+  c.nbuildstep = nbuildstep;
+  c.since_build = nbuildstep;                // the next evaluation builds
   return SEREN_GPU_OK;
 }
 

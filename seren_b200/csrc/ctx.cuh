@@ -157,6 +157,11 @@ struct Ctx {
   double* acc_out = nullptr;
   int* acc_ws = nullptr;
 
+  // build schedule of the device-resident force steps (main/tree_update.F90:
+  // build every nbuildstep evaluations, restock in between)
+  int nbuildstep = 1;
+  int since_build = 0;
+
   bool have_tree = false;
   bool have_sph = false;
   bool have_v = false;
@@ -182,6 +187,10 @@ struct Ctx {
 // tree.cu
 int build_tree(Ctx& c);               // bbox, keys, sort, cells, leaf order, reorder
 void finish_reorder(Ctx& c);          // the deferred v, c_s^2 reorder (reorder_wait set)
+// the stock of the last build's cells at the current positions (no build, no
+// reorder), as tree_update does between builds; rebuilt = true when the
+// particles left the range the node records allow and the tree was built
+int restock(Ctx& c, bool& rebuilt);
 // copy `bytes` (a multiple of 4, at most 1 KiB) of device memory to the host
 // through the mapped words, after the work queued on c.st; 0 or an error code
 int read_dev(Ctx& c, const void* dsrc, void* hdst, size_t bytes);

@@ -817,6 +817,42 @@ int build_tree(Ctx& c) {
   return SEREN_GPU_OK;
 }
 
+// the largest per-axis distance of a particle from the root cell centre, as
+// the bit pattern of a non-negative double (ordered as an integer)
+__global__ void k_max_offset(const double4* __restrict__ pm, int n, double rx, double ry,
+                             double rz, unsigned long long* out) {
+  double m = 0.0;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const double4 p = pm[i];
+    m = fmax(m, fmax(fabs(p.x - rx), fmax(fabs(p.y - ry), fabs(p.z - rz))));
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+int restock(Ctx& c, bool& rebuilt) {
+  rebuilt = false;
+  // the FP32 node records bound the rounding of a coordinate relative to the
+  // root centre by 2^-22 cellsize, which holds while every particle is within
+  // two root half widths of the centre; past that (or on non-finite
+  // positions) the tree is built again instead
+  unsigned long long* out = reinterpret_cast<unsigned long long*>(c.bbox_part);
+  cudaMemsetAsync(out, 0, sizeof(unsigned long long), c.st);
+  k_max_offset<<<std::min(nb(c.ptot, 256), 1184), 256, 0, c.st>>>(
+      c.pm, c.ptot, c.info.root[0], c.info.root[1], c.info.root[2], out); ++c.nlaunch;
+  unsigned long long bits = 0;
+  if (read_dev(c, out, &bits, sizeof(bits))) return SEREN_GPU_ERR_CUDA;
+  double maxoff = 0.0;
+  std::memcpy(&maxoff, &bits, sizeof(double));
+  if (!(maxoff <= 2.0 * c.info.cellsize)) {
+    rebuilt = true;
+    const int rc = build_tree(c);
+    if (rc) return rc;
+  }
+  launch_stock(c);
+  return SEREN_GPU_OK;
+}
+
 void launch_stock(Ctx& c) {
   const double daux = 10.0 * pow(1.7976931348623157e308, -0.2);
   // bound on the rounding of a coordinate relative to the root centre when

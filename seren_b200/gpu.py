@@ -43,6 +43,7 @@ def library(build_if_missing: bool = True) -> C.CDLL:
                            ("sink_timestep", [vp, C.c_double, _dp]),
                            ("accrete", [vp, C.c_int32, _ip, C.c_int32, _dp, _ip, _ip]),
                            ("sink_search", [vp, C.c_void_p, _ip, _ip, _dp, _ip, _ip]),
+                           ("set_build_step", [vp, C.c_int32]),
                            ("set_sinks", [vp, C.c_int32, _dp]),
                            ("download", [vp, _dp, _dp, _dp, _dp, _dp, _dp, _ip]),
                            ("last_step_stats", [vp, _dp, _ip, C.POINTER(C.c_int64)]),
@@ -168,6 +169,11 @@ class GpuHotPath(HotPath):
             self.nsink += 1
         return dict(created=bool(created.value), psink_id=pid.value, angmom=angmom,
                     nremoved=nrem.value)
+
+    def set_build_step(self, nbuildstep: int):
+        """Build the tree every nbuildstep device-resident evaluations and
+        restock it in between (seren_gpu_set_build_step)."""
+        self._call("set_build_step", self._ctx, int(nbuildstep))
 
     def drift(self, dt: float):
         self._call("drift", self._ctx, C.c_double(dt))

@@ -40,7 +40,7 @@ def test_oracle_mirrors_the_abi():
         if tail in ("upload", "force_step", "force_step_io", "drift", "download",
                     "last_step_stats", "get_stream", "fma_peak", "hydro_forces_noalloc",
                     "set_sinks", "timestep", "rk2_step", "set_sink_motion", "get_sinks",
-                    "sink_timestep", "accrete", "sink_search"):
+                    "sink_timestep", "accrete", "sink_search", "set_build_step"):
             continue          # device-resident path (timestep / rk2 / accretion: Python
                               # restatements in oracle.py), device-buffer call, GPU-only
                               # introspection

@@ -619,3 +619,51 @@ def test_sink_search_matches_oracle(libs):
         assert g.ptot == p3.shape[0] and np.array_equal(g.download()["perm"], st3["perm"])
     g.force_step(first_call=False)
     assert np.isfinite(g.download()["a"]).all()
+
+
+def _restock_pipeline(o, parray, v, sound):
+    """The oracle's evaluation on the tree it holds, restocked at new
+    positions (tree_update without a build: main/tree_update.F90 between
+    builds), particles in their current order."""
+    p, _ = o.tree_update(parray, do_build=False)
+    s = o.sph_update(p, v, first_call=False)
+    press = sound * sound * s["rho"]
+    a, gpot = o.grav_forces(o.hydro_forces(press, sound))
+    return dict(parray=s["parray"], a=a, gpot=gpot, rho=s["rho"])
+
+
+def test_rk2_step_restocks_between_builds(libs):
+    """With nbuildstep = 8 (the reference's default) the two evaluations of a
+    Runge-Kutta step after the first build restock the same cells at the new
+    positions instead of building: the particle order stays, and positions,
+    velocities, rho and accelerations match the oracle driven through the same
+    restocks."""
+    from oracle.oracle import rk2_full, rk2_half
+    ic = case("sphere4k")
+    o, g = _pair(libs, ic)
+    g.upload(ic["parray"], ic["v"], ic["sound"] ** 2)
+    g.set_build_step(8)
+    g.force_step(first_call=True)
+    r0 = run_pipeline(o, ic)
+    dt = g.timestep()
+    g.rk2_step(dt)
+    st = g.download()
+    assert np.array_equal(st["perm"], r0["perm"])            # no build: same order
+    p0, v0, snd = r0["sph"]["parray"], r0["v"], r0["sound"]
+    rh, vh = rk2_half(p0[:, 0:3], v0, r0["a"], 0.5 * dt)
+    ph = p0.copy()
+    ph[:, 0:3] = rh
+    r1 = _restock_pipeline(o, ph, vh, snd)
+    x1, v1 = rk2_full(p0[:, 0:3], v0, vh, r1["a"], dt)
+    p1 = r1["parray"].copy()
+    p1[:, 0:3] = x1
+    r2 = _restock_pipeline(o, p1, v1, snd)
+    assert np.abs(st["parray"][:, 0:3] - x1).max() < 1e-13
+    assert rel_rows(st["v"], v1).max() < 1e-10
+    assert np.abs(st["parray"][:, 4] / r2["parray"][:, 4] - 1).max() < TOL
+    assert np.abs(st["rho"] / r2["rho"] - 1).max() < TOL
+    assert rel_rows(st["a"], r2["a"]).max() < 1e-9
+    # a build every evaluation again: the next step reorders
+    g.set_build_step(1)
+    g.rk2_step(g.timestep())
+    assert np.isfinite(g.download()["a"]).all()
