@@ -235,10 +235,12 @@ def run_resident(ic, precision, steps, warmup, ws):
     return res, state
 
 
-def run_rk2(ic, precision, steps, warmup, ws):
+def run_rk2(ic, precision, steps, warmup, ws, nbuildstep=1):
     """Device-resident integration: seren_gpu_timestep then seren_gpu_rk2_step
     (two force evaluations) per step, from the state after one force step;
-    timed with CUDA events on the library's stream, max over ranks."""
+    with nbuildstep > 1 the tree is built every nbuildstep evaluations and
+    restocked in between (the reference's schedule); timed with CUDA events
+    on the library's stream, max over ranks."""
     import torch
 
     from seren_b200.gpu import GpuHotPath
@@ -246,6 +248,7 @@ def run_rk2(ic, precision, steps, warmup, ws):
     g = GpuHotPath(n, params_for(ic, precision))
     g.upload(ic["parray"], ic["v"], ic["sound"] ** 2)
     stream = torch.cuda.ExternalStream(g.stream())
+    g.set_build_step(nbuildstep)
     g.force_step(first_call=True)
     dts = []
     for _ in range(max(warmup, 1)):
@@ -265,7 +268,7 @@ def run_rk2(ic, precision, steps, warmup, ws):
     g.close()
     return dict(ms_per_step=total_ms / steps, force_evals_per_step=2,
                 value=ws * 2 * n * steps / (total_ms * 1e-3), unit=UNIT,
-                dt=[float(x) for x in dts],
+                dt=[float(x) for x in dts], nbuildstep=nbuildstep,
                 api="seren_gpu_timestep + seren_gpu_rk2_step (courant 0.2, accel 0.5)")
 
 
@@ -606,10 +609,12 @@ def main():
         acc = dict(rms_vs_fp64=float(np.sqrt(np.mean(err ** 2))), max_vs_fp64=float(err.max()),
                    same_order=bool(same))
         log(f"[bench] fp64: {fp64['ms_per_step']:.2f} ms/step, stages {fp64['stage_ms']}, {acc}")
-    rk2 = None
+    rk2 = rk2_8 = None
     if args.workload == "core":
         rk2 = run_rk2(ic, 1, args.steps, args.warmup, ws)
         log(f"[bench] rk2 step: {rk2['ms_per_step']:.2f} ms (two force evaluations), dt {rk2['dt']}")
+        rk2_8 = run_rk2(ic, 1, args.steps, args.warmup, ws, nbuildstep=8)
+        log(f"[bench] rk2 step, build every 8 evaluations: {rk2_8['ms_per_step']:.2f} ms")
     e2e = e2e_calls = None
     if not args.no_e2e:
         r = run_e2e_io(ic, 1, args.steps, args.warmup, ws)
@@ -680,6 +685,7 @@ def main():
         "e2e": e2e,
         "e2e_reference_calls": e2e_calls,
         "rk2_step": rk2,
+        "rk2_step_nbuildstep8": rk2_8,
         "gpu_launches": mixed["launches"],
         "clocks": clocks,
     }
