@@ -667,3 +667,45 @@ def test_rk2_step_restocks_between_builds(libs):
     g.set_build_step(1)
     g.rk2_step(g.timestep())
     assert np.isfinite(g.download()["a"]).all()
+
+
+def test_accretion_full_size_properties(libs):
+    """Accretion at the full 4,194,304-particle core, mixed precision (too large
+    for the Python oracle): size-independent properties of the result.  Mass and
+    momentum are conserved; every removed particle lies inside the radius of an
+    accreting sink and the per-sink counts follow the nearest-sink rule; no
+    particle outside every radius is removed; the kept particles keep their
+    order; a force step runs on them."""
+    from seren_b200 import ics
+    ic = ics.turbulent_core(n=1 << 22, seed=4, sound=0.2, mach=2.0, h_fac=1.2,
+                            thetamaxsqd=0.25)
+    g = libs[1](ic["parray"].shape[0], params(ic, precision=1))
+    g.upload(ic["parray"], ic["v"], ic["sound"] ** 2)
+    rng = np.random.default_rng(3)
+    pick = rng.choice(ic["parray"].shape[0], 8, replace=False)
+    sinks = np.c_[ic["parray"][pick, 0:3], np.full(8, 1e-3), np.full(8, 0.01)]
+    sv, srad = np.zeros((8, 3)), np.full(8, 0.03)
+    g.set_sinks(sinks)
+    g.set_sink_motion(sv, srad)
+    g.force_step(first_call=True)
+    st, s0 = g.download(), g.get_sinks()
+    p, v = st["parray"], st["v"]
+    cnt = g.accrete(energy_accrete=True)
+    s1, st1 = g.get_sinks(), g.download()
+    keep_ids = st1["perm"]
+    kept = np.isin(st["perm"], keep_ids)
+    assert np.array_equal(st["perm"][kept], keep_ids)           # order kept
+    assert cnt.sum() == (~kept).sum() > 0
+    m0 = p[:, 3].sum() + s0["rmh"][:, 3].sum()
+    m1 = st1["parray"][:, 3].sum() + s1["rmh"][:, 3].sum()
+    assert abs(m1 / m0 - 1) < 1e-12
+    P0 = (p[:, 3:4] * v).sum(0) + (s0["rmh"][:, 3:4] * s0["v"]).sum(0)
+    P1 = (st1["parray"][:, 3:4] * st1["v"]).sum(0) + (s1["rmh"][:, 3:4] * s1["v"]).sum(0)
+    assert np.abs(P1 - P0).max() < 1e-12 * (np.abs(p[:, 3:4] * v).sum() + 1e-300)
+    d2 = np.stack([((p[:, 0:3] - s0["rmh"][k, 0:3]) ** 2).sum(1) for k in range(8)], axis=1)
+    inside = d2 < srad[None, :] ** 2
+    near = np.where(inside, d2, np.inf).argmin(1)
+    assert inside[~kept].any(1).all() and not (~kept & ~inside.any(1)).any()
+    assert np.array_equal(cnt, np.bincount(near[~kept], minlength=8))
+    g.force_step(first_call=False)
+    assert np.isfinite(g.download()["a"]).all()
