@@ -319,10 +319,28 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
     const float px32 = (float)(P.x - t.rootx), py32 = (float)(P.y - t.rooty),
                 pz32 = (float)(P.z - t.rootz);
     const float ux = (float)(P.x - rx), uy = (float)(P.y - ry), uz = (float)(P.z - rz);
-    // the group's bounding sphere in the walk's FP32 coordinates: centre lane
-    // 0, radius the farthest live lane's distance, rounded up
-    const float gx = __shfl_sync(FULLMASK, px32, 0), gy = __shfl_sync(FULLMASK, py32, 0),
-                gz = __shfl_sync(FULLMASK, pz32, 0);
+    // the group's bounding sphere in the walk's FP32 coordinates: centre the
+    // middle of the live lanes' bounding box, radius the farthest live lane's
+    // distance from it, rounded up
+    float gx, gy, gz;
+    {
+      const float x0 = __shfl_sync(FULLMASK, px32, 0), y0 = __shfl_sync(FULLMASK, py32, 0),
+                  z0 = __shfl_sync(FULLMASK, pz32, 0);
+      float lox = live ? px32 : x0, loy = live ? py32 : y0, loz = live ? pz32 : z0;
+      float hix = lox, hiy = loy, hiz = loz;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        lox = fminf(lox, __shfl_xor_sync(FULLMASK, lox, o));
+        loy = fminf(loy, __shfl_xor_sync(FULLMASK, loy, o));
+        loz = fminf(loz, __shfl_xor_sync(FULLMASK, loz, o));
+        hix = fmaxf(hix, __shfl_xor_sync(FULLMASK, hix, o));
+        hiy = fmaxf(hiy, __shfl_xor_sync(FULLMASK, hiy, o));
+        hiz = fmaxf(hiz, __shfl_xor_sync(FULLMASK, hiz, o));
+      }
+      gx = 0.5f * (lox + hix);
+      gy = 0.5f * (loy + hiy);
+      gz = 0.5f * (loz + hiz);
+    }
     float grad;
     {
       const float e0 = px32 - gx, e1 = py32 - gy, e2 = pz32 - gz;
