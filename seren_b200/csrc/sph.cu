@@ -222,7 +222,8 @@ struct GrShared {
 };
 
 // A group's bounding sphere in the walks' FP32 root-relative coordinates:
-// centre lane 0, radius the farthest live lane's distance (rounded up), and
+// centre the middle of the live lanes' bounding box, radius the farthest live
+// lane's distance from it (rounded up), and
 // the least and largest search radius over its live lanes.
 struct GrGroup {
   float x, y, z, r, rmin, rmax;
@@ -230,9 +231,25 @@ struct GrGroup {
 
 __device__ __forceinline__ GrGroup gr_group(float px, float py, float pz, float R, bool live) {
   GrGroup g;
-  g.x = __shfl_sync(0xffffffffu, px, 0);
-  g.y = __shfl_sync(0xffffffffu, py, 0);
-  g.z = __shfl_sync(0xffffffffu, pz, 0);
+  {
+    // centre: the middle of the live lanes' bounding box (lane 0 is live)
+    const float x0 = __shfl_sync(0xffffffffu, px, 0), y0 = __shfl_sync(0xffffffffu, py, 0),
+                z0 = __shfl_sync(0xffffffffu, pz, 0);
+    float lox = live ? px : x0, loy = live ? py : y0, loz = live ? pz : z0;
+    float hix = lox, hiy = loy, hiz = loz;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      lox = fminf(lox, __shfl_xor_sync(0xffffffffu, lox, o));
+      loy = fminf(loy, __shfl_xor_sync(0xffffffffu, loy, o));
+      loz = fminf(loz, __shfl_xor_sync(0xffffffffu, loz, o));
+      hix = fmaxf(hix, __shfl_xor_sync(0xffffffffu, hix, o));
+      hiy = fmaxf(hiy, __shfl_xor_sync(0xffffffffu, hiy, o));
+      hiz = fmaxf(hiz, __shfl_xor_sync(0xffffffffu, hiz, o));
+    }
+    g.x = 0.5f * (lox + hix);
+    g.y = 0.5f * (loy + hiy);
+    g.z = 0.5f * (loz + hiz);
+  }
   const float e0 = px - g.x, e1 = py - g.y, e2 = pz - g.z;
   float r2 = live ? fmaf(e2, e2, fmaf(e1, e1, e0 * e0)) : 0.0f;
   float lo = live ? R : 3.0e38f, hi = live ? R : 0.0f;
