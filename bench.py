@@ -65,8 +65,6 @@ def parse():
                          "sphere, gravity accuracy over theta^2 in {0.09, 0.25, 0.49}; disc: "
                          "protostellar disc around a sink; batched: 256 independent clouds "
                          "shared out across the ranks")
-    ap.add_argument("--cpu-sample", type=int, default=0,
-                    help="active particles in the CPU sample (default N, or N/8 above 2^20)")
     return ap.parse_args()
 
 
@@ -188,6 +186,12 @@ def workload_info(kind, n):
             f"turbulent molecular-cloud core, N={n} per GPU, uniform sphere R=1 M=1 G=1, "
             "isothermal c_s=0.2, P(k)~k^-4 Mach 2, h_fac=1.2 (pp_gather 57), theta^2=0.25 "
             "quadrupole geometric MAC, MON97 alpha=1; step = full force evaluation + drift")
+
+
+def line_config(wdesc, n):
+    """The `config` object of the JSON line, the same in both arms."""
+    return {"workload": wdesc, "particles": n,
+            "l2": "inputs larger than L2 (particles + tree ~1 GB resident)"}
 
 
 def params_for(ic, precision):
@@ -436,11 +440,15 @@ def traffic_per_launch(n):
 
 
 # ---------------------------------------------------------------------------
-def cpu_eval(ic_tree, sample, first_call=False):
-    """One force evaluation of the CPU oracle (the C++ FP64 restatement of the
-    reference) on all host cores.  The tree is built for all particles; grad-h,
-    neighbour lists, hydro and gravity run for `sample` random active particles
-    (all when sample >= N) and are scaled by N/sample."""
+def cpu_eval(ic_tree, first_call=False):
+    """One full force evaluation of the CPU oracle (the C++ FP64 restatement of
+    the reference) for every particle on all host cores, as the reference's
+    sph_setup.F90:42-66 sequence runs it: tree build + reorder + stock, grad-h
+    h/rho/Omega solve, hmax update, neighbour lists, isothermal thermal, hydro
+    forces, gravity.  No sampling and no scaling.  Returns the wall seconds of
+    the evaluation, the per-stage seconds (the reference's BH_TREE,
+    ALL_SPH_GRADH, BHHYDRO_UPDATE, GET_NEIB, THERMAL, HYDRO_FORCES and
+    GRAVITY_FORCES markers) and the state in the oracle's tree order."""
     from oracle.oracle import Oracle, set_threads
     cores = set_threads(os.cpu_count() or 1)
     parray = ic_tree["parray"]
@@ -451,20 +459,34 @@ def cpu_eval(ic_tree, sample, first_call=False):
     t1 = time.perf_counter()
     v = ic_tree["v"][perm]
     sound = ic_tree["sound"][perm]
-    if sample >= n:
-        act = None
-    else:
-        rng = np.random.Generator(np.random.PCG64(12345))
-        act = np.sort(rng.choice(n, size=sample, replace=False)).astype(np.int32)
-    out = o.sph_update(po, v, first_call=first_call, acclist=act, lists=False)
-    press = sound * sound * out["rho"]
-    a = o.hydro_forces(press, sound, acclist=act)
-    a, gpot = o.grav_forces(a, acclist=act)
     t2 = time.perf_counter()
-    frac = 1.0 if act is None else n / float(sample)
-    sec = (t1 - t0) + (t2 - t1) * frac
+    out = o.sph_update(po, v, first_call=first_call, lists=False)
+    t3 = time.perf_counter()
+    press = sound * sound * out["rho"]
+    t4 = time.perf_counter()
+    a = o.hydro_forces(press, sound)
+    t5 = time.perf_counter()
+    a, gpot = o.grav_forces(a)
+    t6 = time.perf_counter()
+    st = o.stage_seconds()          # tree, grad-h, hmax, neib, hydro, gravity (oracle clocks)
+    stages = {"BH_TREE": t1 - t0, "ALL_SPH_GRADH": st[1], "BHHYDRO_UPDATE": st[2],
+              "GET_NEIB": st[3], "SPH_UPDATE_OTHER": max(0.0, (t3 - t2) - sum(st[1:4])),
+              "THERMAL": t4 - t3, "HYDRO_FORCES": t5 - t4, "GRAVITY_FORCES": t6 - t5}
+    sec = (t1 - t0) + (t3 - t2) + (t6 - t3)   # the host-side gathers of v and c_s are excluded
     return dict(sec=sec, cores=cores, oracle=o, parray=out["parray"], perm=perm, a=a, gpot=gpot,
-                act=act)
+                rho=out["rho"], stages={k: round(x, 3) for k, x in stages.items()})
+
+
+def cpu_host():
+    """CPU model of this host (for the CPU-baseline lines)."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 def gravity_accuracy(ic, parray, nsub=256):
@@ -606,8 +628,10 @@ def main():
         # the particle order and h agree; compare accelerations row by row
         same = np.array_equal(state_m["perm"], state_d["perm"])
         err = np.linalg.norm(am - ad, axis=1) / np.maximum(np.linalg.norm(ad, axis=1), 1e-300)
+        drho = np.abs(state_m["rho"] - state_d["rho"]) / state_d["rho"]
         acc = dict(rms_vs_fp64=float(np.sqrt(np.mean(err ** 2))), max_vs_fp64=float(err.max()),
-                   same_order=bool(same))
+                   rho_rms_vs_fp64=float(np.sqrt(np.mean(drho ** 2))),
+                   rho_max_vs_fp64=float(drho.max()), same_order=bool(same))
         log(f"[bench] fp64: {fp64['ms_per_step']:.2f} ms/step, stages {fp64['stage_ms']}, {acc}")
     rk2 = rk2_8 = None
     if args.workload == "core":
@@ -629,17 +653,20 @@ def main():
                          api="tree_update, sph_update, hydro_forces, grav_forces")
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        sample = args.cpu_sample or (n if n <= (1 << 20) else n // 8)
         st = dict(state_m)
-        ic_cpu = dict(parray=st["parray"], v=st["v"], sound=np.sqrt(0.04) * np.ones(n),
+        assert np.all(ic["sound"] == ic["sound"][0]), "the core is isothermal at one c_s"
+        ic_cpu = dict(parray=st["parray"], v=st["v"], sound=np.full(n, float(ic["sound"][0])),
                       h_fac=ic["h_fac"], thetamaxsqd=ic["thetamaxsqd"], alpha=ic["alpha"])
-        r = cpu_eval(ic_cpu, sample)
+        r = cpu_eval(ic_cpu)
+        log(f"[bench] CPU baseline: {r['sec']:.2f} s per evaluation on {r['cores']} threads, "
+            f"stages {r['stages']}")
         cpu = dict(value=n / r["sec"], unit=UNIT, cores=r["cores"], kind="port",
-                   sample=(f"one force evaluation of the C++ FP64 restatement of the reference "
-                           f"(oracle/) on the state after the GPU run: tree build+stock of all "
-                           f"{n} particles, grad-h/neighbour lists/hydro/gravity for {sample} "
-                           f"random active particles, scaled by N/{sample}; "
-                           f"{r['sec']:.2f} s per evaluation"))
+                   cpu=cpu_host(), seconds_per_evaluation=round(r["sec"], 3),
+                   stage_seconds=r["stages"],
+                   sample=(f"one full force evaluation of all {n} particles (no sampling) by the "
+                           f"C++ FP64 restatement of the reference (oracle/) on the converged "
+                           f"state after the GPU run: tree build+reorder+stock, grad-h, hmax, "
+                           f"neighbour lists, thermal, hydro, gravity; {r['sec']:.2f} s"))
         r["oracle"].close()
     if rank == 0 and ws == 1:
         acc.update(gravity_accuracy(ic, state_m["parray"],
@@ -663,10 +690,9 @@ def main():
         "warmup": args.warmup, "ms_per_step": t_mixed / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "fp32+fp64",
         "data": data,
-        "config": {"workload": wdesc,
-                   "particles": n, "precision": "mixed (FP32 pair arithmetic, FP64 walk/MAC/"
-                   "grad-h)", "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
-                   "l2": "inputs larger than L2 (particles + tree ~1 GB resident)"},
+        "config": line_config(wdesc, n),
+        "precision": "mixed (FP32 pair arithmetic, FP64 walk/MAC/grad-h)",
+        "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
         "stage_ms": {k: round(x, 3) for k, x in zip(
             ("tree", "gradh", "neib", "hydro", "gravity", "total"), mixed["stage_ms"][:6])},
         "fp64": fp64,
@@ -696,8 +722,13 @@ def main():
 
 
 def reference_arm(args, ws, rank, n):
-    """The reference's CPU path (its C++ FP64 restatement in oracle/, since the
-    Fortran reference cannot be compiled here) on the host cores, rank 0 only."""
+    """The reference's CPU path on the host cores, rank 0 only: its C++ FP64
+    restatement in oracle/ (the Fortran reference cannot be compiled here: no
+    Fortran compiler), on all host threads.  Every step is one full force
+    evaluation of all N particles (no sampling), from the state the previous
+    step left: the first warm-up step starts from the h guess (first call),
+    later ones carry every particle's converged h and drift r += v dt, as the
+    repository's arm does on the GPU."""
     if rank != 0:
         if ws > 1:
             import torch.distributed as dist
@@ -705,15 +736,16 @@ def reference_arm(args, ws, rank, n):
         return
     ic = workload(n, args.workload)
     metric, data, wdesc = workload_info(args.workload, n)
-    sample = args.cpu_sample or (n if n <= (1 << 20) else n // 32)
     state = dict(parray=ic["parray"].copy(), v=ic["v"], sound=ic["sound"], h_fac=ic["h_fac"],
                  thetamaxsqd=ic["thetamaxsqd"], alpha=ic["alpha"])
     total = 0.0
     cores = 1
+    stages = {}
     for k in range(args.warmup + args.steps):
-        r = cpu_eval(state, sample, first_call=(k == 0))
+        r = cpu_eval(state, first_call=(k == 0))
         cores = r["cores"]
-        # carry h and zeta forward in the oracle's tree order, then drift
+        log(f"[bench] reference step {k}: {r['sec']:.2f} s, stages {r['stages']}")
+        # carry h and zeta of every particle forward in the oracle's tree order, then drift
         state["parray"] = r["parray"]
         state["v"] = state["v"][r["perm"]]
         state["sound"] = state["sound"][r["perm"]]
@@ -721,18 +753,22 @@ def reference_arm(args, ws, rank, n):
         r["oracle"].close()
         if k >= args.warmup:
             total += r["sec"]
+            for key, x in r["stages"].items():
+                stages[key] = stages.get(key, 0.0) + x / args.steps
     value = n * args.steps / total
     line = {
         "metric": metric, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp64",
-        "data": data, "config": {"workload": wdesc, "particles": n},
+        "data": data, "config": line_config(wdesc, n),
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "cpu": cpu_host(),
+                         "stage_seconds": {key: round(x, 3) for key, x in stages.items()},
                          "sample": (f"C++ FP64 restatement of the reference (oracle/; the Fortran "
-                                    f"reference has no compiler here): tree of all {n} particles, "
-                                    f"per-particle stages for {sample} random active particles "
-                                    f"scaled by N/{sample}, per step")},
+                                    f"reference has no compiler here) on {cores} threads: every "
+                                    f"step one full force evaluation of all {n} particles, no "
+                                    f"sampling, from the previous step's converged h")},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)

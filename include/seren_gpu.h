@@ -123,7 +123,10 @@ int seren_gpu_sink_forces(seren_gpu_ctx* ctx, int32_t nsink, const double* sink_
  * neighbour lists, isothermal thermal (sph/thermal.F90:52-59), hydro and
  * gravity without touching the host; seren_gpu_drift() moves r += v*dt;
  * seren_gpu_download() copies results back in tree order (any pointer may be
- * NULL). */
+ * NULL).  The uploaded particles are all gas particles (the reference's
+ * pgasstart..pgasend range): the device-resident calls that loop over
+ * particles (accretion, sink search) take every uploaded particle as gas, so
+ * a caller with boundary or intercloud particles uploads only its gas range. */
 int seren_gpu_upload(seren_gpu_ctx* ctx, int32_t ptot, const double* parray,
                      const double* v, const double* csq);
 int seren_gpu_force_step(seren_gpu_ctx* ctx, int32_t first_call);
@@ -307,7 +310,10 @@ int seren_gpu_fma_peak(seren_gpu_ctx* ctx, int32_t precision, double* tflops);
  * parray[n][6], v[n][3], rho/omega/press/sound[n], pptot[n],
  * pplist[n][pp_limit] with 0-based ids, output a[n][3] (overwritten).
  * kernel and precision mean what they mean in seren_gpu_params.  stream is a
- * cudaStream_t (NULL for the default stream); the call synchronises it.
+ * cudaStream_t (NULL for the default stream); the call is synchronous: it
+ * waits for that stream before it returns, twice (after the list check and
+ * at the end).  An error that the caller's own earlier work left pending is
+ * neither reported by this call nor cleared.
  *
  * Limits: n <= SEREN_GPU_NOALLOC_PMAX (SEREN_GPU_ERR_CAPACITY beyond); every
  * row must hold its whole neighbour list, 0 <= pptot <= pp_limit
@@ -319,7 +325,9 @@ int seren_gpu_fma_peak(seren_gpu_ctx* ctx, int32_t precision, double* tflops);
  * the particles, per-particle factors, kernel tables and an error block),
  * held by every GPU that loads the library until the process exits.  The
  * first call on a device looks up the array's address and uploads the kernel
- * tables; make that first call before any stream capture.  Every call on a
+ * tables; make that first call before any stream capture.  That set-up is
+ * kept per device ordinal for the life of the process, so the library must not
+ * outlive a cudaDeviceReset of a device it has run on.  Every call on a
  * device shares the array and leaves its contents behind, so calls that
  * overlap on the GPU (other streams, other host threads) race: serialise
  * them. */

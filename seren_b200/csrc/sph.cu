@@ -11,6 +11,7 @@
 // gives one thread to one particle and follows hydro_gradh step by step.
 #include <algorithm>
 #include <mutex>
+#include <tuple>
 #include <type_traits>
 #include <vector>
 
@@ -1865,13 +1866,28 @@ int noalloc_setup(int dev, double** base) {
   return SEREN_GPU_OK;
 }
 
+// Reads the error block after the stream has drained.  Only this call's own
+// return codes are looked at: an error the caller's earlier work left pending
+// stays pending (no cudaGetLastError here), and is not reported as ours.
 int noalloc_status(cudaStream_t st, const DevError* d_err) {
   DevError e{};
   const cudaError_t rc1 = cudaMemcpyAsync(&e, d_err, sizeof(DevError), cudaMemcpyDeviceToHost, st);
   const cudaError_t rc2 = cudaStreamSynchronize(st);
-  if (rc1 != cudaSuccess || rc2 != cudaSuccess || cudaGetLastError() != cudaSuccess)
-    return SEREN_GPU_ERR_CUDA;
+  if (rc1 != cudaSuccess || rc2 != cudaSuccess) return SEREN_GPU_ERR_CUDA;
   return e.code;
+}
+
+// Launches through cudaLaunchKernel, whose return code is this launch's own.
+template <typename... P, typename... A>
+cudaError_t noalloc_launch(void (*kern)(P...), unsigned grid, unsigned block, cudaStream_t st,
+                           A... a) {
+  auto args = std::make_tuple(static_cast<P>(a)...);
+  void* ptrs[sizeof...(P)];
+  std::apply([&](auto&... x) {
+    int k = 0;
+    ((ptrs[k++] = (void*)&x), ...);
+  }, args);
+  return cudaLaunchKernel((const void*)kern, dim3(grid), dim3(block), ptrs, 0, st);
 }
 
 }  // namespace
@@ -1906,18 +1922,24 @@ extern "C" int seren_gpu_hydro_forces_noalloc(int32_t n, const double* parray, c
   const double4* tab = reinterpret_cast<const double4*>(base + NA_TAB + kernel * NA_TABLEN);
   // the array keeps the previous call's contents: only the error block must start at zero
   if (cudaMemsetAsync(d_err, 0, sizeof(DevError), st) != cudaSuccess) return SEREN_GPU_ERR_CUDA;
-  k_noalloc_pack<<<nb(n, 256), 256, 0, st>>>(n, parray, v, pptot, pplist, pp_limit, pm, hz, vel,
-                                              d_err);
+  if (noalloc_launch(k_noalloc_pack, nb(n, 256), 256, st, n, parray, v, pptot, pplist, pp_limit,
+                     pm, hz, vel, d_err) != cudaSuccess)
+    return SEREN_GPU_ERR_CUDA;
   if ((rc = noalloc_status(st, d_err))) return rc;
-  k_hydro_prep<<<nb(n, 256), 256, 0, st>>>(n, hz, rho, omega, press, pf, hf4);
+  if (noalloc_launch(k_hydro_prep, nb(n, 256), 256, st, n, hz, rho, omega, press, pf, hf4) !=
+      cudaSuccess)
+    return SEREN_GPU_ERR_CUDA;
   const HydroTree none{};   // every row fits its list, so the kernel never walks a tree
-  if (precision == 0)
-    k_hydro<false, 1><<<nb(n, 128), 128, 0, st>>>(n, nullptr, pm, hz, vel, rho, pf, hf4, sound,
-                                                 pptot, pplist, pp_limit, none, tab, alpha,
-                                                 kernel == 1, a, nullptr, d_err);
-  else
-    k_hydro<true, HY_SUB><<<nb((long)n * HY_SUB, 128), 128, 0, st>>>(n, nullptr, pm, hz, vel, rho, pf, hf4, sound,
-                                                pptot, pplist, pp_limit, none, tab, alpha,
-                                                kernel == 1, a, nullptr, d_err);
+  const int* no_act = nullptr;
+  double* no_map = nullptr;
+  const cudaError_t lrc =
+      precision == 0
+          ? noalloc_launch(k_hydro<false, 1>, nb(n, 128), 128, st, n, no_act, pm, hz, vel, rho,
+                           pf, hf4, sound, pptot, pplist, pp_limit, none, tab, alpha,
+                           kernel == 1, a, no_map, d_err)
+          : noalloc_launch(k_hydro<true, HY_SUB>, nb((long)n * HY_SUB, 128), 128, st, n, no_act,
+                           pm, hz, vel, rho, pf, hf4, sound, pptot, pplist, pp_limit, none, tab,
+                           alpha, kernel == 1, a, no_map, d_err);
+  if (lrc != cudaSuccess) return SEREN_GPU_ERR_CUDA;
   return noalloc_status(st, d_err);
 }

@@ -55,7 +55,7 @@ def _context_state(name, precision):
         g.close()
 
 
-def _noalloc(st, precision):
+def _noalloc(st, precision, expect=0):
     import torch
     dev = torch.device("cuda:0")
     t = {k: torch.as_tensor(np.ascontiguousarray(st[k]), device=dev)
@@ -65,7 +65,7 @@ def _noalloc(st, precision):
     rc = _fn()(st["n"], *(t[k].data_ptr() for k in ("parray", "v", "rho", "omega", "press",
                                                     "sound", "pptot", "pplist")),
                st["L"], st["kernel"], precision, st["alpha"], a.data_ptr(), None)
-    assert rc == 0, rc
+    assert rc == expect, rc
     return a.cpu().numpy()
 
 
@@ -84,3 +84,21 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
     # refused on the host before anything touches the GPU
     assert _fn()(NOALLOC_PMAX + 1, *([None] * 8), 114, 0, 0, 1.0, None, None) == 2
     assert _fn()(16, *([None] * 8), 114, 0, 0, 1.0, None, None) == 1
+
+
+def test_noalloc_refuses_rows_it_cannot_evaluate_then_recovers():
+    """The list checks made on the device: a row longer than pp_limit (the
+    context entry point would walk the tree for it; there is no tree here)
+    gives SEREN_GPU_ERR_CAPACITY, a listed id outside 0..n-1 gives
+    SEREN_GPU_ERR_ARG.  The check only reads inside each row, and a refused
+    call leaves nothing behind that changes the next call's results."""
+    st = _context_state("ragged777", 0)
+    L = st["L"]
+    long_row = dict(st, pptot=st["pptot"].copy())
+    long_row["pptot"][5] = L + 1
+    _noalloc(long_row, 0, expect=2)
+    bad_id = dict(st, pplist=st["pplist"].copy())
+    bad_id["pplist"][7, 0] = st["n"]
+    _noalloc(bad_id, 0, expect=1)
+    a = _noalloc(st, 0)
+    assert rel_rows(a, st["a_ref"]).max() <= 1e-12
