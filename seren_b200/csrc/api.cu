@@ -249,7 +249,7 @@ void free_all(Ctx& c) {
                 c.orig_alt, c.rho, c.omega, c.div_v, c.drhodt, c.rho_alt, c.omega_alt, c.div_v_alt,
                 c.drhodt_alt, c.press, c.sound, c.acc, c.gpot,
                 c.pf, c.hf4,
-                c.pptot, c.pplist, c.stage, c.istage, c.keys, c.keys_alt, c.idx, c.idx_alt,
+                c.pptot, c.pplist, c.stage, c.istage, c.keys, c.keys_alt, c.keys_hi, c.keys_lo, c.idx, c.idx_alt,
                 c.rs_hist, c.bbox_part, c.branch, c.branch_next, c.nchild, c.choff, c.cstart,
                 c.bflag, c.bscan, c.leaf, c.nextcell, c.ifopen, c.pstart, c.pcount, c.parent,
                 c.level, c.nkids, c.work, c.sinks, c.wstack, c.leaves, c.nleaf, c.npot, c.redo, c.wide, c.wst, c.wacc, c.link, c.gA, c.gB, c.gC, c.wA, c.hN, c.hA, c.hrm, c.hA32, c.hrm32, c.hmax, c.bbmin, c.bbmax, c.d_info,
@@ -290,7 +290,8 @@ int alloc_all(Ctx& c) {
   // stage: host-layout arrays and up to 1024 sinks; istage: active list + id arrays
   bad |= alloc(c.pptot, P) | alloc(c.pplist, P * L) | alloc(c.stage, std::max<size_t>(6 * P, 16384)) |
          alloc(c.istage, P * L + P);
-  bad |= alloc(c.keys, P) | alloc(c.keys_alt, P) | alloc(c.idx, P) | alloc(c.idx_alt, P) |
+  bad |= alloc(c.keys, P) | alloc(c.keys_alt, P) | alloc(c.keys_hi, P) | alloc(c.keys_lo, P) |
+         alloc(c.idx, P) | alloc(c.idx_alt, P) |
          alloc(c.rs_hist, 256 * rsblk) | alloc(c.bbox_part, 6 * 1184);
   bad |= alloc(c.branch, nbr) | alloc(c.branch_next, nbr) | alloc(c.nchild, nbr) |
          alloc(c.choff, nbr) | alloc(c.cstart, 9 * nbr) | alloc(c.bflag, C) | alloc(c.bscan, C);

@@ -38,9 +38,12 @@ constexpr int LISTSIZE = 10000;
 constexpr int GLISTSIZE = 10000;
 
 // key layout: 21 octree levels of 3 bits in one 64-bit word, level-1 octant
-// in the most significant digit.  Trees deeper than this are reported as
-// SEREN_GPU_ERR_LMAX.
+// in the most significant digit.  A tree deeper than that is built again from
+// 30-level keys (DEEP_LEVELS, the reference's LMAX, headers/macros.h:139):
+// levels 1..21 in the 64-bit word, levels 22..30 in a 27-bit second word.
 constexpr int KEY_LEVELS = 21;
+constexpr int DEEP_LEVELS = 30;
+constexpr int LO_LEVELS = DEEP_LEVELS - KEY_LEVELS;
 // cap on h growths in the grad-h candidate search (the reference loops forever
 // when fewer than pp_gather particles exist)
 constexpr int HGROW_CAP = 2000;

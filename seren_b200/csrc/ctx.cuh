@@ -77,6 +77,8 @@ struct Ctx {
   // build scratch
   unsigned long long* keys = nullptr;
   unsigned long long* keys_alt = nullptr;
+  unsigned long long* keys_hi = nullptr;   // deep builds: levels 1..21 in input order
+  unsigned* keys_lo = nullptr;             // deep builds: levels 22..30 in input order
   int* idx = nullptr;
   int* idx_alt = nullptr;
   int* rs_hist = nullptr;     // [256][nblk]

@@ -214,26 +214,30 @@ __device__ __forceinline__ void pair32_far(float d0, float d1, float d2, float i
   ap = fmaf(0.5f * mq, dpot, ap);
 }
 
-// BHgrav_accel.F90:159-189 in FP32, dr = rp - rc
-// q holds q1..q4, q5z (q5, -(q1 + q3)); m the cell mass
+// BHgrav_accel.F90:159-189 in FP32, dr = rp - rc, q holds q1..q4, q5z (q5,
+// -(q1 + q3)), m the cell mass.  Written with the unit vector n = dr/r so that
+// no power of 1/r above the second is formed: with Qn = Q.n and nQn = n.Q.n,
+//   a = (1/r^2) [ n (-m - 2.5 nQn/r^2) + Qn/r^2 ],  phi = (1/r) (m + nQn/(2 r^2)),
+// the reference's -m dr/r^3 + (Q.dr)/r^5 - 2.5 (dr.Q.dr) dr/r^7 and
+// m/r + (dr.Q.dr)/(2 r^5).  |Q|/r^2 is of order m theta^2 for an accepted cell,
+// so every FP32 intermediate stays in range however small the cell and its
+// distance (1/r^7 alone overflows FP32 below r ~ 4e-6).
 __device__ __forceinline__ void cell32(float d0, float d1, float d2, float m, const float4& q,
                                        const float2& q5z, float& ax, float& ay, float& az,
                                        float& ap) {
   const float drsqd = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
-  const float invdrmag = rsqrtf(drsqd);
-  const float invdrsqd = invdrmag * invdrmag;
-  const float invdr3 = invdrsqd * invdrmag;
-  const float invdr5 = invdr3 * invdrsqd;
-  const float qx = fmaf(q.w, d2, fmaf(q.y, d1, q.x * d0));
-  const float qy = fmaf(q5z.x, d2, fmaf(q.z, d1, q.y * d0));
-  const float qz = fmaf(q5z.y, d2, fmaf(q5z.x, d1, q.w * d0));
-  const float qscalar = fmaf(qz, d2, fmaf(qy, d1, qx * d0));
-  // -(2.5 (dr.Q.dr) / r^7 + m / r^3)
-  const float ng = fmaf(-2.5f * qscalar, invdr5 * invdrsqd, -(m * invdr3));
-  ax = fmaf(ng, d0, fmaf(qx, invdr5, ax));
-  ay = fmaf(ng, d1, fmaf(qy, invdr5, ay));
-  az = fmaf(ng, d2, fmaf(qz, invdr5, az));
-  ap = fmaf(m, invdrmag, fmaf(0.5f * qscalar, invdr5, ap));
+  const float invr = rsqrtf(drsqd);
+  const float invr2 = invr * invr;
+  const float n0 = d0 * invr, n1 = d1 * invr, n2 = d2 * invr;
+  const float qx = fmaf(q.w, n2, fmaf(q.y, n1, q.x * n0));
+  const float qy = fmaf(q5z.x, n2, fmaf(q.z, n1, q.y * n0));
+  const float qz = fmaf(q5z.y, n2, fmaf(q5z.x, n1, q.w * n0));
+  const float nqn = fmaf(qz, n2, fmaf(qy, n1, qx * n0)) * invr2;
+  const float g = fmaf(-2.5f, nqn, -m);
+  ax = fmaf(invr2, fmaf(g, n0, qx * invr2), ax);
+  ay = fmaf(invr2, fmaf(g, n1, qy * invr2), ay);
+  az = fmaf(invr2, fmaf(g, n2, qz * invr2), az);
+  ap = fmaf(invr, fmaf(0.5f, nqn, m), ap);
 }
 
 template <bool MIXED>
@@ -319,6 +323,23 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
     const float px32 = (float)(P.x - t.rootx), py32 = (float)(P.y - t.rooty),
                 pz32 = (float)(P.z - t.rootz);
     const float ux = (float)(P.x - rx), uy = (float)(P.y - ry), uz = (float)(P.z - rz);
+    // A separation formed in FP32 from two offsets to the reference point
+    // (d = a - u) carries an error of order 2^-24 |u|, relative 2^-23 |u|/|d|;
+    // the FP64 particle is used instead when some lane lies more than 64
+    // smoothing lengths (the group's least) from the reference point, e.g. a
+    // group that straddles a dense clump and its sparse surroundings (within
+    // that bound a pair at distance h is off by less than 1e-5 relative).
+    bool wide = false;
+    if constexpr (MIXED) {
+      float umax = live ? sqrtf(fmaf(uz, uz, fmaf(uy, uy, ux * ux))) : 0.0f;
+      float hmin = live ? (float)HZ.x : 3.0e38f;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        umax = fmaxf(umax, __shfl_xor_sync(FULLMASK, umax, o));
+        hmin = fminf(hmin, __shfl_xor_sync(FULLMASK, hmin, o));
+      }
+      wide = umax > 64.0f * hmin;
+    }
     // the group's bounding sphere in the walk's FP32 coordinates: centre the
     // middle of the live lanes' bounding box, radius the farthest live lane's
     // distance from it, rounded up
@@ -377,11 +398,21 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
       __syncwarp();
       if constexpr (MIXED) {
         float sx = 0.f, sy = 0.f, sz = 0.f, sp = 0.f;
+        if (!wide) {
 #pragma unroll 2
-        for (int e = 0; e < nc; ++e) {
-          if ((R.cmask[e] >> lane) & 1u) {
-            const float4 a = R.ca[e];
-            cell32(ux + a.x, uy + a.y, uz + a.z, a.w, R.cb[e], R.cq5[e], sx, sy, sz, sp);
+          for (int e = 0; e < nc; ++e) {
+            if ((R.cmask[e] >> lane) & 1u) {
+              const float4 a = R.ca[e];
+              cell32(ux + a.x, uy + a.y, uz + a.z, a.w, R.cb[e], R.cq5[e], sx, sy, sz, sp);
+            }
+          }
+        } else {
+          for (int e = 0; e < nc; ++e) {
+            if ((R.cmask[e] >> lane) & 1u) {
+              const double4 A = t.gA[R.cid[e]];
+              cell32((float)(P.x - A.x), (float)(P.y - A.y), (float)(P.z - A.z), R.ca[e].w,
+                     R.cb[e], R.cq5[e], sx, sy, sz, sp);
+            }
           }
         }
         kc.add(0, sx); kc.add(1, sy); kc.add(2, sz); kc.add(3, sp);
@@ -421,12 +452,10 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
         __syncwarp();
         if constexpr (MIXED) {
           float sx = 0.f, sy = 0.f, sz = 0.f, sp = 0.f;
-#pragma unroll 2
-          for (int e = 0; e < nb; ++e) {
+          auto item = [&](int e, float d0, float d1, float d2) {
             const bool on = ((R.qmask[b0 + e] >> lane) & 1u) && R.qid[b0 + e] != p;
             const float4 a = R.pa[e];
             const float2 b = R.pb[e];
-            const float d0 = a.x - ux, d1 = a.y - uy, d2 = a.z - uz;
             const float drsqd = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
             const float inv = rsqrtf(fmaxf(drsqd, 1.0e-30f));
             const float drmag = drsqd * inv;
@@ -436,6 +465,18 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
               if (on) pair32(d0, d1, d2, invhp32, zo32, a.w, b.x, b.y, tab32, sx, sy, sz, sp);
             } else if (on) {
               pair32_far(d0, d1, d2, inv, a.w, sx, sy, sz, sp);
+            }
+          };
+          if (!wide) {
+#pragma unroll 2
+            for (int e = 0; e < nb; ++e) {
+              const float4 a = R.pa[e];
+              item(e, a.x - ux, a.y - uy, a.z - uz);
+            }
+          } else {
+            for (int e = 0; e < nb; ++e) {
+              const double4 Q = pm[R.qid[b0 + e]];
+              item(e, (float)(Q.x - P.x), (float)(Q.y - P.y), (float)(Q.z - P.z));
             }
           }
           kc.add(0, sx); kc.add(1, sy); kc.add(2, sz); kc.add(3, sp);

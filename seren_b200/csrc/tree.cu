@@ -157,6 +157,44 @@ __global__ void k_keys(const double4* __restrict__ pm, int n, const TreeInfo* __
   idx[i] = (int)i;
 }
 
+// 30-level keys of the same comparisons, for trees deeper than KEY_LEVELS:
+// levels 1..21 in hi (as k_keys), levels 22..30 in lo (27 bits, level 22 in
+// the most significant digit).  keys gets lo as the first sort key.
+__global__ void k_keys_deep(const double4* __restrict__ pm, int n,
+                            const TreeInfo* __restrict__ info, unsigned long long* __restrict__ keys,
+                            unsigned long long* __restrict__ hi, unsigned* __restrict__ lo,
+                            int* __restrict__ idx) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double4 p = pm[i];
+  double cx = info->root[0], cy = info->root[1], cz = info->root[2];
+  double cs = info->cellsize;
+  unsigned long long kh = 0ull;
+  unsigned kl = 0u;
+#pragma unroll 1
+  for (int lev = 0; lev < DEEP_LEVELS; ++lev) {
+    const int d = (p.x > cx ? 1 : 0) | (p.y > cy ? 2 : 0) | (p.z > cz ? 4 : 0);
+    if (lev < KEY_LEVELS) kh = (kh << 3) | (unsigned long long)d;
+    else kl = (kl << 3) | (unsigned)d;
+    cs = 0.5 * cs;
+    cx = (d & 1) ? __dadd_rn(cx, cs) : __dsub_rn(cx, cs);
+    cy = (d & 2) ? __dadd_rn(cy, cs) : __dsub_rn(cy, cs);
+    cz = (d & 4) ? __dadd_rn(cz, cs) : __dsub_rn(cz, cs);
+  }
+  keys[i] = (unsigned long long)kl;
+  hi[i] = kh;
+  lo[i] = kl;
+  idx[i] = (int)i;
+}
+
+// after the stable sort on lo: the hi words in that order, the next sort key
+__global__ void k_gather_hi(const unsigned long long* __restrict__ hi, const int* __restrict__ idx,
+                            int n, unsigned long long* __restrict__ keys) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  keys[i] = hi[idx[i]];
+}
+
 // ---------------------------------------------------------------------------
 // stable LSD radix sort of (64-bit key, int) pairs, 8-bit digits
 constexpr int RS_T = 256;
@@ -252,12 +290,23 @@ __device__ __forceinline__ int key_digit(unsigned long long key, int lev) {
   return (int)((key >> (3 * (KEY_LEVELS - 1 - lev))) & 7ull);
 }
 
+// the octant digit of level lev+1 of the particle at sorted position i: from
+// the sorted 64-bit keys for the first KEY_LEVELS levels, from the input-order
+// lo words (deep builds) below that
+__device__ __forceinline__ int sorted_digit(const unsigned long long* __restrict__ keys,
+                                            const unsigned* __restrict__ lo,
+                                            const int* __restrict__ idx, int i, int lev) {
+  if (lev < KEY_LEVELS) return key_digit(keys[i], lev);
+  return (int)((lo[idx[i]] >> (3 * (DEEP_LEVELS - 1 - lev))) & 7u);
+}
+
 // children of every branch cell on level lev: boundaries of the octant digit
 // runs inside the cell's (sorted) particle range
 __global__ void k_split(const int* __restrict__ branch, const TreeInfo* __restrict__ info, int lev,
                         const int* __restrict__ pstart, const int* __restrict__ pcount,
-                        const unsigned long long* __restrict__ keys, int* __restrict__ nchild,
-                        int* __restrict__ cstart) {
+                        const unsigned long long* __restrict__ keys,
+                        const unsigned* __restrict__ lo_words, const int* __restrict__ idx,
+                        int* __restrict__ nchild, int* __restrict__ cstart) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= info->nbranch) return;
   const int b = branch[j];
@@ -269,7 +318,7 @@ __global__ void k_split(const int* __restrict__ branch, const TreeInfo* __restri
     int lo = st[d - 1], hi = e;
     while (lo < hi) {
       const int mid = lo + ((hi - lo) >> 1);
-      if (key_digit(keys[mid], lev) < d) lo = mid + 1;
+      if (sorted_digit(keys, lo_words, idx, mid, lev) < d) lo = mid + 1;
       else hi = mid;
     }
     st[d] = lo;
@@ -721,42 +770,42 @@ void launch_pack_parray(Ctx& c, double* stage, int n, cudaStream_t s) {
   k_pack_parray<<<nb(n, 256), 256, 0, s ? s : c.st>>>(stage, n, c.pm, c.hz); ++c.nlaunch;
 }
 
-static int radix_sort(Ctx& c, int n) {
+// stable LSD sort of (keys, idx) on the key bits [0, bits), 8 at a time; an
+// even number of passes leaves the sorted data in keys/idx
+static void radix_sort(Ctx& c, int n, int bits) {
   const int nblk = nb(n, RS_TILE);
   unsigned long long* ka = c.keys;
   unsigned long long* kb = c.keys_alt;
   int* va = c.idx;
   int* vb = c.idx_alt;
-  for (int shift = 0; shift < 64; shift += 8) {
+  for (int shift = 0; shift < bits; shift += 8) {
     k_rs_hist<<<nblk, RS_T, 0, c.st>>>(ka, n, shift, c.rs_hist, nblk); ++c.nlaunch;
     scan_exclusive(c, c.rs_hist, c.rs_hist, 256 * nblk);
     k_rs_scatter<<<nblk, RS_T, 0, c.st>>>(ka, va, kb, vb, n, shift, c.rs_hist, nblk); ++c.nlaunch;
     std::swap(ka, kb);
     std::swap(va, vb);
   }
-  // 8 passes: the sorted data are back in keys/idx
-  return 0;
 }
 
-int build_tree(Ctx& c) {
+constexpr int NEED_DEEP_KEYS = -1;
+
+// cells level by level from the sorted keys; with 21-level keys, a tree that
+// needs level 22 returns NEED_DEEP_KEYS
+static int build_cells(Ctx& c, bool deep, int& ctot_out) {
   const int n = c.ptot;
-  const int bblk = std::min(nb(n, BB_T), 1184);
-  k_bbox_partial<<<bblk, BB_T, 0, c.st>>>(c.pm, n, c.bbox_part); ++c.nlaunch;
-  k_bbox_final<<<1, BB_T, 0, c.st>>>(c.bbox_part, bblk, c.d_info); ++c.nlaunch;
-  k_keys<<<nb(n, 256), 256, 0, c.st>>>(c.pm, n, c.d_info, c.keys, c.idx); ++c.nlaunch;
-  radix_sort(c, n);
   k_root<<<1, 1, 0, c.st>>>(n, c.cmax, c.leaf, c.nextcell, c.ifopen, c.pstart, c.pcount, c.parent,
                             c.level, c.branch, c.d_info); ++c.nlaunch;
   int nbranch = 1, ctot = 0, lev = 0;
   int* br = c.branch;
   int* br_next = c.branch_next;
   while (true) {
-    if (lev >= KEY_LEVELS || lev >= c.prm.lmax) {
-      c.err = "tree deeper than the supported number of levels";
+    if (lev >= c.prm.lmax) {                // BHgrav_build.F90:289
+      c.err = "Reached maximum level (tree deeper than lmax)";
       return SEREN_GPU_ERR_LMAX;
     }
+    if (!deep && lev >= KEY_LEVELS) return NEED_DEEP_KEYS;
     k_split<<<nb(nbranch, 128), 128, 0, c.st>>>(br, c.d_info, lev, c.pstart, c.pcount, c.keys,
-                                                c.nchild, c.cstart); ++c.nlaunch;
+                                                c.keys_lo, c.idx, c.nchild, c.cstart); ++c.nlaunch;
     scan_exclusive(c, c.nchild, c.choff, nbranch);
     int nnew = 0;
     if (read_dev(c, c.scan.total, &nnew, sizeof(int))) return SEREN_GPU_ERR_CUDA;
@@ -779,6 +828,30 @@ int build_tree(Ctx& c) {
     nbranch = nbn;
     if (nbranch == 0) break;
   }
+  ctot_out = ctot;
+  return SEREN_GPU_OK;
+}
+
+int build_tree(Ctx& c) {
+  const int n = c.ptot;
+  const int bblk = std::min(nb(n, BB_T), 1184);
+  k_bbox_partial<<<bblk, BB_T, 0, c.st>>>(c.pm, n, c.bbox_part); ++c.nlaunch;
+  k_bbox_final<<<1, BB_T, 0, c.st>>>(c.bbox_part, bblk, c.d_info); ++c.nlaunch;
+  k_keys<<<nb(n, 256), 256, 0, c.st>>>(c.pm, n, c.d_info, c.keys, c.idx); ++c.nlaunch;
+  radix_sort(c, n, 64);
+  int ctot = 0;
+  int rc = build_cells(c, false, ctot);
+  if (rc == NEED_DEEP_KEYS) {
+    // sort on (levels 1..21, levels 22..30): stable passes on the low word,
+    // then on the high word in that order
+    k_keys_deep<<<nb(n, 256), 256, 0, c.st>>>(c.pm, n, c.d_info, c.keys, c.keys_hi, c.keys_lo,
+                                               c.idx); ++c.nlaunch;
+    radix_sort(c, n, 32);
+    k_gather_hi<<<nb(n, 256), 256, 0, c.st>>>(c.keys_hi, c.idx, n, c.keys); ++c.nlaunch;
+    radix_sort(c, n, 64);
+    rc = build_cells(c, true, ctot);
+  }
+  if (rc) return rc;
   k_leaf_order<<<nb(ctot + 1, 256), 256, 0, c.st>>>(c.leaf, c.pstart, ctot, c.idx); ++c.nlaunch;
   if (c.reorder_wait) {                     // velocities and c_s^2 still being copied in
     k_reorder_pos<<<nb(n, 256), 256, 0, c.st>>>(c.idx, n, c.pm, c.hz, c.orig, c.pm_alt, c.hz_alt,

@@ -87,3 +87,16 @@ def lists_equal(pptot_a, pplist_a, pptot_b, pplist_b, limit):
         if k <= limit and not np.array_equal(pplist_a[p, :k], pplist_b[p, :k]):
             return False
     return True
+
+
+def deep_clump(a: float, n_core: int = 4000, n_halo: int = 4000):
+    """A tight Plummer clump (scale radius a, half the mass) inside a uniform
+    halo of radius 10: the root box is ~1e6 clump radii wide, so the octree
+    needs more than 21 levels (24 at a = 1e-5, 29 at a = 3e-7)."""
+    core = ics.plummer(n=n_core, seed=21, a=a, mass=0.5, rtrunc=20 * a)
+    halo = ics.uniform_sphere(n=n_halo, seed=22, radius=10.0, mass=0.5)
+    ic = dict(halo)
+    ic["parray"] = np.vstack([core["parray"], halo["parray"]])
+    ic["v"] = np.vstack([np.zeros((n_core, 3)), halo["v"]])
+    ic["sound"] = np.full(n_core + n_halo, 0.1)
+    return ic

@@ -709,3 +709,53 @@ def test_accretion_full_size_properties(libs):
     assert np.array_equal(cnt, np.bincount(near[~kept], minlength=8))
     g.force_step(first_call=False)
     assert np.isfinite(g.download()["a"]).all()
+
+
+@pytest.mark.parametrize("a", [1e-5, 3e-7])
+def test_deep_tree_bit_exact_and_full_evaluation(libs, a):
+    """Trees of 22-30 levels (the reference's LMAX = 30, headers/macros.h:139):
+    a tight clump inside a wide halo.  The GPU builds them from 30-level keys;
+    cells, order and stock are bit-exact, and the whole evaluation matches."""
+    from tests.helpers import deep_clump
+    ic = deep_clump(a)
+    o, g = _pair(libs, ic)
+    po, permo = o.tree_update(ic["parray"])
+    pg, permg = g.tree_update(ic["parray"])
+    assert np.array_equal(permo, permg)
+    to, tg = o.tree_export(), g.tree_export()
+    assert to["ltot"] > 21 and to["ltot"] == tg["ltot"] and to["ctot"] == tg["ctot"]
+    for k in ("leaf", "nextcell", "ifopen", "plist", "first_cell", "last_cell"):
+        assert np.array_equal(to[k], tg[k]), k
+    for k in ("grav_r", "grav_m", "grav_q", "dminsqd", "hydro_r", "rmax"):
+        assert np.array_equal(to[k], tg[k]), k
+    o, g = _pair(libs, ic)
+    ro = run_pipeline(o, ic)
+    rg = run_pipeline(g, ic)
+    so, sg = ro["sph"], rg["sph"]
+    assert rel_rows(sg["parray"][:, 4], so["parray"][:, 4]).max() < TOL
+    assert rel_rows(sg["rho"], so["rho"]).max() < TOL
+    assert lists_equal(so["pptot"], so["pplist"], sg["pptot"], sg["pplist"], g.params.pp_limit)
+    assert rel_scaled(rg["a_hydro"], ro["a_hydro"]) < TOL
+    assert rel_rows(rg["a"], ro["a"]).max() < 1e-11
+    g32 = libs[1](ic["parray"].shape[0], params(ic, precision=1))
+    r32 = run_pipeline(g32, ic)
+    assert np.array_equal(r32["perm"], rg["perm"])
+    err = rel_rows(r32["a"], rg["a"])
+    assert np.sqrt(np.mean(err ** 2)) < 1e-5
+
+
+def test_tree_beyond_lmax_fails_like_the_reference(libs):
+    """A clump that needs more than 30 levels, and a 24-level tree under
+    lmax = 22: both the oracle and the GPU stop with ERR_LMAX."""
+    from seren_b200.cabi import SerenError
+    from tests.helpers import deep_clump
+    for a, lmax in ((1e-7, 30), (1e-5, 22)):
+        ic = deep_clump(a)
+        n = ic["parray"].shape[0]
+        prm = params(ic)
+        prm.lmax = lmax
+        Oracle, Gpu = libs
+        for hp in (Oracle(n, prm), Gpu(n, prm)):
+            with pytest.raises(SerenError) as e:
+                hp.tree_update(ic["parray"])
+            assert e.value.code == 3
