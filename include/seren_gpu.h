@@ -96,6 +96,19 @@ int seren_gpu_sph_update(seren_gpu_ctx* ctx, int32_t ptot, const int32_t* acclis
 int seren_gpu_get_neib(seren_gpu_ctx* ctx, int32_t ptot, const int32_t* acclist,
                        int32_t nacc, const double* h, int32_t* pptot, int32_t* pplist);
 
+/* h_gather (sph/h_gather.F90:14-203), the standard-SPH smoothing length loop
+ * of sph_sim/sph_update.F90:111-119, then BHhydro_update_hmax (:121-124):
+ * for each active particle (acclist, NULL: all) of the last tree_update,
+ * h = INVKERNRANGE*sqrt(d2) with d2 the pp_gather-th smallest squared
+ * distance to another particle, the value the reference's search and
+ * insertion sort select whatever the guess (MINIMUM_H is not applied).  The
+ * new h is written to column 4 of the active rows of parray (tree order) and
+ * kept on the device for a following seren_gpu_get_neib.  Fewer than
+ * pp_gather other particles (the reference loops forever) give
+ * SEREN_GPU_ERR_WALK. */
+int seren_gpu_h_gather(seren_gpu_ctx* ctx, int32_t ptot, const int32_t* acclist, int32_t nacc,
+                       double* parray);
+
 /* sph_hydro_forces (sph_sim/sph_hydro_forces.F90:41-85) with hydro_gradh
  * (sph/hydro_gradh.F90:9-339, MON97): a[p] is OVERWRITTEN with the hydro
  * acceleration of each active particle (inactive rows are left as they are). */

@@ -649,6 +649,105 @@ struct seren_oracle {
     return pp_pot;
   }
 
+  // sph/h_gather.F90:14-203 (BH_TREE, insertion sort, no MINIMUM_H): h from
+  // exactly pp_gather neighbours.  distance2 is main/distance2.F90:30-60
+  // (dr = r_pp - r_p, dr1^2 + dr2^2 + dr3^2 left to right).  The reference
+  // loops forever when fewer than pp_gather other particles exist; here the
+  // search stops once h_high passes 1e6 root extents (SEREN_GPU_ERR_WALK).
+  int h_gather(int p, double& hguess, int64_t& nodes) const {
+    const double rp[3] = {parray[p * 6 + 0], parray[p * 6 + 1], parray[p * 6 + 2]};
+    const int pp_gather = prm.pp_gather;
+    int pp_pot = 0;                                                       // :46-55
+    int pp_max = LISTSIZE;
+    const double h_old = hguess;
+    double h_high = HMULT * h_old;
+    double h_low = h_old / HMULT;
+    double h_search = 0.0;
+    double hrangesqd_high = (KERNRANGESQD * h_high) * h_high;
+    std::vector<int> potlist;
+    std::vector<int> high_list(pp_max);
+    std::vector<double> rsqd_high(pp_max);
+    int pp_low = 0, pp_high = 0;
+    const double hcap = 1.0e6 * (rextent > 0.0 ? rextent : 1.0);
+    while (true) {                                                        // :62-160
+      while (true) {                                                      // :66-107
+        if (h_high > h_search) {
+          h_search = HMULT * h_high;
+          pp_pot = hgather_walk(rp, KERNRANGE * h_search, pp_max, potlist, nodes);
+        }
+        if (pp_pot < 0) {                                                 // :92-101
+          h_search = 0.0;
+          pp_pot = 0;
+          pp_max = ptot;
+          high_list.assign(pp_max, 0);
+          rsqd_high.assign(pp_max, 0.0);
+        } else if (pp_pot <= pp_gather) {                                 // :102-107
+          pp_pot = 0;
+          h_search = 0.0;
+          h_low = h_high;
+          h_high = HMULT * h_high;
+          hrangesqd_high = (KERNRANGESQD * h_high) * h_high;
+          if (h_high > hcap) return SEREN_GPU_ERR_WALK;
+        }
+        if (pp_pot > 0) break;
+      }
+      int pp_tot = 0;                                                     // :111-113
+      pp_high = 0;
+      pp_low = 0;
+      hrangesqd_high = (KERNRANGESQD * h_high) * h_high;
+      const double hrangesqd_low = (KERNRANGESQD * h_low) * h_low;
+      for (int i = 0; i < pp_pot; ++i) {                                  // :120-139
+        const int pp = potlist[i];
+        if (pp == p) continue;
+        const double dr0 = parray[pp * 6 + 0] - rp[0];
+        const double dr1 = parray[pp * 6 + 1] - rp[1];
+        const double dr2 = parray[pp * 6 + 2] - rp[2];
+        const double drsqd = (dr0 * dr0 + dr1 * dr1) + dr2 * dr2;
+        if (drsqd < hrangesqd_high) {
+          if (drsqd < hrangesqd_low) {
+            pp_low = pp_low + 1;
+          } else {
+            pp_high = pp_high + 1;
+            high_list[pp_high - 1] = pp;
+            rsqd_high[pp_high - 1] = drsqd;
+          }
+        }
+        if (pp_high == pp_max) break;
+      }
+      pp_tot = pp_low + pp_high;                                          // :143
+      if (pp_tot < pp_gather) {                                           // :147-151
+        h_low = h_high;
+        h_high = HMULT * h_high;
+        hrangesqd_high = (KERNRANGESQD * h_high) * h_high;
+        if (h_high > hcap) return SEREN_GPU_ERR_WALK;
+        continue;
+      } else if (pp_low >= pp_gather) {                                   // :154-157
+        h_high = h_low;
+        h_low = h_low / HMULT;
+        continue;
+      } else {                                                            // :160-162
+        break;
+      }
+    }
+    // insertion sort of the annulus (sorts/insertion_sort.F90), then the
+    // (pp_gather - pp_low)-th smallest, :179-183
+    for (int j = 1; j < pp_high; ++j) {
+      const double a = rsqd_high[j];
+      const int ia = high_list[j];
+      int i = j - 1;
+      while (i >= 0 && rsqd_high[i] > a) {
+        rsqd_high[i + 1] = rsqd_high[i];
+        high_list[i + 1] = high_list[i];
+        --i;
+      }
+      rsqd_high[i + 1] = a;
+      high_list[i + 1] = ia;
+    }
+    const double drsqd = rsqd_high[pp_gather - pp_low - 1];
+    hguess = INVKERNRANGE * std::sqrt(drsqd);
+    return SEREN_GPU_OK;
+  }
+
   // BHtree/BHhydro_walk.F90:9-80 (gather and scatter candidate walk)
   int hydro_walk(const double rp[3], double hrange, int pp_max, std::vector<int>& list) const {
     int c = 0;
@@ -1264,6 +1363,33 @@ int seren_oracle_get_neib(seren_oracle* o, int32_t ptot, const int32_t* acclist,
     if (pplist && o->pptot[p] <= L)
       for (int k = 0; k < o->pptot[p]; ++k) pplist[(size_t)p * L + k] = o->pplist[(size_t)p * L + k] + o->base();
   }
+  return SEREN_GPU_OK;
+}
+
+int seren_oracle_h_gather(seren_oracle* o, int32_t ptot, const int32_t* acclist, int32_t nacc,
+                          double* parray) {
+  if (!o || !parray || ptot != o->ptot || !o->have_tree) return SEREN_GPU_ERR_STATE;
+  std::vector<int> act = o->active_list(acclist, nacc);
+  if (!o->active_ok(act)) return o->fail(SEREN_GPU_ERR_ARG, "acclist id out of range");
+  std::vector<double> hnew(act.size());
+  int rc_all = SEREN_GPU_OK;
+  int64_t nodes = 0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : nodes)
+  for (int i = 0; i < (int)act.size(); ++i) {
+    double h = o->parray[act[i] * 6 + 4];
+    const int rc = o->h_gather(act[i], h, nodes);
+    if (rc) {
+#pragma omp critical
+      rc_all = rc;
+    }
+    hnew[i] = h;
+  }
+  if (rc_all) return o->fail(rc_all, "fewer than pp_gather neighbours (h_gather)");
+  for (size_t i = 0; i < act.size(); ++i) {
+    o->parray[act[i] * 6 + 4] = hnew[i];
+    parray[act[i] * 6 + 4] = hnew[i];
+  }
+  o->update_hmax();                      // sph_update.F90:121-124
   return SEREN_GPU_OK;
 }
 

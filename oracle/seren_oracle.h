@@ -58,6 +58,8 @@ int seren_oracle_sph_update(seren_oracle* o, int32_t ptot, const int32_t* acclis
                             int32_t* pplist, int32_t first_call);
 int seren_oracle_get_neib(seren_oracle* o, int32_t ptot, const int32_t* acclist,
                           int32_t nacc, const double* h, int32_t* pptot, int32_t* pplist);
+int seren_oracle_h_gather(seren_oracle* o, int32_t ptot, const int32_t* acclist, int32_t nacc,
+                          double* parray);
 int seren_oracle_hydro_forces(seren_oracle* o, const int32_t* acclist, int32_t nacc,
                               const double* press, const double* sound, double* a);
 int seren_oracle_grav_forces(seren_oracle* o, const int32_t* acclist, int32_t nacc,

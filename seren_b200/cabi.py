@@ -74,6 +74,7 @@ def bind(lib: C.CDLL, prefix: str) -> C.CDLL:
     f("sph_update", [vp, C.c_int32, _ip, C.c_int32, _dp, _dp, _dp, _dp, _dp, _dp, _ip, _ip,
                      C.c_int32])
     f("get_neib", [vp, C.c_int32, _ip, C.c_int32, _dp, _ip, _ip])
+    f("h_gather", [vp, C.c_int32, _ip, C.c_int32, _dp])
     f("hydro_forces", [vp, _ip, C.c_int32, _dp, _dp, _dp])
     f("grav_forces", [vp, _ip, C.c_int32, _dp, _dp, C.c_int32, _dp])
     f("sink_forces", [vp, C.c_int32, _dp, _dp, _dp])
@@ -162,6 +163,15 @@ class HotPath:
         acc, nacc = self._acc(acclist)
         self._call("get_neib", self._ctx, n, _i(acc), nacc, _d(hh), _i(pptot), _i(pplist))
         return pptot, pplist
+
+    def h_gather(self, parray, acclist=None):
+        """Standard-SPH smoothing lengths from exactly pp_gather neighbours
+        (sph/h_gather.F90) for the active particles of the last tree; returns
+        parray with column 4 (h) updated for them."""
+        parray = _f64(parray).copy()
+        acc, nacc = self._acc(acclist)
+        self._call("h_gather", self._ctx, self.ptot, _i(acc), nacc, _d(parray))
+        return parray
 
     def hydro_forces(self, press, sound, a=None, acclist=None):
         n = self.ptot

@@ -633,6 +633,32 @@ int seren_gpu_get_neib(seren_gpu_ctx* h, int32_t ptot, const int32_t* acclist, i
   return SEREN_GPU_OK;
 }
 
+int seren_gpu_h_gather(seren_gpu_ctx* h, int32_t ptot, const int32_t* acclist, int32_t nacc,
+                       double* parray) {
+  if (!h) return SEREN_GPU_ERR_ARG;
+  Ctx& c = h->c;
+  if (!parray) return fail(c, SEREN_GPU_ERR_ARG, "parray is NULL");
+  int rc = seren::check_tree(c, ptot);
+  if (rc) return rc;
+  int nact = 0;
+  rc = seren::set_active(c, acclist, nacc, nact);
+  if (rc) return rc;
+  seren::launch_hgather(c, nact);
+  seren::launch_update_hmax(c);            // sph_sim/sph_update.F90:121-124
+  rc = finish(c, "h_gather");
+  if (rc) return rc;
+  // the new h of the active rows (hz = (h, zeta) per particle, tree order)
+  std::vector<double> hzh((size_t)ptot * 2);
+  cudaError_t e = cudaMemcpy(hzh.data(), c.hz, sizeof(double) * hzh.size(), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return seren::cuda_fail(c, e, "h_gather");
+  const int na = acclist ? nact : ptot;
+  for (int i = 0; i < na; ++i) {
+    const int p = acclist ? acclist[i] - c.prm.index_base : i;
+    parray[(size_t)p * 6 + 4] = hzh[(size_t)p * 2];
+  }
+  return SEREN_GPU_OK;
+}
+
 int seren_gpu_hydro_forces(seren_gpu_ctx* h, const int32_t* acclist, int32_t nacc,
                            const double* press, const double* sound, double* a) {
   if (!h) return SEREN_GPU_ERR_ARG;

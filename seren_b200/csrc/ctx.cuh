@@ -206,6 +206,7 @@ int scan_scratch_alloc(ScanScratch& s, int nmax);
 
 // sph.cu
 void launch_gradh(Ctx& c, int nact);
+void launch_hgather(Ctx& c, int nact);  // h_gather (standard SPH)
 void launch_neib(Ctx& c, int nact);
 void launch_hydro(Ctx& c, int nact, double* amap = nullptr);   // amap: mapped host a (optional)
 void launch_thermal(Ctx& c);

@@ -966,6 +966,142 @@ __global__ void __launch_bounds__(RD_THREADS) k_gradh_redo(
   }
 }
 
+// ---------------------------------------------------------------------------
+// sph/h_gather.F90:14-203 (standard SPH: h from exactly pp_gather neighbours).
+// The reference narrows [h_low, h_high] until 2h_low holds fewer than
+// pp_gather other particles and 2h_high at least pp_gather (:143-162), then
+// sorts the squared distances of the annulus between them and takes the
+// (pp_gather - pp_low)-th (:179-183).  The pp_low particles inside 2h_low are
+// all nearer, so the result is h = INVKERNRANGE*sqrt(d2), d2 the pp_gather-th
+// smallest squared distance (r_pp - r_p, distance2.F90's order of terms) from
+// p to any other particle: it does not depend on the guess or on the path the
+// limits take.  One warp per particle finds that value directly: walks with
+// BHhydrowalk_hgather's test (the redo kernel's breadth-first walk) at a
+// radius R that grows until the ball r < R holds at least pp_gather others
+// (shrinking when it holds more than the selection buffer), then a bitonic
+// sort in shared memory of the squared distances inside the ball.
+constexpr int HG_THREADS = 128;
+constexpr int HG_WARPS = HG_THREADS / 32;
+constexpr int HG_SEL = 1024;       // squared distances sorted per particle at most
+constexpr int HG_ROUNDS = 400;     // radius changes per particle at most
+
+__device__ void hg_sort(double* v, int n, int lane) {
+  int N = 32;
+  while (N < n) N <<= 1;
+  for (int k = n + lane; k < N; k += 32) v[k] = INFINITY;
+  __syncwarp();
+  for (int size = 2; size <= N; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int i = lane; i < (N >> 1); i += 32) {
+        const int lo = 2 * i - (i & (stride - 1));
+        const int hi = lo + stride;
+        const bool up = (lo & size) == 0;
+        const double x = v[lo], y = v[hi];
+        if ((x > y) == up) {
+          v[lo] = y;
+          v[hi] = x;
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+__global__ void __launch_bounds__(HG_THREADS) k_hgather(
+    int nact, const int* __restrict__ act, const double4* __restrict__ pm,
+    double2* __restrict__ hz, HydroTree t, int pp_gather, double rextent,
+    int* __restrict__ scratch, int cap, DevError* err, unsigned long long* counts) {
+  __shared__ double sel_all[HG_WARPS][HG_SEL];
+  __shared__ int cand_all[HG_WARPS][GP_SEG * LEAFMAX];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  double* sel = sel_all[w];
+  int* cand = cand_all[w];
+  const int gw = blockIdx.x * HG_WARPS + w;
+  int* fa = scratch + (size_t)gw * 3 * cap;
+  int* fb = fa + cap;
+  int* lv = fb + cap;
+  const unsigned lt = (1u << lane) - 1u;
+  unsigned long long nwalk = 0, nvisit = 0;
+  const double rcap = 4.0 * (rextent > 0.0 ? rextent : 1.0);   // a ball that holds every particle
+  for (int i = gw; i < nact; i += gridDim.x * HG_WARPS) {
+    const int p = act ? act[i] : i;
+    const double4 P = pm[p];
+    const double rx = P.x, ry = P.y, rz = P.z;
+    const float px = (float)(rx - t.rootx), py = (float)(ry - t.rooty), pz = (float)(rz - t.rootz);
+    double Rw = KERNRANGE * (HMULT * (HMULT * hz[p].x));    // the reference's first search radius
+    if (!(Rw > 0.0) || !isfinite(Rw)) Rw = ldexp(rcap, -12);  // the guess does not change h
+    float R32 = 0.0f;
+    auto gather_test = [&](int c) {                     // BHhydrowalk_hgather.F90:36-40
+      const float4 h32 = t.hA32[c];
+      const float d0 = h32.x - px, d1 = h32.y - py, d2 = h32.z - pz;
+      const int r = test32((d0 * d0 + d1 * d1) + d2 * d2, R32 + h32.w, t.delta);
+      if (r >= 0) return r == 1;
+      const double4 h = t.hA[c];
+      const double e0 = h.x - rx, e1 = h.y - ry, e2 = h.z - rz;
+      const double tt = Rw + h.w;
+      return ((e0 * e0 + e1 * e1) + e2 * e2) <= tt * tt;
+    };
+    double Rlo = 0.0;            // a radius known to hold fewer than pp_gather others
+    double Rhi = INFINITY;       // a radius known to hold more than HG_SEL others (or to overflow)
+    bool done = false;
+    for (int round = 0; round < HG_ROUNDS && !done; ++round) {
+      if (!(Rw > 0.0) || !isfinite(Rw)) break;
+      R32 = (float)Rw;
+      int cnt = 0;
+      ++nwalk;
+      const int nl = rd_walk(t, lane, fa, fb, lv, cap, cnt, nvisit, gather_test);
+      // the opened leaves hold every particle with r <= Rw; count those well
+      // inside (r^2 below Rw^2 (1 - 2^-40), clear of the walk's rounding)
+      const double rc2 = (Rw * Rw) * (1.0 - 0x1p-40);
+      int nin = 0;
+      if (nl >= 0) {
+        for (int s0 = 0; s0 < nl; s0 += GP_SEG) {
+          const int nc = gp_flatten(lv + s0, min(GP_SEG, nl - s0), cand, lane);
+          for (int b = 0; b < nc; b += 32) {
+            const int k = b + lane;
+            double drsqd = 0.0;
+            bool in = false;
+            if (k < nc) {
+              const int q = cand[k];
+              const double4 Q = pm[q];
+              const double d0 = Q.x - rx, d1 = Q.y - ry, d2 = Q.z - rz;   // distance2.F90
+              drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
+              in = q != p && drsqd < rc2;
+            }
+            const unsigned mi = __ballot_sync(FULL, in);
+            const int o = nin + __popc(mi & lt);
+            if (in && o < HG_SEL) sel[o] = drsqd;
+            nin += __popc(mi);
+          }
+        }
+      }
+      double Rn;
+      if (nl >= 0 && nin >= pp_gather && nin <= HG_SEL) {
+        hg_sort(sel, nin, lane);
+        if (lane == 0) hz[p].x = INVKERNRANGE * sqrt(sel[pp_gather - 1]);   // :182-183
+        done = true;
+        __syncwarp();
+        break;
+      } else if (nl >= 0 && nin < pp_gather) {
+        Rlo = Rw;
+        if (Rw > rcap) break;                          // fewer than pp_gather others exist
+        Rn = isfinite(Rhi) ? 0.5 * (Rw + Rhi) : 2.0 * Rw;
+      } else {                                         // too many inside, or the walk overflowed
+        Rhi = Rw;
+        Rn = Rlo > 0.0 ? 0.5 * (Rlo + Rw) : 0.5 * Rw;
+      }
+      __syncwarp();
+      if (!(Rn > Rlo) || !(Rn < Rhi)) break;           // the bracket cannot narrow further
+      Rw = Rn;
+    }
+    if (!done && lane == 0) set_error(err, SEREN_GPU_ERR_WALK, KID_GRADH, p, -2);
+  }
+  if (lane == 0) {
+    atomicAdd(counts + 3, nwalk);
+    atomicAdd(counts + 4, nvisit);
+  }
+}
+
 // sum over the block, the same value on every thread
 __device__ double block_sum(double v, double* sh) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -1760,6 +1896,16 @@ void launch_hydro(Ctx& c, int nact, double* amap) {
         nact, c.act, c.pm, c.hz, c.vel, c.rho, c.pf, c.hf4, c.sound, c.pptot, c.pplist,
         c.prm.pp_limit, hydro_tree(c), c.tabG, c.prm.alpha, c.prm.kernel == 1, c.acc, amap,
         c.d_err);
+  ++c.nlaunch;
+}
+
+void launch_hgather(Ctx& c, int nact) {
+  if (nact <= 0) return;
+  unsigned long long* counts = reinterpret_cast<unsigned long long*>(c.d_counts);
+  // three walk-stack slots of scratch per warp, as the redo kernel
+  k_hgather<<<std::max(1, (c.wstack_slots / 3) / HG_WARPS), HG_THREADS, 0, c.st>>>(
+      nact, c.act, c.pm, c.hz, hydro_tree(c), c.prm.pp_gather, c.info.rextent,
+      reinterpret_cast<int*>(c.wstack), 2 * c.wstack_cap, c.d_err, counts);
   ++c.nlaunch;
 }
 

@@ -8,6 +8,7 @@ within 1e-5 rms / 1e-3 max of the FP64 path.  All calls go through the C ABI.
 import numpy as np
 import pytest
 
+from seren_b200 import ics
 from tests.helpers import case, lists_equal, params, rel_rows, rel_scaled, run_pipeline
 
 pytestmark = pytest.mark.gpu
@@ -759,3 +760,51 @@ def test_tree_beyond_lmax_fails_like_the_reference(libs):
             with pytest.raises(SerenError) as e:
                 hp.tree_update(ic["parray"])
             assert e.value.code == 3
+
+
+@pytest.mark.parametrize("name", ["sphere4k", "plummer16k", "disc12k", "ragged777", "tiny100"])
+def test_h_gather_bit_exact(libs, name):
+    """h_gather (sph/h_gather.F90) for every particle, then for an active
+    subset with Fortran ids: h bit-exact with the oracle's restatement, and
+    the neighbour lists at that h too."""
+    ic = case(name)
+    o, g = _pair(libs, ic)
+    po, permo = o.tree_update(ic["parray"])
+    pg, permg = g.tree_update(ic["parray"])
+    assert np.array_equal(permo, permg)
+    ho = o.h_gather(po)
+    hg = g.h_gather(pg)
+    assert np.array_equal(ho[:, 4], hg[:, 4])
+    pto, plo = o.get_neib()
+    ptg, plg = g.get_neib()
+    assert lists_equal(pto, plo, ptg, plg, g.params.pp_limit)
+    n = ic["parray"].shape[0]
+    o1, g1 = _pair(libs, ic, index_base=1)
+    po, _ = o1.tree_update(ic["parray"])
+    pg, _ = g1.tree_update(ic["parray"])
+    acc = np.arange(1, n + 1, 3, dtype=np.int32)
+    ho = o1.h_gather(po, acclist=acc)
+    hg = g1.h_gather(pg, acclist=acc)
+    assert np.array_equal(ho[:, 4], hg[:, 4])
+    rest = np.setdiff1d(np.arange(n), acc - 1)
+    assert np.array_equal(hg[rest, 4], pg[rest, 4])       # inactive rows untouched
+
+
+def test_h_gather_deep_clump_and_too_few_particles(libs):
+    """A 24-level tree (h spanning seven decades) is bit-exact too; with
+    fewer particles than pp_gather + 1 the reference never ends its search,
+    here both stop with ERR_WALK."""
+    from seren_b200.cabi import SerenError
+    from tests.helpers import deep_clump
+    ic = deep_clump(1e-5)
+    o, g = _pair(libs, ic)
+    po, _ = o.tree_update(ic["parray"])
+    pg, _ = g.tree_update(ic["parray"])
+    assert np.array_equal(o.h_gather(po)[:, 4], g.h_gather(pg)[:, 4])
+    small = ics.uniform_sphere(n=40, seed=8)
+    o, g = _pair(libs, small)
+    for hp in (o, g):
+        p, _ = hp.tree_update(small["parray"])
+        with pytest.raises(SerenError) as e:
+            hp.h_gather(p)
+        assert e.value.code == 5

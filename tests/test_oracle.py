@@ -285,3 +285,25 @@ def test_sink_search_picks_as_the_reference_does():
                      rhosink=np.percentile(rho, 90), sinkrad=0.05, div_v_search=False,
                      div_a_search=False)
     assert s2["psink"] == cand[2] and all(s2["flags"])
+
+
+@pytest.mark.parametrize("name", ["sphere4k", "plummer16k", "disc12k", "ragged777"])
+def test_h_gather_is_the_pp_gather_th_neighbour_distance(name):
+    """The oracle's h_gather (a statement-by-statement restatement of
+    sph/h_gather.F90, insertion sort included) against an independent brute
+    force: h = 0.5 sqrt of the pp_gather-th smallest squared distance to any
+    other particle, bit for bit (the same FP64 expression per pair)."""
+    ic = case(name)
+    n = ic["parray"].shape[0]
+    prm = params(ic)
+    o = Oracle(n, prm)
+    p, _ = o.tree_update(ic["parray"])
+    h = o.h_gather(p)[:, 4]
+    x = p[:, :3]
+    k = prm.pp_gather
+    for i in range(0, n, max(1, n // 300)):
+        d = x - x[i]
+        d2 = (d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2]
+        d2[i] = np.inf
+        assert h[i] == 0.5 * np.sqrt(np.partition(d2, k - 1)[k - 1]), i
+    o.close()
