@@ -165,6 +165,57 @@ int seren_gpu_timestep(seren_gpu_ctx* ctx, double courant_mult, double accel_mul
  * seren_gpu_upload and one seren_gpu_force_step first.  Not a reference
  * entry point: it replaces sph_advance's per-particle loop for one level. */
 int seren_gpu_rk2_step(seren_gpu_ctx* ctx, double dt);
+/* Block timesteps (nlevels > 1) of the reference's main loop for the
+ * second-order Runge-Kutta scheme, on the device-resident particles
+ * (sph_sim/sph_integrate.F90:27-136).  seren_gpu_block_start, after
+ * seren_gpu_upload and a first seren_gpu_force_step (the setup evaluation of
+ * every particle), takes that state as the start of every particle's step
+ * (initialize_sph_variables_2.F90:72-73, :157; n = nresync = 0).  Each
+ * seren_gpu_block_step is one call of sph_integrate: tree_update on the
+ * build schedule (seren_gpu_set_build_step), sph_update, thermal, hydro and
+ * gravity for the accdo particles only, sph_timesteps
+ * (sph_sim/sph_timesteps.F90:11-341: resynchronisation at n == nresync,
+ * levels int(INVLOGETWO*log(dt_max/dt)) + 1, one level up at a time when
+ * synchronised, integer times rescaled when level_max changes),
+ * check_neighbour_timesteps (timestep/check_neighbour_timesteps.F90:11-85),
+ * advance_runge_kutta for every particle (advance/advance_runge_kutta.F90:
+ * 9-111) and, with check_neib = 2, reduce_timesteps
+ * (timestep/reduce_timesteps.F90, reduce_particle_timestep.F90).  The
+ * per-particle level state stays on the device in tree order and follows
+ * every build, with a and gpot.  Timesteps are timestep_size.F90's (as
+ * seren_gpu_timestep).  Moving sinks, accretion and sink search are refused
+ * while block timesteps are on; a new upload turns them off. */
+typedef struct {
+  int32_t nlevels;      /* timestep levels, 1..24 (setup/default_parameters.F90:66)       */
+  int32_t level_mode;   /* 0 free, 1 RESTRICTED_TIMESTEP_LEVELS (the reference's default:
+                           dt_min = dt_fixed/2^k), 2 FIXED_TIMESTEP_LEVELS                 */
+  int32_t check_neib;   /* CHECK_NEIB_TIMESTEP: 0 none, 1 CHECK_NEIGHBOUR_TIMESTEPS (the
+                           default), 2 with IMMEDIATE_TIMESTEP_REDUCTION                   */
+  int32_t reserved;     /* 0 */
+  double dt_fixed;      /* setup/default_parameters.F90:67                                 */
+  double courant_mult;  /* timestep_size.F90 multipliers                                   */
+  double accel_mult;
+} seren_gpu_block_params;
+/* The time_module scalars after a step (sph_timesteps.F90 state). */
+typedef struct {
+  int64_t n;            /* integer time after the step                                  */
+  int64_t nresync;      /* integer time of the next resynchronisation                    */
+  int64_t nsteps;
+  int32_t level_max;
+  int32_t level_step;
+  int32_t nactive;      /* particles whose forces this step evaluated                    */
+  int32_t reserved;
+  double timestep;      /* length of one integer step                                    */
+  double dt_max;
+  double time;
+} seren_gpu_block_state;
+int seren_gpu_block_start(seren_gpu_ctx* ctx, const seren_gpu_block_params* prm);
+int seren_gpu_block_step(seren_gpu_ctx* ctx, seren_gpu_block_state* out);
+/* Per-particle block state in tree order (any pointer may be NULL): level,
+ * integer time of the start of the current step, least neighbour level, accdo. */
+int seren_gpu_block_levels(seren_gpu_ctx* ctx, int32_t* nlevel, int64_t* nlast,
+                           int32_t* nminneib, int32_t* accdo);
+
 /* Sinks that seren_gpu_rk2_step moves with the gas (sinks/advance_sink_RK.F90:
  * 22-51, same step; their accelerations are sph_sink_forces.F90:49-110 on each
  * step's trees): velocities [nsink][3] and radii for the sinks last given to

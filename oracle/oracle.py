@@ -411,6 +411,240 @@ def rk2_full(r_old, v_old, v_half, a_half, dt):
     return r_old + v_half * dt, v_old + a_half * dt
 
 
+INVLOGETWO = 1.442695041              # headers/macros.h:15
+TIMESTEP_LEVEL_DIFF_MAX = 2           # headers/macros.h:185
+
+
+def _level(dt_max, dt):
+    """int(INVLOGETWO*log(dt_max/dt)) + 1 (sph_timesteps.F90:105, :169) with
+    libm's log and Fortran's truncation toward zero."""
+    return int(INVLOGETWO * math.log(dt_max / dt)) + 1
+
+
+class BlockSteps:
+    """Block timesteps of the reference's main loop for the second-order
+    Runge-Kutta scheme with the isothermal grad-h force path
+    (sph_sim/sph_integrate.F90:27-136): per call, tree_update on its build
+    schedule, the forces of the accdo particles (sph_update, thermal, hydro,
+    gravity), sph_timesteps (sph_sim/sph_timesteps.F90:11-341),
+    check_neighbour_timesteps (timestep/check_neighbour_timesteps.F90:11-85),
+    advance_runge_kutta for every particle (advance/advance_runge_kutta.F90:
+    9-111) and, with IMMEDIATE_TIMESTEP_REDUCTION, reduce_timesteps
+    (timestep/reduce_timesteps.F90, reduce_particle_timestep.F90).  The forces
+    come from `hp` (the C++ oracle); every per-particle array is kept in its
+    tree order and permuted at each build, as reorder_particle_arrays does.
+    level_mode: 0 free, 1 RESTRICTED_TIMESTEP_LEVELS, 2 FIXED_TIMESTEP_LEVELS;
+    check_neib: the CHECK_NEIB_TIMESTEP option (0, 1 or 2).  No sinks."""
+
+    def __init__(self, hp, ic, nlevels=3, level_mode=1, check_neib=1, dt_fixed=1.0,
+                 courant_mult=0.2, accel_mult=0.5, nbuildstep=1):
+        self.hp, self.alpha = hp, float(ic["alpha"])
+        self.nlevels, self.level_mode, self.check_neib = int(nlevels), int(level_mode), int(check_neib)
+        self.dt_fixed, self.courant, self.accel = float(dt_fixed), float(courant_mult), float(accel_mult)
+        self.nbuildstep = int(nbuildstep)
+        # sph_setup: the first evaluation of every particle
+        p, perm = hp.tree_update(ic["parray"])
+        v = np.ascontiguousarray(ic["v"][perm], dtype=np.float64)
+        self.csq = np.ascontiguousarray(ic["sound"][perm] ** 2, dtype=np.float64)
+        s = hp.sph_update(p, v, first_call=True)
+        self.perm = perm.astype(np.int64)
+        self.parray, self.v = s["parray"], v
+        self.rho, self.omega, self.div_v = s["rho"], s["omega"], s["div_v"]
+        self._forces(None)
+        n = p.shape[0]
+        # initialize_sph_variables_2.F90:72-73, :157; initialize_seren_variables_2.F90:60-61
+        self.r_old, self.v_old = self.parray[:, 0:3].copy(), self.v.copy()
+        self.v_half = np.zeros((n, 3))
+        self.accdo = np.zeros(n, bool)
+        self.nlast = np.zeros(n, np.int64)
+        self.nlevel = np.zeros(n, np.int64)
+        self.nminneib = np.zeros(n, np.int64)
+        self.laststep = np.zeros(n)
+        self.n = self.nresync = self.nsteps = 0
+        self.level_max = self.level_step = 0
+        self.timestep = self.dt_max = self.time = 0.0
+        self.since_build = 1
+        self.nactive = n
+
+    def _forces(self, act):
+        """thermal (sph/thermal.F90:52-59: press = c_s^2 rho, sound = sqrt(press/rho)),
+        hydro and gravity for the particles act (None: all)."""
+        hp = self.hp
+        press = self.csq * self.rho
+        self.press, self.sound = press, np.sqrt(press / self.rho)
+        a_h = hp.hydro_forces(press, self.sound, acclist=act)
+        a, gpot = hp.grav_forces(a_h, acclist=act)
+        if act is None:
+            self.a, self.gpot = a, gpot
+        else:
+            self.a[act], self.gpot[act] = a[act], gpot[act]
+
+    def _permute(self, perm):
+        for k in ("parray", "v", "csq", "rho", "omega", "div_v", "a", "gpot", "r_old", "v_old",
+                  "v_half", "accdo", "nlast", "nlevel", "nminneib", "laststep"):
+            setattr(self, k, getattr(self, k)[perm])
+        self.perm = self.perm[perm]
+
+    def step(self):
+        hp = self.hp
+        build = self.since_build >= self.nbuildstep               # main/tree_update.F90
+        p, perm = hp.tree_update(self.parray, do_build=build)
+        if build:
+            self._permute(perm.astype(np.int64))
+            self.since_build = 0
+        self.since_build += 1
+        self.parray[:, 0:3] = p[:, 0:3]
+        act = np.nonzero(self.accdo)[0].astype(np.int32)
+        self.nactive = int(act.size)
+        lists = None
+        if act.size:                                               # sph_integrate.F90:36-66
+            s = hp.sph_update(self.parray, self.v, acclist=act)
+            self.parray[act, 4:6] = s["parray"][act, 4:6]
+            for k in ("rho", "omega", "div_v"):
+                getattr(self, k)[act] = s[k][act]
+            lists = (s["pptot"], s["pplist"])
+            self._forces(act)
+        self._timesteps()
+        if self.check_neib >= 1 and act.size:
+            self._check_neighbours(act, lists)
+        self._advance()
+        if self.check_neib == 2:
+            self._reduce()
+
+    def _timesteps(self):
+        """sph_sim/sph_timesteps.F90:11-341 (no sinks)."""
+        dt_all = timestep_sizes(self.parray[:, 4], self.a, self.div_v, self.sound, self.alpha,
+                                self.courant, self.accel)
+        n_p = len(dt_all)
+        if self.n == self.nresync:                                 # :47-147
+            self.n = 0
+            self.nlast[:] = 0
+            dt_min = float(dt_all.min())
+            level_max = self.nlevels - 1
+            if self.level_mode == 1:
+                level = _level(self.dt_fixed, dt_min)
+                dt_min = self.dt_fixed / 2.0 ** level
+            elif self.level_mode == 2:
+                dt_min = self.dt_fixed / 2.0 ** level_max
+            dt_max = dt_min * 2.0 ** level_max
+            for p in range(n_p):
+                lev = max(min(_level(dt_max, float(dt_all[p])), level_max), 0)
+                self.nlevel[p] = lev
+                if self.check_neib >= 1:
+                    self.nminneib[p] = lev
+            self.level_max, self.dt_max = level_max, dt_max
+            self.level_step = level_max + 1
+            self.nresync = 2 ** self.level_step
+            self.timestep = dt_max / float(self.nresync)
+        else:                                                      # :152-296
+            level_old = self.level_max
+            n, level_step = self.n, self.level_step
+            p_update = 0
+            for p in range(n_p):
+                if n == self.nlast[p]:
+                    p_update += 1
+                    last = int(self.nlevel[p])
+                    level = max(_level(self.dt_max, float(dt_all[p])), 0)
+                    if level < last and last > 1 and n % 2 ** (level_step - (last - 1)) == 0:
+                        self.nlevel[p] = last - 1
+                    elif level > last:
+                        self.nlevel[p] = level
+                    else:
+                        self.nlevel[p] = last
+            if p_update > 0:
+                level_max = int(self.nlevel.max())
+                if level_max <= level_old - 1 and level_old > 1 and \
+                        n % 2 ** (level_step - (level_old - 1)) == 0:
+                    level_max = level_old - 1
+                elif level_max < level_old:
+                    level_max = level_old
+                if self.check_neib >= 1:                           # :236-249
+                    D = TIMESTEP_LEVEL_DIFF_MAX
+                    for p in range(n_p):
+                        self.nminneib[p] = min(int(self.nminneib[p]), level_max)
+                        mn, lv = int(self.nminneib[p]), int(self.nlevel[p])
+                        if mn - lv > D and self.nlast[p] == n and \
+                                n % 2 ** (level_step - mn + D) == 0:
+                            self.nlevel[p] = min(mn - D, level_max)
+                            self.nminneib[p] = self.nlevel[p]
+                        elif self.nlast[p] == n:
+                            self.nminneib[p] = lv
+                if level_max > level_old:                          # :259-273
+                    f = 2 ** (level_max - level_old)
+                    self.nlast *= f
+                    self.n *= f
+                    self.nresync *= f
+                elif level_max < level_old:
+                    f = 2 ** (level_old - level_max)
+                    self.nlast //= f
+                    self.n //= f
+                    self.nresync //= f
+                self.level_max = level_max
+                self.level_step = level_max + 1
+                self.timestep = self.dt_max / float(self.nresync)
+        self.n += 1                                                # :333-336
+        self.nsteps += 1
+        self.time += self.timestep
+
+    def _check_neighbours(self, act, lists):
+        """timestep/check_neighbour_timesteps.F90:41-68: every active
+        particle's level reaches its neighbours' nminneib (list of get_neib,
+        or the same test on the fly when it overflowed)."""
+        pptot, pplist = lists
+        L = self.hp.params.pp_limit
+        x, h = self.parray[:, 0:3], self.parray[:, 4]
+        for p in act:
+            lev = int(self.nlevel[p])
+            if pptot[p] <= L:
+                neib = pplist[p, :pptot[p]] - self.hp.params.index_base
+            else:                                                  # get_neib_on_fly
+                d = x - x[p]
+                r2 = (d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2]
+                ok = (r2 <= (4.0 * h[p]) * h[p]) | (r2 <= (4.0 * h) * h)
+                ok[p] = False
+                neib = np.nonzero(ok)[0]
+            for pp in neib:
+                if lev > self.nminneib[pp] and self.nminneib[pp] != -1:
+                    self.nminneib[pp] = lev
+
+    def _advance(self):
+        """advance/advance_runge_kutta.F90:20-97 for every particle."""
+        dn = self.n - self.nlast
+        nfull = 2 ** (self.level_step - self.nlevel)
+        nhalf = nfull // 2
+        dt = (self.timestep * dn.astype(np.float64))[:, None]
+        first = dn <= nhalf
+        rp = np.where(first[:, None], self.r_old + self.v_old * dt, self.r_old + self.v_half * dt)
+        vp = self.v_old + self.a * dt
+        half = first & (dn == nhalf)
+        self.v_half[half] = vp[half]
+        full = dn == nfull
+        self.accdo = half | full
+        self.parray[:, 0:3] = rp
+        self.v = vp
+        self.nlast[full] = self.n
+        self.laststep[full] = self.timestep * nfull[full].astype(np.float64)
+        self.r_old[full] = rp[full]
+        self.v_old[full] = vp[full]
+
+    def _reduce(self):
+        """timestep/reduce_timesteps.F90:20-40 with reduce_particle_timestep.F90."""
+        D = TIMESTEP_LEVEL_DIFF_MAX
+        if np.any(self.nminneib > self.level_max):
+            raise RuntimeError("Problem with nminneib > level_max")
+        for p in range(len(self.nlevel)):
+            mn = int(self.nminneib[p])
+            if mn - int(self.nlevel[p]) > D and mn != -1 and self.nlast[p] != self.n and \
+                    self.n % 2 ** (self.level_step - mn + D) == 0:
+                self.r_old[p] = self.parray[p, 0:3]
+                self.v_old[p] = self.v[p]
+                self.laststep[p] = self.timestep * float(self.n - self.nlast[p])
+                self.nlevel[p] = mn - D
+                self.nlast[p] = self.n
+                self.nminneib[p] = mn - D
+                self.accdo[p] = True
+
+
 class Oracle(HotPath):
     def __init__(self, pmax: int, params: Params):
         super().__init__(library(), "seren_oracle", pmax, params)

@@ -245,6 +245,7 @@ int check_tree(Ctx& c, int32_t ptot) {
 }
 
 void free_all(Ctx& c) {
+  block_free(c);
   void* ps[] = {c.pm, c.hz, c.vel, c.csq, c.orig, c.pm_alt, c.hz_alt, c.vel_alt, c.csq_alt,
                 c.orig_alt, c.rho, c.omega, c.div_v, c.drhodt, c.rho_alt, c.omega_alt, c.div_v_alt,
                 c.drhodt_alt, c.press, c.sound, c.acc, c.gpot,
@@ -342,6 +343,7 @@ int alloc_all(Ctx& c) {
 // new particle set: identity order, clear per-particle state
 void reset_particles(Ctx& c, int ptot) {
   c.ptot = ptot;
+  c.blk.on = false;                          // block timesteps start again after a new upload
   c.have_tree = c.have_sph = c.have_v = c.have_csq = false;
   k_iota<<<nb(ptot, 256), 256, 0, c.st>>>(c.orig, ptot); ++c.nlaunch;
   cudaMemsetAsync(c.vel, 0, sizeof(double4) * ptot, c.st);
@@ -773,7 +775,7 @@ struct IoPlan {
 // stream once the stage that makes it has run: v, c_s^2 and the permutation
 // after the tree build, parray (h), rho and omega after grad-h; a and gpot
 // follow gravity on the compute stream.
-int force_step_body(Ctx& c, int first_call, const IoPlan* io) {
+int force_step_body(Ctx& c, int first_call, const IoPlan* io, bool block = false) {
   const int n = c.ptot;
   const size_t N = (size_t)n;
   c.act = nullptr;
@@ -796,6 +798,10 @@ int force_step_body(Ctx& c, int first_call, const IoPlan* io) {
     if (rebuilt) c.since_build = 0;
   }
   ++c.since_build;
+  // block timesteps: the forces of the accdo particles only (in tree order,
+  // listed after the build's reorder)
+  int nact = n;
+  if (block && (rc = block_active(c, nact))) return rc;
   cudaEventRecord(c.ev[1], c.st);
   if (io) {
     // v and c_s^2 come in on the copy stream while the grad-h walk runs (the
@@ -808,7 +814,7 @@ int force_step_body(Ctx& c, int first_call, const IoPlan* io) {
     if (io->perm) cudaMemcpyAsync(io->perm, c.orig, sizeof(int) * N, cudaMemcpyDeviceToHost, c.st_io);
   }
   if (first_call) launch_hguess(c);
-  launch_gradh(c, n);                         // runs finish_reorder before its passes
+  launch_gradh(c, nact);                      // runs finish_reorder before its passes
   finish_reorder(c);
   cudaEventRecord(c.ev[2], c.st);
   if (io) {
@@ -828,16 +834,16 @@ int force_step_body(Ctx& c, int first_call, const IoPlan* io) {
       cudaMemcpyAsync(io->omega, c.omega, sizeof(double) * N, cudaMemcpyDeviceToHost, c.st_io);
   }
   launch_update_hmax(c);
-  launch_neib(c, n);
+  launch_neib(c, nact);
   cudaEventRecord(c.ev[3], c.st);
   launch_thermal(c);
-  launch_hydro(c, n);
+  launch_hydro(c, nact);
   cudaEventRecord(c.ev[4], c.st);
   // a and gpot go straight to mapped (pinned) host buffers from the gravity
   // kernel, else they are copied after it
   double* amap = io ? mapped_host(io->a) : nullptr;
   double* gmap = io ? mapped_host(io->gpot) : nullptr;
-  launch_grav(c, n, c.nsink, c.nsink > 0 ? c.sinks : nullptr, amap, gmap);
+  launch_grav(c, nact, c.nsink, c.nsink > 0 ? c.sinks : nullptr, amap, gmap);
   cudaEventRecord(c.ev[5], c.st);
   if (io) {
     if (io->a && !amap)
@@ -999,6 +1005,7 @@ int seren_gpu_set_sink_motion(seren_gpu_ctx* h, int32_t nsink, const double* sin
                               const double* sink_radius) {
   if (!h) return SEREN_GPU_ERR_ARG;
   Ctx& c = h->c;
+  if (c.blk.on) return fail(c, SEREN_GPU_ERR_STATE, "set_sink_motion: not available with block timesteps");
   if (nsink < 1 || nsink != c.nsink || !sink_v || !sink_radius)
     return fail(c, SEREN_GPU_ERR_ARG, "set_sink_motion: nsink as in seren_gpu_set_sinks, arrays given");
   c.sink_v.assign(sink_v, sink_v + 3 * (size_t)nsink);
@@ -1097,17 +1104,8 @@ int seren_gpu_rk2_step(seren_gpu_ctx* h, double dt) {
   if (!(dt > 0.0) || !std::isfinite(dt)) return fail(c, SEREN_GPU_ERR_ARG, "rk2_step: dt not positive");
   if (!c.have_v || !c.have_csq || !c.have_sph || c.ptot < 1)
     return fail(c, SEREN_GPU_ERR_STATE, "rk2_step: call seren_gpu_upload and seren_gpu_force_step first");
-  if (!c.r_old) {
-    const size_t P = (size_t)c.pmax;
-    for (double4** p : {&c.r_old, &c.v_old, &c.v_half, &c.r_old_alt, &c.v_old_alt, &c.v_half_alt})
-      if (cudaMalloc(p, sizeof(double4) * P) != cudaSuccess) {
-        *p = nullptr;
-        cudaGetLastError();
-        for (double4** q : {&c.r_old, &c.v_old, &c.v_half, &c.r_old_alt, &c.v_old_alt, &c.v_half_alt})
-          if (*q) { cudaFree(*q); *q = nullptr; }
-        return fail(c, SEREN_GPU_ERR_CUDA, "rk2_step: state allocation failed");
-      }
-  }
+  if (c.blk.on) return fail(c, SEREN_GPU_ERR_STATE, "rk2_step: block timesteps are on (upload again)");
+  if (seren::rk_alloc(c)) return fail(c, SEREN_GPU_ERR_CUDA, "rk2_step: state allocation failed");
   const int n = c.ptot;
   c.nlaunch = 0;
   // sinks set in motion move with the same scheme (sinks/advance_sink_RK.F90:22-51)
@@ -1154,11 +1152,77 @@ int seren_gpu_rk2_step(seren_gpu_ctx* h, double dt) {
   return sinks ? seren::sink_accels(c) : SEREN_GPU_OK;
 }
 
+int seren_gpu_block_start(seren_gpu_ctx* h, const seren_gpu_block_params* prm) {
+  if (!h) return SEREN_GPU_ERR_ARG;
+  Ctx& c = h->c;
+  if (!prm || prm->nlevels < 1 || prm->nlevels > 24 || prm->level_mode < 0 ||
+      prm->level_mode > 2 || prm->check_neib < 0 || prm->check_neib > 2 ||
+      !(prm->dt_fixed > 0.0) || !(prm->courant_mult > 0.0) || !(prm->accel_mult > 0.0))
+    return fail(c, SEREN_GPU_ERR_ARG, "block_start: bad parameters");
+  if (!c.have_v || !c.have_csq || !c.have_sph || c.ptot < 1)
+    return fail(c, SEREN_GPU_ERR_STATE, "block_start: call seren_gpu_upload and seren_gpu_force_step first");
+  if (c.sink_move) return fail(c, SEREN_GPU_ERR_ARG, "block_start: moving sinks are not supported");
+  c.nlaunch = 0;
+  seren::BlockState& b = c.blk;
+  b.nlevels = prm->nlevels;
+  b.level_mode = prm->level_mode;
+  b.check_neib = prm->check_neib;
+  b.dt_fixed = prm->dt_fixed;
+  b.courant = prm->courant_mult;
+  b.accel = prm->accel_mult;
+  int rc = seren::block_start(c);
+  if (rc) return fail(c, rc, "block_start: state allocation failed");
+  return finish(c, "block_start");
+}
+
+int seren_gpu_block_step(seren_gpu_ctx* h, seren_gpu_block_state* out) {
+  if (!h) return SEREN_GPU_ERR_ARG;
+  Ctx& c = h->c;
+  if (!c.blk.on) return fail(c, SEREN_GPU_ERR_STATE, "block_step: call seren_gpu_block_start first");
+  c.nlaunch = 0;
+  int rc = seren::force_step_body(c, 0, nullptr, true);      // sph_integrate.F90:36-66
+  if (rc) return rc;
+  rc = seren::block_after_forces(c);                         // :79-113
+  if (rc) return fail(c, rc, "block_step: device result read failed");
+  rc = finish(c, "block_step");
+  if (rc) return rc;
+  c.step_launches = c.nlaunch;
+  if (out) {
+    const seren::BlockState& b = c.blk;
+    out->n = b.n;
+    out->nresync = b.nresync;
+    out->nsteps = b.nsteps;
+    out->level_max = b.level_max;
+    out->level_step = b.level_step;
+    out->nactive = b.nactive;
+    out->reserved = 0;
+    out->timestep = b.timestep;
+    out->dt_max = b.dt_max;
+    out->time = b.time;
+  }
+  return SEREN_GPU_OK;
+}
+
+int seren_gpu_block_levels(seren_gpu_ctx* h, int32_t* nlevel, int64_t* nlast, int32_t* nminneib,
+                           int32_t* accdo) {
+  if (!h) return SEREN_GPU_ERR_ARG;
+  Ctx& c = h->c;
+  if (!c.blk.on) return fail(c, SEREN_GPU_ERR_STATE, "block_levels: block timesteps are off");
+  const size_t N = (size_t)c.ptot;
+  const seren::BlockState& b = c.blk;
+  if (nlevel) cudaMemcpyAsync(nlevel, b.nlevel, sizeof(int) * N, cudaMemcpyDeviceToHost, c.st);
+  if (nlast) cudaMemcpyAsync(nlast, b.nlast, sizeof(long long) * N, cudaMemcpyDeviceToHost, c.st);
+  if (nminneib) cudaMemcpyAsync(nminneib, b.nminneib, sizeof(int) * N, cudaMemcpyDeviceToHost, c.st);
+  if (accdo) cudaMemcpyAsync(accdo, b.accdo, sizeof(int) * N, cudaMemcpyDeviceToHost, c.st);
+  return finish(c, "block_levels");
+}
+
 int seren_gpu_accrete(seren_gpu_ctx* h, int32_t nsink, const int32_t* accrete,
                       int32_t energy_accrete, double* sink_angmom, int32_t* naccreted,
                       int32_t* ptot_out) {
   if (!h) return SEREN_GPU_ERR_ARG;
   Ctx& c = h->c;
+  if (c.blk.on) return fail(c, SEREN_GPU_ERR_STATE, "accrete: not available with block timesteps");
   if (nsink < 1 || nsink != c.nsink)
     return fail(c, SEREN_GPU_ERR_ARG, "accrete: nsink as in seren_gpu_set_sinks");
   if (!c.sink_move)
@@ -1216,6 +1280,7 @@ int seren_gpu_sink_search(seren_gpu_ctx* h, const seren_gpu_sink_search_params* 
                           int32_t* nremoved, int32_t* ptot_out) {
   if (!h) return SEREN_GPU_ERR_ARG;
   Ctx& c = h->c;
+  if (c.blk.on) return fail(c, SEREN_GPU_ERR_STATE, "sink_search: not available with block timesteps");
   if (!prm || !(prm->sinkrad > 0.0))
     return fail(c, SEREN_GPU_ERR_ARG, "sink_search: parameters with sinkrad > 0");
   if (!c.have_tree || !c.have_v || !c.have_sph || c.ptot < 1)

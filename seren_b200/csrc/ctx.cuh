@@ -17,6 +17,35 @@ struct ScanScratch {
   int* total = nullptr;  // device int: total of the last scan
 };
 
+// Block timesteps of the device-resident step loop (blockstep.cu): the
+// scalars of the reference's time_module on the host, the per-particle level
+// state in tree order on the device (permuted at every build, as
+// reorder_particle_arrays does).
+struct BlockState {
+  bool on = false;
+  int nlevels = 1;
+  int level_mode = 1;        // 0 free, 1 RESTRICTED_TIMESTEP_LEVELS, 2 FIXED_TIMESTEP_LEVELS
+  int check_neib = 1;        // CHECK_NEIB_TIMESTEP: 0, 1 or 2
+  double dt_fixed = 1.0, courant = 0.2, accel = 0.5;
+  long long n = 0, nresync = 0, nsteps = 0;
+  int level_max = 0, level_step = 0, nactive = 0;
+  double timestep = 0.0, dt_max = 0.0, time = 0.0;
+  int* nlevel = nullptr;
+  long long* nlast = nullptr;
+  int* nminneib = nullptr;
+  int* accdo = nullptr;
+  double* laststep = nullptr;
+  int* nlevel_alt = nullptr;
+  long long* nlast_alt = nullptr;
+  int* nminneib_alt = nullptr;
+  int* accdo_alt = nullptr;
+  double* laststep_alt = nullptr;
+  double* acc_alt = nullptr;             // a and gpot follow the particles in block mode
+  double* gpot_alt = nullptr;
+  double* dt = nullptr;                  // per-particle timestep_size
+  unsigned long long* red = nullptr;     // [4] reduction words
+};
+
 struct Ctx {
   seren_gpu_params prm{};
   int64_t pmax = 0;
@@ -159,6 +188,8 @@ struct Ctx {
   double* acc_out = nullptr;
   int* acc_ws = nullptr;
 
+  BlockState blk;
+
   // build schedule of the device-resident force steps (main/tree_update.F90:
   // build every nbuildstep evaluations, restock in between)
   int nbuildstep = 1;
@@ -204,6 +235,14 @@ void launch_hguess(Ctx& c);           // BHhydro_hguess
 void scan_exclusive(Ctx& c, const int* in, int* out, int n);   // total -> c.scan.total
 int scan_scratch_alloc(ScanScratch& s, int nmax);
 
+// blockstep.cu
+void reorder_block(Ctx& c);           // the block state follows a build's permutation
+int block_active(Ctx& c, int& nact);  // c.act = the accdo particles (tree order)
+int block_start(Ctx& c);              // state after a first force step of every particle
+int block_after_forces(Ctx& c);       // sph_timesteps, neighbour checks, advance, reduction
+void block_free(Ctx& c);
+int rk_alloc(Ctx& c);                 // r_old, v_old, v_half (and their reorder targets)
+
 // sph.cu
 void launch_gradh(Ctx& c, int nact);
 void launch_hgather(Ctx& c, int nact);  // h_gather (standard SPH)
@@ -212,6 +251,9 @@ void launch_hydro(Ctx& c, int nact, double* amap = nullptr);   // amap: mapped h
 void launch_thermal(Ctx& c);
 int hydro_walk_slots(const Ctx& c);     // resident warps of the grad-h / neighbour grids
 int wide_scratch_alloc(Ctx& c);         // c.wst, c.wacc; 0 or -1
+// check_neighbour_timesteps: every active particle's level reaches the
+// nminneib of its neighbours (its list, or the same test on the fly)
+void launch_neib_levels(Ctx& c, int nact, const int* nlevel, int* nminneib);
 
 // gravity.cu
 // amap/gmap (optional): host buffers mapped into the device address space

@@ -1102,6 +1102,45 @@ __global__ void __launch_bounds__(HG_THREADS) k_hgather(
   }
 }
 
+// timestep/check_neighbour_timesteps.F90:41-68, thread per active particle:
+// its level reaches the nminneib of each neighbour on its list (get_neib's
+// pptot/pplist of this step) or, for an overflowed list, of each particle that
+// passes get_neib_on_fly's test.  The reference raises nminneib(pp) to levelp
+// when it is larger, never touching -1 entries; that is a maximum over the
+// active neighbours, the same in any order.
+__global__ void k_neib_levels(int nact, const int* __restrict__ act, const double4* __restrict__ pm,
+                              const double2* __restrict__ hz, HydroTree t,
+                              const int* __restrict__ pptot, const int* __restrict__ pplist, int L,
+                              const int* __restrict__ nlevel, int* __restrict__ nminneib,
+                              DevError* err) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nact) return;
+  const int p = act ? act[i] : i;
+  const int lev = nlevel[p];
+  auto raise = [&](int pp) {
+    const int cur = nminneib[pp];
+    if (cur != -1 && lev > cur) atomicMax(nminneib + pp, lev);
+  };
+  const int nn = pptot[p];
+  if (nn <= L) {
+    const int* row = pplist + (size_t)p * L;
+    for (int k = 0; k < nn; ++k) raise(row[k]);
+    return;
+  }
+  const double4 P = pm[p];
+  const double hp = hz[p].x;
+  const double hsp = (KERNRANGESQD * hp) * hp;
+  walk_gather_scatter(t, P.x, P.y, P.z, KERNRANGE * hp, err, p, [&](int q) {
+    if (q == p) return;
+    const double hq = hz[q].x;
+    const double hsq = (KERNRANGESQD * hq) * hq;
+    const double4 Q = pm[q];
+    const double d0 = Q.x - P.x, d1 = Q.y - P.y, d2 = Q.z - P.z;
+    const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
+    if (drsqd <= hsp || drsqd <= hsq) raise(q);
+  });
+}
+
 // sum over the block, the same value on every thread
 __device__ double block_sum(double v, double* sh) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -1906,6 +1945,14 @@ void launch_hgather(Ctx& c, int nact) {
   k_hgather<<<std::max(1, (c.wstack_slots / 3) / HG_WARPS), HG_THREADS, 0, c.st>>>(
       nact, c.act, c.pm, c.hz, hydro_tree(c), c.prm.pp_gather, c.info.rextent,
       reinterpret_cast<int*>(c.wstack), 2 * c.wstack_cap, c.d_err, counts);
+  ++c.nlaunch;
+}
+
+void launch_neib_levels(Ctx& c, int nact, const int* nlevel, int* nminneib) {
+  if (nact <= 0) return;
+  k_neib_levels<<<nb(nact, 128), 128, 0, c.st>>>(nact, c.act, c.pm, c.hz, hydro_tree(c), c.pptot,
+                                                 c.pplist, c.prm.pp_limit, nlevel, nminneib,
+                                                 c.d_err);
   ++c.nlaunch;
 }
 

@@ -882,6 +882,7 @@ int build_tree(Ctx& c) {
     std::swap(c.v_old, c.v_old_alt);
     std::swap(c.v_half, c.v_half_alt);
   }
+  if (c.blk.on) reorder_block(c);           // block-timestep state, a and gpot too
   k_pack_link<<<nb(ctot + 1, 256), 256, 0, c.st>>>(ctot, c.leaf, c.nextcell, c.ifopen, c.pstart,
                                                    c.link); ++c.nlaunch;
   static_assert(sizeof(TreeInfo) % 4 == 0 && sizeof(TreeInfo) <= 1024, "TreeInfo through read_dev");

@@ -48,7 +48,10 @@ def library(build_if_missing: bool = True) -> C.CDLL:
                            ("download", [vp, _dp, _dp, _dp, _dp, _dp, _dp, _ip]),
                            ("last_step_stats", [vp, _dp, _ip, C.POINTER(C.c_int64)]),
                            ("get_stream", [vp, C.POINTER(C.c_void_p)]),
-                           ("fma_peak", [vp, C.c_int32, _dp])):
+                           ("fma_peak", [vp, C.c_int32, _dp]),
+                           ("block_start", [vp, C.c_void_p]),
+                           ("block_step", [vp, C.c_void_p]),
+                           ("block_levels", [vp, _ip, C.POINTER(C.c_int64), _ip, _ip])):
             fn = getattr(lib, f"seren_gpu_{name}")
             fn.argtypes = args
             fn.restype = C.c_int
@@ -62,6 +65,24 @@ class SinkSearchParams(C.Structure):
         (n, C.c_int32) for n in ("hmult_sinkrad", "rho_search", "potmin_search",
                                  "hill_sphere_search", "div_v_search", "div_a_search",
                                  "timescale_search", "reserved")]
+
+
+class BlockParams(C.Structure):
+    """seren_gpu_block_params of include/seren_gpu.h."""
+    _fields_ = [("nlevels", C.c_int32), ("level_mode", C.c_int32), ("check_neib", C.c_int32),
+                ("reserved", C.c_int32), ("dt_fixed", C.c_double), ("courant_mult", C.c_double),
+                ("accel_mult", C.c_double)]
+
+
+class BlockState(C.Structure):
+    """seren_gpu_block_state of include/seren_gpu.h."""
+    _fields_ = [("n", C.c_int64), ("nresync", C.c_int64), ("nsteps", C.c_int64),
+                ("level_max", C.c_int32), ("level_step", C.c_int32), ("nactive", C.c_int32),
+                ("reserved", C.c_int32), ("timestep", C.c_double), ("dt_max", C.c_double),
+                ("time", C.c_double)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_ if n != "reserved"}
 
 
 def _d(a):
@@ -174,6 +195,31 @@ class GpuHotPath(HotPath):
         """Build the tree every nbuildstep device-resident evaluations and
         restock it in between (seren_gpu_set_build_step)."""
         self._call("set_build_step", self._ctx, int(nbuildstep))
+
+    def block_start(self, nlevels=3, level_mode=1, check_neib=1, dt_fixed=1.0,
+                    courant_mult=0.2, accel_mult=0.5):
+        """Block timesteps from the state of the last force step
+        (seren_gpu_block_start)."""
+        prm = BlockParams(int(nlevels), int(level_mode), int(check_neib), 0, float(dt_fixed),
+                          float(courant_mult), float(accel_mult))
+        self._call("block_start", self._ctx, C.cast(C.byref(prm), C.c_void_p))
+
+    def block_step(self) -> dict:
+        """One integer step of the block-timestep loop (seren_gpu_block_step);
+        returns the time scalars after it."""
+        st = BlockState()
+        self._call("block_step", self._ctx, C.cast(C.byref(st), C.c_void_p))
+        return st.as_dict()
+
+    def block_levels(self) -> dict:
+        """Per-particle level state in tree order: nlevel, nlast, nminneib, accdo."""
+        n = self.ptot
+        out = dict(nlevel=np.zeros(n, np.int32), nlast=np.zeros(n, np.int64),
+                   nminneib=np.zeros(n, np.int32), accdo=np.zeros(n, np.int32))
+        self._call("block_levels", self._ctx, out["nlevel"].ctypes.data_as(_ip),
+                   out["nlast"].ctypes.data_as(C.POINTER(C.c_int64)),
+                   out["nminneib"].ctypes.data_as(_ip), out["accdo"].ctypes.data_as(_ip))
+        return out
 
     def drift(self, dt: float):
         self._call("drift", self._ctx, C.c_double(dt))

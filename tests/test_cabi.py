@@ -40,10 +40,11 @@ def test_oracle_mirrors_the_abi():
         if tail in ("upload", "force_step", "force_step_io", "drift", "download",
                     "last_step_stats", "get_stream", "fma_peak", "hydro_forces_noalloc",
                     "set_sinks", "timestep", "rk2_step", "set_sink_motion", "get_sinks",
-                    "sink_timestep", "accrete", "sink_search", "set_build_step"):
-            continue          # device-resident path (timestep / rk2 / accretion: Python
-                              # restatements in oracle.py), device-buffer call, GPU-only
-                              # introspection
+                    "sink_timestep", "accrete", "sink_search", "set_build_step",
+                    "block_start", "block_step", "block_levels"):
+            continue          # device-resident path (timestep / rk2 / accretion / block
+                              # timesteps: Python restatements in oracle.py), device-buffer
+                              # call, GPU-only introspection
         assert hasattr(lib, "seren_oracle_" + tail), tail
 
 

@@ -808,3 +808,47 @@ def test_h_gather_deep_clump_and_too_few_particles(libs):
         with pytest.raises(SerenError) as e:
             hp.h_gather(p)
         assert e.value.code == 5
+
+
+@pytest.mark.parametrize("nlevels,level_mode,check_neib,nbuildstep,nsteps", [
+    (4, 1, 1, 1, 36),        # the reference's default options, a build every step
+    (3, 2, 2, 4, 28),        # fixed levels, immediate reduction, restocks between builds
+])
+def test_block_timesteps_match_oracle(libs, nlevels, level_mode, check_neib, nbuildstep, nsteps):
+    """Block timesteps on the device (seren_gpu_block_step: forces of the
+    accdo particles, sph_timesteps, check_neighbour_timesteps,
+    advance_runge_kutta, reduce_timesteps) against the same loop restated
+    in oracle/oracle.py driving the oracle's force path: after every integer
+    step the particle order, every level, nlast, nminneib and accdo are
+    equal, the time scalars equal, positions within 1e-12 and velocities
+    and accelerations within 1e-9."""
+    from oracle.oracle import BlockSteps
+    ic = case("plummer16k")
+    o, g = _pair(libs, ic)
+    b = BlockSteps(o, ic, nlevels=nlevels, level_mode=level_mode, check_neib=check_neib,
+                   nbuildstep=nbuildstep)
+    g.upload(ic["parray"], ic["v"], ic["sound"] ** 2)
+    g.set_build_step(nbuildstep)
+    g.force_step(first_call=True)
+    g.block_start(nlevels=nlevels, level_mode=level_mode, check_neib=check_neib)
+    seen_levels, seen_active = set(), set()
+    for k in range(nsteps):
+        b.step()
+        st = g.block_step()
+        assert (st["n"], st["nresync"], st["nsteps"], st["level_max"], st["level_step"]) == \
+            (b.n, b.nresync, b.nsteps, b.level_max, b.level_step), k
+        assert st["nactive"] == b.nactive, k
+        assert st["timestep"] == b.timestep and st["time"] == b.time, k
+        d, lv = g.download(), g.block_levels()
+        assert np.array_equal(d["perm"], b.perm), k
+        assert np.array_equal(lv["nlevel"], b.nlevel), k
+        assert np.array_equal(lv["nlast"], b.nlast), k
+        assert np.array_equal(lv["accdo"].astype(bool), b.accdo), k
+        if check_neib:
+            assert np.array_equal(lv["nminneib"], b.nminneib), k
+        assert np.abs(d["parray"][:, 0:3] - b.parray[:, 0:3]).max() < 1e-12, k
+        assert rel_rows(d["v"], b.v).max() < 1e-9, k
+        assert rel_rows(d["a"], b.a).max() < 1e-9, k
+        seen_levels.update(np.unique(b.nlevel).tolist())
+        seen_active.add(b.nactive)
+    assert len(seen_levels) >= 3 and len(seen_active) >= 4     # a real block hierarchy
