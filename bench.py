@@ -276,6 +276,45 @@ def run_rk2(ic, precision, steps, warmup, ws, nbuildstep=1):
                 api="seren_gpu_timestep + seren_gpu_rk2_step (courant 0.2, accel 0.5)")
 
 
+def run_block(ic, precision, steps, warmup, ws, nlevels=3, nbuildstep=1):
+    """Device-resident block timesteps (seren_gpu_block_step: the forces of
+    the accdo particles only, then the reference's level bookkeeping and the
+    Runge-Kutta advance of every particle), nlevels levels with the
+    reference's default options (RESTRICTED levels, CHECK_NEIB_TIMESTEP = 1);
+    integer steps timed with CUDA events on the library's stream after one
+    resynchronisation cycle of warm-up."""
+    import torch
+
+    from seren_b200.gpu import GpuHotPath
+    n = ic["parray"].shape[0]
+    g = GpuHotPath(n, params_for(ic, precision))
+    g.upload(ic["parray"], ic["v"], ic["sound"] ** 2)
+    stream = torch.cuda.ExternalStream(g.stream())
+    g.set_build_step(nbuildstep)
+    g.force_step(first_call=True)
+    g.block_start(nlevels=nlevels)
+    cycle = 2 ** nlevels                      # integer steps between resynchronisations
+    for _ in range(max(warmup, 1) * cycle):
+        g.block_step()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    barrier(ws)
+    start.record(stream)
+    active = 0
+    nsteps = max(steps, 1) * cycle
+    for _ in range(nsteps):
+        active += g.block_step()["nactive"]
+    end.record(stream)
+    torch.cuda.synchronize()
+    barrier(ws)
+    total_ms = max_over_ranks(ws, start.elapsed_time(end))
+    g.close()
+    return dict(ms_per_integer_step=total_ms / nsteps, integer_steps=nsteps, nlevels=nlevels,
+                mean_active_fraction=active / (nsteps * n),
+                value=ws * active / (total_ms * 1e-3), unit="active particle force evals/s",
+                api="seren_gpu_block_step (RESTRICTED levels, CHECK_NEIB_TIMESTEP=1)")
+
+
 def run_e2e_io(ic, precision, steps, warmup, ws):
     """Steps through seren_gpu_force_step_io with pinned host buffers: each
     call copies parray, v and c_s^2 in from the host and parray, v, c_s^2,
@@ -633,12 +672,14 @@ def main():
                    rho_rms_vs_fp64=float(np.sqrt(np.mean(drho ** 2))),
                    rho_max_vs_fp64=float(drho.max()), same_order=bool(same))
         log(f"[bench] fp64: {fp64['ms_per_step']:.2f} ms/step, stages {fp64['stage_ms']}, {acc}")
-    rk2 = rk2_8 = None
+    rk2 = rk2_8 = blk = None
     if args.workload == "core":
         rk2 = run_rk2(ic, 1, args.steps, args.warmup, ws)
         log(f"[bench] rk2 step: {rk2['ms_per_step']:.2f} ms (two force evaluations), dt {rk2['dt']}")
         rk2_8 = run_rk2(ic, 1, args.steps, args.warmup, ws, nbuildstep=8)
         log(f"[bench] rk2 step, build every 8 evaluations: {rk2_8['ms_per_step']:.2f} ms")
+        blk = run_block(ic, 1, 1, 1, ws)
+        log(f"[bench] block timesteps: {blk}")
     e2e = e2e_calls = None
     if not args.no_e2e:
         r = run_e2e_io(ic, 1, args.steps, args.warmup, ws)
@@ -712,6 +753,7 @@ def main():
         "e2e_reference_calls": e2e_calls,
         "rk2_step": rk2,
         "rk2_step_nbuildstep8": rk2_8,
+        "block_timesteps": blk,
         "gpu_launches": mixed["launches"],
         "clocks": clocks,
     }
