@@ -165,6 +165,25 @@ int seren_gpu_timestep(seren_gpu_ctx* ctx, double courant_mult, double accel_mul
  * seren_gpu_upload and one seren_gpu_force_step first.  Not a reference
  * entry point: it replaces sph_advance's per-particle loop for one level. */
 int seren_gpu_rk2_step(seren_gpu_ctx* ctx, double dt);
+/* Many independent clouds in one context (no counterpart in the reference,
+ * which evolves one cloud per run).  After seren_gpu_upload of the clouds'
+ * particles one cloud after another (counts[k] particles each, summing to
+ * ptot), every tree build makes a forest of ncloud trees at once: one sort of
+ * all particles (octant keys from each cloud's own root box, then a stable
+ * pass on the cloud) and one level-by-level split of all clouds' cells, the
+ * roots being cells 0..ncloud-1; the walks, passes, hydro and gravity then
+ * run as single launches over every cloud, each group of 32 particles inside
+ * one cloud (each cloud's particles padded to a multiple of 32) and walking
+ * its own cloud's tree from its own root box.  Every cloud's results equal
+ * those of a context holding that cloud alone, bit for bit.  Particles stay
+ * cloud-major in tree order: cloud k is rows [pstart_k, pstart_k + counts[k])
+ * of seren_gpu_download with pstart_k the sum of the counts before it, and
+ * perm maps them to upload indices.  ncloud = 1 returns to one cloud; a new
+ * upload does too.  Active lists, sinks and block timesteps are refused while
+ * ncloud > 1.  The device-resident force steps build the forest every
+ * evaluation. */
+int seren_gpu_set_clouds(seren_gpu_ctx* ctx, int32_t ncloud, const int32_t* counts);
+
 /* Block timesteps (nlevels > 1) of the reference's main loop for the
  * second-order Runge-Kutta scheme, on the device-resident particles
  * (sph_sim/sph_integrate.F90:27-136).  seren_gpu_block_start, after

@@ -192,6 +192,7 @@ int set_active(Ctx& c, const int32_t* acclist, int32_t nacc, int& nact) {
     nact = c.ptot;
     return SEREN_GPU_OK;
   }
+  if (c.ncloud > 1) return fail(c, SEREN_GPU_ERR_ARG, "no active lists with several clouds");
   if (nacc < 0 || nacc > c.ptot) return fail(c, SEREN_GPU_ERR_ARG, "nacc out of range");
   std::vector<int> a(nacc);
   for (int i = 0; i < nacc; ++i) {
@@ -246,6 +247,8 @@ int check_tree(Ctx& c, int32_t ptot) {
 
 void free_all(Ctx& c) {
   block_free(c);
+  if (c.d_clouds) cudaFree(c.d_clouds);
+  if (c.gact) cudaFree(c.gact);
   void* ps[] = {c.pm, c.hz, c.vel, c.csq, c.orig, c.pm_alt, c.hz_alt, c.vel_alt, c.csq_alt,
                 c.orig_alt, c.rho, c.omega, c.div_v, c.drhodt, c.rho_alt, c.omega_alt, c.div_v_alt,
                 c.drhodt_alt, c.press, c.sound, c.acc, c.gpot,
@@ -344,6 +347,7 @@ int alloc_all(Ctx& c) {
 void reset_particles(Ctx& c, int ptot) {
   c.ptot = ptot;
   c.blk.on = false;                          // block timesteps start again after a new upload
+  c.ncloud = 1;                              // and the particles are one cloud again
   c.have_tree = c.have_sph = c.have_v = c.have_csq = false;
   k_iota<<<nb(ptot, 256), 256, 0, c.st>>>(c.orig, ptot); ++c.nlaunch;
   cudaMemsetAsync(c.vel, 0, sizeof(double4) * ptot, c.st);
@@ -926,6 +930,8 @@ int seren_gpu_set_sinks(seren_gpu_ctx* h, int32_t nsink, const double* sink_rmh)
   Ctx& c = h->c;
   if (nsink < 0 || nsink > 1024 || (nsink > 0 && !sink_rmh))
     return fail(c, SEREN_GPU_ERR_ARG, "set_sinks: 0 <= nsink <= 1024 with sink_rmh given");
+  if (nsink > 0 && c.ncloud > 1)
+    return fail(c, SEREN_GPU_ERR_STATE, "set_sinks: not available with several clouds");
   if (nsink > 0)
     cudaMemcpyAsync(c.sinks, sink_rmh, sizeof(double) * 5 * nsink, cudaMemcpyHostToDevice, c.st);
   c.nsink = nsink;
@@ -1152,6 +1158,53 @@ int seren_gpu_rk2_step(seren_gpu_ctx* h, double dt) {
   return sinks ? seren::sink_accels(c) : SEREN_GPU_OK;
 }
 
+int seren_gpu_set_clouds(seren_gpu_ctx* h, int32_t ncloud, const int32_t* counts) {
+  if (!h) return SEREN_GPU_ERR_ARG;
+  Ctx& c = h->c;
+  if (ncloud < 1 || (ncloud > 1 && !counts)) return fail(c, SEREN_GPU_ERR_ARG, "set_clouds: ncloud < 1 or counts NULL");
+  if (c.ptot < 1) return fail(c, SEREN_GPU_ERR_STATE, "set_clouds: upload the particles first");
+  c.have_tree = false;                               // the next force step builds
+  if (ncloud == 1) {
+    c.ncloud = 1;
+    return SEREN_GPU_OK;
+  }
+  if (c.nsink > 0 || c.blk.on)
+    return fail(c, SEREN_GPU_ERR_STATE, "set_clouds: not available with sinks or block timesteps");
+  std::vector<seren::CloudInfo> cl(ncloud);
+  long long sum = 0;
+  for (int k = 0; k < ncloud; ++k) {
+    if (counts[k] < 1) return fail(c, SEREN_GPU_ERR_ARG, "set_clouds: a cloud without particles");
+    cl[k] = seren::CloudInfo{};
+    cl[k].pstart = (int)sum;
+    cl[k].n = counts[k];
+    cl[k].cell = k;
+    sum += counts[k];
+  }
+  if (sum != c.ptot) return fail(c, SEREN_GPU_ERR_ARG, "set_clouds: counts do not add up to ptot");
+  // the group kernels' list: each cloud's particles, padded to a multiple of 32
+  std::vector<int> gl;
+  gl.reserve((size_t)c.ptot + 32 * (size_t)ncloud);
+  for (int k = 0; k < ncloud; ++k) {
+    for (int i = 0; i < cl[k].n; ++i) gl.push_back(cl[k].pstart + i);
+    while (gl.size() % 32) gl.push_back(-1);
+  }
+  if (c.d_clouds) cudaFree(c.d_clouds);
+  if (c.gact) cudaFree(c.gact);
+  c.d_clouds = nullptr;
+  c.gact = nullptr;
+  if (cudaMalloc(&c.d_clouds, sizeof(seren::CloudInfo) * ncloud) != cudaSuccess ||
+      cudaMalloc(&c.gact, sizeof(int) * gl.size()) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(c, SEREN_GPU_ERR_CUDA, "set_clouds: allocation failed");
+  }
+  cudaMemcpyAsync(c.d_clouds, cl.data(), sizeof(seren::CloudInfo) * ncloud, cudaMemcpyHostToDevice, c.st);
+  cudaMemcpyAsync(c.gact, gl.data(), sizeof(int) * gl.size(), cudaMemcpyHostToDevice, c.st);
+  c.clouds = cl;
+  c.ngact = (int)gl.size();
+  c.ncloud = ncloud;
+  return finish(c, "set_clouds");
+}
+
 int seren_gpu_block_start(seren_gpu_ctx* h, const seren_gpu_block_params* prm) {
   if (!h) return SEREN_GPU_ERR_ARG;
   Ctx& c = h->c;
@@ -1162,6 +1215,7 @@ int seren_gpu_block_start(seren_gpu_ctx* h, const seren_gpu_block_params* prm) {
   if (!c.have_v || !c.have_csq || !c.have_sph || c.ptot < 1)
     return fail(c, SEREN_GPU_ERR_STATE, "block_start: call seren_gpu_upload and seren_gpu_force_step first");
   if (c.sink_move) return fail(c, SEREN_GPU_ERR_ARG, "block_start: moving sinks are not supported");
+  if (c.ncloud > 1) return fail(c, SEREN_GPU_ERR_STATE, "block_start: not available with several clouds");
   c.nlaunch = 0;
   seren::BlockState& b = c.blk;
   b.nlevels = prm->nlevels;

@@ -83,7 +83,33 @@ struct TreeInfo {
   int last_cell[32];
 };
 
-// Kernel table rows (setup/kernel.F90), packed by use:
+// One of several independent clouds sharing a context (seren_gpu_set_clouds).
+// The particles stay cloud-major in every order (upload order, tree order),
+// cloud k holding [pstart, pstart + n); its tree has root cell `cell` (the
+// roots are cells 0..ncloud-1) and its own root box, so each cloud's tree,
+// walks and sums are those of a context holding that cloud alone.
+struct CloudInfo {
+  double root[3];    // root cell centre (BHgrav_build.F90:65-67)
+  double cellsize;   // root half width
+  double rextent;    // largest bounding-box extent (bounding_box.F90)
+  float delta;       // bound on the FP32 rounding of a root-relative coordinate
+  int pstart;
+  int n;
+  int cell;
+};
+
+// the cloud of particle p (cloud-major order): the last k with pstart <= p
+__host__ __device__ __forceinline__ int cloud_of(const CloudInfo* cl, int ncl, int p) {
+  int lo = 0, hi = ncl - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (cl[mid].pstart <= p) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Kernel table rows (setup/kernel.F90), packed by use:// Kernel table rows (setup/kernel.F90), packed by use:
 //   tabA[i] = (w0, wh, w4, wg): grad-h density, omega, div v, zeta
 //   tabG[i] = (w5, w4, w6, w1): gravity softening, potential, hydro gradient
 struct KernelTables {

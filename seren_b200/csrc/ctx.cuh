@@ -190,6 +190,16 @@ struct Ctx {
 
   BlockState blk;
 
+  // independent clouds (seren_gpu_set_clouds): ncloud > 1 makes every tree
+  // build a forest of ncloud trees and the group kernels take gact, the
+  // particles cloud by cloud with each cloud padded (-1) to a multiple of 32,
+  // so that no group of 32 spans two clouds
+  int ncloud = 1;
+  std::vector<CloudInfo> clouds;       // host copy (after a build: roots and extents)
+  CloudInfo* d_clouds = nullptr;
+  int* gact = nullptr;
+  int ngact = 0;
+
   // build schedule of the device-resident force steps (main/tree_update.F90:
   // build every nbuildstep evaluations, restock in between)
   int nbuildstep = 1;

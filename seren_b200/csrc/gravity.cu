@@ -169,6 +169,9 @@ struct GravWalk {
   int ctot;
   int scap;             // stack entries per warp
   double rootx, rooty, rootz;
+  int root;             // root cell of the walks
+  const CloudInfo* cl;  // a forest of ncl trees (NULL: one tree)
+  int ncl;
 };
 
 // gravity_gradh.F90:57-86 in FP32, dr = rpp - rp, invhq precomputed.  The M4
@@ -312,8 +315,18 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
     g = __shfl_sync(FULLMASK, g, 0);
     if ((long long)g * 32 >= nact) break;
     const int i = g * 32 + lane;
-    const bool live = i < nact;
-    const int p = live ? (act ? act[i] : i) : (act ? act[nact - 1] : nact - 1);
+    // act[i] < 0 pads a cloud's last group in a forest; dead lanes take lane
+    // 0's particle (always live)
+    int p = i < nact ? (act ? act[i] : i) : -1;
+    const bool live = p >= 0;
+    p = live ? p : __shfl_sync(FULLMASK, p, 0);
+    if (t.cl) {                                        // the lanes' cloud's tree
+      const CloudInfo& C = t.cl[cloud_of(t.cl, t.ncl, p)];
+      t.root = C.cell;
+      t.rootx = C.root[0];
+      t.rooty = C.root[1];
+      t.rootz = C.root[2];
+    }
     const double4 P = pm[p];
     const double2 HZ = hz[p];
     // warp reference point (lane 0 is always live)
@@ -497,7 +510,7 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
     };
 
     const unsigned rootmask = __ballot_sync(FULLMASK, live);
-    if (lane == 0) S[0] = make_int2(0, (int)rootmask);
+    if (lane == 0) S[0] = make_int2(t.root, (int)rootmask);
     int sp = 1;
     long long gent = 0;
     while (sp > 0) {
@@ -758,17 +771,24 @@ void launch_grav(Ctx& c, int nact, int nsink, const double* d_sinks, double* ama
   if (nact <= 0) return;
   unsigned long long* counts = reinterpret_cast<unsigned long long*>(c.d_counts);
   const GravWalk gw{c.wA, c.gA, c.gB, c.gC, c.info.ctot, c.wstack_cap,
-                    c.info.root[0], c.info.root[1], c.info.root[2]};
+                    c.info.root[0], c.info.root[1], c.info.root[2], 0,
+                    c.ncloud > 1 ? c.d_clouds : nullptr, c.ncloud};
   const bool mixed = c.prm.precision != 0;
+  // in a forest with every particle active the groups follow the clouds
+  const int* gl = c.act;
+  if (!c.act && c.ncloud > 1) {
+    gl = c.gact;
+    nact = c.ngact;
+  }
   const int groups = nb(nact, 32);
   const int blocks = std::min(sm_count(c) * grav_blocks_per_sm(c.dev, mixed), nb(groups, GW_WARPS));
   cudaMemsetAsync(c.work, 0, sizeof(int), c.st);
   if (!mixed)
-    k_grav_walk<false><<<blocks, GW_THREADS, 0, c.st>>>(nact, c.act, c.pm, c.hz, gw, c.tabG,
+    k_grav_walk<false><<<blocks, GW_THREADS, 0, c.st>>>(nact, gl, c.pm, c.hz, gw, c.tabG,
         c.tabG32, c.acc, c.gpot, abase, amap, gmap, nsink, d_sinks, c.wstack, c.work, c.d_err,
         counts);
   else
-    k_grav_walk<true><<<blocks, GW_THREADS, 0, c.st>>>(nact, c.act, c.pm, c.hz, gw, c.tabG,
+    k_grav_walk<true><<<blocks, GW_THREADS, 0, c.st>>>(nact, gl, c.pm, c.hz, gw, c.tabG,
         c.tabG32, c.acc, c.gpot, abase, amap, gmap, nsink, d_sinks, c.wstack, c.work, c.d_err,
         counts);
   ++c.nlaunch;

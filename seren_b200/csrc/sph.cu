@@ -34,14 +34,41 @@ struct HydroTree {
   int ctot;
   double rootx, rooty, rootz;
   float delta;          // bound on the FP32 rounding of a root-relative coordinate
+  int root;             // root cell of the walks
+  double rextent;       // root box extent (the grad-h bisection's first h_upper)
+  const CloudInfo* cl;  // a forest of ncl trees (NULL: one tree)
+  int ncl;
 };
+
+// In a forest, point t at the tree of particle p's cloud: its root cell, root
+// box and rounding bound.  One tree: nothing changes.
+__device__ __forceinline__ void tree_for(HydroTree& t, int p) {
+  if (!t.cl) return;
+  const CloudInfo& C = t.cl[cloud_of(t.cl, t.ncl, p)];
+  t.root = C.cell;
+  t.rootx = C.root[0];
+  t.rooty = C.root[1];
+  t.rootz = C.root[2];
+  t.delta = C.delta;
+  t.rextent = C.rextent;
+}
+
+// Lane i of a group of 32 in an active list: act[i] < 0 pads a cloud's last
+// group in a forest (the groups of each cloud start at its first particle);
+// dead lanes take lane 0's particle (lane 0 is always live).
+__device__ __forceinline__ int group_particle(int i, int nact, const int* act, bool& live) {
+  int p = i < nact ? (act ? act[i] : i) : -1;
+  live = p >= 0;
+  const int p0 = __shfl_sync(0xffffffffu, p, 0);
+  return live ? p : p0;
+}
 
 // BHtree/BHhydro_walk.F90:9-80 (gather or scatter test)
 template <class F>
 __device__ __forceinline__ bool walk_gather_scatter(const HydroTree& t, double rx, double ry,
                                                     double rz, double hrange, DevError* err,
                                                     int who, F&& f) {
-  int c = 0;
+  int c = t.root;
   int visits = 0;
   const int cap = t.ctot + 2;
   while (true) {
@@ -295,7 +322,7 @@ __device__ int gr_walk(const HydroTree& t, unsigned lanes, int2* S, int scap, Gr
                        Test&& test) {
   const unsigned lt = (1u << lane) - 1u;
   __syncwarp();
-  if (lane == 0) S[0] = make_int2(0, (int)lanes);
+  if (lane == 0) S[0] = make_int2(t.root, (int)lanes);
   int sp = 1;
   long long gent = 0;
   while (sp > 0) {
@@ -425,8 +452,9 @@ __global__ void __launch_bounds__(GR_THREADS) k_gradh_walk(
   unsigned nwalk = 0;
   for (int g = gr_next(work, lane); (long long)g * 32 < nact; g = gr_next(work, lane)) {
     const int i = g * 32 + lane;
-    const bool live = i < nact;
-    const int p = live ? (act ? act[i] : i) : (act ? act[nact - 1] : nact - 1);
+    bool live;
+    const int p = group_particle(i, nact, act, live);
+    tree_for(t, p);                                    // lanes share one cloud
     const double4 P = pm[p];
     const double rx = P.x, ry = P.y, rz = P.z;
     const float px = (float)(rx - t.rootx), py = (float)(ry - t.rooty), pz = (float)(rz - t.rootz);
@@ -548,10 +576,10 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
     int nact, const int* __restrict__ act, const double4* __restrict__ pm, double2* __restrict__ hz,
     const double4* __restrict__ vel, double* __restrict__ rho, double* __restrict__ omega,
     double* __restrict__ divv, double* __restrict__ drhodt, const double4* __restrict__ tabA,
-    double h_fac, int pp_gather, double rextent, const int* __restrict__ leaves,
+    double h_fac, int pp_gather, double rextent0, const int* __restrict__ leaves,
     const int* __restrict__ nleaf, const int* __restrict__ npot, int* __restrict__ redo,
     int* __restrict__ nredo, int* __restrict__ prune, int L, DevError* err,
-    unsigned long long* counts, int* work) {
+    unsigned long long* counts, int* work, const CloudInfo* __restrict__ cl, int ncl) {
   __shared__ GpWarp gpw[GP_WARPS];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   GpWarp& W = gpw[w];
@@ -657,8 +685,9 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
 
   for (int g = gr_next(work, lane); (long long)g * 32 < nact; g = gr_next(work, lane)) {
     const int i = g * 32 + lane;
-    const bool live = i < nact;
-    const int p = live ? (act ? act[i] : i) : (act ? act[nact - 1] : nact - 1);
+    bool live;
+    const int p = group_particle(i, nact, act, live);
+    const double rextent = cl ? cl[cloud_of(cl, ncl, p)].rextent : rextent0;
     const int n = live ? nleaf[p] : 0;
     const double4 P = pm[p];
     const double mp = P.w;
@@ -802,7 +831,7 @@ template <class Test>
 __device__ int rd_walk(const HydroTree& t, int lane, int* fa, int* fb, int* leaves, int cap,
                        int& cnt, unsigned long long& nvisit, Test&& test) {
   __syncwarp();
-  if (lane == 0) fa[0] = 0;
+  if (lane == 0) fa[0] = t.root;
   __syncwarp();
   int nf = 1, nleaf = 0, mine = 0;
   while (nf > 0) {
@@ -847,7 +876,7 @@ __global__ void __launch_bounds__(RD_THREADS) k_gradh_redo(
     const int* __restrict__ redo, const int* __restrict__ nredo, const double4* __restrict__ pm,
     double2* __restrict__ hz, const double4* __restrict__ vel, double* __restrict__ rho,
     double* __restrict__ omega, double* __restrict__ divv, double* __restrict__ drhodt,
-    HydroTree t, const double4* __restrict__ tabA, double h_fac, int pp_gather, double rextent,
+    HydroTree t, const double4* __restrict__ tabA, double h_fac, int pp_gather, double rextent0,
     int* __restrict__ scratch, int cap, int* __restrict__ wide, int* __restrict__ nwide,
     DevError* err, unsigned long long* counts) {
   __shared__ int cand_all[RD_WARPS][GP_SEG * LEAFMAX];
@@ -862,6 +891,8 @@ __global__ void __launch_bounds__(RD_THREADS) k_gradh_redo(
   const int nr = *nredo;
   for (int i = gw; i < nr; i += gridDim.x * RD_WARPS) {
     const int p = redo[i];
+    tree_for(t, p);
+    const double rextent = t.cl ? t.rextent : rextent0;
     const double4 P = pm[p];
     const double rx = P.x, ry = P.y, rz = P.z, mp = P.w;
     const float px = (float)(rx - t.rootx), py = (float)(ry - t.rooty), pz = (float)(rz - t.rootz);
@@ -1009,7 +1040,7 @@ __device__ void hg_sort(double* v, int n, int lane) {
 
 __global__ void __launch_bounds__(HG_THREADS) k_hgather(
     int nact, const int* __restrict__ act, const double4* __restrict__ pm,
-    double2* __restrict__ hz, HydroTree t, int pp_gather, double rextent,
+    double2* __restrict__ hz, HydroTree t, int pp_gather, double rextent0,
     int* __restrict__ scratch, int cap, DevError* err, unsigned long long* counts) {
   __shared__ double sel_all[HG_WARPS][HG_SEL];
   __shared__ int cand_all[HG_WARPS][GP_SEG * LEAFMAX];
@@ -1022,9 +1053,11 @@ __global__ void __launch_bounds__(HG_THREADS) k_hgather(
   int* lv = fb + cap;
   const unsigned lt = (1u << lane) - 1u;
   unsigned long long nwalk = 0, nvisit = 0;
-  const double rcap = 4.0 * (rextent > 0.0 ? rextent : 1.0);   // a ball that holds every particle
   for (int i = gw; i < nact; i += gridDim.x * HG_WARPS) {
     const int p = act ? act[i] : i;
+    tree_for(t, p);
+    const double rextent = t.cl ? t.rextent : rextent0;
+    const double rcap = 4.0 * (rextent > 0.0 ? rextent : 1.0);   // a ball that holds every particle
     const double4 P = pm[p];
     const double rx = P.x, ry = P.y, rz = P.z;
     const float px = (float)(rx - t.rootx), py = (float)(ry - t.rooty), pz = (float)(rz - t.rootz);
@@ -1130,6 +1163,7 @@ __global__ void k_neib_levels(int nact, const int* __restrict__ act, const doubl
   const double4 P = pm[p];
   const double hp = hz[p].x;
   const double hsp = (KERNRANGESQD * hp) * hp;
+  tree_for(t, p);
   walk_gather_scatter(t, P.x, P.y, P.z, KERNRANGE * hp, err, p, [&](int q) {
     if (q == p) return;
     const double hq = hz[q].x;
@@ -1187,14 +1221,17 @@ struct WideState {
   double4 P;        // position, mass
   double4 v;        // velocity
   double ih, hf, hs, hp;   // of the pass in progress
+  double rextent;   // of the particle's tree
   int p;
   int job;          // WideJob
+  int q0, q1;       // the particles of its cloud (all of them for one tree)
 };
 
 __global__ void k_wide_init(int n, const int* __restrict__ ids, const double4* __restrict__ pm,
                             const double2* __restrict__ hz, const double4* __restrict__ vel,
-                            double rextent, WideState* __restrict__ ws,
-                            double* __restrict__ acc, unsigned long long* counts) {
+                            double rextent, int ptot, const CloudInfo* __restrict__ cl, int ncl,
+                            WideState* __restrict__ ws, double* __restrict__ acc,
+                            unsigned long long* counts) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   atomicAdd(counts + 8, 1ull);
@@ -1202,7 +1239,16 @@ __global__ void k_wide_init(int n, const int* __restrict__ ids, const double4* _
   w.p = ids[i];
   w.P = pm[w.p];
   w.v = vel[w.p];
-  gh_init(w.s, hz[w.p].x, rextent);
+  w.rextent = rextent;
+  w.q0 = 0;
+  w.q1 = ptot;
+  if (cl) {
+    const CloudInfo& C = cl[cloud_of(cl, ncl, w.p)];
+    w.rextent = C.rextent;
+    w.q0 = C.pstart;
+    w.q1 = C.pstart + C.n;
+  }
+  gh_init(w.s, hz[w.p].x, w.rextent);
   w.job = WJ_COUNT;                 // hp > h_high = 0: the first walk (:154-170)
   w.s.h_high = w.s.hp * HMULT;
   for (int k = 0; k < 4; ++k) acc[4 * i + k] = 0.0;
@@ -1247,6 +1293,7 @@ __global__ void __launch_bounds__(WD_THREADS) k_wide_walk(
     const int lv = level[c];
     const int4 lk = t.link[c];
     if (!(lv == L || (lv < L && lk.x > 0))) continue;
+    if (lk.w < w.q0 || lk.w >= w.q1) continue;                  // another cloud's tree
     bool reach = true;
     for (int a = parent[c]; a >= 0 && reach; a = parent[a]) reach = pass(a);
     if (!reach) continue;
@@ -1320,13 +1367,14 @@ __global__ void __launch_bounds__(WD_THREADS) k_wide_brute(int n, const WideStat
     const WideState& w = ws[i];
     if (!wide_brute(w)) continue;                                 // block-uniform
     const int p = w.p;
+    const int q0 = w.q0, q1 = w.q1;
     const double rx = w.P.x, ry = w.P.y, rz = w.P.z;
     const double hs = w.hs, ih = w.ih, hf = w.hf;
     if (w.job == WJ_PASS) {                                       // :211-235
       double s0 = 0.0;
 #pragma unroll
       for (int k = 0; k < BR_Q; ++k) {
-        if (qi[k] < 0 || qi[k] == p) continue;
+        if (qi[k] < q0 || qi[k] >= q1 || qi[k] == p) continue;
         const double d0 = Q[k].x - rx, d1 = Q[k].y - ry, d2 = Q[k].z - rz;
         const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
         if (drsqd < hs) gh_density_in(drsqd, Q[k].w, ih, hf, s0);
@@ -1339,7 +1387,7 @@ __global__ void __launch_bounds__(WD_THREADS) k_wide_brute(int n, const WideStat
       f.rt = 0.0; f.om = 0.0; f.dv = 0.0; f.zt = 0.0;
 #pragma unroll
       for (int k = 0; k < BR_Q; ++k) {
-        if (qi[k] < 0 || qi[k] == p) continue;
+        if (qi[k] < q0 || qi[k] >= q1 || qi[k] == p) continue;
         const double d0 = Q[k].x - rx, d1 = Q[k].y - ry, d2 = Q[k].z - rz;
         const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
         if (drsqd > hs) continue;
@@ -1391,7 +1439,7 @@ __global__ void k_wide_update(int n, WideState* __restrict__ ws, double* __restr
     atomicAdd(counts + 3, 1ull);
   } else {                                                          // WJ_PASS
     atomicAdd(counts + 5, 1ull);
-    if (gh_after_pass(s, mp, h_fac, rextent, (mp * t0.x) * w.hf + a[0])) {
+    if (gh_after_pass(s, mp, h_fac, w.rextent, (mp * t0.x) * w.hf + a[0])) {
       w.hp = h_fac * pow(mp / s.rho, ONETHIRD);                      // :317
       w.ih = 1.0 / w.hp;
       w.hf = pow(w.ih, NDIMPR);
@@ -1454,8 +1502,9 @@ __global__ void __launch_bounds__(GR_THREADS) k_neib_walk(
   unsigned long long nvisit = 0;
   for (int g = gr_next(work, lane); (long long)g * 32 < nact; g = gr_next(work, lane)) {
     const int i = g * 32 + lane;
-    const bool live = i < nact;
-    const int p = live ? (act ? act[i] : i) : (act ? act[nact - 1] : nact - 1);
+    bool live;
+    const int p = group_particle(i, nact, act, live);
+    tree_for(t, p);                                    // lanes share one cloud
     const double4 P = pm[p];
     const float px = (float)(P.x - t.rootx), py = (float)(P.y - t.rooty),
                 pz = (float)(P.z - t.rootz);
@@ -1514,8 +1563,9 @@ __global__ void __launch_bounds__(GP_THREADS) k_neib_rows(
   unsigned long long ncands = 0, niter = 0, nsingle = 0;
   for (int g = gr_next(work, lane); (long long)g * 32 < nact; g = gr_next(work, lane)) {
     const int i = g * 32 + lane;
-    const bool live = i < nact;
-    const int p = live ? (act ? act[i] : i) : (act ? act[nact - 1] : nact - 1);
+    bool live;
+    const int p = group_particle(i, nact, act, live);
+    tree_for(t, p);                                    // lanes share one cloud
     const int n = live ? nleaf[p] : 0;
     const double4 P = pm[p];
     const double hp = hz[p].x;
@@ -1717,6 +1767,7 @@ __global__ void __launch_bounds__(128, 8) k_hydro(int nact, const int* __restric
     for (int k = sub; k < nn; k += SUB) pair(row[k]);
   } else if (sub == 0) {
     // get_neib_on_fly (sph/get_neib_on_fly.F90:11-130): same test as get_neib
+    tree_for(t, p);
     const double hsp = (KERNRANGESQD * hp) * hp;
     walk_gather_scatter(t, P.x, P.y, P.z, KERNRANGE * hp, err, p, [&](int q) {
       if (q == p) return;
@@ -1777,7 +1828,8 @@ inline int nb(long n, int t) { return (int)((n + t - 1) / t); }
 HydroTree hydro_tree(const Ctx& c) {
   const double delta = ldexp(1.0, -22) * (c.info.cellsize > 0.0 ? c.info.cellsize : 1.0);
   return HydroTree{c.link, c.hA, c.hrm, c.hA32, c.hrm32, c.nkids, c.hN, c.info.ctot, c.info.root[0],
-                   c.info.root[1], c.info.root[2], (float)delta};
+                   c.info.root[1], c.info.root[2], (float)delta, 0, c.info.rextent,
+                   c.ncloud > 1 ? c.d_clouds : nullptr, c.ncloud};
 }
 
 }  // namespace
@@ -1829,13 +1881,23 @@ int wide_scratch_alloc(Ctx& c) {
   return 0;
 }
 
+// the active list of the group kernels: in a forest with every particle
+// active, the particles cloud by cloud with each cloud padded to a multiple of 32
+static const int* group_list(const Ctx& c, int& nact) {
+  if (c.act || c.ncloud <= 1) return c.act;
+  nact = c.ngact;
+  return c.gact;
+}
+
 void launch_gradh(Ctx& c, int nact) {
   if (nact <= 0) return;
   unsigned long long* counts = reinterpret_cast<unsigned long long*>(c.d_counts);
   const HydroTree t = hydro_tree(c);
+  int ngrp = nact;
+  const int* gl = group_list(c, ngrp);
   cudaMemsetAsync(c.work, 0, sizeof(int), c.st);
-  k_gradh_walk<<<gr_grid(c, nact, 0), GR_THREADS, GR_SMEM, c.st>>>(
-      nact, c.act, c.pm, c.hz, t, c.leaves, c.nleaf, c.npot, c.wstack, c.wstack_cap, counts,
+  k_gradh_walk<<<gr_grid(c, ngrp, 0), GR_THREADS, GR_SMEM, c.st>>>(
+      ngrp, gl, c.pm, c.hz, t, c.leaves, c.nleaf, c.npot, c.wstack, c.wstack_cap, counts,
       c.work);
   finish_reorder(c);            // velocities still arriving: the passes need them from here on
   static int occ[16] = {};
@@ -1844,12 +1906,12 @@ void launch_gradh(Ctx& c, int nact) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_gradh_pass, GP_THREADS, 0);
     if (o < 1) o = 1;
   }
-  const int blocks = std::min(sm_count(c) * o, nb(nb(nact, 32), GP_WARPS));
+  const int blocks = std::min(sm_count(c) * o, nb(nb(ngrp, 32), GP_WARPS));
   cudaMemsetAsync(c.work, 0, 3 * sizeof(int), c.st);     // group counter, nredo, nwide
   k_gradh_pass<<<blocks, GP_THREADS, 0, c.st>>>(
-      nact, c.act, c.pm, c.hz, c.vel, c.rho, c.omega, c.div_v, c.drhodt, c.tabA, c.prm.h_fac,
+      ngrp, gl, c.pm, c.hz, c.vel, c.rho, c.omega, c.div_v, c.drhodt, c.tabA, c.prm.h_fac,
       c.prm.pp_gather, c.info.rextent, c.leaves, c.nleaf, c.npot, c.redo, c.work + 1,
-      c.pplist, c.prm.pp_limit, c.d_err, counts, c.work);
+      c.pplist, c.prm.pp_limit, c.d_err, counts, c.work, t.cl, t.ncl);
   // three walk-stack slots of scratch per redo warp
   k_gradh_redo<<<std::max(1, (c.wstack_slots / 3) / RD_WARPS), RD_THREADS, 0, c.st>>>(
       c.redo, c.work + 1, c.pm, c.hz, c.vel, c.rho, c.omega, c.div_v, c.drhodt, t, c.tabA,
@@ -1871,7 +1933,8 @@ void launch_gradh(Ctx& c, int nact) {
     for (int b0 = 0; b0 < nwide; b0 += WD_BATCH) {
       const int n = std::min(WD_BATCH, nwide - b0);
       k_wide_init<<<nb(n, 128), 128, 0, c.st>>>(n, c.wide + b0, c.pm, c.hz, c.vel,
-                                                  c.info.rextent, static_cast<WideState*>(c.wst), c.wacc, counts);
+                                                  c.info.rextent, c.ptot, t.cl, t.ncl,
+                                                  static_cast<WideState*>(c.wst), c.wacc, counts);
       ++c.nlaunch;
       for (int round = 0;; ++round) {
         k_wide_walk<<<n * WD_SLICES, WD_THREADS, 0, c.st>>>(
@@ -1903,18 +1966,20 @@ void launch_neib(Ctx& c, int nact) {
   if (nact <= 0) return;
   unsigned long long* counts = reinterpret_cast<unsigned long long*>(c.d_counts);
   const HydroTree t = hydro_tree(c);
+  int ngrp = nact;
+  const int* gl = group_list(c, ngrp);
   cudaMemsetAsync(c.work, 0, sizeof(int), c.st);
-  k_neib_walk<<<gr_grid(c, nact, 1), GR_THREADS, GR_SMEM, c.st>>>(
-      nact, c.act, c.pm, c.hz, t, c.leaves, c.nleaf, c.wstack, c.wstack_cap, counts, c.work);
+  k_neib_walk<<<gr_grid(c, ngrp, 1), GR_THREADS, GR_SMEM, c.st>>>(
+      ngrp, gl, c.pm, c.hz, t, c.leaves, c.nleaf, c.wstack, c.wstack_cap, counts, c.work);
   static int occ[16] = {};
   int& o = occ[c.dev >= 0 && c.dev < 16 ? c.dev : 0];
   if (o == 0) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_neib_rows, GP_THREADS, 0);
     if (o < 1) o = 1;
   }
-  const int blocks = std::min(sm_count(c) * o, nb(nb(nact, 32), GP_WARPS));
+  const int blocks = std::min(sm_count(c) * o, nb(nb(ngrp, 32), GP_WARPS));
   cudaMemsetAsync(c.work, 0, sizeof(int), c.st);          // group counter
-  k_neib_rows<<<blocks, GP_THREADS, 0, c.st>>>(nact, c.act, c.pm, c.hz, t, c.prm.pp_limit,
+  k_neib_rows<<<blocks, GP_THREADS, 0, c.st>>>(ngrp, gl, c.pm, c.hz, t, c.prm.pp_limit,
                                                c.leaves, c.nleaf, c.pptot, c.pplist, c.d_err,
                                                counts, c.work);
   c.nlaunch += 2;

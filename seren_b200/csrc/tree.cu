@@ -132,17 +132,66 @@ __global__ void k_bbox_final(const double* __restrict__ part, int nblk, TreeInfo
   for (int k = 0; k < 3; ++k) info->root[k] = 0.5 * (rmin[k] + rmax[k]);
 }
 
+// the same per cloud of a forest, one block per cloud; cloud 0 also fills the
+// tree summary's root box
+__global__ void k_bbox_clouds(const double4* __restrict__ pm, CloudInfo* cl, TreeInfo* info) {
+  __shared__ double s[6][BB_T];
+  CloudInfo& C = cl[blockIdx.x];
+  const int p0 = C.pstart, n = C.n;
+  double mx[3] = {-BIG_NUMBER, -BIG_NUMBER, -BIG_NUMBER};
+  double mn[3] = {BIG_NUMBER, BIG_NUMBER, BIG_NUMBER};
+  for (int i = threadIdx.x; i < n; i += BB_T) {
+    const double4 p = pm[p0 + i];
+    mx[0] = fmax(mx[0], p.x); mx[1] = fmax(mx[1], p.y); mx[2] = fmax(mx[2], p.z);
+    mn[0] = fmin(mn[0], p.x); mn[1] = fmin(mn[1], p.y); mn[2] = fmin(mn[2], p.z);
+  }
+  for (int k = 0; k < 3; ++k) { s[k][threadIdx.x] = mx[k]; s[3 + k][threadIdx.x] = mn[k]; }
+  __syncthreads();
+  for (int o = BB_T / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o)
+      for (int k = 0; k < 3; ++k) {
+        s[k][threadIdx.x] = fmax(s[k][threadIdx.x], s[k][threadIdx.x + o]);
+        s[3 + k][threadIdx.x] = fmin(s[3 + k][threadIdx.x], s[3 + k][threadIdx.x + o]);
+      }
+    __syncthreads();
+  }
+  if (threadIdx.x != 0) return;
+  const double rmax[3] = {s[0][0], s[1][0], s[2][0]};
+  const double rmin[3] = {s[3][0], s[4][0], s[5][0]};
+  const double ext = fmax(fmax(rmax[0] - rmin[0], rmax[1] - rmin[1]), rmax[2] - rmin[2]);
+  C.rextent = ext;
+  C.cellsize = 0.5 * ext;
+  for (int k = 0; k < 3; ++k) C.root[k] = 0.5 * (rmin[k] + rmax[k]);
+  C.delta = (float)(ldexp(1.0, -22) * (C.cellsize > 0.0 ? C.cellsize : 1.0));
+  C.cell = blockIdx.x;
+  if (blockIdx.x == 0) {
+    info->rextent = C.rextent;
+    info->cellsize = C.cellsize;
+    for (int k = 0; k < 3; ++k) info->root[k] = C.root[k];
+  }
+}
+
 // ---------------------------------------------------------------------------
+// octant path keys: the comparisons and centre updates of BHgrav_build.F90:// ---------------------------------------------------------------------------
 // octant path keys: the comparisons and centre updates of BHgrav_build.F90:
 // octant bits x=1, y=2, z=4 (:121-126), child centre rc -/+ cellsize (:212-229)
 // with cellsize halved before each level (:95).
+// In a forest (cl != NULL) each particle uses its own cloud's root box, and
+// keep (when given) gets a copy of the keys in input order.
 __global__ void k_keys(const double4* __restrict__ pm, int n, const TreeInfo* __restrict__ info,
-                       unsigned long long* __restrict__ keys, int* __restrict__ idx) {
+                       const CloudInfo* __restrict__ cl, int ncl,
+                       unsigned long long* __restrict__ keys,
+                       unsigned long long* __restrict__ keep, int* __restrict__ idx) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double4 p = pm[i];
   double cx = info->root[0], cy = info->root[1], cz = info->root[2];
   double cs = info->cellsize;
+  if (cl) {
+    const CloudInfo& C = cl[cloud_of(cl, ncl, (int)i)];
+    cx = C.root[0]; cy = C.root[1]; cz = C.root[2];
+    cs = C.cellsize;
+  }
   unsigned long long key = 0ull;
 #pragma unroll 1
   for (int lev = 0; lev < KEY_LEVELS; ++lev) {
@@ -154,6 +203,7 @@ __global__ void k_keys(const double4* __restrict__ pm, int n, const TreeInfo* __
     cz = (d & 4) ? __dadd_rn(cz, cs) : __dsub_rn(cz, cs);
   }
   keys[i] = key;
+  if (keep) keep[i] = key;
   idx[i] = (int)i;
 }
 
@@ -161,7 +211,8 @@ __global__ void k_keys(const double4* __restrict__ pm, int n, const TreeInfo* __
 // levels 1..21 in hi (as k_keys), levels 22..30 in lo (27 bits, level 22 in
 // the most significant digit).  keys gets lo as the first sort key.
 __global__ void k_keys_deep(const double4* __restrict__ pm, int n,
-                            const TreeInfo* __restrict__ info, unsigned long long* __restrict__ keys,
+                            const TreeInfo* __restrict__ info, const CloudInfo* __restrict__ cl,
+                            int ncl, unsigned long long* __restrict__ keys,
                             unsigned long long* __restrict__ hi, unsigned* __restrict__ lo,
                             int* __restrict__ idx) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -169,6 +220,11 @@ __global__ void k_keys_deep(const double4* __restrict__ pm, int n,
   const double4 p = pm[i];
   double cx = info->root[0], cy = info->root[1], cz = info->root[2];
   double cs = info->cellsize;
+  if (cl) {
+    const CloudInfo& C = cl[cloud_of(cl, ncl, (int)i)];
+    cx = C.root[0]; cy = C.root[1]; cz = C.root[2];
+    cs = C.cellsize;
+  }
   unsigned long long kh = 0ull;
   unsigned kl = 0u;
 #pragma unroll 1
@@ -185,6 +241,14 @@ __global__ void k_keys_deep(const double4* __restrict__ pm, int n,
   hi[i] = kh;
   lo[i] = kl;
   idx[i] = (int)i;
+}
+
+// the last sort key of a forest: the cloud of each particle, in the order so far
+__global__ void k_cloud_keys(const int* __restrict__ idx, int n, const CloudInfo* __restrict__ cl,
+                             int ncl, unsigned long long* __restrict__ keys) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  keys[i] = (unsigned long long)cloud_of(cl, ncl, idx[i]);
 }
 
 // after the stable sort on lo: the hi words in that order, the next sort key
@@ -284,6 +348,30 @@ __global__ void k_root(int n, int cmax, int* leaf, int* nextcell, int* ifopen, i
   info->ctot = 0;
   info->first_cell[0] = 0;
   info->last_cell[0] = 0;
+}
+
+// the roots of a forest: cell k is cloud k's root (always split, as the
+// single root, BHgrav_build.F90:74-75), its particles the cloud's sorted range
+__global__ void k_roots(int ncl, const CloudInfo* __restrict__ cl, int cmax, int* leaf,
+                        int* nextcell, int* ifopen, int* pstart, int* pcount, int* parent,
+                        int* level, int* branch, TreeInfo* info) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < ncl) {
+    leaf[k] = 0;
+    nextcell[k] = cmax + 1;
+    ifopen[k] = -1;
+    pstart[k] = cl[k].pstart;
+    pcount[k] = cl[k].n;
+    parent[k] = -1;
+    level[k] = 0;
+    branch[k] = k;
+  }
+  if (k == 0) {
+    info->nbranch = ncl;
+    info->ctot = ncl - 1;
+    info->first_cell[0] = 0;
+    info->last_cell[0] = ncl - 1;
+  }
 }
 
 __device__ __forceinline__ int key_digit(unsigned long long key, int lev) {
@@ -517,10 +605,16 @@ __global__ void k_stock_level(int cfirst, int clast, const int4* __restrict__ li
                               double4* __restrict__ bbmina, double4* __restrict__ bbmaxa,
                               double rootx, double rooty, double rootz, double delta,
                               const int* __restrict__ nkids, float4* __restrict__ wA,
-                              float4* __restrict__ hA32, float4* __restrict__ hN) {
+                              float4* __restrict__ hA32, float4* __restrict__ hN,
+                              const CloudInfo* __restrict__ cl, int ncl) {
   const int c = cfirst + blockIdx.x * blockDim.x + threadIdx.x;
   if (c > clast) return;
   const int4 lk = link[c];
+  if (cl) {                                  // a forest: the cell's own cloud's root box
+    const CloudInfo& C = cl[cloud_of(cl, ncl, lk.w)];
+    rootx = C.root[0]; rooty = C.root[1]; rootz = C.root[2];
+    delta = ldexp(1.0, -22) * (C.cellsize > 0.0 ? C.cellsize : 1.0);
+  }
   double mc = 0.0;
   double rc[3] = {0.0, 0.0, 0.0};
   double qc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
@@ -793,9 +887,16 @@ constexpr int NEED_DEEP_KEYS = -1;
 // needs level 22 returns NEED_DEEP_KEYS
 static int build_cells(Ctx& c, bool deep, int& ctot_out) {
   const int n = c.ptot;
-  k_root<<<1, 1, 0, c.st>>>(n, c.cmax, c.leaf, c.nextcell, c.ifopen, c.pstart, c.pcount, c.parent,
-                            c.level, c.branch, c.d_info); ++c.nlaunch;
-  int nbranch = 1, ctot = 0, lev = 0;
+  const int ncl = c.ncloud;
+  if (ncl > 1)
+    k_roots<<<nb(ncl, 128), 128, 0, c.st>>>(ncl, c.d_clouds, c.cmax, c.leaf, c.nextcell, c.ifopen,
+                                            c.pstart, c.pcount, c.parent, c.level, c.branch,
+                                            c.d_info);
+  else
+    k_root<<<1, 1, 0, c.st>>>(n, c.cmax, c.leaf, c.nextcell, c.ifopen, c.pstart, c.pcount,
+                              c.parent, c.level, c.branch, c.d_info);
+  ++c.nlaunch;
+  int nbranch = ncl, ctot = ncl - 1, lev = 0;
   int* br = c.branch;
   int* br_next = c.branch_next;
   while (true) {
@@ -832,23 +933,41 @@ static int build_cells(Ctx& c, bool deep, int& ctot_out) {
   return SEREN_GPU_OK;
 }
 
+// a forest: a last stable pass on the cloud of each particle makes the order
+// cloud-major again, then the octant words (kept in input order in keys_hi)
+// are gathered into that order for the cell split
+static void sort_by_cloud(Ctx& c, int n) {
+  k_cloud_keys<<<nb(n, 256), 256, 0, c.st>>>(c.idx, n, c.d_clouds, c.ncloud, c.keys); ++c.nlaunch;
+  radix_sort(c, n, c.ncloud <= 65536 ? 16 : 32);      // an even number of passes
+  k_gather_hi<<<nb(n, 256), 256, 0, c.st>>>(c.keys_hi, c.idx, n, c.keys); ++c.nlaunch;
+}
+
 int build_tree(Ctx& c) {
   const int n = c.ptot;
-  const int bblk = std::min(nb(n, BB_T), 1184);
-  k_bbox_partial<<<bblk, BB_T, 0, c.st>>>(c.pm, n, c.bbox_part); ++c.nlaunch;
-  k_bbox_final<<<1, BB_T, 0, c.st>>>(c.bbox_part, bblk, c.d_info); ++c.nlaunch;
-  k_keys<<<nb(n, 256), 256, 0, c.st>>>(c.pm, n, c.d_info, c.keys, c.idx); ++c.nlaunch;
+  const bool forest = c.ncloud > 1;
+  const CloudInfo* cl = forest ? c.d_clouds : nullptr;
+  if (forest) {
+    k_bbox_clouds<<<c.ncloud, BB_T, 0, c.st>>>(c.pm, c.d_clouds, c.d_info); ++c.nlaunch;
+  } else {
+    const int bblk = std::min(nb(n, BB_T), 1184);
+    k_bbox_partial<<<bblk, BB_T, 0, c.st>>>(c.pm, n, c.bbox_part); ++c.nlaunch;
+    k_bbox_final<<<1, BB_T, 0, c.st>>>(c.bbox_part, bblk, c.d_info); ++c.nlaunch;
+  }
+  k_keys<<<nb(n, 256), 256, 0, c.st>>>(c.pm, n, c.d_info, cl, c.ncloud, c.keys,
+                                        forest ? c.keys_hi : nullptr, c.idx); ++c.nlaunch;
   radix_sort(c, n, 64);
+  if (forest) sort_by_cloud(c, n);
   int ctot = 0;
   int rc = build_cells(c, false, ctot);
   if (rc == NEED_DEEP_KEYS) {
     // sort on (levels 1..21, levels 22..30): stable passes on the low word,
     // then on the high word in that order
-    k_keys_deep<<<nb(n, 256), 256, 0, c.st>>>(c.pm, n, c.d_info, c.keys, c.keys_hi, c.keys_lo,
-                                               c.idx); ++c.nlaunch;
+    k_keys_deep<<<nb(n, 256), 256, 0, c.st>>>(c.pm, n, c.d_info, cl, c.ncloud, c.keys, c.keys_hi,
+                                               c.keys_lo, c.idx); ++c.nlaunch;
     radix_sort(c, n, 32);
     k_gather_hi<<<nb(n, 256), 256, 0, c.st>>>(c.keys_hi, c.idx, n, c.keys); ++c.nlaunch;
     radix_sort(c, n, 64);
+    if (forest) sort_by_cloud(c, n);
     rc = build_cells(c, true, ctot);
   }
   if (rc) return rc;
@@ -906,6 +1025,13 @@ __global__ void k_max_offset(const double4* __restrict__ pm, int n, double rx, d
 
 int restock(Ctx& c, bool& rebuilt) {
   rebuilt = false;
+  if (c.ncloud > 1) {                      // a forest is built at every evaluation
+    rebuilt = true;
+    const int rc = build_tree(c);
+    if (rc) return rc;
+    launch_stock(c);
+    return SEREN_GPU_OK;
+  }
   // the FP32 node records bound the rounding of a coordinate relative to the
   // root centre by 2^-22 cellsize, which holds while every particle is within
   // two root half widths of the centre; past that (or on non-finite
@@ -940,7 +1066,9 @@ void launch_stock(Ctx& c) {
     k_stock_level<<<nb(cnt, 128), 128, 0, c.st>>>(f, la, c.link, c.pm, c.hz, c.prm.thetamaxsqd, daux,
                                                  c.gA, c.gB, c.gC, c.hA, c.hmax, c.bbmin, c.bbmax,
                                                  c.info.root[0], c.info.root[1], c.info.root[2],
-                                                 delta, c.nkids, c.wA, c.hA32, c.hN); ++c.nlaunch;
+                                                 delta, c.nkids, c.wA, c.hA32, c.hN,
+                                                 c.ncloud > 1 ? c.d_clouds : nullptr, c.ncloud);
+    ++c.nlaunch;
   }
 }
 

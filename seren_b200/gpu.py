@@ -51,7 +51,8 @@ def library(build_if_missing: bool = True) -> C.CDLL:
                            ("fma_peak", [vp, C.c_int32, _dp]),
                            ("block_start", [vp, C.c_void_p]),
                            ("block_step", [vp, C.c_void_p]),
-                           ("block_levels", [vp, _ip, C.POINTER(C.c_int64), _ip, _ip])):
+                           ("block_levels", [vp, _ip, C.POINTER(C.c_int64), _ip, _ip]),
+                           ("set_clouds", [vp, C.c_int32, _ip])):
             fn = getattr(lib, f"seren_gpu_{name}")
             fn.argtypes = args
             fn.restype = C.c_int
@@ -195,6 +196,13 @@ class GpuHotPath(HotPath):
         """Build the tree every nbuildstep device-resident evaluations and
         restock it in between (seren_gpu_set_build_step)."""
         self._call("set_build_step", self._ctx, int(nbuildstep))
+
+    def set_clouds(self, counts):
+        """The uploaded particles are len(counts) independent clouds, one after
+        another (seren_gpu_set_clouds); every force step then builds and walks
+        a forest of their trees in single launches."""
+        cnt = np.ascontiguousarray(np.atleast_1d(counts), dtype=np.int32)
+        self._call("set_clouds", self._ctx, int(cnt.size), cnt.ctypes.data_as(_ip))
 
     def block_start(self, nlevels=3, level_mode=1, check_neib=1, dt_fixed=1.0,
                     courant_mult=0.2, accel_mult=0.5):

@@ -118,3 +118,70 @@ def test_gpu_batch_equals_single_cloud_runs_and_oracle():
         assert np.array_equal(st["perm"], r["perm"])
         assert rel_rows(st["a"], r["a"]).max() < 1e-11
     b.close()
+
+
+def _forest_clouds():
+    """Uneven clouds, all in the same unit sphere (their trees overlap in
+    space), sizes from just above pp_gather to tens of thousands, ragged."""
+    sizes = [100, 777, 4096, 20000, 333, 2500, 9001]
+    out = []
+    for k, n in enumerate(sizes):
+        ic = ics.uniform_sphere(n=n, seed=500 + k, sound=0.05 + 0.03 * k)
+        ic["v"] = np.random.Generator(np.random.PCG64(600 + k)).normal(0.0, 0.1, (n, 3))
+        out.append(ic)
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [0, 1])
+def test_forest_equals_single_cloud_runs(precision):
+    """seren_gpu_set_clouds: every cloud of a forest, built and walked in single
+    launches over all clouds, equals a context holding that cloud alone bit for
+    bit (order, h, rho, omega, a, gpot) through a first call, a drift and a
+    second force step."""
+    from seren_b200.gpu import GpuHotPath
+    clouds = _forest_clouds()
+    ns = [c["parray"].shape[0] for c in clouds]
+    g = GpuHotPath(sum(ns), params(clouds[0], precision=precision))
+    g.upload(np.vstack([c["parray"] for c in clouds]), np.vstack([c["v"] for c in clouds]),
+             np.concatenate([c["sound"] ** 2 for c in clouds]))
+    g.set_clouds(ns)
+    g.force_step(first_call=True)
+    g.drift(1.0e-3)
+    g.force_step()
+    st = g.download()
+    g.close()
+    off = 0
+    for ic, n in zip(clouds, ns):
+        one = GpuHotPath(n, params(ic, precision=precision))
+        one.upload(ic["parray"], ic["v"], ic["sound"] ** 2)
+        one.force_step(first_call=True)
+        one.drift(1.0e-3)
+        one.force_step()
+        d = one.download()
+        one.close()
+        rows = slice(off, off + n)
+        assert np.array_equal(st["perm"][rows], d["perm"] + off)
+        for k in ("parray", "rho", "omega", "a", "gpot"):
+            assert np.array_equal(st[k][rows], d[k]), k
+        off += n
+
+
+@pytest.mark.gpu
+def test_forest_refuses_what_it_does_not_support():
+    from seren_b200.cabi import SerenError
+    from seren_b200.gpu import GpuHotPath
+    clouds = _forest_clouds()[:3]
+    ns = [c["parray"].shape[0] for c in clouds]
+    g = GpuHotPath(sum(ns), params(clouds[0]))
+    g.upload(np.vstack([c["parray"] for c in clouds]), np.vstack([c["v"] for c in clouds]),
+             np.concatenate([c["sound"] ** 2 for c in clouds]))
+    with pytest.raises(SerenError):
+        g.set_clouds([ns[0], ns[1]])                       # counts must add up to ptot
+    g.set_clouds(ns)
+    with pytest.raises(SerenError):
+        g.set_sinks(np.array([[0.0, 0.0, 0.0, 1.0, 0.05]]))
+    g.force_step(first_call=True)
+    with pytest.raises(SerenError):
+        g.block_start()
+    g.close()
