@@ -319,7 +319,8 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
     // 0's particle (always live)
     int p = i < nact ? (act ? act[i] : i) : -1;
     const bool live = p >= 0;
-    p = live ? p : __shfl_sync(FULLMASK, p, 0);
+    const int p0 = __shfl_sync(FULLMASK, p, 0);        // every lane takes part
+    p = live ? p : p0;
     if (t.cl) {                                        // the lanes' cloud's tree
       const CloudInfo& C = t.cl[cloud_of(t.cl, t.ncl, p)];
       t.root = C.cell;

@@ -172,7 +172,6 @@ __global__ void k_bbox_clouds(const double4* __restrict__ pm, CloudInfo* cl, Tre
 }
 
 // ---------------------------------------------------------------------------
-// octant path keys: the comparisons and centre updates of BHgrav_build.F90:// ---------------------------------------------------------------------------
 // octant path keys: the comparisons and centre updates of BHgrav_build.F90:
 // octant bits x=1, y=2, z=4 (:121-126), child centre rc -/+ cellsize (:212-229)
 // with cellsize halved before each level (:95).
