@@ -88,3 +88,57 @@ class CloudBatch:
         for g in self.ctx:
             g.close()
         self.ctx = []
+
+
+class CloudForest:
+    """One device-resident context holding one rank's clouds as a forest
+    (seren_gpu_set_clouds): every force evaluation builds all the clouds'
+    trees with one sort and one level-by-level split, and runs each stage
+    (grad-h walk and passes, neighbour lists, hydro, gravity) as one launch
+    over every cloud.  The clouds must share h_fac, theta and alpha (their
+    sound speeds differ freely)."""
+
+    def __init__(self, clouds: Sequence[Dict], precision: int = 1):
+        import numpy as np
+
+        from .gpu import GpuHotPath
+        ic0 = clouds[0]
+        for ic in clouds:
+            if (ic["h_fac"], ic["thetamaxsqd"], ic["alpha"]) != \
+                    (ic0["h_fac"], ic0["thetamaxsqd"], ic0["alpha"]):
+                raise ValueError("the clouds of a forest share h_fac, theta and alpha")
+        self.ns = [int(ic["parray"].shape[0]) for ic in clouds]
+        self.offsets = [0]
+        for n in self.ns[:-1]:
+            self.offsets.append(self.offsets[-1] + n)
+        self.n = sum(self.ns)
+        self.g = GpuHotPath(self.n, params_for(ic0, precision))
+        self.g.upload(np.vstack([ic["parray"] for ic in clouds]),
+                      np.vstack([ic["v"] for ic in clouds]),
+                      np.concatenate([np.asarray(ic["sound"]) ** 2 for ic in clouds]))
+        self.g.set_clouds(self.ns)
+
+    def step(self, first_call: bool = False, dt: float = 0.0) -> int:
+        """One force evaluation of every cloud (after a drift by dt when
+        dt != 0); returns the number of kernels launched."""
+        n = 0
+        if dt != 0.0:
+            self.g.drift(dt)
+            n += 1
+        self.g.force_step(first_call=first_call)
+        return n + self.g.last_step_stats()[1]
+
+    def download(self) -> List[Dict]:
+        """Per-cloud results in each cloud's tree order (perm: the cloud's own
+        upload indices), as CloudBatch.download gives them."""
+        st = self.g.download()
+        out = []
+        for off, n in zip(self.offsets, self.ns):
+            rows = slice(off, off + n)
+            d = {k: v[rows] for k, v in st.items()}
+            d["perm"] = d["perm"] - off
+            out.append(d)
+        return out
+
+    def close(self):
+        self.g.close()

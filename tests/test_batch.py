@@ -185,3 +185,22 @@ def test_forest_refuses_what_it_does_not_support():
     with pytest.raises(SerenError):
         g.block_start()
     g.close()
+
+
+@pytest.mark.gpu
+def test_cloud_forest_equals_cloud_batch():
+    """seren_b200.batch.CloudForest (one forest context) gives every cloud the
+    results of CloudBatch (one context per cloud), bit for bit, after two
+    steps with a drift."""
+    from seren_b200.batch import CloudBatch, CloudForest
+    clouds = ics.batched_clouds(ncloud=5, nmin=800, nmax=5000, seed0=1000)
+    got = []
+    for cls in (CloudForest, CloudBatch):
+        b = cls(clouds, precision=1)
+        b.step(first_call=True)
+        b.step(dt=1.0e-3)
+        got.append(b.download())
+        b.close()
+    for f, one in zip(*got):
+        for k in ("perm", "parray", "v", "rho", "omega", "a", "gpot"):
+            assert np.array_equal(f[k], one[k]), k
