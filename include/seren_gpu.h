@@ -184,6 +184,32 @@ int seren_gpu_rk2_step(seren_gpu_ctx* ctx, double dt);
  * evaluation. */
 int seren_gpu_set_clouds(seren_gpu_ctx* ctx, int32_t ncloud, const int32_t* counts);
 
+/* Kernel tuning (no counterpart in the reference).  The knobs: threads per
+ * particle of the mixed-precision hydro kernel (2, 4 or 8), the cell-list tile
+ * of the mixed-precision gravity walk (64 or 96 entries), and the resident
+ * blocks per SM of the gravity walk, the grad-h pass and the neighbour-row
+ * kernels (0: as many as fit).  The defaults (4, 64, 0, 0, 0) suit the 4M-
+ * particle core.  seren_gpu_autotune, after seren_gpu_upload and a first
+ * seren_gpu_force_step, times `trials` force steps on the current state for
+ * each of four configurations, keeps for every stage its fastest, applies
+ * the result to the context and records it for the process under (device,
+ * precision, ceil(log2 ptot)); with trials <= 0 it applies the recorded
+ * choice instead (SEREN_GPU_ERR_STATE when there is none).  The FP64 path's
+ * results do not depend on the knobs; the mixed path's change within FP32
+ * rounding (the order of its partial sums).  ms_per_step (out) is the force
+ * step the chosen knobs give. */
+typedef struct {
+  int32_t hydro_sub;
+  int32_t grav_cap;
+  int32_t grav_bps;
+  int32_t gradh_bps;
+  int32_t neib_bps;
+  int32_t reserved;
+  double ms_per_step;
+} seren_gpu_tuning;
+int seren_gpu_autotune(seren_gpu_ctx* ctx, int32_t trials, seren_gpu_tuning* out);
+int seren_gpu_set_tuning(seren_gpu_ctx* ctx, const seren_gpu_tuning* tuning);
+
 /* Block timesteps (nlevels > 1) of the reference's main loop for the
  * second-order Runge-Kutta scheme, on the device-resident particles
  * (sph_sim/sph_integrate.F90:27-136).  seren_gpu_block_start, after

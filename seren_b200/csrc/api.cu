@@ -9,6 +9,10 @@
 #include <cstring>
 #include <vector>
 
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <array>
 #include "ctx.cuh"
 
 struct seren_gpu_ctx {
@@ -1203,6 +1207,121 @@ int seren_gpu_set_clouds(seren_gpu_ctx* h, int32_t ncloud, const int32_t* counts
   c.ngact = (int)gl.size();
   c.ncloud = ncloud;
   return finish(c, "set_clouds");
+}
+
+namespace {
+// tuned knobs per (device, precision, ceil(log2 N)), shared by the contexts of
+// the process (seren_gpu_autotune with trials = 0 reuses them)
+std::mutex g_tune_mutex;
+std::map<std::tuple<int, int, int>, seren::Tuning> g_tune_cache;
+
+int tune_key_bits(int n) {
+  int b = 0;
+  while ((1ll << b) < (long long)n) ++b;
+  return b;
+}
+
+bool tune_valid(const seren::Tuning& t) {
+  return (t.hydro_sub == 2 || t.hydro_sub == 4 || t.hydro_sub == 8) &&
+         (t.grav_cap == 64 || t.grav_cap == 96) && t.grav_bps >= 0 && t.gradh_bps >= 0 &&
+         t.neib_bps >= 0;
+}
+
+void tune_out(const seren::Tuning& t, double ms, seren_gpu_tuning* out) {
+  if (!out) return;
+  out->hydro_sub = t.hydro_sub;
+  out->grav_cap = t.grav_cap;
+  out->grav_bps = t.grav_bps;
+  out->gradh_bps = t.gradh_bps;
+  out->neib_bps = t.neib_bps;
+  out->reserved = 0;
+  out->ms_per_step = ms;
+}
+}  // namespace
+
+int seren_gpu_set_tuning(seren_gpu_ctx* h, const seren_gpu_tuning* t) {
+  if (!h) return SEREN_GPU_ERR_ARG;
+  Ctx& c = h->c;
+  if (!t) return fail(c, SEREN_GPU_ERR_ARG, "set_tuning: NULL");
+  seren::Tuning k;
+  k.hydro_sub = t->hydro_sub;
+  k.grav_cap = t->grav_cap;
+  k.grav_bps = t->grav_bps;
+  k.gradh_bps = t->gradh_bps;
+  k.neib_bps = t->neib_bps;
+  if (!tune_valid(k)) return fail(c, SEREN_GPU_ERR_ARG, "set_tuning: a knob out of range");
+  c.tune = k;
+  return SEREN_GPU_OK;
+}
+
+int seren_gpu_autotune(seren_gpu_ctx* h, int32_t trials, seren_gpu_tuning* out) {
+  if (!h) return SEREN_GPU_ERR_ARG;
+  Ctx& c = h->c;
+  if (!c.have_v || !c.have_csq || !c.have_sph || c.ptot < 1 || c.blk.on)
+    return fail(c, SEREN_GPU_ERR_STATE, "autotune: upload and a first force step come first");
+  const auto key = std::make_tuple(c.dev, c.prm.precision, tune_key_bits(c.ptot));
+  if (trials <= 0) {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    auto it = g_tune_cache.find(key);
+    if (it == g_tune_cache.end())
+      return fail(c, SEREN_GPU_ERR_STATE, "autotune: nothing tuned yet for this size");
+    c.tune = it->second;
+    tune_out(c.tune, 0.0, out);
+    return SEREN_GPU_OK;
+  }
+  const bool mixed = c.prm.precision != 0;
+  // candidates per knob; round r takes candidate r of the gravity pairs and
+  // candidate r mod n of the others, and each stage keeps its best round
+  struct GravKnob { int cap, bps; };
+  std::vector<GravKnob> grav = mixed
+      ? std::vector<GravKnob>{{64, 0}, {96, 0}, {64, 3}, {96, 4}}
+      : std::vector<GravKnob>{{64, 0}, {64, 3}, {64, 2}, {64, 0}};
+  const int hsub[3] = {4, 2, 8};
+  const int gbps[3] = {0, 4, 2};
+  const int nbps[3] = {0, 4, 2};
+  const int rounds = 4;
+  std::vector<std::array<double, 5>> ms(rounds);
+  const seren::Tuning keep = c.tune;
+  for (int r = 0; r < rounds; ++r) {
+    seren::Tuning t;
+    t.grav_cap = grav[r].cap;
+    t.grav_bps = grav[r].bps;
+    t.hydro_sub = mixed ? hsub[r % 3] : 4;
+    t.gradh_bps = gbps[r % 3];
+    t.neib_bps = nbps[r % 3];
+    c.tune = t;
+    ms[r].fill(0.0);
+    for (int k = 0; k < trials; ++k) {
+      c.nlaunch = 0;
+      int rc = seren::force_step_body(c, 0, nullptr);
+      if (rc) {
+        c.tune = keep;
+        return rc;
+      }
+      for (int st = 0; st < 5; ++st) ms[r][st] += c.stage_ms[st];
+    }
+  }
+  auto best = [&](int stage) {
+    int b = 0;
+    for (int r = 1; r < rounds; ++r)
+      if (ms[r][stage] < ms[b][stage]) b = r;
+    return b;
+  };
+  seren::Tuning t;
+  const int bg = best(4), bh = best(3), bgr = best(1), bn = best(2);
+  t.grav_cap = grav[bg].cap;
+  t.grav_bps = grav[bg].bps;
+  t.hydro_sub = mixed ? hsub[bh % 3] : 4;
+  t.gradh_bps = gbps[bgr % 3];
+  t.neib_bps = nbps[bn % 3];
+  c.tune = t;
+  const double chosen = (ms[0][0] + ms[bgr][1] + ms[bn][2] + ms[bh][3] + ms[bg][4]) / trials;
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    g_tune_cache[key] = t;
+  }
+  tune_out(t, chosen, out);
+  return SEREN_GPU_OK;
 }
 
 int seren_gpu_block_start(seren_gpu_ctx* h, const seren_gpu_block_params* prm) {

@@ -21,6 +21,17 @@ struct ScanScratch {
 // scalars of the reference's time_module on the host, the per-particle level
 // state in tree order on the device (permuted at every build, as
 // reorder_particle_arrays does).
+// Tuning knobs of the kernels (seren_gpu_autotune, seren_gpu_set_tuning).
+// The FP64 path's results do not depend on them; the mixed path's change in
+// the FP32 rounding of its partial sums only (hydro_sub, grav_cap).
+struct Tuning {
+  int hydro_sub = 4;   // threads per particle of the mixed hydro kernel: 2, 4 or 8
+  int grav_cap = 64;   // cell-list tile of the mixed gravity walk: 64 or 96 entries
+  int grav_bps = 0;    // resident blocks per SM of the gravity walk (0: as many as fit)
+  int gradh_bps = 0;   // of the grad-h pass kernel
+  int neib_bps = 0;    // of the neighbour-row kernel
+};
+
 struct BlockState {
   bool on = false;
   int nlevels = 1;
@@ -189,6 +200,7 @@ struct Ctx {
   int* acc_ws = nullptr;
 
   BlockState blk;
+  Tuning tune;
 
   // independent clouds (seren_gpu_set_clouds): ncloud > 1 makes every tree
   // build a forest of ncloud trees and the group kernels take gact, the

@@ -263,14 +263,16 @@ struct GwTypes<false> {
 };
 
 // Per-warp shared state: interaction lists, prepared records, popped cells.
-template <bool MIXED>
+// CAPV: accepted-cell entries per list (the cell-list tile; a tuning knob of
+// the mixed-precision kernel, 64 for the FP64 one).
+template <bool MIXED, int CAPV>
 struct GwRec {
   using T = GwTypes<MIXED>;
-  typename T::R4 ca[T::CAP];       // cell: mixed (r_ref - COM, m), FP64 (COM, m)
-  typename T::R4 cb[T::CAP];       // q1..q4
-  typename T::Q5 cq5[T::CAP];
-  int cid[T::CAP];
-  unsigned cmask[T::CAP];
+  typename T::R4 ca[CAPV];         // cell: mixed (r_ref - COM, m), FP64 (COM, m)
+  typename T::R4 cb[CAPV];         // q1..q4
+  typename T::Q5 cq5[CAPV];
+  int cid[CAPV];
+  unsigned cmask[CAPV];
   int qid[GW_PITEMS];
   unsigned qmask[GW_PITEMS];
   typename T::R4 pa[T::PREP];      // particle: mixed (r_q - r_ref, m), FP64 (r_q, m)
@@ -291,7 +293,7 @@ __device__ __forceinline__ int warp_incl(int v, int lane) {
   return v;
 }
 
-template <bool MIXED>
+template <bool MIXED, int CAPV>
 __global__ void __launch_bounds__(GW_THREADS, MIXED ? 5 : 4)
 k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ pm,
             const double2* __restrict__ hz, GravWalk t, const double4* __restrict__ tabG,
@@ -300,10 +302,10 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
             int nsink, const double* __restrict__ sinks,
             int2* __restrict__ stacks, int* work, DevError* err, unsigned long long* counts) {
   using Cfg = GwTypes<MIXED>;
-  constexpr int CAP = Cfg::CAP;
-  __shared__ GwRec<MIXED> srec[GW_WARPS];
+  constexpr int CAP = CAPV;
+  __shared__ GwRec<MIXED, CAPV> srec[GW_WARPS];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  GwRec<MIXED>& R = srec[w];
+  GwRec<MIXED, CAPV>& R = srec[w];
   int2* const S = stacks + (size_t)(blockIdx.x * GW_WARPS + w) * t.scap;
   const unsigned lt = (1u << lane) - 1u;
   unsigned long long ncell = 0, npair = 0, nent = 0;
@@ -739,16 +741,21 @@ GravTree grav_tree(const Ctx& c) { return GravTree{c.link, c.gA, c.gB, c.gC, c.i
 
 }  // namespace
 
-static int grav_blocks_per_sm(int dev, bool mixed) {
-  static int occ[16][2] = {};
-  int dummy[2] = {0, 0};
+// resident blocks per SM of the walk variant (FP64; mixed with a cell-list
+// tile of 64 or 96 entries)
+static int grav_blocks_per_sm(int dev, bool mixed, int cap = 64) {
+  static int occ[16][3] = {};
+  int dummy[3] = {0, 0, 0};
   int* o = dev >= 0 && dev < 16 ? occ[dev] : dummy;
-  int& r = o[mixed ? 1 : 0];
+  const int which = !mixed ? 0 : (cap > 64 ? 2 : 1);
+  int& r = o[which];
   if (r == 0) {
-    if (mixed)
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_grav_walk<true>, GW_THREADS, 0);
+    if (which == 2)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_grav_walk<true, 96>, GW_THREADS, 0);
+    else if (which == 1)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_grav_walk<true, 64>, GW_THREADS, 0);
     else
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_grav_walk<false>, GW_THREADS, 0);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_grav_walk<false, 64>, GW_THREADS, 0);
     if (r < 1) r = 1;
   }
   return r;
@@ -761,7 +768,9 @@ static int sm_count(const Ctx& c) {
 }
 
 int grav_walk_slots(const Ctx& c) {
-  return sm_count(c) * std::max(grav_blocks_per_sm(c.dev, true), grav_blocks_per_sm(c.dev, false)) *
+  return sm_count(c) *
+         std::max(std::max(grav_blocks_per_sm(c.dev, true, 64), grav_blocks_per_sm(c.dev, true, 96)),
+                  grav_blocks_per_sm(c.dev, false)) *
          GW_WARPS;
 }
 
@@ -782,14 +791,22 @@ void launch_grav(Ctx& c, int nact, int nsink, const double* d_sinks, double* ama
     nact = c.ngact;
   }
   const int groups = nb(nact, 32);
-  const int blocks = std::min(sm_count(c) * grav_blocks_per_sm(c.dev, mixed), nb(groups, GW_WARPS));
+  // the tuning knobs: cell-list tile (mixed) and resident blocks per SM
+  const int cap = mixed && c.tune.grav_cap > 64 ? 96 : 64;
+  int bps = grav_blocks_per_sm(c.dev, mixed, cap);
+  if (c.tune.grav_bps > 0) bps = std::min(bps, c.tune.grav_bps);
+  const int blocks = std::min(sm_count(c) * bps, nb(groups, GW_WARPS));
   cudaMemsetAsync(c.work, 0, sizeof(int), c.st);
   if (!mixed)
-    k_grav_walk<false><<<blocks, GW_THREADS, 0, c.st>>>(nact, gl, c.pm, c.hz, gw, c.tabG,
+    k_grav_walk<false, 64><<<blocks, GW_THREADS, 0, c.st>>>(nact, gl, c.pm, c.hz, gw, c.tabG,
+        c.tabG32, c.acc, c.gpot, abase, amap, gmap, nsink, d_sinks, c.wstack, c.work, c.d_err,
+        counts);
+  else if (cap == 96)
+    k_grav_walk<true, 96><<<blocks, GW_THREADS, 0, c.st>>>(nact, gl, c.pm, c.hz, gw, c.tabG,
         c.tabG32, c.acc, c.gpot, abase, amap, gmap, nsink, d_sinks, c.wstack, c.work, c.d_err,
         counts);
   else
-    k_grav_walk<true><<<blocks, GW_THREADS, 0, c.st>>>(nact, gl, c.pm, c.hz, gw, c.tabG,
+    k_grav_walk<true, 64><<<blocks, GW_THREADS, 0, c.st>>>(nact, gl, c.pm, c.hz, gw, c.tabG,
         c.tabG32, c.acc, c.gpot, abase, amap, gmap, nsink, d_sinks, c.wstack, c.work, c.d_err,
         counts);
   ++c.nlaunch;

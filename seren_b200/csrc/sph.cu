@@ -1906,7 +1906,8 @@ void launch_gradh(Ctx& c, int nact) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_gradh_pass, GP_THREADS, 0);
     if (o < 1) o = 1;
   }
-  const int blocks = std::min(sm_count(c) * o, nb(nb(ngrp, 32), GP_WARPS));
+  const int bps = c.tune.gradh_bps > 0 ? std::min(o, c.tune.gradh_bps) : o;
+  const int blocks = std::min(sm_count(c) * bps, nb(nb(ngrp, 32), GP_WARPS));
   cudaMemsetAsync(c.work, 0, 3 * sizeof(int), c.st);     // group counter, nredo, nwide
   k_gradh_pass<<<blocks, GP_THREADS, 0, c.st>>>(
       ngrp, gl, c.pm, c.hz, c.vel, c.rho, c.omega, c.div_v, c.drhodt, c.tabA, c.prm.h_fac,
@@ -1977,7 +1978,8 @@ void launch_neib(Ctx& c, int nact) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_neib_rows, GP_THREADS, 0);
     if (o < 1) o = 1;
   }
-  const int blocks = std::min(sm_count(c) * o, nb(nb(ngrp, 32), GP_WARPS));
+  const int bps = c.tune.neib_bps > 0 ? std::min(o, c.tune.neib_bps) : o;
+  const int blocks = std::min(sm_count(c) * bps, nb(nb(ngrp, 32), GP_WARPS));
   cudaMemsetAsync(c.work, 0, sizeof(int), c.st);          // group counter
   k_neib_rows<<<blocks, GP_THREADS, 0, c.st>>>(ngrp, gl, c.pm, c.hz, t, c.prm.pp_limit,
                                                c.leaves, c.nleaf, c.pptot, c.pplist, c.d_err,
@@ -1992,6 +1994,16 @@ void launch_hydro(Ctx& c, int nact, double* amap) {
   ++c.nlaunch;
   if (c.prm.precision == 0)
     k_hydro<false, 1><<<nb(nact, 128), 128, 0, c.st>>>(
+        nact, c.act, c.pm, c.hz, c.vel, c.rho, c.pf, c.hf4, c.sound, c.pptot, c.pplist,
+        c.prm.pp_limit, hydro_tree(c), c.tabG, c.prm.alpha, c.prm.kernel == 1, c.acc, amap,
+        c.d_err);
+  else if (c.tune.hydro_sub == 2)
+    k_hydro<true, 2><<<nb((long)nact * 2, 128), 128, 0, c.st>>>(
+        nact, c.act, c.pm, c.hz, c.vel, c.rho, c.pf, c.hf4, c.sound, c.pptot, c.pplist,
+        c.prm.pp_limit, hydro_tree(c), c.tabG, c.prm.alpha, c.prm.kernel == 1, c.acc, amap,
+        c.d_err);
+  else if (c.tune.hydro_sub == 8)
+    k_hydro<true, 8><<<nb((long)nact * 8, 128), 128, 0, c.st>>>(
         nact, c.act, c.pm, c.hz, c.vel, c.rho, c.pf, c.hf4, c.sound, c.pptot, c.pplist,
         c.prm.pp_limit, hydro_tree(c), c.tabG, c.prm.alpha, c.prm.kernel == 1, c.acc, amap,
         c.d_err);

@@ -52,7 +52,9 @@ def library(build_if_missing: bool = True) -> C.CDLL:
                            ("block_start", [vp, C.c_void_p]),
                            ("block_step", [vp, C.c_void_p]),
                            ("block_levels", [vp, _ip, C.POINTER(C.c_int64), _ip, _ip]),
-                           ("set_clouds", [vp, C.c_int32, _ip])):
+                           ("set_clouds", [vp, C.c_int32, _ip]),
+                           ("autotune", [vp, C.c_int32, C.c_void_p]),
+                           ("set_tuning", [vp, C.c_void_p])):
             fn = getattr(lib, f"seren_gpu_{name}")
             fn.argtypes = args
             fn.restype = C.c_int
@@ -81,6 +83,16 @@ class BlockState(C.Structure):
                 ("level_max", C.c_int32), ("level_step", C.c_int32), ("nactive", C.c_int32),
                 ("reserved", C.c_int32), ("timestep", C.c_double), ("dt_max", C.c_double),
                 ("time", C.c_double)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_ if n != "reserved"}
+
+
+class Tuning(C.Structure):
+    """seren_gpu_tuning of include/seren_gpu.h."""
+    _fields_ = [("hydro_sub", C.c_int32), ("grav_cap", C.c_int32), ("grav_bps", C.c_int32),
+                ("gradh_bps", C.c_int32), ("neib_bps", C.c_int32), ("reserved", C.c_int32),
+                ("ms_per_step", C.c_double)]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_ if n != "reserved"}
@@ -196,6 +208,19 @@ class GpuHotPath(HotPath):
         """Build the tree every nbuildstep device-resident evaluations and
         restock it in between (seren_gpu_set_build_step)."""
         self._call("set_build_step", self._ctx, int(nbuildstep))
+
+    def autotune(self, trials: int = 2) -> dict:
+        """Time the kernel knobs on the current state (seren_gpu_autotune) and
+        keep the fastest per stage; trials <= 0 applies the choice recorded
+        for this size instead."""
+        t = Tuning()
+        self._call("autotune", self._ctx, int(trials), C.cast(C.byref(t), C.c_void_p))
+        return t.as_dict()
+
+    def set_tuning(self, hydro_sub=4, grav_cap=64, grav_bps=0, gradh_bps=0, neib_bps=0):
+        t = Tuning(int(hydro_sub), int(grav_cap), int(grav_bps), int(gradh_bps), int(neib_bps), 0,
+                   0.0)
+        self._call("set_tuning", self._ctx, C.cast(C.byref(t), C.c_void_p))
 
     def set_clouds(self, counts):
         """The uploaded particles are len(counts) independent clouds, one after

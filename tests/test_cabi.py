@@ -41,7 +41,8 @@ def test_oracle_mirrors_the_abi():
                     "last_step_stats", "get_stream", "fma_peak", "hydro_forces_noalloc",
                     "set_sinks", "timestep", "rk2_step", "set_sink_motion", "get_sinks",
                     "sink_timestep", "accrete", "sink_search", "set_build_step",
-                    "block_start", "block_step", "block_levels", "set_clouds"):
+                    "block_start", "block_step", "block_levels", "set_clouds", "autotune",
+                    "set_tuning"):
             continue          # device-resident path (timestep / rk2 / accretion / block
                               # timesteps: Python restatements in oracle.py), device-buffer
                               # call, GPU-only introspection

@@ -852,3 +852,42 @@ def test_block_timesteps_match_oracle(libs, nlevels, level_mode, check_neib, nbu
         seen_levels.update(np.unique(b.nlevel).tolist())
         seen_active.add(b.nactive)
     assert len(seen_levels) >= 3 and len(seen_active) >= 4     # a real block hierarchy
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_autotune_keeps_results(libs, precision):
+    """seren_gpu_autotune times four configurations of the kernel knobs and
+    keeps the fastest per stage.  FP64 results are the same bit for bit under
+    any knobs; mixed ones within the mixed-precision bars.  A second context
+    of the same size takes the recorded choice with trials = 0, and bad knobs
+    are refused."""
+    from seren_b200.cabi import SerenError
+    ic = case("sphere32k")
+    n = ic["parray"].shape[0]
+    Oracle, Gpu = libs
+    g = Gpu(n, params(ic, precision=precision))
+    g.upload(ic["parray"], ic["v"], ic["sound"] ** 2)
+    g.force_step(first_call=True)
+    g.force_step()
+    before = g.download()
+    t = g.autotune(trials=1)
+    assert t["hydro_sub"] in (2, 4, 8) and t["grav_cap"] in (64, 96) and t["ms_per_step"] > 0
+    g.force_step()
+    after = g.download()
+    assert np.array_equal(after["perm"], before["perm"])
+    if precision == 0:
+        assert np.array_equal(after["a"], before["a"])
+        assert np.array_equal(after["rho"], before["rho"])
+    else:
+        err = rel_rows(after["a"], before["a"])
+        assert np.sqrt(np.mean(err ** 2)) < 1e-5
+    g2 = Gpu(n, params(ic, precision=precision))
+    g2.upload(ic["parray"], ic["v"], ic["sound"] ** 2)
+    g2.force_step(first_call=True)
+    t2 = g2.autotune(trials=0)
+    assert {k: t2[k] for k in t2 if k != "ms_per_step"} == \
+        {k: t[k] for k in t if k != "ms_per_step"}
+    with pytest.raises(SerenError):
+        g2.set_tuning(hydro_sub=3)
+    g.close()
+    g2.close()
