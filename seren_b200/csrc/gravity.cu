@@ -323,12 +323,16 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
     const bool live = p >= 0;
     const int p0 = __shfl_sync(FULLMASK, p, 0);        // every lane takes part
     p = live ? p : p0;
-    if (t.cl) {                                        // the lanes' cloud's tree
+    // the lanes' tree (a forest: their cloud's), as locals so that t stays a
+    // kernel parameter
+    int root = t.root;
+    double rootx = t.rootx, rooty = t.rooty, rootz = t.rootz;
+    if (t.cl) {
       const CloudInfo& C = t.cl[cloud_of(t.cl, t.ncl, p)];
-      t.root = C.cell;
-      t.rootx = C.root[0];
-      t.rooty = C.root[1];
-      t.rootz = C.root[2];
+      root = C.cell;
+      rootx = C.root[0];
+      rooty = C.root[1];
+      rootz = C.root[2];
     }
     const double4 P = pm[p];
     const double2 HZ = hz[p];
@@ -336,8 +340,8 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
     const double rx = __shfl_sync(FULLMASK, P.x, 0);
     const double ry = __shfl_sync(FULLMASK, P.y, 0);
     const double rz = __shfl_sync(FULLMASK, P.z, 0);
-    const float px32 = (float)(P.x - t.rootx), py32 = (float)(P.y - t.rooty),
-                pz32 = (float)(P.z - t.rootz);
+    const float px32 = (float)(P.x - rootx), py32 = (float)(P.y - rooty),
+                pz32 = (float)(P.z - rootz);
     const float ux = (float)(P.x - rx), uy = (float)(P.y - ry), uz = (float)(P.z - rz);
     // A separation formed in FP32 from two offsets to the reference point
     // (d = a - u) carries an error of order 2^-24 |u|, relative 2^-23 |u|/|d|;
@@ -513,7 +517,7 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
     };
 
     const unsigned rootmask = __ballot_sync(FULLMASK, live);
-    if (lane == 0) S[0] = make_int2(t.root, (int)rootmask);
+    if (lane == 0) S[0] = make_int2(root, (int)rootmask);
     int sp = 1;
     long long gent = 0;
     while (sp > 0) {

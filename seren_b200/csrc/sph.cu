@@ -40,17 +40,20 @@ struct HydroTree {
   int ncl;
 };
 
-// In a forest, point t at the tree of particle p's cloud: its root cell, root
-// box and rounding bound.  One tree: nothing changes.
-__device__ __forceinline__ void tree_for(HydroTree& t, int p) {
-  if (!t.cl) return;
+// The tree particle p walks: its root cell, root box, rounding bound and
+// extent - in a forest those of its cloud, else the one tree's.  (A local
+// value, so the tree's pointers stay kernel parameters.)
+struct TreeFrame {
+  int root;
+  double rootx, rooty, rootz;
+  float delta;
+  double rextent;
+};
+
+__device__ __forceinline__ TreeFrame frame_for(const HydroTree& t, int p) {
+  if (!t.cl) return TreeFrame{t.root, t.rootx, t.rooty, t.rootz, t.delta, t.rextent};
   const CloudInfo& C = t.cl[cloud_of(t.cl, t.ncl, p)];
-  t.root = C.cell;
-  t.rootx = C.root[0];
-  t.rooty = C.root[1];
-  t.rootz = C.root[2];
-  t.delta = C.delta;
-  t.rextent = C.rextent;
+  return TreeFrame{C.cell, C.root[0], C.root[1], C.root[2], C.delta, C.rextent};
 }
 
 // Lane i of a group of 32 in an active list: act[i] < 0 pads a cloud's last
@@ -65,10 +68,11 @@ __device__ __forceinline__ int group_particle(int i, int nact, const int* act, b
 
 // BHtree/BHhydro_walk.F90:9-80 (gather or scatter test)
 template <class F>
-__device__ __forceinline__ bool walk_gather_scatter(const HydroTree& t, double rx, double ry,
+__device__ __forceinline__ bool walk_gather_scatter(const HydroTree& t, int root, double rx,
+                                                    double ry,
                                                     double rz, double hrange, DevError* err,
                                                     int who, F&& f) {
-  int c = t.root;
+  int c = root;
   int visits = 0;
   const int cap = t.ctot + 2;
   while (true) {
@@ -209,7 +213,7 @@ __device__ void neib_one(int p, const double4* __restrict__ pm, const double2* _
   const double hsp = (KERNRANGESQD * hp) * hp;
   int cnt = 0;
   int* row = pplist + (size_t)p * L;
-  walk_gather_scatter(t, P.x, P.y, P.z, KERNRANGE * hp, err, p, [&](int q) {
+  walk_gather_scatter(t, frame_for(t, p).root, P.x, P.y, P.z, KERNRANGE * hp, err, p, [&](int q) {
     if (q == p) return;
     const double hq = hz[q].x;
     const double hsq = (KERNRANGESQD * hq) * hq;
@@ -317,12 +321,12 @@ __device__ __forceinline__ int gr_decide(const GrGroup& g, const float4& c, floa
 // new entry count, or -1 when the list or the stack would overflow (nothing
 // beyond the old count is then valid).
 template <class GTest, class Test>
-__device__ int gr_walk(const HydroTree& t, unsigned lanes, int2* S, int scap, GrShared& R,
+__device__ int gr_walk(const HydroTree& t, int root, unsigned lanes, int2* S, int scap, GrShared& R,
                        int lane, int nent, unsigned long long& nvisit, GTest&& gtest,
                        Test&& test) {
   const unsigned lt = (1u << lane) - 1u;
   __syncwarp();
-  if (lane == 0) S[0] = make_int2(t.root, (int)lanes);
+  if (lane == 0) S[0] = make_int2(root, (int)lanes);
   int sp = 1;
   long long gent = 0;
   while (sp > 0) {
@@ -454,21 +458,21 @@ __global__ void __launch_bounds__(GR_THREADS) k_gradh_walk(
     const int i = g * 32 + lane;
     bool live;
     const int p = group_particle(i, nact, act, live);
-    tree_for(t, p);                                    // lanes share one cloud
+    const TreeFrame fr = frame_for(t, p);             // lanes share one cloud
     const double4 P = pm[p];
     const double rx = P.x, ry = P.y, rz = P.z;
-    const float px = (float)(rx - t.rootx), py = (float)(ry - t.rooty), pz = (float)(rz - t.rootz);
+    const float px = (float)(rx - fr.rootx), py = (float)(ry - fr.rooty), pz = (float)(rz - fr.rootz);
     const double Rw = KERNRANGE * (hz[p].x * HMULT);                  // :157-158
     const float R32 = (float)Rw;
     const unsigned lanes = __ballot_sync(FULL, live);
     nwalk += live ? 1u : 0u;
     const GrGroup grp = gr_group(px, py, pz, R32, live);
-    const int nent = gr_walk(t, lanes, S, scap, R, lane, 0, nvisit, [&](const float4& c, float) {
-      return gr_decide(grp, c, grp.rmin, grp.rmax, t.delta);
+    const int nent = gr_walk(t, fr.root, lanes, S, scap, R, lane, 0, nvisit, [&](const float4& c, float) {
+      return gr_decide(grp, c, grp.rmin, grp.rmax, fr.delta);
     }, [&](int e) {
       const float4 h32 = R.fa[e];                      // BHhydrowalk_hgather.F90:36-40
       const float d0 = h32.x - px, d1 = h32.y - py, d2 = h32.z - pz;
-      const int r = test32((d0 * d0 + d1 * d1) + d2 * d2, R32 + h32.w, t.delta);
+      const int r = test32((d0 * d0 + d1 * d1) + d2 * d2, R32 + h32.w, fr.delta);
       if (r >= 0) return r == 1;
       const double4 h = t.hA[R.fc[e]];
       const double e0 = h.x - rx, e1 = h.y - ry, e2 = h.z - rz;
@@ -828,10 +832,10 @@ constexpr int RD_WARPS = RD_THREADS / 32;
 // particular order) or -1 when a buffer of cap entries would overflow; cnt =
 // the particles in the opened leaves (pp_pot).
 template <class Test>
-__device__ int rd_walk(const HydroTree& t, int lane, int* fa, int* fb, int* leaves, int cap,
+__device__ int rd_walk(const HydroTree& t, int root, int lane, int* fa, int* fb, int* leaves, int cap,
                        int& cnt, unsigned long long& nvisit, Test&& test) {
   __syncwarp();
-  if (lane == 0) fa[0] = t.root;
+  if (lane == 0) fa[0] = root;
   __syncwarp();
   int nf = 1, nleaf = 0, mine = 0;
   while (nf > 0) {
@@ -891,11 +895,11 @@ __global__ void __launch_bounds__(RD_THREADS) k_gradh_redo(
   const int nr = *nredo;
   for (int i = gw; i < nr; i += gridDim.x * RD_WARPS) {
     const int p = redo[i];
-    tree_for(t, p);
-    const double rextent = t.cl ? t.rextent : rextent0;
+    const TreeFrame fr = frame_for(t, p);
+    const double rextent = t.cl ? fr.rextent : rextent0;
     const double4 P = pm[p];
     const double rx = P.x, ry = P.y, rz = P.z, mp = P.w;
-    const float px = (float)(rx - t.rootx), py = (float)(ry - t.rooty), pz = (float)(rz - t.rootz);
+    const float px = (float)(rx - fr.rootx), py = (float)(ry - fr.rooty), pz = (float)(rz - fr.rootz);
     GhState s;
     gh_init(s, hz[p].x, rextent);
     double Rw = 0.0;
@@ -903,7 +907,7 @@ __global__ void __launch_bounds__(RD_THREADS) k_gradh_redo(
     auto gather_test = [&](int c) {                    // BHhydrowalk_hgather.F90:36-40
       const float4 h32 = t.hA32[c];
       const float d0 = h32.x - px, d1 = h32.y - py, d2 = h32.z - pz;
-      const int r = test32((d0 * d0 + d1 * d1) + d2 * d2, R32 + h32.w, t.delta);
+      const int r = test32((d0 * d0 + d1 * d1) + d2 * d2, R32 + h32.w, fr.delta);
       if (r >= 0) return r == 1;
       const double4 h = t.hA[c];
       const double e0 = h.x - rx, e1 = h.y - ry, e2 = h.z - rz;
@@ -920,7 +924,7 @@ __global__ void __launch_bounds__(RD_THREADS) k_gradh_redo(
           R32 = (float)Rw;
           int cnt = 0;
           ++nwalk;
-          nl = rd_walk(t, lane, fa, fb, lv, cap, cnt, nvisit, gather_test);
+          nl = rd_walk(t, fr.root, lane, fa, fb, lv, cap, cnt, nvisit, gather_test);
           if (nl < 0) { over = true; break; }
           s.pp_pot = cnt;
         }
@@ -1055,19 +1059,19 @@ __global__ void __launch_bounds__(HG_THREADS) k_hgather(
   unsigned long long nwalk = 0, nvisit = 0;
   for (int i = gw; i < nact; i += gridDim.x * HG_WARPS) {
     const int p = act ? act[i] : i;
-    tree_for(t, p);
-    const double rextent = t.cl ? t.rextent : rextent0;
+    const TreeFrame fr = frame_for(t, p);
+    const double rextent = t.cl ? fr.rextent : rextent0;
     const double rcap = 4.0 * (rextent > 0.0 ? rextent : 1.0);   // a ball that holds every particle
     const double4 P = pm[p];
     const double rx = P.x, ry = P.y, rz = P.z;
-    const float px = (float)(rx - t.rootx), py = (float)(ry - t.rooty), pz = (float)(rz - t.rootz);
+    const float px = (float)(rx - fr.rootx), py = (float)(ry - fr.rooty), pz = (float)(rz - fr.rootz);
     double Rw = KERNRANGE * (HMULT * (HMULT * hz[p].x));    // the reference's first search radius
     if (!(Rw > 0.0) || !isfinite(Rw)) Rw = ldexp(rcap, -12);  // the guess does not change h
     float R32 = 0.0f;
     auto gather_test = [&](int c) {                     // BHhydrowalk_hgather.F90:36-40
       const float4 h32 = t.hA32[c];
       const float d0 = h32.x - px, d1 = h32.y - py, d2 = h32.z - pz;
-      const int r = test32((d0 * d0 + d1 * d1) + d2 * d2, R32 + h32.w, t.delta);
+      const int r = test32((d0 * d0 + d1 * d1) + d2 * d2, R32 + h32.w, fr.delta);
       if (r >= 0) return r == 1;
       const double4 h = t.hA[c];
       const double e0 = h.x - rx, e1 = h.y - ry, e2 = h.z - rz;
@@ -1082,7 +1086,7 @@ __global__ void __launch_bounds__(HG_THREADS) k_hgather(
       R32 = (float)Rw;
       int cnt = 0;
       ++nwalk;
-      const int nl = rd_walk(t, lane, fa, fb, lv, cap, cnt, nvisit, gather_test);
+      const int nl = rd_walk(t, fr.root, lane, fa, fb, lv, cap, cnt, nvisit, gather_test);
       // the opened leaves hold every particle with r <= Rw; count those well
       // inside (r^2 below Rw^2 (1 - 2^-40), clear of the walk's rounding)
       const double rc2 = (Rw * Rw) * (1.0 - 0x1p-40);
@@ -1163,8 +1167,7 @@ __global__ void k_neib_levels(int nact, const int* __restrict__ act, const doubl
   const double4 P = pm[p];
   const double hp = hz[p].x;
   const double hsp = (KERNRANGESQD * hp) * hp;
-  tree_for(t, p);
-  walk_gather_scatter(t, P.x, P.y, P.z, KERNRANGE * hp, err, p, [&](int q) {
+  walk_gather_scatter(t, frame_for(t, p).root, P.x, P.y, P.z, KERNRANGE * hp, err, p, [&](int q) {
     if (q == p) return;
     const double hq = hz[q].x;
     const double hsq = (KERNRANGESQD * hq) * hq;
@@ -1504,24 +1507,24 @@ __global__ void __launch_bounds__(GR_THREADS) k_neib_walk(
     const int i = g * 32 + lane;
     bool live;
     const int p = group_particle(i, nact, act, live);
-    tree_for(t, p);                                    // lanes share one cloud
+    const TreeFrame fr = frame_for(t, p);             // lanes share one cloud
     const double4 P = pm[p];
-    const float px = (float)(P.x - t.rootx), py = (float)(P.y - t.rooty),
-                pz = (float)(P.z - t.rootz);
+    const float px = (float)(P.x - fr.rootx), py = (float)(P.y - fr.rooty),
+                pz = (float)(P.z - fr.rootz);
     const double Rw = KERNRANGE * hz[p].x;
     const float R32 = (float)Rw;
     const unsigned lanes = __ballot_sync(FULL, live);
     const GrGroup grp = gr_group(px, py, pz, R32, live);
-    const int nent = gr_walk(t, lanes, S, scap, R, lane, 0, nvisit, [&](const float4& c, float fh) {
+    const int nent = gr_walk(t, fr.root, lanes, S, scap, R, lane, 0, nvisit, [&](const float4& c, float fh) {
       // gather or scatter (BHhydro_walk.F90:37-43): a lane passes within
       // max(its 2h, hrangemax) + rmax
-      return gr_decide(grp, c, fmaxf(grp.rmin, fh), fmaxf(grp.rmax, fh), t.delta);
+      return gr_decide(grp, c, fmaxf(grp.rmin, fh), fmaxf(grp.rmax, fh), fr.delta);
     }, [&](int e) {
       const float4 h32 = R.fa[e];
       const float d0 = h32.x - px, d1 = h32.y - py, d2 = h32.z - pz;
       const float d2s = (d0 * d0 + d1 * d1) + d2 * d2;
-      const int r1 = test32(d2s, R32 + h32.w, t.delta);
-      const int r2 = test32(d2s, R.fh[e] + h32.w, t.delta);
+      const int r1 = test32(d2s, R32 + h32.w, fr.delta);
+      const int r2 = test32(d2s, R.fh[e] + h32.w, fr.delta);
       if (r1 == 1 || r2 == 1) return true;
       if (r1 == 0 && r2 == 0) return false;
       const int c = R.fc[e];
@@ -1565,7 +1568,6 @@ __global__ void __launch_bounds__(GP_THREADS) k_neib_rows(
     const int i = g * 32 + lane;
     bool live;
     const int p = group_particle(i, nact, act, live);
-    tree_for(t, p);                                    // lanes share one cloud
     const int n = live ? nleaf[p] : 0;
     const double4 P = pm[p];
     const double hp = hz[p].x;
@@ -1767,9 +1769,8 @@ __global__ void __launch_bounds__(128, 8) k_hydro(int nact, const int* __restric
     for (int k = sub; k < nn; k += SUB) pair(row[k]);
   } else if (sub == 0) {
     // get_neib_on_fly (sph/get_neib_on_fly.F90:11-130): same test as get_neib
-    tree_for(t, p);
     const double hsp = (KERNRANGESQD * hp) * hp;
-    walk_gather_scatter(t, P.x, P.y, P.z, KERNRANGE * hp, err, p, [&](int q) {
+    walk_gather_scatter(t, frame_for(t, p).root, P.x, P.y, P.z, KERNRANGE * hp, err, p, [&](int q) {
       if (q == p) return;
       const double hq = hz[q].x;
       const double hsq = (KERNRANGESQD * hq) * hq;

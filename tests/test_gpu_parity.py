@@ -857,10 +857,10 @@ def test_block_timesteps_match_oracle(libs, nlevels, level_mode, check_neib, nbu
 @pytest.mark.parametrize("precision", [0, 1])
 def test_autotune_keeps_results(libs, precision):
     """seren_gpu_autotune times four configurations of the kernel knobs and
-    keeps the fastest per stage.  FP64 results are the same bit for bit under
-    any knobs; mixed ones within the mixed-precision bars.  A second context
-    of the same size takes the recorded choice with trials = 0, and bad knobs
-    are refused."""
+    keeps the fastest per stage.  The same inputs under the tuned knobs and
+    under the defaults give the same FP64 results bit for bit, and mixed ones
+    within the mixed-precision bars.  A second context of the same size takes
+    the recorded choice with trials = 0, and bad knobs are refused."""
     from seren_b200.cabi import SerenError
     ic = case("sphere32k")
     n = ic["parray"].shape[0]
@@ -868,26 +868,34 @@ def test_autotune_keeps_results(libs, precision):
     g = Gpu(n, params(ic, precision=precision))
     g.upload(ic["parray"], ic["v"], ic["sound"] ** 2)
     g.force_step(first_call=True)
-    g.force_step()
-    before = g.download()
     t = g.autotune(trials=1)
+    g.close()
     assert t["hydro_sub"] in (2, 4, 8) and t["grav_cap"] in (64, 96) and t["ms_per_step"] > 0
-    g.force_step()
-    after = g.download()
-    assert np.array_equal(after["perm"], before["perm"])
+    knobs = {k: t[k] for k in ("hydro_sub", "grav_cap", "grav_bps", "gradh_bps", "neib_bps")}
+    runs = []
+    for tuned in (False, True):
+        h = Gpu(n, params(ic, precision=precision))
+        h.upload(ic["parray"], ic["v"], ic["sound"] ** 2)
+        if tuned:
+            h.set_tuning(**knobs)
+        h.force_step(first_call=True)
+        h.drift(1.0e-3)
+        h.force_step()
+        runs.append(h.download())
+        h.close()
+    d0, d1 = runs
+    assert np.array_equal(d0["perm"], d1["perm"])
+    assert np.array_equal(d0["rho"], d1["rho"])               # grad-h is FP64 in both
     if precision == 0:
-        assert np.array_equal(after["a"], before["a"])
-        assert np.array_equal(after["rho"], before["rho"])
+        assert np.array_equal(d0["a"], d1["a"])
     else:
-        err = rel_rows(after["a"], before["a"])
+        err = rel_rows(d1["a"], d0["a"])
         assert np.sqrt(np.mean(err ** 2)) < 1e-5
     g2 = Gpu(n, params(ic, precision=precision))
     g2.upload(ic["parray"], ic["v"], ic["sound"] ** 2)
     g2.force_step(first_call=True)
     t2 = g2.autotune(trials=0)
-    assert {k: t2[k] for k in t2 if k != "ms_per_step"} == \
-        {k: t[k] for k in t if k != "ms_per_step"}
+    assert {k: t2[k] for k in knobs} == knobs
     with pytest.raises(SerenError):
         g2.set_tuning(hydro_sub=3)
-    g.close()
     g2.close()
