@@ -257,7 +257,7 @@ void free_all(Ctx& c) {
                 c.orig_alt, c.rho, c.omega, c.div_v, c.drhodt, c.rho_alt, c.omega_alt, c.div_v_alt,
                 c.drhodt_alt, c.press, c.sound, c.acc, c.gpot,
                 c.pf, c.hf4,
-                c.pptot, c.pplist, c.rec_r2, c.rec_m, c.rec_dv, c.stage, c.istage, c.keys, c.keys_alt, c.keys_hi, c.keys_lo, c.idx, c.idx_alt,
+                c.pptot, c.pplist, c.stage, c.istage, c.keys, c.keys_alt, c.keys_hi, c.keys_lo, c.idx, c.idx_alt,
                 c.rs_hist, c.bbox_part, c.branch, c.branch_next, c.nchild, c.choff, c.cstart,
                 c.bflag, c.bscan, c.leaf, c.nextcell, c.ifopen, c.pstart, c.pcount, c.parent,
                 c.level, c.nkids, c.work, c.sinks, c.wstack, c.leaves, c.nleaf, c.npot, c.redo, c.wide, c.wst, c.wacc, c.link, c.gA, c.gB, c.gC, c.wA, c.hN, c.hA, c.hrm, c.hA32, c.hrm32, c.hmax, c.bbmin, c.bbmax, c.d_info,
@@ -307,7 +307,6 @@ int alloc_all(Ctx& c) {
          alloc(c.pcount, C) | alloc(c.parent, C) | alloc(c.level, C) | alloc(c.link, C);
   bad |= alloc(c.hA32, C) | alloc(c.hrm32, C) | alloc(c.nkids, C) | alloc(c.work, 4);
   bad |= alloc(c.leaves, P * 256) | alloc(c.nleaf, P) | alloc(c.npot, P) | alloc(c.redo, P) | alloc(c.wide, P);
-  bad |= alloc(c.rec_r2, P * L) | alloc(c.rec_m, P * L) | alloc(c.rec_dv, P * L);
   bad |= wide_scratch_alloc(c);
   bad |= alloc(c.gA, C) | alloc(c.gB, C) | alloc(c.gC, C) | alloc(c.wA, 2 * C) | alloc(c.hN, 2 * C) |
          alloc(c.hA, C) | alloc(c.hrm, C) |

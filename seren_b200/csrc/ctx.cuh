@@ -180,11 +180,6 @@ struct Ctx {
   int* nleaf = nullptr;       // their number (-1: overflow)
   int* npot = nullptr;        // [pmax] particles in those leaves (pp_pot)
   int* redo = nullptr;        // [pmax] particles whose grad-h is redone alone; count in work[1]
-  // the grad-h candidates within 2 h_high recorded by the first pass,
-  // [pmax][pp_limit] each: r^2, mass and dv.dr
-  double* rec_r2 = nullptr;
-  double* rec_m = nullptr;
-  double* rec_dv = nullptr;
   int* wide = nullptr;        // [pmax] particles whose grad-h walks cover most of the tree; count in work[2]
   void* wst = nullptr;        // state of a batch of those particles (sph.cu)
   double* wacc = nullptr;     // their walk accumulators, 4 per particle

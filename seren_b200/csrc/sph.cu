@@ -582,9 +582,8 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
     double* __restrict__ divv, double* __restrict__ drhodt, const double4* __restrict__ tabA,
     double h_fac, int pp_gather, double rextent0, const int* __restrict__ leaves,
     const int* __restrict__ nleaf, const int* __restrict__ npot, int* __restrict__ redo,
-    int* __restrict__ nredo, double* __restrict__ rec_r2, double* __restrict__ rec_m,
-    double* __restrict__ rec_dv, int L, DevError* err, unsigned long long* counts, int* work,
-    const CloudInfo* __restrict__ cl, int ncl) {
+    int* __restrict__ nredo, int* __restrict__ prune, int L, DevError* err,
+    unsigned long long* counts, int* work, const CloudInfo* __restrict__ cl, int ncl) {
   __shared__ GpWarp gpw[GP_WARPS];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   GpWarp& W = gpw[w];
@@ -593,12 +592,9 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
 
   // Density sum (:211-235) of particle j over the candidates getq(0..nc): r^2
   // of each; those inside 2h (:218) are packed into the buffer and their terms
-  // summed 32 at a time.  KEEP (first pass): each candidate within 2 h_high is
-  // recorded, in order, in j's row of the records: r^2, mass and dv.dr (the
-  // positions and velocities stay fixed through grad-h, so every later pass
-  // and the final pass read these instead of gathering the particles again).
-  auto dscan = [&](int j, int nc, auto getq, auto u_, auto keep_, int& kept, double& part,
-                   double vxj, double vyj, double vzj) {
+  // summed 32 at a time.  KEEP (first pass): the candidates within 2 h_high
+  // are recorded, in order, in j's row of `prune`.
+  auto dscan = [&](int j, int nc, auto getq, auto u_, auto keep_, int& kept, double& part) {
     constexpr int U = decltype(u_)::value;
     constexpr bool KEEP = decltype(keep_)::value;
     const double xj = W.x[j], yj = W.y[j], zj = W.z[j], hsj = W.hs[j];
@@ -630,14 +626,7 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
           const bool keep = q[u] != pj && drsqd < W.hh[j];
           const unsigned mk = __ballot_sync(FULL, keep);
           const int pos = kept + __popc(mk & lt);
-          if (keep && pos < L) {
-            const size_t o = (size_t)pj * L + pos;
-            const double4 V = vel[q[u]];
-            const double dv0 = V.x - vxj, dv1 = V.y - vyj, dv2 = V.z - vzj;
-            rec_r2[o] = drsqd;
-            rec_m[o] = Q[u].w;
-            rec_dv[o] = (dv0 * d0 + dv1 * d1) + dv2 * d2;                 // :360-365
-          }
+          if (keep && pos < L) prune[(size_t)pj * L + pos] = q[u];
           kept += __popc(mk);
         }
       }
@@ -698,53 +687,6 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
     niter += (nc + 31) >> 5;
   };
 
-  // The same two sums over particle j's nc recorded candidates (r^2, mass,
-  // dv.dr), read 32*U at a time with coalesced loads; FINAL selects the
-  // final-pass test r^2 <= 4h^2 (:360) and terms, else the density pass's
-  // r^2 < 4h^2 (:218).  The candidates inside are packed and evaluated in
-  // record order, as the scans above evaluate them.
-  auto rscan = [&](int j, int nc, auto final_, double& part, GhFinal& fpart) {
-    constexpr bool FINAL = decltype(final_)::value;
-    constexpr int U = 4;
-    const double hsj = W.hs[j];
-    const size_t base = (size_t)W.p[j] * L;
-    int nin = 0;
-    for (int b = 0; b < nc; b += 32 * U) {
-      double r2[U], mm[U], dd[U];
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int k = b + 32 * u + lane;
-        const bool ok = k < nc;
-        r2[u] = ok ? rec_r2[base + k] : INFINITY;
-        mm[u] = ok ? rec_m[base + k] : 0.0;
-        if constexpr (FINAL) dd[u] = ok ? rec_dv[base + k] : 0.0;
-      }
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const bool in = FINAL ? r2[u] <= hsj : r2[u] < hsj;
-        const unsigned mi = __ballot_sync(FULL, in);
-        if (in) {
-          const int o = nin + __popc(mi & lt);
-          W.d2[o] = r2[u];
-          W.m[o] = mm[u];
-          if constexpr (FINAL) W.dv[o] = dd[u];
-        }
-        nin += __popc(mi);
-      }
-      if (nin > GP_PINB - 32 * U || b + 32 * U >= nc) {
-        __syncwarp();
-        const double ihj = W.ih[j], hfj = W.hf[j];
-        for (int t = lane; t < nin; t += 32) {
-          if constexpr (FINAL) gh_final_in(W.d2[t], W.m[t], W.dv[t], ihj, hfj, fpart);
-          else gh_density_in(W.d2[t], W.m[t], ihj, hfj, part);
-        }
-        nin = 0;
-        __syncwarp();
-      }
-    }
-    niter += (nc + 31) >> 5;
-  };
-
   for (int g = gr_next(work, lane); (long long)g * 32 < nact; g = gr_next(work, lane)) {
     const int i = g * 32 + lane;
     bool live;
@@ -752,7 +694,6 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
     const double rextent = cl ? cl[cloud_of(cl, ncl, p)].rextent : rextent0;
     const int n = live ? nleaf[p] : 0;
     const double4 P = pm[p];
-    const double4 vp = vel[p];
     const double mp = P.w;
     GhState s;
     gh_init(s, hz[p].x, rextent);
@@ -765,7 +706,7 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
     W.y[lane] = P.y;
     W.z[lane] = P.z;
     // The candidates within 2 h_high of the particle, recorded in its row of
-    // records by the first pass: every later pass has h <= h_high (else the
+    // `prune` by the first pass: every later pass has h <= h_high (else the
     // particle walks again), so they hold all the candidates it can count.
     W.hh[lane] = (KERNRANGESQD * s.h_high) * s.h_high;
     W.p[lane] = p;
@@ -790,20 +731,17 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
         if (first || nprj < 0) {
           const int nj = W.n[j];
           const int* row = leaves + (size_t)W.p[j] * GH_LEAVES;
-          const double vxj = __shfl_sync(FULL, vp.x, j), vyj = __shfl_sync(FULL, vp.y, j),
-                       vzj = __shfl_sync(FULL, vp.z, j);
           for (int s0 = 0; s0 < nj; s0 += GP_PSEG) {   // the row, GP_PSEG leaves at a time
             const int nc = gp_flatten(row + s0, min(GP_PSEG, nj - s0), W.cand, lane);
             auto fromrow = [&](int k) { return W.cand[k]; };
-            if (first)
-              dscan(j, nc, fromrow, ICst<2>{}, std::true_type{}, kept, part, vxj, vyj, vzj);
-            else
-              dscan(j, nc, fromrow, ICst<2>{}, std::false_type{}, kept, part, vxj, vyj, vzj);
+            if (first) dscan(j, nc, fromrow, ICst<2>{}, std::true_type{}, kept, part);
+            else dscan(j, nc, fromrow, ICst<2>{}, std::false_type{}, kept, part);
           }
           if (first && lane == 0) W.npr[j] = kept <= L ? kept : -1;
         } else {
-          GhFinal unused;
-          rscan(j, nprj, std::false_type{}, part, unused);
+          const int* prj = prune + (size_t)W.p[j] * L;
+          dscan(j, nprj, [&](int k) { return prj[k]; }, ICst<4>{}, std::false_type{}, kept,
+                part);
         }
         const double sum = warp_sum(part);
         if (lane == j) rt = sum;
@@ -826,6 +764,7 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
     const double hp = h_fac * pow(mp / s.rho, ONETHIRD);
     const double ih = 1.0 / hp;
     const double hf = pow(ih, NDIMPR);
+    const double4 vp = vel[p];
     W.ih[lane] = ih;
     W.hf[lane] = hf;
     W.hs[lane] = (KERNRANGESQD * hp) * hp;
@@ -850,8 +789,8 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
           fscan(j, nc, [&](int k) { return W.cand[k]; }, ICst<1>{}, vxj, vyj, vzj, part);
         }
       } else {
-        double unused = 0.0;
-        rscan(j, nprj, std::true_type{}, unused, part);
+        const int* prj = prune + (size_t)W.p[j] * L;
+        fscan(j, nprj, [&](int k) { return prj[k]; }, ICst<2>{}, vxj, vyj, vzj, part);
       }
       const double srt = warp_sum(part.rt), som = warp_sum(part.om), sdv = warp_sum(part.dv),
                    szt = warp_sum(part.zt);
@@ -1974,7 +1913,7 @@ void launch_gradh(Ctx& c, int nact) {
   k_gradh_pass<<<blocks, GP_THREADS, 0, c.st>>>(
       ngrp, gl, c.pm, c.hz, c.vel, c.rho, c.omega, c.div_v, c.drhodt, c.tabA, c.prm.h_fac,
       c.prm.pp_gather, c.info.rextent, c.leaves, c.nleaf, c.npot, c.redo, c.work + 1,
-      c.rec_r2, c.rec_m, c.rec_dv, c.prm.pp_limit, c.d_err, counts, c.work, t.cl, t.ncl);
+      c.pplist, c.prm.pp_limit, c.d_err, counts, c.work, t.cl, t.ncl);
   // three walk-stack slots of scratch per redo warp
   k_gradh_redo<<<std::max(1, (c.wstack_slots / 3) / RD_WARPS), RD_THREADS, 0, c.st>>>(
       c.redo, c.work + 1, c.pm, c.hz, c.vel, c.rho, c.omega, c.div_v, c.drhodt, t, c.tabA,
