@@ -262,19 +262,11 @@ struct GwTypes<false> {
   static constexpr int PREP = 64;
 };
 
-// the mixed kernel's near-field lists of the 8-lane sub-groups (none in FP64)
-template <bool MIXED>
-struct GwSubLists {
-  unsigned char sl[4][GwTypes<true>::PREP];
-};
-template <>
-struct GwSubLists<false> {};
-
 // Per-warp shared state: interaction lists, prepared records, popped cells.
 // CAPV: accepted-cell entries per list (the cell-list tile; a tuning knob of
 // the mixed-precision kernel, 64 for the FP64 one).
 template <bool MIXED, int CAPV>
-struct GwRec : GwSubLists<MIXED> {
+struct GwRec {
   using T = GwTypes<MIXED>;
   typename T::R4 ca[CAPV];         // cell: mixed (r_ref - COM, m), FP64 (COM, m)
   typename T::R4 cb[CAPV];         // q1..q4
@@ -284,6 +276,7 @@ struct GwRec : GwSubLists<MIXED> {
   int qid[GW_PITEMS];
   unsigned qmask[GW_PITEMS];
   typename T::R4 pa[T::PREP];      // particle: mixed (r_q - r_ref, m), FP64 (r_q, m)
+  unsigned char sl[4][MIXED ? T::PREP : 4];   // mixed: the items each 8-lane sub-group needs
   typename T::R2 pb[T::PREP];      // mixed (1/h, zeta), FP64 (h, zeta)
   float4 fw[32];                   // popped cells: wA
   float flo[32];                   // lower MAC bracket
