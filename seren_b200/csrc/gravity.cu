@@ -276,7 +276,7 @@ struct GwRec {
   int qid[GW_PITEMS];
   unsigned qmask[GW_PITEMS];
   typename T::R4 pa[T::PREP];      // particle: mixed (r_q - r_ref, m), FP64 (r_q, m)
-  unsigned char sl[4][MIXED ? T::PREP : 4];   // mixed: the items each 8-lane sub-group needs
+  unsigned char sl[4][T::PREP];    // mixed: the items each 8-lane sub-group needs
   typename T::R2 pb[T::PREP];      // mixed (1/h, zeta), FP64 (h, zeta)
   float4 fw[32];                   // popped cells: wA
   float flo[32];                   // lower MAC bracket
