@@ -276,7 +276,6 @@ struct GwRec {
   int qid[GW_PITEMS];
   unsigned qmask[GW_PITEMS];
   typename T::R4 pa[T::PREP];      // particle: mixed (r_q - r_ref, m), FP64 (r_q, m)
-  unsigned char sl[4][T::PREP];    // mixed: the items each 8-lane sub-group needs
   typename T::R2 pb[T::PREP];      // mixed (1/h, zeta), FP64 (h, zeta)
   float4 fw[32];                   // popped cells: wA
   float flo[32];                   // lower MAC bracket
@@ -473,8 +472,8 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
         __syncwarp();
         if constexpr (MIXED) {
           float sx = 0.f, sy = 0.f, sz = 0.f, sp = 0.f;
-          auto item = [&](int e, bool has, float d0, float d1, float d2) {
-            const bool on = has && ((R.qmask[b0 + e] >> lane) & 1u) && R.qid[b0 + e] != p;
+          auto item = [&](int e, float d0, float d1, float d2) {
+            const bool on = ((R.qmask[b0 + e] >> lane) & 1u) && R.qid[b0 + e] != p;
             const float4 a = R.pa[e];
             const float2 b = R.pb[e];
             const float drsqd = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
@@ -489,43 +488,15 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
             }
           };
           if (!wide) {
-            // Lanes 8k..8k+7 (sub-group k) run the list of the items that any
-            // of them needs, in item order: a lane meets its own items in the
-            // same order as in one list over all items (its sums are
-            // unchanged), and one warp step serves up to four items (a
-            // near-field item is needed by about a quarter of the lanes).
-            int len0 = 0, len1 = 0, len2 = 0, len3 = 0;
-            for (int e0 = 0; e0 < nb; e0 += 32) {
-              const int e = e0 + lane;
-              const unsigned mk = e < nb ? R.qmask[b0 + e] : 0u;
-              const bool n0 = (mk & 0x000000ffu) != 0u, n1 = (mk & 0x0000ff00u) != 0u,
-                         n2 = (mk & 0x00ff0000u) != 0u, n3 = (mk & 0xff000000u) != 0u;
-              const unsigned w0 = __ballot_sync(FULLMASK, n0), w1 = __ballot_sync(FULLMASK, n1),
-                             w2 = __ballot_sync(FULLMASK, n2), w3 = __ballot_sync(FULLMASK, n3);
-              if (n0) R.sl[0][len0 + __popc(w0 & lt)] = (unsigned char)e;
-              if (n1) R.sl[1][len1 + __popc(w1 & lt)] = (unsigned char)e;
-              if (n2) R.sl[2][len2 + __popc(w2 & lt)] = (unsigned char)e;
-              if (n3) R.sl[3][len3 + __popc(w3 & lt)] = (unsigned char)e;
-              len0 += __popc(w0);
-              len1 += __popc(w1);
-              len2 += __popc(w2);
-              len3 += __popc(w3);
-            }
-            __syncwarp();
-            const int sub = lane >> 3;
-            const int mylen = sub == 0 ? len0 : (sub == 1 ? len1 : (sub == 2 ? len2 : len3));
-            const int maxlen = max(max(len0, len1), max(len2, len3));
 #pragma unroll 2
-            for (int t = 0; t < maxlen; ++t) {
-              const bool has = t < mylen;
-              const int e = has ? (int)R.sl[sub][t] : 0;
+            for (int e = 0; e < nb; ++e) {
               const float4 a = R.pa[e];
-              item(e, has, a.x - ux, a.y - uy, a.z - uz);
+              item(e, a.x - ux, a.y - uy, a.z - uz);
             }
           } else {
             for (int e = 0; e < nb; ++e) {
               const double4 Q = pm[R.qid[b0 + e]];
-              item(e, true, (float)(Q.x - P.x), (float)(Q.y - P.y), (float)(Q.z - P.z));
+              item(e, (float)(Q.x - P.x), (float)(Q.y - P.y), (float)(Q.z - P.z));
             }
           }
           kc.add(0, sx); kc.add(1, sy); kc.add(2, sz); kc.add(3, sp);
