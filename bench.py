@@ -60,6 +60,10 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tuning", default="auto",
+                    help="kernel knobs: auto (the autotuner, default), default (the library's "
+                         "defaults) or k=v pairs, e.g. hydro_sub=4,grav_cap=96,grav_bps=0,"
+                         "gradh_bps=0,neib_bps=0 (fixed knobs make ncu captures reproducible)")
     ap.add_argument("--workload", choices=("core", "plummer", "disc", "batched"), default="core",
                     help="core: the turbulent core (default, the headline); plummer: Plummer "
                          "sphere, gravity accuracy over theta^2 in {0.09, 0.25, 0.49}; disc: "
@@ -200,6 +204,26 @@ def params_for(ic, precision):
                        precision=precision)
 
 
+TUNING = "auto"
+
+
+def apply_tuning(g, precision):
+    """The kernel knobs of context g for --tuning: the autotuner's choice (two
+    force steps per configuration on the live state), the defaults, or the
+    given values.  Returns the knobs in use."""
+    if TUNING == "auto":
+        t = g.autotune(trials=2)
+        log(f"[bench] autotune (precision {precision}): {t}")
+        return t
+    knobs = dict(hydro_sub=4, grav_cap=64, grav_bps=0, gradh_bps=0, neib_bps=0)
+    if TUNING != "default":
+        for kv in TUNING.split(","):
+            k, v = kv.split("=")
+            knobs[k.strip()] = int(v)
+    g.set_tuning(**knobs)
+    return dict(knobs, ms_per_step=None)
+
+
 def run_resident(ic, precision, steps, warmup, ws):
     """Device-resident steps; returns timing/stat dict and the final state."""
     import torch
@@ -214,8 +238,7 @@ def run_resident(ic, precision, steps, warmup, ws):
     g.force_step(first_call=True)
     # the project's autotuner picks the kernel knobs for this size on the live
     # state (four configurations, two force steps each), then the warm-up runs
-    tuning = g.autotune(trials=2)
-    log(f"[bench] autotune (precision {precision}): {tuning}")
+    tuning = apply_tuning(g, precision)
     for _ in range(max(warmup, 1) - 1):
         g.drift(DT)
         g.force_step(first_call=False)
@@ -586,7 +609,7 @@ def batched_main(args, ws, rank, local):
     def timed(b, sample_clocks):
         b.step(first_call=True)
         if hasattr(b, "g"):                  # the forest context: the autotuner's knobs
-            log(f"[bench] autotune (forest): {b.g.autotune(trials=2)}")
+            apply_tuning(b.g, 1)
         for _ in range(max(args.warmup, 1) - 1):
             b.step(dt=DT)
         sampler = ClockSampler(local) if sample_clocks else None
@@ -643,7 +666,9 @@ def batched_main(args, ws, rank, local):
 
 
 def main():
+    global TUNING
     args = parse()
+    TUNING = args.tuning
     ws, rank, local = dist_init(args.gpus)
     if args.workload == "batched":
         if args.impl == "reference":
