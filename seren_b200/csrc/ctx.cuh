@@ -183,6 +183,9 @@ struct Ctx {
   int* wide = nullptr;        // [pmax] particles whose grad-h walks cover most of the tree; count in work[2]
   void* wst = nullptr;        // state of a batch of those particles (sph.cu)
   double* wacc = nullptr;     // their walk accumulators, 4 per particle
+  double* wpart = nullptr;        // their partial sums per walk slice (made on first use)
+  double* wpart_brute = nullptr;  // and per particle tile of the passes
+  size_t wpart_brute_cap = 0;
   int2* wstack = nullptr;     // walk stacks, wstack_cap (cell, lane mask) entries per warp slot
   int wstack_cap = 0;
   int wstack_slots = 0;

@@ -1270,7 +1270,7 @@ __device__ __forceinline__ bool wide_brute(const WideState& w) {
 __global__ void __launch_bounds__(WD_THREADS) k_wide_walk(
     int n, const WideState* __restrict__ ws, const double4* __restrict__ pm,
     const double4* __restrict__ vel, HydroTree t, const int* __restrict__ parent,
-    const int* __restrict__ level, int L, int c1, double* __restrict__ acc, DevError* err) {
+    const int* __restrict__ level, int L, int c1, double* __restrict__ part, DevError* err) {
   __shared__ double red[WD_THREADS / 32];
   const int i = blockIdx.x / WD_SLICES, slice = blockIdx.x % WD_SLICES;
   if (i >= n) return;
@@ -1337,15 +1337,17 @@ __global__ void __launch_bounds__(WD_THREADS) k_wide_walk(
       if (cur == stop || cur > t.ctot) break;
     }
   }
+  // this slice's partial sums; k_wide_reduce adds the slices in order
   const double r0 = block_sum(job == WJ_FINAL ? f.rt : s0, red);
-  if (threadIdx.x == 0) atomicAdd(acc + 4 * i, r0);
+  double r1 = 0.0, r2 = 0.0, r3 = 0.0;
   if (job == WJ_FINAL) {
-    const double r1 = block_sum(f.om, red), r2 = block_sum(f.dv, red), r3 = block_sum(f.zt, red);
-    if (threadIdx.x == 0) {
-      atomicAdd(acc + 4 * i + 1, r1);
-      atomicAdd(acc + 4 * i + 2, r2);
-      atomicAdd(acc + 4 * i + 3, r3);
-    }
+    r1 = block_sum(f.om, red);
+    r2 = block_sum(f.dv, red);
+    r3 = block_sum(f.zt, red);
+  }
+  if (threadIdx.x == 0) {
+    double* o = part + ((size_t)i * WD_SLICES + slice) * 4;
+    o[0] = r0; o[1] = r1; o[2] = r2; o[3] = r3;
   }
 }
 
@@ -1356,7 +1358,7 @@ constexpr int BR_Q = 4;          // particles per thread
 __global__ void __launch_bounds__(WD_THREADS) k_wide_brute(int n, const WideState* __restrict__ ws,
                                                            int ptot, const double4* __restrict__ pm,
                                                            const double4* __restrict__ vel,
-                                                           double* __restrict__ acc) {
+                                                           double* __restrict__ part) {
   __shared__ double red[WD_THREADS / 32];
   int qi[BR_Q];
   double4 Q[BR_Q];
@@ -1383,7 +1385,10 @@ __global__ void __launch_bounds__(WD_THREADS) k_wide_brute(int n, const WideStat
         if (drsqd < hs) gh_density_in(drsqd, Q[k].w, ih, hf, s0);
       }
       const double r0 = block_sum(s0, red);
-      if (threadIdx.x == 0 && r0 != 0.0) atomicAdd(acc + 4 * i, r0);
+      if (threadIdx.x == 0) {
+        double* o = part + ((size_t)i * gridDim.x + blockIdx.x) * 4;
+        o[0] = r0; o[1] = 0.0; o[2] = 0.0; o[3] = 0.0;
+      }
     } else {                                                      // :360-425
       const double4 vp = w.v;
       GhFinal f;
@@ -1401,12 +1406,35 @@ __global__ void __launch_bounds__(WD_THREADS) k_wide_brute(int n, const WideStat
       const double r0 = block_sum(f.rt, red), r1 = block_sum(f.om, red),
                    r2 = block_sum(f.dv, red), r3 = block_sum(f.zt, red);
       if (threadIdx.x == 0) {
-        if (r0 != 0.0) atomicAdd(acc + 4 * i, r0);
-        if (r1 != 0.0) atomicAdd(acc + 4 * i + 1, r1);
-        if (r2 != 0.0) atomicAdd(acc + 4 * i + 2, r2);
-        if (r3 != 0.0) atomicAdd(acc + 4 * i + 3, r3);
+        double* o = part + ((size_t)i * gridDim.x + blockIdx.x) * 4;
+        o[0] = r0; o[1] = r1; o[2] = r2; o[3] = r3;
       }
     }
+  }
+}
+
+// The sums of each pending particle's walk or passes of this round: its
+// partials (one per walk slice, or one per particle tile of the passes) added
+// in slice or tile order by one warp - a fixed order, so the results repeat
+// from run to run.
+__global__ void k_wide_reduce(int n, const WideState* __restrict__ ws,
+                              const double* __restrict__ part_walk,
+                              const double* __restrict__ part_brute, int nbrute,
+                              double* __restrict__ acc) {
+  const int i = blockIdx.x;
+  const int lane = threadIdx.x;
+  if (i >= n) return;
+  const WideState& w = ws[i];
+  if (w.job == WJ_DONE) return;
+  const bool brute = wide_brute(w);
+  const int np = brute ? nbrute : WD_SLICES;
+  const double* src = brute ? part_brute + (size_t)i * nbrute * 4 : part_walk + (size_t)i * WD_SLICES * 4;
+  double s[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int b = lane; b < np; b += 32)
+    for (int k = 0; k < 4; ++k) s[k] = s[k] + src[(size_t)b * 4 + k];
+  for (int k = 0; k < 4; ++k) {
+    const double v = warp_sum(s[k]);
+    if (lane == 0) acc[4 * i + k] = v;
   }
 }
 
@@ -1932,6 +1960,23 @@ void launch_gradh(Ctx& c, int nact) {
         break;
       }
     const int round_cap = 4 * GRADH_ITERATION_MAX + 2 * HGROW_CAP + 16;
+    const int nbrute = nb(c.ptot, WD_THREADS * BR_Q);
+    // the partial sums of a batch (made on first use, grown with ptot)
+    const size_t need_walk = (size_t)WD_BATCH * WD_SLICES * 4;
+    const size_t need_brute = (size_t)WD_BATCH * nbrute * 4;
+    if (!c.wpart || c.wpart_brute_cap < need_brute) {
+      if (c.wpart) cudaFree(c.wpart);
+      if (c.wpart_brute) cudaFree(c.wpart_brute);
+      c.wpart = c.wpart_brute = nullptr;
+      c.wpart_brute_cap = 0;
+      if (cudaMalloc(&c.wpart, sizeof(double) * need_walk) != cudaSuccess ||
+          cudaMalloc(&c.wpart_brute, sizeof(double) * need_brute) != cudaSuccess) {
+        cudaGetLastError();
+        k_flag_error<<<1, 1, 0, c.st>>>(c.d_err, SEREN_GPU_ERR_CUDA, KID_GRADH);
+        return;
+      }
+      c.wpart_brute_cap = need_brute;
+    }
     for (int b0 = 0; b0 < nwide; b0 += WD_BATCH) {
       const int n = std::min(WD_BATCH, nwide - b0);
       k_wide_init<<<nb(n, 128), 128, 0, c.st>>>(n, c.wide + b0, c.pm, c.hz, c.vel,
@@ -1941,11 +1986,12 @@ void launch_gradh(Ctx& c, int nact) {
       for (int round = 0;; ++round) {
         k_wide_walk<<<n * WD_SLICES, WD_THREADS, 0, c.st>>>(
             n, static_cast<WideState*>(c.wst), c.pm, c.vel, t, c.parent, c.level, L,
-            c.info.last_cell[L], c.wacc,
-            c.d_err);
-        k_wide_brute<<<nb(c.ptot, WD_THREADS * BR_Q), WD_THREADS, 0, c.st>>>(
-            n, static_cast<WideState*>(c.wst), c.ptot, c.pm, c.vel, c.wacc);
-        ++c.nlaunch;
+            c.info.last_cell[L], c.wpart, c.d_err);
+        k_wide_brute<<<nbrute, WD_THREADS, 0, c.st>>>(
+            n, static_cast<WideState*>(c.wst), c.ptot, c.pm, c.vel, c.wpart_brute);
+        k_wide_reduce<<<n, 32, 0, c.st>>>(n, static_cast<WideState*>(c.wst), c.wpart,
+                                          c.wpart_brute, nbrute, c.wacc);
+        c.nlaunch += 2;
         cudaMemsetAsync(c.work + 3, 0, sizeof(int), c.st);
         k_wide_update<<<nb(n, 128), 128, 0, c.st>>>(
             n, static_cast<WideState*>(c.wst), c.wacc, c.tabA, c.prm.h_fac, c.prm.pp_gather, c.info.rextent, c.hz, c.rho,

@@ -899,3 +899,22 @@ def test_autotune_keeps_results(libs, precision):
     with pytest.raises(SerenError):
         g2.set_tuning(hydro_sub=3)
     g2.close()
+
+
+def test_whole_gpu_gradh_path_repeats_bit_for_bit(libs):
+    """The whole-GPU grad-h path (particles whose walks outgrow the redo
+    kernel's scratch) sums its walk slices and particle tiles in a fixed order:
+    two runs give the same h, rho, omega, div v and drho/dt bit for bit."""
+    ic = case("turb20k")
+    Oracle, Gpu = libs
+    n = ic["parray"].shape[0]
+    runs = []
+    for _ in range(2):
+        g = Gpu(n, params(ic, redo_cap=8))
+        g.upload(ic["parray"], ic["v"], ic["sound"] ** 2)
+        g.force_step(first_call=True)
+        assert g.last_step_stats()[2][8] > 0            # particles on the whole-GPU path
+        runs.append(g.download())
+        g.close()
+    for k in ("parray", "rho", "omega", "a", "gpot"):
+        assert np.array_equal(runs[0][k], runs[1][k]), k
