@@ -531,63 +531,6 @@ __device__ __forceinline__ void gh_final_in(double d2, double m, double dvdr, do
   f.zt = f.zt + ((m * ih) * ih) * kfn::wg(kern);
 }
 
-// The same terms with the kernel arithmetic in FP32 (mixed precision): the
-// r^2 < 4h^2 decisions stay FP64 (made before these are called), the FP64
-// factors that carry the mass and the powers of 1/h are formed once in FP64
-// and cast (their range would overflow FP32 products for tiny h), the bin and
-// the kernel value (the M4 polynomials of kernel_fns.h at the bin centre) are
-// FP32, and each term joins the FP64 sum.
-__device__ __forceinline__ float w0f(int i) {
-  const float s = (2.0f * (float)i + 1.0f) * 1.0e-4f;
-  if (i < kfn::KERN1) return ((1.0f - (1.5f * s) * s) + 0.75f * (s * (s * s))) * 0.318309886f;
-  const float t = 2.0f - s;
-  return (0.25f * (t * (t * t))) * 0.318309886f;
-}
-
-__device__ __forceinline__ float w4f(int i) {
-  const float s = (2.0f * (float)i + 1.0f) * 1.0e-4f;
-  if (i < kfn::KERN1) return (-(3.0f * s) + (2.25f * s) * s) * 0.318309886f;
-  const float t = 2.0f - s;
-  return (-((0.75f * t) * t)) * 0.318309886f;
-}
-
-__device__ __forceinline__ float whf(int i) {
-  const float s = (2.0f * (float)i + 1.0f) * 1.0e-4f;
-  const float s3 = s * (s * s);
-  if (i < kfn::KERN1) return ((-3.0f + (7.5f * s) * s) - 4.5f * s3) * 0.318309886f;
-  return (((-6.0f + 12.0f * s) - (7.5f * s) * s) + 1.5f * s3) * 0.318309886f;
-}
-
-__device__ __forceinline__ float wgf(int i) {
-  const float s = (2.0f * (float)i + 1.0f) * 1.0e-4f;
-  const float s2 = s * s, s4 = s2 * s2, s5 = s4 * s;
-  if (i < kfn::KERN1) return ((1.4f - 2.0f * s2) + 1.5f * s4) - 0.6f * s5;
-  return (((1.6f - 4.0f * s2) + 4.0f * (s2 * s)) - 1.5f * s4) + 0.2f * s5;
-}
-
-__device__ __forceinline__ void gh_density_in32(double d2, double m, float ih, double hf,
-                                                double& rt) {
-  const float drmag = sqrtf((float)d2) + 1.0e-20f;
-  const int kern = (int)((5000.0f * drmag) * ih);
-  if (kern >= KERNTOT) return;
-  rt = rt + (double)((float)(m * hf) * w0f(kern));
-}
-
-__device__ __forceinline__ void gh_final_in32(double d2, double m, double dvdr, float ih,
-                                              double hf, double hfih, double ih2, GhFinal& f) {
-  const float drmag = sqrtf((float)d2) + 1.0e-20f;
-  const int kern = (int)((5000.0f * drmag) * ih);
-  if (kern > KERNTOT) return;
-  const int k = kern < KERNTOT ? kern : KERNTOT - 1;   // bin KERNTOT is s = 2.0001: the values vanish
-  const float a = (float)(m * hf), b = (float)(m * hfih), c = (float)(m * ih2);
-  const float w0 = kern < KERNTOT ? w0f(k) : 0.0f, w4 = kern < KERNTOT ? w4f(k) : 0.0f;
-  const float wh = kern < KERNTOT ? whf(k) : 0.0f, wg = kern < KERNTOT ? wgf(k) : 0.0f;
-  f.rt = f.rt + (double)(a * w0);
-  f.om = f.om + (double)(b * wh);
-  f.dv = f.dv - (double)(((b * (float)dvdr) * w4) / drmag);
-  f.zt = f.zt + (double)(c * wg);
-}
-
 // A particle's row of opened leaves flattened into its candidates, in order;
 // returns the count.
 __device__ __forceinline__ int gp_flatten(const int* __restrict__ row, int n, int* cand,
@@ -633,7 +576,6 @@ struct GpWarp {
 // of :238-285) runs once per lane for all 32; each particle's candidates are
 // shared out over the 32 lanes in turn, 32*U at a time with all their loads
 // issued together (U = 4 for the recorded candidates of the density passes).
-template <bool MIXED>
 __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
     int nact, const int* __restrict__ act, const double4* __restrict__ pm, double2* __restrict__ hz,
     const double4* __restrict__ vel, double* __restrict__ rho, double* __restrict__ omega,
@@ -691,12 +633,7 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
       if (nin > GP_PINB - 32 * U || b + 32 * U >= nc) {
         __syncwarp();
         const double ihj = W.ih[j], hfj = W.hf[j];
-        if constexpr (MIXED) {
-          const float ih32 = (float)ihj;
-          for (int t = lane; t < nin; t += 32) gh_density_in32(W.d2[t], W.m[t], ih32, hfj, part);
-        } else {
-          for (int t = lane; t < nin; t += 32) gh_density_in(W.d2[t], W.m[t], ihj, hfj, part);
-        }
+        for (int t = lane; t < nin; t += 32) gh_density_in(W.d2[t], W.m[t], ihj, hfj, part);
         nin = 0;
         __syncwarp();
       }
@@ -741,15 +678,8 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
       if (nin > GP_PINB - 32 * U || b + 32 * U >= nc) {
         __syncwarp();
         const double ihj = W.ih[j], hfj = W.hf[j];
-        if constexpr (MIXED) {
-          const float ih32 = (float)ihj;
-          const double hfih = hfj * ihj, ih2 = ihj * ihj;
-          for (int t = lane; t < nin; t += 32)
-            gh_final_in32(W.d2[t], W.m[t], W.dv[t], ih32, hfj, hfih, ih2, part);
-        } else {
-          for (int t = lane; t < nin; t += 32)
-            gh_final_in(W.d2[t], W.m[t], W.dv[t], ihj, hfj, part);
-        }
+        for (int t = lane; t < nin; t += 32)
+          gh_final_in(W.d2[t], W.m[t], W.dv[t], ihj, hfj, part);
         nin = 0;
         __syncwarp();
       }
@@ -2002,15 +1932,13 @@ void launch_gradh(Ctx& c, int nact) {
   static int occ[16] = {};
   int& o = occ[c.dev >= 0 && c.dev < 16 ? c.dev : 0];
   if (o == 0) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_gradh_pass<false>, GP_THREADS, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_gradh_pass, GP_THREADS, 0);
     if (o < 1) o = 1;
   }
   const int bps = c.tune.gradh_bps > 0 ? std::min(o, c.tune.gradh_bps) : o;
   const int blocks = std::min(sm_count(c) * bps, nb(nb(ngrp, 32), GP_WARPS));
   cudaMemsetAsync(c.work, 0, 3 * sizeof(int), c.st);     // group counter, nredo, nwide
-  // mixed precision: the kernel arithmetic of the passes in FP32
-  auto pass = c.prm.precision != 0 ? k_gradh_pass<true> : k_gradh_pass<false>;
-  pass<<<blocks, GP_THREADS, 0, c.st>>>(
+  k_gradh_pass<<<blocks, GP_THREADS, 0, c.st>>>(
       ngrp, gl, c.pm, c.hz, c.vel, c.rho, c.omega, c.div_v, c.drhodt, c.tabA, c.prm.h_fac,
       c.prm.pp_gather, c.info.rextent, c.leaves, c.nleaf, c.npot, c.redo, c.work + 1,
       c.pplist, c.prm.pp_limit, c.d_err, counts, c.work, t.cl, t.ncl);
