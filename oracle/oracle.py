@@ -27,7 +27,7 @@ class Counts(C.Structure):
     _fields_ = [(n, C.c_int64) for n in (
         "grav_cells", "grav_pairs", "grav_nodes", "gradh_tests", "gradh_pairs", "gradh_passes",
         "gradh_walks", "gradh_final_tests", "gradh_final_pairs", "neib_tests", "neib_pairs",
-        "hydro_pairs", "hydro_visc")]
+        "hydro_pairs", "hydro_visc", "gradh_bisections")]
 
     def as_dict(self):
         return {n: int(getattr(self, n)) for n, _ in self._fields_}

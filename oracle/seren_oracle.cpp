@@ -855,6 +855,7 @@ struct seren_oracle {
       if (iteration < GRADH_ITERATION_MAX) {                               // :252-281
         h_new = h_fac * std::pow(mp / rhotemp, ONETHIRD);
       } else if (iteration == GRADH_ITERATION_MAX) {
+        lc.gradh_bisections++;
         h_upper = rextent;
         h_lower = 0.0;
         h_new = 0.5 * (h_lower + h_upper);
@@ -1320,12 +1321,14 @@ int seren_oracle_sph_update(seren_oracle* o, int32_t ptot, const int32_t* acclis
       tot.gradh_tests += lc.gradh_tests; tot.gradh_pairs += lc.gradh_pairs;
       tot.gradh_passes += lc.gradh_passes; tot.gradh_walks += lc.gradh_walks;
       tot.gradh_final_tests += lc.gradh_final_tests; tot.gradh_final_pairs += lc.gradh_final_pairs;
+      tot.gradh_bisections += lc.gradh_bisections;
     }
   }
   if (rc_all) return rc_all;
   o->cnt.gradh_tests = tot.gradh_tests; o->cnt.gradh_pairs = tot.gradh_pairs;
   o->cnt.gradh_passes = tot.gradh_passes; o->cnt.gradh_walks = tot.gradh_walks;
   o->cnt.gradh_final_tests = tot.gradh_final_tests; o->cnt.gradh_final_pairs = tot.gradh_final_pairs;
+  o->cnt.gradh_bisections = tot.gradh_bisections;
   auto t1 = clk::now();
   o->update_hmax();
   auto t2 = clk::now();

@@ -43,6 +43,8 @@ typedef struct {
   int64_t neib_pairs;        /* neighbours found (sum of pptot)           */
   int64_t hydro_pairs;       /* hydro pairs inside either kernel          */
   int64_t hydro_visc;        /* of which with dv.dr < 0 (viscosity)       */
+  int64_t gradh_bisections;  /* particles whose iteration reached the
+                                bisection (all_sph_gradh.F90:256-260)     */
 } seren_oracle_counts;
 
 int seren_oracle_create(seren_oracle** o, int64_t pmax, const seren_gpu_params* prm);

@@ -186,6 +186,8 @@ struct Ctx {
   double* wpart = nullptr;        // their partial sums per walk slice (made on first use)
   double* wpart_brute = nullptr;  // and per particle tile of the passes
   size_t wpart_brute_cap = 0;
+  int* wcover = nullptr;          // the cells their walks are spread over (made on first use)
+  int wcover_cap = 0;
   int2* wstack = nullptr;     // walk stacks, wstack_cap (cell, lane mask) entries per warp slot
   int wstack_cap = 0;
   int wstack_slots = 0;

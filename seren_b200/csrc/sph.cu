@@ -882,7 +882,7 @@ __global__ void __launch_bounds__(RD_THREADS) k_gradh_redo(
     double* __restrict__ omega, double* __restrict__ divv, double* __restrict__ drhodt,
     HydroTree t, const double4* __restrict__ tabA, double h_fac, int pp_gather, double rextent0,
     int* __restrict__ scratch, int cap, int* __restrict__ wide, int* __restrict__ nwide,
-    DevError* err, unsigned long long* counts) {
+    int* __restrict__ leaves, DevError* err, unsigned long long* counts) {
   __shared__ int cand_all[RD_WARPS][GP_SEG * LEAFMAX];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   int* cand = cand_all[w];
@@ -960,7 +960,13 @@ __global__ void __launch_bounds__(RD_THREADS) k_gradh_redo(
       continue;
     }
     if (over) {                                        // more than cap leaves or cells a level
-      if (lane == 0) wide[atomicAdd(nwide, 1)] = p;    // k_gradh_wide starts it again
+      // the whole-GPU path takes the particle from here: its state goes to
+      // its leaf row (no longer read once the particle is redone), and its
+      // next step is the counting walk at s.h_high that outgrew the scratch
+      if (lane == 0) {
+        *reinterpret_cast<GhState*>(leaves + (size_t)p * GH_LEAVES) = s;
+        wide[atomicAdd(nwide, 1)] = p;
+      }
       continue;
     }
     const double hp = h_fac * pow(mp / s.rho, ONETHIRD);              // :317-425
@@ -1194,7 +1200,14 @@ __device__ double block_sum(double v, double* sh) {
 // grad-h for the particles whose walks outgrow the redo kernel's scratch (the
 // reference's bisection, :262-275, starts from h_upper = rextent, so its first
 // walks can cover most of the domain).  They are few, so every walk of every
-// such particle is spread over the whole GPU: the host runs rounds of
+// such particle is spread over the whole GPU.  Each continues from the state
+// the redo kernel reached (its next step: the counting walk that outgrew the
+// scratch), and the host runs rounds of
+//   k_wide_settle - the steps whose outcome a bound decides, without a walk:
+//                   a counting walk whose ball holds a whole cell of at least
+//                   pp_gather particles, and bisection passes whose density
+//                   is certainly too high (a lower bound from the particle's
+//                   tree-order neighbours);
 //   k_wide_walk   - each (particle, slice) block walks a slice of a cover of
 //                   the tree (the cells of one level and the leaves above it):
 //                   a cover cell counts only when each ancestor passes the
@@ -1202,12 +1215,14 @@ __device__ double block_sum(double v, double* sh) {
 //                   opened cells), its subtree is walked with the reference's
 //                   stackless loop, and the candidates' count or terms are
 //                   summed into the particle's accumulators;
+//   k_wide_brute  - passes at a large h: the terms of all particles, in tiles;
 //   k_wide_update - each particle takes the reference's next step from them
 //                   (:154-191 walk / grow, :238-285 density update, :317-425
 //                   final pass) and says what its next walk must compute;
-// until no particle has a walk left.  Nothing is stored per candidate; every
-// walk of a pass uses the radius of the particle's last counting walk, so it
-// sees the same candidates.
+// until no particle has a walk left.  Nothing is stored per candidate: a pass
+// at h <= h_high sums exactly the particles within 2h (see wide_within), and
+// the final pass at h >= h_high walks at the radius of the last counting
+// walk, so each sees the reference's candidates.
 constexpr int WD_THREADS = 256;
 
 __global__ void k_flag_error(DevError* err, int code, int where) {
@@ -1230,8 +1245,10 @@ struct WideState {
   int q0, q1;       // the particles of its cloud (all of them for one tree)
 };
 
+// ids: the particles the redo kernel handed over, each with its iteration
+// state in its row of `stash` (the grad-h leaf rows)
 __global__ void k_wide_init(int n, const int* __restrict__ ids, const double4* __restrict__ pm,
-                            const double2* __restrict__ hz, const double4* __restrict__ vel,
+                            const int* __restrict__ stash, const double4* __restrict__ vel,
                             double rextent, int ptot, const CloudInfo* __restrict__ cl, int ncl,
                             WideState* __restrict__ ws, double* __restrict__ acc,
                             unsigned long long* counts) {
@@ -1251,26 +1268,175 @@ __global__ void k_wide_init(int n, const int* __restrict__ ids, const double4* _
     w.q0 = C.pstart;
     w.q1 = C.pstart + C.n;
   }
-  gh_init(w.s, hz[w.p].x, w.rextent);
-  w.job = WJ_COUNT;                 // hp > h_high = 0: the first walk (:154-170)
-  w.s.h_high = w.s.hp * HMULT;
+  w.s = *reinterpret_cast<const GhState*>(stash + (size_t)w.p * GH_LEAVES);
+  w.job = WJ_COUNT;                 // the walk at s.h_high (:154-170)
   for (int k = 0; k < 4; ++k) acc[4 * i + k] = 0.0;
 }
 
 // A pass at h <= h_high (every density pass; the final pass when its h is
-// below h_high) counts exactly the particles within 2h: each lies in a leaf
-// the walk at h_high opened, since the bounding sphere of every cell that
-// holds it holds it.  Those passes run over all particles (k_wide_brute);
-// k_wide_walk keeps the walks that count candidates and the other final passes.
-__device__ __forceinline__ bool wide_brute(const WideState& w) {
+// below h_high) sums exactly the particles within 2h, all of which the
+// reference's candidates (the leaves the walk at h_high opened) hold, since
+// the bounding sphere of every cell that holds one holds it.  Such a pass
+// walks at radius 2h (1 + 2^-20): every leaf holding a particle within 2h
+// passes that walk's test with room to spare for the rounding of the test.
+// At a large h (2h above an eighth of the tree's extent) the terms of all
+// particles are summed instead (k_wide_brute), which then costs less than the
+// walk.  The counting walks and the final pass at h >= h_high walk at 2h_high.
+__device__ __forceinline__ double wide_h(const WideState& w) {
+  return w.job == WJ_PASS ? w.s.hp : w.hp;
+}
+__device__ __forceinline__ bool wide_within(const WideState& w) {
   return w.job == WJ_PASS || (w.job == WJ_FINAL && w.hp < w.s.h_high);
+}
+__device__ __forceinline__ bool wide_brute(const WideState& w) {
+  return wide_within(w) && KERNRANGE * wide_h(w) >= 0.125 * w.rextent;
+}
+__device__ __forceinline__ double wide_radius(const WideState& w) {
+  return wide_within(w) ? (KERNRANGE * wide_h(w)) * (1.0 + 0x1p-20) : KERNRANGE * w.s.h_high;
+}
+
+// The highest cell on the path from the root to particle p whose every
+// particle lies within R of P with room for the rounding of the walk's test
+// (|P - centre| + rmax <= R (1 - 2^-30)); returns its particle count, 0 if no
+// cell on the path qualifies.  A walk at radius R opens every leaf of such a
+// cell: each cell d that holds one of its particles q passes the test
+// |centre_d - P| <= |centre_d - q| + |q - P| <= rmax_d + R.
+__device__ int wide_cover(const HydroTree& t, const int* __restrict__ pcount, int root, int p,
+                          const double4& P, double R) {
+  const double Rm = R * (1.0 - 0x1p-30);
+  int c = root;
+  for (int depth = 0; depth <= 2 * DEEP_LEVELS + 2; ++depth) {
+    const double4 h = t.hA[c];
+    const double d0 = h.x - P.x, d1 = h.y - P.y, d2 = h.z - P.z;
+    if (sqrt((d0 * d0 + d1 * d1) + d2 * d2) + h.w <= Rm) return pcount[c];
+    const int4 lk = t.link[c];
+    if (lk.x != 0) return 0;                           // a leaf: nothing below
+    const int first = lk.z, nk = t.nkids[c];
+    int next = -1;
+    for (int k = 0; k < nk; ++k) {                     // the child whose range holds p
+      const int ch = first + k;
+      const int s = t.link[ch].w;
+      if (p >= s && p < s + pcount[ch]) {
+        next = ch;
+        break;
+      }
+    }
+    if (next < 0) return 0;
+    c = next;
+  }
+  return 0;
+}
+
+// The steps of each pending particle that a bound decides, taken here without
+// a walk (one block per particle):
+//  * a counting walk (:154-170) whose ball covers a whole cell of at least
+//    pp_gather particles: pp_pot is at least that count, so the reference's
+//    next step is the pass at the same h (:175-191);
+//  * a bisection pass (GRADH_ITERATION_MAX < iteration < 2 GRADH_ITERATION_MAX)
+//    whose density is certainly large: every term of the sum (:211-235) is
+//    non-negative, so the self term plus the terms of the WS_THREADS particles
+//    nearest in tree order (those of them within 2h) bound it from below, up
+//    to the rounding of either sum (covered by a factor 1 - 1e-6).  When that
+//    bound already puts h_fac (m/rho)^(1/3) below h (1 - H_CON) (no
+//    convergence, :246) and makes h^3 - h_fac^3 m/rho positive (:263-268),
+//    the pass's outcome is h_upper = h, h = (h_lower + h_upper)/2 whatever
+//    the full sum; such passes are taken one after another until one is not
+//    decided.  The density of a decided pass is never read: the loop ends
+//    only after a full pass.
+constexpr int WS_THREADS = 256;
+__global__ void __launch_bounds__(WS_THREADS) k_wide_settle(
+    int n, WideState* __restrict__ ws, const double4* __restrict__ pm, HydroTree t,
+    const int* __restrict__ pcount, const double4* __restrict__ tabA, double h_fac,
+    int pp_gather, unsigned long long* counts) {
+  __shared__ double red[WS_THREADS / 32];
+  __shared__ int cover;
+  const int i = blockIdx.x;
+  if (i >= n) return;
+  WideState& w = ws[i];
+  int job = w.job;
+  GhState s = w.s;
+  const bool bisecting = s.iteration > GRADH_ITERATION_MAX && s.iteration < 2 * GRADH_ITERATION_MAX;
+  if (job != WJ_COUNT && !(job == WJ_PASS && bisecting)) return;  // block-uniform
+  const int p = w.p;
+  const double4 P = w.P;
+  const double mp = P.w;
+  bool changed = false;
+  if (job == WJ_COUNT) {
+    if (threadIdx.x == 0)
+      cover = wide_cover(t, pcount, frame_for(t, p).root, p, P, KERNRANGE * s.h_high);
+    __syncthreads();
+    if (cover < pp_gather) return;                                 // the walk counts
+    s.pp_pot = cover;
+    job = WJ_PASS;
+    changed = true;
+  }
+  const int q = p - WS_THREADS / 2 + (int)threadIdx.x;
+  const bool use = q >= w.q0 && q < w.q1 && q != p;
+  double d2 = 0.0, m = 0.0;
+  if (use) {
+    const double4 Q = pm[q];
+    const double d0 = Q.x - P.x, d1 = Q.y - P.y, e2 = Q.z - P.z;   // as the passes form it
+    d2 = (d0 * d0 + d1 * d1) + e2 * e2;
+    m = Q.w;
+  }
+  const double w00 = tabA[0].x;
+  const double hfac3 = pow(h_fac, NDIMPR);
+  unsigned long long nset = 0;
+  while (s.iteration > GRADH_ITERATION_MAX && s.iteration < 2 * GRADH_ITERATION_MAX) {
+    const double ih = 1.0 / s.hp;
+    const double hf = pow(ih, NDIMPR);
+    const double hs = (KERNRANGESQD * s.hp) * s.hp;
+    double part = 0.0;
+    if (use && d2 < hs) gh_density_in(d2, m, ih, hf, part);
+    const double lb = ((mp * w00) * hf + block_sum(part, red)) * (1.0 - 1e-6);
+    if (!(lb > SMALL_NUMBER)) break;
+    const bool noconv = h_fac * pow(mp / lb, ONETHIRD) * (1.0 + 1e-6) <
+                        (s.hp * (1.0 - H_CON)) * (1.0 - 1e-6);
+    const bool fbpos = lb > ((hfac3 * mp) / pow(s.hp, NDIMPR)) * (1.0 + 1e-6);
+    if (!(noconv && fbpos)) break;
+    s.rho = lb;
+    s.h_upper = s.hp;
+    s.hp = 0.5 * (s.h_lower + s.h_upper);
+    s.iteration = s.iteration + 1;
+    ++nset;
+    changed = true;
+  }
+  if (threadIdx.x == 0 && changed) {
+    w.s = s;
+    w.job = job;
+    w.ih = 1.0 / s.hp;                                             // :199-210
+    w.hf = pow(w.ih, NDIMPR);
+    w.hs = (KERNRANGESQD * s.hp) * s.hp;
+    if (nset) atomicAdd(counts + 5, nset);
+  }
+}
+
+// The cover the walks are spread over: the cells of at most WD_COVER
+// particles whose parent holds more (or that are a root).  Every particle lies
+// in exactly one of them (the first cell of at most WD_COVER particles on the
+// path from its root), and no thread walks a subtree of more than WD_COVER
+// particles, however unevenly the particles fill the tree.
+constexpr int WD_COVER = 256;
+__global__ void k_wide_cover_mark(int ctot, const int* __restrict__ pcount,
+                                  const int* __restrict__ parent, int* __restrict__ flag) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c > ctot) return;
+  const int a = parent[c];
+  flag[c] = pcount[c] <= WD_COVER && (a < 0 || pcount[a] > WD_COVER) ? 1 : 0;
+}
+
+// the flagged cells in cell order: out[scan[c]] = c
+__global__ void k_wide_cover_list(int ctot, const int* __restrict__ flag,
+                                  const int* __restrict__ scan, int* __restrict__ out) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c <= ctot && flag[c]) out[scan[c]] = c;
 }
 
 // one walk per pending particle, WD_SLICES blocks each
 __global__ void __launch_bounds__(WD_THREADS) k_wide_walk(
     int n, const WideState* __restrict__ ws, const double4* __restrict__ pm,
     const double4* __restrict__ vel, HydroTree t, const int* __restrict__ parent,
-    const int* __restrict__ level, int L, int c1, double* __restrict__ part, DevError* err) {
+    const int* __restrict__ cover, int ncover, double* __restrict__ part, DevError* err) {
   __shared__ double red[WD_THREADS / 32];
   const int i = blockIdx.x / WD_SLICES, slice = blockIdx.x % WD_SLICES;
   if (i >= n) return;
@@ -1279,7 +1445,7 @@ __global__ void __launch_bounds__(WD_THREADS) k_wide_walk(
   if (job == WJ_DONE || wide_brute(w)) return;                   // block-uniform
   const int p = w.p;
   const double rx = w.P.x, ry = w.P.y, rz = w.P.z;
-  const double hrange = KERNRANGE * w.s.h_high;
+  const double hrange = wide_radius(w);
   const double hs = w.hs, ih = w.ih, hf = w.hf;
   const double4 vp = w.v;
   auto pass = [&](int c) {                             // BHhydrowalk_hgather.F90:36-40
@@ -1292,10 +1458,9 @@ __global__ void __launch_bounds__(WD_THREADS) k_wide_walk(
   GhFinal f;
   f.rt = 0.0; f.om = 0.0; f.dv = 0.0; f.zt = 0.0;
   const int stride = WD_SLICES * WD_THREADS;
-  for (int c = slice * WD_THREADS + threadIdx.x; c <= c1; c += stride) {
-    const int lv = level[c];
+  for (int k = slice * WD_THREADS + threadIdx.x; k < ncover; k += stride) {
+    const int c = cover[k];
     const int4 lk = t.link[c];
-    if (!(lv == L || (lv < L && lk.x > 0))) continue;
     if (lk.w < w.q0 || lk.w >= w.q1) continue;                  // another cloud's tree
     bool reach = true;
     for (int a = parent[c]; a >= 0 && reach; a = parent[a]) reach = pass(a);
@@ -1362,15 +1527,19 @@ __global__ void __launch_bounds__(WD_THREADS) k_wide_brute(int n, const WideStat
   __shared__ double red[WD_THREADS / 32];
   int qi[BR_Q];
   double4 Q[BR_Q];
-#pragma unroll
-  for (int k = 0; k < BR_Q; ++k) {
-    const long q = (long)blockIdx.x * (WD_THREADS * BR_Q) + k * WD_THREADS + threadIdx.x;
-    qi[k] = q < ptot ? (int)q : -1;
-    Q[k] = q < ptot ? pm[q] : make_double4(0.0, 0.0, 0.0, 0.0);
-  }
+  bool loaded = false;
   for (int i = 0; i < n; ++i) {
     const WideState& w = ws[i];
     if (!wide_brute(w)) continue;                                 // block-uniform
+    if (!loaded) {                       // the tile, once a particle needs it
+#pragma unroll
+      for (int k = 0; k < BR_Q; ++k) {
+        const long q = (long)blockIdx.x * (WD_THREADS * BR_Q) + k * WD_THREADS + threadIdx.x;
+        qi[k] = q < ptot ? (int)q : -1;
+        Q[k] = q < ptot ? pm[q] : make_double4(0.0, 0.0, 0.0, 0.0);
+      }
+      loaded = true;
+    }
     const int p = w.p;
     const int q0 = w.q0, q1 = w.q1;
     const double rx = w.P.x, ry = w.P.y, rz = w.P.z;
@@ -1947,18 +2116,12 @@ void launch_gradh(Ctx& c, int nact) {
       c.redo, c.work + 1, c.pm, c.hz, c.vel, c.rho, c.omega, c.div_v, c.drhodt, t, c.tabA,
       c.prm.h_fac, c.prm.pp_gather, c.info.rextent, reinterpret_cast<int*>(c.wstack),
       c.prm.redo_cap > 0 ? std::min(c.prm.redo_cap, 2 * c.wstack_cap) : 2 * c.wstack_cap,
-      c.wide, c.work + 2, c.d_err, counts);
+      c.wide, c.work + 2, c.leaves, c.d_err, counts);
   // the particles whose walks outgrew the redo kernel's scratch: rounds of
   // whole-GPU walks until each has taken its last step
   int nwide = 0;
   read_dev(c, c.work + 2, &nwide, sizeof(int));
   if (nwide > 0) {
-    int L = c.info.ltot;                         // cover: a level with a cell per thread
-    for (int l = 0; l <= c.info.ltot; ++l)
-      if (c.info.last_cell[l] - c.info.first_cell[l] + 1 >= WD_SLICES * WD_THREADS) {
-        L = l;
-        break;
-      }
     const int round_cap = 4 * GRADH_ITERATION_MAX + 2 * HGROW_CAP + 16;
     const int nbrute = nb(c.ptot, WD_THREADS * BR_Q);
     // the partial sums of a batch (made on first use, grown with ptot)
@@ -1977,16 +2140,40 @@ void launch_gradh(Ctx& c, int nact) {
       }
       c.wpart_brute_cap = need_brute;
     }
+    // the cover of the tree the walks are spread over (k_wide_cover_mark),
+    // listed in cell order through the build's flag and scan scratch
+    const int ncell = c.info.ctot + 1;
+    if (c.wcover_cap < ncell) {
+      if (c.wcover) cudaFree(c.wcover);
+      c.wcover = nullptr;
+      c.wcover_cap = 0;
+      if (cudaMalloc(&c.wcover, sizeof(int) * ((size_t)c.cmax + 1)) != cudaSuccess) {
+        cudaGetLastError();
+        k_flag_error<<<1, 1, 0, c.st>>>(c.d_err, SEREN_GPU_ERR_CUDA, KID_GRADH);
+        return;
+      }
+      c.wcover_cap = c.cmax + 1;
+    }
+    k_wide_cover_mark<<<nb(ncell, 256), 256, 0, c.st>>>(c.info.ctot, c.pcount, c.parent, c.bflag);
+    scan_exclusive(c, c.bflag, c.bscan, ncell);
+    k_wide_cover_list<<<nb(ncell, 256), 256, 0, c.st>>>(c.info.ctot, c.bflag, c.bscan, c.wcover);
+    c.nlaunch += 2;
+    int ncover = 0;
+    read_dev(c, c.scan.total, &ncover, sizeof(int));
     for (int b0 = 0; b0 < nwide; b0 += WD_BATCH) {
       const int n = std::min(WD_BATCH, nwide - b0);
-      k_wide_init<<<nb(n, 128), 128, 0, c.st>>>(n, c.wide + b0, c.pm, c.hz, c.vel,
+      k_wide_init<<<nb(n, 128), 128, 0, c.st>>>(n, c.wide + b0, c.pm, c.leaves, c.vel,
                                                   c.info.rextent, c.ptot, t.cl, t.ncl,
                                                   static_cast<WideState*>(c.wst), c.wacc, counts);
       ++c.nlaunch;
       for (int round = 0;; ++round) {
+        k_wide_settle<<<n, WS_THREADS, 0, c.st>>>(n, static_cast<WideState*>(c.wst), c.pm, t,
+                                                   c.pcount, c.tabA, c.prm.h_fac,
+                                                   c.prm.pp_gather, counts);
+        ++c.nlaunch;
         k_wide_walk<<<n * WD_SLICES, WD_THREADS, 0, c.st>>>(
-            n, static_cast<WideState*>(c.wst), c.pm, c.vel, t, c.parent, c.level, L,
-            c.info.last_cell[L], c.wpart, c.d_err);
+            n, static_cast<WideState*>(c.wst), c.pm, c.vel, t, c.parent, c.wcover, ncover,
+            c.wpart, c.d_err);
         k_wide_brute<<<nbrute, WD_THREADS, 0, c.st>>>(
             n, static_cast<WideState*>(c.wst), c.ptot, c.pm, c.vel, c.wpart_brute);
         k_wide_reduce<<<n, 32, 0, c.st>>>(n, static_cast<WideState*>(c.wst), c.wpart,

@@ -94,6 +94,44 @@ def test_whole_gpu_gradh_path_matches_oracle(libs):
     assert g2.last_step_stats()[2][8] > 0           # particles on the whole-GPU path
 
 
+@pytest.mark.parametrize("name,redo_cap,wide", [("clumps12k", 8, True), ("clumps12k", 0, False),
+                                                ("disc100k", 0, True)])
+def test_gradh_bisection_matches_oracle(libs, name, redo_cap, wide):
+    """Cases whose first call (h guess) takes some particles' grad-h iteration
+    to the reference's bisection (all_sph_gradh.F90:256-275), which restarts
+    from h_upper = rextent: three dense clumps, and the protostellar disc with
+    its sink at N = 100,000.  In the clumps the redo kernel's scratch holds
+    the whole tree's leaves, so it runs the bisection itself; with redo_cap = 8,
+    and in the disc, the walks at h ~ rextent outgrow it and those particles
+    continue on the whole-GPU path, where the bisection passes that a lower
+    bound on the density decides, and the counting walks whose ball covers a
+    whole cell of pp_gather particles, are taken without a walk, and the other
+    passes walk at radius 2h.  The results are the oracle's."""
+    ic = case(name) if name == "clumps12k" else ics.protostellar_disc(n=100000, seed=5)
+    o, g = _pair(libs, ic, redo_cap=redo_cap)
+    ro = run_pipeline(o, ic)
+    assert o.counts()["gradh_bisections"] > 0          # the case reaches the bisection
+    rg = run_pipeline(g, ic)
+    so, sg = ro["sph"], rg["sph"]
+    assert rel_rows(sg["parray"][:, 4], so["parray"][:, 4]).max() < TOL
+    for k in ("rho", "omega"):
+        assert rel_rows(sg[k], so[k]).max() < TOL, k
+    for k in ("div_v", "drhodt"):
+        assert rel_scaled(sg[k], so[k]) < TOL, k
+    L = g.params.pp_limit
+    assert lists_equal(so["pptot"], so["pplist"], sg["pptot"], sg["pplist"], L)
+    assert rel_rows(rg["a"], ro["a"]).max() < 1e-11
+    Oracle, Gpu = libs
+    n = ic["parray"].shape[0]
+    g2 = Gpu(n, params(ic, redo_cap=redo_cap))
+    g2.upload(ic["parray"], ic["v"], ic["sound"] ** 2)
+    if ic.get("sink") is not None:
+        g2.set_sinks(ic["sink"])
+    g2.force_step(first_call=True)
+    assert (g2.last_step_stats()[2][8] > 0) == wide      # particles on the whole-GPU path
+    g2.close()
+
+
 @pytest.mark.parametrize("name", ["sphere4k", "plummer16k", "disc12k"])
 def test_neighbour_lists_at_oracle_h(libs, name):
     """get_neib at the same h is bit-exact (sph/get_neib.F90:83-118)."""
