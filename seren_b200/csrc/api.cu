@@ -845,7 +845,7 @@ int force_step_body(Ctx& c, int first_call, const IoPlan* io, bool block = false
       cudaMemcpyAsync(io->omega, c.omega, sizeof(double) * N, cudaMemcpyDeviceToHost, c.st_io);
   }
   launch_update_hmax(c);
-  launch_neib(c, nact);
+  launch_neib(c, nact, false);                // the lists stay on the device
   cudaEventRecord(c.ev[3], c.st);
   launch_thermal(c);
   launch_hydro(c, nact);

@@ -186,6 +186,7 @@ struct Ctx {
   double* wpart = nullptr;        // their partial sums per walk slice (made on first use)
   double* wpart_brute = nullptr;  // and per particle tile of the passes
   size_t wpart_brute_cap = 0;
+  bool gsets = false;             // the last grad-h recorded the gather neighbours (launch_neib)
   int* wcover = nullptr;          // the cells their walks are spread over (made on first use)
   int wcover_cap = 0;
   int2* wstack = nullptr;     // walk stacks, wstack_cap (cell, lane mask) entries per warp slot
@@ -273,7 +274,11 @@ int rk_alloc(Ctx& c);                 // r_old, v_old, v_half (and their reorder
 // sph.cu
 void launch_gradh(Ctx& c, int nact);
 void launch_hgather(Ctx& c, int nact);  // h_gather (standard SPH)
-void launch_neib(Ctx& c, int nact);
+// sorted = false: right after grad-h with every particle active, the rows
+// hold the reference's neighbours and counts in a fixed order of their own
+// (the device's own hydro forces do not depend on it beyond rounding); true:
+// in the reference's order, for lists the caller reads
+void launch_neib(Ctx& c, int nact, bool sorted = true);
 void launch_hydro(Ctx& c, int nact, double* amap = nullptr);   // amap: mapped host a (optional)
 void launch_thermal(Ctx& c);
 int hydro_walk_slots(const Ctx& c);     // resident warps of the grad-h / neighbour grids

@@ -10,6 +10,7 @@
 // from the reference's in the order of their terms.  The hydro force kernel
 // gives one thread to one particle and follows hydro_gradh step by step.
 #include <algorithm>
+#include <climits>
 #include <mutex>
 #include <tuple>
 #include <type_traits>
@@ -567,6 +568,7 @@ struct GpWarp {
   double hs[32], ih[32], hf[32];   // (2h)^2, 1/h, 1/h^3 of the pass in progress
   double hh[32];                   // (2 h_high)^2: radius of the recorded candidates
   int p[32], n[32], npr[32];       // particle, leaves in its row, recorded candidates (-1: none)
+  unsigned cpl;                    // lanes whose final-pass candidates hold every particle within 2h
   int cand[GP_PSEG * LEAFMAX];
   double d2[GP_PINB], m[GP_PINB], dv[GP_PINB];
 };
@@ -581,9 +583,10 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
     const double4* __restrict__ vel, double* __restrict__ rho, double* __restrict__ omega,
     double* __restrict__ divv, double* __restrict__ drhodt, const double4* __restrict__ tabA,
     double h_fac, int pp_gather, double rextent0, const int* __restrict__ leaves,
-    const int* __restrict__ nleaf, const int* __restrict__ npot, int* __restrict__ redo,
+    const int* __restrict__ nleaf, int* __restrict__ npot, int* __restrict__ redo,
     int* __restrict__ nredo, int* __restrict__ prune, int L, DevError* err,
-    unsigned long long* counts, int* work, const CloudInfo* __restrict__ cl, int ncl) {
+    unsigned long long* counts, int* work, const CloudInfo* __restrict__ cl, int ncl, int rec,
+    int* __restrict__ pptot) {
   __shared__ GpWarp gpw[GP_WARPS];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   GpWarp& W = gpw[w];
@@ -644,7 +647,7 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
   // Final-pass sums (:360-425) of particle j over the candidates getq(0..nc),
   // its velocity vj
   auto fscan = [&](int j, int nc, auto getq, auto u_, double vxj, double vyj, double vzj,
-                   GhFinal& part) {
+                   GhFinal& part, int& gcnt) {
     constexpr int U = decltype(u_)::value;
     const double xj = W.x[j], yj = W.y[j], zj = W.z[j], hsj = W.hs[j];
     const int pj = W.p[j];
@@ -672,11 +675,18 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
           W.d2[o] = drsqd;
           W.m[o] = Q[u].w;
           W.dv[o] = (dv0 * d0 + dv1 * d1) + dv2 * d2;
+          // the gather neighbours r^2 <= 4h^2 of the neighbour lists, in
+          // order, into the particle's own row of prune: each goes to a slot
+          // at or before the candidate it came from, whose read is done (the
+          // ballot above waits for every lane's candidate), so no candidate
+          // still to be read is overwritten
+          if (rec && gcnt + o < L) prune[(size_t)pj * L + gcnt + o] = q[u];
         }
         nin += __popc(mi);
       }
       if (nin > GP_PINB - 32 * U || b + 32 * U >= nc) {
         __syncwarp();
+        gcnt += nin;
         const double ihj = W.ih[j], hfj = W.hf[j];
         for (int t = lane; t < nin; t += 32)
           gh_final_in(W.d2[t], W.m[t], W.dv[t], ihj, hfj, part);
@@ -771,6 +781,7 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
     // the recorded candidates serve when 2h < 2 h_high (those within 2h of the
     // final h are among them)
     if (!(hp < s.h_high)) W.npr[lane] = -1;
+    const unsigned cplm = __ballot_sync(FULL, hp < s.h_high);
     __syncwarp();
     GhFinal f;
     gh_final_init(f, mp, ih, hf, tabA[0]);
@@ -781,16 +792,29 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
       const int nprj = W.npr[j];
       GhFinal part;
       part.rt = 0.0; part.om = 0.0; part.dv = 0.0; part.zt = 0.0;
+      int gcnt = 0;
       if (nprj < 0) {
         const int nj = W.n[j];
         const int* row = leaves + (size_t)W.p[j] * GH_LEAVES;
         for (int s0 = 0; s0 < nj; s0 += GP_PSEG) {     // the row, GP_PSEG leaves at a time
           const int nc = gp_flatten(row + s0, min(GP_PSEG, nj - s0), W.cand, lane);
-          fscan(j, nc, [&](int k) { return W.cand[k]; }, ICst<1>{}, vxj, vyj, vzj, part);
+          fscan(j, nc, [&](int k) { return W.cand[k]; }, ICst<1>{}, vxj, vyj, vzj, part, gcnt);
         }
       } else {
         const int* prj = prune + (size_t)W.p[j] * L;
-        fscan(j, nprj, [&](int k) { return prj[k]; }, ICst<2>{}, vxj, vyj, vzj, part);
+        fscan(j, nprj, [&](int k) { return prj[k]; }, ICst<2>{}, vxj, vyj, vzj, part, gcnt);
+      }
+      // the gather count (the row's first entries; pptot grows with the
+      // scatter neighbours later), or -1 when the candidates may miss some
+      // particle within 2h (h >= h_high: the neighbour walk completes the row)
+      if (rec && lane == 0) {
+        const int pj = W.p[j];
+        if ((cplm >> j) & 1u) {
+          npot[pj] = gcnt;
+          pptot[pj] = gcnt;
+        } else {
+          npot[pj] = -1;
+        }
       }
       const double srt = warp_sum(part.rt), som = warp_sum(part.om), sdv = warp_sum(part.dv),
                    szt = warp_sum(part.zt);
@@ -809,6 +833,7 @@ __global__ void __launch_bounds__(GP_THREADS, 8) k_gradh_pass(
     if (single) {
       ++nsingle;
       redo[atomicAdd(nredo, 1)] = p;
+      if (rec) npot[p] = -1;                       // its neighbour list: from a walk
     }
   }
   atomicAdd(counts + 5, (unsigned long long)npass);
@@ -2088,9 +2113,13 @@ static const int* group_list(const Ctx& c, int& nact) {
 }
 
 void launch_gradh(Ctx& c, int nact) {
+  c.gsets = false;
   if (nact <= 0) return;
   unsigned long long* counts = reinterpret_cast<unsigned long long*>(c.d_counts);
   const HydroTree t = hydro_tree(c);
+  // with every particle active, the final passes record each particle's
+  // gather neighbours for the neighbour lists that follow (launch_neib)
+  const bool rec = c.act == nullptr;
   int ngrp = nact;
   const int* gl = group_list(c, ngrp);
   cudaMemsetAsync(c.work, 0, sizeof(int), c.st);
@@ -2110,7 +2139,7 @@ void launch_gradh(Ctx& c, int nact) {
   k_gradh_pass<<<blocks, GP_THREADS, 0, c.st>>>(
       ngrp, gl, c.pm, c.hz, c.vel, c.rho, c.omega, c.div_v, c.drhodt, c.tabA, c.prm.h_fac,
       c.prm.pp_gather, c.info.rextent, c.leaves, c.nleaf, c.npot, c.redo, c.work + 1,
-      c.pplist, c.prm.pp_limit, c.d_err, counts, c.work, t.cl, t.ncl);
+      c.pplist, c.prm.pp_limit, c.d_err, counts, c.work, t.cl, t.ncl, rec ? 1 : 0, c.pptot);
   // three walk-stack slots of scratch per redo warp
   k_gradh_redo<<<std::max(1, (c.wstack_slots / 3) / RD_WARPS), RD_THREADS, 0, c.st>>>(
       c.redo, c.work + 1, c.pm, c.hz, c.vel, c.rho, c.omega, c.div_v, c.drhodt, t, c.tabA,
@@ -2195,10 +2224,19 @@ void launch_gradh(Ctx& c, int nact) {
     }
   }
   c.nlaunch += 3;
+  c.gsets = rec;
 }
 
-void launch_neib(Ctx& c, int nact) {
+static void launch_neib_gsets(Ctx& c, bool sorted);
+
+void launch_neib(Ctx& c, int nact, bool sorted) {
   if (nact <= 0) return;
+  const bool gsets = c.gsets;
+  c.gsets = false;
+  if (gsets) {                   // every particle active, right after grad-h
+    launch_neib_gsets(c, sorted);
+    return;
+  }
   unsigned long long* counts = reinterpret_cast<unsigned long long*>(c.d_counts);
   const HydroTree t = hydro_tree(c);
   int ngrp = nact;
@@ -2218,6 +2256,289 @@ void launch_neib(Ctx& c, int nact) {
   k_neib_rows<<<blocks, GP_THREADS, 0, c.st>>>(ngrp, gl, c.pm, c.hz, t, c.prm.pp_limit,
                                                c.leaves, c.nleaf, c.pptot, c.pplist, c.d_err,
                                                counts, c.work);
+  c.nlaunch += 2;
+}
+
+// get_neib (sph/get_neib.F90:10-140) for every particle right after grad-h,
+// without the walks.  The list of p is the set of q != p with r^2 <= 4h_p^2
+// (gather) or r^2 <= 4h_q^2 (scatter), in increasing particle order: the
+// reference walks the tree depth first (BHhydro_walk.F90), which visits the
+// leaves, and so the particles (numbered in tree order), in increasing order,
+// and its walk reaches every such q (a cell holding q lies within
+// hrangemax + rmax of p).  r^2 is the same in both rows of a pair (the
+// components only change sign).  So the lists follow from the gather sets:
+//  * the grad-h final pass has already applied the test r^2 <= 4h_p^2 with
+//    the final h to candidates that hold every particle within 2h (h <
+//    h_high) and written the gather set to p's row, its size to pptot and npot;
+//    particles it did not finish (npot = -1) get their rows from the
+//    neighbour walk (k_neib_walk, k_neib_rows), listed in order;
+//  * k_neib_transpose adds p to the row of each q in p's gather set that does
+//    not have p in its own (r^2 > 4h_q^2): the scatter neighbours;
+//  * k_neib_sort puts each such row in increasing order.
+// pptot ends as the full count in every row (the reference's pp_tot), and a
+// row of more than pp_limit neighbours keeps no list, as in the reference.
+__global__ void k_neib_flag(int n, const int* __restrict__ npot, int* __restrict__ flag) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < n) flag[p] = npot[p] < 0 ? 1 : 0;
+}
+
+__global__ void k_neib_list(int n, const int* __restrict__ flag, const int* __restrict__ scan,
+                            int* __restrict__ out) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < n && flag[p]) out[scan[p]] = p;
+}
+
+// one warp per particle p: its gather neighbours q, from its row (the first
+// npot[p] entries; the gather part of a walked row), or from a walk when the
+// row has more than L; p joins q's row when q's own gather set lacks it
+constexpr int NT_THREADS = 256;
+__global__ void __launch_bounds__(NT_THREADS) k_neib_transpose(
+    int n, const double4* __restrict__ pm, const double2* __restrict__ hz,
+    const int* __restrict__ npot, int* __restrict__ pptot, int* __restrict__ pplist, int L,
+    HydroTree t, DevError* err, unsigned long long* counts) {
+  const int lane = threadIdx.x & 31;
+  const int nw = gridDim.x * (NT_THREADS / 32);
+  unsigned long long ntest = 0;
+  for (int p = blockIdx.x * (NT_THREADS / 32) + (threadIdx.x >> 5); p < n; p += nw) {
+    const int g0 = npot[p];
+    // a walked row is complete and final; a recorded row grows from g0 on
+    const int ng = g0 >= 0 ? g0 : pptot[p];
+    const double4 P = pm[p];
+    const double hp = hz[p].x;
+    const double hsp = (KERNRANGESQD * hp) * hp;
+    auto visit = [&](int q, bool test_gather) {
+      const double4 Q = pm[q];                       // the three loads issued together
+      const int nq = npot[q];
+      const double hq = hz[q].x;
+      const double d0 = Q.x - P.x, d1 = Q.y - P.y, d2 = Q.z - P.z;
+      const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
+      if (test_gather && !(drsqd <= hsp)) return;
+      if (nq < 0) return;                            // q's row came from a walk
+      if (drsqd <= (KERNRANGESQD * hq) * hq) return; // p is in q's gather set
+      const int slot = atomicAdd(pptot + q, 1);
+      if (slot < L) pplist[(size_t)q * L + slot] = p;
+    };
+    if (ng <= L) {
+      const int* row = pplist + (size_t)p * L;
+      for (int k = lane; k < ng; k += 64) {          // two entries per lane in flight
+        const int q0 = row[k];
+        const int q1 = k + 32 < ng ? row[k + 32] : -1;
+        visit(q0, g0 < 0);
+        if (q1 >= 0) visit(q1, g0 < 0);
+      }
+      ntest += ng;
+    } else if (lane == 0) {                          // more than L: the gather set from a walk
+      walk_gather_scatter(t, frame_for(t, p).root, P.x, P.y, P.z, KERNRANGE * hp, err, p,
+                          [&](int q) {
+                            if (q != p) visit(q, true);
+                          });
+    }
+  }
+  if (lane == 0) atomicAdd(counts + 7, ntest);
+}
+
+// bitonic sort of 32 R values per warp, value r*32 + lane in e[r]
+template <int R>
+__device__ __forceinline__ void warp_bitonic(int (&e)[R], int lane) {
+#pragma unroll
+  for (int size = 2; size <= 32 * R; size <<= 1) {
+#pragma unroll
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      if (stride >= 32) {
+        const int rs = stride >> 5;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          if ((r & rs) == 0) {
+            const int r2 = r | rs;
+            const bool up = ((r * 32 + lane) & size) == 0;
+            const int a = e[r], b = e[r2];
+            const bool sw = up ? (a > b) : (a < b);
+            e[r] = sw ? b : a;
+            e[r2] = sw ? a : b;
+          }
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const bool up = ((r * 32 + lane) & size) == 0;
+          const int o = __shfl_xor_sync(FULL, e[r], stride);
+          const bool lower = (lane & stride) == 0;
+          e[r] = (lower == up) ? min(e[r], o) : max(e[r], o);
+        }
+      }
+    }
+  }
+}
+
+template <int R>
+__device__ __forceinline__ void sort_row(int* row, int m, int lane) {
+  int e[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int k = r * 32 + lane;
+    e[r] = k < m ? row[k] : INT_MAX;
+  }
+  warp_bitonic<R>(e, lane);
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int k = r * 32 + lane;
+    if (k < m) row[k] = e[r];
+  }
+}
+
+// one warp per recorded row that holds its whole list: the row in increasing
+// order (full), or only its scatter part (the entries the transposition
+// appended, in an order that depends on the atomics), so that the row's order
+// is the same from run to run
+__global__ void __launch_bounds__(NT_THREADS) k_neib_sort(int n, const int* __restrict__ npot,
+                                                         const int* __restrict__ pptot,
+                                                         int* __restrict__ pplist, int L,
+                                                         int full) {
+  const int lane = threadIdx.x & 31;
+  const int nw = gridDim.x * (NT_THREADS / 32);
+  for (int p = blockIdx.x * (NT_THREADS / 32) + (threadIdx.x >> 5); p < n; p += nw) {
+    const int g0 = npot[p];
+    if (g0 < 0) continue;                            // a walked row: in order already
+    const int tot = pptot[p];
+    if (tot > L) continue;
+    const int b = full ? 0 : g0;
+    const int m = tot - b;
+    if (m < 2) continue;
+    int* row = pplist + (size_t)p * L + b;
+    if (m <= 32) sort_row<1>(row, m, lane);
+    else if (m <= 64) sort_row<2>(row, m, lane);
+    else if (m <= 128) sort_row<4>(row, m, lane);
+    else if (m <= 256) sort_row<8>(row, m, lane);
+    else if (lane == 0) {                            // pp_limit above 256: insertion sort
+      for (int i = 1; i < m; ++i) {
+        const int x = row[i];
+        int j = i - 1;
+        while (j >= 0 && row[j] > x) {
+          row[j + 1] = row[j];
+          --j;
+        }
+        row[j + 1] = x;
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// The rows of the particles grad-h left to a walk (npot = -1: redone, or
+// h >= h_high at the final pass): one warp per particle, the reference's
+// gather-or-scatter walk (BHhydro_walk.F90:37-43, FP64 test) breadth first
+// through the redo kernel's scratch, the neighbours kept as get_neib keeps
+// them (sph/get_neib.F90:83-118) and put in increasing order; a walk beyond
+// the scratch falls back to the stackless walk of one thread.
+__global__ void __launch_bounds__(RD_THREADS) k_neib_walked(
+    int nw, const int* __restrict__ list, const double4* __restrict__ pm,
+    const double2* __restrict__ hz, HydroTree t, int L, int* __restrict__ pptot,
+    int* __restrict__ pplist, int* __restrict__ scratch, int cap, DevError* err,
+    unsigned long long* counts) {
+  __shared__ int cand_all[RD_WARPS][GP_SEG * LEAFMAX];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int* cand = cand_all[w];
+  const int gw = blockIdx.x * RD_WARPS + w;
+  int* fa = scratch + (size_t)gw * 3 * cap;
+  int* fb = fa + cap;
+  int* lv = fb + cap;
+  const unsigned lt = (1u << lane) - 1u;
+  unsigned long long nvisit = 0, ncands = 0;
+  for (int i = gw; i < nw; i += gridDim.x * RD_WARPS) {
+    const int p = list[i];
+    const double4 P = pm[p];
+    const double hp = hz[p].x;
+    const double hsp = (KERNRANGESQD * hp) * hp;
+    const double R = KERNRANGE * hp;
+    auto test = [&](int c) {
+      const double4 h = t.hA[c];
+      const double d0 = h.x - P.x, d1 = h.y - P.y, d2 = h.z - P.z;
+      const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
+      const double t1 = R + h.w;
+      const double t2 = t.hrm[c] + h.w;
+      return drsqd <= t1 * t1 || drsqd <= t2 * t2;
+    };
+    int cnt = 0;
+    const int nl = rd_walk(t, frame_for(t, p).root, lane, fa, fb, lv, cap, cnt, nvisit, test);
+    if (nl < 0) {
+      if (lane == 0) neib_one(p, pm, hz, t, L, pptot, pplist, err);
+      __syncwarp();
+      continue;
+    }
+    int* row = pplist + (size_t)p * L;
+    int kept = 0;
+    for (int s0 = 0; s0 < nl; s0 += GP_SEG) {
+      const int nc = gp_flatten(lv + s0, min(GP_SEG, nl - s0), cand, lane);
+      for (int b = 0; b < nc; b += 32) {
+        const int k = b + lane;
+        const int q = k < nc ? cand[k] : p;
+        bool keep = false;
+        if (q != p) {
+          const double4 Q = pm[q];
+          const double hq = hz[q].x;
+          const double hsq = (KERNRANGESQD * hq) * hq;
+          const double d0 = Q.x - P.x, d1 = Q.y - P.y, d2 = Q.z - P.z;
+          const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
+          keep = drsqd <= hsp || drsqd <= hsq;
+        }
+        const unsigned m = __ballot_sync(FULL, keep);
+        const int pos = kept + __popc(m & lt);
+        if (keep && pos < L) row[pos] = q;
+        kept += __popc(m);
+      }
+      ncands += nc;
+    }
+    if (lane == 0) pptot[p] = kept;
+    __syncwarp();
+    if (kept <= L && kept >= 2) {
+      if (kept <= 32) sort_row<1>(row, kept, lane);
+      else if (kept <= 64) sort_row<2>(row, kept, lane);
+      else if (kept <= 128) sort_row<4>(row, kept, lane);
+      else if (kept <= 256) sort_row<8>(row, kept, lane);
+      else if (lane == 0) {
+        for (int a = 1; a < kept; ++a) {
+          const int x = row[a];
+          int j = a - 1;
+          while (j >= 0 && row[j] > x) {
+            row[j + 1] = row[j];
+            --j;
+          }
+          row[j + 1] = x;
+        }
+      }
+    }
+    __syncwarp();
+  }
+  if (lane == 0) {
+    atomicAdd(counts + 4, nvisit);
+    atomicAdd(counts + 7, ncands);
+  }
+}
+
+static void launch_neib_gsets(Ctx& c, bool sorted) {
+  unsigned long long* counts = reinterpret_cast<unsigned long long*>(c.d_counts);
+  const HydroTree t = hydro_tree(c);
+  const int n = c.ptot;
+  const int L = c.prm.pp_limit;
+  // the particles grad-h left to a walk, in order (c.redo is free after grad-h)
+  k_neib_flag<<<nb(n, 256), 256, 0, c.st>>>(n, c.npot, c.bflag);
+  scan_exclusive(c, c.bflag, c.bscan, n);
+  k_neib_list<<<nb(n, 256), 256, 0, c.st>>>(n, c.bflag, c.bscan, c.redo);
+  c.nlaunch += 2;
+  int nw = 0;
+  read_dev(c, c.scan.total, &nw, sizeof(int));
+  if (nw > 0) {
+    // three walk-stack slots of scratch per warp, as the redo kernel
+    const int blocks = std::min((c.wstack_slots / 3) / RD_WARPS, nb(nw, RD_WARPS));
+    k_neib_walked<<<std::max(1, blocks), RD_THREADS, 0, c.st>>>(
+        nw, c.redo, c.pm, c.hz, t, L, c.pptot, c.pplist, reinterpret_cast<int*>(c.wstack),
+        2 * c.wstack_cap, c.d_err, counts);
+    ++c.nlaunch;
+  }
+  const int blocks = std::min(sm_count(c) * 8, nb((long)n * 32, NT_THREADS));
+  k_neib_transpose<<<blocks, NT_THREADS, 0, c.st>>>(n, c.pm, c.hz, c.npot, c.pptot, c.pplist, L,
+                                                    t, c.d_err, counts);
+  k_neib_sort<<<blocks, NT_THREADS, 0, c.st>>>(n, c.npot, c.pptot, c.pplist, L, sorted ? 1 : 0);
   c.nlaunch += 2;
 }
 
