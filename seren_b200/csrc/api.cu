@@ -540,7 +540,7 @@ int seren_gpu_sph_update(seren_gpu_ctx* h, int32_t ptot, const int32_t* acclist,
       cudaMemcpyAsync(drhodt, c.drhodt, sizeof(double) * N, cudaMemcpyDeviceToHost, c.st_io);
   }
   seren::launch_update_hmax(c);
-  seren::launch_neib(c, nact);
+  seren::launch_neib(c, nact, pplist != nullptr);  // the reference's order when the caller reads them
   rc = finish(c, "sph_update");
   if (rc) return drain(rc);
   if (overlap) {

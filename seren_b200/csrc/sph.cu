@@ -2288,14 +2288,22 @@ __global__ void k_neib_list(int n, const int* __restrict__ flag, const int* __re
   if (p < n && flag[p]) out[scan[p]] = p;
 }
 
+// h of every particle, negated for a walked row (npot = -1), so that the
+// transposition reads one word per neighbour
+__global__ void k_neib_hflag(int n, const double2* __restrict__ hz, const int* __restrict__ npot,
+                             double* __restrict__ hw) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < n) hw[p] = npot[p] < 0 ? -hz[p].x : hz[p].x;
+}
+
 // one warp per particle p: its gather neighbours q, from its row (the first
 // npot[p] entries; the gather part of a walked row), or from a walk when the
 // row has more than L; p joins q's row when q's own gather set lacks it
 constexpr int NT_THREADS = 256;
 __global__ void __launch_bounds__(NT_THREADS) k_neib_transpose(
     int n, const double4* __restrict__ pm, const double2* __restrict__ hz,
-    const int* __restrict__ npot, int* __restrict__ pptot, int* __restrict__ pplist, int L,
-    HydroTree t, DevError* err, unsigned long long* counts) {
+    const double* __restrict__ hw, const int* __restrict__ npot, int* __restrict__ pptot,
+    int* __restrict__ pplist, int L, HydroTree t, DevError* err, unsigned long long* counts) {
   const int lane = threadIdx.x & 31;
   const int nw = gridDim.x * (NT_THREADS / 32);
   unsigned long long ntest = 0;
@@ -2307,13 +2315,12 @@ __global__ void __launch_bounds__(NT_THREADS) k_neib_transpose(
     const double hp = hz[p].x;
     const double hsp = (KERNRANGESQD * hp) * hp;
     auto visit = [&](int q, bool test_gather) {
-      const double4 Q = pm[q];                       // the three loads issued together
-      const int nq = npot[q];
-      const double hq = hz[q].x;
+      const double4 Q = pm[q];                       // the two loads issued together
+      const double hq = hw[q];
       const double d0 = Q.x - P.x, d1 = Q.y - P.y, d2 = Q.z - P.z;
       const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
       if (test_gather && !(drsqd <= hsp)) return;
-      if (nq < 0) return;                            // q's row came from a walk
+      if (hq < 0.0) return;                          // q's row came from a walk
       if (drsqd <= (KERNRANGESQD * hq) * hq) return; // p is in q's gather set
       const int slot = atomicAdd(pptot + q, 1);
       if (slot < L) pplist[(size_t)q * L + slot] = p;
@@ -2337,11 +2344,13 @@ __global__ void __launch_bounds__(NT_THREADS) k_neib_transpose(
   if (lane == 0) atomicAdd(counts + 7, ntest);
 }
 
-// bitonic sort of 32 R values per warp, value r*32 + lane in e[r]
-template <int R>
+// bitonic sort of N = 32 R values per warp, value r*32 + lane in e[r] (or,
+// with R = 1, of the first N <= 32 lanes' values, each block of N lanes on
+// its own, the first one ascending)
+template <int R, int N = 32 * R>
 __device__ __forceinline__ void warp_bitonic(int (&e)[R], int lane) {
 #pragma unroll
-  for (int size = 2; size <= 32 * R; size <<= 1) {
+  for (int size = 2; size <= N; size <<= 1) {
 #pragma unroll
     for (int stride = size >> 1; stride > 0; stride >>= 1) {
       if (stride >= 32) {
@@ -2370,7 +2379,7 @@ __device__ __forceinline__ void warp_bitonic(int (&e)[R], int lane) {
   }
 }
 
-template <int R>
+template <int R, int N = 32 * R>
 __device__ __forceinline__ void sort_row(int* row, int m, int lane) {
   int e[R];
 #pragma unroll
@@ -2378,7 +2387,7 @@ __device__ __forceinline__ void sort_row(int* row, int m, int lane) {
     const int k = r * 32 + lane;
     e[r] = k < m ? row[k] : INT_MAX;
   }
-  warp_bitonic<R>(e, lane);
+  warp_bitonic<R, N>(e, lane);
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     const int k = r * 32 + lane;
@@ -2405,7 +2414,9 @@ __global__ void __launch_bounds__(NT_THREADS) k_neib_sort(int n, const int* __re
     const int m = tot - b;
     if (m < 2) continue;
     int* row = pplist + (size_t)p * L + b;
-    if (m <= 32) sort_row<1>(row, m, lane);
+    if (m <= 8) sort_row<1, 8>(row, m, lane);
+    else if (m <= 16) sort_row<1, 16>(row, m, lane);
+    else if (m <= 32) sort_row<1>(row, m, lane);
     else if (m <= 64) sort_row<2>(row, m, lane);
     else if (m <= 128) sort_row<4>(row, m, lane);
     else if (m <= 256) sort_row<8>(row, m, lane);
@@ -2535,9 +2546,14 @@ static void launch_neib_gsets(Ctx& c, bool sorted) {
         2 * c.wstack_cap, c.d_err, counts);
     ++c.nlaunch;
   }
+  // h and the walked flag packed in one word per particle, in the rho_alt
+  // reorder target (free between reorders: the next one overwrites it whole)
+  double* hw = c.rho_alt;
+  k_neib_hflag<<<nb(n, 256), 256, 0, c.st>>>(n, c.hz, c.npot, hw);
   const int blocks = std::min(sm_count(c) * 8, nb((long)n * 32, NT_THREADS));
-  k_neib_transpose<<<blocks, NT_THREADS, 0, c.st>>>(n, c.pm, c.hz, c.npot, c.pptot, c.pplist, L,
-                                                    t, c.d_err, counts);
+  k_neib_transpose<<<blocks, NT_THREADS, 0, c.st>>>(n, c.pm, c.hz, hw, c.npot, c.pptot, c.pplist,
+                                                    L, t, c.d_err, counts);
+  ++c.nlaunch;
   k_neib_sort<<<blocks, NT_THREADS, 0, c.st>>>(n, c.npot, c.pptot, c.pplist, L, sorted ? 1 : 0);
   c.nlaunch += 2;
 }
