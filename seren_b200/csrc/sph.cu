@@ -2288,12 +2288,15 @@ __global__ void k_neib_list(int n, const int* __restrict__ flag, const int* __re
   if (p < n && flag[p]) out[scan[p]] = p;
 }
 
-// h of every particle, negated for a walked row (npot = -1), so that the
-// transposition reads one word per neighbour
-__global__ void k_neib_hflag(int n, const double2* __restrict__ hz, const int* __restrict__ npot,
-                             double* __restrict__ hw) {
+// position and h of every particle, h negated for a walked row (npot = -1),
+// so that the transposition gathers one 32-byte record per neighbour
+__global__ void k_neib_hflag(int n, const double4* __restrict__ pm, const double2* __restrict__ hz,
+                             const int* __restrict__ npot, double4* __restrict__ ph) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p < n) hw[p] = npot[p] < 0 ? -hz[p].x : hz[p].x;
+  if (p >= n) return;
+  const double4 P = pm[p];
+  const double h = hz[p].x;
+  ph[p] = make_double4(P.x, P.y, P.z, npot[p] < 0 ? -h : h);
 }
 
 // one warp per particle p: its gather neighbours q, from its row (the first
@@ -2301,8 +2304,7 @@ __global__ void k_neib_hflag(int n, const double2* __restrict__ hz, const int* _
 // row has more than L; p joins q's row when q's own gather set lacks it
 constexpr int NT_THREADS = 256;
 __global__ void __launch_bounds__(NT_THREADS) k_neib_transpose(
-    int n, const double4* __restrict__ pm, const double2* __restrict__ hz,
-    const double* __restrict__ hw, const int* __restrict__ npot, int* __restrict__ pptot,
+    int n, const double4* __restrict__ ph, const int* __restrict__ npot, int* __restrict__ pptot,
     int* __restrict__ pplist, int L, HydroTree t, DevError* err, unsigned long long* counts) {
   const int lane = threadIdx.x & 31;
   const int nw = gridDim.x * (NT_THREADS / 32);
@@ -2311,12 +2313,12 @@ __global__ void __launch_bounds__(NT_THREADS) k_neib_transpose(
     const int g0 = npot[p];
     // a walked row is complete and final; a recorded row grows from g0 on
     const int ng = g0 >= 0 ? g0 : pptot[p];
-    const double4 P = pm[p];
-    const double hp = hz[p].x;
+    const double4 P = ph[p];
+    const double hp = fabs(P.w);
     const double hsp = (KERNRANGESQD * hp) * hp;
     auto visit = [&](int q, bool test_gather) {
-      const double4 Q = pm[q];                       // the two loads issued together
-      const double hq = hw[q];
+      const double4 Q = ph[q];
+      const double hq = Q.w;
       const double d0 = Q.x - P.x, d1 = Q.y - P.y, d2 = Q.z - P.z;
       const double drsqd = (d0 * d0 + d1 * d1) + d2 * d2;
       if (test_gather && !(drsqd <= hsp)) return;
@@ -2546,13 +2548,13 @@ static void launch_neib_gsets(Ctx& c, bool sorted) {
         2 * c.wstack_cap, c.d_err, counts);
     ++c.nlaunch;
   }
-  // h and the walked flag packed in one word per particle, in the rho_alt
-  // reorder target (free between reorders: the next one overwrites it whole)
-  double* hw = c.rho_alt;
-  k_neib_hflag<<<nb(n, 256), 256, 0, c.st>>>(n, c.hz, c.npot, hw);
+  // positions with h and the walked flag, one record per particle, in the
+  // pm_alt reorder target (free between reorders: the next one overwrites it)
+  double4* ph = c.pm_alt;
+  k_neib_hflag<<<nb(n, 256), 256, 0, c.st>>>(n, c.pm, c.hz, c.npot, ph);
   const int blocks = std::min(sm_count(c) * 8, nb((long)n * 32, NT_THREADS));
-  k_neib_transpose<<<blocks, NT_THREADS, 0, c.st>>>(n, c.pm, c.hz, hw, c.npot, c.pptot, c.pplist,
-                                                    L, t, c.d_err, counts);
+  k_neib_transpose<<<blocks, NT_THREADS, 0, c.st>>>(n, ph, c.npot, c.pptot, c.pplist, L, t,
+                                                    c.d_err, counts);
   ++c.nlaunch;
   k_neib_sort<<<blocks, NT_THREADS, 0, c.st>>>(n, c.npot, c.pptot, c.pplist, L, sorted ? 1 : 0);
   c.nlaunch += 2;
