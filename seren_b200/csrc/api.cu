@@ -271,6 +271,7 @@ void free_all(Ctx& c) {
   if (c.wpart) cudaFree(c.wpart);
   if (c.wpart_brute) cudaFree(c.wpart_brute);
   if (c.wcover) cudaFree(c.wcover);
+  if (c.hrec) cudaFree(c.hrec);
   for (double4* p : {c.r_old, c.v_old, c.v_half, c.r_old_alt, c.v_old_alt, c.v_half_alt})
     if (p) cudaFree(p);
   for (void* p : {(void*)c.acc_sinks, (void*)c.acc_out, (void*)c.acc_ws})

@@ -189,6 +189,7 @@ struct Ctx {
   bool gsets = false;             // the last grad-h recorded the gather neighbours (launch_neib)
   int* wcover = nullptr;          // the cells their walks are spread over (made on first use)
   int wcover_cap = 0;
+  double4* hrec = nullptr;        // hydro: 96-byte neighbour records, 3 per particle (first use)
   int2* wstack = nullptr;     // walk stacks, wstack_cap (cell, lane mask) entries per warp slot
   int wstack_cap = 0;
   int wstack_slots = 0;
