@@ -132,6 +132,36 @@ def test_gradh_bisection_matches_oracle(libs, name, redo_cap, wide):
     g2.close()
 
 
+def test_neighbour_lists_with_overflowing_rows(libs):
+    """pp_limit = 40, below the ~56 neighbours of a particle of the core: most
+    rows overflow (get_neib keeps no list for them, pptot is the full count,
+    sph/get_neib.F90:115-118) and so do the gather sets that the grad-h final
+    pass records, whose transposition then walks the tree.  The lists after
+    grad-h (sph_update) and the accelerations of the device-resident force
+    step, whose hydro forces find an overflowing row's neighbours on the fly
+    (get_neib_on_fly.F90), are still the oracle's."""
+    ic = case("turb20k")
+    Oracle, Gpu = libs
+    n = ic["parray"].shape[0]
+    prm = params(ic)
+    prm.pp_limit = 40
+    o, g = Oracle(n, prm), Gpu(n, prm)
+    ro = run_pipeline(o, ic)
+    rg = run_pipeline(g, ic)
+    so, sg = ro["sph"], rg["sph"]
+    assert (so["pptot"] > 40).mean() > 0.5                # most rows overflow
+    assert lists_equal(so["pptot"], so["pplist"], sg["pptot"], sg["pplist"], 40)
+    assert rel_rows(sg["parray"][:, 4], so["parray"][:, 4]).max() < TOL
+    assert rel_scaled(rg["a_hydro"], ro["a_hydro"]) < TOL
+    g2 = Gpu(n, prm)
+    g2.upload(ic["parray"], ic["v"], ic["sound"] ** 2)
+    g2.force_step(first_call=True)
+    st = g2.download()
+    g2.close()
+    assert np.array_equal(st["perm"], ro["perm"])
+    assert rel_rows(st["a"], ro["a"]).max() < 1e-11
+
+
 @pytest.mark.parametrize("name", ["sphere4k", "plummer16k", "disc12k"])
 def test_neighbour_lists_at_oracle_h(libs, name):
     """get_neib at the same h is bit-exact (sph/get_neib.F90:83-118)."""
