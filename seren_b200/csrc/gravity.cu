@@ -178,13 +178,11 @@ struct GravWalk {
 // softened-gravity functions w5, w4, w6 (setup/kernel.F90:80-81, :99-102) come
 // from an FP32 copy of the reference's table at bin int(5000 r/h), clamped to
 // KERNTOT (tab32[k] = w5, w4, w6).
-__device__ __forceinline__ void pair32(float d0, float d1, float d2, float invhp, float zo_p,
-                                       float mq, float invhq, float zq,
+// (inv = 1/r and drmag = r as the caller formed them from d for its branch test)
+__device__ __forceinline__ void pair32(float d0, float d1, float d2, float inv, float drmag,
+                                       float invhp, float zo_p, float mq, float invhq, float zq,
                                        const float4* __restrict__ tab32, float& ax, float& ay,
                                        float& az, float& ap) {
-  const float drsqd = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
-  const float inv = rsqrtf(fmaxf(drsqd, 1.0e-30f));
-  const float drmag = drsqd * inv;
   const float xp = drmag * invhp;
   const float xq = drmag * invhq;
   const float4 wp = tab32[(int)fminf(5000.0f * xp, (float)KERNTOT)];
@@ -482,7 +480,8 @@ k_grav_walk(int nact, const int* __restrict__ act, const double4* __restrict__ p
             // pair32's own branch tests: the kernel is needed only inside 2h of either particle
             const bool soft = on && (drmag * invhp32 < KERNRANGE || drmag * b.x < KERNRANGE);
             if (__any_sync(FULLMASK, soft)) {
-              if (on) pair32(d0, d1, d2, invhp32, zo32, a.w, b.x, b.y, tab32, sx, sy, sz, sp);
+              if (on) pair32(d0, d1, d2, inv, drmag, invhp32, zo32, a.w, b.x, b.y, tab32, sx, sy,
+                             sz, sp);
             } else if (on) {
               pair32_far(d0, d1, d2, inv, a.w, sx, sy, sz, sp);
             }
