@@ -168,6 +168,41 @@ def test_forest_equals_single_cloud_runs(precision):
 
 
 @pytest.mark.gpu
+def test_forest_whole_gpu_gradh_path():
+    """With a tiny redo scratch (redo_cap = 8) the grad-h walks of many particles
+    of every cloud go to the whole-GPU path, whose walks and passes run over a
+    cover of the whole forest restricted to the particle's own cloud.  Its
+    partial sums are grouped by slices and tiles of the whole forest, so the
+    results equal single-cloud runs to the FP64 rounding of that grouping
+    (1e-12), not bit for bit; the tree order is the same."""
+    from seren_b200.gpu import GpuHotPath
+    clouds = _forest_clouds()
+    ns = [c["parray"].shape[0] for c in clouds]
+    g = GpuHotPath(sum(ns), params(clouds[0], redo_cap=8))
+    g.upload(np.vstack([c["parray"] for c in clouds]), np.vstack([c["v"] for c in clouds]),
+             np.concatenate([c["sound"] ** 2 for c in clouds]))
+    g.set_clouds(ns)
+    g.force_step(first_call=True)
+    assert g.last_step_stats()[2][8] > 0            # particles on the whole-GPU path
+    st = g.download()
+    g.close()
+    off = 0
+    for ic, n in zip(clouds, ns):
+        one = GpuHotPath(n, params(ic, redo_cap=8))
+        one.upload(ic["parray"], ic["v"], ic["sound"] ** 2)
+        one.force_step(first_call=True)
+        d = one.download()
+        one.close()
+        rows = slice(off, off + n)
+        assert np.array_equal(st["perm"][rows], d["perm"] + off)
+        assert rel_rows(st["parray"][rows, 4], d["parray"][:, 4]).max() < 1e-12
+        for k in ("rho", "omega"):
+            assert rel_rows(st[k][rows], d[k]).max() < 1e-12, k
+        assert rel_rows(st["a"][rows], d["a"]).max() < 1e-11
+        off += n
+
+
+@pytest.mark.gpu
 def test_forest_refuses_what_it_does_not_support():
     from seren_b200.cabi import SerenError
     from seren_b200.gpu import GpuHotPath
