@@ -281,12 +281,24 @@ __global__ void k_rs_hist(const unsigned long long* __restrict__ keys, int n, in
   hist[threadIdx.x * nblk + blockIdx.x] = cnt[threadIdx.x];
 }
 
+// The tile's items ranked by (digit, then the tile's order) and staged in that
+// order in shared memory (the stable order of the pass), then written out:
+// consecutive threads write consecutive slots of a digit's run, so the stores
+// coalesce.  Shared memory: the tile's keys and values, the per-warp digit
+// counts and the tile's digit starts.
+constexpr size_t RS_SMEM = (size_t)RS_TILE * (sizeof(unsigned long long) + sizeof(int)) +
+                           sizeof(int) * (RS_W * 256 + 256 + RS_W);
 __global__ void __launch_bounds__(RS_T) k_rs_scatter(const unsigned long long* __restrict__ kin,
                                                      const int* __restrict__ vin,
                                                      unsigned long long* __restrict__ kout,
                                                      int* __restrict__ vout, int n, int shift,
                                                      const int* __restrict__ offs, int nblk) {
-  __shared__ int wh[RS_W][256];
+  extern __shared__ __align__(16) unsigned char rs_smem[];
+  unsigned long long* sk = reinterpret_cast<unsigned long long*>(rs_smem);
+  int* sv = reinterpret_cast<int*>(sk + RS_TILE);
+  int (*wh)[256] = reinterpret_cast<int (*)[256]>(sv + RS_TILE);
+  int* tstart = reinterpret_cast<int*>(wh + RS_W);
+  int* wtot = tstart + 256;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   for (int ww = 0; ww < RS_W; ++ww) wh[ww][threadIdx.x] = 0;
   __syncthreads();
@@ -312,22 +324,42 @@ __global__ void __launch_bounds__(RS_T) k_rs_scatter(const unsigned long long* _
     dig[r] = d;
   }
   __syncthreads();
-  {
-    int run = 0;
-    for (int ww = 0; ww < RS_W; ++ww) {
-      const int cnum = wh[ww][threadIdx.x];
-      wh[ww][threadIdx.x] = run;
-      run += cnum;
-    }
+  int run = 0;                       // this thread's digit: counts of the earlier warps
+  for (int ww = 0; ww < RS_W; ++ww) {
+    const int cnum = wh[ww][threadIdx.x];
+    wh[ww][threadIdx.x] = run;
+    run += cnum;
   }
+  // the tile's digit starts: an exclusive scan of the digits' counts
+  int inc = run;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(FULL, inc, o);
+    if (lane >= o) inc += y;
+  }
+  if (lane == 31) wtot[w] = inc;
+  __syncthreads();
+  int wbase = 0;
+  for (int ww = 0; ww < w; ++ww) wbase += wtot[ww];
+  tstart[threadIdx.x] = wbase + inc - run;
   __syncthreads();
 #pragma unroll
   for (int r = 0; r < RS_I; ++r) {
     if (dig[r] < 256) {
-      const int pos = offs[dig[r] * nblk + blockIdx.x] + wh[w][dig[r]] + rank[r];
-      kout[pos] = k[r];
-      vout[pos] = val[r];
+      const int lp = tstart[dig[r]] + wh[w][dig[r]] + rank[r];
+      sk[lp] = k[r];
+      sv[lp] = val[r];
     }
+  }
+  __syncthreads();
+  const long t0 = (long)blockIdx.x * RS_TILE;
+  const int tcount = (int)min((long)RS_TILE, (long)n - t0);
+  for (int t = threadIdx.x; t < tcount; t += RS_T) {
+    const unsigned long long key = sk[t];
+    const int d = (int)((key >> shift) & 255ull);
+    const int pos = offs[d * nblk + blockIdx.x] + (t - tstart[d]);
+    kout[pos] = key;
+    vout[pos] = sv[t];
   }
 }
 
@@ -866,6 +898,12 @@ void launch_pack_parray(Ctx& c, double* stage, int n, cudaStream_t s) {
 // stable LSD sort of (keys, idx) on the key bits [0, bits), 8 at a time; an
 // even number of passes leaves the sorted data in keys/idx
 static void radix_sort(Ctx& c, int n, int bits) {
+  static bool smem_set[16] = {};   // the scatter's shared memory is above the 48 KB default
+  bool& ss = smem_set[c.dev >= 0 && c.dev < 16 ? c.dev : 0];
+  if (!ss) {
+    cudaFuncSetAttribute(k_rs_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RS_SMEM);
+    ss = true;
+  }
   const int nblk = nb(n, RS_TILE);
   unsigned long long* ka = c.keys;
   unsigned long long* kb = c.keys_alt;
@@ -874,7 +912,8 @@ static void radix_sort(Ctx& c, int n, int bits) {
   for (int shift = 0; shift < bits; shift += 8) {
     k_rs_hist<<<nblk, RS_T, 0, c.st>>>(ka, n, shift, c.rs_hist, nblk); ++c.nlaunch;
     scan_exclusive(c, c.rs_hist, c.rs_hist, 256 * nblk);
-    k_rs_scatter<<<nblk, RS_T, 0, c.st>>>(ka, va, kb, vb, n, shift, c.rs_hist, nblk); ++c.nlaunch;
+    k_rs_scatter<<<nblk, RS_T, RS_SMEM, c.st>>>(ka, va, kb, vb, n, shift, c.rs_hist, nblk);
+    ++c.nlaunch;
     std::swap(ka, kb);
     std::swap(va, vb);
   }
