@@ -2305,11 +2305,13 @@ void launch_neib(Ctx& c, int nact, bool sorted) {
 //  * the grad-h final pass has already applied the test r^2 <= 4h_p^2 with
 //    the final h to candidates that hold every particle within 2h (h <
 //    h_high) and written the gather set to p's row, its size to pptot and npot;
-//    particles it did not finish (npot = -1) get their rows from the
-//    neighbour walk (k_neib_walk, k_neib_rows), listed in order;
+//    the particles it did not finish (npot = -1), listed in order, get their
+//    whole rows from a walk of their own (k_neib_walked);
 //  * k_neib_transpose adds p to the row of each q in p's gather set that does
 //    not have p in its own (r^2 > 4h_q^2): the scatter neighbours;
-//  * k_neib_sort puts each such row in increasing order.
+//  * k_neib_sort puts each such row in increasing order when the caller reads
+//    the lists, and otherwise only its scatter part (a fixed order from run
+//    to run: the gather part in the final pass's order, then the scatter part).
 // pptot ends as the full count in every row (the reference's pp_tot), and a
 // row of more than pp_limit neighbours keeps no list, as in the reference.
 __global__ void k_neib_flag(int n, const int* __restrict__ npot, int* __restrict__ flag) {
