@@ -307,3 +307,20 @@ def test_h_gather_is_the_pp_gather_th_neighbour_distance(name):
         d2[i] = np.inf
         assert h[i] == 0.5 * np.sqrt(np.partition(d2, k - 1)[k - 1]), i
     o.close()
+
+
+def test_gradh_bisection_cases():
+    """The cases the GPU's bisection parity test relies on: on the first call
+    (h guess) some particles of three dense clumps reach the reference's
+    bisection (all_sph_gradh.F90:256-275), none of the uniform sphere's do,
+    and every h ends finite and positive."""
+    for name, expect in (("clumps12k", True), ("sphere4k", False)):
+        ic = case(name)
+        n = ic["parray"].shape[0]
+        o = Oracle(n, params(ic))
+        r = run_pipeline(o, ic)
+        nb = o.counts()["gradh_bisections"]
+        o.close()
+        assert (nb > 0) == expect, (name, nb)
+        h = r["sph"]["parray"][:, 4]
+        assert np.all(np.isfinite(h)) and np.all(h > 0.0)
