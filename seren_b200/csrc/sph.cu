@@ -1873,22 +1873,31 @@ constexpr int HY_SUB = 4;        // threads per particle in the mixed hydro kern
 // SUB consecutive threads share one particle, each taking every SUB-th entry
 // of its neighbour list, and their sums are added at the end (SUB = 1 keeps the
 // reference's order of terms).
-// The neighbours' values as one 96-byte record per particle (three 32-byte
-// sectors: x, y, z, m | vx, vy, vz, h | pf, hf4, c_s, rho), so that a pair
-// gathers two or three adjacent sectors instead of one per array.
-__global__ void k_hydro_pack(int n, const double4* __restrict__ pm, const double2* __restrict__ hz,
-                             const double4* __restrict__ vel, const double* __restrict__ pf,
-                             const double* __restrict__ hf4, const double* __restrict__ sound,
-                             const double* __restrict__ rho, double4* __restrict__ rec) {
+// k_hydro_prep for the mixed kernel, which also writes the neighbours' values
+// as one 96-byte record per particle (three 32-byte sectors: x, y, z, m |
+// vx, vy, vz, h | pf, hf4, c_s, rho), so that a pair gathers two or three
+// adjacent sectors instead of one per array
+__global__ void k_hydro_prep_pack(int n, const double4* __restrict__ pm,
+                                  const double2* __restrict__ hz, const double4* __restrict__ vel,
+                                  const double* __restrict__ rho, const double* __restrict__ omega,
+                                  const double* __restrict__ press, const double* __restrict__ sound,
+                                  double* __restrict__ pf, double* __restrict__ hf4,
+                                  double4* __restrict__ rec) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
+  const double r = rho[p];
+  const double pfv = ((press[p] / r) / r) / omega[p];
+  const double h = hz[p].x;
+  const double hfv = pow(1.0 / h, NDIMPLUS1);
+  pf[p] = pfv;
+  hf4[p] = hfv;
   const double4 v = vel[p];
   rec[3 * (size_t)p] = pm[p];
-  rec[3 * (size_t)p + 1] = make_double4(v.x, v.y, v.z, hz[p].x);
-  rec[3 * (size_t)p + 2] = make_double4(pf[p], hf4[p], sound[p], rho[p]);
+  rec[3 * (size_t)p + 1] = make_double4(v.x, v.y, v.z, h);
+  rec[3 * (size_t)p + 2] = make_double4(pfv, hfv, sound[p], r);
 }
 
-// PACKED: the neighbours' values come from k_hydro_pack's records (rec), else
+// PACKED: the neighbours' values come from k_hydro_prep_pack's records (rec), else
 // from the separate arrays (the form without a context keeps those)
 template <bool MIXED, int SUB, bool PACKED = false>
 __global__ void __launch_bounds__(128, 8) k_hydro(int nact, const int* __restrict__ act,
@@ -2599,9 +2608,6 @@ static void launch_neib_gsets(Ctx& c, bool sorted) {
 
 void launch_hydro(Ctx& c, int nact, double* amap) {
   if (nact <= 0) return;
-  k_hydro_prep<<<nb(c.ptot, 256), 256, 0, c.st>>>(c.ptot, c.hz, c.rho, c.omega, c.press, c.pf,
-                                                  c.hf4);
-  ++c.nlaunch;
   if (c.prm.precision != 0 && !c.hrec) {        // made on first use
     if (cudaMalloc(&c.hrec, sizeof(double4) * 3 * (size_t)c.pmax) != cudaSuccess) {
       cudaGetLastError();
@@ -2610,11 +2616,14 @@ void launch_hydro(Ctx& c, int nact, double* amap) {
       return;
     }
   }
-  if (c.prm.precision != 0) {
-    k_hydro_pack<<<nb(c.ptot, 256), 256, 0, c.st>>>(c.ptot, c.pm, c.hz, c.vel, c.pf, c.hf4,
-                                                    c.sound, c.rho, c.hrec);
-    ++c.nlaunch;
-  }
+  if (c.prm.precision != 0)
+    k_hydro_prep_pack<<<nb(c.ptot, 256), 256, 0, c.st>>>(c.ptot, c.pm, c.hz, c.vel, c.rho,
+                                                         c.omega, c.press, c.sound, c.pf, c.hf4,
+                                                         c.hrec);
+  else
+    k_hydro_prep<<<nb(c.ptot, 256), 256, 0, c.st>>>(c.ptot, c.hz, c.rho, c.omega, c.press, c.pf,
+                                                    c.hf4);
+  ++c.nlaunch;
   const HydroTree t = hydro_tree(c);
   const bool tc = c.prm.kernel == 1;
   auto go = [&](auto kern, int sub) {
